@@ -1,0 +1,322 @@
+"""Benchmark: images/s of Kheradpisheh-style 2-layer STDP training + forward.
+
+Workload (one step = one batch of 4096 synthetic 28x28 stroke images, the
+MNIST geometry of the reference's examples):
+  DoG(7x7, (1,2), (2,1), pad 3) -> rank code T=15 ->
+  conv1 30x5x5 pad 2 -> threshold 15 -> inhibit -> convwta(r3, k5) -> fire ->
+  STDP(0.004, -0.003) -> pool 2 ->
+  conv2 100x5x5 pad 2 -> threshold 10 -> inhibit -> convwta(r1, k8) -> fire ->
+  STDP(0.004, -0.003) -> global max pool (the features).
+
+``value``: images/s with the images already on the GPU; ``e2e``: the same
+through the public API from pinned host images, with the H2D copy of the
+images and the D2H copy of the features and both kernels inside the timed
+region.  ``--impl reference`` times the reference's CPU implementation (its
+own compiled CPU backend, oneDNN convolution through torch) on host cores.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BATCH, T, H = 4096, 15, 28
+METRIC = "images/s (STDP train + fwd), BF16-split vs FP32 on 1 B200; spike match %"
+WORKLOAD = "kheradpisheh-2layer-stdp: 4096 x 28x28 strokes, T=15, conv1 30x5x5 th15 r3k5, conv2 100x5x5 th10 r1k8"
+
+
+def flops_per_image():
+    c1 = 2 * T * 28 * 28 * 30 * 2 * 25
+    c2 = 2 * T * 14 * 14 * 100 * 30 * 25
+    return c1, c2
+
+
+# ----------------------------------------------------------------------------
+# clocks
+# ----------------------------------------------------------------------------
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index, self.samples, self.stop = index, [], threading.Event()
+
+    def _run(self):
+        while not self.stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                self.samples.append([v.strip() for v in out.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self.stop.wait(0.2)
+
+    def __enter__(self):
+        self.th = threading.Thread(target=self._run, daemon=True)
+        self.th.start()
+        return self
+
+    def __exit__(self, *a):
+        self.stop.set()
+        self.th.join(timeout=10)
+
+    def summary(self):
+        sm = [float(s[1]) for s in self.samples if len(s) >= 9 and s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if len(s) >= 9 and s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples if len(s) >= 9 for i in range(4) if "Active" in s[5 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+# ----------------------------------------------------------------------------
+# GPU arm
+# ----------------------------------------------------------------------------
+class Network:
+    def __init__(self, spyker, torch, dev, precision):
+        from spyker_b200 import synth
+
+        self.sp, self.torch = spyker, torch
+        self.dog = spyker.DoG(3, [spyker.DoGFilter(1, 2), spyker.DoGFilter(2, 1)], pad=3, device=dev)
+        self.conv1 = spyker.Conv(2, 30, 5, pad=2, device=dev)
+        self.conv2 = spyker.Conv(30, 100, 5, pad=2, device=dev)
+        self.conv1.kernel.copy_(torch.from_numpy(synth.conv_weights(30, 2, 5, seed=1)))
+        self.conv2.kernel.copy_(torch.from_numpy(synth.conv_weights(100, 30, 5, seed=2)))
+        for c in (self.conv1, self.conv2):
+            c.stdpconfig = [spyker.STDPConfig(0.004, -0.003)]
+            c.precision = precision
+        self.conv_events = []
+
+    def _conv(self, layer, x):
+        t = self.torch
+        a, b = t.cuda.Event(enable_timing=True), t.cuda.Event(enable_timing=True)
+        a.record()
+        y = layer(x)
+        b.record()
+        self.conv_events.append((a, b, layer))
+        return y
+
+    def step(self, images_f32):
+        sp = self.sp
+        codes = sp.code(self.dog(images_f32), T)
+        out1 = sp.inhibit(sp.threshold(self._conv(self.conv1, codes), 15.0))
+        spk1 = sp.fire(out1)
+        self.conv1.stdp(codes, sp.convwta(out1, 3, 5), spk1)
+        pooled = sp.pool(spk1, 2)
+        out2 = sp.inhibit(sp.threshold(self._conv(self.conv2, pooled), 10.0))
+        spk2 = sp.fire(out2)
+        self.conv2.stdp(pooled, sp.convwta(out2, 1, 8), spk2)
+        return sp.pool(spk2, 14)
+
+
+def gpu_arm(args, rank, world):
+    import torch
+
+    import spyker_b200 as spyker
+    from spyker_b200 import synth
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    imgs = synth.strokes(BATCH, seed=100 + rank)
+    host = torch.from_numpy(imgs).pin_memory()
+    dev_imgs = host.to(dev).float().div_(255.0)
+    net = Network(spyker, torch, dev, args.precision)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        net.step(dev_imgs)
+    barrier()
+    net.conv_events.clear()
+    l0 = spyker._lib.lib.spk_launch_count()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(dev.index) as clk:
+        barrier()
+        start.record()
+        for _ in range(args.steps):
+            net.step(dev_imgs)
+        end.record()
+        barrier()
+    launches = (spyker._lib.lib.spk_launch_count() - l0) // max(args.steps, 1)
+    ms = start.elapsed_time(end) / args.steps
+    conv_ms = {}
+    for a, b, layer in net.conv_events:
+        conv_ms.setdefault(id(layer), []).append(a.elapsed_time(b))
+    c1f, c2f = flops_per_image()
+    c1_ms = statistics.mean(conv_ms[id(net.conv1)])
+    c2_ms = statistics.mean(conv_ms[id(net.conv2)])
+
+    # end to end: pinned host images -> features on the host
+    feats = None
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    e0.record()
+    for _ in range(args.steps):
+        x = host.to(dev, non_blocking=True).float().div_(255.0)
+        feats = net.step(x).cpu()
+    e1.record()
+    barrier()
+    e2e_ms = e0.elapsed_time(e1) / args.steps
+
+    t_max = torch.tensor([ms, e2e_ms], device=dev)
+    if dist is not None:
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+        dist.destroy_process_group()
+    ms, e2e_ms = float(t_max[0]), float(t_max[1])
+    if rank != 0:
+        return
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    peak = peaks.get("bf16_tflops_sustained", 1390.0)
+    achieved = c2f * BATCH / (c2_ms * 1e-3) / 1e12
+    line = {
+        "metric": METRIC,
+        "value": BATCH * world / (ms * 1e-3),
+        "unit": "images/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": {"fp32": "f32", "bf16x2": "bf16x2-split/f32-acc", "bf16x3": "bf16x3-split/f32-acc"}[args.precision],
+        "data": "synthetic (seeded stroke images, MNIST geometry)",
+        "config": {"workload": WORKLOAD, "global_batch": BATCH * world, "seq_len": T, "parallelism": f"replicas{world}",
+                   "conv_precision": args.precision, "l2": "inputs larger than L2 (potentials 5.8 GB per layer)"},
+        "e2e": {"value": BATCH * world / (e2e_ms * 1e-3), "unit": "images/s", "h2d_bytes_per_step": BATCH * H * H,
+                "d2h_bytes_per_step": int(feats.numel() * feats.element_size())},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "tensor", "kernel": "conv2 (30->100, 5x5, M=12.0M, K=750)", "achieved": achieved,
+                     "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                     "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained (of measured)"},
+        "kernels_ms": {"conv1": c1_ms, "conv2": c2_ms, "rest": ms - c1_ms - c2_ms},
+        "clocks": clk.summary(),
+    }
+    if not args.no_cpu_baseline and world == 1:
+        line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------
+# CPU reference arm (the reference's own CPU backend)
+# ----------------------------------------------------------------------------
+def reference_step(o, torch, imgs, w1, w2, dk):
+    """The same pipeline with the reference's CPU code (oracle/_ref) and the
+    oneDNN convolution its CPU backend uses (through torch), in place."""
+    x = imgs.astype(np.float32) / np.float32(255)
+    dog = o.filter("dog", x[:, None], dk, (3, 3, 3, 3))
+    codes = o.rank_code(dog, T)
+    b = codes.shape[0]
+    f = torch.from_numpy(codes.reshape(b * T, 2, 28, 28).astype(np.float32))
+    p1 = torch.nn.functional.conv2d(f, torch.from_numpy(w1), padding=2).numpy().reshape(b, T, 30, 28, 28)
+    inh1 = o.inhibit(o.threshold(p1, 15.0))
+    s1 = o.fire(inh1)
+    win, cnt = o.convwta(inh1, (3, 3), 5)
+    w1[:] = o.convstdp(codes, w1, s1, [(0.004, -0.003, 1, 0, 1)], win, cnt, (1, 1), (2, 2, 2, 2))
+    q = o.pool(s1, (2, 2))
+    f2 = torch.from_numpy(q.reshape(b * T, 30, 14, 14).astype(np.float32))
+    p2 = torch.nn.functional.conv2d(f2, torch.from_numpy(w2), padding=2).numpy().reshape(b, T, 100, 14, 14)
+    inh2 = o.inhibit(o.threshold(p2, 10.0))
+    s2 = o.fire(inh2)
+    win, cnt = o.convwta(inh2, (1, 1), 8)
+    w2[:] = o.convstdp(q, w2, s2, [(0.004, -0.003, 1, 0, 1)], win, cnt, (1, 1), (2, 2, 2, 2))
+    return o.pool(s2, (14, 14))
+
+
+def _ref_setup():
+    import torch
+
+    import oracle
+    from spyker_b200 import synth
+    from tests.golden.make_golden import dog_kernel
+
+    kind = "reference" if oracle.available("reference") else "port"
+    o = oracle.get(kind)
+    torch.set_num_threads(os.cpu_count() or 1)
+    return o, kind, torch, synth, dog_kernel(o)
+
+
+def cpu_baseline(seconds: float) -> dict:
+    o, kind, torch, synth, dk = _ref_setup()
+    imgs = synth.strokes(64, seed=5)
+    w1, w2 = synth.conv_weights(30, 2, 5, seed=1), synth.conv_weights(100, 30, 5, seed=2)
+    reference_step(o, torch, imgs, w1, w2, dk)
+    n, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < seconds:
+        reference_step(o, torch, imgs, w1, w2, dk)
+        n += 64
+    dt = time.perf_counter() - t0
+    return {"value": n / dt, "unit": "images/s", "cores": torch.get_num_threads(), "kind": kind,
+            "sample": f"{n} images in batches of 64 through the same 2-layer pipeline, {dt:.1f} s"}
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    o, kind, torch, synth, dk = _ref_setup()
+    sample = 256
+    imgs = synth.strokes(sample, seed=100)
+    w1, w2 = synth.conv_weights(30, 2, 5, seed=1), synth.conv_weights(100, 30, 5, seed=2)
+    for _ in range(args.warmup):
+        reference_step(o, torch, imgs, w1, w2, dk)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        reference_step(o, torch, imgs, w1, w2, dk)
+    dt = (time.perf_counter() - t0) / args.steps
+    v = sample / dt
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "images/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded stroke images, MNIST geometry)",
+        "config": {"workload": WORKLOAD, "global_batch": BATCH, "seq_len": T, "parallelism": "cpu",
+                   "reference_sample_images_per_step": sample},
+        "cpu_baseline": {"value": v, "unit": "images/s", "cores": torch.get_num_threads(), "kind": kind,
+                         "sample": f"{sample} images per step through the same pipeline"},
+        "e2e": {"value": v, "unit": "images/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--precision", default=os.environ.get("SPYKER_BENCH_PRECISION", "fp32"),
+                    choices=["fp32", "bf16x2", "bf16x3"])
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", args.gpus if args.impl == "reference" else 1))
+    if args.impl == "reference":
+        reference_arm(args, rank, world)
+    else:
+        gpu_arm(args, rank, world)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,202 @@
+/*
+ * spyker_b200 — C ABI of the B200 (sm_100a) spiking-CNN hot path.
+ *
+ * Drop-in seam: each entry point replaces one `Core::cuda_<op>` /
+ * `Core::cpu_<op>` backend function of Spyker (declared through the
+ * `Declare(...)` table of src/spyker/impl.h:196-322 and the sparse table
+ * impl.h:328-356), with the same argument meaning, but over plain device
+ * pointers, sizes and a CUDA stream instead of Spyker's Dyn/Tensor types.
+ *
+ * Conventions
+ *  - Every pointer named `in`/`out`/`data`/`kernel`/`winners`/`counts`/`ws` is a
+ *    DEVICE pointer unless the comment says "host".
+ *  - Layouts are the reference's: spikes and potentials [B, T, C, H, W]
+ *    row-major; conv kernels [Cout, Cin, KH, KW]; pads are (top, left,
+ *    bottom, right) as in src/spyker/shape.cpp:35-50.
+ *  - Scalars (thresholds, fill values) are passed as double and converted to
+ *    the data type with a C cast, as the reference's Scalar does
+ *    (src/spyker/utils.cpp:290-295).
+ *  - Work is enqueued on `stream` (a cudaStream_t; NULL = legacy default).
+ *    Calls never synchronise the stream unless documented.
+ *  - Winners travel as int32 records [B, count, 5] = (c, t, z, y, x)
+ *    (src/spyker/utils.h:483-502) plus int32 per-sample counts [B].
+ *  - Entry points that need scratch memory take a caller-provided workspace
+ *    (`ws`, `ws_bytes`); the matching `_workspace` query returns the bytes
+ *    needed.  The library never allocates device memory on these paths.
+ *  - Return value: SPK_OK or an error code; spk_last_error() gives the
+ *    message of the calling thread's last failure.  Errors never throw.
+ */
+#ifndef SPYKER_B200_H
+#define SPYKER_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum
+{
+    SPK_OK = 0,
+    SPK_ERR_ARGUMENT = 1,    /* bad shape / size / pointer (reference: SpykerCompare throws) */
+    SPK_ERR_CUDA = 2,        /* a CUDA runtime call or launch failed */
+    SPK_ERR_UNSUPPORTED = 3, /* data type or option not supported by this build */
+    SPK_ERR_DEVICE = 4       /* a kernel reported an error through its device status word */
+} spk_status;
+
+/* Codes of the reference's `enum class Type` (src/spyker/utils.h:96-120). */
+typedef enum
+{
+    SPK_I8 = 0,
+    SPK_I16 = 1,
+    SPK_I32 = 2,
+    SPK_I64 = 3,
+    SPK_U8 = 4,
+    SPK_U16 = 5,
+    SPK_U32 = 6,
+    SPK_U64 = 7,
+    SPK_F16 = 8,
+    SPK_F32 = 9,
+    SPK_F64 = 10
+} spk_dtype;
+
+/* Arithmetic of the spike x weight contraction. */
+typedef enum
+{
+    SPK_CONV_FP32 = 0,   /* plain FP32 SIMT direct convolution */
+    SPK_CONV_BF16X2 = 1, /* tcgen05 tensor cores, weights split in BF16 hi+lo, FP32 accumulate */
+    SPK_CONV_BF16X3 = 2  /* tcgen05 tensor cores, three BF16 terms (exact for weights in [2^-6, 1]) */
+} spk_conv_precision;
+
+typedef void *spk_stream;
+
+/* ---- library ------------------------------------------------------------ */
+const char *spk_last_error(void);
+const char *spk_version(void);
+/* Number of CUDA devices, or -1 when the runtime is unusable. */
+int spk_device_count(void);
+/* Number of kernels this library has launched in the process (all threads). */
+uint64_t spk_launch_count(void);
+
+/* ---- host-side kernel generation (src/spyker/cpu/init.cpp) -------------- */
+/* Global generator: replaces Core::random_seed (src/spyker/impl.cpp:37-43). */
+void spk_random_seed(uint64_t seed);
+/* kernel ~ N(mean, std) from the global mt19937 (cpu/init.cpp:45-49). host. */
+spk_status spk_normal_kernel(double *kernel_host, int64_t n, double mean, double std);
+/* Normalised Gaussian (cpu/init.cpp:51-62). host, [size, size]. */
+spk_status spk_gaussian_kernel(double *kernel_host, int64_t size, double std);
+/* Normalised Gabor, theta in radians (cpu/init.cpp:64-77). host. */
+spk_status spk_gabor_kernel(double *kernel_host, int64_t size, double sigma, double theta, double gamma,
+                            double lambda, double psi);
+/* LoG kernel (cpu/init.cpp:79-90). host. */
+spk_status spk_log_kernel(double *kernel_host, int64_t size, double std);
+
+/* ---- coding (replaces Core::rank_code, impl.h:248; cpu/code.cpp:122) ---- */
+/* in [B, X], out [B, T, X] cumulative spikes.  sort!=0: rank order, ties in
+ * index order (stable); sort==0: latency code. */
+size_t spk_rank_code_workspace(int64_t b, int64_t x, int sort);
+spk_status spk_rank_code(const void *in, spk_dtype itype, void *out, spk_dtype otype, int64_t b, int64_t t, int64_t x,
+                         int sort, void *ws, size_t ws_bytes, spk_stream stream);
+
+/* ---- elementwise (impl.h:240-264; cpu/fire.cpp, cpu/time.cpp) ----------- */
+/* Core::threshold: in place, x <= threshold -> value. */
+spk_status spk_threshold(void *data, spk_dtype type, int64_t n, double threshold, double value, spk_stream stream);
+/* Core::rank_infinite: data [B, T, X], steps 0..T-2 set to value. */
+spk_status spk_rank_infinite(void *data, spk_dtype type, int64_t b, int64_t t, int64_t x, double value,
+                             spk_stream stream);
+/* Core::rank_fire: out = in > threshold. */
+spk_status spk_rank_fire(const void *in, spk_dtype itype, void *out, spk_dtype otype, int64_t n, double threshold,
+                         spk_stream stream);
+/* Core::rank_gather: in [B, T, X] -> out [B, X] first t with in > threshold (T if none). */
+spk_status spk_rank_gather(const void *in, spk_dtype itype, void *out, spk_dtype otype, int64_t b, int64_t t,
+                           int64_t x, double threshold, spk_stream stream);
+/* Core::rank_scatter: in [B, X] -> out [B, T, X] = (t >= in). */
+spk_status spk_rank_scatter(const void *in, spk_dtype itype, void *out, spk_dtype otype, int64_t b, int64_t t,
+                            int64_t x, spk_stream stream);
+/* Core::pad: in [N, H, W] -> out [N, H+top+bottom, W+left+right] (cpu/pool.cpp:41-51). */
+spk_status spk_pad(const void *in, void *out, spk_dtype type, int64_t n, int64_t h, int64_t w, const int64_t *pad4_host,
+                   double value, spk_stream stream);
+
+/* ---- pooling (Core::rank_pool, impl.h:268; cpu/pool.cpp:53-86) ---------- */
+/* in [N, H, W] planes -> out [N, OH, OW]; max over window, zero pad. */
+spk_status spk_rank_pool(const void *in, void *out, spk_dtype type, int64_t n, int64_t h, int64_t w, int64_t oh,
+                         int64_t ow, int64_t ky, int64_t kx, int64_t sy, int64_t sx, const int64_t *pad4_host,
+                         spk_stream stream);
+
+/* ---- lateral inhibition (Core::rank_inhibit, impl.h:272; cpu/inhibit.cpp) */
+/* data [B, T, C, X] in place. */
+spk_status spk_rank_inhibit(void *data, spk_dtype type, int64_t b, int64_t t, int64_t c, int64_t x, double threshold,
+                            spk_stream stream);
+
+/* ---- winner-take-all (Core::rank_convwta/rank_fcwta, impl.h:276-282) ---- */
+size_t spk_rank_convwta_workspace(int64_t b, int64_t t, int64_t c, int64_t h, int64_t w);
+/* in [B, T, C, H, W] -> winners [B, count, 5], counts [B] (cpu/wta.cpp:123-152). */
+spk_status spk_rank_convwta(const void *in, spk_dtype type, int64_t b, int64_t t, int64_t c, int64_t h, int64_t w,
+                            int64_t ry, int64_t rx, int64_t count, double threshold, int32_t *winners, int32_t *counts,
+                            void *ws, size_t ws_bytes, spk_stream stream);
+size_t spk_rank_fcwta_workspace(int64_t b, int64_t t, int64_t n);
+/* in [B, T, N] -> winners (x = neuron) (cpu/wta.cpp:72-96). */
+spk_status spk_rank_fcwta(const void *in, spk_dtype type, int64_t b, int64_t t, int64_t n, int64_t radius,
+                          int64_t count, double threshold, int32_t *winners, int32_t *counts, void *ws, size_t ws_bytes,
+                          spk_stream stream);
+
+/* ---- STDP (Core::rank_convstdp/rank_fcstdp, impl.h:284-296) -------------- */
+/* configs_host: [nconf, 5] = (positive, negative, stabilize, lower, upper),
+ * STDPConfig of src/spyker/utils.h:505-524 (nconf <= 16). */
+size_t spk_rank_convstdp_workspace(int64_t b, int64_t count, int64_t cin, int64_t kh, int64_t kw);
+/* in [B, T, Cin, H, W] spikes, kernel [Cout, Cin, KH, KW] F32 updated in place,
+ * out [B, T, Cout, OH, OW] spikes; sequential in (sample, winner) order per
+ * feature map (cpu/stdp.cpp:99-169). */
+spk_status spk_rank_convstdp(const void *in, spk_dtype itype, int64_t b, int64_t t, int64_t cin, int64_t h, int64_t w,
+                             float *kernel, int64_t cout, int64_t kh, int64_t kw, const void *out, int64_t oh,
+                             int64_t ow, const double *configs_host, int64_t nconf, const int32_t *winners,
+                             const int32_t *counts, int64_t count, int64_t sy, int64_t sx, const int64_t *pad4_host,
+                             void *ws, size_t ws_bytes, spk_stream stream);
+size_t spk_rank_fcstdp_workspace(int64_t b, int64_t t, int64_t ni);
+/* in [B, T, I], kernel [O, I] F32 in place, out [B, T, O] (cpu/stdp.cpp:42-97). */
+spk_status spk_rank_fcstdp(const void *in, spk_dtype itype, int64_t b, int64_t t, int64_t ni, float *kernel,
+                           int64_t no, const void *out, const double *configs_host, int64_t nconf,
+                           const int32_t *winners, const int32_t *counts, int64_t count, void *ws, size_t ws_bytes,
+                           spk_stream stream);
+
+/* ---- convolution (Core::conv, impl.h:224; cuda/conv.cu:257) ------------- */
+/* in [N, Cin, H, W] (U8 spikes or F32), kernel [Cout, Cin, KH, KW] F32,
+ * out [N, Cout, OH, OW] F32.  N folds batch and time. */
+size_t spk_conv_workspace(int64_t n, int64_t cin, int64_t h, int64_t w, int64_t cout, int64_t kh, int64_t kw,
+                          int precision);
+spk_status spk_conv(const void *in, spk_dtype itype, const float *kernel, float *out, int64_t n, int64_t cin, int64_t h,
+                    int64_t w, int64_t cout, int64_t kh, int64_t kw, int64_t sy, int64_t sx, const int64_t *pad4_host,
+                    int precision, void *ws, size_t ws_bytes, spk_stream stream);
+
+/* ---- fully connected (Core::fc / signfc, impl.h:228-236) ---------------- */
+/* in [R, I] (U8 or F32), kernel [O, I] F32 -> out [R, O] F32. */
+spk_status spk_fc(const void *in, spk_dtype itype, const float *kernel, float *out, int64_t r, int64_t ni, int64_t no,
+                  int sign, spk_stream stream);
+
+/* ---- filter banks (Core::dog/gabor/log, impl.h:200-212; cpu/dog.cpp) ---- */
+/* which: 0 DoG, 1 Gabor, 2 LoG.  in [N, H, W] F32 planes; kernel F32
+ * [2, F, KH, KW] (DoG, LoG) or [F, KH, KW] (Gabor); out [N, F or 2F, OH, OW]. */
+spk_status spk_filter(int which, const float *in, const float *kernel, float *out, int64_t n, int64_t h, int64_t w,
+                      int64_t f, int64_t kh, int64_t kw, int64_t oh, int64_t ow, const int64_t *pad4_host,
+                      spk_stream stream);
+
+/* ---- temporal backprop (Core::backward/labelize/fcbackward, impl.h:306-318) */
+/* in/out [B, N] F32 first-spike times; target [B] int64 (cpu/backprop.cpp:40-62). */
+spk_status spk_backward(const float *in, float *out, const int64_t *target, int64_t b, int64_t n, int64_t time,
+                        double gamma, spk_stream stream);
+/* in [B, T, N] -> out [B] int64 (cpu/backprop.cpp:68-99). */
+spk_status spk_labelize(const void *in, spk_dtype type, int64_t *out, int64_t b, int64_t t, int64_t n,
+                        double threshold, spk_stream stream);
+/* kernel [O, I] F32 updated; in [B, I], out/grad [B, O], next [B, I] F32;
+ * bp_host = (sfactor, lrate, lrf, lambda), sfactor updated on return
+ * (synchronises the stream) (cpu/backprop.cpp:105-160). */
+size_t spk_fcbackward_workspace(int64_t no, int64_t ni);
+spk_status spk_fcbackward(float *kernel, int64_t no, int64_t ni, const float *in, const float *out, const float *grad,
+                          float *next, int64_t b, float *bp_host, void *ws, size_t ws_bytes, spk_stream stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPYKER_B200_H */

@@ -1,0 +1,37 @@
+"""spyker_b200 — B200-native (sm_100a) spiking-CNN hot path with Spyker's API.
+
+``import spyker_b200 as spyker`` gives the names of the reference's Python
+package (src/python/spyker/__init__.py): coding, filters, Conv with
+``.stdp()``, fire/threshold/infinite, pool, inhibit, convwta/fcwta, the
+temporal-backprop helpers and the sparse event-list path.  Every operation
+runs on the GPU through the C ABI of ``include/spyker_b200.h``.
+"""
+
+from . import sparse
+from ._lib import SpykerError
+from .module import (FC, ZCA, BPConfig, Conv, DoG, DoGFilter, Gabor, GaborFilter, LoG, STDPConfig, Winner, Winners,
+                     backward, canny, code, conv, conv_precision, convwta, fc, fcwta, fire, gather, infinite,
+                     inhibit, labelize, pad, pool, quantize, random_seed, scatter, set_conv_precision, stdp,
+                     threshold)
+from .sparse import SparseTensor
+from .utils import copy_array, device, expand2, expand4, shape, to_numpy, to_tensor, to_torch
+
+__version__ = "0.1.0"
+
+
+def version() -> str:
+    from ._lib import lib
+
+    return lib.spk_version().decode()
+
+
+def cuda_available() -> bool:
+    import torch
+
+    return torch.cuda.is_available()
+
+
+def cuda_device_count() -> int:
+    from ._lib import lib
+
+    return max(0, int(lib.spk_device_count()))

@@ -1,0 +1,133 @@
+// DoG / Gabor / LoG filter banks (src/spyker/cpu/dog.cpp:40-94) and the FC
+// product (src/spyker/cpu/fc.cpp:140-171).
+//
+// Filters: every plane is correlated with every kernel in FP64 (one exact
+// sum per output, rounded once to F32, matching an exact convolution), then
+//   DoG  : out[f] = max(g1[f] - g2[f], 0)                (F32 arithmetic)
+//   Gabor: out[f] = g[f]
+//   LoG  : d = g1[f] - g2[f]; out[f] = max(d, 0); out[F + f] = max(-d, 0)
+// The rank code that follows orders these values, so they are produced
+// exactly rather than to a tolerance.
+#include "common.cuh"
+
+namespace spk
+{
+namespace
+{
+__device__ __forceinline__ double correlate(const float *__restrict__ plane, int h, int w, const float *__restrict__ k,
+                                            int kh, int kw, int y, int x, int top, int left)
+{
+    double acc = 0.0;
+    for (int a = 0; a < kh; ++a)
+    {
+        int yy = y + a - top;
+        if (yy < 0 || yy >= h) continue;
+        for (int b = 0; b < kw; ++b)
+        {
+            int xx = x + b - left;
+            if (xx < 0 || xx >= w) continue;
+            acc = fma(double(plane[yy * w + xx]), double(k[a * kw + b]), acc);
+        }
+    }
+    return acc;
+}
+
+__global__ void filter_kernel(int which, const float *__restrict__ in, const float *__restrict__ kernel,
+                              float *__restrict__ out, int64_t n, int h, int w, int f, int kh, int kw, int oh, int ow,
+                              int top, int left)
+{
+    const int64_t plane_out = int64_t(oh) * ow;
+    const int64_t total = n * f * plane_out;
+    const int fo = which == 2 ? 2 * f : f;
+    for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < total; k += int64_t(gridDim.x) * blockDim.x)
+    {
+        const int x = int(k % ow), y = int((k / ow) % oh), q = int((k / plane_out) % f);
+        const int64_t p = k / (plane_out * f);
+        const float *plane = in + p * h * w;
+        float *o = out + p * fo * plane_out + int64_t(y) * ow + x;
+        if (which == 1)
+        {
+            o[int64_t(q) * plane_out] = float(correlate(plane, h, w, kernel + q * kh * kw, kh, kw, y, x, top, left));
+        }
+        else
+        {
+            float g1 = float(correlate(plane, h, w, kernel + q * kh * kw, kh, kw, y, x, top, left));
+            float g2 = float(correlate(plane, h, w, kernel + (f + q) * kh * kw, kh, kw, y, x, top, left));
+            float d = __fsub_rn(g1, g2);
+            if (which == 0)
+                o[int64_t(q) * plane_out] = (d < 0.f) ? 0.f : d;  // std::max(d, 0)
+            else
+            {
+                float nd = -d;
+                o[int64_t(q) * plane_out] = (d < 0.f) ? 0.f : d;
+                o[int64_t(f + q) * plane_out] = (nd < 0.f) ? 0.f : nd;
+            }
+        }
+    }
+}
+
+template <typename I>
+__global__ void fc_kernel(const I *__restrict__ in, const float *__restrict__ kernel, float *__restrict__ out, int64_t r,
+                          int ni, int no, int sign)
+{
+    const int64_t total = r * no;
+    for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < total; k += int64_t(gridDim.x) * blockDim.x)
+    {
+        const int64_t row = k / no;
+        const int o = int(k % no);
+        const I *a = in + row * ni;
+        const float *wr = kernel + int64_t(o) * ni;
+        float acc = 0.f;
+        for (int i = 0; i < ni; ++i)
+        {
+            float wv = wr[i];
+            if (sign) wv = wv > 0.f ? 1.f : (wv < 0.f ? -1.f : 0.f);
+            acc = fmaf(float(a[i]), wv, acc);
+        }
+        out[k] = acc;
+    }
+}
+}  // namespace
+}  // namespace spk
+
+using namespace spk;
+
+extern "C" {
+
+spk_status spk_filter(int which, const float *in, const float *kernel, float *out, int64_t n, int64_t h, int64_t w,
+                      int64_t f, int64_t kh, int64_t kw, int64_t oh, int64_t ow, const int64_t *pad4,
+                      spk_stream stream)
+{
+    return guarded([&] {
+        Pad4 p = pad_of(pad4);
+        SPK_REQUIRE(which >= 0 && which <= 2, "unknown filter kind");
+        SPK_REQUIRE(n >= 0 && h >= 1 && w >= 1 && f >= 1 && kh >= 1 && kw >= 1, "invalid dims");
+        SPK_REQUIRE(oh == h + p.top + p.bottom - kh + 1 && ow == w + p.left + p.right - kw + 1 && oh > 0 && ow > 0,
+                    "input and kernel shapes are not compatible");
+        if (n == 0) return;
+        filter_kernel<<<grid_for(n * f * oh * ow, 256), 256, 0, stream_of(stream)>>>(
+            which, in, kernel, out, n, int(h), int(w), int(f), int(kh), int(kw), int(oh), int(ow), int(p.top),
+            int(p.left));
+        SPK_LAUNCHED();
+    });
+}
+
+spk_status spk_fc(const void *in, spk_dtype itype, const float *kernel, float *out, int64_t r, int64_t ni, int64_t no,
+                  int sign, spk_stream stream)
+{
+    return guarded([&] {
+        SPK_REQUIRE(r >= 0 && ni >= 1 && no >= 1, "invalid dims");
+        if (r == 0) return;
+        if (itype == SPK_U8)
+            fc_kernel<uint8_t><<<grid_for(r * no, 256), 256, 0, stream_of(stream)>>>((const uint8_t *)in, kernel, out,
+                                                                                   r, int(ni), int(no), sign);
+        else if (itype == SPK_F32)
+            fc_kernel<float><<<grid_for(r * no, 256), 256, 0, stream_of(stream)>>>((const float *)in, kernel, out, r,
+                                                                                 int(ni), int(no), sign);
+        else
+            throw Error(SPK_ERR_UNSUPPORTED, "fc input must be U8 or F32");
+        SPK_LAUNCHED();
+    });
+}
+
+}  // extern "C"
