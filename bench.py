@@ -76,7 +76,7 @@ class Clocks:
         sm = [float(s[1]) for s in self.samples if len(s) >= 9 and s[1].replace(".", "").isdigit()]
         mx = [float(s[2]) for s in self.samples if len(s) >= 9 and s[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples if len(s) >= 9 for i in range(4) if "Active" in s[5 + i]})
+        reasons = sorted({names[i] for s in self.samples if len(s) >= 9 for i in range(4) if s[5 + i] == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(self.samples)}
 
@@ -138,7 +138,7 @@ def gpu_arm(args, rank, world):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     imgs = synth.strokes(BATCH, seed=100 + rank)
     host = torch.from_numpy(imgs).pin_memory()
-    dev_imgs = host.to(dev).float().div_(255.0)
+    dev_imgs = host.to(dev).float().div_(255.0)[:, None]
     net = Network(spyker, torch, dev, args.precision)
 
     def barrier():
@@ -174,7 +174,7 @@ def gpu_arm(args, rank, world):
     barrier()
     e0.record()
     for _ in range(args.steps):
-        x = host.to(dev, non_blocking=True).float().div_(255.0)
+        x = host.to(dev, non_blocking=True).float().div_(255.0)[:, None]
         feats = net.step(x).cpu()
     e1.record()
     barrier()

@@ -304,7 +304,7 @@ def pad(array, pad=0, value: float = 0.0):
     s = to5(list(x.shape))
     oshape = shape.pad(s, p4)
     out = torch.empty(oshape, dtype=x.dtype, device=x.device)
-    call("spk_pad", ptr(x), type_code(x.dtype), ptr(out), s[0] * s[1] * s[2], s[3], s[4], i64(*p4), float(value),
+    call("spk_pad", ptr(x), ptr(out), type_code(x.dtype), s[0] * s[1] * s[2], s[3], s[4], i64(*p4), float(value),
          stream())
     return a.back(out)
 

@@ -66,6 +66,26 @@ def test_filters_exact(port):
     assert np.array_equal(host(gab(cuda(img))), port.filter("gabor", img, host(gab.kernel), (5, 5, 5, 5)))
 
 
+def stable_code(x: np.ndarray, time: int) -> np.ndarray:
+    """Rank code with ties in index order (the GPU's documented order):
+    cpu/code.cpp:93-101 with a stable sort, U16 conversion as x86-64 GCC."""
+    flat = x.reshape(x.shape[0], -1)
+    out = np.zeros((flat.shape[0], time, flat.shape[1]), np.uint8)
+    for i in range(flat.shape[0]):
+        v = flat[i].astype(np.float32)
+        v = np.where(v == 0, np.float32(0), v)
+        order = np.lexsort((np.arange(v.size), -v))
+        cnt = int((v > v.min()).sum())
+        with np.errstate(divide="ignore", invalid="ignore"):
+            scale = np.float32(np.float32(time) + np.float32(1e-5)) / np.float32(cnt)
+            prod = np.arange(v.size, dtype=np.float32) * scale
+        ok = (prod > -2.0 ** 31) & (prod < 2.0 ** 31)
+        tm = np.zeros(v.size, np.int64)
+        tm[order] = np.where(ok, np.trunc(np.where(ok, prod, 0)).astype(np.int64) & 0xFFFF, 0)
+        out[i] = tm[None, :] <= np.arange(time)[:, None]
+    return out.reshape((x.shape[0], time) + x.shape[1:])
+
+
 @pytest.mark.parametrize("sort", [True, False])
 def test_code(port, dog, sort):
     got = host(spyker.code(cuda(dog), 15, sort=sort))
@@ -75,29 +95,24 @@ def test_code(port, dog, sort):
         return
     # Sorted: exact except for equal values split across a time bin, where the
     # reference's std::sort order is not stable; the GPU order is (value desc,
-    # index asc), which the stable restatement reproduces exactly.
+    # index asc), reproduced exactly by the stable restatement.
     match = (got == want).mean()
     assert match > 0.9999
-    stable = np.zeros_like(want)
-    flat = dog.reshape(dog.shape[0], -1)
-    for i in range(flat.shape[0]):
-        order = np.lexsort((np.arange(flat.shape[1]), -flat[i]))
-        cnt = int((flat[i] > flat[i].min()).sum())
-        scale = np.float32(np.float32(15) + np.float32(1e-5)) / np.float32(cnt)
-        tm = np.empty(flat.shape[1], np.int64)
-        tm[order] = (np.arange(flat.shape[1], dtype=np.float32) * scale).astype(np.int64)
-        stable[i] = (tm[None, :] <= np.arange(15)[:, None]).reshape(stable[i].shape)
-    assert np.array_equal(got, stable)
+    assert np.array_equal(got, stable_code(dog, 15))
 
 
 def test_code_u8_and_edges(port):
     img = synth.strokes(16, seed=3)
     assert np.array_equal(host(spyker.code(cuda(img), 10, sort=False)), port.rank_code(img, 10, False))
+    assert np.array_equal(host(spyker.code(cuda(img), 10)), stable_code(img, 10))
     const = np.ones((3, 50), np.float32)
     assert np.array_equal(host(spyker.code(cuda(const), 15)), port.rank_code(const, 15))
+    # one value above a large tied minimum: the time conversion wraps
     one = np.zeros((2, 9000), np.float32)
     one[:, 5] = 2.0
-    assert np.array_equal(host(spyker.code(cuda(one), 15)), port.rank_code(one, 15))
+    assert np.array_equal(host(spyker.code(cuda(one), 15)), stable_code(one, 15))
+    tiny = np.array([[3.0]], np.float32)
+    assert np.array_equal(host(spyker.code(cuda(tiny), 4)), port.rank_code(tiny, 4))
 
 
 def test_threshold_fire_infinite(port, layer):
@@ -249,7 +264,7 @@ def test_backprop_helpers(port, golden):
 def test_golden_pipeline_ops(golden):
     """Each GPU op on the reference's own intermediate results."""
     dog = spyker.DoG(3, [spyker.DoGFilter(1, 2), spyker.DoGFilter(2, 1)], pad=3)
-    img = cuda(golden["images"].astype(np.float32) / np.float32(255))
+    img = cuda(golden["images"][:, None].astype(np.float32) / np.float32(255))
     d = dog(img)
     assert np.array_equal(host(d), golden["dog"])
     c = spyker.code(d, 15, sort=False)
@@ -271,7 +286,7 @@ def test_golden_pipeline_ops(golden):
 def test_end_to_end_layer(port, golden):
     """DoG -> code -> conv -> threshold -> inhibit -> WTA -> fire -> STDP on
     the GPU (FP32 conv) against the reference's results for the same images."""
-    img = cuda(golden["images"].astype(np.float32) / np.float32(255))
+    img = cuda(golden["images"][:, None].astype(np.float32) / np.float32(255))
     dog = spyker.DoG(3, [spyker.DoGFilter(1, 2), spyker.DoGFilter(2, 1)], pad=3)
     codes = spyker.code(dog(img), 15)
     code_match = (host(codes) == golden["codes"]).mean()
