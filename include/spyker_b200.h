@@ -153,6 +153,21 @@ spk_status spk_rank_convstdp(const void *in, spk_dtype itype, int64_t b, int64_t
                              int64_t ow, const double *configs_host, int64_t nconf, const int32_t *winners,
                              const int32_t *counts, int64_t count, int64_t sy, int64_t sx, const int64_t *pad4_host,
                              void *ws, size_t ws_bytes, spk_stream stream);
+/* No counterpart in the reference.  The same update as spk_rank_convstdp for
+ * callers that cannot allocate device memory (e.g. code that must not call
+ * cudaMalloc while a CUDA graph is being captured, or hosts whose allocator
+ * owns the device): its scratch lives in a static 32 MiB device array that
+ * every GPU loading the library holds until exit, so the call allocates
+ * nothing.  Calls needing more scratch than that (see
+ * spk_rank_convstdp_workspace) fail with SPK_ERR_ARGUMENT; split the batch.
+ * The first call on a device looks up the array's device address; make that
+ * first call before any stream capture.  All calls share the array, so calls
+ * that overlap on the GPU (different streams, or other threads) race. */
+spk_status spk_rank_convstdp_noalloc(const void *in, spk_dtype itype, int64_t b, int64_t t, int64_t cin, int64_t h,
+                                     int64_t w, float *kernel, int64_t cout, int64_t kh, int64_t kw, const void *out,
+                                     int64_t oh, int64_t ow, const double *configs_host, int64_t nconf,
+                                     const int32_t *winners, const int32_t *counts, int64_t count, int64_t sy,
+                                     int64_t sx, const int64_t *pad4_host, spk_stream stream);
 size_t spk_rank_fcstdp_workspace(int64_t b, int64_t t, int64_t ni);
 /* in [B, T, I], kernel [O, I] F32 in place, out [B, T, O] (cpu/stdp.cpp:42-97). */
 spk_status spk_rank_fcstdp(const void *in, spk_dtype itype, int64_t b, int64_t t, int64_t ni, float *kernel,

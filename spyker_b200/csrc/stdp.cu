@@ -199,6 +199,40 @@ Configs make_configs(const double *c, int64_t n)
 
 inline size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 }  // namespace
+
+// Conv STDP with the (pre, post) scratch at a given device address; used by
+// the entry point that draws its scratch from a static device array.
+void convstdp_into(const void *in, spk_dtype itype, int64_t b, int64_t t, int64_t cin, int64_t h, int64_t w,
+                   float *kernel, int64_t cout, int64_t kh, int64_t kw, const void *out, int64_t oh, int64_t ow,
+                   const double *configs, int64_t nconf, const int32_t *winners, const int32_t *counts, int64_t count,
+                   int64_t sy, int64_t sx, const int64_t *pad4, void *scratch, cudaStream_t s)
+{
+    Pad4 p = pad_of(pad4);
+    Configs cfg = make_configs(configs, nconf);
+    SPK_REQUIRE(b >= 0 && t >= 1 && t < 65535 && cin >= 1 && cout >= 1 && kh >= 1 && kw >= 1, "invalid dims");
+    SPK_REQUIRE(count >= 1, "winner count must be positive");
+    SPK_REQUIRE(oh == (h + p.top + p.bottom - kh) / sy + 1 && ow == (w + p.left + p.right - kw) / sx + 1,
+                "tensor shapes are not compatible");
+    if (b == 0) return;
+    const int64_t k = cin * kh * kw;
+    uint16_t *pre = reinterpret_cast<uint16_t *>(scratch);
+    uint16_t *post = reinterpret_cast<uint16_t *>(static_cast<char *>(scratch) + align256(size_t(b * count * k) * 2));
+    if (itype == SPK_U8)
+        conv_prepost_kernel<uint8_t><<<unsigned(b * count), 128, 0, s>>>(
+            (const uint8_t *)in, (const uint8_t *)out, int(t), int(cin), int(h), int(w), int(cout), int(oh), int(ow),
+            int(kh), int(kw), int(sy), int(sx), int(p.top), int(p.left), winners, counts, int(count), pre, post);
+    else if (itype == SPK_F32)
+        conv_prepost_kernel<float><<<unsigned(b * count), 128, 0, s>>>(
+            (const float *)in, (const float *)out, int(t), int(cin), int(h), int(w), int(cout), int(oh), int(ow),
+            int(kh), int(kw), int(sy), int(sx), int(p.top), int(p.left), winners, counts, int(count), pre, post);
+    else
+        throw Error(SPK_ERR_UNSUPPORTED, "STDP spikes must be U8 or F32");
+    SPK_LAUNCHED();
+    dim3 grid(unsigned(cout), unsigned(ceil_div(k, kScanChunk)));
+    stdp_scan_kernel<<<grid, kScanThreads, 0, s>>>(kernel, k, b, int(count), 2, winners, counts, pre, count * k, k,
+                                                   post, cfg);
+    SPK_LAUNCHED();
+}
 }  // namespace spk
 
 using namespace spk;
