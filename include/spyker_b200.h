@@ -78,6 +78,9 @@ const char *spk_version(void);
 int spk_device_count(void);
 /* Number of kernels this library has launched in the process (all threads). */
 uint64_t spk_launch_count(void);
+/* Device status word of the tensor-core kernels: 0 = no error, 1 = a bounded
+ * wait timed out.  Synchronous; reset != 0 clears it. */
+int spk_device_status(int reset);
 
 /* ---- host-side kernel generation (src/spyker/cpu/init.cpp) -------------- */
 /* Global generator: replaces Core::random_seed (src/spyker/impl.cpp:37-43). */

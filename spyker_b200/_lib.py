@@ -23,6 +23,7 @@ SIGNATURES = {
     "spk_version": (C.c_char_p, []),
     "spk_device_count": (_INT, []),
     "spk_launch_count": (C.c_uint64, []),
+    "spk_device_status": (_INT, [_INT]),
     "spk_random_seed": (None, [C.c_uint64]),
     "spk_normal_kernel": (_INT, [_P, _I, _D, _D]),
     "spk_gaussian_kernel": (_INT, [_P, _I, _D]),

@@ -276,6 +276,8 @@ def conv(array, kernel, stride=1, pad=0, precision: str | None = None):
     if x.dtype not in (torch.uint8, torch.float32):
         x = x.float()
     prec = _PRECISION[precision or _conv_precision]
+    if x.dtype != torch.uint8:
+        prec = _PRECISION["fp32"]  # the BF16-split tensor-core path is exact only for u8 spike inputs
     n = s[0] * s[1]
     nb = _lib.lib.spk_conv_workspace(n, s[2], s[3], s[4], k.shape[0], k.shape[2], k.shape[3], prec)
     ws, wsb = _workspace(nb, x.device)

@@ -305,3 +305,78 @@ def test_end_to_end_layer(port, golden):
     if spike_match == 1.0:
         rec, cnt = winners_np(wins)
         assert np.array_equal(cnt, golden["counts"])
+
+
+# ---------------------------------------------------------------------------
+# tcgen05 BF16-split convolution
+# ---------------------------------------------------------------------------
+
+def _tc_case(port, seed, n, t, cin, h, w, cout, k, stride, pad, lo=0.5, hi=1.0):
+    rng = np.random.default_rng(seed)
+    fst = rng.integers(0, t + 3, size=(n, cin, h, w))
+    spikes = (fst[:, None] <= np.arange(t)[None, :, None, None, None]).astype(np.uint8)
+    wts = rng.uniform(lo, hi, size=(cout, cin, k, k)).astype(np.float32)
+    exact = port.conv(spikes, wts, stride, pad, out_dtype=np.float32)
+    ref64 = port.conv(spikes, wts.astype(np.float64), stride, pad, out_dtype=np.float64)
+    return spikes, wts, exact, ref64
+
+
+TC_SHAPES = [
+    # n, t, cin, h, w, cout, k, stride, pad
+    (4, 15, 2, 28, 28, 30, 5, (1, 1), (2, 2, 2, 2)),
+    (3, 15, 30, 14, 14, 100, 5, (1, 1), (2, 2, 2, 2)),
+    (2, 5, 7, 19, 23, 37, 3, (2, 1), (1, 0, 2, 3)),
+    (1, 4, 16, 12, 12, 256, 5, (1, 1), (2, 2, 2, 2)),
+]
+
+
+@pytest.mark.parametrize("shape_", TC_SHAPES)
+def test_conv_tc_bf16x3_exact(port, shape_):
+    n, t, cin, h, w, cout, k, stride, pad = shape_
+    spikes, wts, exact, _ = _tc_case(port, 17, n, t, cin, h, w, cout, k, stride, pad)
+    spyker._lib.lib.spk_device_status(1)
+    got = host(spyker.conv(cuda(spikes), cuda(wts), stride, pad, precision="bf16x3"))
+    assert spyker._lib.lib.spk_device_status(1) == 0
+    assert got.shape == exact.shape
+    assert np.array_equal(got, exact), f"{int((got != exact).sum())} of {got.size} potentials differ"
+
+
+@pytest.mark.parametrize("shape_", TC_SHAPES[:3])
+def test_conv_tc_bf16x2_tolerance(port, shape_):
+    n, t, cin, h, w, cout, k, stride, pad = shape_
+    spikes, wts, _, ref64 = _tc_case(port, 23, n, t, cin, h, w, cout, k, stride, pad, lo=0.0, hi=1.0)
+    got = host(spyker.conv(cuda(spikes), cuda(wts), stride, pad, precision="bf16x2"))
+    rel = np.abs(got - ref64) / np.maximum(np.abs(ref64), 1e-30)
+    assert rel.max() <= 1e-5
+    assert spyker._lib.lib.spk_device_status(1) == 0
+
+
+def test_conv_tc_small_weights_tolerance(port):
+    # weights spanning eight decades: partial sums are no longer exact, but
+    # the potentials stay within the 1e-5 relative bound of the FP64 oracle
+    spikes, _, _, _ = _tc_case(port, 5, 2, 15, 30, 14, 14, 100, 5, (1, 1), (2, 2, 2, 2))
+    rng = np.random.default_rng(6)
+    wts = (10.0 ** rng.uniform(-8, 0, size=(100, 30, 5, 5))).astype(np.float32)
+    ref64 = port.conv(spikes, wts.astype(np.float64), (1, 1), (2, 2, 2, 2), out_dtype=np.float64)
+    got = host(spyker.conv(cuda(spikes), cuda(wts), 1, 2, precision="bf16x3"))
+    rel = np.abs(got - ref64) / np.maximum(np.abs(ref64), 1e-30)
+    assert rel.max() <= 1e-5
+
+
+def test_end_to_end_layer_bf16x3(golden):
+    """With the exact tensor-core conv the whole layer matches the reference."""
+    codes = cuda(golden["codes"])
+    conv = spyker.Conv(2, 30, 5, pad=2)
+    conv.kernel.copy_(cuda(golden["kernel"]))
+    conv.stdpconfig = [spyker.STDPConfig(0.004, -0.003)]
+    conv.precision = "bf16x3"
+    out = spyker.inhibit(spyker.threshold(conv(codes), 15.0))
+    spk = spyker.fire(out)
+    assert np.array_equal(host(spk), golden["fire"])
+    wins = spyker.convwta(out, 3, 5)
+    rec, cnt = winners_np(wins)
+    assert np.array_equal(cnt, golden["counts"])
+    assert np.array_equal(rec, oracle_winners(golden["winners"], golden["counts"])[0])
+    conv.stdp(codes, wins, spk)
+    assert np.array_equal(host(conv.kernel), golden["stdp_kernel"])
+    assert np.array_equal(host(spyker.pool(spk, 2)), golden["pooled"])
