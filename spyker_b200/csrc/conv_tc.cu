@@ -2,22 +2,29 @@
 //
 // Implicit GEMM: D[m, n] = sum_k A[m, k] * W[n, k] with
 //   m = (image, oy, ox) over N*OH*OW output positions (N folds batch, time),
-//   k = (c, ky, kx) over Cin*KH*KW (the reference's kernel flattening),
-//   A[m, k] = spike u8 of the receptive field (0/1, exact in BF16).
+//   k = a receptive-field tap (ky, kx) and input channel c,
+//   A[m, k] = spike u8 of the receptive field (exact in BF16).
 // Each F32 weight is split into BF16 terms w = h + m (+ l) (h = bf16(w),
 // m = bf16(w - h), l = bf16(w - h - m)); every term gets its own FP32
 // accumulator in tensor memory, so each partial sum stays exact for weights
-// in [2^-6, 1] and the terms are added once in FP64 and rounded once to F32:
-// BF16X3 reproduces the exactly rounded potential, BF16X2 (hi+lo) is within
-// 2^-18 relative.
+// in [2^-6, 1]; the terms are added once in FP64 and rounded once to F32.
+// BF16X3 therefore reproduces the exactly rounded potential; BF16X2 (hi+lo)
+// is within 2^-18 relative.
 //
-// CTA (persistent, 128 threads): per 128-row M tile and N tile, K is walked in
-// 64-wide blocks through a two-stage shared-memory ring.  All threads gather
-// the A block (u8 -> BF16) into the K-major no-swizzle canonical layout; the
-// pre-split weight block is already stored in global memory in exactly that
-// layout and is copied with 16-byte loads.  Thread 0 issues the tcgen05.mma
+// Two A layouts:
+//  * channels-last (Cin >= 8): the spikes are first transposed to
+//    [N, H, W, Cpad] u8 (Cpad = Cin rounded up to 8) and k = tap * Cpad + c,
+//    so every 8-wide K chunk of a row is one 8-byte load;
+//  * channel-major (Cin < 8): k = c * KH*KW + tap (the reference's order),
+//    gathered element by element (keeps K small for 1-2 input channels).
+//
+// CTA (persistent, 256 threads) per 128-row M tile and N tile walks K in
+// 64-wide blocks through a two-stage shared-memory ring: thread 0 starts a
+// bulk copy (TMA engine, no multicast) of the pre-split weight block, stored
+// in global memory in the K-major no-swizzle canonical layout, while all
+// threads gather the A block; thread 0 then issues the tcgen05.mma
 // instructions (M=128, N=n_tile, K=16) and commits them to the stage's
-// mbarrier; the epilogue reads the accumulators with tcgen05.ld.  Every
+// mbarrier.  The epilogue reads the accumulators with tcgen05.ld.  Every
 // mbarrier wait is bounded: on timeout the kernel records an error in the
 // device status word (spk_device_status) and leaves.
 #include <algorithm>
@@ -35,33 +42,71 @@ namespace
 {
 using namespace tc;
 
-constexpr int BM = 128, BK = 64, kTcThreads = 128;
+constexpr int BM = 128, BK = 64, kTcThreads = 256;
 constexpr uint32_t kMaxProbes = 1u << 22;
-constexpr int kMaxK = 4096;
+constexpr int kMaxKBlocks = 128;  // K up to 8192
 
 struct TcParams
 {
-    const uint8_t *in;
-    const uint4 *wimg;
+    const uint8_t *in;  // channel-major input, or its channels-last copy
+    const uint8_t *wimg;
     float *out;
-    int64_t M, tiles, chw, ohw;
+    int64_t M, tiles, img_stride, ohw;
     int cin, h, w, cout, kh, kw, oh, ow, sy, sx, top, left;
-    int K, kblocks, n_tile, n_tiles, nsplit;
+    int kblocks, n_tile, n_tiles, nsplit, cpad, nhwc;
     uint32_t tmem_cols, idesc;
 };
 
-__device__ __forceinline__ uint32_t bf16_bits(float v)
+__device__ __forceinline__ uint32_t bf16_of_byte(uint32_t b)
 {
-    return uint32_t(__bfloat16_as_ushort(__float2bfloat16_rn(v)));
+    // exact: float(b) for b < 256 has at most 8 significant bits
+    return __float_as_uint(__uint_as_float(0x4B000000u | b) - 8388608.0f) >> 16;
 }
 
-// Weight images: [n_tiles][kblocks][nsplit][n_tile x 64] BF16 in the
-// K-major no-swizzle layout (8-row groups of 1024 B, 8 K-chunks of 128 B,
-// 16 B per row).  One thread per (n_tile block, k block, row, K chunk).
-__global__ void split_weights_kernel(const float *__restrict__ kernel, uint4 *__restrict__ wimg, int cout, int K,
-                                     int kblocks, int n_tile, int n_tiles, int nsplit)
+__device__ __forceinline__ uint4 bf16x8_of_bytes(uint2 v)
+{
+    uint4 r;
+    r.x = bf16_of_byte(v.x & 0xFF) | (bf16_of_byte((v.x >> 8) & 0xFF) << 16);
+    r.y = bf16_of_byte((v.x >> 16) & 0xFF) | (bf16_of_byte(v.x >> 24) << 16);
+    r.z = bf16_of_byte(v.y & 0xFF) | (bf16_of_byte((v.y >> 8) & 0xFF) << 16);
+    r.w = bf16_of_byte((v.y >> 16) & 0xFF) | (bf16_of_byte(v.y >> 24) << 16);
+    return r;
+}
+
+// [N, C, H, W] -> [N, H, W, Cpad] (zero-filled pad channels), 8 channels per thread.
+__global__ void to_channels_last_kernel(const uint8_t *__restrict__ in, uint2 *__restrict__ out, int64_t n, int c,
+                                        int64_t hw, int cpad)
+{
+    const int groups = cpad / 8;
+    const int64_t total = n * hw * groups;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += int64_t(gridDim.x) * blockDim.x)
+    {
+        const int g = int(i % groups);
+        const int64_t px = (i / groups) % hw, img = i / (int64_t(groups) * hw);
+        const uint8_t *src = in + img * c * hw + px;
+        uint32_t lo = 0, hi = 0;
+#pragma unroll
+        for (int e = 0; e < 8; ++e)
+        {
+            const int ch = g * 8 + e;
+            const uint32_t v = ch < c ? src[int64_t(ch) * hw] : 0u;
+            if (e < 4)
+                lo |= v << (8 * e);
+            else
+                hi |= v << (8 * (e - 4));
+        }
+        out[i] = make_uint2(lo, hi);
+    }
+}
+
+// Weight images: [n_tiles][kblocks][nsplit][n_tile x 64] BF16 in the K-major
+// no-swizzle layout (8-row groups of 1024 B, 8 K-chunks of 128 B, 16 B per
+// row), K ordered as the A operand.  One thread per (tile, block, row, chunk).
+__global__ void split_weights_kernel(const float *__restrict__ kernel, uint4 *__restrict__ wimg, int cout, int cin,
+                                     int taps, int nhwc, int cpad, int kblocks, int n_tile, int n_tiles, int nsplit)
 {
     const int64_t total = int64_t(n_tiles) * kblocks * n_tile * 8;
+    const int kreal = nhwc ? taps * cpad : taps * cin;
     for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += int64_t(gridDim.x) * blockDim.x)
     {
         const int kc = int(i % 8);
@@ -73,25 +118,31 @@ __global__ void split_weights_kernel(const float *__restrict__ kernel, uint4 *__
 #pragma unroll
         for (int e = 0; e < 8; e += 2)
         {
-            uint32_t lo[3], hi[3];
+            uint32_t bits[2][3];
 #pragma unroll
             for (int q = 0; q < 2; ++q)
             {
                 const int k = kb * BK + kc * 8 + e + q;
-                const float wv = (n < cout && k < K) ? kernel[int64_t(n) * K + k] : 0.f;
+                float wv = 0.f;
+                if (n < cout && k < kreal)
+                {
+                    int c, tap;
+                    if (nhwc)
+                        tap = k / cpad, c = k % cpad;
+                    else
+                        c = k / taps, tap = k % taps;
+                    if (c < cin) wv = kernel[(int64_t(n) * cin + c) * taps + tap];
+                }
                 const __nv_bfloat16 h = __float2bfloat16_rn(wv);
                 const float r1 = __fsub_rn(wv, __bfloat162float(h));
                 const __nv_bfloat16 m = __float2bfloat16_rn(r1);
                 const float r2 = __fsub_rn(r1, __bfloat162float(m));
                 const __nv_bfloat16 l = __float2bfloat16_rn(r2);
-                const uint32_t b0 = __bfloat16_as_ushort(h), b1 = __bfloat16_as_ushort(m), b2 = __bfloat16_as_ushort(l);
-                if (q == 0)
-                    lo[0] = b0, lo[1] = b1, lo[2] = b2;
-                else
-                    hi[0] = b0, hi[1] = b1, hi[2] = b2;
+                bits[q][0] = __bfloat16_as_ushort(h), bits[q][1] = __bfloat16_as_ushort(m);
+                bits[q][2] = __bfloat16_as_ushort(l);
             }
 #pragma unroll
-            for (int p = 0; p < 3; ++p) parts[p][e / 2] = lo[p] | (hi[p] << 16);
+            for (int p = 0; p < 3; ++p) parts[p][e / 2] = bits[0][p] | (bits[1][p] << 16);
         }
         const int64_t block = (int64_t(nt) * kblocks + kb) * nsplit;
         for (int p = 0; p < nsplit; ++p)
@@ -110,30 +161,62 @@ __device__ __forceinline__ bool wait_bounded(uint64_t *bar, uint32_t parity)
     return false;
 }
 
+__device__ __forceinline__ void arrive_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+// Bulk (non-tensor) global -> shared copy completing on `bar`; both addresses
+// 16-byte aligned, size a multiple of 16.
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
 __global__ void __launch_bounds__(kTcThreads, 1) conv_tc_kernel(TcParams P)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
-    __shared__ __align__(8) uint64_t mbar[2];
+    __shared__ __align__(8) uint64_t full_bar[2], done_bar[2];
     __shared__ uint32_t tmem_slot;
 
     const int tid = threadIdx.x, warp = tid >> 5;
+    const int row = tid & (BM - 1);
+    const int chunk0 = (tid >> 7) * 4;  // this thread gathers K chunks chunk0..chunk0+3 of its row
     const int a_bytes = BM * BK * 2;                  // 16 KB
     const int b_bytes = P.nsplit * P.n_tile * BK * 2;  // nsplit x n_tile x 128 B
-    unsigned char *sA[2] = {smem, smem + a_bytes};
-    unsigned char *sB[2] = {smem + 2 * a_bytes, smem + 2 * a_bytes + b_bytes};
+    unsigned char *const sA0 = smem;
+    unsigned char *const sB0 = smem + 2 * a_bytes;
     int4 *tab = reinterpret_cast<int4 *>(smem + 2 * a_bytes + 2 * b_bytes);
+    const int taps = P.kh * P.kw;
 
-    // k -> (offset within the image block, ky, kx, valid)
-    for (int k = tid; k < P.kblocks * BK; k += blockDim.x)
+    if (P.nhwc)
     {
-        const int khw = P.kh * P.kw;
-        const int c = k / khw, r = k % khw, ky = r / P.kw, kx = r % P.kw;
-        tab[k] = make_int4(c * P.h * P.w + ky * P.w + kx, ky, kx, k < P.K ? 1 : 0);
+        // one entry per 8-wide K chunk: (ky, kx, channel offset, valid)
+        const int groups = P.cpad / 8;
+        for (int q = tid; q < P.kblocks * 8; q += blockDim.x)
+        {
+            const int tap = q / groups, g = q % groups;
+            tab[q] = make_int4(tap / P.kw, tap % P.kw, g * 8, tap < taps ? 1 : 0);
+        }
+    }
+    else
+    {
+        // one entry per k: (offset in the image, ky, kx, valid)
+        for (int k = tid; k < P.kblocks * BK; k += blockDim.x)
+        {
+            const int c = k / taps, tap = k % taps, ky = tap / P.kw, kx = tap % P.kw;
+            tab[k] = make_int4(c * P.h * P.w + ky * P.w + kx, ky, kx, c < P.cin ? 1 : 0);
+        }
     }
     if (tid == 0)
     {
-        mbar_init(&mbar[0], 1);
-        mbar_init(&mbar[1], 1);
+        mbar_init(&full_bar[0], 1);
+        mbar_init(&full_bar[1], 1);
+        mbar_init(&done_bar[0], 1);
+        mbar_init(&done_bar[1], 1);
         fence_mbar_init();
     }
     if (warp == 0)
@@ -150,11 +233,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) conv_tc_kernel(TcParams P)
     uint32_t it = 0;
     bool failed = false;
 
-    for (int64_t tile = blockIdx.x; tile < P.tiles && !failed; tile += gridDim.x)
+    for (int64_t tile = blockIdx.x; tile < P.tiles; tile += gridDim.x)
     {
         const int64_t mt = tile / P.n_tiles;
         const int nt = int(tile % P.n_tiles);
-        const int64_t m = mt * BM + tid;
+        const int64_t m = mt * BM + row;
         const bool row_ok = m < P.M;
         int64_t img = 0, pix = 0;
         int iy0 = 0, ix0 = 0;
@@ -166,55 +249,86 @@ __global__ void __launch_bounds__(kTcThreads, 1) conv_tc_kernel(TcParams P)
             iy0 = oy * P.sy - P.top;
             ix0 = ox * P.sx - P.left;
         }
-        const int64_t rowoff = img * P.chw + int64_t(iy0) * P.w + ix0;
+        const uint8_t *img_base = P.in + img * P.img_stride;
 
         for (int kb = 0; kb < P.kblocks; ++kb, ++it)
         {
             const int st = it & 1;
+            unsigned char *sA = sA0 + st * a_bytes;
+            unsigned char *sB = sB0 + st * b_bytes;
+            bool ok = true;
             if (waited[st] < uses[st])
             {
-                const bool ok = wait_bounded(&mbar[st], (uses[st] - 1) & 1);
-                if (__syncthreads_or(!ok))
-                {
-                    failed = true;
-                    break;
-                }
+                ok = wait_bounded(&done_bar[st], (uses[st] - 1) & 1);
                 waited[st] = uses[st];
             }
-            // A block: row tid, 8 chunks of 8 K values.
-            unsigned char *a = sA[st] + (tid / 8) * 1024 + (tid % 8) * 16;
-#pragma unroll 2
-            for (int kc = 0; kc < 8; ++kc)
+            if (__syncthreads_or(!ok))
             {
-                uint32_t pk[4];
-#pragma unroll
-                for (int e = 0; e < 8; e += 2)
-                {
-                    uint32_t v2[2];
-#pragma unroll
-                    for (int q = 0; q < 2; ++q)
-                    {
-                        const int4 t = tab[kb * BK + kc * 8 + e + q];
-                        const int iy = iy0 + t.y, ix = ix0 + t.z;
-                        uint32_t v = 0;
-                        if (row_ok && t.w && iy >= 0 && iy < P.h && ix >= 0 && ix < P.w)
-                            v = bf16_bits(float(P.in[rowoff + t.x]));
-                        v2[q] = v;
-                    }
-                    pk[e / 2] = v2[0] | (v2[1] << 16);
-                }
-                *reinterpret_cast<uint4 *>(a + kc * 128) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+                failed = true;
+                break;
             }
-            // B block: contiguous image of this (n tile, k block).
-            const uint4 *src = P.wimg + (int64_t(nt) * P.kblocks + kb) * (b_bytes / 16);
-            uint4 *dst = reinterpret_cast<uint4 *>(sB[st]);
-            for (int i = tid; i < b_bytes / 16; i += blockDim.x) dst[i] = src[i];
+            // Stage st is free: fetch the weight block with the bulk-copy engine.
+            if (tid == 0)
+            {
+                arrive_expect_tx(&full_bar[st], uint32_t(b_bytes));
+                bulk_g2s(sB, P.wimg + (int64_t(nt) * P.kblocks + kb) * b_bytes, uint32_t(b_bytes), &full_bar[st]);
+            }
+            // Gather this thread's 4 K chunks of its row.
+            unsigned char *a = sA + (row >> 3) * 1024 + (row & 7) * 16;
+            if (P.nhwc)
+            {
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                {
+                    const int kc = chunk0 + j;
+                    const int4 t = tab[kb * 8 + kc];
+                    const int iy = iy0 + t.x, ix = ix0 + t.y;
+                    uint4 v = make_uint4(0, 0, 0, 0);
+                    if (row_ok && t.w && iy >= 0 && iy < P.h && ix >= 0 && ix < P.w)
+                        v = bf16x8_of_bytes(*reinterpret_cast<const uint2 *>(
+                            img_base + (int64_t(iy) * P.w + ix) * P.cpad + t.z));
+                    *reinterpret_cast<uint4 *>(a + kc * 128) = v;
+                }
+            }
+            else
+            {
+                const int64_t rowoff = int64_t(iy0) * P.w + ix0;
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                {
+                    const int kc = chunk0 + j;
+                    uint32_t pk[4];
+#pragma unroll
+                    for (int e = 0; e < 8; e += 2)
+                    {
+                        uint32_t v2[2];
+#pragma unroll
+                        for (int q = 0; q < 2; ++q)
+                        {
+                            const int4 t = tab[kb * BK + kc * 8 + e + q];
+                            const int iy = iy0 + t.y, ix = ix0 + t.z;
+                            uint32_t v = 0;
+                            if (row_ok && t.w && iy >= 0 && iy < P.h && ix >= 0 && ix < P.w)
+                                v = bf16_of_byte(img_base[rowoff + t.x]);
+                            v2[q] = v;
+                        }
+                        pk[e / 2] = v2[0] | (v2[1] << 16);
+                    }
+                    *reinterpret_cast<uint4 *>(a + kc * 128) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+                }
+            }
+            // The weight block must have landed before anyone proceeds.
+            ok = wait_bounded(&full_bar[st], uses[st] & 1);
             fence_proxy_async_smem();
-            __syncthreads();
+            if (__syncthreads_or(!ok))
+            {
+                failed = true;
+                break;
+            }
             if (tid == 0)
             {
                 tc_fence_after();
-                const uint32_t a_base = smem_u32(sA[st]), b_base = smem_u32(sB[st]);
+                const uint32_t a_base = smem_u32(sA), b_base = smem_u32(sB);
                 for (int p = 0; p < P.nsplit; ++p)
 #pragma unroll
                     for (int s = 0; s < BK / 16; ++s)
@@ -223,26 +337,26 @@ __global__ void __launch_bounds__(kTcThreads, 1) conv_tc_kernel(TcParams P)
                         const uint64_t bd = smem_desc(b_base + p * P.n_tile * 128 + s * 256, 128, 1024);
                         mma_bf16(tmem + uint32_t(p * P.n_tile), ad, bd, P.idesc, (kb > 0 || s > 0) ? 1u : 0u);
                     }
-                mma_commit(&mbar[st]);
+                mma_commit(&done_bar[st]);
             }
             ++uses[st];
         }
         if (failed) break;
 
-        // Epilogue: all MMAs of the tile are complete once the last commit is.
-        const int last = (it - 1) & 1;
+        // Epilogue: all MMAs of the tile are complete once its last commit is.
         {
-            const bool ok = wait_bounded(&mbar[last], (uses[last] - 1) & 1);
+            const int last = (it - 1) & 1;
+            const bool ok = wait_bounded(&done_bar[last], (uses[last] - 1) & 1);
+            waited[0] = uses[0], waited[1] = uses[1];
             if (__syncthreads_or(!ok))
             {
                 failed = true;
                 break;
             }
-            waited[0] = uses[0], waited[1] = uses[1];
         }
         tc_fence_after();
-        const uint32_t lane_base = tmem + (uint32_t(warp * 32) << 16);
-        for (int c0 = 0; c0 < P.n_tile; c0 += 16)
+        const uint32_t lane_base = tmem + (uint32_t((warp & 3) * 32) << 16);
+        for (int c0 = (warp >> 2) * 16; c0 < P.n_tile; c0 += 32)
         {
             uint32_t r0[16], r1[16], r2[16];
             tmem_ld16(lane_base + uint32_t(c0), r0);
@@ -268,10 +382,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) conv_tc_kernel(TcParams P)
         __syncthreads();
     }
 
-    // Teardown: make sure no MMA is still writing tensor memory, then free it.
+    // Teardown: no MMA may still be writing tensor memory when it is freed.
     if (!failed)
         for (int st = 0; st < 2; ++st)
-            if (waited[st] < uses[st]) wait_bounded(&mbar[st], (uses[st] - 1) & 1);
+            if (waited[st] < uses[st]) wait_bounded(&done_bar[st], (uses[st] - 1) & 1);
     tc_fence_before();
     __syncthreads();
     if (warp == 0)
@@ -283,12 +397,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) conv_tc_kernel(TcParams P)
 
 struct Plan
 {
-    int nsplit, n_tile, n_tiles, K, kblocks;
+    int nsplit, n_tile, n_tiles, kblocks, cpad;
+    bool nhwc;
     uint32_t tmem_cols;
-    size_t wimg_bytes, smem;
+    size_t wimg_bytes, xt_bytes, smem;
 };
 
-Plan make_plan(int64_t cin, int64_t cout, int64_t kh, int64_t kw, int precision)
+Plan make_plan(int64_t n, int64_t cin, int64_t h, int64_t w, int64_t cout, int64_t kh, int64_t kw, int precision)
 {
     Plan pl{};
     pl.nsplit = precision == SPK_CONV_BF16X3 ? 3 : 2;
@@ -296,13 +411,17 @@ Plan make_plan(int64_t cin, int64_t cout, int64_t kh, int64_t kw, int precision)
     const int64_t cap = pl.nsplit == 3 ? 128 : 256;
     pl.n_tiles = int(ceil_div(npad, cap));
     pl.n_tile = int(ceil_div(ceil_div(npad, pl.n_tiles), 16) * 16);
-    pl.K = int(cin * kh * kw);
-    pl.kblocks = int(ceil_div(pl.K, BK));
+    pl.nhwc = cin >= 8;
+    pl.cpad = int(ceil_div(cin, 8) * 8);
+    const int64_t kreal = pl.nhwc ? kh * kw * pl.cpad : kh * kw * cin;
+    pl.kblocks = int(ceil_div(kreal, BK));
     uint32_t need = uint32_t(pl.nsplit * pl.n_tile), cols = 32;
     while (cols < need) cols <<= 1;
     pl.tmem_cols = cols;
     pl.wimg_bytes = size_t(pl.n_tiles) * pl.kblocks * pl.nsplit * pl.n_tile * BK * 2;
-    size_t smem = 2 * size_t(BM * BK * 2) + 2 * size_t(pl.nsplit) * pl.n_tile * BK * 2 + size_t(pl.kblocks) * BK * 16;
+    pl.xt_bytes = pl.nhwc ? size_t(n) * h * w * pl.cpad : 0;
+    const size_t tab = pl.nhwc ? size_t(pl.kblocks) * 8 * 16 : size_t(pl.kblocks) * BK * 16;
+    size_t smem = 2 * size_t(BM * BK * 2) + 2 * size_t(pl.nsplit) * pl.n_tile * BK * 2 + tab;
     // At most 512 / tmem_cols CTAs may share an SM's tensor memory: size the
     // shared memory so that no more fit.
     const int per_sm = int(512 / cols);
@@ -310,12 +429,15 @@ Plan make_plan(int64_t cin, int64_t cout, int64_t kh, int64_t kw, int precision)
     pl.smem = std::max(smem, floor_smem) + 1024;
     return pl;
 }
+
+inline size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 }  // namespace
 
-size_t conv_tc_workspace(int64_t, int64_t cin, int64_t, int64_t, int64_t cout, int64_t kh, int64_t kw, int precision)
+size_t conv_tc_workspace(int64_t n, int64_t cin, int64_t h, int64_t w, int64_t cout, int64_t kh, int64_t kw,
+                         int precision)
 {
-    Plan pl = make_plan(cin, cout, kh, kw, precision);
-    return pl.wimg_bytes + 256;
+    Plan pl = make_plan(n, cin, h, w, cout, kh, kw, precision);
+    return align256(pl.wimg_bytes) + align256(pl.xt_bytes);
 }
 
 void conv_tc(const void *in, spk_dtype itype, const float *kernel, float *out, int64_t n, int64_t cin, int64_t h,
@@ -323,32 +445,48 @@ void conv_tc(const void *in, spk_dtype itype, const float *kernel, float *out, i
              int precision, void *ws, size_t ws_bytes, cudaStream_t s)
 {
     if (itype != SPK_U8) throw Error(SPK_ERR_UNSUPPORTED, "the tensor-core path takes U8 spikes");
-    Plan pl = make_plan(cin, cout, kh, kw, precision);
-    SPK_REQUIRE(pl.K <= kMaxK, "Cin*KH*KW is limited to 4096 on the tensor-core path");
+    Plan pl = make_plan(n, cin, h, w, cout, kh, kw, precision);
+    SPK_REQUIRE(pl.kblocks <= kMaxKBlocks, "Cin*KH*KW is too large for the tensor-core path");
     SPK_REQUIRE(pl.smem <= 227 * 1024, "tile does not fit in shared memory");
-    SPK_REQUIRE(ws != nullptr && ws_bytes >= pl.wimg_bytes, "workspace is too small");
-    SPK_REQUIRE((reinterpret_cast<uintptr_t>(ws) & 15) == 0, "workspace must be 16-byte aligned");
-    uint4 *wimg = reinterpret_cast<uint4 *>(ws);
+    SPK_REQUIRE(ws != nullptr && ws_bytes >= align256(pl.wimg_bytes) + align256(pl.xt_bytes), "workspace is too small");
+    SPK_REQUIRE((reinterpret_cast<uintptr_t>(ws) & 255) == 0, "workspace must be 256-byte aligned");
+    uint8_t *wimg = reinterpret_cast<uint8_t *>(ws);
+    const int taps = int(kh * kw);
     const int64_t wthreads = int64_t(pl.n_tiles) * pl.kblocks * pl.n_tile * 8;
-    split_weights_kernel<<<grid_for(wthreads, 256), 256, 0, s>>>(kernel, wimg, int(cout), pl.K, pl.kblocks, pl.n_tile,
-                                                                pl.n_tiles, pl.nsplit);
+    split_weights_kernel<<<grid_for(wthreads, 256), 256, 0, s>>>(kernel, reinterpret_cast<uint4 *>(wimg), int(cout),
+                                                                int(cin), taps, pl.nhwc ? 1 : 0, pl.cpad, pl.kblocks,
+                                                                pl.n_tile, pl.n_tiles, pl.nsplit);
     SPK_LAUNCHED();
+    const uint8_t *a_src = static_cast<const uint8_t *>(in);
+    if (pl.nhwc)
+    {
+        uint8_t *xt = wimg + align256(pl.wimg_bytes);
+        const int64_t work = n * h * w * (pl.cpad / 8);
+        to_channels_last_kernel<<<grid_for(work, 256), 256, 0, s>>>(a_src, reinterpret_cast<uint2 *>(xt), n,
+                                                                    int(cin), h * w, pl.cpad);
+        SPK_LAUNCHED();
+        a_src = xt;
+    }
 
     TcParams P{};
-    P.in = static_cast<const uint8_t *>(in);
+    P.in = a_src;
     P.wimg = wimg;
     P.out = out;
     P.M = n * oh * ow;
     P.tiles = ceil_div(P.M, BM) * pl.n_tiles;
-    P.chw = cin * h * w;
+    P.img_stride = pl.nhwc ? h * w * pl.cpad : cin * h * w;
     P.ohw = oh * ow;
     P.cin = int(cin), P.h = int(h), P.w = int(w), P.cout = int(cout), P.kh = int(kh), P.kw = int(kw);
     P.oh = int(oh), P.ow = int(ow), P.sy = int(sy), P.sx = int(sx), P.top = int(p.top), P.left = int(p.left);
-    P.K = pl.K, P.kblocks = pl.kblocks, P.n_tile = pl.n_tile, P.n_tiles = pl.n_tiles, P.nsplit = pl.nsplit;
+    P.kblocks = pl.kblocks, P.n_tile = pl.n_tile, P.n_tiles = pl.n_tiles, P.nsplit = pl.nsplit;
+    P.cpad = pl.cpad, P.nhwc = pl.nhwc ? 1 : 0;
     P.tmem_cols = pl.tmem_cols;
     P.idesc = idesc_bf16_f32(BM, pl.n_tile);
     SPK_CUDA(cudaFuncSetAttribute(conv_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(pl.smem)));
-    const int64_t grid = std::min<int64_t>(P.tiles, int64_t(sm_count()));
+    int per_sm = 1;
+    SPK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, conv_tc_kernel, kTcThreads, pl.smem));
+    per_sm = std::max(1, std::min<int>(per_sm, int(512 / pl.tmem_cols)));
+    const int64_t grid = std::min<int64_t>(P.tiles, int64_t(sm_count()) * per_sm);
     conv_tc_kernel<<<unsigned(grid), kTcThreads, pl.smem, s>>>(P);
     SPK_LAUNCHED();
 }
