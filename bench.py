@@ -108,16 +108,29 @@ class Network:
         self.conv_events.append((a, b, layer))
         return y
 
+    def _layer(self, layer, x, theta, radius, count):
+        """conv -> threshold -> inhibit -> (fire, convwta): fused on the
+        tensor-core precisions, op by op on the FP32 path."""
+        t = self.torch
+        a, b = t.cuda.Event(enable_timing=True), t.cuda.Event(enable_timing=True)
+        a.record()
+        if layer.precision == "fp32":
+            out = self.sp.inhibit(self.sp.threshold(layer(x), theta))
+            spk, wins = self.sp.fire(out), self.sp.convwta(out, radius, count)
+        else:
+            spk, wins = self.sp.conv_fire_wta(x, layer, theta, radius, count)
+        b.record()
+        self.conv_events.append((a, b, layer))
+        return spk, wins
+
     def step(self, images_f32):
         sp = self.sp
         codes = sp.code(self.dog(images_f32), T)
-        out1 = sp.inhibit(sp.threshold(self._conv(self.conv1, codes), 15.0))
-        spk1 = sp.fire(out1)
-        self.conv1.stdp(codes, sp.convwta(out1, 3, 5), spk1)
+        spk1, win1 = self._layer(self.conv1, codes, 15.0, 3, 5)
+        self.conv1.stdp(codes, win1, spk1)
         pooled = sp.pool(spk1, 2)
-        out2 = sp.inhibit(sp.threshold(self._conv(self.conv2, pooled), 10.0))
-        spk2 = sp.fire(out2)
-        self.conv2.stdp(pooled, sp.convwta(out2, 1, 8), spk2)
+        spk2, win2 = self._layer(self.conv2, pooled, 10.0, 1, 8)
+        self.conv2.stdp(pooled, win2, spk2)
         return sp.pool(spk2, 14)
 
 

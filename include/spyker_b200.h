@@ -187,6 +187,26 @@ spk_status spk_conv(const void *in, spk_dtype itype, const float *kernel, float 
                     int64_t w, int64_t cout, int64_t kh, int64_t kw, int64_t sy, int64_t sx, const int64_t *pad4_host,
                     int precision, void *ws, size_t ws_bytes, spk_stream stream);
 
+/* ---- fused layer: conv -> threshold -> inhibit -> fire + convwta -------- */
+/* No single reference function: the composition of Core::conv, threshold,
+ * rank_inhibit, rank_fire and rank_convwta (impl.h:224-282) that every STDP
+ * training step of the reference's examples performs
+ * (examples/kheradpisheh_mnist_dense.py:62-64), in one tcgen05 kernel whose
+ * epilogue never writes the potentials.  in [B, T, Cin, H, W] U8 spikes,
+ * kernel [Cout, Cin, KH, KW] F32; spikes out [B, T, Cout, OH, OW] U8 =
+ * fire(out, fire_threshold) and winners = convwta(out, (ry, rx), count,
+ * wta_threshold) with out = inhibit(threshold(conv(in), threshold, value),
+ * inhibit_threshold).  Requires T <= 32, Cout >= 2, fire/WTA thresholds >= 0
+ * and a tensor-core precision. */
+size_t spk_conv_fire_wta_workspace(int64_t b, int64_t t, int64_t cin, int64_t h, int64_t w, int64_t cout, int64_t kh,
+                                   int64_t kw, int64_t sy, int64_t sx, const int64_t *pad4_host, int precision);
+spk_status spk_conv_fire_wta(const void *in, spk_dtype itype, const float *kernel, int64_t b, int64_t t, int64_t cin,
+                             int64_t h, int64_t w, int64_t cout, int64_t kh, int64_t kw, int64_t sy, int64_t sx,
+                             const int64_t *pad4_host, double threshold, double value, double inhibit_threshold,
+                             double fire_threshold, int64_t ry, int64_t rx, int64_t count, double wta_threshold,
+                             uint8_t *spikes, int32_t *winners, int32_t *counts, int precision, void *ws,
+                             size_t ws_bytes, spk_stream stream);
+
 /* ---- fully connected (Core::fc / signfc, impl.h:228-236) ---------------- */
 /* in [R, I] (U8 or F32), kernel [O, I] F32 -> out [R, O] F32. */
 spk_status spk_fc(const void *in, spk_dtype itype, const float *kernel, float *out, int64_t r, int64_t ni, int64_t no,

@@ -9,7 +9,7 @@ runs on the GPU through the C ABI of ``include/spyker_b200.h``.
 
 from . import sparse
 from ._lib import SpykerError
-from .module import (FC, ZCA, BPConfig, Conv, DoG, DoGFilter, Gabor, GaborFilter, LoG, STDPConfig, Winner, Winners,
+from .module import (FC, ZCA, BPConfig, Conv, conv_fire_wta, DoG, DoGFilter, Gabor, GaborFilter, LoG, STDPConfig, Winner, Winners,
                      backward, canny, code, conv, conv_precision, convwta, fc, fcwta, fire, gather, infinite,
                      inhibit, labelize, pad, pool, quantize, random_seed, scatter, set_conv_precision, stdp,
                      threshold)

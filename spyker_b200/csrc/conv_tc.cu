@@ -52,10 +52,32 @@ struct TcParams
     const uint8_t *wimg;
     float *out;
     int64_t M, tiles, img_stride, ohw;
+    // gather strides: element address = base + iy * rs + ix * ps + c * cs
+    // (base = image, or sample + step * ts in the fused (pixel, time) layout)
+    int64_t rs, ps, cs, ts;
     int cin, h, w, cout, kh, kw, oh, ow, sy, sx, top, left;
     int kblocks, n_tile, n_tiles, nsplit, cpad, nhwc;
     uint32_t tmem_cols, idesc;
+    // fused spiking epilogue (kFused): rows are (pixel, t) with t fastest
+    int T, tp_log2, pp, lp_log2;
+    int64_t npix;
+    float thr, thv, inh_thr, fire_thr, wta_thr;
+    uint8_t *spikes;    // [B, T, Cout, OH, OW]
+    int4 *records;      // [B * OH * OW]: (winning channel, first step, value bits, 0)
+    unsigned *mins, *maxs;  // [B] order-preserving encodings
 };
+
+constexpr int kPotentials = 0, kFused = 1;
+
+__device__ __forceinline__ unsigned order_enc(float f)
+{
+    const unsigned u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float order_dec(unsigned e)
+{
+    return __uint_as_float((e & 0x80000000u) ? (e & 0x7FFFFFFFu) : ~e);
+}
 
 __device__ __forceinline__ uint32_t bf16_of_byte(uint32_t b)
 {
@@ -66,6 +88,15 @@ __device__ __forceinline__ uint32_t bf16_of_byte(uint32_t b)
 __device__ __forceinline__ uint4 bf16x8_of_bytes(uint2 v)
 {
     uint4 r;
+    if (((v.x | v.y) & 0xFEFEFEFEu) == 0)
+    {
+        // spikes: every byte is 0 or 1, and bf16(1) = 0x3F80 (two per word)
+        r.x = __byte_perm(v.x, 0, 0x7170) * 0x3F80u;
+        r.y = __byte_perm(v.x, 0, 0x7372) * 0x3F80u;
+        r.z = __byte_perm(v.y, 0, 0x7170) * 0x3F80u;
+        r.w = __byte_perm(v.y, 0, 0x7372) * 0x3F80u;
+        return r;
+    }
     r.x = bf16_of_byte(v.x & 0xFF) | (bf16_of_byte((v.x >> 8) & 0xFF) << 16);
     r.y = bf16_of_byte((v.x >> 16) & 0xFF) | (bf16_of_byte(v.x >> 24) << 16);
     r.z = bf16_of_byte(v.y & 0xFF) | (bf16_of_byte((v.y >> 8) & 0xFF) << 16);
@@ -176,6 +207,102 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
                  : "memory");
 }
 
+// 16 consecutive accumulator columns of this warp's 32 rows, the BF16 terms
+// added in FP64 and rounded once to F32.  Warp-uniform (tcgen05.ld is .sync).
+__device__ __forceinline__ void load_exact16(uint32_t lane_base, int c0, int n_tile, int nsplit, float (&v)[16])
+{
+    uint32_t r0[16], r1[16], r2[16];
+    tmem_ld16(lane_base + uint32_t(c0), r0);
+    tmem_ld16(lane_base + uint32_t(n_tile + c0), r1);
+    if (nsplit == 3) tmem_ld16(lane_base + uint32_t(2 * n_tile + c0), r2);
+    tmem_ld_wait();
+#pragma unroll
+    for (int j = 0; j < 16; ++j)
+    {
+        double acc = double(__uint_as_float(r0[j])) + double(__uint_as_float(r1[j]));
+        if (nsplit == 3) acc += double(__uint_as_float(r2[j]));
+        v[j] = float(acc);
+    }
+}
+
+// Fused spiking epilogue over a tile of PP pixels x TP steps, with every
+// output channel of a pixel in this CTA's tensor memory.  Restates, for the
+// pipeline  out = inhibit(threshold(conv(x), thr, thv), inh_thr);
+// spikes = fire(out, fire_thr); convwta(out, r, k, wta_thr):
+//   threshold  cpu/fire.cpp:41-51    x <= thr -> thv
+//   inhibit    cpu/inhibit.cpp:41-121 first-max channel per step, winner taken
+//              at step T - max(#steps whose max > inh_thr, 1), others x * 0
+//   fire       cpu/fire.cpp:67-82    x > fire_thr
+//   WTA key    cpu/wta.cpp:45-64     first step with x > wta_thr and its value
+// With fire_thr, wta_thr >= 0 only the winning channel of a pixel can spike or
+// hold a WTA key, so each pixel yields one record (channel, first step,
+// value) and the per-sample min / max of the inhibited potentials.
+// Warps 0-3 own the tensor-memory lanes; all warps write the spikes out.
+__device__ void fused_epilogue(const TcParams &P, unsigned char *smem, uint32_t lane_base, int warp, bool row_ok,
+                               int tstep, int64_t sample, int64_t pix)
+{
+    if (warp >= 4) return;  // warps 0-3 own the 128 tensor-memory lanes (one row each)
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int TP = 1 << P.tp_log2, T = P.T, C = P.cout;
+    // exact thresholded potentials of this row, cached in the idle stage buffers
+    const int ld = P.n_tile + 1;
+    float *vals = reinterpret_cast<float *>(smem) + tid * ld;
+    // pass over the accumulators: thresholded first-max channel of this (pixel, step)
+    float mx = 0.f;
+    int am = 0;
+    for (int c0 = 0; c0 < P.n_tile; c0 += 16)
+    {
+        float v[16];
+        load_exact16(lane_base, c0, P.n_tile, P.nsplit, v);
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+        {
+            const int c = c0 + j;
+            const float x = (v[j] <= P.thr) ? P.thv : v[j];
+            vals[c] = x;
+            if (c == 0)
+                mx = x;
+            else if (c < C && x > mx)
+                mx = x, am = c;
+        }
+    }
+    const int base = (lane >> P.tp_log2) << P.tp_log2;  // first lane of this pixel
+    const unsigned grp = (TP == 32) ? 0xffffffffu : (((1u << TP) - 1u) << base);
+    const unsigned above = __ballot_sync(0xffffffffu, row_ok && mx > P.inh_thr) & grp;
+    const int n = __popc(above);
+    const int ts = T - (n > 1 ? n : 1);
+    const int win = __shfl_sync(0xffffffffu, am, base + ts);
+    const float vw = vals[win];  // thresholded value of the winning channel at this step
+    // spike of the winning channel (the others stay 0 since fire_thr >= 0;
+    // the spike tensor was zero-filled before the launch)
+    if (row_ok && vw > P.fire_thr) P.spikes[((sample * T + tstep) * C + win) * P.ohw + pix] = 1;
+    // WTA record: first step whose inhibited value exceeds wta_thr
+    const unsigned keyed = __ballot_sync(0xffffffffu, row_ok && vw > P.wta_thr) & grp;
+    const int first_lane = keyed ? __ffs(keyed) - 1 : base;
+    const float first_v = __shfl_sync(0xffffffffu, vw, first_lane);
+    const bool pixel_ok = __shfl_sync(0xffffffffu, row_ok ? 1 : 0, base) != 0;  // step 0 of the pixel is valid
+    if (lane == base && pixel_ok)
+        P.records[sample * P.ohw + pix] = make_int4(win, keyed ? first_lane - base : T, __float_as_int(first_v), 0);
+    // per-sample min / max of the inhibited values (winner value, and a zero
+    // from every losing channel when there is more than one channel)
+    float rmin = vw, rmax = vw;
+    if (C > 1)
+    {
+        rmin = (0.f < rmin) ? 0.f : rmin;
+        rmax = (rmax < 0.f) ? 0.f : rmax;
+    }
+    const int key = row_ok ? int(sample) : -1;
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    const unsigned emin = __reduce_min_sync(peers, order_enc(rmin));
+    const unsigned emax = __reduce_max_sync(peers, order_enc(rmax));
+    if (row_ok && lane == __ffs(peers) - 1)
+    {
+        atomicMin(P.mins + sample, emin);
+        atomicMax(P.maxs + sample, emax);
+    }
+}
+
+template <int MODE>
 __global__ void __launch_bounds__(kTcThreads, 1) conv_tc_kernel(TcParams P)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
@@ -208,7 +335,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) conv_tc_kernel(TcParams P)
         for (int k = tid; k < P.kblocks * BK; k += blockDim.x)
         {
             const int c = k / taps, tap = k % taps, ky = tap / P.kw, kx = tap % P.kw;
-            tab[k] = make_int4(c * P.h * P.w + ky * P.w + kx, ky, kx, c < P.cin ? 1 : 0);
+            tab[k] = make_int4(int(c * P.cs + ky * P.rs + kx * P.ps), ky, kx, c < P.cin ? 1 : 0);
         }
     }
     if (tid == 0)
@@ -237,19 +364,32 @@ __global__ void __launch_bounds__(kTcThreads, 1) conv_tc_kernel(TcParams P)
     {
         const int64_t mt = tile / P.n_tiles;
         const int nt = int(tile % P.n_tiles);
-        const int64_t m = mt * BM + row;
-        const bool row_ok = m < P.M;
-        int64_t img = 0, pix = 0;
+        bool row_ok;
+        int64_t img = 0, pix = 0, sample = 0, gp = 0;
+        int tstep = 0;
+        if constexpr (MODE == kPotentials)
+        {
+            const int64_t m = mt * BM + row;
+            row_ok = m < P.M;
+            if (row_ok) img = m / P.ohw, pix = m % P.ohw;
+        }
+        else
+        {
+            // row = (pixel in tile) * TP + t; all steps of a pixel in one warp
+            tstep = row & ((1 << P.tp_log2) - 1);
+            gp = mt * P.pp + (row >> P.tp_log2);
+            row_ok = tstep < P.T && gp < P.npix;
+            if (row_ok) sample = gp / P.ohw, pix = gp % P.ohw, img = sample * P.T + tstep;
+        }
         int iy0 = 0, ix0 = 0;
         if (row_ok)
         {
-            img = m / P.ohw;
-            pix = m % P.ohw;
             const int oy = int(pix / P.ow), ox = int(pix % P.ow);
             iy0 = oy * P.sy - P.top;
             ix0 = ox * P.sx - P.left;
         }
-        const uint8_t *img_base = P.in + img * P.img_stride;
+        const uint8_t *img_base =
+            (MODE == kPotentials) ? P.in + img * P.img_stride : P.in + sample * P.img_stride + tstep * P.ts;
 
         for (int kb = 0; kb < P.kblocks; ++kb, ++it)
         {
@@ -286,13 +426,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) conv_tc_kernel(TcParams P)
                     uint4 v = make_uint4(0, 0, 0, 0);
                     if (row_ok && t.w && iy >= 0 && iy < P.h && ix >= 0 && ix < P.w)
                         v = bf16x8_of_bytes(*reinterpret_cast<const uint2 *>(
-                            img_base + (int64_t(iy) * P.w + ix) * P.cpad + t.z));
+                            img_base + int64_t(iy) * P.rs + int64_t(ix) * P.ps + t.z));
                     *reinterpret_cast<uint4 *>(a + kc * 128) = v;
                 }
             }
             else
             {
-                const int64_t rowoff = int64_t(iy0) * P.w + ix0;
+                const int64_t rowoff = int64_t(iy0) * P.rs + int64_t(ix0) * P.ps;
 #pragma unroll
                 for (int j = 0; j < 4; ++j)
                 {
@@ -309,7 +449,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) conv_tc_kernel(TcParams P)
                             const int iy = iy0 + t.y, ix = ix0 + t.z;
                             uint32_t v = 0;
                             if (row_ok && t.w && iy >= 0 && iy < P.h && ix >= 0 && ix < P.w)
-                                v = bf16_of_byte(img_base[rowoff + t.x]);
+                            {
+                                const uint32_t u = img_base[rowoff + t.x];
+                                v = u <= 1u ? u * 0x3F80u : bf16_of_byte(u);
+                            }
                             v2[q] = v;
                         }
                         pk[e / 2] = v2[0] | (v2[1] << 16);
@@ -356,27 +499,26 @@ __global__ void __launch_bounds__(kTcThreads, 1) conv_tc_kernel(TcParams P)
         }
         tc_fence_after();
         const uint32_t lane_base = tmem + (uint32_t((warp & 3) * 32) << 16);
-        for (int c0 = (warp >> 2) * 16; c0 < P.n_tile; c0 += 32)
+        if constexpr (MODE == kPotentials)
         {
-            uint32_t r0[16], r1[16], r2[16];
-            tmem_ld16(lane_base + uint32_t(c0), r0);
-            tmem_ld16(lane_base + uint32_t(P.n_tile + c0), r1);
-            if (P.nsplit == 3) tmem_ld16(lane_base + uint32_t(2 * P.n_tile + c0), r2);
-            tmem_ld_wait();
-            if (row_ok)
+            for (int c0 = (warp >> 2) * 16; c0 < P.n_tile; c0 += 32)
             {
-#pragma unroll
-                for (int j = 0; j < 16; ++j)
+                float v[16];
+                load_exact16(lane_base, c0, P.n_tile, P.nsplit, v);
+                if (row_ok)
                 {
-                    const int n = nt * P.n_tile + c0 + j;
-                    if (n < P.cout)
+#pragma unroll
+                    for (int j = 0; j < 16; ++j)
                     {
-                        double acc = double(__uint_as_float(r0[j])) + double(__uint_as_float(r1[j]));
-                        if (P.nsplit == 3) acc += double(__uint_as_float(r2[j]));
-                        P.out[(img * P.cout + n) * P.ohw + pix] = float(acc);
+                        const int n = nt * P.n_tile + c0 + j;
+                        if (n < P.cout) P.out[(img * P.cout + n) * P.ohw + pix] = v[j];
                     }
                 }
             }
+        }
+        else
+        {
+            fused_epilogue(P, smem, lane_base, warp, row_ok, tstep, sample, pix);
         }
         tc_fence_before();
         __syncthreads();
@@ -395,6 +537,74 @@ __global__ void __launch_bounds__(kTcThreads, 1) conv_tc_kernel(TcParams P)
     }
 }
 
+// WTA over the per-pixel records of one sample (one CTA per sample).  Keys
+// follow cpu/wta.cpp:53-62 with the sample's min / max; ties resolve to the
+// lowest flat index channel * H*W + pixel, as std::max_element does.
+__global__ void wta_records_kernel(const int4 *__restrict__ records, const unsigned *__restrict__ mins,
+                                   const unsigned *__restrict__ maxs, int hw, int w, int T, int ry, int rx, int count,
+                                   int32_t *__restrict__ winners, int32_t *__restrict__ counts)
+{
+    extern __shared__ __align__(16) unsigned char wsm[];
+    float *key = reinterpret_cast<float *>(wsm);
+    int *flat = reinterpret_cast<int *>(key + hw);
+    __shared__ float s_v[32];
+    __shared__ int s_i[32];
+    const int64_t b = blockIdx.x;
+    const float mn = order_dec(mins[b]), mx = order_dec(maxs[b]);
+    const float diff = __fmul_rn(__fsub_rn(mx, mn), 2.0f);
+    for (int p = threadIdx.x; p < hw; p += blockDim.x)
+    {
+        const int4 r = records[b * hw + p];
+        if (r.y < T)
+        {
+            key[p] = __fadd_rn(float(T - r.y - 1), __fdiv_rn(__fsub_rn(__int_as_float(r.z), mn), diff));
+            flat[p] = r.x * hw + p;
+        }
+        else
+        {
+            key[p] = -INFINITY;
+            flat[p] = INT_MAX;
+        }
+    }
+    __syncthreads();
+    int found = 0;
+    for (int round = 0; round < count; ++round)
+    {
+        float bv = -INFINITY;
+        int bi = INT_MAX;
+        for (int p = threadIdx.x; p < hw; p += blockDim.x)
+            if (key[p] > bv || (key[p] == bv && flat[p] < bi)) bv = key[p], bi = flat[p];
+        for (int o = 16; o > 0; o >>= 1)
+        {
+            const float ov = __shfl_xor_sync(0xffffffffu, bv, o);
+            const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+            if (ov > bv || (ov == bv && oi < bi)) bv = ov, bi = oi;
+        }
+        if ((threadIdx.x & 31) == 0) s_v[threadIdx.x >> 5] = bv, s_i[threadIdx.x >> 5] = bi;
+        __syncthreads();
+        bv = s_v[0], bi = s_i[0];
+        for (int q = 1; q < int(blockDim.x >> 5); ++q)
+            if (s_v[q] > bv || (s_v[q] == bv && s_i[q] < bi)) bv = s_v[q], bi = s_i[q];
+        __syncthreads();
+        if (bi == INT_MAX) break;  // only sentinels left
+        const int z = bi / hw, p0 = bi % hw, y = p0 / w, x = p0 % w;
+        if (threadIdx.x == 0)
+        {
+            int32_t *e = winners + (b * count + round) * 5;
+            e[0] = 0, e[1] = 0, e[2] = z, e[3] = y, e[4] = x;
+        }
+        for (int p = threadIdx.x; p < hw; p += blockDim.x)
+        {
+            const int py = p / w, px = p % w;
+            const bool box = py >= y - ry && py <= y + ry && px >= x - rx && px <= x + rx;
+            if (box || (flat[p] != INT_MAX && flat[p] / hw == z)) key[p] = -INFINITY, flat[p] = INT_MAX;
+        }
+        __syncthreads();
+        ++found;
+    }
+    if (threadIdx.x == 0) counts[b] = found;
+}
+
 struct Plan
 {
     int nsplit, n_tile, n_tiles, kblocks, cpad;
@@ -403,12 +613,14 @@ struct Plan
     size_t wimg_bytes, xt_bytes, smem;
 };
 
-Plan make_plan(int64_t n, int64_t cin, int64_t h, int64_t w, int64_t cout, int64_t kh, int64_t kw, int precision)
+// single_tile: all output channels in one CTA (required by the fused epilogue).
+Plan make_plan(int64_t n, int64_t cin, int64_t h, int64_t w, int64_t cout, int64_t kh, int64_t kw, int precision,
+               bool single_tile)
 {
     Plan pl{};
     pl.nsplit = precision == SPK_CONV_BF16X3 ? 3 : 2;
     const int64_t npad = ceil_div(cout, 16) * 16;
-    const int64_t cap = pl.nsplit == 3 ? 128 : 256;
+    const int64_t cap = single_tile ? npad : (pl.nsplit == 3 ? 128 : 256);
     pl.n_tiles = int(ceil_div(npad, cap));
     pl.n_tile = int(ceil_div(ceil_div(npad, pl.n_tiles), 16) * 16);
     pl.nhwc = cin >= 8;
@@ -419,7 +631,9 @@ Plan make_plan(int64_t n, int64_t cin, int64_t h, int64_t w, int64_t cout, int64
     while (cols < need) cols <<= 1;
     pl.tmem_cols = cols;
     pl.wimg_bytes = size_t(pl.n_tiles) * pl.kblocks * pl.nsplit * pl.n_tile * BK * 2;
-    pl.xt_bytes = pl.nhwc ? size_t(n) * h * w * pl.cpad : 0;
+    // staged copy of the spikes: channels-last [N, H, W, Cpad] (plain), or
+    // [B, H, W, T, Cpad or Cin] (fused; single_tile), where every call stages
+    pl.xt_bytes = pl.nhwc ? size_t(n) * h * w * pl.cpad : (single_tile ? size_t(n) * h * w * cin : 0);
     const size_t tab = pl.nhwc ? size_t(pl.kblocks) * 8 * 16 : size_t(pl.kblocks) * BK * 16;
     size_t smem = 2 * size_t(BM * BK * 2) + 2 * size_t(pl.nsplit) * pl.n_tile * BK * 2 + tab;
     // At most 512 / tmem_cols CTAs may share an SM's tensor memory: size the
@@ -431,12 +645,152 @@ Plan make_plan(int64_t n, int64_t cin, int64_t h, int64_t w, int64_t cout, int64
 }
 
 inline size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
+
+// Split the weights and (channels-last) transpose the spikes into the
+// workspace; fill the fields of P shared by both epilogues.
+// Fused layout: [B, T, C, H, W] -> [B, H, W, T, Cp] (Cp = Cpad or Cin, pad
+// channels zero), so the TP rows of a pixel read adjacent bytes.
+__global__ void to_pixel_time_kernel(const uint8_t *__restrict__ in, uint8_t *__restrict__ out, int64_t b, int t,
+                                     int c, int64_t hw, int cp)
+{
+    const int groups = (cp + 7) / 8;
+    const int64_t total = b * hw * t * groups;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += int64_t(gridDim.x) * blockDim.x)
+    {
+        const int g = int(i % groups);
+        const int64_t r = i / groups;  // (sample, pixel, step) in output order
+        const int q = int(r % t);
+        const int64_t px = (r / t) % hw, s = r / (int64_t(t) * hw);
+        const uint8_t *src = in + ((s * t + q) * c) * hw + px;
+        uint8_t *dst = out + r * cp + g * 8;
+        const int n8 = min(8, cp - g * 8);
+        if (n8 == 8)
+        {
+            uint32_t lo = 0, hi = 0;
+#pragma unroll
+            for (int e = 0; e < 8; ++e)
+            {
+                const int ch = g * 8 + e;
+                const uint32_t v = ch < c ? src[int64_t(ch) * hw] : 0u;
+                if (e < 4)
+                    lo |= v << (8 * e);
+                else
+                    hi |= v << (8 * (e - 4));
+            }
+            *reinterpret_cast<uint2 *>(dst) = make_uint2(lo, hi);
+        }
+        else
+            for (int e = 0; e < n8; ++e)
+            {
+                const int ch = g * 8 + e;
+                dst[e] = ch < c ? src[int64_t(ch) * hw] : 0;
+            }
+    }
+}
+
+// t_fused > 0: stage for the fused (pixel, time) rows of t_fused steps.
+TcParams prepare(const Plan &pl, const void *in, const float *kernel, int64_t n, int64_t cin, int64_t h, int64_t w,
+                 int64_t cout, int64_t kh, int64_t kw, int64_t sy, int64_t sx, Pad4 p, int64_t oh, int64_t ow,
+                 uint8_t *ws, cudaStream_t s, int64_t t_fused = 0)
+{
+    SPK_REQUIRE(pl.kblocks <= kMaxKBlocks, "Cin*KH*KW is too large for the tensor-core path");
+    SPK_REQUIRE(pl.smem <= 227 * 1024, "tile does not fit in shared memory");
+    SPK_REQUIRE((reinterpret_cast<uintptr_t>(ws) & 255) == 0, "workspace must be 256-byte aligned");
+    uint8_t *wimg = ws;
+    const int64_t wthreads = int64_t(pl.n_tiles) * pl.kblocks * pl.n_tile * 8;
+    split_weights_kernel<<<grid_for(wthreads, 256), 256, 0, s>>>(kernel, reinterpret_cast<uint4 *>(wimg), int(cout),
+                                                                int(cin), int(kh * kw), pl.nhwc ? 1 : 0, pl.cpad,
+                                                                pl.kblocks, pl.n_tile, pl.n_tiles, pl.nsplit);
+    SPK_LAUNCHED();
+    const uint8_t *a_src = static_cast<const uint8_t *>(in);
+    TcParams P{};
+    uint8_t *xt = wimg + align256(pl.wimg_bytes);
+    if (t_fused > 0)
+    {
+        const int64_t b = n / t_fused, cp = pl.nhwc ? pl.cpad : cin;
+        const int64_t work = n * h * w * ((cp + 7) / 8);
+        to_pixel_time_kernel<<<grid_for(work, 256), 256, 0, s>>>(a_src, xt, b, int(t_fused), int(cin), h * w, int(cp));
+        SPK_LAUNCHED();
+        a_src = xt;
+        P.ts = cp, P.ps = t_fused * cp, P.rs = w * t_fused * cp, P.cs = 1;
+        P.img_stride = h * w * t_fused * cp;  // per sample
+    }
+    else if (pl.nhwc)
+    {
+        const int64_t work = n * h * w * (pl.cpad / 8);
+        to_channels_last_kernel<<<grid_for(work, 256), 256, 0, s>>>(a_src, reinterpret_cast<uint2 *>(xt), n,
+                                                                    int(cin), h * w, pl.cpad);
+        SPK_LAUNCHED();
+        a_src = xt;
+        P.ps = pl.cpad, P.rs = w * pl.cpad, P.cs = 1;
+        P.img_stride = h * w * pl.cpad;
+    }
+    else
+    {
+        P.ps = 1, P.rs = w, P.cs = h * w;
+        P.img_stride = cin * h * w;
+    }
+    P.in = a_src;
+    P.wimg = wimg;
+    P.ohw = oh * ow;
+    P.cin = int(cin), P.h = int(h), P.w = int(w), P.cout = int(cout), P.kh = int(kh), P.kw = int(kw);
+    P.oh = int(oh), P.ow = int(ow), P.sy = int(sy), P.sx = int(sx), P.top = int(p.top), P.left = int(p.left);
+    P.kblocks = pl.kblocks, P.n_tile = pl.n_tile, P.n_tiles = pl.n_tiles, P.nsplit = pl.nsplit;
+    P.cpad = pl.cpad, P.nhwc = pl.nhwc ? 1 : 0;
+    P.tmem_cols = pl.tmem_cols;
+    P.idesc = idesc_bf16_f32(BM, pl.n_tile);
+    return P;
+}
+
+template <int MODE>
+void launch(const TcParams &P, const Plan &pl, cudaStream_t s)
+{
+    auto kern = conv_tc_kernel<MODE>;
+    SPK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(pl.smem)));
+    int per_sm = 1;
+    SPK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTcThreads, pl.smem));
+    per_sm = std::max(1, std::min<int>(per_sm, int(512 / pl.tmem_cols)));
+    const int64_t grid = std::min<int64_t>(P.tiles, int64_t(sm_count()) * per_sm);
+    kern<<<unsigned(grid), kTcThreads, pl.smem, s>>>(P);
+    SPK_LAUNCHED();
+}
+
+struct FusedLayout
+{
+    Plan pl;
+    int tp_log2, pp;
+    int64_t npix, oh, ow;
+    size_t rec_off, min_off, max_off, total;
+};
+
+FusedLayout fused_layout(int64_t b, int64_t t, int64_t cin, int64_t h, int64_t w, int64_t cout, int64_t kh, int64_t kw,
+                         int64_t sy, int64_t sx, Pad4 p, int precision)
+{
+    FusedLayout L{};
+    L.oh = (h + p.top + p.bottom - kh) / sy + 1;
+    L.ow = (w + p.left + p.right - kw) / sx + 1;
+    L.pl = make_plan(b * t, cin, h, w, cout, kh, kw, precision, true);
+    int tp = 1, lg = 0;
+    while (tp < t) tp <<= 1, ++lg;
+    L.tp_log2 = lg;
+    L.pp = BM / tp;
+    L.npix = b * L.oh * L.ow;
+    size_t off = align256(L.pl.wimg_bytes) + align256(L.pl.xt_bytes);
+    L.rec_off = off;
+    off += align256(size_t(L.npix) * 16);
+    L.min_off = off;
+    off += align256(size_t(b) * 4);
+    L.max_off = off;
+    off += align256(size_t(b) * 4);
+    L.total = off;
+    return L;
+}
 }  // namespace
 
 size_t conv_tc_workspace(int64_t n, int64_t cin, int64_t h, int64_t w, int64_t cout, int64_t kh, int64_t kw,
                          int precision)
 {
-    Plan pl = make_plan(n, cin, h, w, cout, kh, kw, precision);
+    Plan pl = make_plan(n, cin, h, w, cout, kh, kw, precision, false);
     return align256(pl.wimg_bytes) + align256(pl.xt_bytes);
 }
 
@@ -445,54 +799,21 @@ void conv_tc(const void *in, spk_dtype itype, const float *kernel, float *out, i
              int precision, void *ws, size_t ws_bytes, cudaStream_t s)
 {
     if (itype != SPK_U8) throw Error(SPK_ERR_UNSUPPORTED, "the tensor-core path takes U8 spikes");
-    Plan pl = make_plan(n, cin, h, w, cout, kh, kw, precision);
-    SPK_REQUIRE(pl.kblocks <= kMaxKBlocks, "Cin*KH*KW is too large for the tensor-core path");
-    SPK_REQUIRE(pl.smem <= 227 * 1024, "tile does not fit in shared memory");
+    Plan pl = make_plan(n, cin, h, w, cout, kh, kw, precision, false);
     SPK_REQUIRE(ws != nullptr && ws_bytes >= align256(pl.wimg_bytes) + align256(pl.xt_bytes), "workspace is too small");
-    SPK_REQUIRE((reinterpret_cast<uintptr_t>(ws) & 255) == 0, "workspace must be 256-byte aligned");
-    uint8_t *wimg = reinterpret_cast<uint8_t *>(ws);
-    const int taps = int(kh * kw);
-    const int64_t wthreads = int64_t(pl.n_tiles) * pl.kblocks * pl.n_tile * 8;
-    split_weights_kernel<<<grid_for(wthreads, 256), 256, 0, s>>>(kernel, reinterpret_cast<uint4 *>(wimg), int(cout),
-                                                                int(cin), taps, pl.nhwc ? 1 : 0, pl.cpad, pl.kblocks,
-                                                                pl.n_tile, pl.n_tiles, pl.nsplit);
-    SPK_LAUNCHED();
-    const uint8_t *a_src = static_cast<const uint8_t *>(in);
-    if (pl.nhwc)
-    {
-        uint8_t *xt = wimg + align256(pl.wimg_bytes);
-        const int64_t work = n * h * w * (pl.cpad / 8);
-        to_channels_last_kernel<<<grid_for(work, 256), 256, 0, s>>>(a_src, reinterpret_cast<uint2 *>(xt), n,
-                                                                    int(cin), h * w, pl.cpad);
-        SPK_LAUNCHED();
-        a_src = xt;
-    }
-
-    TcParams P{};
-    P.in = a_src;
-    P.wimg = wimg;
+    TcParams P = prepare(pl, in, kernel, n, cin, h, w, cout, kh, kw, sy, sx, p, oh, ow, static_cast<uint8_t *>(ws), s);
     P.out = out;
     P.M = n * oh * ow;
     P.tiles = ceil_div(P.M, BM) * pl.n_tiles;
-    P.img_stride = pl.nhwc ? h * w * pl.cpad : cin * h * w;
-    P.ohw = oh * ow;
-    P.cin = int(cin), P.h = int(h), P.w = int(w), P.cout = int(cout), P.kh = int(kh), P.kw = int(kw);
-    P.oh = int(oh), P.ow = int(ow), P.sy = int(sy), P.sx = int(sx), P.top = int(p.top), P.left = int(p.left);
-    P.kblocks = pl.kblocks, P.n_tile = pl.n_tile, P.n_tiles = pl.n_tiles, P.nsplit = pl.nsplit;
-    P.cpad = pl.cpad, P.nhwc = pl.nhwc ? 1 : 0;
-    P.tmem_cols = pl.tmem_cols;
-    P.idesc = idesc_bf16_f32(BM, pl.n_tile);
-    SPK_CUDA(cudaFuncSetAttribute(conv_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(pl.smem)));
-    int per_sm = 1;
-    SPK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, conv_tc_kernel, kTcThreads, pl.smem));
-    per_sm = std::max(1, std::min<int>(per_sm, int(512 / pl.tmem_cols)));
-    const int64_t grid = std::min<int64_t>(P.tiles, int64_t(sm_count()) * per_sm);
-    conv_tc_kernel<<<unsigned(grid), kTcThreads, pl.smem, s>>>(P);
-    SPK_LAUNCHED();
+    launch<kPotentials>(P, pl, s);
 }
 }  // namespace spk
 
-extern "C" int spk_device_status(int reset)
+using namespace spk;
+
+extern "C" {
+
+int spk_device_status(int reset)
 {
     int v = 0;
     if (cudaMemcpyFromSymbol(&v, spk::g_tc_status, sizeof(int)) != cudaSuccess) return -1;
@@ -503,3 +824,66 @@ extern "C" int spk_device_status(int reset)
     }
     return v;
 }
+
+size_t spk_conv_fire_wta_workspace(int64_t b, int64_t t, int64_t cin, int64_t h, int64_t w, int64_t cout, int64_t kh,
+                                   int64_t kw, int64_t sy, int64_t sx, const int64_t *pad4, int precision)
+{
+    try
+    {
+        return fused_layout(b, t, cin, h, w, cout, kh, kw, sy, sx, pad_of(pad4), precision).total;
+    }
+    catch (...)
+    {
+        return 0;
+    }
+}
+
+spk_status spk_conv_fire_wta(const void *in, spk_dtype itype, const float *kernel, int64_t b, int64_t t, int64_t cin,
+                             int64_t h, int64_t w, int64_t cout, int64_t kh, int64_t kw, int64_t sy, int64_t sx,
+                             const int64_t *pad4, double threshold, double value, double inhibit_threshold,
+                             double fire_threshold, int64_t ry, int64_t rx, int64_t count, double wta_threshold,
+                             uint8_t *spikes, int32_t *winners, int32_t *counts, int precision, void *ws,
+                             size_t ws_bytes, spk_stream stream)
+{
+    return guarded([&] {
+        Pad4 p = pad_of(pad4);
+        SPK_REQUIRE(itype == SPK_U8, "the fused layer takes U8 spikes");
+        SPK_REQUIRE(precision == SPK_CONV_BF16X2 || precision == SPK_CONV_BF16X3, "the fused layer runs on tcgen05");
+        SPK_REQUIRE(b >= 0 && t >= 1 && t <= 32 && cin >= 1 && cout >= 2 && kh >= 1 && kw >= 1 && sy >= 1 && sx >= 1,
+                    "the fused layer needs 1 <= T <= 32 and at least 2 output channels");
+        SPK_REQUIRE(fire_threshold >= 0 && wta_threshold >= 0, "the fused layer needs fire/WTA thresholds >= 0");
+        SPK_REQUIRE(count >= 1 && ry >= 0 && rx >= 0, "invalid WTA radius or count");
+        SPK_REQUIRE(winners != nullptr && counts != nullptr && spikes != nullptr, "null output");
+        FusedLayout L = fused_layout(b, t, cin, h, w, cout, kh, kw, sy, sx, p, precision);
+        SPK_REQUIRE(L.oh > 0 && L.ow > 0, "input and kernel shapes are not compatible");
+        SPK_REQUIRE(L.pl.n_tiles == 1 && L.pl.nsplit * L.pl.n_tile <= 512, "too many output channels for one CTA");
+        SPK_REQUIRE(L.oh * L.ow <= 16384, "the fused WTA keeps at most 16384 pixels per sample");
+        SPK_REQUIRE(ws != nullptr && ws_bytes >= L.total, "workspace is too small");
+        if (b == 0) return;
+        cudaStream_t s = stream_of(stream);
+        uint8_t *base = static_cast<uint8_t *>(ws);
+        TcParams P = prepare(L.pl, in, kernel, b * t, cin, h, w, cout, kh, kw, sy, sx, p, L.oh, L.ow, base, s, t);
+        P.T = int(t), P.tp_log2 = L.tp_log2, P.pp = L.pp, P.npix = L.npix;
+        int lp = 0;
+        while ((1 << lp) < L.pp) ++lp;
+        P.lp_log2 = lp;
+        P.thr = float(threshold), P.thv = float(value), P.inh_thr = float(inhibit_threshold);
+        P.fire_thr = float(fire_threshold), P.wta_thr = float(wta_threshold);
+        P.spikes = spikes;
+        P.records = reinterpret_cast<int4 *>(base + L.rec_off);
+        P.mins = reinterpret_cast<unsigned *>(base + L.min_off);
+        P.maxs = reinterpret_cast<unsigned *>(base + L.max_off);
+        P.M = L.npix * (int64_t(1) << L.tp_log2);
+        P.tiles = ceil_div(L.npix, L.pp);
+        SPK_CUDA(cudaMemsetAsync(spikes, 0, size_t(b) * t * cout * L.oh * L.ow, s));
+        SPK_CUDA(cudaMemsetAsync(P.mins, 0xFF, size_t(b) * 4, s));
+        SPK_CUDA(cudaMemsetAsync(P.maxs, 0x00, size_t(b) * 4, s));
+        launch<kFused>(P, L.pl, s);
+        const int hw = int(L.oh * L.ow);
+        wta_records_kernel<<<unsigned(b), 256, size_t(hw) * 8, s>>>(P.records, P.mins, P.maxs, hw, int(L.ow), int(t),
+                                                                    int(ry), int(rx), int(count), winners, counts);
+        SPK_LAUNCHED();
+    });
+}
+
+}  // extern "C"

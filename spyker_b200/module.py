@@ -320,6 +320,9 @@ def threshold(array, threshold: float, value: float = 0.0, inplace: bool = True)
     return a.write_back() if a.kind != "cuda" else array
 
 
+_threshold_op = threshold
+
+
 def quantize(array, lower: float, middle: float, upper: float, inplace: bool = True):
     raise NotImplementedError("quantize is not part of the GPU hot path of this build")
 
@@ -566,6 +569,50 @@ class FC:
              wsb, stream())
         self.bpconfig.sfactor = float(bp[0])
         return x.back(nxt)
+
+
+def conv_fire_wta(array, conv: "Conv", threshold: float, radius, count: int, value: float = 0.0,
+                  inhibit_threshold: float = 0.0, fire_threshold: float = 0.0, wta_threshold: float = 0.0,
+                  precision: str | None = None):
+    """One fused layer step; returns ``(spikes, winners)`` equal to::
+
+        out = inhibit(threshold(conv(array), threshold, value), inhibit_threshold)
+        spikes, winners = fire(out, fire_threshold), convwta(out, radius, count, wta_threshold)
+
+    On the tensor-core precisions with u8 spikes, T <= 32, at least two output
+    channels and non-negative fire/WTA thresholds, a single tcgen05 kernel does
+    it without writing the potentials; otherwise the ops run one by one.
+    """
+    r2 = expand2(radius)
+    prec = precision or conv.precision or _conv_precision
+    x = Bound(array, conv.device).dev
+    s = to5(list(x.shape))
+    k = conv.kernel if conv.kernel.dtype == torch.float32 else conv.kernel.float()
+    k = k.contiguous()
+    cout, cin, kh, kw = k.shape
+    fused = (prec != "fp32" and x.dtype == torch.uint8 and s[1] <= 32 and cout >= 2 and fire_threshold >= 0
+             and wta_threshold >= 0 and count > 0 and min(r2) >= 0)
+    if fused:
+        oshape = shape.conv(s, list(k.shape), conv._stride, conv._pad)
+        nb = _lib.lib.spk_conv_fire_wta_workspace(s[0], s[1], cin, s[3], s[4], cout, kh, kw, conv._stride[0],
+                                                  conv._stride[1], i64(*conv._pad), _PRECISION[prec])
+        fused = nb > 0 and s[1] * cout * (128 // (1 << (s[1] - 1).bit_length())) <= 32768
+    if not fused:
+        out = inhibit(_threshold_op(conv_(x, conv, prec), threshold, value), inhibit_threshold)
+        return fire(out, fire_threshold), convwta(out, r2, count, wta_threshold)
+    spikes = torch.empty(oshape, dtype=torch.uint8, device=x.device)
+    rec = torch.zeros((s[0], count, 5), dtype=torch.int32, device=x.device)
+    cnt = torch.zeros((s[0],), dtype=torch.int32, device=x.device)
+    ws, wsb = _workspace(nb, x.device)
+    call("spk_conv_fire_wta", ptr(x), type_code(x.dtype), ptr(k), s[0], s[1], cin, s[3], s[4], cout, kh, kw,
+         conv._stride[0], conv._stride[1], i64(*conv._pad), float(threshold), float(value), float(inhibit_threshold),
+         float(fire_threshold), r2[0], r2[1], count, float(wta_threshold), ptr(spikes), ptr(rec), ptr(cnt),
+         _PRECISION[prec], ptr(ws), wsb, stream())
+    return spikes, Winners(rec, cnt)
+
+
+def conv_(x, layer: "Conv", prec: str):
+    return conv(x, layer.kernel, layer._stride, layer._pad, prec)
 
 
 def stdp(conv: Conv, array, winners, output) -> None:

@@ -380,3 +380,47 @@ def test_end_to_end_layer_bf16x3(golden):
     conv.stdp(codes, wins, spk)
     assert np.array_equal(host(conv.kernel), golden["stdp_kernel"])
     assert np.array_equal(host(spyker.pool(spk, 2)), golden["pooled"])
+
+
+# ---------------------------------------------------------------------------
+# fused layer: conv -> threshold -> inhibit -> fire + convwta in one kernel
+# ---------------------------------------------------------------------------
+
+FUSED = [
+    # b, t, cin, h, w, cout, k, pad, theta, radius, count
+    (16, 15, 2, 28, 28, 30, 5, 2, 15.0, 3, 5),
+    (12, 15, 30, 14, 14, 100, 5, 2, 10.0, 1, 8),
+    (3, 30, 8, 21, 19, 64, 7, 3, 20.0, 2, 6),
+    (7, 5, 3, 9, 11, 17, 3, 1, 2.5, 0, 40),
+]
+
+
+@pytest.mark.parametrize("case", FUSED)
+@pytest.mark.parametrize("prec", ["bf16x3", "bf16x2"])
+def test_fused_layer_matches_ops(port, case, prec):
+    b, t, cin, h, w, cout, k, pad, theta, radius, count = case
+    rng = np.random.default_rng(b * 7 + t)
+    fst = rng.integers(0, t + 4, size=(b, cin, h, w))
+    x = cuda((fst[:, None] <= np.arange(t)[None, :, None, None, None]).astype(np.uint8))
+    conv = spyker.Conv(cin, cout, k, pad=pad)
+    conv.kernel.copy_(cuda(rng.uniform(0.3, 1.0, size=(cout, cin, k, k)).astype(np.float32)))
+    conv.precision = prec
+    spikes, wins = spyker.conv_fire_wta(x, conv, theta, radius, count)
+    out = spyker.inhibit(spyker.threshold(conv(x), theta))
+    ref_spikes, ref_wins = spyker.fire(out), spyker.convwta(out, radius, count)
+    assert spyker._lib.lib.spk_device_status(1) == 0
+    assert np.array_equal(host(spikes), host(ref_spikes))
+    got, want = winners_np(wins), winners_np(ref_wins)
+    assert np.array_equal(got[1], want[1]) and np.array_equal(got[0], want[0])
+    assert int(got[1].sum()) > 0
+
+
+def test_fused_layer_golden(golden):
+    conv = spyker.Conv(2, 30, 5, pad=2)
+    conv.kernel.copy_(cuda(golden["kernel"]))
+    conv.precision = "bf16x3"
+    spikes, wins = spyker.conv_fire_wta(cuda(golden["codes"]), conv, 15.0, 3, 5)
+    assert np.array_equal(host(spikes), golden["fire"])
+    rec, cnt = winners_np(wins)
+    assert np.array_equal(cnt, golden["counts"])
+    assert np.array_equal(rec, oracle_winners(golden["winners"], golden["counts"])[0])
