@@ -58,6 +58,7 @@ struct TcParams
     int cin, h, w, cout, kh, kw, oh, ow, sy, sx, top, left;
     int kblocks, n_tile, n_tiles, nsplit, cpad, nhwc;
     uint32_t tmem_cols, idesc;
+    int stages, nacc;
     // fused spiking epilogue (kFused): rows are (pixel, t) with t fastest
     int T, tp_log2, pp, lp_log2;
     int64_t npix;
@@ -225,29 +226,25 @@ __device__ __forceinline__ void load_exact16(uint32_t lane_base, int c0, int n_t
     }
 }
 
-// Fused spiking epilogue over a tile of PP pixels x TP steps, with every
+// Fused spiking epilogue of one tile of PP pixels x TP steps, with every
 // output channel of a pixel in this CTA's tensor memory.  Restates, for the
 // pipeline  out = inhibit(threshold(conv(x), thr, thv), inh_thr);
 // spikes = fire(out, fire_thr); convwta(out, r, k, wta_thr):
-//   threshold  cpu/fire.cpp:41-51    x <= thr -> thv
+//   threshold  cpu/fire.cpp:41-51     x <= thr -> thv
 //   inhibit    cpu/inhibit.cpp:41-121 first-max channel per step, winner taken
 //              at step T - max(#steps whose max > inh_thr, 1), others x * 0
-//   fire       cpu/fire.cpp:67-82    x > fire_thr
-//   WTA key    cpu/wta.cpp:45-64     first step with x > wta_thr and its value
+//   fire       cpu/fire.cpp:67-82     x > fire_thr
+//   WTA key    cpu/wta.cpp:45-64      first step with x > wta_thr, its value
 // With fire_thr, wta_thr >= 0 only the winning channel of a pixel can spike or
 // hold a WTA key, so each pixel yields one record (channel, first step,
-// value) and the per-sample min / max of the inhibited potentials.
-// Warps 0-3 own the tensor-memory lanes; all warps write the spikes out.
-__device__ void fused_epilogue(const TcParams &P, unsigned char *smem, uint32_t lane_base, int warp, bool row_ok,
-                               int tstep, int64_t sample, int64_t pix)
+// value) and the per-sample min / max of the inhibited potentials.  Run by
+// warps 0-3, one (pixel, step) row per thread; `acc` is the accumulator base.
+__device__ void fused_epilogue(const TcParams &P, uint32_t acc, bool row_ok, int tstep, int64_t sample, int64_t pix)
 {
-    if (warp >= 4) return;  // warps 0-3 own the 128 tensor-memory lanes (one row each)
-    const int tid = threadIdx.x, lane = tid & 31;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int TP = 1 << P.tp_log2, T = P.T, C = P.cout;
-    // exact thresholded potentials of this row, cached in the idle stage buffers
-    const int ld = P.n_tile + 1;
-    float *vals = reinterpret_cast<float *>(smem) + tid * ld;
-    // pass over the accumulators: thresholded first-max channel of this (pixel, step)
+    const uint32_t lane_base = acc + (uint32_t(warp * 32) << 16);
+    // thresholded first-max channel of this (pixel, step)
     float mx = 0.f;
     int am = 0;
     for (int c0 = 0; c0 < P.n_tile; c0 += 16)
@@ -259,7 +256,6 @@ __device__ void fused_epilogue(const TcParams &P, unsigned char *smem, uint32_t 
         {
             const int c = c0 + j;
             const float x = (v[j] <= P.thr) ? P.thv : v[j];
-            vals[c] = x;
             if (c == 0)
                 mx = x;
             else if (c < C && x > mx)
@@ -272,19 +268,43 @@ __device__ void fused_epilogue(const TcParams &P, unsigned char *smem, uint32_t 
     const int n = __popc(above);
     const int ts = T - (n > 1 ? n : 1);
     const int win = __shfl_sync(0xffffffffu, am, base + ts);
-    const float vw = vals[win];  // thresholded value of the winning channel at this step
-    // spike of the winning channel (the others stay 0 since fire_thr >= 0;
-    // the spike tensor was zero-filled before the launch)
+    // exact value of the winning channel at this step: reload only the column
+    // chunks that hold the warp's winners
+    uint32_t pieces[3] = {0, 0, 0};
+    unsigned pending = 0xffffffffu;
+    while (pending)
+    {
+        const int c0 = (__shfl_sync(0xffffffffu, win, __ffs(pending) - 1) >> 4) << 4;
+        uint32_t r0[16], r1[16], r2[16];
+        tmem_ld16(lane_base + uint32_t(c0), r0);
+        tmem_ld16(lane_base + uint32_t(P.n_tile + c0), r1);
+        if (P.nsplit == 3) tmem_ld16(lane_base + uint32_t(2 * P.n_tile + c0), r2);
+        tmem_ld_wait();
+        const bool mine = (win >> 4) == (c0 >> 4);
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+            if (mine && c0 + j == win)
+            {
+                pieces[0] = r0[j], pieces[1] = r1[j];
+                if (P.nsplit == 3) pieces[2] = r2[j];
+            }
+        pending &= ~__ballot_sync(0xffffffffu, mine);
+    }
+    double accv = double(__uint_as_float(pieces[0])) + double(__uint_as_float(pieces[1]));
+    if (P.nsplit == 3) accv += double(__uint_as_float(pieces[2]));
+    const float raw = float(accv);
+    const float vw = (raw <= P.thr) ? P.thv : raw;
+    // spike of the winning channel (the spike tensor was zero-filled first)
     if (row_ok && vw > P.fire_thr) P.spikes[((sample * T + tstep) * C + win) * P.ohw + pix] = 1;
     // WTA record: first step whose inhibited value exceeds wta_thr
     const unsigned keyed = __ballot_sync(0xffffffffu, row_ok && vw > P.wta_thr) & grp;
     const int first_lane = keyed ? __ffs(keyed) - 1 : base;
     const float first_v = __shfl_sync(0xffffffffu, vw, first_lane);
-    const bool pixel_ok = __shfl_sync(0xffffffffu, row_ok ? 1 : 0, base) != 0;  // step 0 of the pixel is valid
+    const bool pixel_ok = __shfl_sync(0xffffffffu, row_ok ? 1 : 0, base) != 0;
     if (lane == base && pixel_ok)
         P.records[sample * P.ohw + pix] = make_int4(win, keyed ? first_lane - base : T, __float_as_int(first_v), 0);
-    // per-sample min / max of the inhibited values (winner value, and a zero
-    // from every losing channel when there is more than one channel)
+    // per-sample min / max of the inhibited values: the winner's value, and a
+    // zero from every losing channel when there is more than one channel
     float rmin = vw, rmax = vw;
     if (C > 1)
     {
@@ -302,26 +322,124 @@ __device__ void fused_epilogue(const TcParams &P, unsigned char *smem, uint32_t 
     }
 }
 
-template <int MODE>
-__global__ void __launch_bounds__(kTcThreads, 1) conv_tc_kernel(TcParams P)
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
 {
-    extern __shared__ __align__(1024) unsigned char smem[];
-    __shared__ __align__(8) uint64_t full_bar[2], done_bar[2];
-    __shared__ uint32_t tmem_slot;
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
 
-    const int tid = threadIdx.x, warp = tid >> 5;
-    const int row = tid & (BM - 1);
-    const int chunk0 = (tid >> 7) * 4;  // this thread gathers K chunks chunk0..chunk0+3 of its row
-    const int a_bytes = BM * BK * 2;                  // 16 KB
-    const int b_bytes = P.nsplit * P.n_tile * BK * 2;  // nsplit x n_tile x 128 B
-    unsigned char *const sA0 = smem;
-    unsigned char *const sB0 = smem + 2 * a_bytes;
-    int4 *tab = reinterpret_cast<int4 *>(smem + 2 * a_bytes + 2 * b_bytes);
-    const int taps = P.kh * P.kw;
+// Row of a tile: (image for the A gather, sample, step, output pixel).
+struct RowInfo
+{
+    bool ok;
+    int64_t img, sample, pix;
+    int tstep, iy0, ix0;
+};
 
+template <int MODE>
+__device__ __forceinline__ RowInfo row_info(const TcParams &P, int64_t mt, int row)
+{
+    RowInfo r{};
+    if constexpr (MODE == kPotentials)
+    {
+        const int64_t m = mt * BM + row;
+        r.ok = m < P.M;
+        if (r.ok) r.img = m / P.ohw, r.pix = m % P.ohw;
+    }
+    else
+    {
+        // row = (pixel in tile) * TP + t: all steps of a pixel in one warp
+        r.tstep = row & ((1 << P.tp_log2) - 1);
+        const int64_t gp = mt * P.pp + (row >> P.tp_log2);
+        r.ok = r.tstep < P.T && gp < P.npix;
+        if (r.ok) r.sample = gp / P.ohw, r.pix = gp % P.ohw, r.img = r.sample * P.T + r.tstep;
+    }
+    if (r.ok)
+    {
+        const int oy = int(r.pix / P.ow), ox = int(r.pix % P.ow);
+        r.iy0 = oy * P.sy - P.top;
+        r.ix0 = ox * P.sx - P.left;
+    }
+    return r;
+}
+
+// Raw bytes of four 8-wide K chunks of one A row (loads in flight until used).
+struct Gathered
+{
+    uint2 v[4];
+};
+
+template <typename RI>
+__device__ __forceinline__ void gather_load(const TcParams &P, const int4 *tab, const RI &r, const uint8_t *ib, int kb,
+                                            int c_lo, Gathered &g)
+{
     if (P.nhwc)
     {
-        // one entry per 8-wide K chunk: (ky, kx, channel offset, valid)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+        {
+            const int4 t = tab[kb * 8 + c_lo + j];
+            const int iy = r.iy0 + t.x, ix = r.ix0 + t.y;
+            g.v[j] = make_uint2(0, 0);
+            if (r.ok && t.w && iy >= 0 && iy < P.h && ix >= 0 && ix < P.w)
+                g.v[j] = *reinterpret_cast<const uint2 *>(ib + int64_t(iy) * P.rs + int64_t(ix) * P.ps + t.z);
+        }
+    }
+    else
+    {
+        const int64_t rowoff = int64_t(r.iy0) * P.rs + int64_t(r.ix0) * P.ps;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+        {
+            uint32_t w[2] = {0, 0};
+#pragma unroll
+            for (int e = 0; e < 8; ++e)
+            {
+                const int4 t = tab[kb * BK + (c_lo + j) * 8 + e];
+                const int iy = r.iy0 + t.y, ix = r.ix0 + t.z;
+                uint32_t b8 = 0;
+                if (r.ok && t.w && iy >= 0 && iy < P.h && ix >= 0 && ix < P.w) b8 = ib[rowoff + t.x];
+                w[e >> 2] |= b8 << (8 * (e & 3));
+            }
+            g.v[j] = make_uint2(w[0], w[1]);
+        }
+    }
+}
+
+__device__ __forceinline__ void gather_store(const TcParams &, const Gathered &g, unsigned char *a, int c_lo)
+{
+#pragma unroll
+    for (int j = 0; j < 4; ++j) *reinterpret_cast<uint4 *>(a + (c_lo + j) * 128) = bf16x8_of_bytes(g.v[j]);
+}
+
+// Warp-specialised persistent kernel (416 threads):
+//   warps 4-11 producers: per K block, wait for a free stage, bulk-copy the
+//              weight block (thread 128) and gather half an A row each;
+//   warp 12    one thread issues the tcgen05.mma of every stage into one of
+//              (up to) two tensor-memory accumulators and commits;
+//   warps 0-3  epilogue: read the accumulator of a finished tile (one row per
+//              thread) while the next tile is being multiplied.
+// Stage ring: full[s] (256 producer arrivals + the weight bytes), empty[s]
+// (MMA commit); accumulators: acc_full[a] (MMA commit), acc_empty[a] (128
+// epilogue arrivals).  Every wait is bounded; a timeout raises the device
+// status word and makes every role leave.
+constexpr int kWsThreads = 416, kMaxStages = 6;
+
+template <int MODE>
+__global__ void __launch_bounds__(kWsThreads, 1) conv_ws_kernel(TcParams P)
+{
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ __align__(8) uint64_t full_bar[kMaxStages], empty_bar[kMaxStages], accf_bar[2], acce_bar[2];
+    __shared__ uint32_t tmem_slot;
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int S = P.stages, nacc = P.nacc;
+    const int a_bytes = BM * BK * 2;
+    const int b_bytes = P.nsplit * P.n_tile * BK * 2;
+    const int stage_bytes = a_bytes + b_bytes;
+    int4 *tab = reinterpret_cast<int4 *>(smem + S * stage_bytes);
+    const int taps = P.kh * P.kw;
+    if (P.nhwc)
+    {
         const int groups = P.cpad / 8;
         for (int q = tid; q < P.kblocks * 8; q += blockDim.x)
         {
@@ -331,7 +449,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) conv_tc_kernel(TcParams P)
     }
     else
     {
-        // one entry per k: (offset in the image, ky, kx, valid)
         for (int k = tid; k < P.kblocks * BK; k += blockDim.x)
         {
             const int c = k / taps, tap = k % taps, ky = tap / P.kw, kx = tap % P.kw;
@@ -340,10 +457,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) conv_tc_kernel(TcParams P)
     }
     if (tid == 0)
     {
-        mbar_init(&full_bar[0], 1);
-        mbar_init(&full_bar[1], 1);
-        mbar_init(&done_bar[0], 1);
-        mbar_init(&done_bar[1], 1);
+        for (int s = 0; s < S; ++s) mbar_init(&full_bar[s], 257), mbar_init(&empty_bar[s], 1);
+        for (int a = 0; a < 2; ++a) mbar_init(&accf_bar[a], 1), mbar_init(&acce_bar[a], 128);
         fence_mbar_init();
     }
     if (warp == 0)
@@ -355,179 +470,147 @@ __global__ void __launch_bounds__(kTcThreads, 1) conv_tc_kernel(TcParams P)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = tmem_slot;
+    const int acc_cols = P.nsplit * P.n_tile;
 
-    uint32_t uses[2] = {0, 0}, waited[2] = {0, 0};
-    uint32_t it = 0;
-    bool failed = false;
-
-    for (int64_t tile = blockIdx.x; tile < P.tiles; tile += gridDim.x)
+    if (warp >= 4 && warp < 12)
     {
-        const int64_t mt = tile / P.n_tiles;
-        const int nt = int(tile % P.n_tiles);
-        bool row_ok;
-        int64_t img = 0, pix = 0, sample = 0, gp = 0;
-        int tstep = 0;
-        if constexpr (MODE == kPotentials)
+        // ---------------- producers (8 warps) ----------------
+        // Thread p gathers K chunks c_lo..c_lo+3 of row prow.  The loads of the
+        // next K block are issued before waiting for a free stage, so the
+        // gather latency overlaps the wait and the previous block's stores.
+        const int p = tid - 128;
+        const int prow = p & (BM - 1), c_lo = (p >> 7) * 4;
+        uint32_t it = 0;
+        int64_t tile = blockIdx.x;
+        int kb = 0;
+        if (tile < P.tiles)
         {
-            const int64_t m = mt * BM + row;
-            row_ok = m < P.M;
-            if (row_ok) img = m / P.ohw, pix = m % P.ohw;
-        }
-        else
-        {
-            // row = (pixel in tile) * TP + t; all steps of a pixel in one warp
-            tstep = row & ((1 << P.tp_log2) - 1);
-            gp = mt * P.pp + (row >> P.tp_log2);
-            row_ok = tstep < P.T && gp < P.npix;
-            if (row_ok) sample = gp / P.ohw, pix = gp % P.ohw, img = sample * P.T + tstep;
-        }
-        int iy0 = 0, ix0 = 0;
-        if (row_ok)
-        {
-            const int oy = int(pix / P.ow), ox = int(pix % P.ow);
-            iy0 = oy * P.sy - P.top;
-            ix0 = ox * P.sx - P.left;
-        }
-        const uint8_t *img_base =
-            (MODE == kPotentials) ? P.in + img * P.img_stride : P.in + sample * P.img_stride + tstep * P.ts;
-
-        for (int kb = 0; kb < P.kblocks; ++kb, ++it)
-        {
-            const int st = it & 1;
-            unsigned char *sA = sA0 + st * a_bytes;
-            unsigned char *sB = sB0 + st * b_bytes;
-            bool ok = true;
-            if (waited[st] < uses[st])
+            RowInfo r = row_info<MODE>(P, tile / P.n_tiles, prow);
+            const uint8_t *ib = (MODE == kPotentials) ? P.in + r.img * P.img_stride
+                                                      : P.in + r.sample * P.img_stride + r.tstep * P.ts;
+            Gathered cur;
+            gather_load(P, tab, r, ib, kb, c_lo, cur);
+            while (true)
             {
-                ok = wait_bounded(&done_bar[st], (uses[st] - 1) & 1);
-                waited[st] = uses[st];
-            }
-            if (__syncthreads_or(!ok))
-            {
-                failed = true;
-                break;
-            }
-            // Stage st is free: fetch the weight block with the bulk-copy engine.
-            if (tid == 0)
-            {
-                arrive_expect_tx(&full_bar[st], uint32_t(b_bytes));
-                bulk_g2s(sB, P.wimg + (int64_t(nt) * P.kblocks + kb) * b_bytes, uint32_t(b_bytes), &full_bar[st]);
-            }
-            // Gather this thread's 4 K chunks of its row.
-            unsigned char *a = sA + (row >> 3) * 1024 + (row & 7) * 16;
-            if (P.nhwc)
-            {
-#pragma unroll
-                for (int j = 0; j < 4; ++j)
+                // next (tile, k block) and its loads
+                int64_t ntile = tile;
+                int nkb = kb + 1;
+                if (nkb == P.kblocks) nkb = 0, ntile += gridDim.x;
+                const bool more = ntile < P.tiles;
+                RowInfo nr = r;
+                const uint8_t *nib = ib;
+                Gathered nxt;
+                if (more)
                 {
-                    const int kc = chunk0 + j;
-                    const int4 t = tab[kb * 8 + kc];
-                    const int iy = iy0 + t.x, ix = ix0 + t.y;
-                    uint4 v = make_uint4(0, 0, 0, 0);
-                    if (row_ok && t.w && iy >= 0 && iy < P.h && ix >= 0 && ix < P.w)
-                        v = bf16x8_of_bytes(*reinterpret_cast<const uint2 *>(
-                            img_base + int64_t(iy) * P.rs + int64_t(ix) * P.ps + t.z));
-                    *reinterpret_cast<uint4 *>(a + kc * 128) = v;
+                    if (ntile != tile)
+                    {
+                        nr = row_info<MODE>(P, ntile / P.n_tiles, prow);
+                        nib = (MODE == kPotentials) ? P.in + nr.img * P.img_stride
+                                                    : P.in + nr.sample * P.img_stride + nr.tstep * P.ts;
+                    }
+                    gather_load(P, tab, nr, nib, nkb, c_lo, nxt);
+                }
+                const int s = int(it % uint32_t(S));
+                const uint32_t u = it / uint32_t(S);
+                if (u > 0 && !wait_bounded(&empty_bar[s], (u - 1) & 1)) break;
+                unsigned char *sA = smem + s * stage_bytes;
+                if (p == 0)
+                {
+                    const int nt = int(tile % P.n_tiles);
+                    arrive_expect_tx(&full_bar[s], uint32_t(b_bytes));
+                    bulk_g2s(sA + a_bytes, P.wimg + (int64_t(nt) * P.kblocks + kb) * b_bytes, uint32_t(b_bytes),
+                             &full_bar[s]);
+                }
+                gather_store(P, cur, sA + (prow >> 3) * 1024 + (prow & 7) * 16, c_lo);
+                fence_proxy_async_smem();
+                mbar_arrive(&full_bar[s]);
+                ++it;
+                if (!more) break;
+                tile = ntile, kb = nkb, r = nr, ib = nib, cur = nxt;
+            }
+        }
+    }
+    else if (warp == 12)
+    {
+        // ---------------- MMA issuer ----------------
+        if (lane == 0)
+        {
+            uint32_t it = 0, j = 0;
+            bool failed = false;
+            for (int64_t tile = blockIdx.x; tile < P.tiles && !failed; tile += gridDim.x, ++j)
+            {
+                const int a = int(j % uint32_t(nacc));
+                const uint32_t ua = j / uint32_t(nacc);
+                if (ua > 0 && !wait_bounded(&acce_bar[a], (ua - 1) & 1)) break;
+                tc_fence_after();
+                const uint32_t d = tmem + uint32_t(a * acc_cols);
+                for (int kb = 0; kb < P.kblocks; ++kb, ++it)
+                {
+                    const int s = int(it % uint32_t(S));
+                    const uint32_t u = it / uint32_t(S);
+                    if (!wait_bounded(&full_bar[s], u & 1))
+                    {
+                        failed = true;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t a_base = smem_u32(smem + s * stage_bytes);
+                    const uint32_t b_base = a_base + uint32_t(a_bytes);
+                    for (int p = 0; p < P.nsplit; ++p)
+#pragma unroll
+                        for (int k16 = 0; k16 < BK / 16; ++k16)
+                        {
+                            const uint64_t ad = smem_desc(a_base + k16 * 256, 128, 1024);
+                            const uint64_t bd = smem_desc(b_base + p * P.n_tile * 128 + k16 * 256, 128, 1024);
+                            mma_bf16(d + uint32_t(p * P.n_tile), ad, bd, P.idesc, (kb > 0 || k16 > 0) ? 1u : 0u);
+                        }
+                    mma_commit(&empty_bar[s]);
+                }
+                if (!failed) mma_commit(&accf_bar[a]);
+            }
+        }
+        __syncwarp();
+    }
+    else
+    {
+        // ---------------- epilogue (warps 0-3) ----------------
+        uint32_t j = 0;
+        for (int64_t tile = blockIdx.x; tile < P.tiles; tile += gridDim.x, ++j)
+        {
+            const int a = int(j % uint32_t(nacc));
+            const uint32_t ua = j / uint32_t(nacc);
+            if (!wait_bounded(&accf_bar[a], ua & 1)) break;
+            tc_fence_after();
+            const int64_t mt = tile / P.n_tiles;
+            const int nt = int(tile % P.n_tiles);
+            const RowInfo r = row_info<MODE>(P, mt, tid);
+            const uint32_t acc = tmem + uint32_t(a * acc_cols);
+            if constexpr (MODE == kPotentials)
+            {
+                const uint32_t lane_base = acc + (uint32_t(warp * 32) << 16);
+                for (int c0 = 0; c0 < P.n_tile; c0 += 16)
+                {
+                    float v[16];
+                    load_exact16(lane_base, c0, P.n_tile, P.nsplit, v);
+                    if (r.ok)
+                    {
+#pragma unroll
+                        for (int q = 0; q < 16; ++q)
+                        {
+                            const int n = nt * P.n_tile + c0 + q;
+                            if (n < P.cout) P.out[(r.img * P.cout + n) * P.ohw + r.pix] = v[q];
+                        }
+                    }
                 }
             }
             else
             {
-                const int64_t rowoff = int64_t(iy0) * P.rs + int64_t(ix0) * P.ps;
-#pragma unroll
-                for (int j = 0; j < 4; ++j)
-                {
-                    const int kc = chunk0 + j;
-                    uint32_t pk[4];
-#pragma unroll
-                    for (int e = 0; e < 8; e += 2)
-                    {
-                        uint32_t v2[2];
-#pragma unroll
-                        for (int q = 0; q < 2; ++q)
-                        {
-                            const int4 t = tab[kb * BK + kc * 8 + e + q];
-                            const int iy = iy0 + t.y, ix = ix0 + t.z;
-                            uint32_t v = 0;
-                            if (row_ok && t.w && iy >= 0 && iy < P.h && ix >= 0 && ix < P.w)
-                            {
-                                const uint32_t u = img_base[rowoff + t.x];
-                                v = u <= 1u ? u * 0x3F80u : bf16_of_byte(u);
-                            }
-                            v2[q] = v;
-                        }
-                        pk[e / 2] = v2[0] | (v2[1] << 16);
-                    }
-                    *reinterpret_cast<uint4 *>(a + kc * 128) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
-                }
+                fused_epilogue(P, acc, r.ok, r.tstep, r.sample, r.pix);
             }
-            // The weight block must have landed before anyone proceeds.
-            ok = wait_bounded(&full_bar[st], uses[st] & 1);
-            fence_proxy_async_smem();
-            if (__syncthreads_or(!ok))
-            {
-                failed = true;
-                break;
-            }
-            if (tid == 0)
-            {
-                tc_fence_after();
-                const uint32_t a_base = smem_u32(sA), b_base = smem_u32(sB);
-                for (int p = 0; p < P.nsplit; ++p)
-#pragma unroll
-                    for (int s = 0; s < BK / 16; ++s)
-                    {
-                        const uint64_t ad = smem_desc(a_base + s * 256, 128, 1024);
-                        const uint64_t bd = smem_desc(b_base + p * P.n_tile * 128 + s * 256, 128, 1024);
-                        mma_bf16(tmem + uint32_t(p * P.n_tile), ad, bd, P.idesc, (kb > 0 || s > 0) ? 1u : 0u);
-                    }
-                mma_commit(&done_bar[st]);
-            }
-            ++uses[st];
+            tc_fence_before();
+            mbar_arrive(&acce_bar[a]);
         }
-        if (failed) break;
-
-        // Epilogue: all MMAs of the tile are complete once its last commit is.
-        {
-            const int last = (it - 1) & 1;
-            const bool ok = wait_bounded(&done_bar[last], (uses[last] - 1) & 1);
-            waited[0] = uses[0], waited[1] = uses[1];
-            if (__syncthreads_or(!ok))
-            {
-                failed = true;
-                break;
-            }
-        }
-        tc_fence_after();
-        const uint32_t lane_base = tmem + (uint32_t((warp & 3) * 32) << 16);
-        if constexpr (MODE == kPotentials)
-        {
-            for (int c0 = (warp >> 2) * 16; c0 < P.n_tile; c0 += 32)
-            {
-                float v[16];
-                load_exact16(lane_base, c0, P.n_tile, P.nsplit, v);
-                if (row_ok)
-                {
-#pragma unroll
-                    for (int j = 0; j < 16; ++j)
-                    {
-                        const int n = nt * P.n_tile + c0 + j;
-                        if (n < P.cout) P.out[(img * P.cout + n) * P.ohw + pix] = v[j];
-                    }
-                }
-            }
-        }
-        else
-        {
-            fused_epilogue(P, smem, lane_base, warp, row_ok, tstep, sample, pix);
-        }
-        tc_fence_before();
-        __syncthreads();
     }
-
-    // Teardown: no MMA may still be writing tensor memory when it is freed.
-    if (!failed)
-        for (int st = 0; st < 2; ++st)
-            if (waited[st] < uses[st]) wait_bounded(&done_bar[st], (uses[st] - 1) & 1);
     tc_fence_before();
     __syncthreads();
     if (warp == 0)
@@ -607,7 +690,7 @@ __global__ void wta_records_kernel(const int4 *__restrict__ records, const unsig
 
 struct Plan
 {
-    int nsplit, n_tile, n_tiles, kblocks, cpad;
+    int nsplit, n_tile, n_tiles, kblocks, cpad, stages, nacc;
     bool nhwc;
     uint32_t tmem_cols;
     size_t wimg_bytes, xt_bytes, smem;
@@ -627,15 +710,22 @@ Plan make_plan(int64_t n, int64_t cin, int64_t h, int64_t w, int64_t cout, int64
     pl.cpad = int(ceil_div(cin, 8) * 8);
     const int64_t kreal = pl.nhwc ? kh * kw * pl.cpad : kh * kw * cin;
     pl.kblocks = int(ceil_div(kreal, BK));
-    uint32_t need = uint32_t(pl.nsplit * pl.n_tile), cols = 32;
-    while (cols < need) cols <<= 1;
+    // two accumulators (the epilogue of one tile overlaps the MMAs of the
+    // next) when they fit in the 512 tensor-memory columns
+    const uint32_t acc_cols = uint32_t(pl.nsplit * pl.n_tile);
+    pl.nacc = 2 * acc_cols <= 512 ? 2 : 1;
+    uint32_t cols = 32;
+    while (cols < pl.nacc * acc_cols) cols <<= 1;
     pl.tmem_cols = cols;
     pl.wimg_bytes = size_t(pl.n_tiles) * pl.kblocks * pl.nsplit * pl.n_tile * BK * 2;
     // staged copy of the spikes: channels-last [N, H, W, Cpad] (plain), or
     // [B, H, W, T, Cpad or Cin] (fused; single_tile), where every call stages
     pl.xt_bytes = pl.nhwc ? size_t(n) * h * w * pl.cpad : (single_tile ? size_t(n) * h * w * cin : 0);
     const size_t tab = pl.nhwc ? size_t(pl.kblocks) * 8 * 16 : size_t(pl.kblocks) * BK * 16;
-    size_t smem = 2 * size_t(BM * BK * 2) + 2 * size_t(pl.nsplit) * pl.n_tile * BK * 2 + tab;
+    const size_t stage = size_t(BM * BK * 2) + size_t(pl.nsplit) * pl.n_tile * BK * 2;
+    const size_t budget = 225 * 1024 - tab;
+    pl.stages = int(std::min<size_t>(4, budget / stage));
+    size_t smem = size_t(pl.stages) * stage + tab;
     // At most 512 / tmem_cols CTAs may share an SM's tensor memory: size the
     // shared memory so that no more fit.
     const int per_sm = int(512 / cols);
@@ -694,7 +784,7 @@ TcParams prepare(const Plan &pl, const void *in, const float *kernel, int64_t n,
                  uint8_t *ws, cudaStream_t s, int64_t t_fused = 0)
 {
     SPK_REQUIRE(pl.kblocks <= kMaxKBlocks, "Cin*KH*KW is too large for the tensor-core path");
-    SPK_REQUIRE(pl.smem <= 227 * 1024, "tile does not fit in shared memory");
+    SPK_REQUIRE(pl.stages >= 2 && pl.smem <= 227 * 1024, "tile does not fit in shared memory");
     SPK_REQUIRE((reinterpret_cast<uintptr_t>(ws) & 255) == 0, "workspace must be 256-byte aligned");
     uint8_t *wimg = ws;
     const int64_t wthreads = int64_t(pl.n_tiles) * pl.kblocks * pl.n_tile * 8;
@@ -738,6 +828,7 @@ TcParams prepare(const Plan &pl, const void *in, const float *kernel, int64_t n,
     P.kblocks = pl.kblocks, P.n_tile = pl.n_tile, P.n_tiles = pl.n_tiles, P.nsplit = pl.nsplit;
     P.cpad = pl.cpad, P.nhwc = pl.nhwc ? 1 : 0;
     P.tmem_cols = pl.tmem_cols;
+    P.stages = pl.stages, P.nacc = pl.nacc;
     P.idesc = idesc_bf16_f32(BM, pl.n_tile);
     return P;
 }
@@ -745,13 +836,13 @@ TcParams prepare(const Plan &pl, const void *in, const float *kernel, int64_t n,
 template <int MODE>
 void launch(const TcParams &P, const Plan &pl, cudaStream_t s)
 {
-    auto kern = conv_tc_kernel<MODE>;
+    auto kern = conv_ws_kernel<MODE>;
     SPK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(pl.smem)));
     int per_sm = 1;
-    SPK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTcThreads, pl.smem));
+    SPK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kWsThreads, pl.smem));
     per_sm = std::max(1, std::min<int>(per_sm, int(512 / pl.tmem_cols)));
     const int64_t grid = std::min<int64_t>(P.tiles, int64_t(sm_count()) * per_sm);
-    kern<<<unsigned(grid), kTcThreads, pl.smem, s>>>(P);
+    kern<<<unsigned(grid), kWsThreads, pl.smem, s>>>(P);
     SPK_LAUNCHED();
 }
 
