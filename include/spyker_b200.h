@@ -147,7 +147,8 @@ spk_status spk_rank_fcwta(const void *in, spk_dtype type, int64_t b, int64_t t, 
 /* ---- STDP (Core::rank_convstdp/rank_fcstdp, impl.h:284-296) -------------- */
 /* configs_host: [nconf, 5] = (positive, negative, stabilize, lower, upper),
  * STDPConfig of src/spyker/utils.h:505-524 (nconf <= 16). */
-size_t spk_rank_convstdp_workspace(int64_t b, int64_t count, int64_t cin, int64_t kh, int64_t kw);
+size_t spk_rank_convstdp_workspace(int64_t b, int64_t count, int64_t cin, int64_t h, int64_t w, int64_t kh,
+                                   int64_t kw);
 /* in [B, T, Cin, H, W] spikes, kernel [Cout, Cin, KH, KW] F32 updated in place,
  * out [B, T, Cout, OH, OW] spikes; sequential in (sample, winner) order per
  * feature map (cpu/stdp.cpp:99-169). */
@@ -161,8 +162,9 @@ spk_status spk_rank_convstdp(const void *in, spk_dtype itype, int64_t b, int64_t
  * cudaMalloc while a CUDA graph is being captured, or hosts whose allocator
  * owns the device): its scratch lives in a static 32 MiB device array that
  * every GPU loading the library holds until exit, so the call allocates
- * nothing.  Calls needing more scratch than that (see
- * spk_rank_convstdp_workspace) fail with SPK_ERR_ARGUMENT; split the batch.
+ * nothing.  Calls needing more scratch than that (2*B*count*Cin*KH*KW bytes
+ * plus 2*B*count, each rounded up to 256) fail with SPK_ERR_ARGUMENT; split
+ * the batch.
  * The first call on a device looks up the array's device address; make that
  * first call before any stream capture.  All calls share the array, so calls
  * that overlap on the GPU (different streams, or other threads) race. */

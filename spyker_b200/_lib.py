@@ -43,7 +43,7 @@ SIGNATURES = {
     "spk_rank_convwta": (_INT, [_P, _INT, _I, _I, _I, _I, _I, _I, _I, _I, _D, _P, _P, _P, _S, _P]),
     "spk_rank_fcwta_workspace": (_S, [_I, _I, _I]),
     "spk_rank_fcwta": (_INT, [_P, _INT, _I, _I, _I, _I, _I, _D, _P, _P, _P, _S, _P]),
-    "spk_rank_convstdp_workspace": (_S, [_I, _I, _I, _I, _I]),
+    "spk_rank_convstdp_workspace": (_S, [_I, _I, _I, _I, _I, _I, _I]),
     "spk_rank_convstdp": (_INT, [_P, _INT, _I, _I, _I, _I, _I, _P, _I, _I, _I, _P, _I, _I, _P, _I, _P, _P, _I,
                                  _I, _I, _P, _P, _S, _P]),
     "spk_rank_convstdp_noalloc": (_INT, [_P, _INT, _I, _I, _I, _I, _I, _P, _I, _I, _I, _P, _I, _I, _P, _I, _P, _P,

@@ -5,30 +5,77 @@ namespace spk
 {
 namespace
 {
+// shuffle-able carrier of each element type
+template <typename T>
+struct Wide
+{
+    using type = T;
+};
+template <>
+struct Wide<uint8_t>
+{
+    using type = int;
+};
 // src/spyker/cpu/pool.cpp:53-86: zero pad, then max over the window
 // (initial value Limits<T>::min()); on cumulative spikes this is the earliest
 // spike in the window.  One thread per output element.
-template <typename T>
-__global__ void pool_kernel(const T *__restrict__ in, T *__restrict__ out, int64_t n, int64_t h, int64_t w, int64_t oh,
-                            int64_t ow, int ky, int kx, int sy, int sx, int top, int left)
+// Index type I: 32-bit when the output has fewer than 2^31 elements (integer
+// division by a runtime value is several times cheaper than in 64 bits).
+template <typename T, typename I>
+__global__ void pool_kernel(const T *__restrict__ in, T *__restrict__ out, I n, I h, I w, I oh, I ow, int ky, int kx,
+                            int sy, int sx, int top, int left)
 {
-    const int64_t total = n * oh * ow;
-    for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < total; k += int64_t(gridDim.x) * blockDim.x)
+    const I total = n * oh * ow;
+    for (I k = I(blockIdx.x) * blockDim.x + threadIdx.x; k < total; k += I(gridDim.x) * blockDim.x)
     {
-        int64_t xo = k % ow, r = k / ow, yo = r % oh, p = r / oh;
-        const T *plane = in + p * h * w;
+        const I r = k / ow, xo = k - r * ow, p = r / oh, yo = r - p * oh;
+        const T *plane = in + int64_t(p) * h * w;
         T m = Lowest<T>::v();
         for (int a = 0; a < ky; ++a)
         {
-            int64_t yy = yo * sy + a - top;
+            const int yy = int(yo) * sy + a - top;
             for (int b = 0; b < kx; ++b)
             {
-                int64_t xx = xo * sx + b - left;
-                T v = (yy >= 0 && yy < h && xx >= 0 && xx < w) ? plane[yy * w + xx] : T(0);
+                const int xx = int(xo) * sx + b - left;
+                T v = (yy >= 0 && yy < int(h) && xx >= 0 && xx < int(w)) ? plane[yy * int64_t(w) + xx] : T(0);
                 m = (m < v) ? v : m;  // std::max(m, v)
             }
         }
         out[k] = m;
+    }
+}
+
+// Large windows (e.g. global pooling): one warp per output element, the
+// lanes striding over the window and a shuffle max at the end (max is order
+// independent, so this equals the reference's sequential scan).
+template <typename T, typename I>
+__global__ void pool_warp_kernel(const T *__restrict__ in, T *__restrict__ out, I n, I h, I w, I oh, I ow, int ky,
+                                 int kx, int sy, int sx, int top, int left)
+{
+    const int lane = threadIdx.x & 31;
+    const I total = n * oh * ow;
+    const I warps = (I(gridDim.x) * blockDim.x) >> 5;
+    for (I k = (I(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; k < total; k += warps)
+    {
+        const I r = k / ow, xo = k - r * ow, p = r / oh, yo = r - p * oh;
+        const T *plane = in + int64_t(p) * h * w;
+        T m = Lowest<T>::v();
+        int a = lane / kx, b = lane % kx;  // window position of this lane, advanced by 32 per step
+        const int da = 32 / kx, db = 32 % kx;
+        for (int i = lane; i < ky * kx; i += 32)
+        {
+            const int yy = int(yo) * sy + a - top, xx = int(xo) * sx + b - left;
+            const T v = (yy >= 0 && yy < int(h) && xx >= 0 && xx < int(w)) ? plane[yy * int64_t(w) + xx] : T(0);
+            m = (m < v) ? v : m;
+            a += da, b += db;
+            if (b >= kx) b -= kx, ++a;
+        }
+        for (int o = 16; o > 0; o >>= 1)
+        {
+            const T v = T(__shfl_xor_sync(0xffffffffu, (typename Wide<T>::type)(m), o));
+            m = (m < v) ? v : m;
+        }
+        if (lane == 0) out[k] = m;
     }
 }
 
@@ -94,8 +141,22 @@ spk_status spk_rank_pool(const void *in, void *out, spk_dtype type, int64_t n, i
         if (n == 0) return;
         dispatch(type, [&](auto z) {
             using T = decltype(z);
-            pool_kernel<T><<<grid_for(n * oh * ow, 256), 256, 0, stream_of(stream)>>>(
-                (const T *)in, (T *)out, n, h, w, oh, ow, int(ky), int(kx), int(sy), int(sx), int(p.top), int(p.left));
+            const bool small = n * oh * ow * 32 < (int64_t(1) << 31) && n * h * w < (int64_t(1) << 31);
+            auto go = [&](auto idx) {
+                using I = decltype(idx);
+                if (ky * kx >= 64)
+                    pool_warp_kernel<T, I><<<grid_for(n * oh * ow * 32, 256, 16), 256, 0, stream_of(stream)>>>(
+                        (const T *)in, (T *)out, I(n), I(h), I(w), I(oh), I(ow), int(ky), int(kx), int(sy), int(sx),
+                        int(p.top), int(p.left));
+                else
+                    pool_kernel<T, I><<<grid_for(n * oh * ow, 256, 16), 256, 0, stream_of(stream)>>>(
+                        (const T *)in, (T *)out, I(n), I(h), I(w), I(oh), I(ow), int(ky), int(kx), int(sy), int(sx),
+                        int(p.top), int(p.left));
+            };
+            if (small)
+                go(uint32_t());
+            else
+                go(int64_t());
             SPK_LAUNCHED();
         });
     });

@@ -15,6 +15,9 @@
 
 namespace spk
 {
+inline size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
+size_t convstdp_prepost_bytes(int64_t b, int64_t count, int64_t cin, int64_t kh, int64_t kw);
+
 namespace
 {
 constexpr int kMaxConfigs = 16;
@@ -22,6 +25,7 @@ constexpr int kScanThreads = 256;
 constexpr int kScanPerThread = 4;  // weights per thread held in registers
 constexpr int kScanChunk = kScanThreads * kScanPerThread;
 constexpr int kWinnerTile = 1024;
+constexpr int kPreBatch = 14;  // winners whose pre rows are staged at once (28 KB)
 
 struct Configs
 {
@@ -70,6 +74,51 @@ __global__ void conv_prepost_kernel(const T *__restrict__ in, const T *__restric
     }
 }
 
+// First-spike map of the whole input, [B, Cin, H, W] u16 (T when silent):
+// one coalesced pass over the spikes instead of T strided loads per
+// receptive-field element and winner.
+template <typename T>
+__global__ void first_spike_map_kernel(const T *__restrict__ in, uint16_t *__restrict__ fst, int64_t b, int t,
+                                       int64_t x)
+{
+    const int64_t total = b * x;
+    for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < total; k += int64_t(gridDim.x) * blockDim.x)
+    {
+        const int64_t s = k / x, j = k - s * x;
+        fst[k] = first_spike(in + s * t * x + j, t, x);
+    }
+}
+
+// Kernel A (conv) on the first-spike map: one CTA per (sample, winner slot).
+template <typename T>
+__global__ void conv_prepost_map_kernel(const uint16_t *__restrict__ fst, const T *__restrict__ out, int t, int cin,
+                                        int h, int w, int cout, int oh, int ow, int kh, int kw, int sy, int sx, int top,
+                                        int left, const int32_t *__restrict__ winners,
+                                        const int32_t *__restrict__ counts, int count, uint16_t *__restrict__ pre,
+                                        uint16_t *__restrict__ post)
+{
+    const int s = blockIdx.x / count, j = blockIdx.x % count;
+    if (j >= counts[s]) return;
+    const int32_t *e = winners + (int64_t(s) * count + j) * 5;
+    const int wz = e[2], wy = e[3], wx = e[4];
+    const int k = cin * kh * kw;
+    uint16_t *p = pre + (int64_t(s) * count + j) * k;
+    const uint16_t *f = fst + int64_t(s) * cin * h * w;
+    for (int i = threadIdx.x; i < k; i += blockDim.x)
+    {
+        const int c = i / (kh * kw), r = i % (kh * kw), ky = r / kw, kx = r % kw;
+        const int yy = wy * sy + ky - top, xx = wx * sx + kx - left;
+        p[i] = (yy >= 0 && yy < h && xx >= 0 && xx < w) ? f[(int64_t(c) * h + yy) * w + xx] : uint16_t(t);
+    }
+    if (threadIdx.x == 0)
+    {
+        const int64_t ostride = int64_t(cout) * oh * ow;
+        const bool ok = wz >= 0 && wz < cout && wy >= 0 && wy < oh && wx >= 0 && wx < ow;
+        post[int64_t(s) * count + j] =
+            ok ? first_spike(out + int64_t(s) * t * ostride + (int64_t(wz) * oh + wy) * ow + wx, t, ostride) : 0;
+    }
+}
+
 // Kernel A (fc): pre per (sample, input), post per (sample, winner slot).
 template <typename T>
 __global__ void fc_prepost_kernel(const T *__restrict__ in, const T *__restrict__ out, int64_t b, int t, int ni, int no,
@@ -102,6 +151,8 @@ __global__ void __launch_bounds__(kScanThreads)
                      Configs cfg)
 {
     __shared__ int32_t s_rec[kWinnerTile][3];  // (config, sample, slot) of matching winners
+    __shared__ uint16_t s_pre[kPreBatch][kScanChunk];
+    __shared__ uint16_t s_post[kPreBatch];
     __shared__ int s_n;
     const int map = blockIdx.x;
     const int64_t base = int64_t(blockIdx.y) * kScanChunk;
@@ -155,27 +206,41 @@ __global__ void __launch_bounds__(kScanThreads)
             __syncthreads();
         }
         const int n = s_n;
-        for (int q = 0; q < n; ++q)
+        // Matching winners in batches: their pre rows (this CTA's chunk) are
+        // staged in shared memory with coalesced loads, then applied in order.
+        for (int q0 = 0; q0 < n; q0 += kPreBatch)
         {
-            const int c = s_rec[q][0];
-            const int64_t s = s_rec[q][1], j = s_rec[q][2];
-            const uint16_t po = post[s * count + j];
-            const uint16_t *pr = pre + s * ps + j * pw;
-            const double pos = cfg.pos[c], neg = cfg.neg[c], lo = cfg.lo[c], hi = cfg.hi[c];
-            const bool stab = cfg.stab[c] != 0;
+            const int nb = min(kPreBatch, n - q0);
+            const int len = (k - base < int64_t(kScanChunk)) ? int(k - base) : kScanChunk;
+            for (int i = threadIdx.x; i < nb * len; i += blockDim.x)
+            {
+                const int q = i / len, e = i % len;
+                const int64_t s = s_rec[q0 + q][1], j = s_rec[q0 + q][2];
+                s_pre[q][e] = pre[s * ps + j * pw + base + e];
+                if (e == 0) s_post[q] = post[s * count + j];
+            }
+            __syncthreads();
+            for (int q = 0; q < nb; ++q)
+            {
+                const int c = s_rec[q0 + q][0];
+                const uint16_t po = s_post[q];
+                const double pos = cfg.pos[c], neg = cfg.neg[c], lo = cfg.lo[c], hi = cfg.hi[c];
+                const bool stab = cfg.stab[c] != 0;
 #pragma unroll
-            for (int u = 0; u < kScanPerThread; ++u)
-                if (idx[u] < k)
-                {
-                    double old = double(wv[u]);
-                    double m = stab ? (old - lo) * (hi - old) : 1.0;
-                    double v = fma(pr[idx[u]] <= po ? pos : neg, m, old);
-                    v = (hi < v) ? hi : v;  // std::min(v, upper)
-                    v = (lo < v) ? v : lo;  // std::max(lower, .)
-                    wv[u] = __double2float_rn(v);
-                }
+                for (int u = 0; u < kScanPerThread; ++u)
+                    if (idx[u] < k)
+                    {
+                        double old = double(wv[u]);
+                        double m = stab ? (old - lo) * (hi - old) : 1.0;
+                        double v = fma(s_pre[q][idx[u] - base] <= po ? pos : neg, m, old);
+                        v = (hi < v) ? hi : v;  // std::min(v, upper)
+                        v = (lo < v) ? v : lo;  // std::max(lower, .)
+                        wv[u] = __double2float_rn(v);
+                    }
+            }
+            __syncthreads();
         }
-        __syncthreads();
+        __syncthreads();  // everyone has read s_n before it is reset
     }
 #pragma unroll
     for (int q = 0; q < kScanPerThread; ++q)
@@ -197,8 +262,13 @@ Configs make_configs(const double *c, int64_t n)
     return cfg;
 }
 
-inline size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 }  // namespace
+
+// Bytes of the (pre, post) first-spike scratch of conv STDP.
+size_t convstdp_prepost_bytes(int64_t b, int64_t count, int64_t cin, int64_t kh, int64_t kw)
+{
+    return align256(size_t(b * count * cin * kh * kw) * 2) + align256(size_t(b * count) * 2);
+}
 
 // Conv STDP with the (pre, post) scratch at a given device address; used by
 // the entry point that draws its scratch from a static device array.
@@ -239,9 +309,10 @@ using namespace spk;
 
 extern "C" {
 
-size_t spk_rank_convstdp_workspace(int64_t b, int64_t count, int64_t cin, int64_t kh, int64_t kw)
+size_t spk_rank_convstdp_workspace(int64_t b, int64_t count, int64_t cin, int64_t h, int64_t w, int64_t kh,
+                                   int64_t kw)
 {
-    return align256(size_t(b * count * cin * kh * kw) * 2) + align256(size_t(b * count) * 2);
+    return spk::convstdp_prepost_bytes(b, count, cin, kh, kw) + align256(size_t(b * cin * h * w) * 2);
 }
 
 spk_status spk_rank_convstdp(const void *in, spk_dtype itype, int64_t b, int64_t t, int64_t cin, int64_t h, int64_t w,
@@ -259,16 +330,21 @@ spk_status spk_rank_convstdp(const void *in, spk_dtype itype, int64_t b, int64_t
                     "tensor shapes are not compatible");
         if (b == 0) return;
         const int64_t k = cin * kh * kw;
-        const size_t need = spk_rank_convstdp_workspace(b, count, cin, kh, kw);
+        const size_t need = spk_rank_convstdp_workspace(b, count, cin, h, w, kh, kw);
         SPK_REQUIRE(ws != nullptr && ws_bytes >= need, "workspace is too small");
         uint16_t *pre = reinterpret_cast<uint16_t *>(ws);
         uint16_t *post = reinterpret_cast<uint16_t *>(static_cast<char *>(ws) + align256(size_t(b * count * k) * 2));
         cudaStream_t s = stream_of(stream);
+        uint16_t *fst = reinterpret_cast<uint16_t *>(static_cast<char *>(ws) +
+                                                     convstdp_prepost_bytes(b, count, cin, kh, kw));
         auto prep = [&](auto z) {
             using T = decltype(z);
-            conv_prepost_kernel<T><<<unsigned(b * count), 128, 0, s>>>(
-                (const T *)in, (const T *)out, int(t), int(cin), int(h), int(w), int(cout), int(oh), int(ow), int(kh),
-                int(kw), int(sy), int(sx), int(p.top), int(p.left), winners, counts, int(count), pre, post);
+            first_spike_map_kernel<T><<<grid_for(b * cin * h * w, 256, 16), 256, 0, s>>>((const T *)in, fst, b, int(t),
+                                                                                        cin * h * w);
+            SPK_LAUNCHED();
+            conv_prepost_map_kernel<T><<<unsigned(b * count), 128, 0, s>>>(
+                fst, (const T *)out, int(t), int(cin), int(h), int(w), int(cout), int(oh), int(ow), int(kh), int(kw),
+                int(sy), int(sx), int(p.top), int(p.left), winners, counts, int(count), pre, post);
         };
         if (itype == SPK_U8)
             prep(uint8_t());

@@ -23,6 +23,7 @@ void convstdp_into(const void *in, spk_dtype itype, int64_t b, int64_t t, int64_
                    float *kernel, int64_t cout, int64_t kh, int64_t kw, const void *out, int64_t oh, int64_t ow,
                    const double *configs, int64_t nconf, const int32_t *winners, const int32_t *counts, int64_t count,
                    int64_t sy, int64_t sx, const int64_t *pad4, void *scratch, cudaStream_t s);
+size_t convstdp_prepost_bytes(int64_t b, int64_t count, int64_t cin, int64_t kh, int64_t kw);
 
 namespace
 {
@@ -70,7 +71,7 @@ spk_status spk_rank_convstdp_noalloc(const void *in, spk_dtype itype, int64_t b,
 {
     return guarded([&] {
         SPK_REQUIRE(b >= 0 && count >= 1 && cin >= 1 && kh >= 1 && kw >= 1, "invalid dims");
-        const size_t need = spk_rank_convstdp_workspace(b, count, cin, kh, kw);
+        const size_t need = convstdp_prepost_bytes(b, count, cin, kh, kw);
         if (need > kNoAllocScratchBytes)
             throw Error(SPK_ERR_ARGUMENT, "spk_rank_convstdp_noalloc: this call needs " + std::to_string(need) +
                                               " bytes of scratch but the static scratch holds " +

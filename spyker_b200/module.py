@@ -516,7 +516,7 @@ class Conv:
         w = Winners.from_lists(winners, x.device)
         _check_winners(w, len(self.stdpconfig), s[0])
         cout, cin, kh, kw = self.kernel.shape
-        ws, wsb = _workspace(_lib.lib.spk_rank_convstdp_workspace(s[0], w.count, cin, kh, kw), x.device)
+        ws, wsb = _workspace(_lib.lib.spk_rank_convstdp_workspace(s[0], w.count, cin, s[3], s[4], kh, kw), x.device)
         call("spk_rank_convstdp", ptr(x), type_code(x.dtype), s[0], s[1], cin, s[3], s[4], ptr(self.kernel), cout, kh,
              kw, ptr(o), so[3], so[4], _configs(self.stdpconfig), len(self.stdpconfig), ptr(w.records), ptr(w.counts),
              w.count, self._stride[0], self._stride[1], i64(*self._pad), ptr(ws), wsb, stream())

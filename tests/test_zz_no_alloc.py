@@ -47,7 +47,7 @@ def _run(entry, codes, w, spk, win, cnt):
     common = (x.data_ptr(), 4, b, t, cin, h, wd, k.data_ptr(), cout, kh, kw, o.data_ptr(), spk.shape[3],
               spk.shape[4], cfg, 1, rec.data_ptr(), cn.data_ptr(), win.shape[1], 1, 1, pad)
     if entry == "workspace":
-        nb = _lib.lib.spk_rank_convstdp_workspace(b, win.shape[1], cin, kh, kw)
+        nb = _lib.lib.spk_rank_convstdp_workspace(b, win.shape[1], cin, h, wd, kh, kw)
         ws = torch.empty(nb, dtype=torch.uint8, device=dev)
         _lib.call("spk_rank_convstdp", *common, ws.data_ptr(), nb, s)
     else:
@@ -69,7 +69,7 @@ def test_noalloc_matches_workspace_entry_point_twice(port):
 def test_noalloc_rejects_oversized_calls(port):
     # 2 * B * count * Cin*KH*KW bytes beyond 32 MiB: refused before any launch.
     b, count, cin, kh, kw = 4096, 8, 30, 11, 11
-    assert _lib.lib.spk_rank_convstdp_workspace(b, count, cin, kh, kw) > (32 << 20)
+    assert _lib.lib.spk_rank_convstdp_workspace(b, count, cin, 14, 14, kh, kw) > (32 << 20)
     st = _lib.lib.spk_rank_convstdp_noalloc(None, 4, b, 15, cin, 14, 14, None, 100, kh, kw, None, 14, 14,
                                             _lib.f64(CFG), 1, None, None, count, 1, 1, _lib.i64(5, 5, 5, 5), None)
     assert st == 1
