@@ -193,6 +193,22 @@ def gpu_arm(args, rank, world):
     barrier()
     e2e_ms = e0.elapsed_time(e1) / args.steps
 
+    # the same step on the plain FP32 path (the comparison the metric names)
+    fp32 = None
+    if args.precision != "fp32" and not args.no_fp32_compare:
+        ref_net = Network(spyker, torch, dev, "fp32")
+        ref_net.step(dev_imgs)
+        barrier()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record()
+        for _ in range(2):
+            ref_net.step(dev_imgs)
+        f1.record()
+        barrier()
+        fp32_ms = f0.elapsed_time(f1) / 2
+        fp32 = {"value": BATCH / (fp32_ms * 1e-3), "unit": "images/s", "ms_per_step": fp32_ms, "steps": 2}
+        del ref_net
+
     t_max = torch.tensor([ms, e2e_ms], device=dev)
     if dist is not None:
         dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
@@ -228,9 +244,40 @@ def gpu_arm(args, rank, world):
         "kernels_ms": {"conv1": c1_ms, "conv2": c2_ms, "rest": ms - c1_ms - c2_ms},
         "clocks": clk.summary(),
     }
+    if fp32 is not None:
+        line["fp32_path"] = fp32
     if not args.no_cpu_baseline and world == 1:
+        # the CPU leg: the oracle as the timed baseline and as the checker
         line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
+        if not args.no_spike_match:
+            line["spike_match"] = spike_match(spyker, torch, dev, args.precision)
     print(json.dumps(line), flush=True)
+
+
+def spike_match(spyker, torch, dev, precision, n=32):
+    """Spike match %: both layers' fire spikes (fresh weights, no STDP) of
+    this path against the oracle's FP64 pipeline on `n` images."""
+    import oracle
+    from spyker_b200 import synth
+    from tests.golden.make_golden import dog_kernel
+
+    kind = "reference" if oracle.available("reference") else "port"
+    o = oracle.get(kind)
+    imgs = synth.strokes(n, seed=7)
+    w1, w2 = synth.conv_weights(30, 2, 5, seed=1), synth.conv_weights(100, 30, 5, seed=2)
+    net = Network(spyker, torch, dev, precision)
+    x = torch.from_numpy(imgs).to(dev).float().div_(255.0)[:, None]
+    codes = spyker.code(net.dog(x), T)
+    s1, _ = net._layer(net.conv1, codes, 15.0, 3, 5)
+    s2, _ = net._layer(net.conv2, spyker.pool(s1, 2), 10.0, 1, 8)
+    g1, g2 = s1.cpu().numpy(), s2.cpu().numpy()
+
+    ref_codes = o.rank_code(o.filter("dog", imgs.astype(np.float32)[:, None] / np.float32(255), dog_kernel(o),
+                                     (3, 3, 3, 3)), T)
+    r1 = o.fire(o.inhibit(o.threshold(o.conv(ref_codes, w1, (1, 1), (2, 2, 2, 2)), 15.0)))
+    r2 = o.fire(o.inhibit(o.threshold(o.conv(o.pool(r1, (2, 2)), w2, (1, 1), (2, 2, 2, 2)), 10.0)))
+    return {"layer1_pct": 100.0 * float(np.mean(g1 == r1)), "layer2_pct": 100.0 * float(np.mean(g2 == r2)),
+            "images": n, "oracle": f"{kind} (FP64 convolution)"}
 
 
 # ----------------------------------------------------------------------------
@@ -318,10 +365,12 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--precision", default=os.environ.get("SPYKER_BENCH_PRECISION", "fp32"),
+    ap.add_argument("--precision", default=os.environ.get("SPYKER_BENCH_PRECISION", "bf16x3"),
                     choices=["fp32", "bf16x2", "bf16x3"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp32-compare", action="store_true")
+    ap.add_argument("--no-spike-match", action="store_true")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", args.gpus if args.impl == "reference" else 1))

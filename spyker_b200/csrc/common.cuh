@@ -153,6 +153,39 @@ __device__ __forceinline__ uint16_t f2u16(float v)
 
 __host__ __device__ inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
+// Block-wide copy of the global byte range [src, src + n) into shared memory
+// (dst 16-byte aligned).  Byte i lands at dst[(src & 15) + i], so the range's
+// 16-byte-aligned interior moves with 16-byte loads and stores (four in
+// flight per thread) and only the ragged ends go byte by byte.  Returns the
+// offset (src & 15).  No barrier inside.
+__device__ __forceinline__ int stage_bytes(unsigned char *dst, const unsigned char *src, int64_t n)
+{
+    const uintptr_t a = reinterpret_cast<uintptr_t>(src);
+    const int shift = int(a & 15);
+    unsigned char *d = dst + shift;
+    const uintptr_t lo = (a + 15) & ~uintptr_t(15), hi = (a + uintptr_t(n)) & ~uintptr_t(15);
+    if (lo >= hi)
+    {
+        for (int64_t i = threadIdx.x; i < n; i += blockDim.x) d[i] = src[i];
+        return shift;
+    }
+    const int64_t head = int64_t(lo - a), tail = int64_t(hi - a);
+    for (int64_t i = threadIdx.x; i < head; i += blockDim.x) d[i] = src[i];
+    for (int64_t i = tail + threadIdx.x; i < n; i += blockDim.x) d[i] = src[i];
+    const uint4 *s4 = reinterpret_cast<const uint4 *>(lo);
+    uint4 *d4 = reinterpret_cast<uint4 *>(d + head);
+    const int64_t n4 = int64_t(hi - lo) >> 4, step = blockDim.x;
+    int64_t i = threadIdx.x;
+    for (; i + 3 * step < n4; i += 4 * step)
+    {
+        const uint4 v0 = __ldg(s4 + i), v1 = __ldg(s4 + i + step), v2 = __ldg(s4 + i + 2 * step),
+                    v3 = __ldg(s4 + i + 3 * step);
+        d4[i] = v0, d4[i + step] = v1, d4[i + 2 * step] = v2, d4[i + 3 * step] = v3;
+    }
+    for (; i < n4; i += step) d4[i] = __ldg(s4 + i);
+    return shift;
+}
+
 struct Pad4
 {
     int64_t top, left, bottom, right;

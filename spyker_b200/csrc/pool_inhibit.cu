@@ -45,6 +45,9 @@ __global__ void pool_kernel(const T *__restrict__ in, T *__restrict__ out, I n, 
     }
 }
 
+constexpr int64_t kPoolTileBytes = 16 * 1024;  // planes staged per CTA (at least one)
+constexpr int64_t kPoolPlaneMax = 96 * 1024;   // larger planes take the direct kernels
+
 // Large windows (e.g. global pooling): one warp per output element, the
 // lanes striding over the window and a shuffle max at the end (max is order
 // independent, so this equals the reference's sequential scan).
@@ -76,6 +79,77 @@ __global__ void pool_warp_kernel(const T *__restrict__ in, T *__restrict__ out, 
             m = (m < v) ? v : m;
         }
         if (lane == 0) out[k] = m;
+    }
+}
+
+// Whole planes staged in shared memory: a CTA takes `per_tile` consecutive
+// planes (one contiguous byte range, copied with 16-byte loads) and computes
+// their outputs from shared memory, so global traffic is one coalesced read
+// of the input and one of the output.  Thread per output for small windows
+// (taps in the reference's row-major order), warp per output for windows of
+// 64 taps and more.
+template <typename T, bool WARP>
+__global__ void __launch_bounds__(256) pool_plane_kernel(const T *__restrict__ in, T *__restrict__ out, int64_t n,
+                                                         int h, int w, int oh, int ow, int ky, int kx, int sy, int sx,
+                                                         int top, int left, int per_tile)
+{
+    extern __shared__ __align__(16) unsigned char pool_smem[];
+    const int hw = h * w, ohw = oh * ow;
+    const int64_t tiles = (n + per_tile - 1) / per_tile;
+    for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x)
+    {
+        const int64_t p0 = tile * per_tile;
+        const int np = int(min(int64_t(per_tile), n - p0));
+        __syncthreads();  // the previous tile's outputs are done
+        const int shift = stage_bytes(pool_smem, reinterpret_cast<const unsigned char *>(in + p0 * hw),
+                                      int64_t(np) * hw * int64_t(sizeof(T)));
+        __syncthreads();
+        const T *sp = reinterpret_cast<const T *>(pool_smem + shift);
+        T *op = out + p0 * ohw;
+        const int cnt = np * ohw;
+        if (!WARP)
+        {
+            for (int o = threadIdx.x; o < cnt; o += blockDim.x)
+            {
+                const int pl = o / ohw, r = o - pl * ohw, yo = r / ow, xo = r - yo * ow;
+                const T *plane = sp + pl * hw;
+                T m = Lowest<T>::v();
+                for (int a = 0; a < ky; ++a)
+                {
+                    const int yy = yo * sy + a - top;
+                    for (int b = 0; b < kx; ++b)
+                    {
+                        const int xx = xo * sx + b - left;
+                        const T v = (yy >= 0 && yy < h && xx >= 0 && xx < w) ? plane[yy * w + xx] : T(0);
+                        m = (m < v) ? v : m;
+                    }
+                }
+                op[o] = m;
+            }
+        }
+        else
+        {
+            const int lane = threadIdx.x & 31, warps = blockDim.x >> 5;
+            for (int o = threadIdx.x >> 5; o < cnt; o += warps)
+            {
+                const int pl = o / ohw, r = o - pl * ohw, yo = r / ow, xo = r - yo * ow;
+                const T *plane = sp + pl * hw;
+                T m = Lowest<T>::v();
+                for (int i = lane; i < ky * kx; i += 32)
+                {
+                    const int a = i / kx, b = i - a * kx;
+                    const int yy = yo * sy + a - top, xx = xo * sx + b - left;
+                    const T v = (yy >= 0 && yy < h && xx >= 0 && xx < w) ? plane[yy * w + xx] : T(0);
+                    m = (m < v) ? v : m;
+                }
+                for (int q = 16; q > 0; q >>= 1)
+                {
+                    const T v = T(__shfl_xor_sync(0xffffffffu, (typename Wide<T>::type)(m), q));
+                    m = (m < v) ? v : m;
+                }
+                if (lane == 0) op[o] = m;
+            }
+        }
     }
 }
 
@@ -141,7 +215,27 @@ spk_status spk_rank_pool(const void *in, void *out, spk_dtype type, int64_t n, i
         if (n == 0) return;
         dispatch(type, [&](auto z) {
             using T = decltype(z);
-            const bool small = n * oh * ow * 32 < (int64_t(1) << 31) && n * h * w < (int64_t(1) << 31);
+            const int64_t plane = h * w * int64_t(sizeof(T));
+            const int per_tile = int(std::max<int64_t>(1, std::min<int64_t>(kPoolTileBytes / plane, n)));
+            if (plane + 16 <= kPoolPlaneMax && per_tile * oh * ow < (int64_t(1) << 30))
+            {
+                const int smem = int(per_tile * plane + 16);
+                const bool warp = ky * kx >= 64;
+                auto k = warp ? pool_plane_kernel<T, true> : pool_plane_kernel<T, false>;
+                if (smem > 48 * 1024)
+                    SPK_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+                int occ = 0;
+                SPK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, 256, smem));
+                const int64_t tiles = ceil_div(n, per_tile);
+                const unsigned grid = unsigned(std::max<int64_t>(1, std::min<int64_t>(tiles, int64_t(sm_count()) * std::max(occ, 1))));
+                k<<<grid, 256, smem, stream_of(stream)>>>((const T *)in, (T *)out, n, int(h), int(w), int(oh), int(ow),
+                                                         int(ky), int(kx), int(sy), int(sx), int(p.top), int(p.left),
+                                                         per_tile);
+                SPK_LAUNCHED();
+                return;
+            }
+            // the grid is capped, so thread indexes always fit in 32 bits
+            const bool small = n * oh * ow < (int64_t(1) << 31) && n * h * w < (int64_t(1) << 31);
             auto go = [&](auto idx) {
                 using I = decltype(idx);
                 if (ky * kx >= 64)

@@ -34,11 +34,23 @@ struct Configs
     int n;
 };
 
+// First step with a non-zero value (t when none).  Loads go in groups of 8
+// independent reads, so a thread waits for memory twice per 16 steps instead
+// of once per step.
 template <typename T>
 __device__ __forceinline__ uint16_t first_spike(const T *p, int t, int64_t stride)
 {
-    for (int q = 0; q < t; ++q)
-        if (p[int64_t(q) * stride] != T(0)) return uint16_t(q);
+    for (int q0 = 0; q0 < t; q0 += 8)
+    {
+        T v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) v[u] = (q0 + u < t) ? p[int64_t(q0 + u) * stride] : T(0);
+        int f = -1;
+#pragma unroll
+        for (int u = 7; u >= 0; --u)
+            if (v[u] != T(0)) f = u;
+        if (f >= 0) return uint16_t(q0 + f);
+    }
     return uint16_t(t);
 }
 
@@ -86,6 +98,34 @@ __global__ void first_spike_map_kernel(const T *__restrict__ in, uint16_t *__res
     {
         const int64_t s = k / x, j = k - s * x;
         fst[k] = first_spike(in + s * t * x + j, t, x);
+    }
+}
+
+// U8 spikes with X a multiple of 4: four neighbouring positions per thread
+// from 32-bit loads.
+__global__ void first_spike_map_u8x4_kernel(const uint32_t *__restrict__ in, uint2 *__restrict__ fst, int64_t b, int t,
+                                            int64_t x4)
+{
+    const int64_t total = b * x4;
+    for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < total; k += int64_t(gridDim.x) * blockDim.x)
+    {
+        const int64_t s = k / x4, j = k - s * x4;
+        const uint32_t *p = in + s * t * x4 + j;
+        uint32_t f[4] = {uint32_t(t), uint32_t(t), uint32_t(t), uint32_t(t)};
+        uint32_t seen = 0;  // byte lanes that have spiked
+        for (int q0 = 0; q0 < t && seen != 0x0f; q0 += 8)
+        {
+            uint32_t v[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) v[u] = (q0 + u < t) ? p[int64_t(q0 + u) * x4] : 0u;
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+#pragma unroll
+                for (int l = 0; l < 4; ++l)
+                    if (!(seen & (1u << l)) && ((v[u] >> (8 * l)) & 0xffu))
+                        f[l] = uint32_t(q0 + u), seen |= 1u << l;
+        }
+        fst[k] = make_uint2(f[0] | (f[1] << 16), f[2] | (f[3] << 16));
     }
 }
 
@@ -339,8 +379,12 @@ spk_status spk_rank_convstdp(const void *in, spk_dtype itype, int64_t b, int64_t
                                                      convstdp_prepost_bytes(b, count, cin, kh, kw));
         auto prep = [&](auto z) {
             using T = decltype(z);
-            first_spike_map_kernel<T><<<grid_for(b * cin * h * w, 256, 16), 256, 0, s>>>((const T *)in, fst, b, int(t),
-                                                                                        cin * h * w);
+            const int64_t x = cin * h * w;
+            if (sizeof(T) == 1 && x % 4 == 0 && reinterpret_cast<uintptr_t>(in) % 4 == 0)
+                first_spike_map_u8x4_kernel<<<grid_for(b * x / 4, 256, 16), 256, 0, s>>>(
+                    (const uint32_t *)in, reinterpret_cast<uint2 *>(fst), b, int(t), x / 4);
+            else
+                first_spike_map_kernel<T><<<grid_for(b * x, 256, 16), 256, 0, s>>>((const T *)in, fst, b, int(t), x);
             SPK_LAUNCHED();
             conv_prepost_map_kernel<T><<<unsigned(b * count), 128, 0, s>>>(
                 fst, (const T *)out, int(t), int(cin), int(h), int(w), int(cout), int(oh), int(ow), int(kh), int(kw),

@@ -153,6 +153,24 @@ def test_pool(port, layer, args):
         assert np.array_equal(got, port.pool(a, spyker.expand2(k), spyker.expand2(s or k), p4))
 
 
+def test_pool_staging_edges(port):
+    """Planes staged from an unaligned view, tiles that end mid-range, and
+    planes too large to stage (direct kernels)."""
+    rng = np.random.default_rng(11)
+    base = cuda(rng.random((7 * 3 * 5 * 13 * 11 + 3,), dtype=np.float32))
+    view = base[3:].view(7, 3, 5, 13, 11)  # 12-byte offset from the allocation
+    want = port.pool(host(view), (3, 2), (2, 3), (1, 0, 2, 1))
+    assert np.array_equal(host(spyker.pool(view, (3, 2), (2, 3), (1, 0, 2, 1))), want)
+    u8 = (rng.random((3, 4, 7, 9, 9)) < 0.3).astype(np.uint8)
+    for k, s, p in (((2, 2), None, 0), ((9, 9), None, 0), ((4, 3), (1, 2), (3, 2, 1, 0))):
+        got = host(spyker.pool(cuda(u8), k, s, p))
+        assert np.array_equal(got, port.pool(u8, spyker.expand2(k), spyker.expand2(s or k), spyker.expand4(p)))
+    big = rng.random((1, 2, 1, 180, 170), dtype=np.float32)  # 122 KB planes
+    for k in (2, 10):
+        got = host(spyker.pool(cuda(big), k))
+        assert np.array_equal(got, port.pool(big, (k, k), (k, k), (0, 0, 0, 0)))
+
+
 def test_inhibit(port, layer):
     for a, thr in ((layer["th"], 0.0), (layer["pot"], 25.0)):
         t = cuda(a)
