@@ -149,6 +149,7 @@ def gpu_arm(args, rank, world):
         import torch.distributed as dist
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    BATCH = args.batch
     imgs = synth.strokes(BATCH, seed=100 + rank)
     host = torch.from_numpy(imgs).pin_memory()
     dev_imgs = host.to(dev).float().div_(255.0)[:, None]
@@ -233,8 +234,8 @@ def gpu_arm(args, rank, world):
         "vs_baseline": None,
         "dtype": {"fp32": "f32", "bf16x2": "bf16x2-split/f32-acc", "bf16x3": "bf16x3-split/f32-acc"}[args.precision],
         "data": "synthetic (seeded stroke images, MNIST geometry)",
-        "config": {"workload": WORKLOAD, "global_batch": BATCH * world, "seq_len": T, "parallelism": f"replicas{world}",
-                   "conv_precision": args.precision, "l2": "inputs larger than L2 (potentials 5.8 GB per layer)"},
+        "config": {"workload": WORKLOAD.replace("4096 x", f"{BATCH} x"), "global_batch": BATCH * world, "seq_len": T, "parallelism": f"replicas{world}",
+                   "conv_precision": args.precision, "l2": "inputs larger than L2: each step streams its own 289 MB layer-1 spike tensor (126 MB L2)"},
         "e2e": {"value": BATCH * world / (e2e_ms * 1e-3), "unit": "images/s", "h2d_bytes_per_step": BATCH * H * H,
                 "d2h_bytes_per_step": int(feats.numel() * feats.element_size())},
         "gpu_launches": int(launches),
@@ -368,6 +369,7 @@ def main():
     ap.add_argument("--precision", default=os.environ.get("SPYKER_BENCH_PRECISION", "bf16x3"),
                     choices=["fp32", "bf16x2", "bf16x3"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--batch", type=int, default=BATCH, help="images per GPU per step (small cases for profiling)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32-compare", action="store_true")
     ap.add_argument("--no-spike-match", action="store_true")

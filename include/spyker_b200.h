@@ -235,6 +235,77 @@ size_t spk_fcbackward_workspace(int64_t no, int64_t ni);
 spk_status spk_fcbackward(float *kernel, int64_t no, int64_t ni, const float *in, const float *out, const float *grad,
                           float *next, int64_t b, float *bp_host, void *ws, size_t ws_bytes, spk_stream stream);
 
+/* ---- event lists (the `sparse_*` table of impl.h:328-356; src/spyker/sparse) ----
+ * A sparse spike tensor [U, T, C, H, W] (SparseTensor, utils.h:369-420; Sparse5,
+ * base.h:493-528) is one CSR array on the device:
+ *   offsets int64 [U*T + 1]: list i = u*T + t holds events offsets[i] .. offsets[i+1]-1;
+ *   events  uint32: x | y << 8 | z << 16 (8-bit coordinates as Spridx).
+ * Event order inside a list is the reference's.  Producers write into
+ * caller buffers of at least the stated capacity (the worst case), so no call
+ * waits for the host; offsets[U*T] is the number of events written.
+ * C, H, W (and conv outputs) are limited to 256, T to 16384. */
+
+/* Sparse::code, sparse/code.cpp:39-130: one event at the rank-order (sort) or
+ * latency first-spike time of every position (none when it is >= T), lists in
+ * (z, y, x) order.  cap >= U*C*H*W. */
+size_t spk_sparse_code_workspace(int64_t u, int64_t t, int64_t c, int64_t h, int64_t w);
+spk_status spk_sparse_code(const void *in, spk_dtype itype, int64_t u, int64_t c, int64_t h, int64_t w, int64_t t,
+                           int sort, int64_t *offsets, uint32_t *events, int64_t cap, void *ws, size_t ws_bytes,
+                           spk_stream stream);
+/* SparseTensor(Tensor, threshold), sparse/opers.cpp:59-86: an event at the
+ * first step whose value exceeds the threshold.  cap >= U*C*H*W. */
+size_t spk_sparse_from_dense_workspace(int64_t u, int64_t t, int64_t c, int64_t h, int64_t w);
+spk_status spk_sparse_from_dense(const void *in, spk_dtype itype, int64_t u, int64_t t, int64_t c, int64_t h,
+                                 int64_t w, double threshold, int64_t *offsets, uint32_t *events, int64_t cap,
+                                 void *ws, size_t ws_bytes, spk_stream stream);
+/* SparseTensor::dense, sparse/opers.cpp:88-104: cumulative spikes [U, T, C, H, W];
+ * Sparse::gather, sparse/opers.cpp:106-118: first event time [U, C, H, W] (T when none). */
+size_t spk_sparse_dense_workspace(int64_t u, int64_t c, int64_t h, int64_t w);
+spk_status spk_sparse_to_dense(const int64_t *offsets, const uint32_t *events, int64_t u, int64_t t, int64_t c,
+                               int64_t h, int64_t w, void *out, spk_dtype otype, void *ws, size_t ws_bytes,
+                               spk_stream stream);
+spk_status spk_sparse_gather(const int64_t *offsets, const uint32_t *events, int64_t u, int64_t t, int64_t c,
+                             int64_t h, int64_t w, void *out, spk_dtype otype, void *ws, size_t ws_bytes,
+                             spk_stream stream);
+/* Sparse::pad, sparse/pad.cpp:37-55: coordinates shifted by (top, left), 8-bit
+ * wrap.  cap >= in_cap (the input's event capacity). */
+spk_status spk_sparse_pad(const int64_t *offsets, const uint32_t *events, int64_t in_cap, int64_t u, int64_t t,
+                          int64_t c, int64_t h, int64_t w, const int64_t *pad4_host, int64_t *out_offsets,
+                          uint32_t *out_events, int64_t cap, spk_stream stream);
+/* Sparse::pool, sparse/pool.cpp:37-64: the first event of every pooled cell;
+ * stride must equal the kernel.  cap >= min(in_cap, U*C*OH*OW). */
+size_t spk_sparse_pool_workspace(int64_t u, int64_t c, int64_t oh, int64_t ow, int64_t in_cap);
+spk_status spk_sparse_pool(const int64_t *offsets, const uint32_t *events, int64_t in_cap, int64_t u, int64_t t,
+                           int64_t c, int64_t h, int64_t w, const int64_t *kernel2_host, const int64_t *stride2_host,
+                           const int64_t *pad4_host, int64_t oh, int64_t ow, int64_t *out_offsets,
+                           uint32_t *out_events, int64_t cap, void *ws, size_t ws_bytes, spk_stream stream);
+/* Sparse::inhibit, sparse/inhibit.cpp:37-65: per pixel only the channel of its
+ * first event survives.  cap >= in_cap. */
+size_t spk_sparse_inhibit_workspace(int64_t u, int64_t h, int64_t w, int64_t in_cap);
+spk_status spk_sparse_inhibit(const int64_t *offsets, const uint32_t *events, int64_t in_cap, int64_t u, int64_t t,
+                              int64_t c, int64_t h, int64_t w, int64_t *out_offsets, uint32_t *out_events, int64_t cap,
+                              void *ws, size_t ws_bytes, spk_stream stream);
+/* Sparse::conv, sparse/conv.cpp:42-160: incremental F32 potentials and fire
+ * once above threshold; stride must be 1; kernel F32 [Cout, C, KH, KW].
+ * cap >= U*Cout*OH*OW. */
+size_t spk_sparse_conv_workspace(int64_t u, int64_t t, int64_t h, int64_t w, int64_t cout, int64_t kh, int64_t kw,
+                                 const int64_t *pad4_host);
+spk_status spk_sparse_conv(const int64_t *offsets, const uint32_t *events, int64_t u, int64_t t, int64_t c, int64_t h,
+                           int64_t w, const float *kernel, int64_t cout, int64_t kh, int64_t kw, double threshold,
+                           const int64_t *stride2_host, const int64_t *pad4_host, int64_t *out_offsets,
+                           uint32_t *out_events, int64_t cap, void *ws, size_t ws_bytes, spk_stream stream);
+/* Sparse::convwta, sparse/wta.cpp:44-95 -> winners [U, count, 5] = (0, t, z, y, x), counts [U]. */
+spk_status spk_sparse_convwta(const int64_t *offsets, const uint32_t *events, int64_t u, int64_t t, int64_t c,
+                              int64_t h, int64_t w, const int64_t *radius2_host, int64_t count, int32_t *winners,
+                              int32_t *counts, spk_stream stream);
+/* Conv::stdp(SparseTensor), sparse/stdp.cpp:41-133 (F32 update arithmetic). */
+size_t spk_sparse_stdp_workspace(int64_t u, int64_t count, int64_t c, int64_t h, int64_t w, int64_t kh, int64_t kw,
+                                 const int64_t *pad4_host);
+spk_status spk_sparse_stdp(const int64_t *offsets, const uint32_t *events, int64_t u, int64_t t, int64_t c, int64_t h,
+                           int64_t w, float *kernel, int64_t cout, int64_t kh, int64_t kw, const double *configs_host,
+                           int64_t nconf, const int32_t *winners, const int32_t *counts, int64_t count,
+                           const int64_t *pad4_host, void *ws, size_t ws_bytes, spk_stream stream);
+
 #ifdef __cplusplus
 }
 #endif

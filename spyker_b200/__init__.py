@@ -13,7 +13,7 @@ from .module import (FC, ZCA, BPConfig, Conv, conv_fire_wta, DoG, DoGFilter, Gab
                      backward, canny, code, conv, conv_precision, convwta, fc, fcwta, fire, gather, infinite,
                      inhibit, labelize, pad, pool, quantize, random_seed, scatter, set_conv_precision, stdp,
                      threshold)
-from .sparse import SparseTensor
+from .sparse import SparseTensor, to_sparse
 from .utils import copy_array, device, expand2, expand4, shape, to_numpy, to_tensor, to_torch
 
 __version__ = "0.1.0"

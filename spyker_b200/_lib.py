@@ -61,6 +61,23 @@ SIGNATURES = {
     "spk_labelize": (_INT, [_P, _INT, _P, _I, _I, _I, _D, _P]),
     "spk_fcbackward_workspace": (_S, [_I, _I]),
     "spk_fcbackward": (_INT, [_P, _I, _I, _P, _P, _P, _P, _I, _P, _P, _S, _P]),
+    "spk_sparse_code_workspace": (_S, [_I, _I, _I, _I, _I]),
+    "spk_sparse_code": (_INT, [_P, _INT, _I, _I, _I, _I, _I, _INT, _P, _P, _I, _P, _S, _P]),
+    "spk_sparse_from_dense_workspace": (_S, [_I, _I, _I, _I, _I]),
+    "spk_sparse_from_dense": (_INT, [_P, _INT, _I, _I, _I, _I, _I, _D, _P, _P, _I, _P, _S, _P]),
+    "spk_sparse_dense_workspace": (_S, [_I, _I, _I, _I]),
+    "spk_sparse_to_dense": (_INT, [_P, _P, _I, _I, _I, _I, _I, _P, _INT, _P, _S, _P]),
+    "spk_sparse_gather": (_INT, [_P, _P, _I, _I, _I, _I, _I, _P, _INT, _P, _S, _P]),
+    "spk_sparse_pad": (_INT, [_P, _P, _I, _I, _I, _I, _I, _I, _P, _P, _P, _I, _P]),
+    "spk_sparse_pool_workspace": (_S, [_I, _I, _I, _I, _I]),
+    "spk_sparse_pool": (_INT, [_P, _P, _I, _I, _I, _I, _I, _I, _P, _P, _P, _I, _I, _P, _P, _I, _P, _S, _P]),
+    "spk_sparse_inhibit_workspace": (_S, [_I, _I, _I, _I]),
+    "spk_sparse_inhibit": (_INT, [_P, _P, _I, _I, _I, _I, _I, _I, _P, _P, _I, _P, _S, _P]),
+    "spk_sparse_conv_workspace": (_S, [_I, _I, _I, _I, _I, _I, _I, _P]),
+    "spk_sparse_conv": (_INT, [_P, _P, _I, _I, _I, _I, _I, _P, _I, _I, _I, _D, _P, _P, _P, _P, _I, _P, _S, _P]),
+    "spk_sparse_convwta": (_INT, [_P, _P, _I, _I, _I, _I, _I, _P, _I, _P, _P, _P]),
+    "spk_sparse_stdp_workspace": (_S, [_I, _I, _I, _I, _I, _I, _I, _P]),
+    "spk_sparse_stdp": (_INT, [_P, _P, _I, _I, _I, _I, _I, _P, _I, _I, _I, _P, _I, _P, _P, _I, _P, _P, _S, _P]),
 }
 
 

@@ -72,7 +72,9 @@ __device__ __forceinline__ void write_rows(O *__restrict__ out, const uint16_t *
     }
 }
 
-template <typename I, typename O>
+// TIMES: write the u16 times [B, X] instead of the spike rows (event lists
+// are built from them).
+template <typename I, typename O, bool TIMES = false>
 __global__ void __launch_bounds__(kCodeThreads) rank_sorted_kernel(const I *__restrict__ in, O *__restrict__ out,
                                                                     int64_t x, int t, int npow2)
 {
@@ -121,7 +123,12 @@ __global__ void __launch_bounds__(kCodeThreads) rank_sorted_kernel(const I *__re
         tm[j] = f2u16(float(i) * scale);
     }
     __syncthreads();
-    write_rows<O>(out + int64_t(blockIdx.x) * t * x, tm, x, t);
+    if constexpr (TIMES)
+    {
+        for (int64_t j = threadIdx.x; j < x; j += blockDim.x) out[int64_t(blockIdx.x) * x + j] = O(tm[j]);
+    }
+    else
+        write_rows<O>(out + int64_t(blockIdx.x) * t * x, tm, x, t);
 }
 
 // Reduction type of the latency code: the value itself for floats, int for
@@ -137,7 +144,7 @@ struct Acc<uint8_t>
     using T = int;
 };
 
-template <typename I, typename O>
+template <typename I, typename O, bool TIMES = false>
 __global__ void __launch_bounds__(kCodeThreads) latency_kernel(const I *__restrict__ in, O *__restrict__ out, int64_t x,
                                                                 int t)
 {
@@ -172,10 +179,43 @@ __global__ void __launch_bounds__(kCodeThreads) latency_kernel(const I *__restri
     {
         // end - scale * d, fused as the reference's -O3 FMA build computes it.
         uint16_t m = f2u16(__fmaf_rn(-scale, float(A(row[j]) - mn), end));
-        for (int s = 0; s < t; ++s) orow[int64_t(s) * x + j] = O(m <= uint16_t(s));
+        if constexpr (TIMES)
+            out[int64_t(blockIdx.x) * x + j] = O(m);
+        else
+            for (int s = 0; s < t; ++s) orow[int64_t(s) * x + j] = O(m <= uint16_t(s));
     }
 }
 }  // namespace
+
+// First-spike times [B, X] u16 of the rank-order (sort) or latency code.
+void rank_times(const void *in, spk_dtype itype, uint16_t *times, int64_t b, int64_t t, int64_t x, int sort,
+                cudaStream_t s)
+{
+    SPK_REQUIRE(itype == SPK_F32 || itype == SPK_U8, "coding supports F32/U8 input");
+    if (b == 0) return;
+    if (sort)
+    {
+        if (x > kMaxSortX)
+            throw Error(SPK_ERR_UNSUPPORTED, "sorted rank coding supports at most 16384 values per image");
+        int npow2 = 2;
+        while (npow2 < x) npow2 <<= 1;
+        const size_t smem = size_t(npow2) * 8 + size_t(x) * 2 + 16;
+        auto go = [&](auto k, const auto *p) {
+            SPK_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+            k<<<unsigned(b), kCodeThreads, smem, s>>>(p, times, x, int(t), npow2);
+        };
+        if (itype == SPK_F32)
+            go(rank_sorted_kernel<float, uint16_t, true>, (const float *)in);
+        else
+            go(rank_sorted_kernel<uint8_t, uint16_t, true>, (const uint8_t *)in);
+    }
+    else if (itype == SPK_F32)
+        latency_kernel<float, uint16_t, true><<<unsigned(b), kCodeThreads, 0, s>>>((const float *)in, times, x, int(t));
+    else
+        latency_kernel<uint8_t, uint16_t, true><<<unsigned(b), kCodeThreads, 0, s>>>((const uint8_t *)in, times, x,
+                                                                                    int(t));
+    SPK_LAUNCHED();
+}
 }  // namespace spk
 
 using namespace spk;

@@ -184,6 +184,9 @@ __global__ void fc_prepost_kernel(const T *__restrict__ in, const T *__restrict_
 // Kernel B: CTA (map, chunk) walks winners in (sample, slot) order.  The map
 // index of a winner is field `field` of its record (z for conv, x for fc).
 // pre address: pre + s * ps + j * pw + element.
+// F32_RULE: the event-list STDP of src/spyker/sparse/stdp.cpp:95-97, which
+// rounds the soft-bound factor and the updated weight to F32 before the clamp.
+template <bool F32_RULE>
 __global__ void __launch_bounds__(kScanThreads)
     stdp_scan_kernel(float *__restrict__ kernel, int64_t k, int64_t b, int count, int field,
                      const int32_t *__restrict__ winners, const int32_t *__restrict__ counts,
@@ -270,12 +273,24 @@ __global__ void __launch_bounds__(kScanThreads)
                 for (int u = 0; u < kScanPerThread; ++u)
                     if (idx[u] < k)
                     {
-                        double old = double(wv[u]);
-                        double m = stab ? (old - lo) * (hi - old) : 1.0;
-                        double v = fma(s_pre[q][idx[u] - base] <= po ? pos : neg, m, old);
-                        v = (hi < v) ? hi : v;  // std::min(v, upper)
-                        v = (lo < v) ? v : lo;  // std::max(lower, .)
-                        wv[u] = __double2float_rn(v);
+                        const double old = double(wv[u]);
+                        const double d = s_pre[q][idx[u] - base] <= po ? pos : neg;
+                        if (F32_RULE)
+                        {
+                            const float m = __double2float_rn(stab ? (old - lo) * (hi - old) : 1.0);
+                            double v = double(__double2float_rn(fma(d, double(m), old)));
+                            v = (hi < v) ? hi : v;
+                            v = (lo < v) ? v : lo;
+                            wv[u] = __double2float_rn(v);
+                        }
+                        else
+                        {
+                            const double m = stab ? (old - lo) * (hi - old) : 1.0;
+                            double v = fma(d, m, old);
+                            v = (hi < v) ? hi : v;  // std::min(v, upper)
+                            v = (lo < v) ? v : lo;  // std::max(lower, .)
+                            wv[u] = __double2float_rn(v);
+                        }
                     }
             }
             __syncthreads();
@@ -303,6 +318,23 @@ Configs make_configs(const double *c, int64_t n)
 }
 
 }  // namespace
+
+// Ordered per-map STDP scan over precomputed (pre, post) times; the entry
+// point of the event-list STDP.
+void launch_stdp_scan(float *kernel, int64_t k, int64_t nmaps, int64_t b, int64_t count, int field,
+                      const int32_t *winners, const int32_t *counts, const uint16_t *pre, int64_t ps, int64_t pw,
+                      const uint16_t *post, const double *configs, int64_t nconf, bool f32_rule, cudaStream_t s)
+{
+    Configs cfg = make_configs(configs, nconf);
+    dim3 grid(unsigned(nmaps), unsigned(ceil_div(k, kScanChunk)));
+    if (f32_rule)
+        stdp_scan_kernel<true><<<grid, kScanThreads, 0, s>>>(kernel, k, b, int(count), field, winners, counts, pre, ps,
+                                                            pw, post, cfg);
+    else
+        stdp_scan_kernel<false><<<grid, kScanThreads, 0, s>>>(kernel, k, b, int(count), field, winners, counts, pre,
+                                                             ps, pw, post, cfg);
+    SPK_LAUNCHED();
+}
 
 // Bytes of the (pre, post) first-spike scratch of conv STDP.
 size_t convstdp_prepost_bytes(int64_t b, int64_t count, int64_t cin, int64_t kh, int64_t kw)
@@ -339,7 +371,7 @@ void convstdp_into(const void *in, spk_dtype itype, int64_t b, int64_t t, int64_
         throw Error(SPK_ERR_UNSUPPORTED, "STDP spikes must be U8 or F32");
     SPK_LAUNCHED();
     dim3 grid(unsigned(cout), unsigned(ceil_div(k, kScanChunk)));
-    stdp_scan_kernel<<<grid, kScanThreads, 0, s>>>(kernel, k, b, int(count), 2, winners, counts, pre, count * k, k,
+    stdp_scan_kernel<false><<<grid, kScanThreads, 0, s>>>(kernel, k, b, int(count), 2, winners, counts, pre, count * k, k,
                                                    post, cfg);
     SPK_LAUNCHED();
 }
@@ -398,7 +430,7 @@ spk_status spk_rank_convstdp(const void *in, spk_dtype itype, int64_t b, int64_t
             throw Error(SPK_ERR_UNSUPPORTED, "STDP spikes must be U8 or F32");
         SPK_LAUNCHED();
         dim3 grid(unsigned(cout), unsigned(ceil_div(k, kScanChunk)));
-        stdp_scan_kernel<<<grid, kScanThreads, 0, s>>>(kernel, k, b, int(count), 2, winners, counts, pre, count * k, k,
+        stdp_scan_kernel<false><<<grid, kScanThreads, 0, s>>>(kernel, k, b, int(count), 2, winners, counts, pre, count * k, k,
                                                        post, cfg);
         SPK_LAUNCHED();
     });
@@ -435,7 +467,7 @@ spk_status spk_rank_fcstdp(const void *in, spk_dtype itype, int64_t b, int64_t t
             throw Error(SPK_ERR_UNSUPPORTED, "STDP spikes must be U8 or F32");
         SPK_LAUNCHED();
         dim3 grid(unsigned(no), unsigned(ceil_div(ni, kScanChunk)));
-        stdp_scan_kernel<<<grid, kScanThreads, 0, s>>>(kernel, ni, b, int(count), 4, winners, counts, pre, ni, 0, post,
+        stdp_scan_kernel<false><<<grid, kScanThreads, 0, s>>>(kernel, ni, b, int(count), 4, winners, counts, pre, ni, 0, post,
                                                        cfg);
         SPK_LAUNCHED();
     });
