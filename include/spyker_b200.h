@@ -97,7 +97,9 @@ spk_status spk_log_kernel(double *kernel_host, int64_t size, double std);
 
 /* ---- coding (replaces Core::rank_code, impl.h:248; cpu/code.cpp:122) ---- */
 /* in [B, X], out [B, T, X] cumulative spikes.  sort!=0: rank order, ties in
- * index order (stable); sort==0: latency code. */
+ * index order (stable); sort==0: latency code.  Images of more than 16384
+ * values take a device-wide sort that needs the workspace (16*B*X bytes plus
+ * 2*B*X, rounded up); smaller images need none. */
 size_t spk_rank_code_workspace(int64_t b, int64_t x, int sort);
 spk_status spk_rank_code(const void *in, spk_dtype itype, void *out, spk_dtype otype, int64_t b, int64_t t, int64_t x,
                          int sort, void *ws, size_t ws_bytes, spk_stream stream);

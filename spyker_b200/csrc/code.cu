@@ -185,18 +185,196 @@ __global__ void __launch_bounds__(kCodeThreads) latency_kernel(const I *__restri
             for (int s = 0; s < t; ++s) orow[int64_t(s) * x + j] = O(m <= uint16_t(s));
     }
 }
+// ---- images larger than one CTA's shared memory (X > 16384) ---------------
+// The same (value desc, index asc) order from a device-wide sort per image:
+// CTAs sort 8192-key chunks in shared memory, then merge-path rounds double
+// the sorted runs until each image is one run; times and rows follow.
+constexpr int kChunk = 8192, kMergeItems = 8;
+
+inline int64_t padded_x(int64_t x) { return ceil_div(x, kChunk) * kChunk; }
+
+template <typename I>
+__global__ void __launch_bounds__(kCodeThreads) chunk_sort_kernel(const I *__restrict__ in, uint64_t *__restrict__ keys,
+                                                                   int64_t x, int64_t xp)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    uint64_t *sk = reinterpret_cast<uint64_t *>(smem);
+    const int64_t img = blockIdx.y, base = int64_t(blockIdx.x) * kChunk;
+    const I *row = in + img * x;
+    for (int i = threadIdx.x; i < kChunk; i += blockDim.x)
+    {
+        const int64_t j = base + i;
+        sk[i] = (j < x) ? ((uint64_t(~order_key(row[j])) << 32) | uint32_t(j)) : ~uint64_t(0);
+    }
+    __syncthreads();
+    for (int size = 2; size <= kChunk; size <<= 1)
+        for (int stride = size >> 1; stride > 0; stride >>= 1)
+        {
+            for (int i = threadIdx.x; i < kChunk / 2; i += blockDim.x)
+            {
+                const int lo = 2 * i - (i & (stride - 1)), hi = lo + stride;
+                const bool up = (lo & size) == 0;
+                const uint64_t a = sk[lo], b = sk[hi];
+                if ((a > b) == up) sk[lo] = b, sk[hi] = a;
+            }
+            __syncthreads();
+        }
+    uint64_t *out = keys + img * xp + base;
+    for (int i = threadIdx.x; i < kChunk; i += blockDim.x) out[i] = sk[i];
+}
+
+// One merge round: runs of length L pairwise into runs of 2L; each thread
+// finds its diagonal on the merge path and writes kMergeItems outputs.
+__global__ void merge_round_kernel(const uint64_t *__restrict__ src, uint64_t *__restrict__ dst, int64_t b, int64_t xp,
+                                   int64_t L)
+{
+    const int64_t total = b * xp / kMergeItems;
+    for (int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < total; g += int64_t(gridDim.x) * blockDim.x)
+    {
+        const int64_t o = g * kMergeItems, img = o / xp, p = o - img * xp;
+        const int64_t start = (p / (2 * L)) * (2 * L);
+        const int64_t la = min(L, xp - start), lb = min(L, xp - start - la);
+        const uint64_t *A = src + img * xp + start, *B = A + la;
+        const int64_t d = p - start;
+        int64_t lo = d > lb ? d - lb : 0, hi = d < la ? d : la;
+        while (lo < hi)
+        {
+            const int64_t mid = (lo + hi) >> 1;
+            if (A[mid] <= B[d - mid - 1])
+                lo = mid + 1;
+            else
+                hi = mid;
+        }
+        int64_t i = lo, j = d - lo;
+        uint64_t *out = dst + img * xp + p;
+#pragma unroll
+        for (int k = 0; k < kMergeItems; ++k)
+        {
+            const bool take_a = j >= lb || (i < la && A[i] <= B[j]);
+            out[k] = take_a ? A[i++] : B[j++];
+        }
+    }
+}
+
+// Per image: cnt = values strictly above the minimum (the position of the
+// first key carrying the minimum's value), then time of every sorted position.
+__global__ void sorted_times_kernel(const uint64_t *__restrict__ keys, uint16_t *__restrict__ tm, int64_t b, int64_t x,
+                                    int64_t xp, int t)
+{
+    const int64_t img = blockIdx.y;
+    const uint64_t *S = keys + img * xp;
+    const uint32_t vmin = uint32_t(S[x - 1] >> 32);
+    int64_t lo = 0, hi = x - 1;
+    while (lo < hi)
+    {
+        const int64_t mid = (lo + hi) >> 1;
+        if (uint32_t(S[mid] >> 32) < vmin)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    const float scale = (float(t) + 1e-5f) / float(lo);
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < x; i += int64_t(gridDim.x) * blockDim.x)
+        tm[img * x + uint32_t(S[i])] = f2u16(float(i) * scale);
+}
+
+// out[img, s, j] = (tm[img, j] <= s), 16 positions per thread.
+template <typename O>
+__global__ void rows_from_times_kernel(const uint16_t *__restrict__ tm, O *__restrict__ out, int64_t b, int t,
+                                       int64_t x)
+{
+    const int64_t groups = ceil_div(x, 16), total = b * groups;
+    const bool vec = sizeof(O) == 1 && x % 16 == 0 && (reinterpret_cast<uintptr_t>(out) & 15) == 0;
+    for (int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < total; g += int64_t(gridDim.x) * blockDim.x)
+    {
+        const int64_t img = g / groups, j0 = (g - img * groups) * 16;
+        uint16_t m[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) m[q] = (j0 + q < x) ? tm[img * x + j0 + q] : uint16_t(0xffff);
+        O *orow = out + img * t * x + j0;
+        for (int s = 0; s < t; ++s)
+        {
+            if (vec)
+            {
+                uint32_t w[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                {
+                    uint32_t a = 0;
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) a |= uint32_t(m[q * 4 + e] <= uint16_t(s)) << (8 * e);
+                    w[q] = a;
+                }
+                *reinterpret_cast<uint4 *>(orow + int64_t(s) * x) = make_uint4(w[0], w[1], w[2], w[3]);
+            }
+            else
+            {
+#pragma unroll
+                for (int q = 0; q < 16; ++q)
+                    if (j0 + q < x) orow[int64_t(s) * x + q] = O(m[q] <= uint16_t(s));
+            }
+        }
+    }
+}
+
+size_t large_sort_ws(int64_t b, int64_t x)
+{
+    const int64_t xp = padded_x(x);
+    return 2 * ((size_t(b * xp) * 8 + 255) / 256) * 256 + ((size_t(b * x) * 2 + 255) / 256) * 256;
+}
+
+// Sorted times of images with X > 16384 into `tm` (inside or outside ws).
+template <typename I>
+void large_sorted_times(const I *in, uint16_t *tm, int64_t b, int64_t t, int64_t x, void *ws, cudaStream_t s)
+{
+    const int64_t xp = padded_x(x);
+    SPK_REQUIRE(x < (int64_t(1) << 32), "at most 2^32 - 1 values per image");
+    SPK_REQUIRE(b <= 65535, "at most 65535 images per call on the large-image path");
+    uint64_t *k0 = static_cast<uint64_t *>(ws);
+    uint64_t *k1 = reinterpret_cast<uint64_t *>(static_cast<char *>(ws) + ((size_t(b * xp) * 8 + 255) / 256) * 256);
+    const size_t smem = size_t(kChunk) * 8;
+    SPK_CUDA(cudaFuncSetAttribute(chunk_sort_kernel<I>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    chunk_sort_kernel<I><<<dim3(unsigned(xp / kChunk), unsigned(b)), kCodeThreads, smem, s>>>(in, k0, x, xp);
+    SPK_LAUNCHED();
+    for (int64_t L = kChunk; L < xp; L *= 2)
+    {
+        merge_round_kernel<<<grid_for(b * xp / kMergeItems, 256), 256, 0, s>>>(k0, k1, b, xp, L);
+        SPK_LAUNCHED();
+        std::swap(k0, k1);
+    }
+    sorted_times_kernel<<<dim3(unsigned(std::min<int64_t>(ceil_div(x, 256), 1024)), unsigned(b)), 256, 0, s>>>(
+        k0, tm, b, x, xp, int(t));
+    SPK_LAUNCHED();
+}
+
+// Workspace tail of the large path that holds the times.
+uint16_t *large_times_slot(void *ws, int64_t b, int64_t x)
+{
+    const int64_t xp = padded_x(x);
+    return reinterpret_cast<uint16_t *>(static_cast<char *>(ws) + 2 * ((size_t(b * xp) * 8 + 255) / 256) * 256);
+}
 }  // namespace
 
+// Bytes of scratch the sorted code needs (0 when X <= 16384).
+size_t rank_times_ws(int64_t b, int64_t x, int sort) { return (sort && x > kMaxSortX) ? large_sort_ws(b, x) : 0; }
+
 // First-spike times [B, X] u16 of the rank-order (sort) or latency code.
-void rank_times(const void *in, spk_dtype itype, uint16_t *times, int64_t b, int64_t t, int64_t x, int sort,
+void rank_times(const void *in, spk_dtype itype, uint16_t *times, int64_t b, int64_t t, int64_t x, int sort, void *ws,
                 cudaStream_t s)
 {
     SPK_REQUIRE(itype == SPK_F32 || itype == SPK_U8, "coding supports F32/U8 input");
     if (b == 0) return;
+    if (sort && x > kMaxSortX)
+    {
+        SPK_REQUIRE(ws != nullptr, "workspace is too small");
+        if (itype == SPK_F32)
+            large_sorted_times((const float *)in, times, b, t, x, ws, s);
+        else
+            large_sorted_times((const uint8_t *)in, times, b, t, x, ws, s);
+        return;
+    }
     if (sort)
     {
-        if (x > kMaxSortX)
-            throw Error(SPK_ERR_UNSUPPORTED, "sorted rank coding supports at most 16384 values per image");
         int npow2 = 2;
         while (npow2 < x) npow2 <<= 1;
         const size_t smem = size_t(npow2) * 8 + size_t(x) * 2 + 16;
@@ -222,20 +400,35 @@ using namespace spk;
 
 extern "C" {
 
-size_t spk_rank_code_workspace(int64_t, int64_t, int) { return 0; }
+size_t spk_rank_code_workspace(int64_t b, int64_t x, int sort) { return rank_times_ws(b, x, sort); }
 
 spk_status spk_rank_code(const void *in, spk_dtype itype, void *out, spk_dtype otype, int64_t b, int64_t t, int64_t x,
-                         int sort, void *, size_t, spk_stream stream)
+                         int sort, void *ws, size_t ws_bytes, spk_stream stream)
 {
     return guarded([&] {
         SPK_REQUIRE(t > 0, "input time can't be less than 1");
         SPK_REQUIRE(b >= 0 && x >= 1, "invalid dims");
         SPK_REQUIRE(t <= 65535, "time is limited to 65535 steps");
         if (b == 0) return;
+        if (sort && x > kMaxSortX)
+        {
+            SPK_REQUIRE(itype == SPK_F32 || itype == SPK_U8, "sorted rank coding supports F32/U8 input");
+            SPK_REQUIRE(otype == SPK_U8 || otype == SPK_F32, "output type must be U8 or F32");
+            SPK_REQUIRE(ws != nullptr && ws_bytes >= large_sort_ws(b, x), "workspace is too small");
+            cudaStream_t s = stream_of(stream);
+            uint16_t *tm = large_times_slot(ws, b, x);
+            rank_times(in, itype, tm, b, t, x, sort, ws, s);
+            if (otype == SPK_U8)
+                rows_from_times_kernel<uint8_t><<<grid_for(b * ceil_div(x, 16), 256), 256, 0, s>>>(tm, (uint8_t *)out,
+                                                                                                  b, int(t), x);
+            else
+                rows_from_times_kernel<float><<<grid_for(b * ceil_div(x, 16), 256), 256, 0, s>>>(tm, (float *)out, b,
+                                                                                                int(t), x);
+            SPK_LAUNCHED();
+            return;
+        }
         if (sort)
         {
-            if (x > kMaxSortX)
-                throw Error(SPK_ERR_UNSUPPORTED, "sorted rank coding supports at most 16384 values per image");
             int npow2 = 2;
             while (npow2 < x) npow2 <<= 1;
             size_t smem = size_t(npow2) * 8 + size_t(x) * 2 + 16;

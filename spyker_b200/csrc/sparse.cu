@@ -20,8 +20,9 @@
 
 namespace spk
 {
-void rank_times(const void *in, spk_dtype itype, uint16_t *times, int64_t b, int64_t t, int64_t x, int sort,
+void rank_times(const void *in, spk_dtype itype, uint16_t *times, int64_t b, int64_t t, int64_t x, int sort, void *ws,
                 cudaStream_t s);
+size_t rank_times_ws(int64_t b, int64_t x, int sort);
 void launch_stdp_scan(float *kernel, int64_t k, int64_t nmaps, int64_t b, int64_t count, int field,
                       const int32_t *winners, const int32_t *counts, const uint16_t *pre, int64_t ps, int64_t pw,
                       const uint16_t *post, const double *configs, int64_t nconf, bool f32_rule, cudaStream_t s);
@@ -575,7 +576,7 @@ extern "C" {
 
 size_t spk_sparse_code_workspace(int64_t u, int64_t t, int64_t c, int64_t h, int64_t w)
 {
-    return al(size_t(u * c * h * w) * 2) + times_to_lists_ws(u, t);
+    return al(size_t(u * c * h * w) * 2) + times_to_lists_ws(u, t) + al(rank_times_ws(u, c * h * w, 1));
 }
 
 spk_status spk_sparse_code(const void *in, spk_dtype itype, int64_t u, int64_t c, int64_t h, int64_t w, int64_t t,
@@ -594,14 +595,15 @@ spk_status spk_sparse_code(const void *in, spk_dtype itype, int64_t u, int64_t c
         }
         Carve cv{static_cast<char *>(ws)};
         uint16_t *tm = cv.take<uint16_t>(size_t(u * c * h * w));
-        rank_times(in, itype, tm, u, t, c * h * w, sort, s);
+        void *sort_ws = cv.take<char>(rank_times_ws(u, c * h * w, sort));
+        rank_times(in, itype, tm, u, t, c * h * w, sort, sort_ws, s);
         times_to_lists(tm, u, t, c, h, w, offsets, events, cv, s);
     });
 }
 
 size_t spk_sparse_from_dense_workspace(int64_t u, int64_t t, int64_t c, int64_t h, int64_t w)
 {
-    return spk_sparse_code_workspace(u, t, c, h, w);
+    return al(size_t(u * c * h * w) * 2) + times_to_lists_ws(u, t);
 }
 
 spk_status spk_sparse_from_dense(const void *in, spk_dtype itype, int64_t u, int64_t t, int64_t c, int64_t h,

@@ -341,8 +341,9 @@ def code(array, time: int, sort: bool = True, dtype: str = "u8", code: str = "ra
     x = x.reshape(s)
     out = torch.empty(shape.code(s, time), dtype=torch_dtype(dtype), device=x.device)
     x_elems = int(numpy.prod(s[1:]))
+    ws, wsb = _workspace(_lib.lib.spk_rank_code_workspace(s[0], x_elems, int(sort)), x.device)
     call("spk_rank_code", ptr(x), type_code(x.dtype), ptr(out), type_code(out.dtype), s[0], time, x_elems, int(sort),
-         None, 0, stream())
+         ptr(ws), wsb, stream())
     return a.back(out)
 
 

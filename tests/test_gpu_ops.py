@@ -101,6 +101,28 @@ def test_code(port, dog, sort):
     assert np.array_equal(got, stable_code(dog, 15))
 
 
+def test_code_large_images(port):
+    """Images above 16384 values (device-wide sort): the 8 x 256 x 256 Gabor
+    geometry, a size that is not a multiple of the sort chunk, and u8 input
+    full of ties."""
+    rng = np.random.default_rng(21)
+    big = rng.random((2, 8, 256, 256), dtype=np.float32)
+    big[big < 0.3] = 0  # a large tied minimum
+    got = host(spyker.code(cuda(big), 30))
+    assert np.array_equal(got, stable_code(big, 30))
+    odd = rng.random((3, 3, 100, 111), dtype=np.float32)
+    got = host(spyker.code(cuda(odd), 15))
+    assert np.array_equal(got, stable_code(odd, 15))
+    assert np.array_equal(got, port.rank_code(odd, 15))  # no ties: the reference order too
+    u8 = (rng.random((2, 40000)) * 7).astype(np.uint8)
+    got = host(spyker.code(cuda(u8), 12, dtype="f32"))
+    assert np.array_equal(got, stable_code(u8, 12).astype(np.float32))
+    ev = spyker.sparse.code(cuda(odd), 15)
+    want = port.sparse_from_dense(stable_code(odd, 15))
+    off, zyx = ev.lists()
+    assert np.array_equal(off, want[0]) and np.array_equal(zyx, want[1].reshape(-1, 3))
+
+
 def test_code_u8_and_edges(port):
     img = synth.strokes(16, seed=3)
     assert np.array_equal(host(spyker.code(cuda(img), 10, sort=False)), port.rank_code(img, 10, False))
