@@ -66,6 +66,11 @@ struct TcParams
     uint8_t *spikes;    // [B, T, Cout, OH, OW]
     int4 *records;      // [B * OH * OW]: (winning channel, first step, value bits, 0)
     unsigned *mins, *maxs;  // [B] order-preserving encodings
+    // fused producers: `in` is the first-spike map [B, H, W, Cp]; when *flag
+    // is set the input was not cumulative 0/1 spikes and rows are gathered
+    // from `raw` [B, T, Cin, H, W] instead
+    const uint8_t *raw;
+    const int *flag;
 };
 
 constexpr int kPotentials = 0, kFused = 1;
@@ -239,29 +244,126 @@ __device__ __forceinline__ void load_exact16(uint32_t lane_base, int c0, int n_t
 // hold a WTA key, so each pixel yields one record (channel, first step,
 // value) and the per-sample min / max of the inhibited potentials.  Run by
 // warps 0-3, one (pixel, step) row per thread; `acc` is the accumulator base.
+// Fast first-max state of one row (see row_argmax).
+struct FastMax
+{
+    float r1 = -INFINITY, r2 = -INFINITY, amax = 0.f, dmin = INFINITY;
+    int a1 = -1, b1 = INT_MAX;
+};
+
+constexpr int kEpiChunk = 8;  // accumulator columns per tensor-memory load
+
+template <int NS>
+__device__ __forceinline__ void tmem_chunk(uint32_t lane_base, int c0, int n_tile, uint32_t (&q)[3][kEpiChunk])
+{
+    tmem_ld8(lane_base + uint32_t(c0), q[0]);
+    tmem_ld8(lane_base + uint32_t(n_tile + c0), q[1]);
+    if (NS == 3) tmem_ld8(lane_base + uint32_t(2 * n_tile + c0), q[2]);
+}
+
+template <int NS>
+__device__ __forceinline__ void tmem_chunk_wait(uint32_t (&q)[3][kEpiChunk])
+{
+    tmem_ld_wait8(q[0]);
+    tmem_ld_wait8(q[1]);
+    if (NS == 3) tmem_ld_wait8(q[2]);
+}
+
+// One chunk of columns: f = (h + m) + l in FP32, the largest above-threshold
+// value (first index on ties) and the runner-up, the first below-threshold
+// channel, the largest |h| + |m| + |l| and the closest distance to the
+// threshold.  Branch-free.
+template <int NS>
+__device__ __forceinline__ void fast_chunk(const TcParams &P, const uint32_t (&q)[3][kEpiChunk], int c0, FastMax &st)
+{
+#pragma unroll
+    for (int j = 0; j < kEpiChunk; ++j)
+    {
+        const int c = c0 + j;
+        const float h = __uint_as_float(q[0][j]), m = __uint_as_float(q[1][j]);
+        const float l = NS == 3 ? __uint_as_float(q[2][j]) : 0.f;
+        const float f = __fadd_rn(__fadd_rn(h, m), l);
+        const float a = __fadd_rn(__fadd_rn(fabsf(h), fabsf(m)), fabsf(l));
+        const bool valid = c < P.cout;
+        const bool real = valid && f > P.thr;
+        const bool gt = real && f > st.r1;
+        st.amax = valid ? fmaxf(st.amax, a) : st.amax;
+        st.dmin = valid ? fminf(st.dmin, fabsf(__fsub_rn(f, P.thr))) : st.dmin;
+        st.r2 = gt ? st.r1 : (real ? fmaxf(st.r2, f) : st.r2);
+        st.r1 = gt ? f : st.r1;
+        st.a1 = gt ? c : st.a1;
+        st.b1 = (valid && !real) ? min(st.b1, c) : st.b1;
+    }
+}
+
+// Thresholded first-max channel of one row, exactly as with the FP64-summed
+// potentials.  Fast pass: the BF16 terms are added in FP32, f = (h + m) + l,
+// which is within 3.01 * 2^-24 * (|h| + |m| + |l|) of the exactly rounded
+// potential; with tol = 2^-21 times the row's largest such sum, every
+// decision is certain unless some potential is within tol of the threshold,
+// the two largest above-threshold values are within 2 tol, or the largest is
+// within tol of the below-threshold value or of the inhibition threshold.
+// Such rows (rare) are redone with FP64 sums.  Tensor-memory loads of the
+// next chunk are in flight while a chunk is processed.
+template <int NS>
+__device__ __forceinline__ void row_argmax(const TcParams &P, uint32_t lane_base, bool row_ok, int &am, float &xam)
+{
+    FastMax st;
+    constexpr int W = kEpiChunk;
+    uint32_t qa[3][W], qb[3][W];
+    tmem_chunk<NS>(lane_base, 0, P.n_tile, qa);
+    for (int c0 = 0; c0 < P.n_tile; c0 += 2 * W)
+    {
+        // n_tile is a multiple of 16 = 2 W: both halves exist
+        tmem_chunk_wait<NS>(qa);
+        tmem_chunk<NS>(lane_base, c0 + W, P.n_tile, qb);
+        fast_chunk<NS>(P, qa, c0, st);
+        tmem_chunk_wait<NS>(qb);
+        if (c0 + 2 * W < P.n_tile) tmem_chunk<NS>(lane_base, c0 + 2 * W, P.n_tile, qa);
+        fast_chunk<NS>(P, qb, c0 + W, st);
+    }
+    const float tol = __fmaf_rn(st.amax, 0x1p-21f, 0x1p-140f);
+    bool unsure = st.dmin <= tol;
+    const bool has_real = st.a1 >= 0, has_low = st.b1 != INT_MAX;
+    if (has_real && has_low) unsure |= fabsf(__fsub_rn(st.r1, P.thv)) <= tol;
+    const bool real_wins = has_real && (!has_low || st.r1 > P.thv);
+    if (real_wins) unsure |= __fsub_rn(st.r1, st.r2) <= 2.f * tol || fabsf(__fsub_rn(st.r1, P.inh_thr)) <= tol;
+    am = real_wins ? st.a1 : st.b1;
+    xam = real_wins ? st.r1 : P.thv;
+    if (__any_sync(0xffffffffu, unsure && row_ok))
+    {
+        // exact pass: FP64 sums rounded once to F32 (warp-uniform tcgen05.ld)
+        float mx = 0.f;
+        int ae = 0;
+        for (int c0 = 0; c0 < P.n_tile; c0 += 16)
+        {
+            float v[16];
+            load_exact16(lane_base, c0, P.n_tile, NS, v);
+#pragma unroll
+            for (int j = 0; j < 16; ++j)
+            {
+                const int c = c0 + j;
+                const float x = (v[j] <= P.thr) ? P.thv : v[j];
+                if (c == 0)
+                    mx = x;
+                else if (c < P.cout && x > mx)
+                    mx = x, ae = c;
+            }
+        }
+        if (unsure) am = ae, xam = mx;
+    }
+}
+
+template <int NS>
 __device__ void fused_epilogue(const TcParams &P, uint32_t acc, bool row_ok, int tstep, int64_t sample, int64_t pix)
 {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int TP = 1 << P.tp_log2, T = P.T, C = P.cout;
-    const uint32_t lane_base = acc + (uint32_t(warp * 32) << 16);
+    const uint32_t lane_base = acc + (uint32_t((warp & 3) * 32) << 16);
     // thresholded first-max channel of this (pixel, step)
-    float mx = 0.f;
-    int am = 0;
-    for (int c0 = 0; c0 < P.n_tile; c0 += 16)
-    {
-        float v[16];
-        load_exact16(lane_base, c0, P.n_tile, P.nsplit, v);
-#pragma unroll
-        for (int j = 0; j < 16; ++j)
-        {
-            const int c = c0 + j;
-            const float x = (v[j] <= P.thr) ? P.thv : v[j];
-            if (c == 0)
-                mx = x;
-            else if (c < C && x > mx)
-                mx = x, am = c;
-        }
-    }
+    float mx;
+    int am;
+    row_argmax<NS>(P, lane_base, row_ok, am, mx);
     const int base = (lane >> P.tp_log2) << P.tp_log2;  // first lane of this pixel
     const unsigned grp = (TP == 32) ? 0xffffffffu : (((1u << TP) - 1u) << base);
     const unsigned above = __ballot_sync(0xffffffffu, row_ok && mx > P.inh_thr) & grp;
@@ -411,6 +513,171 @@ __device__ __forceinline__ void gather_store(const TcParams &, const Gathered &g
     for (int j = 0; j < 4; ++j) *reinterpret_cast<uint4 *>(a + (c_lo + j) * 128) = bf16x8_of_bytes(g.v[j]);
 }
 
+// ---- fused producers ---------------------------------------------------------
+// A rows (pixel, t) of a fused tile from the first-spike map: a unit (pixel,
+// 8-wide K chunk, R consecutive steps) loads the chunk's 8 first-spike bytes
+// once (one 8-byte load channels-last, or 8 byte gathers when Cin < 8) and
+// writes R rows of BF16 {0, 1}.  K order and table entries (c, ky, kx,
+// valid) as the weight image.
+struct FusedPixel
+{
+    bool ok;
+    int64_t sample;
+    int iy0, ix0;
+};
+
+__device__ __forceinline__ FusedPixel fused_pixel(const TcParams &P, int64_t mt, int pl)
+{
+    FusedPixel u{};
+    const int64_t gp = mt * P.pp + pl;
+    u.ok = gp < P.npix;
+    if (u.ok)
+    {
+        u.sample = gp / P.ohw;
+        const int pix = int(gp - u.sample * P.ohw), oy = pix / P.ow, ox = pix - oy * P.ow;
+        u.iy0 = oy * P.sy - P.top;
+        u.ix0 = ox * P.sx - P.left;
+    }
+    return u;
+}
+
+// First-spike bytes of K chunk (kb, kc) for a pixel; 0xFF = never.
+__device__ __forceinline__ uint2 fst_chunk(const TcParams &P, const int4 *tab, const FusedPixel &u, int kb, int kc)
+{
+    if (!u.ok) return make_uint2(~0u, ~0u);
+    const uint8_t *base = P.in + u.sample * P.img_stride;
+    if (P.nhwc)
+    {
+        const int4 e = tab[kb * BK + kc * 8];
+        const int iy = u.iy0 + e.y, ix = u.ix0 + e.z;
+        if (e.w && iy >= 0 && iy < P.h && ix >= 0 && ix < P.w)
+            return *reinterpret_cast<const uint2 *>(base + (int64_t(iy) * P.w + ix) * P.cpad + e.x);
+        return make_uint2(~0u, ~0u);
+    }
+    uint32_t w[2] = {0, 0};
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+    {
+        const int4 e = tab[kb * BK + kc * 8 + i];
+        const int iy = u.iy0 + e.y, ix = u.ix0 + e.z;
+        uint32_t b = 0xFF;
+        if (e.w && iy >= 0 && iy < P.h && ix >= 0 && ix < P.w) b = base[(int64_t(iy) * P.w + ix) * P.cin + e.x];
+        w[i >> 2] |= b << (8 * (i & 3));
+    }
+    return make_uint2(w[0], w[1]);
+}
+
+__device__ __forceinline__ unsigned char *a_row_chunk(unsigned char *sA, int r, int kc)
+{
+    return sA + (r >> 3) * 1024 + (r & 7) * 16 + kc * 128;
+}
+
+// Rows t0 .. t0+R-1: byte b of the chunk is 1 where first-spike[b] <= t.
+// (f | 0x80) - (t + 1) keeps bit 7 of a byte iff f > t, with no borrow
+// between bytes since t + 1 <= 32.
+__device__ __forceinline__ void store_fst_rows(unsigned char *sA, int row0, int t0, int R, int kc, uint2 f)
+{
+    const uint32_t lo = f.x | 0x80808080u, hi = f.y | 0x80808080u;
+    for (int i = 0; i < R; ++i)
+    {
+        const uint32_t tt = uint32_t(t0 + i + 1) * 0x01010101u;
+        const uint32_t sl = (~(lo - tt) >> 7) & 0x01010101u, sh = (~(hi - tt) >> 7) & 0x01010101u;
+        uint4 v;
+        v.x = __byte_perm(sl, 0, 0x7170) * 0x3F80u;
+        v.y = __byte_perm(sl, 0, 0x7372) * 0x3F80u;
+        v.z = __byte_perm(sh, 0, 0x7170) * 0x3F80u;
+        v.w = __byte_perm(sh, 0, 0x7372) * 0x3F80u;
+        *reinterpret_cast<uint4 *>(a_row_chunk(sA, row0 + i, kc)) = v;
+    }
+}
+
+// Fallback rows gathered from the spikes themselves (any u8 values).
+__device__ __forceinline__ void store_raw_rows(const TcParams &P, const int4 *tab, const FusedPixel &u,
+                                               unsigned char *sA, int row0, int t0, int R, int kb, int kc)
+{
+    for (int i = 0; i < R; ++i)
+    {
+        const int t = t0 + i;
+        uint32_t w[2] = {0, 0};
+        if (u.ok && t < P.T)
+        {
+            const uint8_t *base = P.raw + (u.sample * P.T + t) * int64_t(P.cin) * P.h * P.w;
+            for (int e8 = 0; e8 < 8; ++e8)
+            {
+                const int4 e = tab[kb * BK + kc * 8 + e8];
+                const int iy = u.iy0 + e.y, ix = u.ix0 + e.z;
+                uint32_t b = 0;
+                if (e.w && iy >= 0 && iy < P.h && ix >= 0 && ix < P.w)
+                    b = base[(int64_t(e.x) * P.h + iy) * P.w + ix];
+                w[e8 >> 2] |= b << (8 * (e8 & 3));
+            }
+        }
+        *reinterpret_cast<uint4 *>(a_row_chunk(sA, row0 + i, kc)) = bf16x8_of_bytes(make_uint2(w[0], w[1]));
+    }
+}
+
+// Fused producer loop of thread p (0..255) with NU unit slots (units per
+// thread: 1 when a unit covers 4 steps, up to 4 for T <= 2).
+template <int NU>
+__device__ __forceinline__ void fused_producer(const TcParams &P, const int4 *tab, unsigned char *smem,
+                                               uint64_t *full_bar, uint64_t *empty_bar, int S, int stage_bytes,
+                                               int a_bytes, int b_bytes, int p)
+{
+    const int TP = 1 << P.tp_log2, R = TP < 4 ? TP : 4, G = TP / R;
+    const int units = P.pp * 8 * G;  // 1024 / R
+    const bool raw = *P.flag != 0;
+    int upl[NU], ukc[NU], ug[NU];
+#pragma unroll
+    for (int i = 0; i < NU; ++i)
+    {
+        const int q = p + i * 256;
+        ug[i] = q % G, ukc[i] = (q / G) & 7, upl[i] = q / (G * 8);
+    }
+    uint32_t it = 0;
+    bool failed = false;
+    for (int64_t tile = blockIdx.x; tile < P.tiles && !failed; tile += gridDim.x)
+    {
+        FusedPixel fu[NU];
+#pragma unroll
+        for (int i = 0; i < NU; ++i)
+            if (p + i * 256 < units) fu[i] = fused_pixel(P, tile, upl[i]);
+        for (int kb = 0; kb < P.kblocks; ++kb, ++it)
+        {
+            // the loads are in flight while waiting for the stage
+            uint2 f[NU];
+            if (!raw)
+#pragma unroll
+                for (int i = 0; i < NU; ++i)
+                    if (p + i * 256 < units) f[i] = fst_chunk(P, tab, fu[i], kb, ukc[i]);
+            const int s = int(it % uint32_t(S));
+            const uint32_t u = it / uint32_t(S);
+            if (u > 0 && !wait_bounded(&empty_bar[s], (u - 1) & 1))
+            {
+                failed = true;
+                break;
+            }
+            unsigned char *sA = smem + s * stage_bytes;
+            if (p == 0)
+            {
+                arrive_expect_tx(&full_bar[s], uint32_t(b_bytes));
+                bulk_g2s(sA + a_bytes, P.wimg + int64_t(kb) * b_bytes, uint32_t(b_bytes), &full_bar[s]);
+            }
+#pragma unroll
+            for (int i = 0; i < NU; ++i)
+                if (p + i * 256 < units)
+                {
+                    const int row0 = upl[i] * TP + ug[i] * R, t0 = ug[i] * R;
+                    if (raw)
+                        store_raw_rows(P, tab, fu[i], sA, row0, t0, R, kb, ukc[i]);
+                    else
+                        store_fst_rows(sA, row0, t0, R, ukc[i], f[i]);
+                }
+            fence_proxy_async_smem();
+            mbar_arrive(&full_bar[s]);
+        }
+    }
+}
+
 // Warp-specialised persistent kernel (416 threads):
 //   warps 4-11 producers: per K block, wait for a free stage, bulk-copy the
 //              weight block (thread 128) and gather half an A row each;
@@ -423,6 +690,7 @@ __device__ __forceinline__ void gather_store(const TcParams &, const Gathered &g
 // epilogue arrivals).  Every wait is bounded; a timeout raises the device
 // status word and makes every role leave.
 constexpr int kWsThreads = 416, kMaxStages = 6;
+__host__ __device__ constexpr int ws_threads(int) { return kWsThreads; }
 
 template <int MODE>
 __global__ void __launch_bounds__(kWsThreads, 1) conv_ws_kernel(TcParams P)
@@ -438,7 +706,20 @@ __global__ void __launch_bounds__(kWsThreads, 1) conv_ws_kernel(TcParams P)
     const int stage_bytes = a_bytes + b_bytes;
     int4 *tab = reinterpret_cast<int4 *>(smem + S * stage_bytes);
     const int taps = P.kh * P.kw;
-    if (P.nhwc)
+    if constexpr (MODE == kFused)
+    {
+        // per K element: (channel, ky, kx, valid) in the weight image's order
+        for (int k = tid; k < P.kblocks * BK; k += blockDim.x)
+        {
+            int c, tap;
+            if (P.nhwc)
+                tap = k / P.cpad, c = k % P.cpad;
+            else
+                c = k / taps, tap = k % taps;
+            tab[k] = make_int4(c, tap / P.kw, tap % P.kw, (tap < taps && c < P.cin) ? 1 : 0);
+        }
+    }
+    else if (P.nhwc)
     {
         const int groups = P.cpad / 8;
         for (int q = tid; q < P.kblocks * 8; q += blockDim.x)
@@ -472,7 +753,15 @@ __global__ void __launch_bounds__(kWsThreads, 1) conv_ws_kernel(TcParams P)
     const uint32_t tmem = tmem_slot;
     const int acc_cols = P.nsplit * P.n_tile;
 
-    if (warp >= 4 && warp < 12)
+    if (MODE == kFused && warp >= 4 && warp < 12)
+    {
+        // ---------------- fused producers (8 warps) ----------------
+        if (P.tp_log2 >= 2)
+            fused_producer<1>(P, tab, smem, full_bar, empty_bar, S, stage_bytes, a_bytes, b_bytes, tid - 128);
+        else
+            fused_producer<4>(P, tab, smem, full_bar, empty_bar, S, stage_bytes, a_bytes, b_bytes, tid - 128);
+    }
+    else if (warp >= 4 && warp < 12)
     {
         // ---------------- producers (8 warps) ----------------
         // Thread p gathers K chunks c_lo..c_lo+3 of row prow.  The loads of the
@@ -574,6 +863,8 @@ __global__ void __launch_bounds__(kWsThreads, 1) conv_ws_kernel(TcParams P)
     else
     {
         // ---------------- epilogue (warps 0-3) ----------------
+        // warp w reads tensor-memory lanes 32 w .. 32 w + 31 (rows of the tile)
+        const int row = (warp & 3) * 32 + lane;
         uint32_t j = 0;
         for (int64_t tile = blockIdx.x; tile < P.tiles; tile += gridDim.x, ++j)
         {
@@ -583,11 +874,11 @@ __global__ void __launch_bounds__(kWsThreads, 1) conv_ws_kernel(TcParams P)
             tc_fence_after();
             const int64_t mt = tile / P.n_tiles;
             const int nt = int(tile % P.n_tiles);
-            const RowInfo r = row_info<MODE>(P, mt, tid);
+            const RowInfo r = row_info<MODE>(P, mt, row);
             const uint32_t acc = tmem + uint32_t(a * acc_cols);
             if constexpr (MODE == kPotentials)
             {
-                const uint32_t lane_base = acc + (uint32_t(warp * 32) << 16);
+                const uint32_t lane_base = acc + (uint32_t((warp & 3) * 32) << 16);
                 for (int c0 = 0; c0 < P.n_tile; c0 += 16)
                 {
                     float v[16];
@@ -603,10 +894,10 @@ __global__ void __launch_bounds__(kWsThreads, 1) conv_ws_kernel(TcParams P)
                     }
                 }
             }
+            else if (P.nsplit == 3)
+                fused_epilogue<3>(P, acc, r.ok, r.tstep, r.sample, r.pix);
             else
-            {
-                fused_epilogue(P, acc, r.ok, r.tstep, r.sample, r.pix);
-            }
+                fused_epilogue<2>(P, acc, r.ok, r.tstep, r.sample, r.pix);
             tc_fence_before();
             mbar_arrive(&acce_bar[a]);
         }
@@ -688,6 +979,8 @@ __global__ void wta_records_kernel(const int4 *__restrict__ records, const unsig
     if (threadIdx.x == 0) counts[b] = found;
 }
 
+inline size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
+
 struct Plan
 {
     int nsplit, n_tile, n_tiles, kblocks, cpad, stages, nacc;
@@ -698,7 +991,7 @@ struct Plan
 
 // single_tile: all output channels in one CTA (required by the fused epilogue).
 Plan make_plan(int64_t n, int64_t cin, int64_t h, int64_t w, int64_t cout, int64_t kh, int64_t kw, int precision,
-               bool single_tile)
+               bool single_tile, int64_t t_fused = 0)
 {
     Plan pl{};
     pl.nsplit = precision == SPK_CONV_BF16X3 ? 3 : 2;
@@ -719,9 +1012,12 @@ Plan make_plan(int64_t n, int64_t cin, int64_t h, int64_t w, int64_t cout, int64
     pl.tmem_cols = cols;
     pl.wimg_bytes = size_t(pl.n_tiles) * pl.kblocks * pl.nsplit * pl.n_tile * BK * 2;
     // staged copy of the spikes: channels-last [N, H, W, Cpad] (plain), or
-    // [B, H, W, T, Cpad or Cin] (fused; single_tile), where every call stages
-    pl.xt_bytes = pl.nhwc ? size_t(n) * h * w * pl.cpad : (single_tile ? size_t(n) * h * w * cin : 0);
-    const size_t tab = pl.nhwc ? size_t(pl.kblocks) * 8 * 16 : size_t(pl.kblocks) * BK * 16;
+    // the first-spike map [B, H, W, Cpad or Cin] plus a flag word (fused)
+    if (t_fused > 0)
+        pl.xt_bytes = align256(size_t(n / t_fused) * h * w * (pl.nhwc ? pl.cpad : cin)) + 256;
+    else
+        pl.xt_bytes = pl.nhwc ? size_t(n) * h * w * pl.cpad : 0;
+    const size_t tab = (t_fused > 0 || !pl.nhwc) ? size_t(pl.kblocks) * BK * 16 : size_t(pl.kblocks) * 8 * 16;
     const size_t stage = size_t(BM * BK * 2) + size_t(pl.nsplit) * pl.n_tile * BK * 2;
     const size_t budget = 225 * 1024 - tab;
     pl.stages = int(std::min<size_t>(4, budget / stage));
@@ -734,48 +1030,44 @@ Plan make_plan(int64_t n, int64_t cin, int64_t h, int64_t w, int64_t cout, int64
     return pl;
 }
 
-inline size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
-
-// Split the weights and (channels-last) transpose the spikes into the
-// workspace; fill the fields of P shared by both epilogues.
-// Fused layout: [B, T, C, H, W] -> [B, H, W, T, Cp] (Cp = Cpad or Cin, pad
-// channels zero), so the TP rows of a pixel read adjacent bytes.
-__global__ void to_pixel_time_kernel(const uint8_t *__restrict__ in, uint8_t *__restrict__ out, int64_t b, int t,
-                                     int c, int64_t hw, int cp)
+// Split the weights and stage the spikes into the workspace; fill the
+// fields of P shared by both epilogues.
+//
+// Fused staging: the first-spike map [B, H, W, Cp] u8 (Cp = Cpad or Cin) of
+// the input [B, T, Cin, H, W]: the first step with a non-zero value, T when
+// none, 0xFF in pad channels.  A value other than 0/1, or a zero after a
+// one, sets *flag: the producers then gather from the spikes themselves.
+__global__ void fst_stage_kernel(const uint8_t *__restrict__ in, uint8_t *__restrict__ fst, int *__restrict__ flag,
+                                 int64_t b, int t, int c, int64_t hw, int cp)
 {
-    const int groups = (cp + 7) / 8;
-    const int64_t total = b * hw * t * groups;
+    const int64_t total = b * cp * hw, st = int64_t(c) * hw;
+    bool bad = false;
     for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += int64_t(gridDim.x) * blockDim.x)
     {
-        const int g = int(i % groups);
-        const int64_t r = i / groups;  // (sample, pixel, step) in output order
-        const int q = int(r % t);
-        const int64_t px = (r / t) % hw, s = r / (int64_t(t) * hw);
-        const uint8_t *src = in + ((s * t + q) * c) * hw + px;
-        uint8_t *dst = out + r * cp + g * 8;
-        const int n8 = min(8, cp - g * 8);
-        if (n8 == 8)
+        const int64_t px = i % hw, r = i / hw, smp = r / cp;
+        const int ch = int(r - smp * cp);
+        int first = 0xFF;
+        if (ch < c)
         {
-            uint32_t lo = 0, hi = 0;
+            const uint8_t *p = in + (smp * t * c + ch) * hw + px;
+            first = t;
+            for (int q0 = 0; q0 < t; q0 += 8)
+            {
+                uint32_t v[8];
 #pragma unroll
-            for (int e = 0; e < 8; ++e)
-            {
-                const int ch = g * 8 + e;
-                const uint32_t v = ch < c ? src[int64_t(ch) * hw] : 0u;
-                if (e < 4)
-                    lo |= v << (8 * e);
-                else
-                    hi |= v << (8 * (e - 4));
+                for (int u = 0; u < 8; ++u) v[u] = (q0 + u < t) ? p[int64_t(q0 + u) * st] : 0u;
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+                    if (q0 + u < t)
+                    {
+                        bad |= v[u] > 1 || (v[u] == 0 && first < t);
+                        if (v[u] != 0 && first == t) first = q0 + u;
+                    }
             }
-            *reinterpret_cast<uint2 *>(dst) = make_uint2(lo, hi);
         }
-        else
-            for (int e = 0; e < n8; ++e)
-            {
-                const int ch = g * 8 + e;
-                dst[e] = ch < c ? src[int64_t(ch) * hw] : 0;
-            }
+        fst[(smp * hw + px) * cp + ch] = uint8_t(first);
     }
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
 }
 
 // t_fused > 0: stage for the fused (pixel, time) rows of t_fused steps.
@@ -798,12 +1090,15 @@ TcParams prepare(const Plan &pl, const void *in, const float *kernel, int64_t n,
     if (t_fused > 0)
     {
         const int64_t b = n / t_fused, cp = pl.nhwc ? pl.cpad : cin;
-        const int64_t work = n * h * w * ((cp + 7) / 8);
-        to_pixel_time_kernel<<<grid_for(work, 256), 256, 0, s>>>(a_src, xt, b, int(t_fused), int(cin), h * w, int(cp));
+        int *flag = reinterpret_cast<int *>(xt + align256(size_t(b) * h * w * cp));
+        SPK_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), s));
+        fst_stage_kernel<<<grid_for(b * cp * h * w, 256), 256, 0, s>>>(a_src, xt, flag, b, int(t_fused), int(cin),
+                                                                       h * w, int(cp));
         SPK_LAUNCHED();
+        P.raw = a_src;
+        P.flag = flag;
         a_src = xt;
-        P.ts = cp, P.ps = t_fused * cp, P.rs = w * t_fused * cp, P.cs = 1;
-        P.img_stride = h * w * t_fused * cp;  // per sample
+        P.img_stride = h * w * cp;  // per sample
     }
     else if (pl.nhwc)
     {
@@ -839,10 +1134,10 @@ void launch(const TcParams &P, const Plan &pl, cudaStream_t s)
     auto kern = conv_ws_kernel<MODE>;
     SPK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(pl.smem)));
     int per_sm = 1;
-    SPK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kWsThreads, pl.smem));
+    SPK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, ws_threads(MODE), pl.smem));
     per_sm = std::max(1, std::min<int>(per_sm, int(512 / pl.tmem_cols)));
     const int64_t grid = std::min<int64_t>(P.tiles, int64_t(sm_count()) * per_sm);
-    kern<<<unsigned(grid), kWsThreads, pl.smem, s>>>(P);
+    kern<<<unsigned(grid), ws_threads(MODE), pl.smem, s>>>(P);
     SPK_LAUNCHED();
 }
 
@@ -860,7 +1155,7 @@ FusedLayout fused_layout(int64_t b, int64_t t, int64_t cin, int64_t h, int64_t w
     FusedLayout L{};
     L.oh = (h + p.top + p.bottom - kh) / sy + 1;
     L.ow = (w + p.left + p.right - kw) / sx + 1;
-    L.pl = make_plan(b * t, cin, h, w, cout, kh, kw, precision, true);
+    L.pl = make_plan(b * t, cin, h, w, cout, kh, kw, precision, true, t);
     int tp = 1, lg = 0;
     while (tp < t) tp <<= 1, ++lg;
     L.tp_log2 = lg;

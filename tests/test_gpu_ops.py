@@ -432,6 +432,10 @@ FUSED = [
     (12, 15, 30, 14, 14, 100, 5, 2, 10.0, 1, 8),
     (3, 30, 8, 21, 19, 64, 7, 3, 20.0, 2, 6),
     (7, 5, 3, 9, 11, 17, 3, 1, 2.5, 0, 40),
+    (5, 32, 4, 10, 10, 20, 3, 1, 3.0, 1, 4),
+    (6, 3, 9, 8, 9, 16, 3, 1, 4.0, 1, 3),
+    (4, 2, 2, 12, 12, 8, 5, 2, 3.0, 2, 5),
+    (4, 1, 5, 7, 6, 12, 3, 0, 2.0, 1, 2),
 ]
 
 
@@ -453,6 +457,27 @@ def test_fused_layer_matches_ops(port, case, prec):
     got, want = winners_np(wins), winners_np(ref_wins)
     assert np.array_equal(got[1], want[1]) and np.array_equal(got[0], want[0])
     assert int(got[1].sum()) > 0
+
+
+@pytest.mark.parametrize("kind", ["random", "values"])
+def test_fused_layer_noncumulative(kind):
+    """Inputs that are not cumulative 0/1 spikes take the producers' direct
+    gather; results still equal the op-by-op pipeline."""
+    rng = np.random.default_rng(5 if kind == "random" else 6)
+    b, t, cin, h, w, cout = 6, 7, 10, 9, 8, 24
+    x = (rng.random((b, t, cin, h, w)) < 0.3).astype(np.uint8)
+    if kind == "values":
+        x = np.cumsum(x, axis=1).clip(0, 3).astype(np.uint8)  # monotone but not 0/1
+    x = cuda(x)
+    conv = spyker.Conv(cin, cout, 3, pad=1)
+    conv.kernel.copy_(cuda(rng.uniform(0.3, 1.0, size=(cout, cin, 3, 3)).astype(np.float32)))
+    conv.precision = "bf16x3"
+    spikes, wins = spyker.conv_fire_wta(x, conv, 3.0, 1, 4)
+    out = spyker.inhibit(spyker.threshold(conv(x), 3.0))
+    assert np.array_equal(host(spikes), host(spyker.fire(out)))
+    got, want = winners_np(wins), winners_np(spyker.convwta(out, 1, 4))
+    assert np.array_equal(got[1], want[1]) and np.array_equal(got[0], want[0])
+    assert spyker._lib.lib.spk_device_status(1) == 0
 
 
 def test_fused_layer_golden(golden):
