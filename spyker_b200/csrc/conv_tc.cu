@@ -575,11 +575,14 @@ __device__ __forceinline__ unsigned char *a_row_chunk(unsigned char *sA, int r, 
 // Rows t0 .. t0+R-1: byte b of the chunk is 1 where first-spike[b] <= t.
 // (f | 0x80) - (t + 1) keeps bit 7 of a byte iff f > t, with no borrow
 // between bytes since t + 1 <= 32.
-__device__ __forceinline__ void store_fst_rows(unsigned char *sA, int row0, int t0, int R, int kc, uint2 f)
+// `rot` rotates the order of the R rows so that the 8 lanes of a quarter
+// warp store to 8 different 16-byte bank groups.
+__device__ __forceinline__ void store_fst_rows(unsigned char *sA, int row0, int t0, int R, int kc, uint2 f, int rot)
 {
     const uint32_t lo = f.x | 0x80808080u, hi = f.y | 0x80808080u;
-    for (int i = 0; i < R; ++i)
+    for (int i0 = 0; i0 < R; ++i0)
     {
+        const int i = (i0 + rot) & (R - 1);
         const uint32_t tt = uint32_t(t0 + i + 1) * 0x01010101u;
         const uint32_t sl = (~(lo - tt) >> 7) & 0x01010101u, sh = (~(hi - tt) >> 7) & 0x01010101u;
         uint4 v;
@@ -670,7 +673,7 @@ __device__ __forceinline__ void fused_producer(const TcParams &P, const int4 *ta
                     if (raw)
                         store_raw_rows(P, tab, fu[i], sA, row0, t0, R, kb, ukc[i]);
                     else
-                        store_fst_rows(sA, row0, t0, R, ukc[i], f[i]);
+                        store_fst_rows(sA, row0, t0, R, ukc[i], f[i], (ug[i] >> 1) + 2 * (ukc[i] & 1));
                 }
             fence_proxy_async_smem();
             mbar_arrive(&full_bar[s]);
@@ -845,14 +848,23 @@ __global__ void __launch_bounds__(kWsThreads, 1) conv_ws_kernel(TcParams P)
                     tc_fence_after();
                     const uint32_t a_base = smem_u32(smem + s * stage_bytes);
                     const uint32_t b_base = a_base + uint32_t(a_bytes);
-                    for (int p = 0; p < P.nsplit; ++p)
+                    // The split terms' weight rows are stacked in one K-major
+                    // B of nsplit * n_tile rows whose accumulators are
+                    // adjacent: one MMA covers up to 256 of them, so the A
+                    // tile is read once per 256 columns, not once per term.
+                    const int ncols = P.nsplit * P.n_tile;
+                    for (int c = 0; c < ncols; c += 256)
+                    {
+                        const int n = ncols - c < 256 ? ncols - c : 256;
+                        const uint32_t idesc = idesc_bf16_f32(BM, n);
 #pragma unroll
                         for (int k16 = 0; k16 < BK / 16; ++k16)
                         {
                             const uint64_t ad = smem_desc(a_base + k16 * 256, 128, 1024);
-                            const uint64_t bd = smem_desc(b_base + p * P.n_tile * 128 + k16 * 256, 128, 1024);
-                            mma_bf16(d + uint32_t(p * P.n_tile), ad, bd, P.idesc, (kb > 0 || k16 > 0) ? 1u : 0u);
+                            const uint64_t bd = smem_desc(b_base + c * 128 + k16 * 256, 128, 1024);
+                            mma_bf16(d + uint32_t(c), ad, bd, idesc, (kb > 0 || k16 > 0) ? 1u : 0u);
                         }
+                    }
                     mma_commit(&empty_bar[s]);
                 }
                 if (!failed) mma_commit(&accf_bar[a]);
