@@ -82,17 +82,28 @@ __global__ void pool_warp_kernel(const T *__restrict__ in, T *__restrict__ out, 
     }
 }
 
+// Byte-wise max of four u8 lanes; spikes (0/1 bytes) take the OR.
+__device__ __forceinline__ uint32_t bmax4(uint32_t a, uint32_t b)
+{
+    const uint32_t o = a | b;
+    return (o & 0xFEFEFEFEu) ? __vmaxu4(a, b) : o;
+}
+
 // Whole planes staged in shared memory: a CTA takes `per_tile` consecutive
 // planes (one contiguous byte range, copied with 16-byte loads) and computes
 // their outputs from shared memory, so global traffic is one coalesced read
-// of the input and one of the output.  Thread per output for small windows
-// (taps in the reference's row-major order), warp per output for windows of
-// 64 taps and more.
-template <typename T, bool WARP>
+// of the input and one of the output.  Max is order independent except for
+// NaN, and the thread kind takes the taps in the reference's row-major order.
+// KIND 0: thread per output; 1: warp per output (windows of 64 taps and
+// more); 2: u8, windows 2 wide with stride 2 and no padding: four outputs
+// per thread from 32-bit words; 3: u8, the window is the whole plane: a
+// thread reduces a plane's words.
+template <typename T, int KIND>
 __global__ void __launch_bounds__(256) pool_plane_kernel(const T *__restrict__ in, T *__restrict__ out, int64_t n,
                                                          int h, int w, int oh, int ow, int ky, int kx, int sy, int sx,
                                                          int top, int left, int per_tile)
 {
+    constexpr bool WARP = KIND == 1;
     extern __shared__ __align__(16) unsigned char pool_smem[];
     const int hw = h * w, ohw = oh * ow;
     const int64_t tiles = (n + per_tile - 1) / per_tile;
@@ -107,7 +118,40 @@ __global__ void __launch_bounds__(256) pool_plane_kernel(const T *__restrict__ i
         const T *sp = reinterpret_cast<const T *>(pool_smem + shift);
         T *op = out + p0 * ohw;
         const int cnt = np * ohw;
-        if (!WARP)
+        if constexpr (KIND == 2)
+        {
+            const unsigned char *sb = pool_smem + shift;
+            const int G = (ow + 3) >> 2;
+            for (int it = threadIdx.x; it < np * oh * G; it += blockDim.x)
+            {
+                const int g = it % G, r = it / G, yo = r % oh, pl = r / oh;
+                const unsigned char *row = sb + pl * hw + yo * ky * w + 8 * g;
+                uint32_t a0 = *reinterpret_cast<const uint32_t *>(row), a1 = *reinterpret_cast<const uint32_t *>(row + 4);
+                for (int a = 1; a < ky; ++a)
+                {
+                    a0 = bmax4(a0, *reinterpret_cast<const uint32_t *>(row + a * w));
+                    a1 = bmax4(a1, *reinterpret_cast<const uint32_t *>(row + a * w + 4));
+                }
+                const uint32_t v = __byte_perm(bmax4(a0, a0 >> 8), bmax4(a1, a1 >> 8), 0x6420);
+                unsigned char *o = reinterpret_cast<unsigned char *>(op) + pl * ohw + yo * ow + 4 * g;
+                const int nv = min(4, ow - 4 * g);
+                for (int q = 0; q < nv; ++q) o[q] = (unsigned char)(v >> (8 * q));
+            }
+        }
+        else if constexpr (KIND == 3)
+        {
+            const uint32_t *sw = reinterpret_cast<const uint32_t *>(pool_smem + shift);
+            const int words = hw >> 2;
+            for (int pl = threadIdx.x; pl < np; pl += blockDim.x)
+            {
+                uint32_t v = 0;
+                for (int q = 0; q < words; ++q) v = bmax4(v, sw[pl * words + q]);
+                v = bmax4(v, v >> 16);
+                v = bmax4(v, v >> 8);
+                reinterpret_cast<unsigned char *>(op)[pl] = (unsigned char)(v & 0xFF);
+            }
+        }
+        else if constexpr (!WARP)
         {
             for (int o = threadIdx.x; o < cnt; o += blockDim.x)
             {
@@ -129,6 +173,7 @@ __global__ void __launch_bounds__(256) pool_plane_kernel(const T *__restrict__ i
         }
         else
         {
+            static_assert(KIND == 1, "pool kind");
             const int lane = threadIdx.x & 31, warps = blockDim.x >> 5;
             for (int o = threadIdx.x >> 5; o < cnt; o += warps)
             {
@@ -216,12 +261,21 @@ spk_status spk_rank_pool(const void *in, void *out, spk_dtype type, int64_t n, i
         dispatch(type, [&](auto z) {
             using T = decltype(z);
             const int64_t plane = h * w * int64_t(sizeof(T));
-            const int per_tile = int(std::max<int64_t>(1, std::min<int64_t>(kPoolTileBytes / plane, n)));
-            if (plane + 16 <= kPoolPlaneMax && per_tile * oh * ow < (int64_t(1) << 30))
+            // word kernels: u8, 4-byte aligned rows and planes, no padding
+            const bool words = sizeof(T) == 1 && reinterpret_cast<uintptr_t>(in) % 4 == 0 && (h * w) % 4 == 0 &&
+                               p.top == 0 && p.left == 0 && p.bottom == 0 && p.right == 0;
+            const bool pairs = words && kx == 2 && sx == 2 && ky == sy && w % 4 == 0;
+            const bool whole = words && ky == h && kx == w && oh == 1 && ow == 1;
+            const int64_t tile_bytes = whole ? 48 * 1024 : kPoolTileBytes;
+            const int per_tile = int(std::max<int64_t>(1, std::min<int64_t>(tile_bytes / plane, n)));
+            if (plane + 32 <= kPoolPlaneMax && per_tile * oh * ow < (int64_t(1) << 30))
             {
-                const int smem = int(per_tile * plane + 16);
+                const int smem = int(per_tile * plane + 32);  // + alignment shift and word over-reads
                 const bool warp = ky * kx >= 64;
-                auto k = warp ? pool_plane_kernel<T, true> : pool_plane_kernel<T, false>;
+                auto k = pairs   ? pool_plane_kernel<T, 2>
+                         : whole ? pool_plane_kernel<T, 3>
+                         : warp  ? pool_plane_kernel<T, 1>
+                                 : pool_plane_kernel<T, 0>;
                 if (smem > 48 * 1024)
                     SPK_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
                 int occ = 0;

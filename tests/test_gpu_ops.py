@@ -193,6 +193,23 @@ def test_pool_staging_edges(port):
         assert np.array_equal(got, port.pool(big, (k, k), (k, k), (0, 0, 0, 0)))
 
 
+@pytest.mark.parametrize("values", ["spikes", "bytes"])
+def test_pool_word_kernels(port, values):
+    """u8 pooling from 32-bit words: 2-wide windows (rows of 2 and 3, output
+    rows that end mid-word) and whole-plane windows, on 0/1 spikes and on any
+    byte values; an unaligned view takes the per-output kernel."""
+    rng = np.random.default_rng(17)
+    hi = 2 if values == "spikes" else 256
+    for shp, k in (((3, 5, 4, 12, 12), (2, 2)), ((2, 3, 5, 9, 20), (3, 2)), ((4, 2, 3, 6, 10), (6, 10)),
+                   ((2, 15, 30, 14, 14), (14, 14)), ((2, 15, 30, 28, 28), (2, 2))):
+        a = rng.integers(0, hi, size=shp).astype(np.uint8)
+        got = host(spyker.pool(cuda(a), k))
+        assert np.array_equal(got, port.pool(a, k, k, (0, 0, 0, 0)))
+    base = cuda(rng.integers(0, hi, size=(2 * 3 * 12 * 12 + 1,)).astype(np.uint8))
+    view = base[1:].view(2, 1, 3, 12, 12)
+    assert np.array_equal(host(spyker.pool(view, 2)), port.pool(host(view), (2, 2), (2, 2), (0, 0, 0, 0)))
+
+
 def test_inhibit(port, layer):
     for a, thr in ((layer["th"], 0.0), (layer["pot"], 25.0)):
         t = cuda(a)
