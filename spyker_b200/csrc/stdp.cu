@@ -22,10 +22,7 @@ namespace
 {
 constexpr int kMaxConfigs = 16;
 constexpr int kScanThreads = 256;
-constexpr int kScanPerThread = 4;  // weights per thread held in registers
-constexpr int kScanChunk = kScanThreads * kScanPerThread;
-constexpr int kWinnerTile = 1024;
-constexpr int kPreBatch = 14;  // winners whose pre rows are staged at once (28 KB)
+constexpr int kWinnerTile = 1024;  // winner records compacted per pass (4 per thread)
 
 struct Configs
 {
@@ -181,11 +178,96 @@ __global__ void fc_prepost_kernel(const T *__restrict__ in, const T *__restrict_
     }
 }
 
-// Kernel B: CTA (map, chunk) walks winners in (sample, slot) order.  The map
-// index of a winner is field `field` of its record (z for conv, x for fc).
-// pre address: pre + s * ps + j * pw + element.
+// Kernel B: CTA (map, chunk of 256 weights); every thread owns one weight
+// and applies the map's winners to it in (sample, slot) order.  Per tile of
+// 1024 winner records the CTA compacts the ones of its map (order kept) into
+// shared memory; then each thread walks them with the (pre, post) loads of
+// the next 8 winners in flight while it updates its weight, so the critical
+// path is the weight's own chain of dependent updates.  The map index of a
+// winner is field `field` of its record (z for conv, x for fc).
+// pre address: pre + s * ps + j * pw + element; post index s * count + j.
 // F32_RULE: the event-list STDP of src/spyker/sparse/stdp.cpp:95-97, which
 // rounds the soft-bound factor and the updated weight to F32 before the clamp.
+// v rounded to the nearest F32 (ties to even), returned as a double.  In the
+// normal F32 range this is integer arithmetic on the double's bits (drop 29
+// mantissa bits, round to nearest even; a carry into the exponent is the
+// correct result), which keeps conversions off the weight's dependency
+// chain; zeros, F32 denormals and the top binade go through the conversion.
+__device__ __forceinline__ double round_f32(double v)
+{
+    const unsigned long long u = static_cast<unsigned long long>(__double_as_longlong(v));
+    const int ex = int((u >> 52) & 0x7FF);
+    if ((u << 1) == 0) return v;
+    if (ex < 1023 - 126 || ex >= 1023 + 127) return double(__double2float_rn(v));
+    const unsigned long long r = (u + 0x0FFFFFFFull + ((u >> 29) & 1ull)) & ~0x1FFFFFFFull;
+    return __longlong_as_double(static_cast<long long>(r));
+}
+
+// One update of a weight kept as a double holding an F32 value.
+template <bool F32_RULE>
+__device__ __forceinline__ double stdp_update(double old, double d, double lo, double hi, bool stab)
+{
+    if (F32_RULE)
+    {
+        const double m = round_f32(stab ? (old - lo) * (hi - old) : 1.0);
+        double v = round_f32(fma(d, m, old));
+        v = (hi < v) ? hi : v;
+        v = (lo < v) ? v : lo;
+        return round_f32(v);
+    }
+    const double m = stab ? (old - lo) * (hi - old) : 1.0;
+    double v = fma(d, m, old);
+    v = (hi < v) ? hi : v;  // std::min(v, upper)
+    v = (lo < v) ? v : lo;  // std::max(lower, .)
+    return round_f32(v);
+}
+
+constexpr int kAhead = 8;  // winners whose loads are in flight
+
+// The weight's chain over the n compacted winners of this tile; with one
+// STDP config (the common case) its constants stay in registers.
+template <bool F32_RULE, bool ONE>
+__device__ __forceinline__ double stdp_chain(double w, int n, int64_t e, bool act, const int64_t *s_off,
+                                             const uint16_t *s_post, const uint8_t *s_cfg,
+                                             const uint16_t *__restrict__ pre, const double *s_pos,
+                                             const double *s_neg, const double *s_lo, const double *s_hi,
+                                             const int *s_stab)
+{
+    const double pos0 = s_pos[0], neg0 = s_neg[0], lo0 = s_lo[0], hi0 = s_hi[0];
+    const bool stab0 = s_stab[0] != 0;
+    uint16_t pv[kAhead];
+#pragma unroll
+    for (int u = 0; u < kAhead; ++u) pv[u] = (act && u < n) ? pre[s_off[u] + e] : 0;
+    for (int i0 = 0; i0 < n; i0 += kAhead)
+    {
+        uint16_t cv[kAhead];
+#pragma unroll
+        for (int u = 0; u < kAhead; ++u)
+        {
+            cv[u] = pv[u];
+            const int i = i0 + kAhead + u;
+            pv[u] = (act && i < n) ? pre[s_off[i] + e] : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < kAhead; ++u)
+        {
+            const int i = i0 + u;
+            if (i < n)
+            {
+                const bool direct = cv[u] <= s_post[i];
+                if (ONE)
+                    w = stdp_update<F32_RULE>(w, direct ? pos0 : neg0, lo0, hi0, stab0);
+                else
+                {
+                    const int c = s_cfg[i];
+                    w = stdp_update<F32_RULE>(w, direct ? s_pos[c] : s_neg[c], s_lo[c], s_hi[c], s_stab[c] != 0);
+                }
+            }
+        }
+    }
+    return w;
+}
+
 template <bool F32_RULE>
 __global__ void __launch_bounds__(kScanThreads)
     stdp_scan_kernel(float *__restrict__ kernel, int64_t k, int64_t b, int count, int field,
@@ -193,113 +275,86 @@ __global__ void __launch_bounds__(kScanThreads)
                      const uint16_t *__restrict__ pre, int64_t ps, int64_t pw, const uint16_t *__restrict__ post,
                      Configs cfg)
 {
-    __shared__ int32_t s_rec[kWinnerTile][3];  // (config, sample, slot) of matching winners
-    __shared__ uint16_t s_pre[kPreBatch][kScanChunk];
-    __shared__ uint16_t s_post[kPreBatch];
-    __shared__ int s_n;
+    // per compacted winner: offset of its pre row, its post time, its config
+    __shared__ int64_t s_off[kWinnerTile];
+    __shared__ uint16_t s_post[kWinnerTile];
+    __shared__ uint8_t s_cfg[kWinnerTile];
+    __shared__ int s_warp[kScanThreads / 32];
+    __shared__ double s_pos[kMaxConfigs], s_neg[kMaxConfigs], s_lo[kMaxConfigs], s_hi[kMaxConfigs];
+    __shared__ int s_stab[kMaxConfigs];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid < cfg.n)
+        s_pos[tid] = cfg.pos[tid], s_neg[tid] = cfg.neg[tid], s_lo[tid] = cfg.lo[tid], s_hi[tid] = cfg.hi[tid],
+        s_stab[tid] = cfg.stab[tid];
     const int map = blockIdx.x;
-    const int64_t base = int64_t(blockIdx.y) * kScanChunk;
-    float wv[kScanPerThread];
-    int64_t idx[kScanPerThread];
-#pragma unroll
-    for (int q = 0; q < kScanPerThread; ++q)
-    {
-        idx[q] = base + threadIdx.x + int64_t(q) * kScanThreads;
-        wv[q] = idx[q] < k ? kernel[int64_t(map) * k + idx[q]] : 0.f;
-    }
+    const int64_t e = int64_t(blockIdx.y) * kScanThreads + tid;
+    const bool act = e < k;
+    // warps whose weights are all past k only help with the compaction
+    const bool warp_act = int64_t(blockIdx.y) * kScanThreads + warp * 32 < k;
+    double w = act ? double(kernel[int64_t(map) * k + e]) : 0.0;
     const int64_t total = b * count;
+    constexpr int per = kWinnerTile / kScanThreads;
     for (int64_t start = 0; start < total; start += kWinnerTile)
     {
-        if (threadIdx.x == 0) s_n = 0;
-        __syncthreads();
-        // Compact the matching winners of this tile, preserving order.
-        const int64_t end = min(total, start + kWinnerTile);
-        for (int64_t r0 = start; r0 < end; r0 += blockDim.x)
+        // records start + 4 tid .. + 3: ordered compaction of this map's ones
+        unsigned m4 = 0;
+        int32_t rr[per];
+        uint8_t c4[per];
+#pragma unroll
+        for (int q = 0; q < per; ++q)
         {
-            int64_t r = r0 + threadIdx.x;
-            bool m = false;
-            int32_t c = 0;
-            if (r < end)
+            const int64_t r = start + int64_t(tid) * per + q;
+            c4[q] = 0, rr[q] = int32_t(r);
+            if (r < total)
             {
-                int64_t s = r / count, j = r % count;
-                if (j < counts[s])
+                const int smp = int(r) / count, j = int(r) - smp * count;  // r < 2^31
+                if (j < counts[smp])
                 {
-                    const int32_t *e = winners + r * 5;
-                    c = e[0];
-                    m = (e[field] == map) && c >= 0 && c < cfg.n;
+                    const int32_t *rec = winners + r * 5;
+                    const int32_t c = rec[0];
+                    if (rec[field] == map && c >= 0 && c < cfg.n) m4 |= 1u << q, c4[q] = uint8_t(c);
                 }
             }
-            unsigned bal = __ballot_sync(0xffffffffu, m);
-            // Order-preserving slot: block-wide prefix over warps.
-            __shared__ int s_warp[kScanThreads / 32];
-            const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-            if (lane == 0) s_warp[warp] = __popc(bal);
-            __syncthreads();
-            int before = 0;
-            for (int q = 0; q < warp; ++q) before += s_warp[q];
-            int total_here = 0;
-            for (int q = 0; q < kScanThreads / 32; ++q) total_here += s_warp[q];
-            if (m)
-            {
-                int slot = s_n + before + __popc(bal & ((1u << lane) - 1));
-                s_rec[slot][0] = c, s_rec[slot][1] = int32_t(r / count), s_rec[slot][2] = int32_t(r % count);
-            }
-            __syncthreads();
-            if (threadIdx.x == 0) s_n += total_here;
-            __syncthreads();
         }
-        const int n = s_n;
-        // Matching winners in batches: their pre rows (this CTA's chunk) are
-        // staged in shared memory with coalesced loads, then applied in order.
-        for (int q0 = 0; q0 < n; q0 += kPreBatch)
+        int x = __popc(m4);
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1)
         {
-            const int nb = min(kPreBatch, n - q0);
-            const int len = (k - base < int64_t(kScanChunk)) ? int(k - base) : kScanChunk;
-            for (int i = threadIdx.x; i < nb * len; i += blockDim.x)
-            {
-                const int q = i / len, e = i % len;
-                const int64_t s = s_rec[q0 + q][1], j = s_rec[q0 + q][2];
-                s_pre[q][e] = pre[s * ps + j * pw + base + e];
-                if (e == 0) s_post[q] = post[s * count + j];
-            }
-            __syncthreads();
-            for (int q = 0; q < nb; ++q)
-            {
-                const int c = s_rec[q0 + q][0];
-                const uint16_t po = s_post[q];
-                const double pos = cfg.pos[c], neg = cfg.neg[c], lo = cfg.lo[c], hi = cfg.hi[c];
-                const bool stab = cfg.stab[c] != 0;
-#pragma unroll
-                for (int u = 0; u < kScanPerThread; ++u)
-                    if (idx[u] < k)
-                    {
-                        const double old = double(wv[u]);
-                        const double d = s_pre[q][idx[u] - base] <= po ? pos : neg;
-                        if (F32_RULE)
-                        {
-                            const float m = __double2float_rn(stab ? (old - lo) * (hi - old) : 1.0);
-                            double v = double(__double2float_rn(fma(d, double(m), old)));
-                            v = (hi < v) ? hi : v;
-                            v = (lo < v) ? v : lo;
-                            wv[u] = __double2float_rn(v);
-                        }
-                        else
-                        {
-                            const double m = stab ? (old - lo) * (hi - old) : 1.0;
-                            double v = fma(d, m, old);
-                            v = (hi < v) ? hi : v;  // std::min(v, upper)
-                            v = (lo < v) ? v : lo;  // std::max(lower, .)
-                            wv[u] = __double2float_rn(v);
-                        }
-                    }
-            }
-            __syncthreads();
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
         }
-        __syncthreads();  // everyone has read s_n before it is reset
-    }
+        if (lane == 31) s_warp[warp] = x;
+        __syncthreads();
+        int before = x - __popc(m4), n = 0;
 #pragma unroll
-    for (int q = 0; q < kScanPerThread; ++q)
-        if (idx[q] < k) kernel[int64_t(map) * k + idx[q]] = wv[q];
+        for (int q = 0; q < kScanThreads / 32; ++q)
+        {
+            before += q < warp ? s_warp[q] : 0;
+            n += s_warp[q];
+        }
+#pragma unroll
+        for (int q = 0; q < per; ++q)
+            if (m4 & (1u << q))
+            {
+                const int r = rr[q], smp = r / count, j = r - smp * count;
+                s_off[before] = int64_t(smp) * ps + int64_t(j) * pw;
+                s_post[before] = post[r];
+                s_cfg[before] = c4[q];
+                ++before;
+            }
+        __syncthreads();
+        if (warp_act)
+        {
+            if (cfg.n == 1)
+                w = stdp_chain<F32_RULE, true>(w, n, e, act, s_off, s_post, s_cfg, pre, s_pos, s_neg, s_lo, s_hi,
+                                               s_stab);
+            else
+                w = stdp_chain<F32_RULE, false>(w, n, e, act, s_off, s_post, s_cfg, pre, s_pos, s_neg, s_lo, s_hi,
+                                                s_stab);
+        }
+        __syncthreads();  // the per-winner arrays are rewritten by the next tile
+    }
+    if (act) kernel[int64_t(map) * k + e] = float(w);  // exact: w holds an F32 value
 }
 
 Configs make_configs(const double *c, int64_t n)
@@ -326,7 +381,8 @@ void launch_stdp_scan(float *kernel, int64_t k, int64_t nmaps, int64_t b, int64_
                       const uint16_t *post, const double *configs, int64_t nconf, bool f32_rule, cudaStream_t s)
 {
     Configs cfg = make_configs(configs, nconf);
-    dim3 grid(unsigned(nmaps), unsigned(ceil_div(k, kScanChunk)));
+    SPK_REQUIRE(b * count < (int64_t(1) << 31), "at most 2^31 - 1 winner records");
+    dim3 grid(unsigned(nmaps), unsigned(ceil_div(k, kScanThreads)));
     if (f32_rule)
         stdp_scan_kernel<true><<<grid, kScanThreads, 0, s>>>(kernel, k, b, int(count), field, winners, counts, pre, ps,
                                                             pw, post, cfg);
@@ -352,7 +408,7 @@ void convstdp_into(const void *in, spk_dtype itype, int64_t b, int64_t t, int64_
     Pad4 p = pad_of(pad4);
     Configs cfg = make_configs(configs, nconf);
     SPK_REQUIRE(b >= 0 && t >= 1 && t < 65535 && cin >= 1 && cout >= 1 && kh >= 1 && kw >= 1, "invalid dims");
-    SPK_REQUIRE(count >= 1, "winner count must be positive");
+    SPK_REQUIRE(count >= 1 && b * count < (int64_t(1) << 31), "winner count must be positive (at most 2^31 - 1 records)");
     SPK_REQUIRE(oh == (h + p.top + p.bottom - kh) / sy + 1 && ow == (w + p.left + p.right - kw) / sx + 1,
                 "tensor shapes are not compatible");
     if (b == 0) return;
@@ -370,7 +426,7 @@ void convstdp_into(const void *in, spk_dtype itype, int64_t b, int64_t t, int64_
     else
         throw Error(SPK_ERR_UNSUPPORTED, "STDP spikes must be U8 or F32");
     SPK_LAUNCHED();
-    dim3 grid(unsigned(cout), unsigned(ceil_div(k, kScanChunk)));
+    dim3 grid(unsigned(cout), unsigned(ceil_div(k, kScanThreads)));
     stdp_scan_kernel<false><<<grid, kScanThreads, 0, s>>>(kernel, k, b, int(count), 2, winners, counts, pre, count * k, k,
                                                    post, cfg);
     SPK_LAUNCHED();
@@ -397,7 +453,7 @@ spk_status spk_rank_convstdp(const void *in, spk_dtype itype, int64_t b, int64_t
         Pad4 p = pad_of(pad4);
         Configs cfg = make_configs(configs, nconf);
         SPK_REQUIRE(b >= 0 && t >= 1 && t < 65535 && cin >= 1 && cout >= 1 && kh >= 1 && kw >= 1, "invalid dims");
-        SPK_REQUIRE(count >= 1, "winner count must be positive");
+        SPK_REQUIRE(count >= 1 && b * count < (int64_t(1) << 31), "winner count must be positive (at most 2^31 - 1 records)");
         SPK_REQUIRE(oh == (h + p.top + p.bottom - kh) / sy + 1 && ow == (w + p.left + p.right - kw) / sx + 1,
                     "tensor shapes are not compatible");
         if (b == 0) return;
@@ -429,7 +485,7 @@ spk_status spk_rank_convstdp(const void *in, spk_dtype itype, int64_t b, int64_t
         else
             throw Error(SPK_ERR_UNSUPPORTED, "STDP spikes must be U8 or F32");
         SPK_LAUNCHED();
-        dim3 grid(unsigned(cout), unsigned(ceil_div(k, kScanChunk)));
+        dim3 grid(unsigned(cout), unsigned(ceil_div(k, kScanThreads)));
         stdp_scan_kernel<false><<<grid, kScanThreads, 0, s>>>(kernel, k, b, int(count), 2, winners, counts, pre, count * k, k,
                                                        post, cfg);
         SPK_LAUNCHED();
@@ -466,7 +522,7 @@ spk_status spk_rank_fcstdp(const void *in, spk_dtype itype, int64_t b, int64_t t
         else
             throw Error(SPK_ERR_UNSUPPORTED, "STDP spikes must be U8 or F32");
         SPK_LAUNCHED();
-        dim3 grid(unsigned(no), unsigned(ceil_div(ni, kScanChunk)));
+        dim3 grid(unsigned(no), unsigned(ceil_div(ni, kScanThreads)));
         stdp_scan_kernel<false><<<grid, kScanThreads, 0, s>>>(kernel, ni, b, int(count), 4, winners, counts, pre, ni, 0, post,
                                                        cfg);
         SPK_LAUNCHED();
