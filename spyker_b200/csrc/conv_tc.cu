@@ -526,6 +526,15 @@ struct FusedPixel
     int iy0, ix0;
 };
 
+// Table slot of K element (kb, kc, i) of the fused producers: the 8 lanes of
+// a quarter warp read chunks kc = 0..7 of the same K block at once, so the
+// chunks of a block sit in 8 different 16-byte bank groups (kc * (8 kblocks
+// + 1) is kc mod 8).
+__device__ __forceinline__ int ftab(int kblocks, int kb, int kc, int i)
+{
+    return kc * (8 * kblocks + 1) + i * kblocks + kb;
+}
+
 __device__ __forceinline__ FusedPixel fused_pixel(const TcParams &P, int64_t mt, int pl)
 {
     FusedPixel u{};
@@ -548,7 +557,7 @@ __device__ __forceinline__ uint2 fst_chunk(const TcParams &P, const int4 *tab, c
     const uint8_t *base = P.in + u.sample * P.img_stride;
     if (P.nhwc)
     {
-        const int4 e = tab[kb * BK + kc * 8];
+        const int4 e = tab[ftab(P.kblocks, kb, kc, 0)];
         const int iy = u.iy0 + e.y, ix = u.ix0 + e.z;
         if (e.w && iy >= 0 && iy < P.h && ix >= 0 && ix < P.w)
             return *reinterpret_cast<const uint2 *>(base + (int64_t(iy) * P.w + ix) * P.cpad + e.x);
@@ -558,7 +567,7 @@ __device__ __forceinline__ uint2 fst_chunk(const TcParams &P, const int4 *tab, c
 #pragma unroll
     for (int i = 0; i < 8; ++i)
     {
-        const int4 e = tab[kb * BK + kc * 8 + i];
+        const int4 e = tab[ftab(P.kblocks, kb, kc, i)];
         const int iy = u.iy0 + e.y, ix = u.ix0 + e.z;
         uint32_t b = 0xFF;
         if (e.w && iy >= 0 && iy < P.h && ix >= 0 && ix < P.w) b = base[(int64_t(iy) * P.w + ix) * P.cin + e.x];
@@ -607,7 +616,7 @@ __device__ __forceinline__ void store_raw_rows(const TcParams &P, const int4 *ta
             const uint8_t *base = P.raw + (u.sample * P.T + t) * int64_t(P.cin) * P.h * P.w;
             for (int e8 = 0; e8 < 8; ++e8)
             {
-                const int4 e = tab[kb * BK + kc * 8 + e8];
+                const int4 e = tab[ftab(P.kblocks, kb, kc, e8)];
                 const int iy = u.iy0 + e.y, ix = u.ix0 + e.z;
                 uint32_t b = 0;
                 if (e.w && iy >= 0 && iy < P.h && ix >= 0 && ix < P.w)
@@ -719,7 +728,8 @@ __global__ void __launch_bounds__(kWsThreads, 1) conv_ws_kernel(TcParams P)
                 tap = k / P.cpad, c = k % P.cpad;
             else
                 c = k / taps, tap = k % taps;
-            tab[k] = make_int4(c, tap / P.kw, tap % P.kw, (tap < taps && c < P.cin) ? 1 : 0);
+            tab[ftab(P.kblocks, k / BK, (k / 8) % 8, k % 8)] =
+                make_int4(c, tap / P.kw, tap % P.kw, (tap < taps && c < P.cin) ? 1 : 0);
         }
     }
     else if (P.nhwc)
@@ -1029,7 +1039,9 @@ Plan make_plan(int64_t n, int64_t cin, int64_t h, int64_t w, int64_t cout, int64
         pl.xt_bytes = align256(size_t(n / t_fused) * h * w * (pl.nhwc ? pl.cpad : cin)) + 256;
     else
         pl.xt_bytes = pl.nhwc ? size_t(n) * h * w * pl.cpad : 0;
-    const size_t tab = (t_fused > 0 || !pl.nhwc) ? size_t(pl.kblocks) * BK * 16 : size_t(pl.kblocks) * 8 * 16;
+    const size_t tab = t_fused > 0  ? (size_t(pl.kblocks) * BK + 8) * 16
+                       : !pl.nhwc   ? size_t(pl.kblocks) * BK * 16
+                                    : size_t(pl.kblocks) * 8 * 16;
     const size_t stage = size_t(BM * BK * 2) + size_t(pl.nsplit) * pl.n_tile * BK * 2;
     const size_t budget = 225 * 1024 - tab;
     pl.stages = int(std::min<size_t>(4, budget / stage));
