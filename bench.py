@@ -32,6 +32,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 BATCH, T, H = 4096, 15, 28
+# DRAM bytes (read + write) of one conv2 launch of the fused layer kernel,
+# from an ncu capture of the 256-image case scaled by 16 (the kernel's traffic
+# grows with the batch): profiles/conv_ws_fused_b256_bf16x3.md.
+CONV2_TRAFFIC_BYTES = int((3.428352 + 1.160448) * 1e6 * 16)
 METRIC = "images/s (STDP train + fwd), BF16-split vs FP32 on 1 B200; spike match %"
 WORKLOAD = "kheradpisheh-2layer-stdp: 4096 x 28x28 strokes, T=15, conv1 30x5x5 th15 r3k5, conv2 100x5x5 th10 r1k8"
 
@@ -240,7 +244,9 @@ def gpu_arm(args, rank, world):
                 "d2h_bytes_per_step": int(feats.numel() * feats.element_size())},
         "gpu_launches": int(launches),
         "roofline": {"bound": "tensor", "kernel": "conv2 (30->100, 5x5, M=12.0M, K=750)", "achieved": achieved,
-                     "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                     "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                     "traffic": CONV2_TRAFFIC_BYTES * BATCH // 4096 if args.precision != "fp32" else None,
+                     "traffic_source": "ncu dram__bytes_read+write of the 256-image capture, scaled",
                      "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained (of measured)"},
         "kernels_ms": {"conv1": c1_ms, "conv2": c2_ms, "rest": ms - c1_ms - c2_ms},
         "clocks": clk.summary(),
