@@ -32,9 +32,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 BATCH, T, H = 4096, 15, 28
-# DRAM bytes (read + write) of one conv2 launch of the fused layer kernel,
-# from an ncu capture of the 256-image case scaled by 16 (the kernel's traffic
-# grows with the batch): profiles/conv_ws_fused_b256_bf16x3.md.
+# DRAM bytes (read + write) of one conv2 launch of the fused layer kernel:
+# ncu's dram__bytes_read.sum + dram__bytes_write.sum for the 256-image case
+# (--batch 256), scaled by 16 (the kernel's traffic grows with the batch).
 CONV2_TRAFFIC_BYTES = int((3.428352 + 1.160448) * 1e6 * 16)
 METRIC = "images/s (STDP train + fwd), BF16-split vs FP32 on 1 B200; spike match %"
 WORKLOAD = "kheradpisheh-2layer-stdp: 4096 x 28x28 strokes, T=15, conv1 30x5x5 th15 r3k5, conv2 100x5x5 th10 r1k8"
