@@ -175,6 +175,25 @@ spk_status spk_rank_convstdp_noalloc(const void *in, spk_dtype itype, int64_t b,
                                      int64_t oh, int64_t ow, const double *configs_host, int64_t nconf,
                                      const int32_t *winners, const int32_t *counts, int64_t count, int64_t sy,
                                      int64_t sx, const int64_t *pad4_host, spk_stream stream);
+/* The two halves of spk_rank_convstdp (cpu/stdp.cpp:99-169), for STDP over
+ * winners gathered from several GPUs: spk_rank_convstdp_prepost writes, for
+ * every winner slot, the first-spike times of its receptive field
+ * pre [B, count, Cin*KH*KW] u16 (T = silent or padding) and of the winner
+ * post [B, count] u16; spk_stdp_scan applies the reference's ordered update
+ * (sample after sample, slot after slot) to a kernel from such arrays.  The
+ * map of a winner is record field `field` (2 = z for conv, 4 = x for fc);
+ * pre of slot (s, j) starts at s * pre_sample_stride + j * pre_slot_stride.
+ * f32_rule != 0 takes the event-list update of sparse/stdp.cpp:95-97. */
+size_t spk_rank_convstdp_prepost_workspace(int64_t b, int64_t cin, int64_t h, int64_t w);
+spk_status spk_rank_convstdp_prepost(const void *in, spk_dtype itype, int64_t b, int64_t t, int64_t cin, int64_t h,
+                                     int64_t w, int64_t cout, int64_t kh, int64_t kw, const void *out, int64_t oh,
+                                     int64_t ow, const int32_t *winners, const int32_t *counts, int64_t count,
+                                     int64_t sy, int64_t sx, const int64_t *pad4_host, uint16_t *pre, uint16_t *post,
+                                     void *ws, size_t ws_bytes, spk_stream stream);
+spk_status spk_stdp_scan(float *kernel, int64_t nmaps, int64_t k, int64_t b, int64_t count, int64_t field,
+                         const int32_t *winners, const int32_t *counts, const uint16_t *pre, int64_t pre_sample_stride,
+                         int64_t pre_slot_stride, const uint16_t *post, const double *configs_host, int64_t nconf,
+                         int f32_rule, spk_stream stream);
 size_t spk_rank_fcstdp_workspace(int64_t b, int64_t t, int64_t ni);
 /* in [B, T, I], kernel [O, I] F32 in place, out [B, T, O] (cpu/stdp.cpp:42-97). */
 spk_status spk_rank_fcstdp(const void *in, spk_dtype itype, int64_t b, int64_t t, int64_t ni, float *kernel,

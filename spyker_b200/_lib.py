@@ -48,6 +48,10 @@ SIGNATURES = {
                                  _I, _I, _P, _P, _S, _P]),
     "spk_rank_convstdp_noalloc": (_INT, [_P, _INT, _I, _I, _I, _I, _I, _P, _I, _I, _I, _P, _I, _I, _P, _I, _P, _P,
                                          _I, _I, _I, _P, _P]),
+    "spk_rank_convstdp_prepost_workspace": (_S, [_I, _I, _I, _I]),
+    "spk_rank_convstdp_prepost": (_INT, [_P, _INT, _I, _I, _I, _I, _I, _I, _I, _I, _P, _I, _I, _P, _P, _I, _I, _I, _P,
+                                         _P, _P, _P, _S, _P]),
+    "spk_stdp_scan": (_INT, [_P, _I, _I, _I, _I, _I, _P, _P, _P, _I, _I, _P, _P, _I, _INT, _P]),
     "spk_rank_fcstdp_workspace": (_S, [_I, _I, _I]),
     "spk_rank_fcstdp": (_INT, [_P, _INT, _I, _I, _I, _P, _I, _P, _P, _I, _P, _P, _I, _P, _S, _P]),
     "spk_conv_workspace": (_S, [_I, _I, _I, _I, _I, _I, _I, _INT]),

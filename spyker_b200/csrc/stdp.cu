@@ -392,6 +392,35 @@ void launch_stdp_scan(float *kernel, int64_t k, int64_t nmaps, int64_t b, int64_
     SPK_LAUNCHED();
 }
 
+// (pre, post) times of every conv winner: the first-spike map of the input
+// (fst, [B, Cin, H, W] u16), then each winner's receptive field.
+void conv_prepost(const void *in, spk_dtype itype, int64_t b, int64_t t, int64_t cin, int64_t h, int64_t w,
+                  int64_t cout, int64_t kh, int64_t kw, const void *out, int64_t oh, int64_t ow,
+                  const int32_t *winners, const int32_t *counts, int64_t count, int64_t sy, int64_t sx, Pad4 p,
+                  uint16_t *fst, uint16_t *pre, uint16_t *post, cudaStream_t s)
+{
+    auto prep = [&](auto z) {
+        using T = decltype(z);
+        const int64_t x = cin * h * w;
+        if (sizeof(T) == 1 && x % 4 == 0 && reinterpret_cast<uintptr_t>(in) % 4 == 0)
+            first_spike_map_u8x4_kernel<<<grid_for(b * x / 4, 256, 16), 256, 0, s>>>(
+                (const uint32_t *)in, reinterpret_cast<uint2 *>(fst), b, int(t), x / 4);
+        else
+            first_spike_map_kernel<T><<<grid_for(b * x, 256, 16), 256, 0, s>>>((const T *)in, fst, b, int(t), x);
+        SPK_LAUNCHED();
+        conv_prepost_map_kernel<T><<<unsigned(b * count), 128, 0, s>>>(
+            fst, (const T *)out, int(t), int(cin), int(h), int(w), int(cout), int(oh), int(ow), int(kh), int(kw),
+            int(sy), int(sx), int(p.top), int(p.left), winners, counts, int(count), pre, post);
+        SPK_LAUNCHED();
+    };
+    if (itype == SPK_U8)
+        prep(uint8_t());
+    else if (itype == SPK_F32)
+        prep(float());
+    else
+        throw Error(SPK_ERR_UNSUPPORTED, "STDP spikes must be U8 or F32");
+}
+
 // Bytes of the (pre, post) first-spike scratch of conv STDP.
 size_t convstdp_prepost_bytes(int64_t b, int64_t count, int64_t cin, int64_t kh, int64_t kw)
 {
@@ -465,30 +494,53 @@ spk_status spk_rank_convstdp(const void *in, spk_dtype itype, int64_t b, int64_t
         cudaStream_t s = stream_of(stream);
         uint16_t *fst = reinterpret_cast<uint16_t *>(static_cast<char *>(ws) +
                                                      convstdp_prepost_bytes(b, count, cin, kh, kw));
-        auto prep = [&](auto z) {
-            using T = decltype(z);
-            const int64_t x = cin * h * w;
-            if (sizeof(T) == 1 && x % 4 == 0 && reinterpret_cast<uintptr_t>(in) % 4 == 0)
-                first_spike_map_u8x4_kernel<<<grid_for(b * x / 4, 256, 16), 256, 0, s>>>(
-                    (const uint32_t *)in, reinterpret_cast<uint2 *>(fst), b, int(t), x / 4);
-            else
-                first_spike_map_kernel<T><<<grid_for(b * x, 256, 16), 256, 0, s>>>((const T *)in, fst, b, int(t), x);
-            SPK_LAUNCHED();
-            conv_prepost_map_kernel<T><<<unsigned(b * count), 128, 0, s>>>(
-                fst, (const T *)out, int(t), int(cin), int(h), int(w), int(cout), int(oh), int(ow), int(kh), int(kw),
-                int(sy), int(sx), int(p.top), int(p.left), winners, counts, int(count), pre, post);
-        };
-        if (itype == SPK_U8)
-            prep(uint8_t());
-        else if (itype == SPK_F32)
-            prep(float());
-        else
-            throw Error(SPK_ERR_UNSUPPORTED, "STDP spikes must be U8 or F32");
-        SPK_LAUNCHED();
+        conv_prepost(in, itype, b, t, cin, h, w, cout, kh, kw, out, oh, ow, winners, counts, count, sy, sx, p, fst,
+                     pre, post, s);
         dim3 grid(unsigned(cout), unsigned(ceil_div(k, kScanThreads)));
         stdp_scan_kernel<false><<<grid, kScanThreads, 0, s>>>(kernel, k, b, int(count), 2, winners, counts, pre, count * k, k,
                                                        post, cfg);
         SPK_LAUNCHED();
+    });
+}
+
+size_t spk_rank_convstdp_prepost_workspace(int64_t b, int64_t cin, int64_t h, int64_t w)
+{
+    return align256(size_t(b * cin * h * w) * 2);
+}
+
+spk_status spk_rank_convstdp_prepost(const void *in, spk_dtype itype, int64_t b, int64_t t, int64_t cin, int64_t h,
+                                     int64_t w, int64_t cout, int64_t kh, int64_t kw, const void *out, int64_t oh,
+                                     int64_t ow, const int32_t *winners, const int32_t *counts, int64_t count,
+                                     int64_t sy, int64_t sx, const int64_t *pad4_host, uint16_t *pre, uint16_t *post,
+                                     void *ws, size_t ws_bytes, spk_stream stream)
+{
+    return guarded([&] {
+        Pad4 p = pad_of(pad4_host);
+        SPK_REQUIRE(b >= 0 && t >= 1 && t < 65535 && cin >= 1 && cout >= 1 && kh >= 1 && kw >= 1, "invalid dims");
+        SPK_REQUIRE(count >= 1, "winner count must be positive");
+        SPK_REQUIRE(oh == (h + p.top + p.bottom - kh) / sy + 1 && ow == (w + p.left + p.right - kw) / sx + 1,
+                    "tensor shapes are not compatible");
+        SPK_REQUIRE(pre != nullptr && post != nullptr, "null output");
+        if (b == 0) return;
+        SPK_REQUIRE(ws != nullptr && ws_bytes >= spk_rank_convstdp_prepost_workspace(b, cin, h, w),
+                    "workspace is too small");
+        conv_prepost(in, itype, b, t, cin, h, w, cout, kh, kw, out, oh, ow, winners, counts, count, sy, sx, p,
+                     static_cast<uint16_t *>(ws), pre, post, stream_of(stream));
+    });
+}
+
+spk_status spk_stdp_scan(float *kernel, int64_t nmaps, int64_t k, int64_t b, int64_t count, int64_t field,
+                         const int32_t *winners, const int32_t *counts, const uint16_t *pre, int64_t pre_sample_stride,
+                         int64_t pre_slot_stride, const uint16_t *post, const double *configs_host, int64_t nconf,
+                         int f32_rule, spk_stream stream)
+{
+    return guarded([&] {
+        SPK_REQUIRE(nmaps >= 1 && k >= 1 && b >= 0 && count >= 1, "invalid dims");
+        SPK_REQUIRE(field == 2 || field == 4, "the map field is 2 (z, conv) or 4 (x, fc)");
+        SPK_REQUIRE(kernel && winners && counts && pre && post, "null pointer");
+        if (b == 0) return;
+        launch_stdp_scan(kernel, k, nmaps, b, count, int(field), winners, counts, pre, pre_sample_stride,
+                         pre_slot_stride, post, configs_host, nconf, f32_rule != 0, stream_of(stream));
     });
 }
 
