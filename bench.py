@@ -135,6 +135,7 @@ class Network:
         pooled = sp.pool(spk1, 2)
         spk2, win2 = self._layer(self.conv2, pooled, 10.0, 1, 8)
         self.conv2.stdp(pooled, win2, spk2)
+        self.last_spikes = (spk1, spk2)
         return sp.pool(spk2, 14)
 
 
@@ -169,6 +170,7 @@ def gpu_arm(args, rank, world):
     barrier()
     net.conv_events.clear()
     l0 = spyker._lib.lib.spk_launch_count()
+    spyker._lib.lib.spk_recheck_count(1)
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with Clocks(dev.index) as clk:
         barrier()
@@ -178,7 +180,10 @@ def gpu_arm(args, rank, world):
         end.record()
         barrier()
     launches = (spyker._lib.lib.spk_launch_count() - l0) // max(args.steps, 1)
+    rechecks = spyker._lib.lib.spk_recheck_count(1) / max(args.steps, 1)
     ms = start.elapsed_time(end) / args.steps
+    # fired neurons of one step: a cumulative spike tensor's last step
+    spikes_per_step = sum(int(s[:, -1].sum().item()) for s in net.last_spikes)
     conv_ms = {}
     for a, b, layer in net.conv_events:
         conv_ms.setdefault(id(layer), []).append(a.elapsed_time(b))
@@ -250,6 +255,8 @@ def gpu_arm(args, rank, world):
                      "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained (of measured)"},
         "kernels_ms": {"conv1": c1_ms, "conv2": c2_ms, "rest": ms - c1_ms - c2_ms},
         "clocks": clk.summary(),
+        "spikes_per_s": spikes_per_step * world / (ms * 1e-3),
+        "near_threshold_rechecks_per_step": rechecks,
     }
     if fp32 is not None:
         line["fp32_path"] = fp32

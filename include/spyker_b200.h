@@ -81,6 +81,10 @@ uint64_t spk_launch_count(void);
 /* Device status word of the tensor-core kernels: 0 = no error, 1 = a bounded
  * wait timed out.  Synchronous; reset != 0 clears it. */
 int spk_device_status(int reset);
+/* Number of (pixel, step) rows of the fused layer whose thresholded
+ * channel decision was within the FP32 error bound and was recomputed with
+ * FP64 sums, since the last reset.  Synchronous; reset != 0 clears it. */
+unsigned long long spk_recheck_count(int reset);
 
 /* ---- host-side kernel generation (src/spyker/cpu/init.cpp) -------------- */
 /* Global generator: replaces Core::random_seed (src/spyker/impl.cpp:37-43). */

@@ -37,6 +37,9 @@
 namespace spk
 {
 static __device__ int g_tc_status;
+// Rows (one pixel at one step) whose channel decision the FP32 bound could
+// not certify and that were recomputed with FP64 sums.
+static __device__ unsigned long long g_rechecks;
 
 namespace
 {
@@ -330,8 +333,10 @@ __device__ __forceinline__ void row_argmax(const TcParams &P, uint32_t lane_base
     if (real_wins) unsure |= __fsub_rn(st.r1, st.r2) <= 2.f * tol || fabsf(__fsub_rn(st.r1, P.inh_thr)) <= tol;
     am = real_wins ? st.a1 : st.b1;
     xam = real_wins ? st.r1 : P.thv;
-    if (__any_sync(0xffffffffu, unsure && row_ok))
+    const unsigned redo = __ballot_sync(0xffffffffu, unsure && row_ok);
+    if (redo)
     {
+        if ((threadIdx.x & 31) == 0) atomicAdd(&g_rechecks, (unsigned long long)__popc(redo));
         // exact pass: FP64 sums rounded once to F32 (warp-uniform tcgen05.ld)
         float mx = 0.f;
         int ae = 0;
@@ -1222,6 +1227,18 @@ void conv_tc(const void *in, spk_dtype itype, const float *kernel, float *out, i
 using namespace spk;
 
 extern "C" {
+
+unsigned long long spk_recheck_count(int reset)
+{
+    unsigned long long v = 0;
+    if (cudaMemcpyFromSymbol(&v, spk::g_rechecks, sizeof(v)) != cudaSuccess) return ~0ull;
+    if (reset)
+    {
+        unsigned long long z = 0;
+        if (cudaMemcpyToSymbol(spk::g_rechecks, &z, sizeof(z)) != cudaSuccess) return ~0ull;
+    }
+    return v;
+}
 
 int spk_device_status(int reset)
 {
