@@ -112,31 +112,31 @@ class Network:
         self.conv_events.append((a, b, layer))
         return y
 
-    def _layer(self, layer, x, theta, radius, count):
-        """conv -> threshold -> inhibit -> (fire, convwta): fused on the
-        tensor-core precisions, op by op on the FP32 path."""
+    def _layer(self, layer, x, theta, radius, count, pool):
+        """conv -> threshold -> inhibit -> (fire, convwta) -> pool: one fused
+        kernel on the tensor-core precisions, op by op on the FP32 path."""
         t = self.torch
         a, b = t.cuda.Event(enable_timing=True), t.cuda.Event(enable_timing=True)
         a.record()
         if layer.precision == "fp32":
             out = self.sp.inhibit(self.sp.threshold(layer(x), theta))
             spk, wins = self.sp.fire(out), self.sp.convwta(out, radius, count)
+            pooled = self.sp.pool(spk, pool)
         else:
-            spk, wins = self.sp.conv_fire_wta(x, layer, theta, radius, count)
+            spk, wins, pooled = self.sp.conv_fire_wta(x, layer, theta, radius, count, pool=pool)
         b.record()
         self.conv_events.append((a, b, layer))
-        return spk, wins
+        return spk, wins, pooled
 
     def step(self, images_f32):
         sp = self.sp
         codes = sp.code(self.dog(images_f32), T)
-        spk1, win1 = self._layer(self.conv1, codes, 15.0, 3, 5)
+        spk1, win1, pooled = self._layer(self.conv1, codes, 15.0, 3, 5, 2)
         self.conv1.stdp(codes, win1, spk1)
-        pooled = sp.pool(spk1, 2)
-        spk2, win2 = self._layer(self.conv2, pooled, 10.0, 1, 8)
+        spk2, win2, feats = self._layer(self.conv2, pooled, 10.0, 1, 8, 14)
         self.conv2.stdp(pooled, win2, spk2)
         self.last_spikes = (spk1, spk2)
-        return sp.pool(spk2, 14)
+        return feats
 
 
 def gpu_arm(args, rank, world):
@@ -244,7 +244,7 @@ def gpu_arm(args, rank, world):
         "dtype": {"fp32": "f32", "bf16x2": "bf16x2-split/f32-acc", "bf16x3": "bf16x3-split/f32-acc"}[args.precision],
         "data": "synthetic (seeded stroke images, MNIST geometry)",
         "config": {"workload": WORKLOAD.replace("4096 x", f"{BATCH} x"), "global_batch": BATCH * world, "seq_len": T, "parallelism": f"replicas{world}",
-                   "conv_precision": args.precision, "l2": "inputs larger than L2: each step streams its own 289 MB layer-1 spike tensor (126 MB L2)"},
+                   "conv_precision": args.precision, "l2": "inputs larger than L2: each step writes its own 1.44 GB layer-1 spike tensor (126 MB L2)"},
         "e2e": {"value": BATCH * world / (e2e_ms * 1e-3), "unit": "images/s", "h2d_bytes_per_step": BATCH * H * H,
                 "d2h_bytes_per_step": int(feats.numel() * feats.element_size())},
         "gpu_launches": int(launches),
@@ -282,8 +282,8 @@ def spike_match(spyker, torch, dev, precision, n=32):
     net = Network(spyker, torch, dev, precision)
     x = torch.from_numpy(imgs).to(dev).float().div_(255.0)[:, None]
     codes = spyker.code(net.dog(x), T)
-    s1, _ = net._layer(net.conv1, codes, 15.0, 3, 5)
-    s2, _ = net._layer(net.conv2, spyker.pool(s1, 2), 10.0, 1, 8)
+    s1, _, p1 = net._layer(net.conv1, codes, 15.0, 3, 5, 2)
+    s2, _, _ = net._layer(net.conv2, p1, 10.0, 1, 8, 14)
     g1, g2 = s1.cpu().numpy(), s2.cpu().numpy()
 
     ref_codes = o.rank_code(o.filter("dog", imgs.astype(np.float32)[:, None] / np.float32(255), dog_kernel(o),

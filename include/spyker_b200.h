@@ -224,15 +224,18 @@ spk_status spk_conv(const void *in, spk_dtype itype, const float *kernel, float 
  * fire(out, fire_threshold) and winners = convwta(out, (ry, rx), count,
  * wta_threshold) with out = inhibit(threshold(conv(in), threshold, value),
  * inhibit_threshold).  Requires T <= 32, Cout >= 2, fire/WTA thresholds >= 0
- * and a tensor-core precision. */
+ * and a tensor-core precision.  With pool_ky > 0 it also writes pooled =
+ * pool(spikes, (pool_ky, pool_kx)) (stride = window, no padding; the
+ * rank_pool of impl.h:268 on the spikes), [B, T, Cout, OH / pool_ky,
+ * OW / pool_kx] U8; pooled may be null when pool_ky == 0. */
 size_t spk_conv_fire_wta_workspace(int64_t b, int64_t t, int64_t cin, int64_t h, int64_t w, int64_t cout, int64_t kh,
                                    int64_t kw, int64_t sy, int64_t sx, const int64_t *pad4_host, int precision);
 spk_status spk_conv_fire_wta(const void *in, spk_dtype itype, const float *kernel, int64_t b, int64_t t, int64_t cin,
                              int64_t h, int64_t w, int64_t cout, int64_t kh, int64_t kw, int64_t sy, int64_t sx,
                              const int64_t *pad4_host, double threshold, double value, double inhibit_threshold,
                              double fire_threshold, int64_t ry, int64_t rx, int64_t count, double wta_threshold,
-                             uint8_t *spikes, int32_t *winners, int32_t *counts, int precision, void *ws,
-                             size_t ws_bytes, spk_stream stream);
+                             uint8_t *spikes, int32_t *winners, int32_t *counts, int64_t pool_ky, int64_t pool_kx,
+                             uint8_t *pooled, int precision, void *ws, size_t ws_bytes, spk_stream stream);
 
 /* ---- fully connected (Core::fc / signfc, impl.h:228-236) ---------------- */
 /* in [R, I] (U8 or F32), kernel [O, I] F32 -> out [R, O] F32. */

@@ -59,7 +59,7 @@ SIGNATURES = {
     "spk_conv": (_INT, [_P, _INT, _P, _P, _I, _I, _I, _I, _I, _I, _I, _I, _I, _P, _INT, _P, _S, _P]),
     "spk_conv_fire_wta_workspace": (_S, [_I, _I, _I, _I, _I, _I, _I, _I, _I, _I, _P, _INT]),
     "spk_conv_fire_wta": (_INT, [_P, _INT, _P, _I, _I, _I, _I, _I, _I, _I, _I, _I, _I, _P, _D, _D, _D, _D, _I, _I,
-                                 _I, _D, _P, _P, _P, _INT, _P, _S, _P]),
+                                 _I, _D, _P, _P, _P, _I, _I, _P, _INT, _P, _S, _P]),
     "spk_fc": (_INT, [_P, _INT, _P, _P, _I, _I, _I, _INT, _P]),
     "spk_filter": (_INT, [_INT, _P, _P, _P, _I, _I, _I, _I, _I, _I, _I, _I, _P, _P]),
     "spk_backward": (_INT, [_P, _P, _P, _I, _I, _I, _D, _P]),

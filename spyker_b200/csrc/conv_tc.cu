@@ -67,6 +67,8 @@ struct TcParams
     int64_t npix;
     float thr, thv, inh_thr, fire_thr, wta_thr;
     uint8_t *spikes;    // [B, T, Cout, OH, OW]
+    uint8_t *pooled;    // [B, T, Cout, POH, POW] or null: spikes pooled over pky x pkx windows
+    int pky, pkx, poh, pow_;
     int4 *records;      // [B * OH * OW]: (winning channel, first step, value bits, 0)
     unsigned *mins, *maxs;  // [B] order-preserving encodings
     // fused producers: `in` is the first-spike map [B, H, W, Cp]; when *flag
@@ -402,7 +404,19 @@ __device__ void fused_epilogue(const TcParams &P, uint32_t acc, bool row_ok, int
     const float raw = float(accv);
     const float vw = (raw <= P.thr) ? P.thv : raw;
     // spike of the winning channel (the spike tensor was zero-filled first)
-    if (row_ok && vw > P.fire_thr) P.spikes[((sample * T + tstep) * C + win) * P.ohw + pix] = 1;
+    if (row_ok && vw > P.fire_thr)
+    {
+        P.spikes[((sample * T + tstep) * C + win) * P.ohw + pix] = 1;
+        if (P.pooled)
+        {
+            // max of 0/1 spikes over the window: any spike marks the cell
+            // (several pixels may store the same 1)
+            const int oy = int(pix / P.ow), ox = int(pix - int64_t(oy) * P.ow);
+            const int py = oy / P.pky, px = ox / P.pkx;
+            if (py < P.poh && px < P.pow_)
+                P.pooled[((sample * T + tstep) * C + win) * int64_t(P.poh) * P.pow_ + py * P.pow_ + px] = 1;
+        }
+    }
     // WTA record: first step whose inhibited value exceeds wta_thr
     const unsigned keyed = __ballot_sync(0xffffffffu, row_ok && vw > P.wta_thr) & grp;
     const int first_lane = keyed ? __ffs(keyed) - 1 : base;
@@ -1269,8 +1283,8 @@ spk_status spk_conv_fire_wta(const void *in, spk_dtype itype, const float *kerne
                              int64_t h, int64_t w, int64_t cout, int64_t kh, int64_t kw, int64_t sy, int64_t sx,
                              const int64_t *pad4, double threshold, double value, double inhibit_threshold,
                              double fire_threshold, int64_t ry, int64_t rx, int64_t count, double wta_threshold,
-                             uint8_t *spikes, int32_t *winners, int32_t *counts, int precision, void *ws,
-                             size_t ws_bytes, spk_stream stream)
+                             uint8_t *spikes, int32_t *winners, int32_t *counts, int64_t pool_ky, int64_t pool_kx,
+                             uint8_t *pooled, int precision, void *ws, size_t ws_bytes, spk_stream stream)
 {
     return guarded([&] {
         Pad4 p = pad_of(pad4);
@@ -1297,12 +1311,21 @@ spk_status spk_conv_fire_wta(const void *in, spk_dtype itype, const float *kerne
         P.thr = float(threshold), P.thv = float(value), P.inh_thr = float(inhibit_threshold);
         P.fire_thr = float(fire_threshold), P.wta_thr = float(wta_threshold);
         P.spikes = spikes;
+        int64_t poh = 0, pow_ = 0;
+        if (pool_ky > 0)
+        {
+            SPK_REQUIRE(pool_kx > 0 && pooled != nullptr, "pooling needs a window and an output");
+            poh = (L.oh - pool_ky) / pool_ky + 1, pow_ = (L.ow - pool_kx) / pool_kx + 1;
+            SPK_REQUIRE(L.oh >= pool_ky && L.ow >= pool_kx, "the pooling window is larger than the output");
+            P.pooled = pooled, P.pky = int(pool_ky), P.pkx = int(pool_kx), P.poh = int(poh), P.pow_ = int(pow_);
+        }
         P.records = reinterpret_cast<int4 *>(base + L.rec_off);
         P.mins = reinterpret_cast<unsigned *>(base + L.min_off);
         P.maxs = reinterpret_cast<unsigned *>(base + L.max_off);
         P.M = L.npix * (int64_t(1) << L.tp_log2);
         P.tiles = ceil_div(L.npix, L.pp);
         SPK_CUDA(cudaMemsetAsync(spikes, 0, size_t(b) * t * cout * L.oh * L.ow, s));
+        if (pool_ky > 0) SPK_CUDA(cudaMemsetAsync(pooled, 0, size_t(b) * t * cout * poh * pow_, s));
         SPK_CUDA(cudaMemsetAsync(P.mins, 0xFF, size_t(b) * 4, s));
         SPK_CUDA(cudaMemsetAsync(P.maxs, 0x00, size_t(b) * 4, s));
         launch<kFused>(P, L.pl, s);

@@ -410,6 +410,9 @@ def pool(array, kernel, stride=None, pad=0, rates=None):
     return a.back(out)
 
 
+_pool_op = pool
+
+
 def inhibit(array, threshold: float = 0.0, inplace: bool = True):
     if not inplace:
         array = clone_array(array)
@@ -574,11 +577,15 @@ class FC:
 
 def conv_fire_wta(array, conv: "Conv", threshold: float, radius, count: int, value: float = 0.0,
                   inhibit_threshold: float = 0.0, fire_threshold: float = 0.0, wta_threshold: float = 0.0,
-                  precision: str | None = None):
+                  precision: str | None = None, pool=None):
     """One fused layer step; returns ``(spikes, winners)`` equal to::
 
         out = inhibit(threshold(conv(array), threshold, value), inhibit_threshold)
         spikes, winners = fire(out, fire_threshold), convwta(out, radius, count, wta_threshold)
+
+    With ``pool`` (a window, stride = window, no padding) it returns
+    ``(spikes, winners, pool(spikes, pool))``, the pooled spikes written by the
+    same kernel.
 
     On the tensor-core precisions with u8 spikes, T <= 32, at least two output
     channels and non-negative fire/WTA thresholds, a single tcgen05 kernel does
@@ -598,18 +605,26 @@ def conv_fire_wta(array, conv: "Conv", threshold: float, radius, count: int, val
         nb = _lib.lib.spk_conv_fire_wta_workspace(s[0], s[1], cin, s[3], s[4], cout, kh, kw, conv._stride[0],
                                                   conv._stride[1], i64(*conv._pad), _PRECISION[prec])
         fused = nb > 0 and s[1] * cout * (128 // (1 << (s[1] - 1).bit_length())) <= 32768
+    p2 = expand2(pool) if pool is not None else None
+    if p2 is not None and min(p2) < 1:
+        raise ValueError("Kernel, stride or pad items are incorrect.")
     if not fused:
         out = inhibit(_threshold_op(conv_(x, conv, prec), threshold, value), inhibit_threshold)
-        return fire(out, fire_threshold), convwta(out, r2, count, wta_threshold)
+        spk = fire(out, fire_threshold)
+        wins = convwta(out, r2, count, wta_threshold)
+        return (spk, wins) if p2 is None else (spk, wins, _pool_op(spk, p2))
     spikes = torch.empty(oshape, dtype=torch.uint8, device=x.device)
+    pooled = None
+    if p2 is not None:
+        pooled = torch.empty(shape.pool(oshape, p2, p2, (0, 0, 0, 0)), dtype=torch.uint8, device=x.device)
     rec = torch.zeros((s[0], count, 5), dtype=torch.int32, device=x.device)
     cnt = torch.zeros((s[0],), dtype=torch.int32, device=x.device)
     ws, wsb = _workspace(nb, x.device)
     call("spk_conv_fire_wta", ptr(x), type_code(x.dtype), ptr(k), s[0], s[1], cin, s[3], s[4], cout, kh, kw,
          conv._stride[0], conv._stride[1], i64(*conv._pad), float(threshold), float(value), float(inhibit_threshold),
          float(fire_threshold), r2[0], r2[1], count, float(wta_threshold), ptr(spikes), ptr(rec), ptr(cnt),
-         _PRECISION[prec], ptr(ws), wsb, stream())
-    return spikes, Winners(rec, cnt)
+         p2[0] if p2 else 0, p2[1] if p2 else 0, ptr(pooled), _PRECISION[prec], ptr(ws), wsb, stream())
+    return (spikes, Winners(rec, cnt)) if p2 is None else (spikes, Winners(rec, cnt), pooled)
 
 
 def conv_(x, layer: "Conv", prec: str):

@@ -476,6 +476,25 @@ def test_fused_layer_matches_ops(port, case, prec):
     assert int(got[1].sum()) > 0
 
 
+@pytest.mark.parametrize("case", [((6, 15, 2, 28, 28, 30, 5, 2), (2, 2)), ((5, 15, 30, 14, 14, 100, 5, 2), (14, 14)),
+                                  ((4, 9, 3, 13, 11, 12, 3, 1), (3, 2))])
+def test_fused_layer_pooled(case):
+    """The pooled spikes written by the fused kernel equal pool(spikes)."""
+    (b, t, cin, h, w, cout, k, pad), p = case
+    rng = np.random.default_rng(b + t)
+    fst = rng.integers(0, t + 3, size=(b, cin, h, w))
+    x = cuda((fst[:, None] <= np.arange(t)[None, :, None, None, None]).astype(np.uint8))
+    conv = spyker.Conv(cin, cout, k, pad=pad)
+    conv.kernel.copy_(cuda(rng.uniform(0.3, 1.0, size=(cout, cin, k, k)).astype(np.float32)))
+    conv.precision = "bf16x3"
+    theta = 0.4 * cin * k * k * 0.65
+    spikes, wins, pooled = spyker.conv_fire_wta(x, conv, theta, 1, 3, pool=p)
+    assert int(host(spikes).sum()) > 0
+    assert np.array_equal(host(pooled), host(spyker.pool(spikes, p)))
+    s2, w2 = spyker.conv_fire_wta(x, conv, theta, 1, 3)
+    assert np.array_equal(host(s2), host(spikes))
+
+
 @pytest.mark.parametrize("kind", ["random", "values"])
 def test_fused_layer_noncumulative(kind):
     """Inputs that are not cumulative 0/1 spikes take the producers' direct
