@@ -379,28 +379,40 @@ __device__ void fused_epilogue(const TcParams &P, uint32_t acc, bool row_ok, int
     const int win = __shfl_sync(0xffffffffu, am, base + ts);
     // exact value of the winning channel at this step: reload only the column
     // chunks that hold the warp's winners
+    // (up to two 8-column chunks per round trip)
     uint32_t pieces[3] = {0, 0, 0};
     unsigned pending = 0xffffffffu;
     while (pending)
     {
-        const int c0 = (__shfl_sync(0xffffffffu, win, __ffs(pending) - 1) >> 4) << 4;
-        uint32_t r0[16], r1[16], r2[16];
-        tmem_ld16(lane_base + uint32_t(c0), r0);
-        tmem_ld16(lane_base + uint32_t(P.n_tile + c0), r1);
-        if (P.nsplit == 3) tmem_ld16(lane_base + uint32_t(2 * P.n_tile + c0), r2);
-        tmem_ld_wait();
-        const bool mine = (win >> 4) == (c0 >> 4);
+        const int ca = (__shfl_sync(0xffffffffu, win, __ffs(pending) - 1) >> 3) << 3;
+        const bool ma = (win >> 3) == (ca >> 3);
+        const unsigned rest = pending & ~__ballot_sync(0xffffffffu, ma);
+        const bool two = rest != 0;
+        const int cb = two ? (__shfl_sync(0xffffffffu, win, __ffs(rest) - 1) >> 3) << 3 : ca;
+        const bool mb = two && (win >> 3) == (cb >> 3);
+        uint32_t qa[3][kEpiChunk], qb[3][kEpiChunk];
+        tmem_chunk<NS>(lane_base, ca, P.n_tile, qa);
+        if (two) tmem_chunk<NS>(lane_base, cb, P.n_tile, qb);
+        tmem_chunk_wait<NS>(qa);
+        if (two) tmem_chunk_wait<NS>(qb);
 #pragma unroll
-        for (int j = 0; j < 16; ++j)
-            if (mine && c0 + j == win)
+        for (int j = 0; j < kEpiChunk; ++j)
+        {
+            if (ma && ca + j == win)
             {
-                pieces[0] = r0[j], pieces[1] = r1[j];
-                if (P.nsplit == 3) pieces[2] = r2[j];
+                pieces[0] = qa[0][j], pieces[1] = qa[1][j];
+                if (NS == 3) pieces[2] = qa[2][j];
             }
-        pending &= ~__ballot_sync(0xffffffffu, mine);
+            if (mb && cb + j == win)
+            {
+                pieces[0] = qb[0][j], pieces[1] = qb[1][j];
+                if (NS == 3) pieces[2] = qb[2][j];
+            }
+        }
+        pending &= ~__ballot_sync(0xffffffffu, ma || mb);
     }
     double accv = double(__uint_as_float(pieces[0])) + double(__uint_as_float(pieces[1]));
-    if (P.nsplit == 3) accv += double(__uint_as_float(pieces[2]));
+    if (NS == 3) accv += double(__uint_as_float(pieces[2]));
     const float raw = float(accv);
     const float vw = (raw <= P.thr) ? P.thv : raw;
     // spike of the winning channel (the spike tensor was zero-filled first)
@@ -468,11 +480,20 @@ __device__ __forceinline__ RowInfo row_info(const TcParams &P, int64_t mt, int r
     }
     else
     {
-        // row = (pixel in tile) * TP + t: all steps of a pixel in one warp
+        // row = (pixel in tile) * TP + t: all steps of a pixel in one warp;
+        // pixel indexes fit in 32 bits (checked on the host)
         r.tstep = row & ((1 << P.tp_log2) - 1);
-        const int64_t gp = mt * P.pp + (row >> P.tp_log2);
-        r.ok = r.tstep < P.T && gp < P.npix;
-        if (r.ok) r.sample = gp / P.ohw, r.pix = gp % P.ohw, r.img = r.sample * P.T + r.tstep;
+        const uint32_t gp = uint32_t(mt) * uint32_t(P.pp) + uint32_t(row >> P.tp_log2);
+        r.ok = r.tstep < P.T && int64_t(gp) < P.npix;
+        if (r.ok)
+        {
+            const uint32_t ohw = uint32_t(P.ohw), smp = gp / ohw, pix = gp - smp * ohw;
+            r.sample = smp, r.pix = pix, r.img = int64_t(smp) * P.T + r.tstep;
+            const int oy = int(pix / uint32_t(P.ow)), ox = int(pix) - oy * P.ow;
+            r.iy0 = oy * P.sy - P.top;
+            r.ix0 = ox * P.sx - P.left;
+        }
+        return r;
     }
     if (r.ok)
     {
@@ -1299,6 +1320,7 @@ spk_status spk_conv_fire_wta(const void *in, spk_dtype itype, const float *kerne
         SPK_REQUIRE(L.oh > 0 && L.ow > 0, "input and kernel shapes are not compatible");
         SPK_REQUIRE(L.pl.n_tiles == 1 && L.pl.nsplit * L.pl.n_tile <= 512, "too many output channels for one CTA");
         SPK_REQUIRE(L.oh * L.ow <= 16384, "the fused WTA keeps at most 16384 pixels per sample");
+        SPK_REQUIRE(L.npix < (int64_t(1) << 31), "at most 2^31 - 1 output pixels per call");
         SPK_REQUIRE(ws != nullptr && ws_bytes >= L.total, "workspace is too small");
         if (b == 0) return;
         cudaStream_t s = stream_of(stream);
