@@ -227,7 +227,10 @@ spk_status spk_conv(const void *in, spk_dtype itype, const float *kernel, float 
  * and a tensor-core precision.  With pool_ky > 0 it also writes pooled =
  * pool(spikes, (pool_ky, pool_kx)) (stride = window, no padding; the
  * rank_pool of impl.h:268 on the spikes), [B, T, Cout, OH / pool_ky,
- * OW / pool_kx] U8; pooled may be null when pool_ky == 0. */
+ * OW / pool_kx] U8; pooled may be null when pool_ky == 0.  count == 0
+ * skips the winner selection (winners and counts may then be null).  The
+ * workspace query returns 0 for layers whose accumulators (terms x Cout,
+ * Cout rounded up to 16) exceed the 512 tensor-memory columns of a CTA. */
 size_t spk_conv_fire_wta_workspace(int64_t b, int64_t t, int64_t cin, int64_t h, int64_t w, int64_t cout, int64_t kh,
                                    int64_t kw, int64_t sy, int64_t sx, const int64_t *pad4_host, int precision);
 spk_status spk_conv_fire_wta(const void *in, spk_dtype itype, const float *kernel, int64_t b, int64_t t, int64_t cin,

@@ -429,6 +429,7 @@ __device__ void fused_epilogue(const TcParams &P, uint32_t acc, bool row_ok, int
                 P.pooled[((sample * T + tstep) * C + win) * int64_t(P.poh) * P.pow_ + py * P.pow_ + px] = 1;
         }
     }
+    if (P.records == nullptr) return;  // no WTA on this call (uniform)
     // WTA record: first step whose inhibited value exceeds wta_thr
     const unsigned keyed = __ballot_sync(0xffffffffu, row_ok && vw > P.wta_thr) & grp;
     const int first_lane = keyed ? __ffs(keyed) - 1 : base;
@@ -1292,7 +1293,10 @@ size_t spk_conv_fire_wta_workspace(int64_t b, int64_t t, int64_t cin, int64_t h,
 {
     try
     {
-        return fused_layout(b, t, cin, h, w, cout, kh, kw, sy, sx, pad_of(pad4), precision).total;
+        const FusedLayout L = fused_layout(b, t, cin, h, w, cout, kh, kw, sy, sx, pad_of(pad4), precision);
+        // 0: this layer does not fit one CTA's tensor memory (no fused path)
+        if (L.pl.n_tiles != 1 || L.pl.nsplit * L.pl.n_tile > 512) return 0;
+        return L.total;
     }
     catch (...)
     {
@@ -1314,12 +1318,14 @@ spk_status spk_conv_fire_wta(const void *in, spk_dtype itype, const float *kerne
         SPK_REQUIRE(b >= 0 && t >= 1 && t <= 32 && cin >= 1 && cout >= 2 && kh >= 1 && kw >= 1 && sy >= 1 && sx >= 1,
                     "the fused layer needs 1 <= T <= 32 and at least 2 output channels");
         SPK_REQUIRE(fire_threshold >= 0 && wta_threshold >= 0, "the fused layer needs fire/WTA thresholds >= 0");
-        SPK_REQUIRE(count >= 1 && ry >= 0 && rx >= 0, "invalid WTA radius or count");
-        SPK_REQUIRE(winners != nullptr && counts != nullptr && spikes != nullptr, "null output");
+        // count == 0: no winner selection (forward passes); winners and
+        // counts may then be null
+        SPK_REQUIRE(count >= 0 && ry >= 0 && rx >= 0, "invalid WTA radius or count");
+        SPK_REQUIRE(spikes != nullptr && (count == 0 || (winners != nullptr && counts != nullptr)), "null output");
         FusedLayout L = fused_layout(b, t, cin, h, w, cout, kh, kw, sy, sx, p, precision);
         SPK_REQUIRE(L.oh > 0 && L.ow > 0, "input and kernel shapes are not compatible");
         SPK_REQUIRE(L.pl.n_tiles == 1 && L.pl.nsplit * L.pl.n_tile <= 512, "too many output channels for one CTA");
-        SPK_REQUIRE(L.oh * L.ow <= 16384, "the fused WTA keeps at most 16384 pixels per sample");
+        SPK_REQUIRE(count == 0 || L.oh * L.ow <= 16384, "the fused WTA keeps at most 16384 pixels per sample");
         SPK_REQUIRE(L.npix < (int64_t(1) << 31), "at most 2^31 - 1 output pixels per call");
         SPK_REQUIRE(ws != nullptr && ws_bytes >= L.total, "workspace is too small");
         if (b == 0) return;
@@ -1341,16 +1347,20 @@ spk_status spk_conv_fire_wta(const void *in, spk_dtype itype, const float *kerne
             SPK_REQUIRE(L.oh >= pool_ky && L.ow >= pool_kx, "the pooling window is larger than the output");
             P.pooled = pooled, P.pky = int(pool_ky), P.pkx = int(pool_kx), P.poh = int(poh), P.pow_ = int(pow_);
         }
-        P.records = reinterpret_cast<int4 *>(base + L.rec_off);
-        P.mins = reinterpret_cast<unsigned *>(base + L.min_off);
-        P.maxs = reinterpret_cast<unsigned *>(base + L.max_off);
+        if (count > 0)
+        {
+            P.records = reinterpret_cast<int4 *>(base + L.rec_off);
+            P.mins = reinterpret_cast<unsigned *>(base + L.min_off);
+            P.maxs = reinterpret_cast<unsigned *>(base + L.max_off);
+            SPK_CUDA(cudaMemsetAsync(P.mins, 0xFF, size_t(b) * 4, s));
+            SPK_CUDA(cudaMemsetAsync(P.maxs, 0x00, size_t(b) * 4, s));
+        }
         P.M = L.npix * (int64_t(1) << L.tp_log2);
         P.tiles = ceil_div(L.npix, L.pp);
         SPK_CUDA(cudaMemsetAsync(spikes, 0, size_t(b) * t * cout * L.oh * L.ow, s));
         if (pool_ky > 0) SPK_CUDA(cudaMemsetAsync(pooled, 0, size_t(b) * t * cout * poh * pow_, s));
-        SPK_CUDA(cudaMemsetAsync(P.mins, 0xFF, size_t(b) * 4, s));
-        SPK_CUDA(cudaMemsetAsync(P.maxs, 0x00, size_t(b) * 4, s));
         launch<kFused>(P, L.pl, s);
+        if (count == 0) return;
         const int hw = int(L.oh * L.ow);
         wta_records_kernel<<<unsigned(b), 256, size_t(hw) * 8, s>>>(P.records, P.mins, P.maxs, hw, int(L.ow), int(t),
                                                                     int(ry), int(rx), int(count), winners, counts);

@@ -431,8 +431,8 @@ def convwta(array, radius, count: int, threshold: float = 0.0) -> Winners:
         raise ValueError("Winners count can't be less than 1.")
     x = Bound(array).dev
     s = to5(list(x.shape))
-    rec = torch.zeros((s[0], count, 5), dtype=torch.int32, device=x.device)
-    cnt = torch.zeros((s[0],), dtype=torch.int32, device=x.device)
+    rec = torch.zeros((s[0], count, 5), dtype=torch.int32, device=x.device) if count > 0 else None
+    cnt = torch.zeros((s[0],), dtype=torch.int32, device=x.device) if count > 0 else None
     ws, wsb = _workspace(_lib.lib.spk_rank_convwta_workspace(*s), x.device)
     call("spk_rank_convwta", ptr(x), type_code(x.dtype), *s, r2[0], r2[1], count, float(threshold), ptr(rec), ptr(cnt),
          ptr(ws), wsb, stream())
@@ -446,8 +446,8 @@ def fcwta(array, radius: int, count: int, threshold: float = 0.0) -> Winners:
         raise ValueError("Winners count can't be less than 1.")
     x = Bound(array).dev
     s = to3(list(x.shape))
-    rec = torch.zeros((s[0], count, 5), dtype=torch.int32, device=x.device)
-    cnt = torch.zeros((s[0],), dtype=torch.int32, device=x.device)
+    rec = torch.zeros((s[0], count, 5), dtype=torch.int32, device=x.device) if count > 0 else None
+    cnt = torch.zeros((s[0],), dtype=torch.int32, device=x.device) if count > 0 else None
     ws, wsb = _workspace(_lib.lib.spk_rank_fcwta_workspace(*s), x.device)
     call("spk_rank_fcwta", ptr(x), type_code(x.dtype), *s, radius, count, float(threshold), ptr(rec), ptr(cnt), ptr(ws),
          wsb, stream())
@@ -585,7 +585,8 @@ def conv_fire_wta(array, conv: "Conv", threshold: float, radius, count: int, val
 
     With ``pool`` (a window, stride = window, no padding) it returns
     ``(spikes, winners, pool(spikes, pool))``, the pooled spikes written by the
-    same kernel.
+    same kernel.  ``count=0`` skips the winner selection (forward passes);
+    winners is then None.
 
     On the tensor-core precisions with u8 spikes, T <= 32, at least two output
     channels and non-negative fire/WTA thresholds, a single tcgen05 kernel does
@@ -598,8 +599,10 @@ def conv_fire_wta(array, conv: "Conv", threshold: float, radius, count: int, val
     k = conv.kernel if conv.kernel.dtype == torch.float32 else conv.kernel.float()
     k = k.contiguous()
     cout, cin, kh, kw = k.shape
+    if count < 0:
+        raise ValueError("Winners count can't be less than 0.")
     fused = (prec != "fp32" and x.dtype == torch.uint8 and s[1] <= 32 and cout >= 2 and fire_threshold >= 0
-             and wta_threshold >= 0 and count > 0 and min(r2) >= 0)
+             and wta_threshold >= 0 and min(r2) >= 0)
     if fused:
         oshape = shape.conv(s, list(k.shape), conv._stride, conv._pad)
         nb = _lib.lib.spk_conv_fire_wta_workspace(s[0], s[1], cin, s[3], s[4], cout, kh, kw, conv._stride[0],
@@ -611,20 +614,21 @@ def conv_fire_wta(array, conv: "Conv", threshold: float, radius, count: int, val
     if not fused:
         out = inhibit(_threshold_op(conv_(x, conv, prec), threshold, value), inhibit_threshold)
         spk = fire(out, fire_threshold)
-        wins = convwta(out, r2, count, wta_threshold)
+        wins = convwta(out, r2, count, wta_threshold) if count > 0 else None
         return (spk, wins) if p2 is None else (spk, wins, _pool_op(spk, p2))
     spikes = torch.empty(oshape, dtype=torch.uint8, device=x.device)
     pooled = None
     if p2 is not None:
         pooled = torch.empty(shape.pool(oshape, p2, p2, (0, 0, 0, 0)), dtype=torch.uint8, device=x.device)
-    rec = torch.zeros((s[0], count, 5), dtype=torch.int32, device=x.device)
-    cnt = torch.zeros((s[0],), dtype=torch.int32, device=x.device)
+    rec = torch.zeros((s[0], count, 5), dtype=torch.int32, device=x.device) if count > 0 else None
+    cnt = torch.zeros((s[0],), dtype=torch.int32, device=x.device) if count > 0 else None
     ws, wsb = _workspace(nb, x.device)
     call("spk_conv_fire_wta", ptr(x), type_code(x.dtype), ptr(k), s[0], s[1], cin, s[3], s[4], cout, kh, kw,
          conv._stride[0], conv._stride[1], i64(*conv._pad), float(threshold), float(value), float(inhibit_threshold),
          float(fire_threshold), r2[0], r2[1], count, float(wta_threshold), ptr(spikes), ptr(rec), ptr(cnt),
          p2[0] if p2 else 0, p2[1] if p2 else 0, ptr(pooled), _PRECISION[prec], ptr(ws), wsb, stream())
-    return (spikes, Winners(rec, cnt)) if p2 is None else (spikes, Winners(rec, cnt), pooled)
+    wins = Winners(rec, cnt) if count > 0 else None
+    return (spikes, wins) if p2 is None else (spikes, wins, pooled)
 
 
 def conv_(x, layer: "Conv", prec: str):

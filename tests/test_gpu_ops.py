@@ -495,6 +495,38 @@ def test_fused_layer_pooled(case):
     assert np.array_equal(host(s2), host(spikes))
 
 
+def test_gabor_forward_pipeline(port):
+    """The large-image forward pipeline at a reduced size: Gabor bank (4
+    orientations x 2 wavelengths, 11x11) -> rank code T=30 -> conv1 64x7x7
+    th20 fused with inhibition and pool 2 (no winner selection) -> conv2
+    256x5x5 th12 (op by op: 3 x 256 accumulator columns exceed tensor
+    memory) -> pool 2, against the oracle's FP64 pipeline on the same codes."""
+    imgs = synth.textures(1, seed=5, size=32)
+    filters = [spyker.GaborFilter(2.5, th, 0.5, lam, 0.0) for th in (0, 45, 90, 135) for lam in (5.0, 10.0)]
+    gab = spyker.Gabor(5, filters, pad=5)
+    g = gab(cuda(imgs[:, None]))
+    assert np.array_equal(host(g), port.filter("gabor", imgs[:, None], host(gab.kernel), (5, 5, 5, 5)))
+    codes = spyker.code(g, 30)
+    assert np.array_equal(host(codes), stable_code(host(g), 30))
+    w1 = synth.conv_weights(64, 8, 7, seed=11)
+    w2 = synth.conv_weights(256, 64, 5, seed=12)
+    c1, c2 = spyker.Conv(8, 64, 7, pad=3), spyker.Conv(64, 256, 5, pad=2)
+    c1.kernel.copy_(cuda(w1)), c2.kernel.copy_(cuda(w2))
+    c1.precision = c2.precision = "bf16x3"
+    s1, none, p1 = spyker.conv_fire_wta(codes, c1, 20.0, 0, 0, pool=2)
+    assert none is None
+    s2, _, p2 = spyker.conv_fire_wta(p1, c2, 12.0, 0, 0, pool=2)
+    hc = host(codes)
+    r1 = port.fire(port.inhibit(port.threshold(port.conv(hc, w1, (1, 1), (3, 3, 3, 3)), 20.0)))
+    assert np.array_equal(host(s1), r1)
+    q1 = port.pool(r1, (2, 2))
+    assert np.array_equal(host(p1), q1)
+    r2 = port.fire(port.inhibit(port.threshold(port.conv(q1, w2, (1, 1), (2, 2, 2, 2)), 12.0)))
+    assert np.array_equal(host(s2), r2)
+    assert np.array_equal(host(p2), port.pool(r2, (2, 2)))
+    assert int(r2.sum()) > 0
+
+
 @pytest.mark.parametrize("kind", ["random", "values"])
 def test_fused_layer_noncumulative(kind):
     """Inputs that are not cumulative 0/1 spikes take the producers' direct
