@@ -1135,6 +1135,75 @@ __global__ void fst_stage_kernel(const uint8_t *__restrict__ in, uint8_t *__rest
     if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
 }
 
+// The same map from 32-bit words (H*W a multiple of 4, input 4-byte
+// aligned): a CTA takes one sample and a range of npx pixels of every
+// channel.  For one step those are C runs of npx bytes, the whole contiguous
+// [C, H*W] block when the range is the image, so consecutive threads read
+// consecutive words (four pixels of one channel).  The [pixel][channel] tile
+// (rows padded to Cp + 1 bytes, which spreads a warp's stores over the
+// banks) goes out as contiguous rows.
+__global__ void __launch_bounds__(256) fst_stage_words_kernel(const uint8_t *__restrict__ in, uint8_t *__restrict__ fst,
+                                                              int *__restrict__ flag, int t, int c, int hw, int cp,
+                                                              int ppc)
+{
+    extern __shared__ uint8_t tile[];  // [ppc][cp + 1]
+    const int rs = cp + 1;
+    const int64_t smp = blockIdx.y;
+    const int px0 = blockIdx.x * ppc;
+    const int npx = min(ppc, hw - px0);
+    const int gw = npx / 4;  // words per channel run
+    const int64_t st = int64_t(c) * hw / 4;
+    const uint32_t *base = reinterpret_cast<const uint32_t *>(in + smp * t * c * int64_t(hw) + px0);
+    bool bad = false;
+    for (int it = threadIdx.x; it < c * gw; it += blockDim.x)
+    {
+        const int ch = it / gw, p = 4 * (it - ch * gw);
+        const uint32_t *src = base + (int64_t(ch) * hw + p) / 4;
+        // On cumulative 0/1 input the first spike is the number of zero
+        // steps: T minus the byte-wise sum of the words (no carries, as each
+        // byte sum is at most T < 256).  Any other byte value, or a one
+        // followed by a zero, is flagged.
+        // All (up to 16) steps' loads are in flight together.
+        uint32_t sum = 0, prev = 0, odd = 0;
+        for (int q0 = 0; q0 < t; q0 += 16)
+        {
+            uint32_t v[16];
+#pragma unroll
+            for (int u = 0; u < 16; ++u) v[u] = (q0 + u < t) ? src[int64_t(q0 + u) * st] : 0u;
+#pragma unroll
+            for (int u = 0; u < 16; ++u)
+                if (q0 + u < t)  // the same for every thread
+                {
+                    sum += v[u];
+                    odd |= (v[u] & 0xFEFEFEFEu) | (prev & ~v[u]);
+                    prev = v[u];
+                }
+        }
+        bad |= odd != 0;
+        const uint32_t first = uint32_t(t) * 0x01010101u - sum;
+#pragma unroll
+        for (int l = 0; l < 4; ++l) tile[(p + l) * rs + ch] = uint8_t(first >> (8 * l));
+    }
+    for (int it = threadIdx.x; it < npx * (cp - c); it += blockDim.x)
+    {
+        const int px = it / (cp - c);
+        tile[px * rs + c + (it - px * (cp - c))] = 0xFF;
+    }
+    __syncthreads();
+    uint8_t *dst = fst + (smp * hw + px0) * int64_t(cp);
+    if (cp % 4 == 0)
+        for (int i = threadIdx.x; i < npx * cp / 4; i += blockDim.x)
+        {
+            const int px = (4 * i) / cp, ch = 4 * i - px * cp;
+            const uint8_t *r = tile + px * rs + ch;
+            reinterpret_cast<uint32_t *>(dst)[i] =
+                uint32_t(r[0]) | uint32_t(r[1]) << 8 | uint32_t(r[2]) << 16 | uint32_t(r[3]) << 24;
+        }
+    else
+        for (int i = threadIdx.x; i < npx * cp; i += blockDim.x) dst[i] = tile[(i / cp) * rs + i % cp];
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
+}
+
 // t_fused > 0: stage for the fused (pixel, time) rows of t_fused steps.
 TcParams prepare(const Plan &pl, const void *in, const float *kernel, int64_t n, int64_t cin, int64_t h, int64_t w,
                  int64_t cout, int64_t kh, int64_t kw, int64_t sy, int64_t sx, Pad4 p, int64_t oh, int64_t ow,
@@ -1157,8 +1226,17 @@ TcParams prepare(const Plan &pl, const void *in, const float *kernel, int64_t n,
         const int64_t b = n / t_fused, cp = pl.nhwc ? pl.cpad : cin;
         int *flag = reinterpret_cast<int *>(xt + align256(size_t(b) * h * w * cp));
         SPK_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), s));
-        fst_stage_kernel<<<grid_for(b * cp * h * w, 256), 256, 0, s>>>(a_src, xt, flag, b, int(t_fused), int(cin),
-                                                                       h * w, int(cp));
+        // whole images when their tile fits in 48 KB, else the longest runs
+        // of whole words that do
+        const int64_t ppc = std::min<int64_t>(h * w, (48 * 1024 / (cp + 1)) & ~int64_t(3));
+        const size_t tile = size_t(ppc) * (cp + 1);
+        if ((h * w) % 4 == 0 && reinterpret_cast<uintptr_t>(a_src) % 4 == 0 && ppc >= 4 &&
+            h * w < (int64_t(1) << 31) && b <= 65535)
+            fst_stage_words_kernel<<<dim3(unsigned(ceil_div(h * w, ppc)), unsigned(b)), 256, tile, s>>>(
+                a_src, xt, flag, int(t_fused), int(cin), int(h * w), int(cp), int(ppc));
+        else
+            fst_stage_kernel<<<grid_for(b * cp * h * w, 256), 256, 0, s>>>(a_src, xt, flag, b, int(t_fused), int(cin),
+                                                                           h * w, int(cp));
         SPK_LAUNCHED();
         P.raw = a_src;
         P.flag = flag;

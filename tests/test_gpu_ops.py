@@ -453,6 +453,7 @@ FUSED = [
     (6, 3, 9, 8, 9, 16, 3, 1, 4.0, 1, 3),
     (4, 2, 2, 12, 12, 8, 5, 2, 3.0, 2, 5),
     (4, 1, 5, 7, 6, 12, 3, 0, 2.0, 1, 2),
+    (2, 6, 64, 32, 32, 32, 3, 1, 120.0, 1, 4),  # first-spike staging in two pixel runs
 ]
 
 
