@@ -258,6 +258,20 @@ struct FastMax
 
 constexpr int kEpiChunk = 8;  // accumulator columns per tensor-memory load
 
+// Merge the state of another set of channels into s: the larger maximum
+// wins, ties going to the lower channel; the loser's maximum competes for
+// the runner-up.
+__device__ __forceinline__ void merge_fast(FastMax &s, const FastMax &o)
+{
+    const bool take = o.r1 > s.r1 || (o.r1 == s.r1 && o.a1 >= 0 && (s.a1 < 0 || o.a1 < s.a1));
+    s.r2 = fmaxf(fmaxf(s.r2, o.r2), take ? s.r1 : o.r1);
+    s.r1 = take ? o.r1 : s.r1;
+    s.a1 = take ? o.a1 : s.a1;
+    s.amax = fmaxf(s.amax, o.amax);
+    s.dmin = fminf(s.dmin, o.dmin);
+    s.b1 = min(s.b1, o.b1);
+}
+
 template <int NS>
 __device__ __forceinline__ void tmem_chunk(uint32_t lane_base, int c0, int n_tile, uint32_t (&q)[3][kEpiChunk])
 {
@@ -309,11 +323,12 @@ __device__ __forceinline__ void fast_chunk(const TcParams &P, const uint32_t (&q
 // the two largest above-threshold values are within 2 tol, or the largest is
 // within tol of the below-threshold value or of the inhibition threshold.
 // Such rows (rare) are redone with FP64 sums.  Tensor-memory loads of the
-// next chunk are in flight while a chunk is processed.
+// next chunk are in flight while a chunk is processed; even and odd chunks
+// keep separate states (two independent dependency chains), merged at the end.
 template <int NS>
 __device__ __forceinline__ void row_argmax(const TcParams &P, uint32_t lane_base, bool row_ok, int &am, float &xam)
 {
-    FastMax st;
+    FastMax st, st2;
     constexpr int W = kEpiChunk;
     uint32_t qa[3][W], qb[3][W];
     tmem_chunk<NS>(lane_base, 0, P.n_tile, qa);
@@ -325,8 +340,9 @@ __device__ __forceinline__ void row_argmax(const TcParams &P, uint32_t lane_base
         fast_chunk<NS>(P, qa, c0, st);
         tmem_chunk_wait<NS>(qb);
         if (c0 + 2 * W < P.n_tile) tmem_chunk<NS>(lane_base, c0 + 2 * W, P.n_tile, qa);
-        fast_chunk<NS>(P, qb, c0 + W, st);
+        fast_chunk<NS>(P, qb, c0 + W, st2);
     }
+    merge_fast(st, st2);
     const float tol = __fmaf_rn(st.amax, 0x1p-21f, 0x1p-140f);
     bool unsure = st.dmin <= tol;
     const bool has_real = st.a1 >= 0, has_low = st.b1 != INT_MAX;
@@ -361,8 +377,17 @@ __device__ __forceinline__ void row_argmax(const TcParams &P, uint32_t lane_base
     }
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// `release` (the accumulator's empty barrier) is arrived at as soon as the
+// last tensor-memory load of the tile has completed, so the next tile's MMAs
+// overlap the stores below.
 template <int NS>
-__device__ void fused_epilogue(const TcParams &P, uint32_t acc, bool row_ok, int tstep, int64_t sample, int64_t pix)
+__device__ void fused_epilogue(const TcParams &P, uint32_t acc, bool row_ok, int tstep, int64_t sample, int64_t pix,
+                               uint64_t *release)
 {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int TP = 1 << P.tp_log2, T = P.T, C = P.cout;
@@ -411,6 +436,8 @@ __device__ void fused_epilogue(const TcParams &P, uint32_t acc, bool row_ok, int
         }
         pending &= ~__ballot_sync(0xffffffffu, ma || mb);
     }
+    tc_fence_before();
+    mbar_arrive(release);
     double accv = double(__uint_as_float(pieces[0])) + double(__uint_as_float(pieces[1]));
     if (NS == 3) accv += double(__uint_as_float(pieces[2]));
     const float raw = float(accv);
@@ -445,7 +472,22 @@ __device__ void fused_epilogue(const TcParams &P, uint32_t acc, bool row_ok, int
         rmin = (0.f < rmin) ? 0.f : rmin;
         rmax = (rmax < 0.f) ? 0.f : rmax;
     }
+    const unsigned okm = __ballot_sync(0xffffffffu, row_ok);
+    if (okm == 0) return;
+    const int src = __ffs(okm) - 1;
     const int key = row_ok ? int(sample) : -1;
+    const int k0 = __shfl_sync(0xffffffffu, key, src);
+    if (__all_sync(0xffffffffu, !row_ok || key == k0))
+    {
+        const unsigned emin = __reduce_min_sync(0xffffffffu, row_ok ? order_enc(rmin) : 0xFFFFFFFFu);
+        const unsigned emax = __reduce_max_sync(0xffffffffu, row_ok ? order_enc(rmax) : 0u);
+        if (lane == src)
+        {
+            atomicMin(P.mins + sample, emin);
+            atomicMax(P.maxs + sample, emax);
+        }
+        return;
+    }
     const unsigned peers = __match_any_sync(0xffffffffu, key);
     const unsigned emin = __reduce_min_sync(peers, order_enc(rmin));
     const unsigned emax = __reduce_max_sync(peers, order_enc(rmax));
@@ -454,11 +496,6 @@ __device__ void fused_epilogue(const TcParams &P, uint32_t acc, bool row_ok, int
         atomicMin(P.mins + sample, emin);
         atomicMax(P.maxs + sample, emax);
     }
-}
-
-__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
-{
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
 // Row of a tile: (image for the A gather, sample, step, output pixel).
@@ -957,12 +994,18 @@ __global__ void __launch_bounds__(kWsThreads, 1) conv_ws_kernel(TcParams P)
                     }
                 }
             }
-            else if (P.nsplit == 3)
-                fused_epilogue<3>(P, acc, r.ok, r.tstep, r.sample, r.pix);
+            if constexpr (MODE == kFused)
+            {
+                if (P.nsplit == 3)
+                    fused_epilogue<3>(P, acc, r.ok, r.tstep, r.sample, r.pix, &acce_bar[a]);
+                else
+                    fused_epilogue<2>(P, acc, r.ok, r.tstep, r.sample, r.pix, &acce_bar[a]);
+            }
             else
-                fused_epilogue<2>(P, acc, r.ok, r.tstep, r.sample, r.pix);
-            tc_fence_before();
-            mbar_arrive(&acce_bar[a]);
+            {
+                tc_fence_before();
+                mbar_arrive(&acce_bar[a]);
+            }
         }
     }
     tc_fence_before();
