@@ -484,6 +484,99 @@ def gabor_arm(args, rank, world):
     }), flush=True)
 
 
+# ----------------------------------------------------------------------------
+# Temporal backprop (--workload backprop)
+# ----------------------------------------------------------------------------
+BP_WORKLOAD = ("temporal-backprop: 256 x 28x28 labelled strokes (10 classes), T=64, conv 32x5x5 -> pool 2 -> "
+               "conv 64x3x3 -> pool 2 -> fc 10, first-spike-time loss, SGD")
+
+
+def backprop_arm(args, rank, world):
+    """One training step = rank code -> 3 first-spike layers -> target-rule
+    loss -> hand-written backward kernels (autograd) -> SGD update."""
+    import torch
+
+    import spyker_b200 as spyker
+    from spyker_b200 import synth, temporal
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    batch = args.batch if args.batch != BATCH else 256
+    imgs, labels = synth.labelled_strokes(batch, seed=20 + rank)
+    host = torch.from_numpy(imgs).pin_memory()
+    x = host.to(dev).float().div_(255.0)[:, None]
+    y = torch.from_numpy(labels).to(dev)
+    net = temporal.TemporalNet(time=64, seed=4, device=dev, precision=args.precision)
+    for _ in range(args.warmup):
+        net.step(x, y)
+    torch.cuda.synchronize()
+    l0 = spyker._lib.lib.spk_launch_count()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(dev.index) as clk:
+        torch.cuda.synchronize()
+        a.record()
+        for _ in range(args.steps):
+            loss, t_out = net.step(x, y)
+        b.record()
+        torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / args.steps
+    launches = (spyker._lib.lib.spk_launch_count() - l0) // max(args.steps, 1)
+    # forward / backward split of one step
+    f0, f1, f2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    f0.record()
+    t_fwd = net.forward(net.input_times(x))
+    lo = net.loss(t_fwd, y)
+    f1.record()
+    torch.autograd.grad(lo, net.weights)
+    f2.record()
+    torch.cuda.synchronize()
+    fwd_ms, bwd_ms = f0.elapsed_time(f1), f1.elapsed_time(f2)
+    # end to end: pinned host images -> loss on the host
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(args.steps):
+        xe = host.to(dev, non_blocking=True).float().div_(255.0)[:, None]
+        loss_host = net.step(xe, y)[0].cpu()
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / args.steps
+    fp32 = None
+    if args.precision != "fp32" and not args.no_fp32_compare:
+        ref = temporal.TemporalNet(time=64, seed=4, device=dev, precision="fp32")
+        ref.step(x, y)
+        torch.cuda.synchronize()
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record()
+        ref.step(x, y)
+        g1.record()
+        torch.cuda.synchronize()
+        fp32 = {"value": batch / (g0.elapsed_time(g1) * 1e-3), "unit": "images/s", "steps": 1}
+    fwd_flops = 2 * 64 * (784 * 32 * 25 + 196 * 64 * 288 + 10 * 3136)
+    line = {
+        "metric": "images/s (temporal-backprop training step) on 1 B200",
+        "value": batch / (ms * 1e-3), "unit": "images/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": {"fp32": "f32", "bf16x2": "bf16x2-split/f32-acc", "bf16x3": "bf16x3-split/f32-acc"}[args.precision]
+        + " forward, f32/f64 backward",
+        "data": "synthetic (seeded labelled stroke images, 10 classes)",
+        "config": {"workload": BP_WORKLOAD.replace("256 x", f"{batch} x"), "global_batch": batch, "seq_len": 64,
+                   "parallelism": "replicas1", "conv_precision": args.precision,
+                   "l2": "inputs larger than L2: the layer-1 potentials are 1.6 GB per step"},
+        "e2e": {"value": batch / (e2e_ms * 1e-3), "unit": "images/s", "h2d_bytes_per_step": int(host.numel()),
+                "d2h_bytes_per_step": int(loss_host.numel() * loss_host.element_size())},
+        "gpu_launches": int(launches),
+        "kernels_ms": {"forward_and_loss": fwd_ms, "backward": bwd_ms},
+        "forward_tflops": fwd_flops * batch / (fwd_ms * 1e-3) / 1e12,
+        "loss": float(loss_host),
+        "outputs_fired_pct": 100.0 * float((t_out < 64).float().mean()),
+        "clocks": clk.summary(),
+    }
+    if fp32 is not None:
+        line["fp32_path"] = fp32
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -497,8 +590,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32-compare", action="store_true")
     ap.add_argument("--no-spike-match", action="store_true")
-    ap.add_argument("--workload", default="kheradpisheh", choices=["kheradpisheh", "gabor256"],
-                    help="kheradpisheh: the 2-layer STDP training step (the headline); gabor256: large-image forward")
+    ap.add_argument("--workload", default="kheradpisheh", choices=["kheradpisheh", "gabor256", "backprop"],
+                    help="kheradpisheh: the 2-layer STDP training step (the headline); gabor256: large-image "
+                         "forward; backprop: temporal-backprop training of a 3-layer first-spike network")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", args.gpus if args.impl == "reference" else 1))
@@ -506,6 +600,8 @@ def main():
         reference_arm(args, rank, world)
     elif args.workload == "gabor256":
         gabor_arm(args, rank, world)
+    elif args.workload == "backprop":
+        backprop_arm(args, rank, world)
     else:
         gpu_arm(args, rank, world)
 

@@ -266,6 +266,44 @@ size_t spk_fcbackward_workspace(int64_t no, int64_t ni);
 spk_status spk_fcbackward(float *kernel, int64_t no, int64_t ni, const float *in, const float *out, const float *grad,
                           float *next, int64_t b, float *bp_host, void *ws, size_t ws_bytes, spk_stream stream);
 
+/* ---- first-spike layers trained through their spike times ----
+ * The rule of the fc backward above (select = (t_in < t_out) * grad,
+ * next = sum kernel * select; cpu/backprop.cpp:116-144) written for a conv
+ * weight shared over output pixels (fc = the 1x1 case), as derivatives with
+ * grad_out = dL/dt_out (= -grad of the target rule, cpu/backprop.cpp:40-52):
+ *   grad_kernel[z,c,ky,kx] = -sum_{b,oy,ox} grad_out[b,z,oy,ox] * [t_in[b,c,iy,ix] < t_out[b,z,oy,ox]]
+ *   grad_in[b,c,iy,ix]     =  sum_{z,ky,kx} kernel[z,c,ky,kx] * grad_out[b,z,oy,ox] * [same mask]
+ * (iy, ix) = (oy*sy - top + ky, ox*sx - left + kx); padding never spikes.
+ * Times are F32 [B, C, H, W] (T = never).  Replaces nothing in the reference
+ * (its conv layers have no backward); the fc case equals Core::fcbackward's
+ * select / next with lrate = lambda = 0 (impl.h:316-318). */
+/* Earliest spike of each window (pool of cumulative spikes, cpu/pool.cpp:41-86);
+ * padding = `time` (never).  stride2/pad4/kernel2 on the host. */
+spk_status spk_fst_pool(const float *in, int64_t b, int64_t c, int64_t h, int64_t w, float *out, int64_t oh,
+                        int64_t ow, const int64_t *kernel2_host, const int64_t *stride2_host, const int64_t *pad4_host,
+                        double time, spk_stream stream);
+/* Gradient of each window to its earliest in-range input (first in raster
+ * order on ties); overlapping windows add up. */
+spk_status spk_fst_pool_backward(const float *in, int64_t b, int64_t c, int64_t h, int64_t w, const float *grad_out,
+                                 int64_t oh, int64_t ow, const int64_t *kernel2_host, const int64_t *stride2_host,
+                                 const int64_t *pad4_host, float *grad_in, spk_stream stream);
+/* grad_in [B, Cin, H, W] and / or grad_kernel [Cout, Cin, KH, KW] (either may be
+ * null; grad_in needs H*W <= 1024).  grad_kernel is summed in FP64 in a fixed
+ * order (deterministic); the workspace holds its per-group partial sums. */
+size_t spk_fst_conv_backward_workspace(int64_t b, int64_t cin, int64_t cout, int64_t kh, int64_t kw);
+spk_status spk_fst_conv_backward(const float *t_in, int64_t b, int64_t cin, int64_t h, int64_t w,
+                                 const float *kernel, int64_t cout, int64_t kh, int64_t kw, const float *t_out,
+                                 const float *grad_out, int64_t oh, int64_t ow, const int64_t *stride2_host,
+                                 const int64_t *pad4_host, float *grad_in, float *grad_kernel, void *ws,
+                                 size_t ws_bytes, spk_stream stream);
+/* The potential one step before each output spike, in FP64:
+ * out[b,z,oy,ox] = sum kernel[z,c,ky,kx] * [t_in[b,c,iy,ix] < t_out[b,z,oy,ox]]
+ * (the potential-level loss sum g * out has grad_kernel as its exact gradient). */
+spk_status spk_fst_conv_prespike(const float *t_in, int64_t b, int64_t cin, int64_t h, int64_t w,
+                                 const float *kernel, int64_t cout, int64_t kh, int64_t kw, const float *t_out,
+                                 int64_t oh, int64_t ow, const int64_t *stride2_host, const int64_t *pad4_host,
+                                 double *out, spk_stream stream);
+
 /* ---- event lists (the `sparse_*` table of impl.h:328-356; src/spyker/sparse) ----
  * A sparse spike tensor [U, T, C, H, W] (SparseTensor, utils.h:369-420; Sparse5,
  * base.h:493-528) is one CSR array on the device:

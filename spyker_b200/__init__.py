@@ -7,7 +7,7 @@ temporal-backprop helpers and the sparse event-list path.  Every operation
 runs on the GPU through the C ABI of ``include/spyker_b200.h``.
 """
 
-from . import sparse
+from . import sparse, temporal
 from ._lib import SpykerError
 from .module import (FC, ZCA, BPConfig, Conv, conv_fire_wta, DoG, DoGFilter, Gabor, GaborFilter, LoG, STDPConfig, Winner, Winners,
                      backward, canny, code, conv, conv_precision, convwta, fc, fcwta, fire, gather, infinite,

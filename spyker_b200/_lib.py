@@ -66,6 +66,12 @@ SIGNATURES = {
     "spk_labelize": (_INT, [_P, _INT, _P, _I, _I, _I, _D, _P]),
     "spk_fcbackward_workspace": (_S, [_I, _I]),
     "spk_fcbackward": (_INT, [_P, _I, _I, _P, _P, _P, _P, _I, _P, _P, _S, _P]),
+    "spk_fst_pool": (_INT, [_P, _I, _I, _I, _I, _P, _I, _I, _P, _P, _P, _D, _P]),
+    "spk_fst_pool_backward": (_INT, [_P, _I, _I, _I, _I, _P, _I, _I, _P, _P, _P, _P, _P]),
+    "spk_fst_conv_backward_workspace": (_S, [_I, _I, _I, _I, _I]),
+    "spk_fst_conv_backward": (_INT, [_P, _I, _I, _I, _I, _P, _I, _I, _I, _P, _P, _I, _I, _P, _P, _P, _P, _P, _S,
+                                     _P]),
+    "spk_fst_conv_prespike": (_INT, [_P, _I, _I, _I, _I, _P, _I, _I, _I, _P, _I, _I, _P, _P, _P, _P]),
     "spk_sparse_code_workspace": (_S, [_I, _I, _I, _I, _I]),
     "spk_sparse_code": (_INT, [_P, _INT, _I, _I, _I, _I, _I, _INT, _P, _P, _I, _P, _S, _P]),
     "spk_sparse_from_dense_workspace": (_S, [_I, _I, _I, _I, _I]),

@@ -60,6 +60,44 @@ def strokes(n: int, seed: int = 0, size: int | tuple = 28) -> np.ndarray:
     return out
 
 
+def labelled_strokes(n: int, classes: int = 10, seed: int = 4, size: int = 28):
+    """``n`` images ``[n, size, size]`` u8 of ``classes`` seeded stroke
+    templates (2-3 lines / arcs each) with per-image jitter (shift of up to 2
+    px, control points moved by up to 1.5 px, width U[2, 3], intensity
+    U[180, 255]), and their labels ``[n]`` int64."""
+    rng = np.random.default_rng(seed)
+    h = w = int(size)
+    templates = []
+    for _ in range(classes):
+        parts = []
+        for _ in range(int(rng.integers(2, 4))):
+            if rng.random() < 0.5:
+                parts.append(("line", rng.uniform(0.2 * h, 0.8 * h, size=4)))
+            else:
+                a0 = rng.uniform(0, 2 * np.pi)
+                parts.append(("arc", np.array([*rng.uniform(0.35 * h, 0.65 * h, size=2), rng.uniform(0.15 * h, 0.3 * h),
+                                               a0, a0 + rng.uniform(0.6 * np.pi, 1.5 * np.pi)])))
+        templates.append(parts)
+    py, px = np.mgrid[0:h, 0:w].astype(np.float64) + 0.5
+    labels = rng.integers(0, classes, size=n).astype(np.int64)
+    out = np.zeros((n, h, w), dtype=np.uint8)
+    for i in range(n):
+        dy, dx = rng.uniform(-2.0, 2.0, size=2)
+        img = np.zeros((h, w), dtype=np.float64)
+        for kind, prm in templates[labels[i]]:
+            width, level = rng.uniform(2.0, 3.0), rng.uniform(180.0, 255.0)
+            if kind == "line":
+                y0, x0, y1, x1 = prm + rng.uniform(-1.5, 1.5, size=4) + np.array([dy, dx, dy, dx])
+                d = _segment_distance(py, px, y0, x0, y1, x1)
+            else:
+                cy, cx, r, a0, a1 = prm
+                d = _arc_distance(py, px, cy + dy + rng.uniform(-1.5, 1.5), cx + dx + rng.uniform(-1.5, 1.5),
+                                  r + rng.uniform(-1.0, 1.0), a0, a1)
+            img = np.maximum(img, level * np.clip(width / 2.0 + 0.5 - d, 0.0, 1.0))
+        out[i] = np.clip(np.rint(img), 0, 255).astype(np.uint8)
+    return out, labels
+
+
 def textures(n: int, seed: int = 2, size: int = 256) -> np.ndarray:
     """``n`` texture images ``[n, size, size]`` f32 in [0, 1]."""
     rng = np.random.default_rng(seed)
