@@ -101,9 +101,11 @@ __global__ void fst_pool_backward_kernel(const float *__restrict__ in, const flo
 // dL/dt_in.  CTA = (sample, block of cb channels); thread items = (channel,
 // input pixel), up to kItems per thread; the output times, gradients and
 // weights of zc maps at a time are staged in shared memory.  Per item the
-// maps and taps are summed in a fixed order (deterministic).
+// maps and taps are summed in a fixed order (deterministic).  UNIT: stride 1
+// (no divisibility tests).
 constexpr int kItems = 4, kGiThreads = 256;
 
+template <bool UNIT>
 __global__ void __launch_bounds__(kGiThreads) fst_conv_grad_in_kernel(
     const float *__restrict__ tin, const float *__restrict__ kern, const float *__restrict__ tout,
     const float *__restrict__ go, float *__restrict__ gi, int cin, int cout, Geo g, int cb, int zc)
@@ -153,20 +155,35 @@ __global__ void __launch_bounds__(kGiThreads) fst_conv_grad_in_kernel(
             for (int zz = 0; zz < nz; ++zz)
             {
                 const float *wz = s_w + (zz * cb + ic[u]) * KK;
+                const float *to = s_to + zz * P, *gz = s_go + zz * P;
                 for (int ky = 0; ky < g.kh; ++ky)
                 {
-                    const int ny = iy[u] + g.top - ky;
-                    if (ny < 0 || ny % g.sy) continue;
-                    const int oy = ny / g.sy;
-                    if (oy >= g.oh) continue;
+                    int oy = iy[u] + g.top - ky;
+                    if (UNIT)
+                    {
+                        if (oy < 0 || oy >= g.oh) continue;
+                    }
+                    else
+                    {
+                        if (oy < 0 || oy % g.sy) continue;
+                        oy /= g.sy;
+                        if (oy >= g.oh) continue;
+                    }
                     for (int kx = 0; kx < g.kw; ++kx)
                     {
-                        const int nx = ix[u] + g.left - kx;
-                        if (nx < 0 || nx % g.sx) continue;
-                        const int ox = nx / g.sx;
-                        if (ox >= g.ow) continue;
-                        const int p = zz * P + oy * g.ow + ox;
-                        if (ti[u] < s_to[p]) acc[u] = __fmaf_rn(wz[ky * g.kw + kx], s_go[p], acc[u]);
+                        int ox = ix[u] + g.left - kx;
+                        if (UNIT)
+                        {
+                            if (ox < 0 || ox >= g.ow) continue;
+                        }
+                        else
+                        {
+                            if (ox < 0 || ox % g.sx) continue;
+                            ox /= g.sx;
+                            if (ox >= g.ow) continue;
+                        }
+                        const int p = oy * g.ow + ox;
+                        if (ti[u] < to[p]) acc[u] = __fmaf_rn(wz[ky * g.kw + kx], gz[p], acc[u]);
                     }
                 }
             }
@@ -177,66 +194,96 @@ __global__ void __launch_bounds__(kGiThreads) fst_conv_grad_in_kernel(
         if (ic[u] >= 0) gi[(b * cin + c0 + ic[u]) * HW + iy[u] * g.w + ix[u]] = acc[u];
 }
 
-// dL/dW, first pass.  CTA = (map z, group of sb samples); thread = (weight
-// element, slice of the output pixels); FP64 sums; per-group partials
-// part[group][z][Cin*KH*KW] (the second pass adds the groups in order).
-constexpr int kGwThreads = 256, kGwChunk = 2048;
+// dL/dW, first pass.  CTA = (map z, group of sb samples, block of up to 2048
+// weight elements).  Work pairs =
+// (weight element, slice of the output rows): `slices` row slices per weight
+// so that the pairs fill the CTA's threads; each pair walks its rows and
+// columns (no divisions) and sums in FP64; the slices are then added in
+// order.  The sample's input times (when they fit) and a chunk of rows of
+// the map's output times and gradients are staged in shared memory.
+// Per-group partials part[group][z][Cin*KH*KW]; the second pass adds the
+// groups in order (deterministic).
+constexpr int kGwThreads = 256, kGwRounds = 8;
 
 __global__ void __launch_bounds__(kGwThreads) fst_conv_grad_w_kernel(const float *__restrict__ tin,
                                                                       const float *__restrict__ tout,
                                                                       const float *__restrict__ go,
                                                                       double *__restrict__ part, int64_t b, int cin,
-                                                                      int cout, Geo g, int sb)
+                                                                      int cout, Geo g, int sb, int slices, int rows,
+                                                                      int stage_in)
 {
-    __shared__ float s_to[kGwChunk], s_go[kGwChunk];
-    __shared__ double s_red[kGwThreads];
+    extern __shared__ double gsm[];
     const int z = blockIdx.x, grp = blockIdx.y;
-    const int KK = g.kh * g.kw, WK = cin * KK, P = g.oh * g.ow, HW = g.h * g.w;
-    const int slices = WK >= kGwThreads ? 1 : kGwThreads / WK;
-    const int sl = threadIdx.x / (WK >= kGwThreads ? kGwThreads : WK);
-    const bool lead = sl < slices;  // threads past slices * WK only help with staging
+    const int KK = g.kh * g.kw, WK = cin * KK, HW = g.h * g.w;
+    const int wk0 = blockIdx.z * (kGwThreads * kGwRounds), wkn = min(WK - wk0, kGwThreads * kGwRounds / slices);
+    const int pairs = wkn * slices;
+    double *s_red = gsm;                                              // [pairs]
+    float *s_to = reinterpret_cast<float *>(s_red + pairs);          // [rows * ow]
+    float *s_go = s_to + rows * g.ow;                                 // [rows * ow]
+    float *s_in = s_go + rows * g.ow;                                 // [cin * HW] when staged
     const int64_t s0 = int64_t(grp) * sb, s1 = min(b, s0 + sb);
-    for (int wk0 = 0; wk0 < WK; wk0 += (WK >= kGwThreads ? kGwThreads : WK))
+    double acc[kGwRounds];
+    int pc[kGwRounds], pky[kGwRounds], pkx[kGwRounds], psl[kGwRounds];
+#pragma unroll
+    for (int r = 0; r < kGwRounds; ++r)
     {
-        const int wk = wk0 + (WK >= kGwThreads ? threadIdx.x : threadIdx.x % WK);
-        const bool act = lead && wk < WK;
-        int c = 0, ky = 0, kx = 0;
-        if (act) c = wk / KK, ky = (wk % KK) / g.kw, kx = wk % g.kw;
-        double acc = 0.0;
-        for (int64_t s = s0; s < s1; ++s)
+        acc[r] = 0.0;
+        const int pi = threadIdx.x + r * kGwThreads;
+        psl[r] = -1;
+        if (pi < pairs)
         {
-            const float *ti = tin + (s * cin + c) * HW;
-            for (int p0 = 0; p0 < P; p0 += kGwChunk)
+            const int wk = wk0 + pi % wkn;
+            psl[r] = pi / wkn;
+            pc[r] = wk / KK, pky[r] = (wk % KK) / g.kw, pkx[r] = wk % g.kw;
+        }
+    }
+    for (int64_t s = s0; s < s1; ++s)
+    {
+        if (stage_in)
+        {
+            __syncthreads();
+            for (int i = threadIdx.x; i < cin * HW; i += kGwThreads) s_in[i] = tin[s * cin * HW + i];
+        }
+        for (int oy0 = 0; oy0 < g.oh; oy0 += rows)
+        {
+            const int nr = min(rows, g.oh - oy0);
+            __syncthreads();
+            for (int i = threadIdx.x; i < nr * g.ow; i += kGwThreads)
             {
-                const int np = min(kGwChunk, P - p0);
-                __syncthreads();
-                for (int i = threadIdx.x; i < np; i += kGwThreads)
+                const int64_t src = (s * cout + z) * int64_t(g.oh) * g.ow + int64_t(oy0) * g.ow + i;
+                s_to[i] = tout[src];
+                s_go[i] = go[src];
+            }
+            __syncthreads();
+#pragma unroll
+            for (int r = 0; r < kGwRounds; ++r)
+            {
+                if (psl[r] < 0) continue;
+                const float *ti = stage_in ? s_in + pc[r] * HW : tin + (s * cin + pc[r]) * HW;
+                // rows oy0 + j with j = slice index mod slices
+                for (int j = (psl[r] - oy0 % slices + slices) % slices; j < nr; j += slices)
                 {
-                    const int64_t src = (s * cout + z) * P + p0 + i;
-                    s_to[i] = tout[src];
-                    s_go[i] = go[src];
-                }
-                __syncthreads();
-                if (!act) continue;
-                for (int i = sl; i < np; i += slices)
-                {
-                    const int p = p0 + i, oy = p / g.ow, ox = p - oy * g.ow;
-                    const int iy = oy * g.sy - g.top + ky, ix = ox * g.sx - g.left + kx;
-                    if (iy < 0 || iy >= g.h || ix < 0 || ix >= g.w) continue;
-                    if (__ldg(ti + iy * g.w + ix) < s_to[i]) acc += double(s_go[i]);
+                    const int iy = (oy0 + j) * g.sy - g.top + pky[r];
+                    if (iy < 0 || iy >= g.h) continue;
+                    const float *trow = ti + iy * g.w;
+                    const float *to = s_to + j * g.ow, *gr = s_go + j * g.ow;
+                    int ix = pkx[r] - g.left;
+                    for (int ox = 0; ox < g.ow; ++ox, ix += g.sx)
+                        if (ix >= 0 && ix < g.w && trow[ix] < to[ox]) acc[r] += double(gr[ox]);
                 }
             }
         }
-        // sum the slices in order
-        __syncthreads();
-        s_red[threadIdx.x] = act ? acc : 0.0;
-        __syncthreads();
-        if (act && sl == 0)
-        {
-            double sum = 0.0;
-            for (int q = 0; q < slices; ++q) sum += s_red[threadIdx.x + q * WK];
-            part[(int64_t(grp) * cout + z) * WK + wk] = sum;
-        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kGwRounds; ++r)
+        if (psl[r] >= 0) s_red[threadIdx.x + r * kGwThreads] = acc[r];
+    __syncthreads();
+    for (int w = threadIdx.x; w < wkn; w += kGwThreads)
+    {
+        double sum = 0.0;
+        for (int q = 0; q < slices; ++q) sum += s_red[q * wkn + w];
+        part[(int64_t(grp) * cout + z) * WK + wk0 + w] = sum;
     }
 }
 
@@ -373,8 +420,13 @@ spk_status spk_fst_conv_backward(const float *t_in, int64_t b, int64_t cin, int6
             const int zc = int(std::min<int64_t>(cout, 12288 / per_z));
             SPK_REQUIRE(b <= 65535, "batch too large for one call (split it)");
             const dim3 grid(unsigned(ceil_div(cin, cb)), unsigned(b));
-            fst_conv_grad_in_kernel<<<grid, kGiThreads, size_t(zc) * per_z * 4, s>>>(
-                t_in, kernel, t_out, grad_out, grad_in, int(cin), int(cout), g, cb, zc);
+            const size_t smem = size_t(zc) * per_z * 4;
+            if (g.sy == 1 && g.sx == 1)
+                fst_conv_grad_in_kernel<true><<<grid, kGiThreads, smem, s>>>(t_in, kernel, t_out, grad_out, grad_in,
+                                                                               int(cin), int(cout), g, cb, zc);
+            else
+                fst_conv_grad_in_kernel<false><<<grid, kGiThreads, smem, s>>>(t_in, kernel, t_out, grad_out, grad_in,
+                                                                                int(cin), int(cout), g, cb, zc);
             SPK_LAUNCHED();
         }
         if (grad_kernel)
@@ -384,8 +436,19 @@ spk_status spk_fst_conv_backward(const float *t_in, int64_t b, int64_t cin, int6
             const int groups = int(ceil_div(b, kGwSamples));
             SPK_REQUIRE(groups <= 65535, "batch too large for one call (split it)");
             double *part = static_cast<double *>(workspace);
-            fst_conv_grad_w_kernel<<<dim3(unsigned(cout), unsigned(groups)), kGwThreads, 0, s>>>(
-                t_in, t_out, grad_out, part, b, int(cin), int(cout), g, kGwSamples);
+            // row slices per weight: enough pairs to fill the threads, at most one per row
+            const int64_t wk = cin * kh * kw, cap = int64_t(kGwThreads) * kGwRounds;
+            int slices = 1;  // a power of two
+            while (slices * 2 <= oh && wk * slices * 2 <= cap) slices *= 2;
+            const int64_t wblocks = ceil_div(wk, cap / slices);
+            SPK_REQUIRE(wblocks <= 65535, "kernel too large");
+            SPK_REQUIRE(ow <= 2048, "output rows are too wide for the kernel gradient");
+            const int rows = int(std::max<int64_t>(1, std::min<int64_t>(oh, 2048 / ow)));
+            const size_t base = size_t(std::min(wk, cap / slices) * slices) * 8 + size_t(2 * rows * ow) * 4;
+            const bool stage_in = base + size_t(cin * h * w) * 4 <= 48 * 1024;
+            const size_t smem = base + (stage_in ? size_t(cin * h * w) * 4 : 0);
+            fst_conv_grad_w_kernel<<<dim3(unsigned(cout), unsigned(groups), unsigned(wblocks)), kGwThreads, smem, s>>>(
+                t_in, t_out, grad_out, part, b, int(cin), int(cout), g, kGwSamples, slices, rows, stage_in ? 1 : 0);
             SPK_LAUNCHED();
             const int64_t n = cout * cin * kh * kw;
             fst_conv_grad_w_reduce_kernel<<<grid_for(n, 256), 256, 0, s>>>(part, grad_kernel, n, groups);

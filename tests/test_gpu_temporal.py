@@ -31,6 +31,8 @@ GEOS = [
     (4, 32, 14, 14, 16, 3, (1, 1), (1, 1, 1, 1), 64),
     (5, 70, 1, 1, 10, 1, (1, 1), (0, 0, 0, 0), 32),  # fc as a 1x1 conv
     (2, 1, 28, 28, 8, 5, (1, 1), (2, 2, 2, 2), 64),
+    (3, 3136, 1, 1, 10, 1, (1, 1), (0, 0, 0, 0), 64),  # the network's fc: two weight blocks
+    (2, 64, 14, 14, 8, 3, (1, 1), (1, 1, 1, 1), 32),  # input times read from global memory
 ]
 
 
