@@ -577,6 +577,96 @@ def backprop_arm(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+# ----------------------------------------------------------------------------
+# Hyperparameter sweep (--workload sweep)
+# ----------------------------------------------------------------------------
+SWEEP_WORKLOAD = ("sweep: 32 independent 2-layer STDP networks x 512 stroke images of side 20/28/40/64, T=15, "
+                  "conv1 30x5x5 + conv2 100x5x5, per-network threshold U[8,20] and a+ U[0.001,0.01], a- = -0.75 a+")
+
+
+def sweep_arm(args, rank, world):
+    """All networks' training step: per size one multi-network fused launch
+    per layer and one multi-network STDP scan per layer, captured once as a
+    CUDA graph and replayed; schedules picked by the autotuner."""
+    import torch
+
+    import spyker_b200 as spyker
+    from spyker_b200 import sweep
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    nets = 32
+    images = 512 if args.batch == BATCH else args.batch
+    sw = sweep.Sweep(nets=nets, images=images, seed=10 * rank, device=dev, precision=args.precision, tune=True)
+    sw.capture()
+    for _ in range(max(args.warmup - 1, 0)):
+        sw.replay()
+    torch.cuda.synchronize()
+    l0 = spyker._lib.lib.spk_launch_count()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(dev.index) as clk:
+        torch.cuda.synchronize()
+        a.record()
+        for _ in range(args.steps):
+            sw.replay()
+        b.record()
+        torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / args.steps
+    # launches inside one graph (counted while capturing a second one)
+    l1 = spyker._lib.lib.spk_launch_count()
+    g2 = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g2):
+        sw.step()
+    launches = spyker._lib.lib.spk_launch_count() - l1
+    del g2
+    # eager step (no graph) for comparison
+    e_a, e_b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e_a.record()
+    sw.step()
+    e_b.record()
+    torch.cuda.synchronize()
+    eager_ms = e_a.elapsed_time(e_b)
+    # end to end: pinned host images into the graph's inputs, features back
+    h2d = sum(int(g.host.numel()) for g in sw.groups)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(args.steps):
+        for g in sw.groups:
+            g.images.copy_(g.host.to(dev, non_blocking=True).float().div_(255.0)[:, None])
+        feats = [f.cpu() for f in sw.replay()]
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / args.steps
+    n_img = sw.images_per_step
+    flops = sum(
+        sum(len(g.per_net[n][1]) for n in range(nets)) * 2 * 15 * (g.size ** 2 * 30 * 50 + (g.size // 2) ** 2 * 100 * 750)
+        for g in sw.groups)
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    peak = peaks.get("bf16_tflops_sustained", 1390.0)
+    achieved = flops / (ms * 1e-3) / 1e12
+    print(json.dumps({
+        "metric": "images/s (32-network STDP sweep, train + fwd) on 1 B200",
+        "value": n_img / (ms * 1e-3), "unit": "images/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": {"fp32": "f32", "bf16x2": "bf16x2-split/f32-acc", "bf16x3": "bf16x3-split/f32-acc"}[args.precision],
+        "data": "synthetic (seeded stroke images of 4 sizes)",
+        "config": {"workload": SWEEP_WORKLOAD, "global_batch": n_img, "seq_len": 15, "parallelism": "replicas1",
+                   "networks": nets, "padded_samples": sw.total, "cuda_graph": True,
+                   "schedules": {f"{sw.groups[g].size}px/layer{l + 1}": list(v) for (g, l), v in sw.schedules.items()},
+                   "l2": "inputs larger than L2: 2.0 GB of layer-1 spikes per step"},
+        "e2e": {"value": n_img / (e2e_ms * 1e-3), "unit": "images/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": int(sum(f.numel() for f in feats))},
+        "gpu_launches": int(launches),
+        "eager_step_ms": eager_ms,
+        "roofline": {"bound": "tensor", "kernel": "all fused layers (algorithmic conv FLOPs of the real images)",
+                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                     "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained (of measured)"},
+        "clocks": clk.summary(),
+    }), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -590,9 +680,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32-compare", action="store_true")
     ap.add_argument("--no-spike-match", action="store_true")
-    ap.add_argument("--workload", default="kheradpisheh", choices=["kheradpisheh", "gabor256", "backprop"],
+    ap.add_argument("--workload", default="kheradpisheh", choices=["kheradpisheh", "gabor256", "backprop", "sweep"],
                     help="kheradpisheh: the 2-layer STDP training step (the headline); gabor256: large-image "
-                         "forward; backprop: temporal-backprop training of a 3-layer first-spike network")
+                         "forward; backprop: temporal-backprop training of a 3-layer first-spike network; "
+                         "sweep: 32 STDP networks on uneven image sizes in one CUDA graph")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", args.gpus if args.impl == "reference" else 1))
@@ -602,6 +693,8 @@ def main():
         gabor_arm(args, rank, world)
     elif args.workload == "backprop":
         backprop_arm(args, rank, world)
+    elif args.workload == "sweep":
+        sweep_arm(args, rank, world)
     else:
         gpu_arm(args, rank, world)
 

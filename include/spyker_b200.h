@@ -85,6 +85,12 @@ int spk_device_status(int reset);
  * channel decision was within the FP32 error bound and was recomputed with
  * FP64 sums, since the last reset.  Synchronous; reset != 0 clears it. */
 unsigned long long spk_recheck_count(int reset);
+/* Schedule of the tensor-core conv / fused-layer kernels for the calls that
+ * follow (0 = automatic): pipeline stages (2..6, capped by shared memory),
+ * tensor-memory accumulators (1 or 2, where 2 fit), resident CTAs per SM.
+ * Results do not depend on it; an autotuner picks it per layer shape.
+ * Process-wide (not thread-safe). */
+spk_status spk_set_conv_schedule(int stages, int nacc, int ctas_per_sm);
 
 /* ---- host-side kernel generation (src/spyker/cpu/init.cpp) -------------- */
 /* Global generator: replaces Core::random_seed (src/spyker/impl.cpp:37-43). */
@@ -198,6 +204,18 @@ spk_status spk_stdp_scan(float *kernel, int64_t nmaps, int64_t k, int64_t b, int
                          const int32_t *winners, const int32_t *counts, const uint16_t *pre, int64_t pre_sample_stride,
                          int64_t pre_slot_stride, const uint16_t *post, const double *configs_host, int64_t nconf,
                          int f32_rule, spk_stream stream);
+/* The scan of several networks in one launch (kernels [N, maps, k]): network
+ * n walks the samples order[net_offsets[n] .. net_offsets[n+1]) (global sample
+ * indexes into winners / counts / pre / post; null order = the range itself)
+ * in that order with its configs net_configs[n][nconf][5] (positive, negative,
+ * stabilize, lower, upper).  net_offsets, order and net_configs are device
+ * arrays.  Each network's update equals spk_stdp_scan over its samples in
+ * that order (the reference's per-sample sequential rule, cpu/stdp.cpp:99-169). */
+spk_status spk_stdp_scan_nets(float *kernels, int64_t nnets, int64_t nmaps, int64_t k, int64_t b, int64_t count,
+                              int64_t field, const int32_t *winners, const int32_t *counts, const uint16_t *pre,
+                              int64_t pre_sample_stride, int64_t pre_slot_stride, const uint16_t *post,
+                              const int64_t *net_offsets, const int32_t *order, const double *net_configs,
+                              int64_t nconf, int f32_rule, spk_stream stream);
 size_t spk_rank_fcstdp_workspace(int64_t b, int64_t t, int64_t ni);
 /* in [B, T, I], kernel [O, I] F32 in place, out [B, T, O] (cpu/stdp.cpp:42-97). */
 spk_status spk_rank_fcstdp(const void *in, spk_dtype itype, int64_t b, int64_t t, int64_t ni, float *kernel,
@@ -239,6 +257,25 @@ spk_status spk_conv_fire_wta(const void *in, spk_dtype itype, const float *kerne
                              double fire_threshold, int64_t ry, int64_t rx, int64_t count, double wta_threshold,
                              uint8_t *spikes, int32_t *winners, int32_t *counts, int64_t pool_ky, int64_t pool_kx,
                              uint8_t *pooled, int precision, void *ws, size_t ws_bytes, spk_stream stream);
+/* Several networks in one launch (a hyperparameter sweep): kernels
+ * [N, Cout, Cin, KH, KW]; samples net_offsets_host[n] .. [n+1] belong to
+ * network n (host array, checked: each network must start on a tile, i.e.
+ * net_offsets[n] * OH * OW a multiple of 128 / pow2ceil(T), so pad batches);
+ * sample_net [B] int32 and net_threshold [N] F32 are device arrays (the
+ * threshold of Core::threshold per network; the other thresholds shared).
+ * Per sample the results equal spk_conv_fire_wta with that network's kernel
+ * and threshold. */
+size_t spk_conv_fire_wta_nets_workspace(int64_t nnets, int64_t b, int64_t t, int64_t cin, int64_t h, int64_t w,
+                                        int64_t cout, int64_t kh, int64_t kw, int64_t sy, int64_t sx,
+                                        const int64_t *pad4_host, int precision);
+spk_status spk_conv_fire_wta_nets(const void *in, spk_dtype itype, const float *kernels, int64_t nnets,
+                                  const int64_t *net_offsets_host, const int32_t *sample_net,
+                                  const float *net_threshold, int64_t b, int64_t t, int64_t cin, int64_t h, int64_t w,
+                                  int64_t cout, int64_t kh, int64_t kw, int64_t sy, int64_t sx,
+                                  const int64_t *pad4_host, double value, double inhibit_threshold,
+                                  double fire_threshold, int64_t ry, int64_t rx, int64_t count, double wta_threshold,
+                                  uint8_t *spikes, int32_t *winners, int32_t *counts, int64_t pool_ky, int64_t pool_kx,
+                                  uint8_t *pooled, int precision, void *ws, size_t ws_bytes, spk_stream stream);
 
 /* ---- fully connected (Core::fc / signfc, impl.h:228-236) ---------------- */
 /* in [R, I] (U8 or F32), kernel [O, I] F32 -> out [R, O] F32. */

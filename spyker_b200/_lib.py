@@ -25,6 +25,7 @@ SIGNATURES = {
     "spk_launch_count": (C.c_uint64, []),
     "spk_device_status": (_INT, [_INT]),
     "spk_recheck_count": (C.c_ulonglong, [_INT]),
+    "spk_set_conv_schedule": (_INT, [_INT, _INT, _INT]),
     "spk_random_seed": (None, [C.c_uint64]),
     "spk_normal_kernel": (_INT, [_P, _I, _D, _D]),
     "spk_gaussian_kernel": (_INT, [_P, _I, _D]),
@@ -53,6 +54,10 @@ SIGNATURES = {
     "spk_rank_convstdp_prepost": (_INT, [_P, _INT, _I, _I, _I, _I, _I, _I, _I, _I, _P, _I, _I, _P, _P, _I, _I, _I, _P,
                                          _P, _P, _P, _S, _P]),
     "spk_stdp_scan": (_INT, [_P, _I, _I, _I, _I, _I, _P, _P, _P, _I, _I, _P, _P, _I, _INT, _P]),
+    "spk_stdp_scan_nets": (_INT, [_P, _I, _I, _I, _I, _I, _I, _P, _P, _P, _I, _I, _P, _P, _P, _P, _I, _INT, _P]),
+    "spk_conv_fire_wta_nets_workspace": (_S, [_I, _I, _I, _I, _I, _I, _I, _I, _I, _I, _I, _P, _INT]),
+    "spk_conv_fire_wta_nets": (_INT, [_P, _INT, _P, _I, _P, _P, _P, _I, _I, _I, _I, _I, _I, _I, _I, _I, _I, _P, _D,
+                                      _D, _D, _I, _I, _I, _D, _P, _P, _P, _I, _I, _P, _INT, _P, _S, _P]),
     "spk_rank_fcstdp_workspace": (_S, [_I, _I, _I]),
     "spk_rank_fcstdp": (_INT, [_P, _INT, _I, _I, _I, _P, _I, _P, _P, _I, _P, _P, _I, _P, _S, _P]),
     "spk_conv_workspace": (_S, [_I, _I, _I, _I, _I, _I, _I, _INT]),

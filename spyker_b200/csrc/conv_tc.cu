@@ -76,6 +76,12 @@ struct TcParams
     // from `raw` [B, T, Cin, H, W] instead
     const uint8_t *raw;
     const int *flag;
+    // several networks in one launch (snet null: one network): network of
+    // each sample, each network's threshold, byte stride between the
+    // networks' weight images.  No tile holds pixels of two networks.
+    const int32_t *snet;
+    const float *net_thr;
+    int64_t wimg_stride;
 };
 
 constexpr int kPotentials = 0, kFused = 1;
@@ -145,8 +151,12 @@ __global__ void to_channels_last_kernel(const uint8_t *__restrict__ in, uint2 *_
 // no-swizzle layout (8-row groups of 1024 B, 8 K-chunks of 128 B, 16 B per
 // row), K ordered as the A operand.  One thread per (tile, block, row, chunk).
 __global__ void split_weights_kernel(const float *__restrict__ kernel, uint4 *__restrict__ wimg, int cout, int cin,
-                                     int taps, int nhwc, int cpad, int kblocks, int n_tile, int n_tiles, int nsplit)
+                                     int taps, int nhwc, int cpad, int kblocks, int n_tile, int n_tiles, int nsplit,
+                                     int64_t wimg_stride16)
 {
+    // blockIdx.y: network (kernels [N, Cout, Cin, KH, KW], images wimg_stride16 uint4 apart)
+    kernel += int64_t(blockIdx.y) * cout * cin * taps;
+    wimg += int64_t(blockIdx.y) * wimg_stride16;
     const int64_t total = int64_t(n_tiles) * kblocks * n_tile * 8;
     const int kreal = nhwc ? taps * cpad : taps * cin;
     for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += int64_t(gridDim.x) * blockDim.x)
@@ -293,7 +303,8 @@ __device__ __forceinline__ void tmem_chunk_wait(uint32_t (&q)[3][kEpiChunk])
 // channel, the largest |h| + |m| + |l| and the closest distance to the
 // threshold.  Branch-free.
 template <int NS>
-__device__ __forceinline__ void fast_chunk(const TcParams &P, const uint32_t (&q)[3][kEpiChunk], int c0, FastMax &st)
+__device__ __forceinline__ void fast_chunk(const TcParams &P, float thr, const uint32_t (&q)[3][kEpiChunk], int c0,
+                                           FastMax &st)
 {
 #pragma unroll
     for (int j = 0; j < kEpiChunk; ++j)
@@ -304,10 +315,10 @@ __device__ __forceinline__ void fast_chunk(const TcParams &P, const uint32_t (&q
         const float f = __fadd_rn(__fadd_rn(h, m), l);
         const float a = __fadd_rn(__fadd_rn(fabsf(h), fabsf(m)), fabsf(l));
         const bool valid = c < P.cout;
-        const bool real = valid && f > P.thr;
+        const bool real = valid && f > thr;
         const bool gt = real && f > st.r1;
         st.amax = valid ? fmaxf(st.amax, a) : st.amax;
-        st.dmin = valid ? fminf(st.dmin, fabsf(__fsub_rn(f, P.thr))) : st.dmin;
+        st.dmin = valid ? fminf(st.dmin, fabsf(__fsub_rn(f, thr))) : st.dmin;
         st.r2 = gt ? st.r1 : (real ? fmaxf(st.r2, f) : st.r2);
         st.r1 = gt ? f : st.r1;
         st.a1 = gt ? c : st.a1;
@@ -326,7 +337,8 @@ __device__ __forceinline__ void fast_chunk(const TcParams &P, const uint32_t (&q
 // next chunk are in flight while a chunk is processed; even and odd chunks
 // keep separate states (two independent dependency chains), merged at the end.
 template <int NS>
-__device__ __forceinline__ void row_argmax(const TcParams &P, uint32_t lane_base, bool row_ok, int &am, float &xam)
+__device__ __forceinline__ void row_argmax(const TcParams &P, float thr, uint32_t lane_base, bool row_ok, int &am,
+                                           float &xam)
 {
     FastMax st, st2;
     constexpr int W = kEpiChunk;
@@ -337,10 +349,10 @@ __device__ __forceinline__ void row_argmax(const TcParams &P, uint32_t lane_base
         // n_tile is a multiple of 16 = 2 W: both halves exist
         tmem_chunk_wait<NS>(qa);
         tmem_chunk<NS>(lane_base, c0 + W, P.n_tile, qb);
-        fast_chunk<NS>(P, qa, c0, st);
+        fast_chunk<NS>(P, thr, qa, c0, st);
         tmem_chunk_wait<NS>(qb);
         if (c0 + 2 * W < P.n_tile) tmem_chunk<NS>(lane_base, c0 + 2 * W, P.n_tile, qa);
-        fast_chunk<NS>(P, qb, c0 + W, st2);
+        fast_chunk<NS>(P, thr, qb, c0 + W, st2);
     }
     merge_fast(st, st2);
     const float tol = __fmaf_rn(st.amax, 0x1p-21f, 0x1p-140f);
@@ -366,7 +378,7 @@ __device__ __forceinline__ void row_argmax(const TcParams &P, uint32_t lane_base
             for (int j = 0; j < 16; ++j)
             {
                 const int c = c0 + j;
-                const float x = (v[j] <= P.thr) ? P.thv : v[j];
+                const float x = (v[j] <= thr) ? P.thv : v[j];
                 if (c == 0)
                     mx = x;
                 else if (c < P.cout && x > mx)
@@ -386,8 +398,8 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar)
 // last tensor-memory load of the tile has completed, so the next tile's MMAs
 // overlap the stores below.
 template <int NS>
-__device__ void fused_epilogue(const TcParams &P, uint32_t acc, bool row_ok, int tstep, int64_t sample, int64_t pix,
-                               uint64_t *release)
+__device__ void fused_epilogue(const TcParams &P, float thr, uint32_t acc, bool row_ok, int tstep, int64_t sample,
+                               int64_t pix, uint64_t *release)
 {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int TP = 1 << P.tp_log2, T = P.T, C = P.cout;
@@ -395,7 +407,7 @@ __device__ void fused_epilogue(const TcParams &P, uint32_t acc, bool row_ok, int
     // thresholded first-max channel of this (pixel, step)
     float mx;
     int am;
-    row_argmax<NS>(P, lane_base, row_ok, am, mx);
+    row_argmax<NS>(P, thr, lane_base, row_ok, am, mx);
     const int base = (lane >> P.tp_log2) << P.tp_log2;  // first lane of this pixel
     const unsigned grp = (TP == 32) ? 0xffffffffu : (((1u << TP) - 1u) << base);
     const unsigned above = __ballot_sync(0xffffffffu, row_ok && mx > P.inh_thr) & grp;
@@ -441,7 +453,7 @@ __device__ void fused_epilogue(const TcParams &P, uint32_t acc, bool row_ok, int
     double accv = double(__uint_as_float(pieces[0])) + double(__uint_as_float(pieces[1]));
     if (NS == 3) accv += double(__uint_as_float(pieces[2]));
     const float raw = float(accv);
-    const float vw = (raw <= P.thr) ? P.thv : raw;
+    const float vw = (raw <= thr) ? P.thv : raw;
     // spike of the winning channel (the spike tensor was zero-filled first)
     if (row_ok && vw > P.fire_thr)
     {
@@ -731,6 +743,8 @@ __device__ __forceinline__ void fused_producer(const TcParams &P, const int4 *ta
 #pragma unroll
         for (int i = 0; i < NU; ++i)
             if (p + i * 256 < units) fu[i] = fused_pixel(P, tile, upl[i]);
+        const uint8_t *wbase = P.wimg;
+        if (P.snet) wbase += P.snet[(uint32_t(tile) * uint32_t(P.pp)) / uint32_t(P.ohw)] * P.wimg_stride;
         for (int kb = 0; kb < P.kblocks; ++kb, ++it)
         {
             // the loads are in flight while waiting for the stage
@@ -750,7 +764,7 @@ __device__ __forceinline__ void fused_producer(const TcParams &P, const int4 *ta
             if (p == 0)
             {
                 arrive_expect_tx(&full_bar[s], uint32_t(b_bytes));
-                bulk_g2s(sA + a_bytes, P.wimg + int64_t(kb) * b_bytes, uint32_t(b_bytes), &full_bar[s]);
+                bulk_g2s(sA + a_bytes, wbase + int64_t(kb) * b_bytes, uint32_t(b_bytes), &full_bar[s]);
             }
 #pragma unroll
             for (int i = 0; i < NU; ++i)
@@ -996,10 +1010,12 @@ __global__ void __launch_bounds__(kWsThreads, 1) conv_ws_kernel(TcParams P)
             }
             if constexpr (MODE == kFused)
             {
+                float thr = P.thr;
+                if (P.snet) thr = P.net_thr[P.snet[(uint32_t(mt) * uint32_t(P.pp)) / uint32_t(P.ohw)]];
                 if (P.nsplit == 3)
-                    fused_epilogue<3>(P, acc, r.ok, r.tstep, r.sample, r.pix, &acce_bar[a]);
+                    fused_epilogue<3>(P, thr, acc, r.ok, r.tstep, r.sample, r.pix, &acce_bar[a]);
                 else
-                    fused_epilogue<2>(P, acc, r.ok, r.tstep, r.sample, r.pix, &acce_bar[a]);
+                    fused_epilogue<2>(P, thr, acc, r.ok, r.tstep, r.sample, r.pix, &acce_bar[a]);
             }
             else
             {
@@ -1087,6 +1103,15 @@ __global__ void wta_records_kernel(const int4 *__restrict__ records, const unsig
 
 inline size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 
+// Schedule overrides of the tensor-core kernels (0 = automatic), set by an
+// autotuner through spk_set_conv_schedule: pipeline stages, accumulators,
+// resident CTAs per SM.
+struct Schedule
+{
+    int stages = 0, nacc = 0, ctas = 0;
+};
+Schedule g_schedule;
+
 struct Plan
 {
     int nsplit, n_tile, n_tiles, kblocks, cpad, stages, nacc;
@@ -1113,6 +1138,7 @@ Plan make_plan(int64_t n, int64_t cin, int64_t h, int64_t w, int64_t cout, int64
     // next) when they fit in the 512 tensor-memory columns
     const uint32_t acc_cols = uint32_t(pl.nsplit * pl.n_tile);
     pl.nacc = 2 * acc_cols <= 512 ? 2 : 1;
+    if (g_schedule.nacc == 1) pl.nacc = 1;
     uint32_t cols = 32;
     while (cols < pl.nacc * acc_cols) cols <<= 1;
     pl.tmem_cols = cols;
@@ -1128,7 +1154,7 @@ Plan make_plan(int64_t n, int64_t cin, int64_t h, int64_t w, int64_t cout, int64
                                     : size_t(pl.kblocks) * 8 * 16;
     const size_t stage = size_t(BM * BK * 2) + size_t(pl.nsplit) * pl.n_tile * BK * 2;
     const size_t budget = 225 * 1024 - tab;
-    pl.stages = int(std::min<size_t>(4, budget / stage));
+    pl.stages = int(std::min<size_t>(g_schedule.stages > 0 ? size_t(g_schedule.stages) : 4, budget / stage));
     size_t smem = size_t(pl.stages) * stage + tab;
     // At most 512 / tmem_cols CTAs may share an SM's tensor memory: size the
     // shared memory so that no more fit.
@@ -1250,20 +1276,23 @@ __global__ void __launch_bounds__(256) fst_stage_words_kernel(const uint8_t *__r
 // t_fused > 0: stage for the fused (pixel, time) rows of t_fused steps.
 TcParams prepare(const Plan &pl, const void *in, const float *kernel, int64_t n, int64_t cin, int64_t h, int64_t w,
                  int64_t cout, int64_t kh, int64_t kw, int64_t sy, int64_t sx, Pad4 p, int64_t oh, int64_t ow,
-                 uint8_t *ws, cudaStream_t s, int64_t t_fused = 0)
+                 uint8_t *ws, cudaStream_t s, int64_t t_fused = 0, int64_t nnets = 1)
 {
     SPK_REQUIRE(pl.kblocks <= kMaxKBlocks, "Cin*KH*KW is too large for the tensor-core path");
     SPK_REQUIRE(pl.stages >= 2 && pl.smem <= 227 * 1024, "tile does not fit in shared memory");
     SPK_REQUIRE((reinterpret_cast<uintptr_t>(ws) & 255) == 0, "workspace must be 256-byte aligned");
     uint8_t *wimg = ws;
     const int64_t wthreads = int64_t(pl.n_tiles) * pl.kblocks * pl.n_tile * 8;
-    split_weights_kernel<<<grid_for(wthreads, 256), 256, 0, s>>>(kernel, reinterpret_cast<uint4 *>(wimg), int(cout),
-                                                                int(cin), int(kh * kw), pl.nhwc ? 1 : 0, pl.cpad,
-                                                                pl.kblocks, pl.n_tile, pl.n_tiles, pl.nsplit);
+    SPK_REQUIRE(nnets >= 1 && nnets <= 65535, "invalid number of networks");
+    const dim3 sgrid(grid_for(wthreads, 256), unsigned(nnets));
+    split_weights_kernel<<<sgrid, 256, 0, s>>>(kernel, reinterpret_cast<uint4 *>(wimg), int(cout), int(cin),
+                                               int(kh * kw), pl.nhwc ? 1 : 0, pl.cpad, pl.kblocks, pl.n_tile,
+                                               pl.n_tiles, pl.nsplit, int64_t(align256(pl.wimg_bytes) / 16));
     SPK_LAUNCHED();
     const uint8_t *a_src = static_cast<const uint8_t *>(in);
     TcParams P{};
-    uint8_t *xt = wimg + align256(pl.wimg_bytes);
+    P.wimg_stride = int64_t(align256(pl.wimg_bytes));
+    uint8_t *xt = wimg + size_t(nnets) * align256(pl.wimg_bytes);
     if (t_fused > 0)
     {
         const int64_t b = n / t_fused, cp = pl.nhwc ? pl.cpad : cin;
@@ -1322,6 +1351,7 @@ void launch(const TcParams &P, const Plan &pl, cudaStream_t s)
     int per_sm = 1;
     SPK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, ws_threads(MODE), pl.smem));
     per_sm = std::max(1, std::min<int>(per_sm, int(512 / pl.tmem_cols)));
+    if (g_schedule.ctas > 0) per_sm = std::min(per_sm, g_schedule.ctas);
     const int64_t grid = std::min<int64_t>(P.tiles, int64_t(sm_count()) * per_sm);
     kern<<<unsigned(grid), ws_threads(MODE), pl.smem, s>>>(P);
     SPK_LAUNCHED();
@@ -1336,7 +1366,7 @@ struct FusedLayout
 };
 
 FusedLayout fused_layout(int64_t b, int64_t t, int64_t cin, int64_t h, int64_t w, int64_t cout, int64_t kh, int64_t kw,
-                         int64_t sy, int64_t sx, Pad4 p, int precision)
+                         int64_t sy, int64_t sx, Pad4 p, int precision, int64_t nnets = 1)
 {
     FusedLayout L{};
     L.oh = (h + p.top + p.bottom - kh) / sy + 1;
@@ -1347,7 +1377,7 @@ FusedLayout fused_layout(int64_t b, int64_t t, int64_t cin, int64_t h, int64_t w
     L.tp_log2 = lg;
     L.pp = BM / tp;
     L.npix = b * L.oh * L.ow;
-    size_t off = align256(L.pl.wimg_bytes) + align256(L.pl.xt_bytes);
+    size_t off = size_t(nnets) * align256(L.pl.wimg_bytes) + align256(L.pl.xt_bytes);
     L.rec_off = off;
     off += align256(size_t(L.npix) * 16);
     L.min_off = off;
@@ -1384,6 +1414,16 @@ void conv_tc(const void *in, spk_dtype itype, const float *kernel, float *out, i
 using namespace spk;
 
 extern "C" {
+
+spk_status spk_set_conv_schedule(int stages, int nacc, int ctas_per_sm)
+{
+    return guarded([&] {
+        SPK_REQUIRE(stages == 0 || (stages >= 2 && stages <= kMaxStages), "stages must be 0 or 2..6");
+        SPK_REQUIRE(nacc == 0 || nacc == 1 || nacc == 2, "accumulators must be 0, 1 or 2");
+        SPK_REQUIRE(ctas_per_sm >= 0 && ctas_per_sm <= 4, "CTAs per SM must be 0..4");
+        g_schedule = Schedule{stages, nacc, ctas_per_sm};
+    });
+}
 
 unsigned long long spk_recheck_count(int reset)
 {
@@ -1425,6 +1465,95 @@ size_t spk_conv_fire_wta_workspace(int64_t b, int64_t t, int64_t cin, int64_t h,
     }
 }
 
+namespace
+{
+// Networks of a multi-network call: sample ranges on the host (checked),
+// sample -> network and per-network thresholds on the device.
+struct Nets
+{
+    int64_t n = 1;
+    const int64_t *offsets = nullptr;
+    const int32_t *sample_net = nullptr;
+    const float *threshold = nullptr;
+};
+
+void fused_layer(const void *in, spk_dtype itype, const float *kernel, int64_t b, int64_t t, int64_t cin, int64_t h,
+                 int64_t w, int64_t cout, int64_t kh, int64_t kw, int64_t sy, int64_t sx, const int64_t *pad4,
+                 double threshold, double value, double inhibit_threshold, double fire_threshold, int64_t ry,
+                 int64_t rx, int64_t count, double wta_threshold, uint8_t *spikes, int32_t *winners, int32_t *counts,
+                 int64_t pool_ky, int64_t pool_kx, uint8_t *pooled, int precision, void *ws, size_t ws_bytes,
+                 spk_stream stream, const Nets &nets)
+{
+    Pad4 p = pad_of(pad4);
+    SPK_REQUIRE(itype == SPK_U8, "the fused layer takes U8 spikes");
+    SPK_REQUIRE(precision == SPK_CONV_BF16X2 || precision == SPK_CONV_BF16X3, "the fused layer runs on tcgen05");
+    SPK_REQUIRE(b >= 0 && t >= 1 && t <= 32 && cin >= 1 && cout >= 2 && kh >= 1 && kw >= 1 && sy >= 1 && sx >= 1,
+                "the fused layer needs 1 <= T <= 32 and at least 2 output channels");
+    SPK_REQUIRE(fire_threshold >= 0 && wta_threshold >= 0, "the fused layer needs fire/WTA thresholds >= 0");
+    // count == 0: no winner selection (forward passes); winners and
+    // counts may then be null
+    SPK_REQUIRE(count >= 0 && ry >= 0 && rx >= 0, "invalid WTA radius or count");
+    SPK_REQUIRE(spikes != nullptr && (count == 0 || (winners != nullptr && counts != nullptr)), "null output");
+    FusedLayout L = fused_layout(b, t, cin, h, w, cout, kh, kw, sy, sx, p, precision, nets.n);
+    SPK_REQUIRE(L.oh > 0 && L.ow > 0, "input and kernel shapes are not compatible");
+    SPK_REQUIRE(L.pl.n_tiles == 1 && L.pl.nsplit * L.pl.n_tile <= 512, "too many output channels for one CTA");
+    SPK_REQUIRE(count == 0 || L.oh * L.ow <= 16384, "the fused WTA keeps at most 16384 pixels per sample");
+    SPK_REQUIRE(L.npix < (int64_t(1) << 31), "at most 2^31 - 1 output pixels per call");
+    SPK_REQUIRE(ws != nullptr && ws_bytes >= L.total, "workspace is too small");
+    if (nets.n > 1 || nets.offsets)
+    {
+        SPK_REQUIRE(nets.offsets != nullptr && nets.sample_net != nullptr && nets.threshold != nullptr,
+                    "null network tables");
+        SPK_REQUIRE(nets.offsets[0] == 0 && nets.offsets[nets.n] == b, "network offsets must span the batch");
+        for (int64_t q = 0; q < nets.n; ++q)
+        {
+            SPK_REQUIRE(nets.offsets[q] <= nets.offsets[q + 1], "network offsets must not decrease");
+            // a tile is pp consecutive output pixels: none may hold two networks
+            SPK_REQUIRE((nets.offsets[q] * L.oh * L.ow) % L.pp == 0,
+                        "each network's first output pixel must start a tile (pad the networks' batches)");
+        }
+    }
+    if (b == 0) return;
+    cudaStream_t s = stream_of(stream);
+    uint8_t *base = static_cast<uint8_t *>(ws);
+    TcParams P = prepare(L.pl, in, kernel, b * t, cin, h, w, cout, kh, kw, sy, sx, p, L.oh, L.ow, base, s, t, nets.n);
+    if (nets.offsets) P.snet = nets.sample_net, P.net_thr = nets.threshold;
+    P.T = int(t), P.tp_log2 = L.tp_log2, P.pp = L.pp, P.npix = L.npix;
+    int lp = 0;
+    while ((1 << lp) < L.pp) ++lp;
+    P.lp_log2 = lp;
+    P.thr = float(threshold), P.thv = float(value), P.inh_thr = float(inhibit_threshold);
+    P.fire_thr = float(fire_threshold), P.wta_thr = float(wta_threshold);
+    P.spikes = spikes;
+    int64_t poh = 0, pow_ = 0;
+    if (pool_ky > 0)
+    {
+        SPK_REQUIRE(pool_kx > 0 && pooled != nullptr, "pooling needs a window and an output");
+        poh = (L.oh - pool_ky) / pool_ky + 1, pow_ = (L.ow - pool_kx) / pool_kx + 1;
+        SPK_REQUIRE(L.oh >= pool_ky && L.ow >= pool_kx, "the pooling window is larger than the output");
+        P.pooled = pooled, P.pky = int(pool_ky), P.pkx = int(pool_kx), P.poh = int(poh), P.pow_ = int(pow_);
+    }
+    if (count > 0)
+    {
+        P.records = reinterpret_cast<int4 *>(base + L.rec_off);
+        P.mins = reinterpret_cast<unsigned *>(base + L.min_off);
+        P.maxs = reinterpret_cast<unsigned *>(base + L.max_off);
+        SPK_CUDA(cudaMemsetAsync(P.mins, 0xFF, size_t(b) * 4, s));
+        SPK_CUDA(cudaMemsetAsync(P.maxs, 0x00, size_t(b) * 4, s));
+    }
+    P.M = L.npix * (int64_t(1) << L.tp_log2);
+    P.tiles = ceil_div(L.npix, L.pp);
+    SPK_CUDA(cudaMemsetAsync(spikes, 0, size_t(b) * t * cout * L.oh * L.ow, s));
+    if (pool_ky > 0) SPK_CUDA(cudaMemsetAsync(pooled, 0, size_t(b) * t * cout * poh * pow_, s));
+    launch<kFused>(P, L.pl, s);
+    if (count == 0) return;
+    const int hw = int(L.oh * L.ow);
+    wta_records_kernel<<<unsigned(b), 256, size_t(hw) * 8, s>>>(P.records, P.mins, P.maxs, hw, int(L.ow), int(t),
+                                                                int(ry), int(rx), int(count), winners, counts);
+    SPK_LAUNCHED();
+}
+}  // namespace
+
 spk_status spk_conv_fire_wta(const void *in, spk_dtype itype, const float *kernel, int64_t b, int64_t t, int64_t cin,
                              int64_t h, int64_t w, int64_t cout, int64_t kh, int64_t kw, int64_t sy, int64_t sx,
                              const int64_t *pad4, double threshold, double value, double inhibit_threshold,
@@ -1433,59 +1562,45 @@ spk_status spk_conv_fire_wta(const void *in, spk_dtype itype, const float *kerne
                              uint8_t *pooled, int precision, void *ws, size_t ws_bytes, spk_stream stream)
 {
     return guarded([&] {
-        Pad4 p = pad_of(pad4);
-        SPK_REQUIRE(itype == SPK_U8, "the fused layer takes U8 spikes");
-        SPK_REQUIRE(precision == SPK_CONV_BF16X2 || precision == SPK_CONV_BF16X3, "the fused layer runs on tcgen05");
-        SPK_REQUIRE(b >= 0 && t >= 1 && t <= 32 && cin >= 1 && cout >= 2 && kh >= 1 && kw >= 1 && sy >= 1 && sx >= 1,
-                    "the fused layer needs 1 <= T <= 32 and at least 2 output channels");
-        SPK_REQUIRE(fire_threshold >= 0 && wta_threshold >= 0, "the fused layer needs fire/WTA thresholds >= 0");
-        // count == 0: no winner selection (forward passes); winners and
-        // counts may then be null
-        SPK_REQUIRE(count >= 0 && ry >= 0 && rx >= 0, "invalid WTA radius or count");
-        SPK_REQUIRE(spikes != nullptr && (count == 0 || (winners != nullptr && counts != nullptr)), "null output");
-        FusedLayout L = fused_layout(b, t, cin, h, w, cout, kh, kw, sy, sx, p, precision);
-        SPK_REQUIRE(L.oh > 0 && L.ow > 0, "input and kernel shapes are not compatible");
-        SPK_REQUIRE(L.pl.n_tiles == 1 && L.pl.nsplit * L.pl.n_tile <= 512, "too many output channels for one CTA");
-        SPK_REQUIRE(count == 0 || L.oh * L.ow <= 16384, "the fused WTA keeps at most 16384 pixels per sample");
-        SPK_REQUIRE(L.npix < (int64_t(1) << 31), "at most 2^31 - 1 output pixels per call");
-        SPK_REQUIRE(ws != nullptr && ws_bytes >= L.total, "workspace is too small");
-        if (b == 0) return;
-        cudaStream_t s = stream_of(stream);
-        uint8_t *base = static_cast<uint8_t *>(ws);
-        TcParams P = prepare(L.pl, in, kernel, b * t, cin, h, w, cout, kh, kw, sy, sx, p, L.oh, L.ow, base, s, t);
-        P.T = int(t), P.tp_log2 = L.tp_log2, P.pp = L.pp, P.npix = L.npix;
-        int lp = 0;
-        while ((1 << lp) < L.pp) ++lp;
-        P.lp_log2 = lp;
-        P.thr = float(threshold), P.thv = float(value), P.inh_thr = float(inhibit_threshold);
-        P.fire_thr = float(fire_threshold), P.wta_thr = float(wta_threshold);
-        P.spikes = spikes;
-        int64_t poh = 0, pow_ = 0;
-        if (pool_ky > 0)
-        {
-            SPK_REQUIRE(pool_kx > 0 && pooled != nullptr, "pooling needs a window and an output");
-            poh = (L.oh - pool_ky) / pool_ky + 1, pow_ = (L.ow - pool_kx) / pool_kx + 1;
-            SPK_REQUIRE(L.oh >= pool_ky && L.ow >= pool_kx, "the pooling window is larger than the output");
-            P.pooled = pooled, P.pky = int(pool_ky), P.pkx = int(pool_kx), P.poh = int(poh), P.pow_ = int(pow_);
-        }
-        if (count > 0)
-        {
-            P.records = reinterpret_cast<int4 *>(base + L.rec_off);
-            P.mins = reinterpret_cast<unsigned *>(base + L.min_off);
-            P.maxs = reinterpret_cast<unsigned *>(base + L.max_off);
-            SPK_CUDA(cudaMemsetAsync(P.mins, 0xFF, size_t(b) * 4, s));
-            SPK_CUDA(cudaMemsetAsync(P.maxs, 0x00, size_t(b) * 4, s));
-        }
-        P.M = L.npix * (int64_t(1) << L.tp_log2);
-        P.tiles = ceil_div(L.npix, L.pp);
-        SPK_CUDA(cudaMemsetAsync(spikes, 0, size_t(b) * t * cout * L.oh * L.ow, s));
-        if (pool_ky > 0) SPK_CUDA(cudaMemsetAsync(pooled, 0, size_t(b) * t * cout * poh * pow_, s));
-        launch<kFused>(P, L.pl, s);
-        if (count == 0) return;
-        const int hw = int(L.oh * L.ow);
-        wta_records_kernel<<<unsigned(b), 256, size_t(hw) * 8, s>>>(P.records, P.mins, P.maxs, hw, int(L.ow), int(t),
-                                                                    int(ry), int(rx), int(count), winners, counts);
-        SPK_LAUNCHED();
+        fused_layer(in, itype, kernel, b, t, cin, h, w, cout, kh, kw, sy, sx, pad4, threshold, value,
+                    inhibit_threshold, fire_threshold, ry, rx, count, wta_threshold, spikes, winners, counts, pool_ky,
+                    pool_kx, pooled, precision, ws, ws_bytes, stream, Nets{});
+    });
+}
+
+size_t spk_conv_fire_wta_nets_workspace(int64_t nnets, int64_t b, int64_t t, int64_t cin, int64_t h, int64_t w,
+                                        int64_t cout, int64_t kh, int64_t kw, int64_t sy, int64_t sx,
+                                        const int64_t *pad4, int precision)
+{
+    try
+    {
+        if (nnets < 1) return 0;
+        const FusedLayout L = fused_layout(b, t, cin, h, w, cout, kh, kw, sy, sx, pad_of(pad4), precision, nnets);
+        if (L.pl.n_tiles != 1 || L.pl.nsplit * L.pl.n_tile > 512) return 0;
+        return L.total;
+    }
+    catch (...)
+    {
+        return 0;
+    }
+}
+
+spk_status spk_conv_fire_wta_nets(const void *in, spk_dtype itype, const float *kernels, int64_t nnets,
+                                  const int64_t *net_offsets_host, const int32_t *sample_net,
+                                  const float *net_threshold, int64_t b, int64_t t, int64_t cin, int64_t h, int64_t w,
+                                  int64_t cout, int64_t kh, int64_t kw, int64_t sy, int64_t sx, const int64_t *pad4,
+                                  double value, double inhibit_threshold, double fire_threshold, int64_t ry,
+                                  int64_t rx, int64_t count, double wta_threshold, uint8_t *spikes, int32_t *winners,
+                                  int32_t *counts, int64_t pool_ky, int64_t pool_kx, uint8_t *pooled, int precision,
+                                  void *ws, size_t ws_bytes, spk_stream stream)
+{
+    return guarded([&] {
+        SPK_REQUIRE(nnets >= 1, "at least one network");
+        Nets nets;
+        nets.n = nnets, nets.offsets = net_offsets_host, nets.sample_net = sample_net, nets.threshold = net_threshold;
+        fused_layer(in, itype, kernels, b, t, cin, h, w, cout, kh, kw, sy, sx, pad4, 0.0, value, inhibit_threshold,
+                    fire_threshold, ry, rx, count, wta_threshold, spikes, winners, counts, pool_ky, pool_kx, pooled,
+                    precision, ws, ws_bytes, stream, nets);
     });
 }
 

@@ -268,12 +268,23 @@ __device__ __forceinline__ double stdp_chain(double w, int n, int64_t e, bool ac
     return w;
 }
 
-template <bool F32_RULE>
+// Several networks (NETS): blockIdx.z = network n with kernels
+// [N, maps, k], its samples order[noff[n] .. noff[n+1]) (or the range itself
+// when order is null) walked in that order, and its configs
+// net_cfg[n][nconf][5] (positive, negative, stabilize, lower, upper).
+struct NetScan
+{
+    const int64_t *noff;
+    const int32_t *order;
+    const double *net_cfg;
+};
+
+template <bool F32_RULE, bool NETS>
 __global__ void __launch_bounds__(kScanThreads)
     stdp_scan_kernel(float *__restrict__ kernel, int64_t k, int64_t b, int count, int field,
                      const int32_t *__restrict__ winners, const int32_t *__restrict__ counts,
                      const uint16_t *__restrict__ pre, int64_t ps, int64_t pw, const uint16_t *__restrict__ post,
-                     Configs cfg)
+                     Configs cfg, NetScan nets)
 {
     // per compacted winner: offset of its pre row, its post time, its config
     __shared__ int64_t s_off[kWinnerTile];
@@ -283,9 +294,23 @@ __global__ void __launch_bounds__(kScanThreads)
     __shared__ double s_pos[kMaxConfigs], s_neg[kMaxConfigs], s_lo[kMaxConfigs], s_hi[kMaxConfigs];
     __shared__ int s_stab[kMaxConfigs];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (tid < cfg.n)
+    int64_t s_first = 0;  // the network's first slot in order / first sample
+    if (NETS)
+    {
+        const int net = blockIdx.z;
+        s_first = nets.noff[net];
+        b = nets.noff[net + 1] - s_first;
+        kernel += int64_t(net) * gridDim.x * k;
+        if (tid < cfg.n)
+        {
+            const double *c = nets.net_cfg + (int64_t(net) * cfg.n + tid) * 5;
+            s_pos[tid] = c[0], s_neg[tid] = c[1], s_stab[tid] = c[2] != 0.0, s_lo[tid] = c[3], s_hi[tid] = c[4];
+        }
+    }
+    else if (tid < cfg.n)
         s_pos[tid] = cfg.pos[tid], s_neg[tid] = cfg.neg[tid], s_lo[tid] = cfg.lo[tid], s_hi[tid] = cfg.hi[tid],
         s_stab[tid] = cfg.stab[tid];
+    __syncthreads();
     const int map = blockIdx.x;
     const int64_t e = int64_t(blockIdx.y) * kScanThreads + tid;
     const bool act = e < k;
@@ -307,10 +332,12 @@ __global__ void __launch_bounds__(kScanThreads)
             c4[q] = 0, rr[q] = int32_t(r);
             if (r < total)
             {
-                const int smp = int(r) / count, j = int(r) - smp * count;  // r < 2^31
+                int smp = int(r) / count;
+                const int j = int(r) - smp * count;  // r < 2^31
+                if (NETS) smp = nets.order ? nets.order[s_first + smp] : int(s_first) + smp;
                 if (j < counts[smp])
                 {
-                    const int32_t *rec = winners + r * 5;
+                    const int32_t *rec = winners + (int64_t(smp) * count + j) * 5;
                     const int32_t c = rec[0];
                     if (rec[field] == map && c >= 0 && c < cfg.n) m4 |= 1u << q, c4[q] = uint8_t(c);
                 }
@@ -336,9 +363,11 @@ __global__ void __launch_bounds__(kScanThreads)
         for (int q = 0; q < per; ++q)
             if (m4 & (1u << q))
             {
-                const int r = rr[q], smp = r / count, j = r - smp * count;
+                const int r = rr[q], j = r - (r / count) * count;
+                int smp = r / count;
+                if (NETS) smp = nets.order ? nets.order[s_first + smp] : int(s_first) + smp;
                 s_off[before] = int64_t(smp) * ps + int64_t(j) * pw;
-                s_post[before] = post[r];
+                s_post[before] = post[int64_t(smp) * count + j];
                 s_cfg[before] = c4[q];
                 ++before;
             }
@@ -384,11 +413,33 @@ void launch_stdp_scan(float *kernel, int64_t k, int64_t nmaps, int64_t b, int64_
     SPK_REQUIRE(b * count < (int64_t(1) << 31), "at most 2^31 - 1 winner records");
     dim3 grid(unsigned(nmaps), unsigned(ceil_div(k, kScanThreads)));
     if (f32_rule)
-        stdp_scan_kernel<true><<<grid, kScanThreads, 0, s>>>(kernel, k, b, int(count), field, winners, counts, pre, ps,
-                                                            pw, post, cfg);
+        stdp_scan_kernel<true, false><<<grid, kScanThreads, 0, s>>>(kernel, k, b, int(count), field, winners, counts,
+                                                                   pre, ps, pw, post, cfg, NetScan{});
     else
-        stdp_scan_kernel<false><<<grid, kScanThreads, 0, s>>>(kernel, k, b, int(count), field, winners, counts, pre,
-                                                             ps, pw, post, cfg);
+        stdp_scan_kernel<false, false><<<grid, kScanThreads, 0, s>>>(kernel, k, b, int(count), field, winners, counts,
+                                                                    pre, ps, pw, post, cfg, NetScan{});
+    SPK_LAUNCHED();
+}
+
+// The scan of several networks in one launch (see NetScan).
+void launch_stdp_scan_nets(float *kernels, int64_t nnets, int64_t k, int64_t nmaps, int64_t b, int64_t count,
+                           int field, const int32_t *winners, const int32_t *counts, const uint16_t *pre, int64_t ps,
+                           int64_t pw, const uint16_t *post, const int64_t *noff, const int32_t *order,
+                           const double *net_cfg, int64_t nconf, bool f32_rule, cudaStream_t s)
+{
+    SPK_REQUIRE(nconf >= 1 && nconf <= kMaxConfigs, "1 to 16 STDP configs per network");
+    SPK_REQUIRE(nnets >= 1 && nnets <= 65535 && noff != nullptr && net_cfg != nullptr, "invalid network tables");
+    SPK_REQUIRE(b * count < (int64_t(1) << 31), "at most 2^31 - 1 winner records");
+    Configs cfg{};
+    cfg.n = int(nconf);
+    const NetScan nets{noff, order, net_cfg};
+    dim3 grid(unsigned(nmaps), unsigned(ceil_div(k, kScanThreads)), unsigned(nnets));
+    if (f32_rule)
+        stdp_scan_kernel<true, true><<<grid, kScanThreads, 0, s>>>(kernels, k, b, int(count), field, winners, counts,
+                                                                  pre, ps, pw, post, cfg, nets);
+    else
+        stdp_scan_kernel<false, true><<<grid, kScanThreads, 0, s>>>(kernels, k, b, int(count), field, winners, counts,
+                                                                   pre, ps, pw, post, cfg, nets);
     SPK_LAUNCHED();
 }
 
@@ -456,8 +507,8 @@ void convstdp_into(const void *in, spk_dtype itype, int64_t b, int64_t t, int64_
         throw Error(SPK_ERR_UNSUPPORTED, "STDP spikes must be U8 or F32");
     SPK_LAUNCHED();
     dim3 grid(unsigned(cout), unsigned(ceil_div(k, kScanThreads)));
-    stdp_scan_kernel<false><<<grid, kScanThreads, 0, s>>>(kernel, k, b, int(count), 2, winners, counts, pre, count * k, k,
-                                                   post, cfg);
+    stdp_scan_kernel<false, false><<<grid, kScanThreads, 0, s>>>(kernel, k, b, int(count), 2, winners, counts, pre,
+                                                                count * k, k, post, cfg, NetScan{});
     SPK_LAUNCHED();
 }
 }  // namespace spk
@@ -497,8 +548,8 @@ spk_status spk_rank_convstdp(const void *in, spk_dtype itype, int64_t b, int64_t
         conv_prepost(in, itype, b, t, cin, h, w, cout, kh, kw, out, oh, ow, winners, counts, count, sy, sx, p, fst,
                      pre, post, s);
         dim3 grid(unsigned(cout), unsigned(ceil_div(k, kScanThreads)));
-        stdp_scan_kernel<false><<<grid, kScanThreads, 0, s>>>(kernel, k, b, int(count), 2, winners, counts, pre, count * k, k,
-                                                       post, cfg);
+        stdp_scan_kernel<false, false><<<grid, kScanThreads, 0, s>>>(kernel, k, b, int(count), 2, winners, counts, pre,
+                                                                    count * k, k, post, cfg, NetScan{});
         SPK_LAUNCHED();
     });
 }
@@ -544,6 +595,23 @@ spk_status spk_stdp_scan(float *kernel, int64_t nmaps, int64_t k, int64_t b, int
     });
 }
 
+spk_status spk_stdp_scan_nets(float *kernels, int64_t nnets, int64_t nmaps, int64_t k, int64_t b, int64_t count,
+                              int64_t field, const int32_t *winners, const int32_t *counts, const uint16_t *pre,
+                              int64_t pre_sample_stride, int64_t pre_slot_stride, const uint16_t *post,
+                              const int64_t *net_offsets, const int32_t *order, const double *net_configs,
+                              int64_t nconf, int f32_rule, spk_stream stream)
+{
+    return guarded([&] {
+        SPK_REQUIRE(nmaps >= 1 && nmaps <= 65535 && k >= 1 && b >= 0 && count >= 1, "invalid dims");
+        SPK_REQUIRE(field == 2 || field == 4, "the map field is 2 (z, conv) or 4 (x, fc)");
+        SPK_REQUIRE(kernels && winners && counts && pre && post && net_offsets && net_configs, "null pointer");
+        if (b == 0) return;
+        launch_stdp_scan_nets(kernels, nnets, k, nmaps, b, count, int(field), winners, counts, pre, pre_sample_stride,
+                              pre_slot_stride, post, net_offsets, order, net_configs, nconf, f32_rule != 0,
+                              stream_of(stream));
+    });
+}
+
 size_t spk_rank_fcstdp_workspace(int64_t b, int64_t, int64_t ni)
 {
     // pre [B, I] + post [B, 64] (count is bounded by 64 on this path)
@@ -575,8 +643,8 @@ spk_status spk_rank_fcstdp(const void *in, spk_dtype itype, int64_t b, int64_t t
             throw Error(SPK_ERR_UNSUPPORTED, "STDP spikes must be U8 or F32");
         SPK_LAUNCHED();
         dim3 grid(unsigned(no), unsigned(ceil_div(ni, kScanThreads)));
-        stdp_scan_kernel<false><<<grid, kScanThreads, 0, s>>>(kernel, ni, b, int(count), 4, winners, counts, pre, ni, 0, post,
-                                                       cfg);
+        stdp_scan_kernel<false, false><<<grid, kScanThreads, 0, s>>>(kernel, ni, b, int(count), 4, winners, counts, pre,
+                                                                    ni, 0, post, cfg, NetScan{});
         SPK_LAUNCHED();
     });
 }
