@@ -667,6 +667,128 @@ def sweep_arm(args, rank, world):
     }), flush=True)
 
 
+# ----------------------------------------------------------------------------
+# Event-list (sparse) input path (--workload sparse)
+# ----------------------------------------------------------------------------
+SPARSE_WORKLOAD = ("sparse-2layer-stdp: 4096 x [2, 28, 28] event lists at 1/2/5 % density (seeded first-spike "
+                   "times), T=15, conv1 30x5x5 -> inhibit -> convwta(r3,k5) -> STDP -> pool 2 -> conv2 100x5x5 -> "
+                   "inhibit -> convwta(r1,k8) -> STDP")
+SPARSE_DENSITIES = (0.01, 0.02, 0.05)
+
+
+def _sparse_thresholds(d):
+    # the dense rank code of the stroke images fires about 20 % of its
+    # inputs: conv1's threshold follows the input density (at least one
+    # weight); conv2 sees the pooled layer-1 events and keeps its 10
+    return max(1.0, 15.0 * d / 0.2), 10.0
+
+
+def _sparse_times(n, d, seed):
+    rng = np.random.default_rng(seed)
+    t = rng.integers(0, T, size=(n, 2, 28, 28))
+    return np.where(rng.random((n, 2, 28, 28)) < d, t, T).astype(np.float32)
+
+
+def sparse_arm(args, rank, world):
+    """The 2-layer STDP step of the Kheradpisheh example on event lists
+    (Sparse::conv / inhibit / convwta / STDP / pool) at 1, 2 and 5 % input
+    density; the reference's own CPU sparse backend times a sample."""
+    import torch
+
+    import spyker_b200 as spyker
+    from spyker_b200 import sparse, synth
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    batch = args.batch
+    per_density = {}
+    launches = 0
+    for d in SPARSE_DENSITIES:
+        th1, th2 = _sparse_thresholds(d)
+        times = torch.from_numpy(_sparse_times(batch, d, 7 + rank)).to(dev)
+        dense = spyker.scatter(times.reshape(batch, -1), T).view(batch, T, 2, 28, 28)
+        ev = spyker.SparseTensor(dense, 0.0)
+        del dense
+        c1, c2 = spyker.Conv(2, 30, 5, pad=2, device=dev), spyker.Conv(30, 100, 5, pad=2, device=dev)
+        c1.kernel.copy_(torch.from_numpy(synth.conv_weights(30, 2, 5, seed=1)))
+        c2.kernel.copy_(torch.from_numpy(synth.conv_weights(100, 30, 5, seed=2)))
+        for c in (c1, c2):
+            c.stdpconfig = [spyker.STDPConfig(0.004, -0.003)]
+
+        def step():
+            o1 = sparse.inhibit(sparse.conv(ev, c1.kernel, th1, 1, 2))
+            w1 = sparse.convwta(o1, 3, 5)
+            sparse.stdp(c1, ev, w1)
+            q = sparse.pool(o1, 2)
+            o2 = sparse.inhibit(sparse.conv(q, c2.kernel, th2, 1, 2))
+            w2 = sparse.convwta(o2, 1, 8)
+            sparse.stdp(c2, q, w2)
+            return o1, o2
+
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        l0 = spyker._lib.lib.spk_launch_count()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(args.steps):
+            o1, o2 = step()
+        b.record()
+        torch.cuda.synchronize()
+        launches = (spyker._lib.lib.spk_launch_count() - l0) // max(args.steps, 1)
+        ms = a.elapsed_time(b) / args.steps
+        per_density[f"{int(d * 100)}%"] = {
+            "images_per_s": batch / (ms * 1e-3), "ms_per_step": ms, "thresholds": [th1, th2],
+            "input_events": int(ev.numel), "layer1_events": int(o1.numel), "layer2_events": int(o2.numel),
+            "input_density_measured": float(ev.numel) / (batch * 2 * 28 * 28)}
+    head = per_density["2%"]
+    line = {
+        "metric": "images/s (event-list STDP train + fwd) at 1-5 % input density on 1 B200",
+        "value": head["images_per_s"], "unit": "images/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 (event lists; F32 STDP rule of sparse/stdp.cpp)",
+        "data": "synthetic (seeded first-spike times at the stated density)",
+        "config": {"workload": SPARSE_WORKLOAD.replace("4096 x", f"{batch} x"), "global_batch": batch,
+                   "seq_len": T, "parallelism": "replicas1", "headline_density": "2%"},
+        "per_density": per_density,
+        "gpu_launches": int(launches),
+    }
+    if not args.no_cpu_baseline:
+        import oracle
+
+        kind = "reference" if oracle.available("reference") else "port"
+        o = oracle.get(kind)
+        n = 64
+        dense = (np.arange(T)[None, :, None, None, None] >= _sparse_times(n, 0.02, 7)[:, None]).astype(np.uint8)
+        ev = o.sparse_from_dense(dense, 0.0)
+        w1, w2 = synth.conv_weights(30, 2, 5, seed=1), synth.conv_weights(100, 30, 5, seed=2)
+        th1, th2 = _sparse_thresholds(0.02)
+        cfg = [(0.004, -0.003, 1.0, 0.0, 1.0)]
+
+        def ref_step(w1, w2):
+            o1, s1 = o.sparse_conv(ev, (n, T, 2, 28, 28), w1, th1, (2, 2, 2, 2))
+            i1 = o.sparse_inhibit(o1, s1)
+            win, cnt = o.sparse_convwta(i1, s1, (3, 3), 5)
+            w1 = o.sparse_stdp(ev, (n, T, 2, 28, 28), w1, cfg, win, cnt, (2, 2, 2, 2))
+            q, sq = o.sparse_pool(i1, s1, (2, 2))
+            o2, s2 = o.sparse_conv(q, sq, w2, th2, (2, 2, 2, 2))
+            i2 = o.sparse_inhibit(o2, s2)
+            win, cnt = o.sparse_convwta(i2, s2, (1, 1), 8)
+            w2 = o.sparse_stdp(q, sq, w2, cfg, win, cnt, (2, 2, 2, 2))
+            return w1, w2
+
+        ref_step(w1, w2)
+        t0, k = time.perf_counter(), 0
+        while time.perf_counter() - t0 < min(args.cpu_seconds, 10.0):
+            ref_step(w1, w2)
+            k += n
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": k / dt, "unit": "images/s", "cores": os.cpu_count() or 1, "kind": kind,
+                                "sample": f"{k} images at 2 % density in batches of {n} (reference sparse backend, "
+                                          f"its OpenMP threads), {dt:.1f} s"}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -680,10 +802,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32-compare", action="store_true")
     ap.add_argument("--no-spike-match", action="store_true")
-    ap.add_argument("--workload", default="kheradpisheh", choices=["kheradpisheh", "gabor256", "backprop", "sweep"],
+    ap.add_argument("--workload", default="kheradpisheh", choices=["kheradpisheh", "gabor256", "backprop", "sweep", "sparse"],
                     help="kheradpisheh: the 2-layer STDP training step (the headline); gabor256: large-image "
                          "forward; backprop: temporal-backprop training of a 3-layer first-spike network; "
-                         "sweep: 32 STDP networks on uneven image sizes in one CUDA graph")
+                         "sweep: 32 STDP networks on uneven image sizes in one CUDA graph; sparse: the event-list "
+                         "path at 1-5 % input density")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", args.gpus if args.impl == "reference" else 1))
@@ -695,6 +818,8 @@ def main():
         backprop_arm(args, rank, world)
     elif args.workload == "sweep":
         sweep_arm(args, rank, world)
+    elif args.workload == "sparse":
+        sparse_arm(args, rank, world)
     else:
         gpu_arm(args, rank, world)
 
