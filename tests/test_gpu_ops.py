@@ -477,6 +477,29 @@ def test_fused_layer_matches_ops(port, case, prec):
     assert int(got[1].sum()) > 0
 
 
+@pytest.mark.parametrize("case", [FUSED[0], FUSED[1], FUSED[4]])
+def test_fused_layer_schedules_do_not_change_results(case):
+    """Pipeline stages, accumulators and CTAs per SM change the speed only."""
+    b, t, cin, h, w, cout, k, pad, theta, radius, count = case
+    rng = np.random.default_rng(b * 3 + t)
+    fst = rng.integers(0, t + 4, size=(b, cin, h, w))
+    x = cuda((fst[:, None] <= np.arange(t)[None, :, None, None, None]).astype(np.uint8))
+    conv = spyker.Conv(cin, cout, k, pad=pad)
+    conv.kernel.copy_(cuda(rng.uniform(0.3, 1.0, size=(cout, cin, k, k)).astype(np.float32)))
+    conv.precision = "bf16x3"
+    base = spyker.conv_fire_wta(x, conv, theta, radius, count, pool=2)
+    try:
+        for st in [(3, 1, 0), (2, 0, 1), (6, 0, 0), (0, 1, 2)]:
+            spyker._lib.call("spk_set_conv_schedule", *st)
+            got = spyker.conv_fire_wta(x, conv, theta, radius, count, pool=2)
+            assert torch.equal(got[0], base[0]) and torch.equal(got[2], base[2]), st
+            assert np.array_equal(winners_np(got[1])[0], winners_np(base[1])[0]), st
+            assert np.array_equal(winners_np(got[1])[1], winners_np(base[1])[1]), st
+    finally:
+        spyker._lib.call("spk_set_conv_schedule", 0, 0, 0)
+    assert spyker._lib.lib.spk_device_status(1) == 0
+
+
 @pytest.mark.parametrize("case", [((6, 15, 2, 28, 28, 30, 5, 2), (2, 2)), ((5, 15, 30, 14, 14, 100, 5, 2), (14, 14)),
                                   ((4, 9, 3, 13, 11, 12, 3, 1), (3, 2))])
 def test_fused_layer_pooled(case):
