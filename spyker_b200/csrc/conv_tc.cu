@@ -82,6 +82,9 @@ struct TcParams
     const int32_t *snet;
     const float *net_thr;
     int64_t wimg_stride;
+    // set by the weight split when some weight is negative (then the fused
+    // epilogue takes its general argmax)
+    int *negw;
 };
 
 constexpr int kPotentials = 0, kFused = 1;
@@ -152,7 +155,7 @@ __global__ void to_channels_last_kernel(const uint8_t *__restrict__ in, uint2 *_
 // row), K ordered as the A operand.  One thread per (tile, block, row, chunk).
 __global__ void split_weights_kernel(const float *__restrict__ kernel, uint4 *__restrict__ wimg, int cout, int cin,
                                      int taps, int nhwc, int cpad, int kblocks, int n_tile, int n_tiles, int nsplit,
-                                     int64_t wimg_stride16)
+                                     int64_t wimg_stride16, int *negw)
 {
     // blockIdx.y: network (kernels [N, Cout, Cin, KH, KW], images wimg_stride16 uint4 apart)
     kernel += int64_t(blockIdx.y) * cout * cin * taps;
@@ -185,6 +188,7 @@ __global__ void split_weights_kernel(const float *__restrict__ kernel, uint4 *__
                         c = k / taps, tap = k % taps;
                     if (c < cin) wv = kernel[(int64_t(n) * cin + c) * taps + tap];
                 }
+                if (negw != nullptr && !(wv >= 0.f)) atomicOr(negw, 1);
                 const __nv_bfloat16 h = __float2bfloat16_rn(wv);
                 const float r1 = __fsub_rn(wv, __bfloat162float(h));
                 const __nv_bfloat16 m = __float2bfloat16_rn(r1);
@@ -268,6 +272,22 @@ struct FastMax
 
 constexpr int kEpiChunk = 8;  // accumulator columns per tensor-memory load
 
+// Lean first-max state (non-negative weights, value <= threshold): the
+// largest potential (first index) and the runner-up over all channels.
+struct LeanMax
+{
+    float r1 = -INFINITY, r2 = -INFINITY;
+    int a1 = -1;
+};
+
+__device__ __forceinline__ void merge_lean(LeanMax &s, const LeanMax &o)
+{
+    const bool take = o.r1 > s.r1 || (o.r1 == s.r1 && o.a1 >= 0 && (s.a1 < 0 || o.a1 < s.a1));
+    s.r2 = fmaxf(fmaxf(s.r2, o.r2), take ? s.r1 : o.r1);
+    s.r1 = take ? o.r1 : s.r1;
+    s.a1 = take ? o.a1 : s.a1;
+}
+
 // Merge the state of another set of channels into s: the larger maximum
 // wins, ties going to the lower channel; the loser's maximum competes for
 // the runner-up.
@@ -326,6 +346,26 @@ __device__ __forceinline__ void fast_chunk(const TcParams &P, float thr, const u
     }
 }
 
+// The lean chunk: f = (h + m) + l and the running first max / runner-up;
+// channels past Cout (padding) never win.
+template <int NS>
+__device__ __forceinline__ void lean_chunk(const TcParams &P, const uint32_t (&q)[3][kEpiChunk], int c0, LeanMax &st)
+{
+    const int lim = P.cout - c0;
+#pragma unroll
+    for (int j = 0; j < kEpiChunk; ++j)
+    {
+        const float h = __uint_as_float(q[0][j]), m = __uint_as_float(q[1][j]);
+        const float l = NS == 3 ? __uint_as_float(q[2][j]) : 0.f;
+        float f = __fadd_rn(__fadd_rn(h, m), l);
+        f = j < lim ? f : -INFINITY;
+        const bool gt = f > st.r1;
+        st.r2 = gt ? st.r1 : fmaxf(st.r2, f);
+        st.r1 = gt ? f : st.r1;
+        st.a1 = gt ? c0 + j : st.a1;
+    }
+}
+
 // Thresholded first-max channel of one row, exactly as with the FP64-summed
 // potentials.  Fast pass: the BF16 terms are added in FP32, f = (h + m) + l,
 // which is within 3.01 * 2^-24 * (|h| + |m| + |l|) of the exactly rounded
@@ -337,32 +377,61 @@ __device__ __forceinline__ void fast_chunk(const TcParams &P, float thr, const u
 // next chunk are in flight while a chunk is processed; even and odd chunks
 // keep separate states (two independent dependency chains), merged at the end.
 template <int NS>
-__device__ __forceinline__ void row_argmax(const TcParams &P, float thr, uint32_t lane_base, bool row_ok, int &am,
-                                           float &xam)
+__device__ __forceinline__ void row_argmax(const TcParams &P, float thr, bool lean, uint32_t lane_base, bool row_ok,
+                                           int &am, float &xam)
 {
-    FastMax st, st2;
     constexpr int W = kEpiChunk;
     uint32_t qa[3][W], qb[3][W];
+    bool unsure;
     tmem_chunk<NS>(lane_base, 0, P.n_tile, qa);
-    for (int c0 = 0; c0 < P.n_tile; c0 += 2 * W)
+    if (lean)
     {
-        // n_tile is a multiple of 16 = 2 W: both halves exist
-        tmem_chunk_wait<NS>(qa);
-        tmem_chunk<NS>(lane_base, c0 + W, P.n_tile, qb);
-        fast_chunk<NS>(P, thr, qa, c0, st);
-        tmem_chunk_wait<NS>(qb);
-        if (c0 + 2 * W < P.n_tile) tmem_chunk<NS>(lane_base, c0 + 2 * W, P.n_tile, qa);
-        fast_chunk<NS>(P, thr, qb, c0 + W, st2);
+        // Non-negative weights: every BF16 term of a channel has |m|, |l| <=
+        // 2^-7.9 h, so |h| + |m| + |l| <= 1.0625 f and 1.0625 * max(r1, 0)
+        // bounds the row's term sums.  With value <= threshold a channel at or
+        // below the threshold never beats one above it, so only the maximum,
+        // its runner-up and the two thresholds decide (no per-channel checks).
+        LeanMax st, st2;
+        for (int c0 = 0; c0 < P.n_tile; c0 += 2 * W)
+        {
+            tmem_chunk_wait<NS>(qa);
+            tmem_chunk<NS>(lane_base, c0 + W, P.n_tile, qb);
+            lean_chunk<NS>(P, qa, c0, st);
+            tmem_chunk_wait<NS>(qb);
+            if (c0 + 2 * W < P.n_tile) tmem_chunk<NS>(lane_base, c0 + 2 * W, P.n_tile, qa);
+            lean_chunk<NS>(P, qb, c0 + W, st2);
+        }
+        merge_lean(st, st2);
+        const float tol = __fmaf_rn(1.0625f * fmaxf(st.r1, 0.f), 0x1p-21f, 0x1p-140f);
+        const bool real = st.r1 > thr;
+        unsure = fabsf(__fsub_rn(st.r1, thr)) <= tol;
+        if (real) unsure |= __fsub_rn(st.r1, st.r2) <= 2.f * tol || fabsf(__fsub_rn(st.r1, P.inh_thr)) <= tol;
+        am = real ? st.a1 : 0;
+        xam = real ? st.r1 : P.thv;
     }
-    merge_fast(st, st2);
-    const float tol = __fmaf_rn(st.amax, 0x1p-21f, 0x1p-140f);
-    bool unsure = st.dmin <= tol;
-    const bool has_real = st.a1 >= 0, has_low = st.b1 != INT_MAX;
-    if (has_real && has_low) unsure |= fabsf(__fsub_rn(st.r1, P.thv)) <= tol;
-    const bool real_wins = has_real && (!has_low || st.r1 > P.thv);
-    if (real_wins) unsure |= __fsub_rn(st.r1, st.r2) <= 2.f * tol || fabsf(__fsub_rn(st.r1, P.inh_thr)) <= tol;
-    am = real_wins ? st.a1 : st.b1;
-    xam = real_wins ? st.r1 : P.thv;
+    else
+    {
+        FastMax st, st2;
+        for (int c0 = 0; c0 < P.n_tile; c0 += 2 * W)
+        {
+            // n_tile is a multiple of 16 = 2 W: both halves exist
+            tmem_chunk_wait<NS>(qa);
+            tmem_chunk<NS>(lane_base, c0 + W, P.n_tile, qb);
+            fast_chunk<NS>(P, thr, qa, c0, st);
+            tmem_chunk_wait<NS>(qb);
+            if (c0 + 2 * W < P.n_tile) tmem_chunk<NS>(lane_base, c0 + 2 * W, P.n_tile, qa);
+            fast_chunk<NS>(P, thr, qb, c0 + W, st2);
+        }
+        merge_fast(st, st2);
+        const float tol = __fmaf_rn(st.amax, 0x1p-21f, 0x1p-140f);
+        unsure = st.dmin <= tol;
+        const bool has_real = st.a1 >= 0, has_low = st.b1 != INT_MAX;
+        if (has_real && has_low) unsure |= fabsf(__fsub_rn(st.r1, P.thv)) <= tol;
+        const bool real_wins = has_real && (!has_low || st.r1 > P.thv);
+        if (real_wins) unsure |= __fsub_rn(st.r1, st.r2) <= 2.f * tol || fabsf(__fsub_rn(st.r1, P.inh_thr)) <= tol;
+        am = real_wins ? st.a1 : st.b1;
+        xam = real_wins ? st.r1 : P.thv;
+    }
     const unsigned redo = __ballot_sync(0xffffffffu, unsure && row_ok);
     if (redo)
     {
@@ -407,7 +476,9 @@ __device__ void fused_epilogue(const TcParams &P, float thr, uint32_t acc, bool 
     // thresholded first-max channel of this (pixel, step)
     float mx;
     int am;
-    row_argmax<NS>(P, thr, lane_base, row_ok, am, mx);
+    // lean argmax: no negative weight and value <= threshold (uniform)
+    const bool lean = !*P.negw && P.thv <= thr;
+    row_argmax<NS>(P, thr, lean, lane_base, row_ok, am, mx);
     const int base = (lane >> P.tp_log2) << P.tp_log2;  // first lane of this pixel
     const unsigned grp = (TP == 32) ? 0xffffffffu : (((1u << TP) - 1u) << base);
     const unsigned above = __ballot_sync(0xffffffffu, row_ok && mx > P.inh_thr) & grp;
@@ -1284,13 +1355,23 @@ TcParams prepare(const Plan &pl, const void *in, const float *kernel, int64_t n,
     uint8_t *wimg = ws;
     const int64_t wthreads = int64_t(pl.n_tiles) * pl.kblocks * pl.n_tile * 8;
     SPK_REQUIRE(nnets >= 1 && nnets <= 65535, "invalid number of networks");
+    int *negw = nullptr;
+    if (t_fused > 0)
+    {
+        // the flag word sits after the first-spike map's flag
+        const int64_t cp = pl.nhwc ? pl.cpad : cin;
+        negw = reinterpret_cast<int *>(ws + size_t(nnets) * align256(pl.wimg_bytes) +
+                                       align256(size_t(n / t_fused) * h * w * cp) + 128);
+        SPK_CUDA(cudaMemsetAsync(negw, 0, sizeof(int), s));
+    }
     const dim3 sgrid(grid_for(wthreads, 256), unsigned(nnets));
     split_weights_kernel<<<sgrid, 256, 0, s>>>(kernel, reinterpret_cast<uint4 *>(wimg), int(cout), int(cin),
                                                int(kh * kw), pl.nhwc ? 1 : 0, pl.cpad, pl.kblocks, pl.n_tile,
-                                               pl.n_tiles, pl.nsplit, int64_t(align256(pl.wimg_bytes) / 16));
+                                               pl.n_tiles, pl.nsplit, int64_t(align256(pl.wimg_bytes) / 16), negw);
     SPK_LAUNCHED();
     const uint8_t *a_src = static_cast<const uint8_t *>(in);
     TcParams P{};
+    P.negw = negw;
     P.wimg_stride = int64_t(align256(pl.wimg_bytes));
     uint8_t *xt = wimg + size_t(nnets) * align256(pl.wimg_bytes);
     if (t_fused > 0)

@@ -477,6 +477,29 @@ def test_fused_layer_matches_ops(port, case, prec):
     assert int(got[1].sum()) > 0
 
 
+@pytest.mark.parametrize("kind", ["negative_weights", "value_above_threshold"])
+def test_fused_layer_general_argmax(kind):
+    """Negative weights, or a threshold value above the threshold, take the
+    epilogue's general argmax (the lean one needs neither); results equal
+    the op-by-op pipeline."""
+    b, t, cin, h, w, cout = 6, 15, 4, 12, 11, 20
+    rng = np.random.default_rng(11 if kind == "negative_weights" else 12)
+    fst = rng.integers(0, t + 4, size=(b, cin, h, w))
+    x = cuda((fst[:, None] <= np.arange(t)[None, :, None, None, None]).astype(np.uint8))
+    lo = -0.5 if kind == "negative_weights" else 0.3
+    conv = spyker.Conv(cin, cout, 3, pad=1)
+    conv.kernel.copy_(cuda(rng.uniform(lo, 1.0, size=(cout, cin, 3, 3)).astype(np.float32)))
+    conv.precision = "bf16x3"
+    theta, value = (2.0, 0.0) if kind == "negative_weights" else (6.0, 7.5)
+    spikes, wins = spyker.conv_fire_wta(x, conv, theta, 1, 4, value=value)
+    out = spyker.inhibit(spyker.threshold(conv(x), theta, value))
+    assert np.array_equal(host(spikes), host(spyker.fire(out)))
+    got, want = winners_np(wins), winners_np(spyker.convwta(out, 1, 4))
+    assert np.array_equal(got[1], want[1]) and np.array_equal(got[0], want[0])
+    assert int(host(spikes).sum()) > 0
+    assert spyker._lib.lib.spk_device_status(1) == 0
+
+
 @pytest.mark.parametrize("case", [FUSED[0], FUSED[1], FUSED[4]])
 def test_fused_layer_schedules_do_not_change_results(case):
     """Pipeline stages, accumulators and CTAs per SM change the speed only."""
