@@ -333,6 +333,20 @@ spk_status spk_fst_conv_backward(const float *t_in, int64_t b, int64_t cin, int6
                                  const float *grad_out, int64_t oh, int64_t ow, const int64_t *stride2_host,
                                  const int64_t *pad4_host, float *grad_in, float *grad_kernel, void *ws,
                                  size_t ws_bytes, spk_stream stream);
+/* Forward of a first-spike conv layer on the tensor cores in one fused
+ * kernel: t_out[b,z,oy,ox] = first t in 0..T-1 with potential(t) > threshold,
+ * T when none, where potential(t) = conv of the cumulative spikes [t_in <= t]
+ * (BF16x2/x3 split weights, the FP64 sum of the split terms rounded once to
+ * F32, exactly as spk_conv's potentials followed by spk_rank_gather); the
+ * potentials are never written.  t_in [B, Cin, H, W] F32 (values >= T =
+ * never); T <= 126; all output channels in one CTA (workspace query 0
+ * otherwise). */
+size_t spk_fst_conv_times_workspace(int64_t b, int64_t cin, int64_t h, int64_t w, int64_t cout, int64_t kh,
+                                    int64_t kw, int64_t time, int precision);
+spk_status spk_fst_conv_times(const float *t_in, int64_t b, int64_t cin, int64_t h, int64_t w, const float *kernel,
+                              int64_t cout, int64_t kh, int64_t kw, int64_t sy, int64_t sx, const int64_t *pad4_host,
+                              int64_t time, double threshold, float *t_out, int precision, void *ws, size_t ws_bytes,
+                              spk_stream stream);
 /* The potential one step before each output spike, in FP64:
  * out[b,z,oy,ox] = sum kernel[z,c,ky,kx] * [t_in[b,c,iy,ix] < t_out[b,z,oy,ox]]
  * (the potential-level loss sum g * out has grad_kernel as its exact gradient). */

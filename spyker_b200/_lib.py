@@ -76,6 +76,8 @@ SIGNATURES = {
     "spk_fst_conv_backward_workspace": (_S, [_I, _I, _I, _I, _I]),
     "spk_fst_conv_backward": (_INT, [_P, _I, _I, _I, _I, _P, _I, _I, _I, _P, _P, _I, _I, _P, _P, _P, _P, _P, _S,
                                      _P]),
+    "spk_fst_conv_times_workspace": (_S, [_I, _I, _I, _I, _I, _I, _I, _I, _INT]),
+    "spk_fst_conv_times": (_INT, [_P, _I, _I, _I, _I, _P, _I, _I, _I, _I, _I, _P, _I, _D, _P, _INT, _P, _S, _P]),
     "spk_fst_conv_prespike": (_INT, [_P, _I, _I, _I, _I, _P, _I, _I, _I, _P, _I, _I, _P, _P, _P, _P]),
     "spk_sparse_code_workspace": (_S, [_I, _I, _I, _I, _I]),
     "spk_sparse_code": (_INT, [_P, _INT, _I, _I, _I, _I, _I, _INT, _P, _P, _I, _P, _S, _P]),

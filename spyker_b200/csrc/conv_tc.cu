@@ -85,9 +85,13 @@ struct TcParams
     // set by the weight split when some weight is negative (then the fused
     // epilogue takes its general argmax)
     int *negw;
+    // kTimes: output times [B, Cout, OH, OW]
+    float *tout;
 };
 
-constexpr int kPotentials = 0, kFused = 1;
+// kTimes: the fused (pixel, time) rows with an epilogue that writes each
+// neuron's first step above threshold (F32 time, T = never).
+constexpr int kPotentials = 0, kFused = 1, kTimes = 2;
 
 __device__ __forceinline__ unsigned order_enc(float f)
 {
@@ -581,6 +585,71 @@ __device__ void fused_epilogue(const TcParams &P, float thr, uint32_t acc, bool 
     }
 }
 
+// First-spike epilogue (kTimes) of one tile of PP pixels x TP steps: per
+// (row, channel) the potential is the FP64 sum of the BF16 terms rounded once
+// to F32 (the value the op-by-op conv writes), a spike is potential > thr
+// (cpu/fire.cpp:67-82), and a neuron's time is its first spiking step, T
+// when none (cpu/time.cpp:40-58).  A warp's ballot per channel finds it for
+// the rows it holds; pixels spread over several warps (TP > 32) take the
+// minimum of the warps' candidates through shared memory (double-buffered by
+// tile parity; `tbar`, an mbarrier of the 128 epilogue threads, completes
+// once per tile and its wait is bounded like every other).
+template <int NS>
+__device__ void times_epilogue(const TcParams &P, uint32_t acc, bool row_ok, int64_t mt, uint64_t *release,
+                               int *s_cand, uint32_t j, uint64_t *tbar)
+{
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int TP = 1 << P.tp_log2;
+    const uint32_t lane_base = acc + (uint32_t((warp & 3) * 32) << 16);
+    const bool split = TP > 32;
+    int *cand = s_cand + int(j & 1) * 4 * P.n_tile + warp * P.n_tile;
+    const int gsz = split ? 32 : TP, base = (lane / gsz) * gsz;
+    const unsigned gmask = gsz == 32 ? 0xffffffffu : (((1u << gsz) - 1u) << base);
+    // (sample, pixel) of this lane's group (TP <= 32: a whole pixel)
+    const uint32_t gp = uint32_t(mt) * uint32_t(P.pp) + uint32_t((warp * 32 + base) >> P.tp_log2);
+    const bool pix_ok = int64_t(gp) < P.npix;
+    const uint32_t smp = gp / uint32_t(P.ohw), pix = gp - smp * uint32_t(P.ohw);
+    const int t_lane0 = (warp * 32) & (TP - 1);
+    for (int c0 = 0; c0 < P.n_tile; c0 += kEpiChunk)
+    {
+        uint32_t q[3][kEpiChunk];
+        tmem_chunk<NS>(lane_base, c0, P.n_tile, q);
+        tmem_chunk_wait<NS>(q);
+#pragma unroll
+        for (int e = 0; e < kEpiChunk; ++e)
+        {
+            const int c = c0 + e;
+            double v = double(__uint_as_float(q[0][e])) + double(__uint_as_float(q[1][e]));
+            if (NS == 3) v += double(__uint_as_float(q[2][e]));
+            const bool spike = row_ok && c < P.cout && float(v) > P.thr;
+            const unsigned bal = __ballot_sync(0xffffffffu, spike) & gmask;
+            if (split)
+            {
+                if (lane == 0) cand[c] = bal ? t_lane0 + __ffs(bal) - 1 : P.T;
+            }
+            else if (lane == base && pix_ok && c < P.cout)
+                P.tout[(int64_t(smp) * P.cout + c) * P.ohw + pix] = float(bal ? __ffs(bal) - 1 - base : P.T);
+        }
+    }
+    tc_fence_before();
+    mbar_arrive(release);
+    if (!split) return;
+    mbar_arrive(tbar);
+    if (!wait_bounded(tbar, j & 1)) return;
+    const int wpp = TP / 32;  // warps per pixel
+    const int *cb = s_cand + int(j & 1) * 4 * P.n_tile;
+    for (int i = tid; i < P.pp * P.cout; i += 128)
+    {
+        const int pl = i / P.cout, c = i - pl * P.cout;
+        const uint32_t g = uint32_t(mt) * uint32_t(P.pp) + uint32_t(pl);
+        if (int64_t(g) >= P.npix) continue;
+        int t = P.T;
+        for (int w = pl * wpp; w < pl * wpp + wpp; ++w) t = min(t, cb[w * P.n_tile + c]);
+        const uint32_t sm = g / uint32_t(P.ohw), px = g - sm * uint32_t(P.ohw);
+        P.tout[(int64_t(sm) * P.cout + c) * P.ohw + px] = float(t);
+    }
+}
+
 // Row of a tile: (image for the A gather, sample, step, output pixel).
 struct RowInfo
 {
@@ -871,7 +940,7 @@ template <int MODE>
 __global__ void __launch_bounds__(kWsThreads, 1) conv_ws_kernel(TcParams P)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
-    __shared__ __align__(8) uint64_t full_bar[kMaxStages], empty_bar[kMaxStages], accf_bar[2], acce_bar[2];
+    __shared__ __align__(8) uint64_t full_bar[kMaxStages], empty_bar[kMaxStages], accf_bar[2], acce_bar[2], tim_bar;
     __shared__ uint32_t tmem_slot;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -881,7 +950,7 @@ __global__ void __launch_bounds__(kWsThreads, 1) conv_ws_kernel(TcParams P)
     const int stage_bytes = a_bytes + b_bytes;
     int4 *tab = reinterpret_cast<int4 *>(smem + S * stage_bytes);
     const int taps = P.kh * P.kw;
-    if constexpr (MODE == kFused)
+    if constexpr (MODE != kPotentials)
     {
         // per K element: (channel, ky, kx, valid) in the weight image's order
         for (int k = tid; k < P.kblocks * BK; k += blockDim.x)
@@ -916,6 +985,7 @@ __global__ void __launch_bounds__(kWsThreads, 1) conv_ws_kernel(TcParams P)
     {
         for (int s = 0; s < S; ++s) mbar_init(&full_bar[s], 257), mbar_init(&empty_bar[s], 1);
         for (int a = 0; a < 2; ++a) mbar_init(&accf_bar[a], 1), mbar_init(&acce_bar[a], 128);
+        mbar_init(&tim_bar, 128);
         fence_mbar_init();
     }
     if (warp == 0)
@@ -929,7 +999,7 @@ __global__ void __launch_bounds__(kWsThreads, 1) conv_ws_kernel(TcParams P)
     const uint32_t tmem = tmem_slot;
     const int acc_cols = P.nsplit * P.n_tile;
 
-    if (MODE == kFused && warp >= 4 && warp < 12)
+    if (MODE != kPotentials && warp >= 4 && warp < 12)
     {
         // ---------------- fused producers (8 warps) ----------------
         if (P.tp_log2 >= 2)
@@ -1079,7 +1149,15 @@ __global__ void __launch_bounds__(kWsThreads, 1) conv_ws_kernel(TcParams P)
                     }
                 }
             }
-            if constexpr (MODE == kFused)
+            if constexpr (MODE == kTimes)
+            {
+                int *s_cand = reinterpret_cast<int *>(smem + S * stage_bytes + (P.kblocks * BK + 8) * 16);
+                if (P.nsplit == 3)
+                    times_epilogue<3>(P, acc, r.ok, mt, &acce_bar[a], s_cand, j, &tim_bar);
+                else
+                    times_epilogue<2>(P, acc, r.ok, mt, &acce_bar[a], s_cand, j, &tim_bar);
+            }
+            else if constexpr (MODE == kFused)
             {
                 float thr = P.thr;
                 if (P.snet) thr = P.net_thr[P.snet[(uint32_t(mt) * uint32_t(P.pp)) / uint32_t(P.ohw)]];
@@ -1193,7 +1271,7 @@ struct Plan
 
 // single_tile: all output channels in one CTA (required by the fused epilogue).
 Plan make_plan(int64_t n, int64_t cin, int64_t h, int64_t w, int64_t cout, int64_t kh, int64_t kw, int precision,
-               bool single_tile, int64_t t_fused = 0)
+               bool single_tile, int64_t t_fused = 0, bool times = false)
 {
     Plan pl{};
     pl.nsplit = precision == SPK_CONV_BF16X3 ? 3 : 2;
@@ -1220,7 +1298,9 @@ Plan make_plan(int64_t n, int64_t cin, int64_t h, int64_t w, int64_t cout, int64
         pl.xt_bytes = align256(size_t(n / t_fused) * h * w * (pl.nhwc ? pl.cpad : cin)) + 256;
     else
         pl.xt_bytes = pl.nhwc ? size_t(n) * h * w * pl.cpad : 0;
-    const size_t tab = t_fused > 0  ? (size_t(pl.kblocks) * BK + 8) * 16
+    // (kTimes: the table is followed by the per-warp first-step candidates,
+    // two buffers of 4 warps x n_tile ints)
+    const size_t tab = t_fused > 0  ? (size_t(pl.kblocks) * BK + 8) * 16 + (times ? size_t(pl.n_tile) * 32 : 0)
                        : !pl.nhwc   ? size_t(pl.kblocks) * BK * 16
                                     : size_t(pl.kblocks) * 8 * 16;
     const size_t stage = size_t(BM * BK * 2) + size_t(pl.nsplit) * pl.n_tile * BK * 2;
@@ -1344,10 +1424,30 @@ __global__ void __launch_bounds__(256) fst_stage_words_kernel(const uint8_t *__r
     if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
 }
 
+// First-spike map [B, H, W, Cp] from F32 times [B, C, H, W] (values >= T or
+// not finite: never = T; pad channels 0xFF).
+__global__ void times_fst_kernel(const float *__restrict__ tin, uint8_t *__restrict__ fst, int64_t b, int c, int64_t hw,
+                                 int cp, int T)
+{
+    const int64_t total = b * hw * cp;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += int64_t(gridDim.x) * blockDim.x)
+    {
+        const int ch = int(i % cp);
+        const int64_t r = i / cp, px = r % hw, smp = r / hw;
+        uint8_t v = 0xFF;
+        if (ch < c)
+        {
+            const float t = tin[(smp * c + ch) * hw + px];
+            v = uint8_t((t >= 0.f && t < float(T)) ? int(t) : T);
+        }
+        fst[i] = v;
+    }
+}
+
 // t_fused > 0: stage for the fused (pixel, time) rows of t_fused steps.
 TcParams prepare(const Plan &pl, const void *in, const float *kernel, int64_t n, int64_t cin, int64_t h, int64_t w,
                  int64_t cout, int64_t kh, int64_t kw, int64_t sy, int64_t sx, Pad4 p, int64_t oh, int64_t ow,
-                 uint8_t *ws, cudaStream_t s, int64_t t_fused = 0, int64_t nnets = 1)
+                 uint8_t *ws, cudaStream_t s, int64_t t_fused = 0, int64_t nnets = 1, const float *times = nullptr)
 {
     SPK_REQUIRE(pl.kblocks <= kMaxKBlocks, "Cin*KH*KW is too large for the tensor-core path");
     SPK_REQUIRE(pl.stages >= 2 && pl.smem <= 227 * 1024, "tile does not fit in shared memory");
@@ -1379,22 +1479,35 @@ TcParams prepare(const Plan &pl, const void *in, const float *kernel, int64_t n,
         const int64_t b = n / t_fused, cp = pl.nhwc ? pl.cpad : cin;
         int *flag = reinterpret_cast<int *>(xt + align256(size_t(b) * h * w * cp));
         SPK_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), s));
-        // whole images when their tile fits in 48 KB, else the longest runs
-        // of whole words that do
-        const int64_t ppc = std::min<int64_t>(h * w, (48 * 1024 / (cp + 1)) & ~int64_t(3));
-        const size_t tile = size_t(ppc) * (cp + 1);
-        if ((h * w) % 4 == 0 && reinterpret_cast<uintptr_t>(a_src) % 4 == 0 && ppc >= 4 &&
-            h * w < (int64_t(1) << 31) && b <= 65535)
-            fst_stage_words_kernel<<<dim3(unsigned(ceil_div(h * w, ppc)), unsigned(b)), 256, tile, s>>>(
-                a_src, xt, flag, int(t_fused), int(cin), int(h * w), int(cp), int(ppc));
+        if (times)
+        {
+            times_fst_kernel<<<grid_for(b * h * w * cp, 256), 256, 0, s>>>(times, xt, b, int(cin), h * w, int(cp),
+                                                                          int(t_fused));
+            SPK_LAUNCHED();
+            P.raw = nullptr;
+            P.flag = flag;
+            P.img_stride = h * w * cp;
+            a_src = xt;
+        }
         else
-            fst_stage_kernel<<<grid_for(b * cp * h * w, 256), 256, 0, s>>>(a_src, xt, flag, b, int(t_fused), int(cin),
-                                                                           h * w, int(cp));
-        SPK_LAUNCHED();
-        P.raw = a_src;
-        P.flag = flag;
-        a_src = xt;
-        P.img_stride = h * w * cp;  // per sample
+        {
+            // whole images when their tile fits in 48 KB, else the longest runs
+            // of whole words that do
+            const int64_t ppc = std::min<int64_t>(h * w, (48 * 1024 / (cp + 1)) & ~int64_t(3));
+            const size_t tile = size_t(ppc) * (cp + 1);
+            if ((h * w) % 4 == 0 && reinterpret_cast<uintptr_t>(a_src) % 4 == 0 && ppc >= 4 &&
+                h * w < (int64_t(1) << 31) && b <= 65535)
+                fst_stage_words_kernel<<<dim3(unsigned(ceil_div(h * w, ppc)), unsigned(b)), 256, tile, s>>>(
+                    a_src, xt, flag, int(t_fused), int(cin), int(h * w), int(cp), int(ppc));
+            else
+                fst_stage_kernel<<<grid_for(b * cp * h * w, 256), 256, 0, s>>>(a_src, xt, flag, b, int(t_fused), int(cin),
+                                                                               h * w, int(cp));
+            SPK_LAUNCHED();
+            P.raw = a_src;
+            P.flag = flag;
+            a_src = xt;
+            P.img_stride = h * w * cp;  // per sample
+        }
     }
     else if (pl.nhwc)
     {
@@ -1646,6 +1759,57 @@ spk_status spk_conv_fire_wta(const void *in, spk_dtype itype, const float *kerne
         fused_layer(in, itype, kernel, b, t, cin, h, w, cout, kh, kw, sy, sx, pad4, threshold, value,
                     inhibit_threshold, fire_threshold, ry, rx, count, wta_threshold, spikes, winners, counts, pool_ky,
                     pool_kx, pooled, precision, ws, ws_bytes, stream, Nets{});
+    });
+}
+
+size_t spk_fst_conv_times_workspace(int64_t b, int64_t cin, int64_t h, int64_t w, int64_t cout, int64_t kh,
+                                    int64_t kw, int64_t time, int precision)
+{
+    try
+    {
+        const Plan pl = make_plan(b * time, cin, h, w, cout, kh, kw, precision, true, time, true);
+        if (pl.n_tiles != 1 || pl.nsplit * pl.n_tile > 512) return 0;
+        return align256(pl.wimg_bytes) + align256(pl.xt_bytes);
+    }
+    catch (...)
+    {
+        return 0;
+    }
+}
+
+spk_status spk_fst_conv_times(const float *t_in, int64_t b, int64_t cin, int64_t h, int64_t w, const float *kernel,
+                              int64_t cout, int64_t kh, int64_t kw, int64_t sy, int64_t sx, const int64_t *pad4,
+                              int64_t time, double threshold, float *t_out, int precision, void *ws, size_t ws_bytes,
+                              spk_stream stream)
+{
+    return guarded([&] {
+        const Pad4 p = pad_of(pad4);
+        SPK_REQUIRE(precision == SPK_CONV_BF16X2 || precision == SPK_CONV_BF16X3, "the layer runs on tcgen05");
+        SPK_REQUIRE(b >= 0 && time >= 1 && time <= 126 && cin >= 1 && cout >= 1 && kh >= 1 && kw >= 1 && sy >= 1 &&
+                        sx >= 1,
+                    "needs 1 <= T <= 126");
+        SPK_REQUIRE(t_in != nullptr && kernel != nullptr && t_out != nullptr, "null pointer");
+        const int64_t oh = (h + p.top + p.bottom - kh) / sy + 1, ow = (w + p.left + p.right - kw) / sx + 1;
+        SPK_REQUIRE(oh > 0 && ow > 0 && h + p.top + p.bottom >= kh && w + p.left + p.right >= kw,
+                    "input and kernel shapes are not compatible");
+        Plan pl = make_plan(b * time, cin, h, w, cout, kh, kw, precision, true, time, true);
+        SPK_REQUIRE(pl.n_tiles == 1 && pl.nsplit * pl.n_tile <= 512, "too many output channels for one CTA");
+        SPK_REQUIRE(ws != nullptr && ws_bytes >= align256(pl.wimg_bytes) + align256(pl.xt_bytes),
+                    "workspace is too small");
+        const int64_t npix = b * oh * ow;
+        SPK_REQUIRE(npix < (int64_t(1) << 31), "at most 2^31 - 1 output pixels per call");
+        if (b == 0) return;
+        cudaStream_t s = stream_of(stream);
+        TcParams P = prepare(pl, nullptr, kernel, b * time, cin, h, w, cout, kh, kw, sy, sx, p, oh, ow,
+                             static_cast<uint8_t *>(ws), s, time, 1, t_in);
+        int tp = 1, lg = 0;
+        while (tp < time) tp <<= 1, ++lg;
+        P.T = int(time), P.tp_log2 = lg, P.pp = BM / tp, P.npix = npix;
+        P.thr = float(threshold);
+        P.tout = t_out;
+        P.M = npix * tp;
+        P.tiles = ceil_div(npix, P.pp);
+        launch<kTimes>(P, pl, s);
     });
 }
 

@@ -42,9 +42,28 @@ def times_of(spikes: torch.Tensor) -> torch.Tensor:
 
 def conv_forward(t_in: torch.Tensor, kernel: torch.Tensor, threshold: float, time: int, stride=1, pad=0,
                  precision: str = "bf16x3") -> torch.Tensor:
-    """Output first-spike times of a conv layer (no gradient tracking)."""
+    """Output first-spike times of a conv layer (no gradient tracking).
+
+    On the tensor-core precisions one fused kernel (``spk_fst_conv_times``)
+    writes the times without materialising the potentials; otherwise (FP32,
+    or layers that do not fit one CTA) the potentials of every step are
+    computed and gathered, in batch chunks."""
     s2, p4 = expand2(stride), expand4(pad)
     b = t_in.shape[0]
+    if precision != "fp32" and time <= 126:
+        k = kernel.float().contiguous()
+        ti = t_in.float().contiguous()
+        _, c, h, w = ti.shape
+        z, _, kh, kw = k.shape
+        nb = _lib.lib.spk_fst_conv_times_workspace(b, c, h, w, z, kh, kw, time, M._PRECISION[precision])
+        if nb > 0:
+            oh = (h + p4[0] + p4[2] - kh) // s2[0] + 1
+            ow = (w + p4[1] + p4[3] - kw) // s2[1] + 1
+            out = torch.empty((b, z, oh, ow), dtype=torch.float32, device=ti.device)
+            ws, wsb = _ws(nb, ti.device)
+            call("spk_fst_conv_times", ptr(ti), b, c, h, w, ptr(k), z, kh, kw, s2[0], s2[1], i64(*p4), int(time),
+                 float(threshold), ptr(out), M._PRECISION[precision], ptr(ws), wsb, stream())
+            return out
     z = kernel.shape[0]
     oh = (t_in.shape[2] + p4[0] + p4[2] - kernel.shape[2]) // s2[0] + 1
     ow = (t_in.shape[3] + p4[1] + p4[3] - kernel.shape[3]) // s2[1] + 1

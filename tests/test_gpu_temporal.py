@@ -99,6 +99,32 @@ def test_forward_times_match_oracle(g, precision):
     assert 0 < (want < time).mean() < 1
 
 
+@pytest.mark.parametrize("g", [
+    (3, 4, 9, 8, 5, 3, (1, 1), (1, 1, 1, 1), 16),
+    (2, 3, 11, 10, 6, 5, (2, 1), (2, 0, 1, 2), 20),
+    (2, 8, 12, 12, 40, 3, (1, 1), (1, 1, 1, 1), 64),  # 2 pixels per tile, 2 warps per pixel
+    (2, 2, 6, 7, 12, 3, (1, 1), (1, 1, 1, 1), 100),  # 1 pixel per tile, 4 warps per pixel
+    (3, 2, 10, 10, 8, 3, (1, 1), (1, 1, 1, 1), 2),
+    (2, 64, 7, 7, 10, 1, (1, 1), (0, 0, 0, 0), 64),
+])
+@pytest.mark.parametrize("precision", ["bf16x3", "bf16x2"])
+def test_fused_times_equal_potentials_then_gather(g, precision):
+    """The fused first-spike kernel equals the tensor-core potentials of
+    every step followed by gather, bit for bit."""
+    b, c, h, w, z, k, stride, pad, time = g
+    rng = np.random.default_rng(b * 5 + c + time)
+    t_in = rng.integers(0, time + 1, size=(b, c, h, w)).astype(np.float32)
+    kern = rng.uniform(0.0, 0.2, size=(z, c, k, k)).astype(np.float32)
+    thr = 0.05 * c * k * k
+    ti = cuda(t_in)
+    got = temporal.conv_forward(ti, cuda(kern), thr, time, stride, pad, precision)
+    spikes = spyker.scatter(ti.reshape(b, -1), time).view(b, time, c, h, w)
+    want = spyker.gather(spyker.conv(spikes, cuda(kern), stride, pad, precision), thr, dtype="f32")
+    assert torch.equal(got, want)
+    assert 0 < float((want < time).float().mean()) < 1
+    assert spyker._lib.lib.spk_device_status(1) == 0
+
+
 @pytest.mark.parametrize("seed", [0, 1])
 def test_fc_gradients_are_reference_fcbackward(ref, seed):
     """The GPU fc backward against the reference's own (cpu/backprop.cpp:105-160)."""
