@@ -35,9 +35,20 @@ BATCH, T, H = 4096, 15, 28
 # DRAM bytes (read + write) of one conv2 launch of the fused layer kernel:
 # ncu's dram__bytes_read.sum + dram__bytes_write.sum for the 256-image case
 # (--batch 256), scaled by 16 (the kernel's traffic grows with the batch).
-CONV2_TRAFFIC_BYTES = int((3.428352 + 1.160448) * 1e6 * 16)
+CONV2_TRAFFIC_BYTES = int((3.516928 + 1.249536) * 1e6 * 16)
 METRIC = "images/s (STDP train + fwd), BF16-split vs FP32 on 1 B200; spike match %"
 WORKLOAD = "kheradpisheh-2layer-stdp: 4096 x 28x28 strokes, T=15, conv1 30x5x5 th15 r3k5, conv2 100x5x5 th10 r1k8"
+
+
+def bf16_peak():
+    """Sustained BF16 denominator: the pool's measured figure when the
+    measurement file is present, else the profiling recipe's fallback."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        v = json.load(open(path)).get("bf16_tflops_sustained")
+        if v:
+            return float(v), "MEASURED_PEAKS.json bf16_tflops_sustained (of measured)"
+    return 1400.0, "sustained cuBLAS BF16 of an earlier measurement on this pool (of fallback)"
 
 
 def flops_per_image():
@@ -226,9 +237,7 @@ def gpu_arm(args, rank, world):
     ms, e2e_ms = float(t_max[0]), float(t_max[1])
     if rank != 0:
         return
-    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
-        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
-    peak = peaks.get("bf16_tflops_sustained", 1390.0)
+    peak, peak_source = bf16_peak()
     achieved = c2f * BATCH / (c2_ms * 1e-3) / 1e12
     line = {
         "metric": METRIC,
@@ -252,7 +261,7 @@ def gpu_arm(args, rank, world):
                      "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                      "traffic": CONV2_TRAFFIC_BYTES * BATCH // 4096 if args.precision != "fp32" else None,
                      "traffic_source": "ncu dram__bytes_read+write of the 256-image capture, scaled",
-                     "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained (of measured)"},
+                     "peak_source": peak_source},
         "kernels_ms": {"conv1": c1_ms, "conv2": c2_ms, "rest": ms - c1_ms - c2_ms},
         "clocks": clk.summary(),
         "spikes_per_s": spikes_per_step * world / (ms * 1e-3),
@@ -459,9 +468,7 @@ def gabor_arm(args, rank, world):
     rel = float(((pot[0].double() - pot64).abs() / pot64.abs().clamp_min(1e-30)).max().item())
     c1 = 2 * 30 * 256 * 256 * 64 * 8 * 49
     c2 = 2 * 30 * 128 * 128 * 256 * 64 * 25
-    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
-        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
-    peak = peaks.get("bf16_tflops_sustained", 1390.0)
+    peak, peak_source = bf16_peak()
     achieved = (c1 + c2) * batch / (ms * 1e-3) / 1e12
     print(json.dumps({
         "metric": "images/s (forward feature extraction), BF16-split vs FP32 on 1 B200; spike match %",
@@ -475,7 +482,7 @@ def gabor_arm(args, rank, world):
                 "d2h_bytes_per_step": int(out.numel() * out.element_size())},
         "roofline": {"bound": "tensor", "kernel": "both fused layers (algorithmic conv FLOPs)", "achieved": achieved,
                      "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                     "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained (of measured)"},
+                     "peak_source": peak_source},
         "fp32_path": {"value": sub / (fp32_ms * 1e-3), "unit": "images/s", "sample": f"{sub} images"},
         "feature_match_vs_fp32_pct": match,
         "conv1_potential_max_rel_error_vs_fp64": rel,
@@ -642,9 +649,7 @@ def sweep_arm(args, rank, world):
     flops = sum(
         sum(len(g.per_net[n][1]) for n in range(nets)) * 2 * 15 * (g.size ** 2 * 30 * 50 + (g.size // 2) ** 2 * 100 * 750)
         for g in sw.groups)
-    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
-        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
-    peak = peaks.get("bf16_tflops_sustained", 1390.0)
+    peak, peak_source = bf16_peak()
     achieved = flops / (ms * 1e-3) / 1e12
     print(json.dumps({
         "metric": "images/s (32-network STDP sweep, train + fwd) on 1 B200",
@@ -662,7 +667,7 @@ def sweep_arm(args, rank, world):
         "eager_step_ms": eager_ms,
         "roofline": {"bound": "tensor", "kernel": "all fused layers (algorithmic conv FLOPs of the real images)",
                      "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                     "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained (of measured)"},
+                     "peak_source": peak_source},
         "clocks": clk.summary(),
     }), flush=True)
 
