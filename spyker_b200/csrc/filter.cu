@@ -66,6 +66,89 @@ __global__ void filter_kernel(int which, const float *__restrict__ in, const flo
     }
 }
 
+// The same filters with the plane staged in shared memory as FP64 (zero
+// halo) and the kernels as FP64: a CTA takes rows [r0, r0 + rows) of one
+// plane for every filter; a thread computes kXB neighbouring outputs of a
+// row, reusing each loaded input for kXB products.  Every output is still
+// one FMA chain over (a, b) in row-major order, so the result equals
+// filter_kernel's bit for bit (a zero-halo term adds +-0 to the chain, which
+// leaves it unchanged).
+constexpr int kXB = 4, kMaxKw = 16;
+
+__global__ void __launch_bounds__(256) filter_tiled_kernel(int which, const float *__restrict__ in,
+                                                           const float *__restrict__ kernel, float *__restrict__ out,
+                                                           int h, int w, int f, int kh, int kw, int oh, int ow, int top,
+                                                           int left, int rows)
+{
+    extern __shared__ double fsm[];
+    const int nk = which == 1 ? f : 2 * f, kk = kh * kw;
+    const int sw = ow + kw - 1 + kXB;  // staged row width (zero beyond the plane)
+    const int srows = rows + kh - 1;
+    double *sk = fsm, *sp = fsm + nk * kk;
+    const int64_t p = blockIdx.y;
+    const int r0 = blockIdx.x * rows, nr = min(rows, oh - r0);
+    const float *plane = in + p * h * w;
+    for (int i = threadIdx.x; i < nk * kk; i += blockDim.x) sk[i] = double(kernel[i]);
+    for (int i = threadIdx.x; i < srows * sw; i += blockDim.x)
+    {
+        const int yy = r0 + i / sw - top, xx = i % sw - left;
+        sp[i] = (yy >= 0 && yy < h && xx >= 0 && xx < w) ? double(plane[yy * w + xx]) : 0.0;
+    }
+    __syncthreads();
+    const int fo = which == 2 ? 2 * f : f;
+    const int64_t plane_out = int64_t(oh) * ow;
+    const int xg = (ow + kXB - 1) / kXB;
+    for (int it = threadIdx.x; it < f * nr * xg; it += blockDim.x)
+    {
+        const int q = it / (nr * xg), rem = it - q * nr * xg, ry = rem / xg, x0 = (rem - ry * xg) * kXB;
+        double g1[kXB], g2[kXB];
+#pragma unroll
+        for (int i = 0; i < kXB; ++i) g1[i] = 0.0, g2[i] = 0.0;
+        const double *k1 = sk + q * kk, *k2 = sk + (f + q) * kk;
+        for (int a = 0; a < kh; ++a)
+        {
+            const double *row = sp + (ry + a) * sw + x0;
+            double v[kMaxKw + kXB - 1];
+#pragma unroll
+            for (int j = 0; j < kMaxKw + kXB - 1; ++j)
+                if (j < kw + kXB - 1) v[j] = row[j];
+#pragma unroll
+            for (int bb = 0; bb < kMaxKw; ++bb)
+            {
+                if (bb >= kw) break;
+                const double c1 = k1[a * kw + bb];
+#pragma unroll
+                for (int i = 0; i < kXB; ++i) g1[i] = fma(v[i + bb], c1, g1[i]);
+                if (which != 1)
+                {
+                    const double c2 = k2[a * kw + bb];
+#pragma unroll
+                    for (int i = 0; i < kXB; ++i) g2[i] = fma(v[i + bb], c2, g2[i]);
+                }
+            }
+        }
+        float *o = out + p * fo * plane_out + int64_t(r0 + ry) * ow;
+#pragma unroll
+        for (int i = 0; i < kXB; ++i)
+        {
+            const int x = x0 + i;
+            if (x >= ow) break;
+            if (which == 1)
+                o[int64_t(q) * plane_out + x] = float(g1[i]);
+            else
+            {
+                const float d = __fsub_rn(float(g1[i]), float(g2[i]));
+                o[int64_t(q) * plane_out + x] = (d < 0.f) ? 0.f : d;
+                if (which == 2)
+                {
+                    const float nd = -d;
+                    o[int64_t(f + q) * plane_out + x] = (nd < 0.f) ? 0.f : nd;
+                }
+            }
+        }
+    }
+}
+
 template <typename I>
 __global__ void fc_kernel(const I *__restrict__ in, const float *__restrict__ kernel, float *__restrict__ out, int64_t r,
                           int ni, int no, int sign)
@@ -105,9 +188,21 @@ spk_status spk_filter(int which, const float *in, const float *kernel, float *ou
         SPK_REQUIRE(oh == h + p.top + p.bottom - kh + 1 && ow == w + p.left + p.right - kw + 1 && oh > 0 && ow > 0,
                     "input and kernel shapes are not compatible");
         if (n == 0) return;
-        filter_kernel<<<grid_for(n * f * oh * ow, 256), 256, 0, stream_of(stream)>>>(
-            which, in, kernel, out, n, int(h), int(w), int(f), int(kh), int(kw), int(oh), int(ow), int(p.top),
-            int(p.left));
+        // tiled: as many output rows per CTA as fit 48 KB of FP64 staging
+        const int64_t nk = which == 1 ? f : 2 * f, sw = ow + kw - 1 + kXB;
+        const int64_t avail = (48 * 1024) / 8 - nk * kh * kw;
+        const int64_t rows = std::min<int64_t>(oh, avail / sw - (kh - 1));
+        if (kw <= kMaxKw && rows >= 1 && n <= 65535 && h * w < (int64_t(1) << 31))
+        {
+            const size_t smem = size_t(nk * kh * kw + (rows + kh - 1) * sw) * 8;
+            filter_tiled_kernel<<<dim3(unsigned(ceil_div(oh, rows)), unsigned(n)), 256, smem, stream_of(stream)>>>(
+                which, in, kernel, out, int(h), int(w), int(f), int(kh), int(kw), int(oh), int(ow), int(p.top),
+                int(p.left), int(rows));
+        }
+        else
+            filter_kernel<<<grid_for(n * f * oh * ow, 256), 256, 0, stream_of(stream)>>>(
+                which, in, kernel, out, n, int(h), int(w), int(f), int(kh), int(kw), int(oh), int(ow), int(p.top),
+                int(p.left));
         SPK_LAUNCHED();
     });
 }

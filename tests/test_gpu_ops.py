@@ -66,6 +66,19 @@ def test_filters_exact(port):
     assert np.array_equal(host(gab(cuda(img))), port.filter("gabor", img, host(gab.kernel), (5, 5, 5, 5)))
 
 
+def test_filters_exact_large_planes(port):
+    """Planes taller than one CTA's staged rows (256 x 256, 11 x 11 Gabor
+    bank; DoG on 64 x 96) against the FP64 oracle, bit for bit."""
+    img = synth.textures(2, seed=3, size=256)[:, None]
+    gab = spyker.Gabor(5, [spyker.GaborFilter(2.5, th, 0.5, lam, 0.0) for th in (0, 45, 90, 135) for lam in (5.0, 10.0)],
+                       pad=5)
+    assert np.array_equal(host(gab(cuda(img))), port.filter("gabor", img, host(gab.kernel), (5, 5, 5, 5)))
+    img2 = synth.textures(3, seed=4, size=96)[:, None, :64, :]
+    dog = spyker.DoG(3, [spyker.DoGFilter(1, 2), spyker.DoGFilter(2, 1)], pad=(2, 3))
+    assert np.array_equal(host(dog(cuda(np.ascontiguousarray(img2)))),
+                          port.filter("dog", np.ascontiguousarray(img2), host(dog.kernel), (2, 3, 2, 3)))
+
+
 def stable_code(x: np.ndarray, time: int) -> np.ndarray:
     """Rank code with ties in index order (the GPU's documented order):
     cpu/code.cpp:93-101 with a stable sort, U16 conversion as x86-64 GCC."""
