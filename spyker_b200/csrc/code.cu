@@ -93,7 +93,10 @@ __global__ void __launch_bounds__(kCodeThreads) rank_sorted_kernel(const I *__re
     if (threadIdx.x == 0) s_cnt = 0;
     __syncthreads();
 
-    // Bitonic sort ascending.
+    // Bitonic sort ascending.  Pair i of a stage is handled by thread i mod
+    // blockDim; for strides <= 32 the pairs of a warp's 32 consecutive i
+    // stay inside one 64-key segment, so two such stages in a row need only
+    // the warp to synchronise.
     for (int size = 2; size <= npow2; size <<= 1)
         for (int stride = size >> 1; stride > 0; stride >>= 1)
         {
@@ -105,8 +108,13 @@ __global__ void __launch_bounds__(kCodeThreads) rank_sorted_kernel(const I *__re
                 uint64_t a = keys[lo], b = keys[hi];
                 if ((a > b) == up) keys[lo] = b, keys[hi] = a;
             }
-            __syncthreads();
+            const int next = stride > 1 ? stride >> 1 : size;  // stride of the next stage
+            if (stride >= 64 || next >= 64)
+                __syncthreads();
+            else
+                __syncwarp();
         }
+    __syncthreads();
 
     // cnt = number of values strictly greater than the row minimum.
     const I vmin = row[uint32_t(keys[x - 1])];
