@@ -126,6 +126,55 @@ __global__ void first_spike_map_u8x4_kernel(const uint32_t *__restrict__ in, uin
     }
 }
 
+// The same for T < 256 with every step's load in flight (16 at a time):
+// on cumulative 0/1 spikes the first spike of a byte lane is T minus the
+// lane's byte sum (no carries for T < 256); a word with any other value, or a
+// one followed by a zero, is redone with the lane-by-lane scan.
+__global__ void first_spike_map_u8x4_sum_kernel(const uint32_t *__restrict__ in, uint2 *__restrict__ fst, int64_t b,
+                                                int t, int64_t x4)
+{
+    const int64_t total = b * x4;
+    for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < total; k += int64_t(gridDim.x) * blockDim.x)
+    {
+        const int64_t s = k / x4, j = k - s * x4;
+        const uint32_t *p = in + s * t * x4 + j;
+        uint32_t sum = 0, prev = 0, odd = 0;
+        for (int q0 = 0; q0 < t; q0 += 16)
+        {
+            uint32_t v[16];
+#pragma unroll
+            for (int u = 0; u < 16; ++u) v[u] = (q0 + u < t) ? __ldg(p + int64_t(q0 + u) * x4) : 0u;
+#pragma unroll
+            for (int u = 0; u < 16; ++u)
+                if (q0 + u < t)  // the same for every thread
+                {
+                    sum += v[u];
+                    odd |= (v[u] & 0xFEFEFEFEu) | (prev & ~v[u]);
+                    prev = v[u];
+                }
+        }
+        uint32_t f[4];
+        if (odd == 0)
+        {
+#pragma unroll
+            for (int l = 0; l < 4; ++l) f[l] = uint32_t(t) - ((sum >> (8 * l)) & 0xffu);
+        }
+        else
+        {
+            f[0] = f[1] = f[2] = f[3] = uint32_t(t);
+            uint32_t seen = 0;
+            for (int q = 0; q < t && seen != 0x0f; ++q)
+            {
+                const uint32_t v = p[int64_t(q) * x4];
+#pragma unroll
+                for (int l = 0; l < 4; ++l)
+                    if (!(seen & (1u << l)) && ((v >> (8 * l)) & 0xffu)) f[l] = uint32_t(q), seen |= 1u << l;
+            }
+        }
+        fst[k] = make_uint2(f[0] | (f[1] << 16), f[2] | (f[3] << 16));
+    }
+}
+
 // Kernel A (conv) on the first-spike map: one CTA per (sample, winner slot).
 template <typename T>
 __global__ void conv_prepost_map_kernel(const uint16_t *__restrict__ fst, const T *__restrict__ out, int t, int cin,
@@ -453,7 +502,10 @@ void conv_prepost(const void *in, spk_dtype itype, int64_t b, int64_t t, int64_t
     auto prep = [&](auto z) {
         using T = decltype(z);
         const int64_t x = cin * h * w;
-        if (sizeof(T) == 1 && x % 4 == 0 && reinterpret_cast<uintptr_t>(in) % 4 == 0)
+        if (sizeof(T) == 1 && x % 4 == 0 && reinterpret_cast<uintptr_t>(in) % 4 == 0 && t < 256)
+            first_spike_map_u8x4_sum_kernel<<<grid_for(b * x / 4, 256, 16), 256, 0, s>>>(
+                (const uint32_t *)in, reinterpret_cast<uint2 *>(fst), b, int(t), x / 4);
+        else if (sizeof(T) == 1 && x % 4 == 0 && reinterpret_cast<uintptr_t>(in) % 4 == 0)
             first_spike_map_u8x4_kernel<<<grid_for(b * x / 4, 256, 16), 256, 0, s>>>(
                 (const uint32_t *)in, reinterpret_cast<uint2 *>(fst), b, int(t), x / 4);
         else

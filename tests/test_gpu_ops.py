@@ -297,6 +297,29 @@ def test_conv_stdp(port, layer):
     assert np.array_equal(host(conv.kernel), want)
 
 
+@pytest.mark.parametrize("kind", ["random01", "values"])
+def test_conv_stdp_noncumulative_input(port, kind):
+    """STDP inputs that are not cumulative 0/1 spikes (a word of four
+    positions then takes the lane-by-lane first-spike scan) against the
+    oracle; the other positions of the batch take the byte-sum path."""
+    rng = np.random.default_rng(21 if kind == "random01" else 22)
+    b, t, c, h, w = 6, 12, 3, 12, 12
+    fst = rng.integers(0, t + 3, size=(b, c, h, w))
+    x = (fst[:, None] <= np.arange(t)[None, :, None, None, None]).astype(np.uint8)
+    flip = rng.random(x.shape) < 0.02
+    x = np.where(flip, (1 - x) if kind == "random01" else 3 * x + 1, x).astype(np.uint8)
+    wgt = rng.uniform(0.3, 0.9, size=(10, c, 3, 3)).astype(np.float32)
+    o = (port.conv(x, wgt, (1, 1), (1, 1, 1, 1)) > 4.0).astype(np.uint8)
+    win, cnt = port.convwta(o.astype(np.float32), (1, 1), 4)
+    conv = spyker.Conv(c, 10, 3, pad=1)
+    conv.kernel.copy_(cuda(wgt))
+    conv.stdpconfig = [spyker.STDPConfig(0.004, -0.003)]
+    conv.stdp(cuda(x), spyker.convwta(cuda(o.astype(np.float32)), 1, 4), cuda(o))
+    want = port.convstdp(x, wgt, o, CFG, win, cnt, (1, 1), (1, 1, 1, 1))
+    assert np.array_equal(host(conv.kernel), want)
+    assert not np.array_equal(want, wgt)
+
+
 def test_fc_stdp(port):
     rng = np.random.default_rng(3)
     x = (rng.random((12, 15, 64)) > 0.6).astype(np.uint8)
