@@ -418,6 +418,8 @@ class GaborNet:
 def gabor_arm(args, rank, world):
     """Config-2 style forward pass (no STDP): BF16-split fused layers against
     the FP32 op-by-op path, potential errors against FP64 on the same GPU."""
+    if rank != 0:
+        return  # a one-GPU workload: under torchrun only rank 0 runs it
     import torch
 
     import spyker_b200 as spyker
@@ -506,6 +508,8 @@ BP_WORKLOAD = ("temporal-backprop: 256 x 28x28 labelled strokes (10 classes), T=
 def backprop_arm(args, rank, world):
     """One training step = rank code -> 3 first-spike layers -> target-rule
     loss -> hand-written backward kernels (autograd) -> SGD update."""
+    if rank != 0:
+        return  # a one-GPU workload: under torchrun only rank 0 runs it
     import torch
 
     import spyker_b200 as spyker
@@ -603,6 +607,8 @@ def sweep_arm(args, rank, world):
     """All networks' training step: per size one multi-network fused launch
     per layer and one multi-network STDP scan per layer, captured once as a
     CUDA graph and replayed; schedules picked by the autotuner."""
+    if rank != 0:
+        return  # a one-GPU workload: under torchrun only rank 0 runs it
     import torch
 
     import spyker_b200 as spyker
@@ -706,6 +712,8 @@ def sparse_arm(args, rank, world):
     """The 2-layer STDP step of the Kheradpisheh example on event lists
     (Sparse::conv / inhibit / convwta / STDP / pool) at 1, 2 and 5 % input
     density; the reference's own CPU sparse backend times a sample."""
+    if rank != 0:
+        return  # a one-GPU workload: under torchrun only rank 0 runs it
     import torch
 
     import spyker_b200 as spyker
