@@ -355,6 +355,33 @@ spk_status spk_fst_conv_prespike(const float *t_in, int64_t b, int64_t cin, int6
                                  int64_t oh, int64_t ow, const int64_t *stride2_host, const int64_t *pad4_host,
                                  double *out, spk_stream stream);
 
+/* ---- rate (Poisson) coding (Core::rate_code / rate_fire / rate_gather /
+ * rate_pool, impl.h:295-309) ----
+ * Counts are cumulative: step t holds each neuron's spikes up to t. */
+/* cpu/code.cpp:134-243: every position's rank (sort) or latency time picks a
+ * row of the inter-spike interval table (cpu/init.cpp:120-149); a Poisson
+ * process per position counts spikes.  Rows are the reference's multisets,
+ * the draws come from a counter-based generator seeded from the library's
+ * global generator (spk_random_seed), so results match the reference in
+ * distribution, not draw for draw.  out [B, T, X]. */
+size_t spk_rate_code_workspace(int64_t b, int64_t t, int64_t x, int sort);
+spk_status spk_rate_code(const void *in, spk_dtype itype, void *out, spk_dtype otype, int64_t b, int64_t t, int64_t x,
+                         int sort, void *ws, size_t ws_bytes, spk_stream stream);
+/* The interval table [time][1024] U16 the rate code uses (host memory). */
+void spk_rate_interval_table(int64_t time, uint16_t *out_host);
+/* cpu/fire.cpp:84-113: in [B, T, X] -> running spike counts [B, T, X]. */
+spk_status spk_rate_fire(const void *in, spk_dtype itype, void *out, spk_dtype otype, int64_t b, int64_t t, int64_t x,
+                         double threshold, spk_stream stream);
+/* cpu/time.cpp:87-92: the last step's counts, [B, T, X] -> [B, X]. */
+spk_status spk_rate_gather(const void *in, spk_dtype itype, void *out, spk_dtype otype, int64_t b, int64_t t,
+                           int64_t x, spk_stream stream);
+/* cpu/pool.cpp:88-137: per window the position of highest rate (rates
+ * [B, C, H, W]; first in row-major window order on ties), its values at
+ * every step; in/out [B, T, C, H, W] / [B, T, C, OH, OW]; no padding. */
+spk_status spk_rate_pool(const void *in, const void *rates, spk_dtype type, spk_dtype rtype, void *out, int64_t b,
+                         int64_t t, int64_t c, int64_t h, int64_t w, int64_t oh, int64_t ow, const int64_t *kernel2_host,
+                         const int64_t *stride2_host, const int64_t *pad4_host, spk_stream stream);
+
 /* ---- event lists (the `sparse_*` table of impl.h:328-356; src/spyker/sparse) ----
  * A sparse spike tensor [U, T, C, H, W] (SparseTensor, utils.h:369-420; Sparse5,
  * base.h:493-528) is one CSR array on the device:

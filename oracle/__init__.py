@@ -290,6 +290,44 @@ class Oracle:
         self._call("orc_fcbackward", kernel, no, ni, x, out, grad, nxt, _CODES[x.dtype], x.shape[0], bpa)
         return kernel, nxt, float(bpa[0])
 
+    # -- rate coding -------------------------------------------------------
+    def poisson_table(self, time: int, bins: int = 1024) -> np.ndarray:
+        out = np.zeros((time, bins), dtype=np.uint16)
+        self._call("orc_poisson_table", time, bins, out)
+        return out
+
+    def rate_code(self, x, time: int, sort: bool = True, dtype=np.uint8) -> np.ndarray:
+        x = self._c(x)
+        b = x.shape[0]
+        out = np.zeros((b, time) + x.shape[1:], dtype=dtype)
+        self._call("orc_rate_code", x, _CODES[x.dtype], out, _CODES[out.dtype], b, time, x[0].size, int(sort))
+        return out
+
+    def rate_fire(self, x, thr: float = 0.0, dtype=np.uint8) -> np.ndarray:
+        x = self._c(x)
+        b, t = x.shape[:2]
+        out = np.zeros(x.shape, dtype=dtype)
+        self._call("orc_rate_fire", x, _CODES[x.dtype], out, _CODES[out.dtype], b, t, x[0, 0].size, float(thr))
+        return out
+
+    def rate_gather(self, x, dtype=np.uint8) -> np.ndarray:
+        x = self._c(x)
+        b, t = x.shape[:2]
+        out = np.zeros((b,) + x.shape[2:], dtype=dtype)
+        self._call("orc_rate_gather", x, _CODES[x.dtype], out, _CODES[out.dtype], b, t, x[0, 0].size)
+        return out
+
+    def rate_pool(self, x, rates, kernel2, stride2=None) -> np.ndarray:
+        x, rates = self._c(x), self._c(rates)
+        stride2 = stride2 or kernel2
+        b, t, c, h, w = x.shape
+        oh = (h - kernel2[0]) // stride2[0] + 1
+        ow = (w - kernel2[1]) // stride2[1] + 1
+        out = np.zeros((b, t, c, oh, ow), dtype=x.dtype)
+        self._call("orc_rate_pool", x, rates, _CODES[x.dtype], _CODES[rates.dtype], out, b, t, c, h, w, oh, ow,
+                   _i64(*kernel2), _i64(*stride2))
+        return out
+
     # -- sparse event lists (offsets [U*T+1], zyx [N, 3]) -----------------
     def sparse_code(self, x, time: int, sort: bool = True):
         x = self._c(x)

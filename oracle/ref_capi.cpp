@@ -15,6 +15,7 @@
 // rounded once to the output type.  Every other op runs the reference code.
 
 #include <spyker/impl.h>
+#include <spyker/cpu/base.h>
 #include <spyker/shape.h>
 
 #include <cmath>
@@ -511,4 +512,43 @@ int orc_sparse_stdp(const int64_t *offsets, const uint8_t *zyx, int64_t u, int64
     });
 }
 
+
+// ---- rate coding (cpu/code.cpp:134-243, fire.cpp:84-113, time.cpp:87-92,
+// pool.cpp:88-137, init.cpp:120-149) ----
+int orc_rate_code(const void *in, int itype, void *out, int otype, int64_t b, int64_t t, int64_t x, int sort)
+{
+    return guard([&] { cpu_rate_code(Dyn2((void *)in, ty(itype), b, x), Dyn3(out, ty(otype), b, t, x), sort != 0); });
+}
+
+int orc_rate_fire(const void *in, int itype, void *out, int otype, int64_t b, int64_t t, int64_t x, double thr)
+{
+    return guard(
+        [&] { cpu_rate_fire(Dyn3((void *)in, ty(itype), b, t, x), Dyn3(out, ty(otype), b, t, x), Scalar(thr)); });
+}
+
+int orc_rate_gather(const void *in, int itype, void *out, int otype, int64_t b, int64_t t, int64_t x)
+{
+    return guard(
+        [&] { cpu_rate_gather(Dyn3((void *)in, ty(itype), b, t, x), Dyn2(out, ty(otype), b, x), Scalar(0.0)); });
+}
+
+int orc_rate_pool(const void *in, const void *rates, int type, int rtype, void *out, int64_t b, int64_t t, int64_t c,
+                  int64_t h, int64_t w, int64_t oh, int64_t ow, const int64_t *kernel2, const int64_t *stride2)
+{
+    return guard([&] {
+        cpu_rate_pool(Dyn5((void *)in, ty(type), b, t, c, h, w), Dyn4((void *)rates, ty(rtype), b, c, h, w),
+                      Dyn5(out, ty(type), b, t, c, oh, ow), Len2(kernel2[0], kernel2[1]), Len2(stride2[0], stride2[1]),
+                      Len4(0, 0, 0, 0));
+    });
+}
+
+// The interval table [time][bins] (rows in the reference's shuffled order).
+int orc_poisson_table(int64_t time, int64_t bins, uint16_t *out)
+{
+    return guard([&] {
+        auto v = poisson_create(time, bins);
+        std::memcpy(out, v.data, size_t(time * bins) * sizeof(uint16_t));
+        CPU::deinit(v);
+    });
+}
 }  // extern "C"

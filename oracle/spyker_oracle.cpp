@@ -24,6 +24,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <limits>
+#include <random>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -1237,4 +1238,161 @@ int orc_sparse_stdp(const int64_t *offsets, const uint8_t *zyx, int64_t u, int64
     });
 }
 
+
+// ------------------------------------------------------------------------
+// Rate coding.  Interval table (cpu/init.cpp:120-149): row i, lambda = i + 1,
+// r = ceil(scale sqrt(lambda)) (5 for row 0, else 4), each j in
+// [max(1, lambda - r), lambda + r] nearbyint(ztp(j, lambda) bins) times, the
+// rest lambda; the reference then std::random_shuffle-s each row (order
+// implementation-defined) -- here Fisher-Yates with std::mt19937(i + 1).
+// ------------------------------------------------------------------------
+int orc_poisson_table(int64_t time, int64_t bins, uint16_t *out)
+{
+    return guard([&] {
+        auto ztp = [](uint16_t k, float a) {
+            float p = 1 / (std::exp(a) - 1);
+            for (int64_t i = 1; i <= k; ++i) p *= a / i;
+            return p;
+        };
+        for (int64_t i = 0; i < time; ++i)
+        {
+            float scale = i < 1 ? 5 : 4;
+            uint16_t lambda = uint16_t(i + 1), range = uint16_t(std::ceil(scale * std::sqrt(lambda)));
+            uint16_t start = uint16_t(std::max(1, lambda - range)), end = uint16_t(lambda + range);
+            uint16_t *row = out + i * bins;
+            int64_t index = 0;
+            for (uint16_t j = start; j <= end; ++j)
+            {
+                int64_t count = int64_t(std::nearbyint(ztp(j, lambda) * bins));
+                if (index + count > bins) count = bins - index;
+                std::fill(row + index, row + index + count, j);
+                index += count;
+                if (j == 65535) break;
+            }
+            std::fill(row + index, row + bins, lambda);
+            std::mt19937 rng(static_cast<std::mt19937::result_type>(i + 1));
+            for (int64_t k = bins - 1; k > 0; --k) std::swap(row[k], row[rng() % uint32_t(k + 1)]);
+        }
+    });
+}
+
+// cpu/code.cpp:177-217: per position the Poisson process of its time's row
+// (rows past the table: never); one std::mt19937 per sample seeded seed + i.
+int orc_rate_code_seeded(const void *in, int itype, void *out, int otype, int64_t b, int64_t t, int64_t x, int sort,
+                         uint64_t seed)
+{
+    return guard([&] {
+        const int64_t bins = 1024;
+        std::vector<uint16_t> table(size_t(t * bins));
+        orc_poisson_table(t, bins, table.data());
+        dispatch(itype, [&](auto zi) {
+            dispatch(otype, [&](auto zo) {
+                using I = decltype(zi);
+                using O = decltype(zo);
+                std::vector<uint16_t> temp(x), times(x), values(x);
+                std::vector<uint32_t> index;
+                for (int64_t i = 0; i < b; ++i)
+                {
+                    std::mt19937 random(static_cast<std::mt19937::result_type>(seed + uint64_t(i)));
+                    code_times((const I *)in + i * x, x, t, sort != 0, temp.data(), index);
+                    auto draw = [&](int64_t j) -> uint32_t {
+                        const uint32_t idx = random() & uint32_t(bins - 1);
+                        return temp[j] < t ? table[size_t(temp[j]) * bins + idx] : uint32_t(0);
+                    };
+                    std::fill(values.begin(), values.end(), uint16_t(0));
+                    for (int64_t j = 0; j < x; ++j) times[j] = temp[j] < t ? uint16_t(draw(j)) : uint16_t(65535);
+                    for (int64_t s = 0; s < t; ++s)
+                    {
+                        O *od = (O *)out + (i * t + s) * x;
+                        for (int64_t j = 0; j < x; ++j)
+                        {
+                            if (times[j] == s) values[j] += 1, times[j] = uint16_t(times[j] + draw(j));
+                            od[j] = O(values[j]);
+                        }
+                    }
+                }
+            });
+        });
+    });
+}
+
+int orc_rate_code(const void *in, int itype, void *out, int otype, int64_t b, int64_t t, int64_t x, int sort)
+{
+    return orc_rate_code_seeded(in, itype, out, otype, b, t, x, sort, 1);
+}
+
+// cpu/fire.cpp:84-113: a spike when the input exceeds the value at the last
+// spike by more than the threshold; outputs are the running counts.
+int orc_rate_fire(const void *in, int itype, void *out, int otype, int64_t b, int64_t t, int64_t x, double thr)
+{
+    return guard([&] {
+        dispatch(itype, [&](auto zi) {
+            dispatch(otype, [&](auto zo) {
+                using I = decltype(zi);
+                using O = decltype(zo);
+                I th = scal<I>(thr);
+                for (int64_t i = 0; i < b; ++i)
+                    for (int64_t j = 0; j < x; ++j)
+                    {
+                        I value = I(0);
+                        O spikes = O(0);
+                        for (int64_t s = 0; s < t; ++s)
+                        {
+                            I v = ((const I *)in)[(i * t + s) * x + j];
+                            if (value + th < v) spikes = O(spikes + O(1)), value = v;
+                            ((O *)out)[(i * t + s) * x + j] = spikes;
+                        }
+                    }
+            });
+        });
+    });
+}
+
+// cpu/time.cpp:87-92: the last step.
+int orc_rate_gather(const void *in, int itype, void *out, int otype, int64_t b, int64_t t, int64_t x)
+{
+    return guard([&] {
+        dispatch(itype, [&](auto zi) {
+            dispatch(otype, [&](auto zo) {
+                using I = decltype(zi);
+                using O = decltype(zo);
+                for (int64_t i = 0; i < b; ++i)
+                    for (int64_t j = 0; j < x; ++j) ((O *)out)[i * x + j] = O(((const I *)in)[(i * t + t - 1) * x + j]);
+            });
+        });
+    });
+}
+
+// cpu/pool.cpp:88-137: the window position of highest rate (first in window
+// row-major order, strict <), its value at every step.
+int orc_rate_pool(const void *in, const void *rates, int type, int rtype, void *out, int64_t b, int64_t t, int64_t c,
+                  int64_t h, int64_t w, int64_t oh, int64_t ow, const int64_t *kernel2, const int64_t *stride2)
+{
+    return guard([&] {
+        dispatch(type, [&](auto zt) {
+            dispatch(rtype, [&](auto zr) {
+                using T = decltype(zt);
+                using R = decltype(zr);
+                for (int64_t i = 0; i < b; ++i)
+                    for (int64_t k = 0; k < c; ++k)
+                        for (int64_t oy = 0; oy < oh; ++oy)
+                            for (int64_t ox = 0; ox < ow; ++ox)
+                            {
+                                const R *r = (const R *)rates + (i * c + k) * h * w;
+                                R best = lowest<R>();
+                                int64_t bi = 0;
+                                for (int64_t a = 0; a < kernel2[0]; ++a)
+                                    for (int64_t q = 0; q < kernel2[1]; ++q)
+                                    {
+                                        int64_t idx = (oy * stride2[0] + a) * w + ox * stride2[1] + q;
+                                        if (best < r[idx]) best = r[idx], bi = idx;
+                                    }
+                                for (int64_t s = 0; s < t; ++s)
+                                    ((T *)out)[(((i * t + s) * c + k) * oh + oy) * ow + ox] =
+                                        ((const T *)in)[((i * t + s) * c + k) * h * w + bi];
+                            }
+            });
+        });
+    });
+}
 }  // extern "C"

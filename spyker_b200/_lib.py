@@ -33,6 +33,12 @@ SIGNATURES = {
     "spk_log_kernel": (_INT, [_P, _I, _D]),
     "spk_rank_code_workspace": (_S, [_I, _I, _INT]),
     "spk_rank_code": (_INT, [_P, _INT, _P, _INT, _I, _I, _I, _INT, _P, _S, _P]),
+    "spk_rate_code_workspace": (_S, [_I, _I, _I, _INT]),
+    "spk_rate_code": (_INT, [_P, _INT, _P, _INT, _I, _I, _I, _INT, _P, _S, _P]),
+    "spk_rate_interval_table": (None, [_I, _P]),
+    "spk_rate_fire": (_INT, [_P, _INT, _P, _INT, _I, _I, _I, _D, _P]),
+    "spk_rate_gather": (_INT, [_P, _INT, _P, _INT, _I, _I, _I, _P]),
+    "spk_rate_pool": (_INT, [_P, _P, _INT, _INT, _P, _I, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P]),
     "spk_threshold": (_INT, [_P, _INT, _I, _D, _D, _P]),
     "spk_rank_infinite": (_INT, [_P, _INT, _I, _I, _I, _D, _P]),
     "spk_rank_fire": (_INT, [_P, _INT, _P, _INT, _I, _D, _P]),

@@ -54,6 +54,16 @@ size_t dtype_size(spk_dtype t)
 // and the same sequence of constructors give the same initial weights.
 static std::mt19937 g_generator(static_cast<std::mt19937::result_type>(time(nullptr)));
 static std::mutex g_generator_mutex;
+
+// A 64-bit seed drawn from the global generator (the rate code's random
+// streams: reproducible after spk_random_seed, like the reference's
+// Generator() draws, cpu/code.cpp:192).
+uint64_t draw_seed()
+{
+    std::lock_guard<std::mutex> lock(g_generator_mutex);
+    const uint64_t hi = g_generator(), lo = g_generator();
+    return (hi << 32) | lo;
+}
 }  // namespace spk
 
 using namespace spk;

@@ -328,9 +328,10 @@ def quantize(array, lower: float, middle: float, upper: float, inplace: bool = T
 
 
 def code(array, time: int, sort: bool = True, dtype: str = "u8", code: str = "rank"):
-    """Rank-order (``sort=True``) or latency coding into cumulative spikes."""
-    if code != "rank":
-        raise NotImplementedError("rate coding is not implemented in spyker_b200")
+    """Rank-order (``sort=True``) or latency coding into cumulative spikes;
+    ``code="rate"``: Poisson spike counts driven by those times."""
+    if code not in ("rank", "rate"):
+        raise ValueError(f"Unknown code {code}.")
     if time <= 0:
         raise ValueError("Input time can't be less than 1.")
     a = Bound(array)
@@ -341,6 +342,11 @@ def code(array, time: int, sort: bool = True, dtype: str = "u8", code: str = "ra
     x = x.reshape(s)
     out = torch.empty(shape.code(s, time), dtype=torch_dtype(dtype), device=x.device)
     x_elems = int(numpy.prod(s[1:]))
+    if code == "rate":
+        ws, wsb = _workspace(_lib.lib.spk_rate_code_workspace(s[0], time, x_elems, int(sort)), x.device)
+        call("spk_rate_code", ptr(x), type_code(x.dtype), ptr(out), type_code(out.dtype), s[0], time, x_elems,
+             int(sort), ptr(ws), wsb, stream())
+        return a.back(out)
     ws, wsb = _workspace(_lib.lib.spk_rank_code_workspace(s[0], x_elems, int(sort)), x.device)
     call("spk_rank_code", ptr(x), type_code(x.dtype), ptr(out), type_code(out.dtype), s[0], time, x_elems, int(sort),
          ptr(ws), wsb, stream())
@@ -358,23 +364,32 @@ def infinite(array, value: float = 0.0, inplace: bool = True):
 
 
 def fire(array, threshold: float = 0.0, dtype: str = "u8", code: str = "rank"):
-    if code != "rank":
-        raise NotImplementedError("rate fire is not implemented in spyker_b200")
+    if code not in ("rank", "rate"):
+        raise ValueError(f"Unknown code {code}.")
     a = Bound(array)
-    x = a.dev
+    x = a.dev.contiguous()
     out = torch.empty(x.shape, dtype=torch_dtype(dtype), device=x.device)
+    if code == "rate":
+        s = least3(list(x.shape))
+        call("spk_rate_fire", ptr(x), type_code(x.dtype), ptr(out), type_code(out.dtype), s[0], s[1],
+             int(numpy.prod(s[2:])), float(threshold), stream())
+        return a.back(out)
     call("spk_rank_fire", ptr(x), type_code(x.dtype), ptr(out), type_code(out.dtype), x.numel(), float(threshold),
          stream())
     return a.back(out)
 
 
 def gather(array, threshold: float = 0.0, dtype: str = "u8", code: str = "rank"):
-    if code != "rank":
-        raise NotImplementedError("rate gather is not implemented in spyker_b200")
+    if code not in ("rank", "rate"):
+        raise ValueError(f"Unknown code {code}.")
     a = Bound(array)
-    x = a.dev
+    x = a.dev.contiguous()
     s = least3(list(x.shape))
     out = torch.empty(shape.gather(s), dtype=torch_dtype(dtype), device=x.device)
+    if code == "rate":
+        call("spk_rate_gather", ptr(x), type_code(x.dtype), ptr(out), type_code(out.dtype), s[0], s[1],
+             int(numpy.prod(s[2:])), stream())
+        return a.back(out)
     call("spk_rank_gather", ptr(x), type_code(x.dtype), ptr(out), type_code(out.dtype), s[0], s[1],
          int(numpy.prod(s[2:])), float(threshold), stream())
     return a.back(out)
@@ -394,7 +409,7 @@ def scatter(array, time: int, dtype: str = "u8"):
 
 def pool(array, kernel, stride=None, pad=0, rates=None):
     if rates is not None:
-        raise NotImplementedError("rate pooling is not implemented in spyker_b200")
+        return _rate_pool(array, kernel, stride, pad, rates)
     k2 = expand2(kernel)
     s2 = expand2(kernel if stride is None else stride)
     p4 = expand4(pad)
@@ -411,6 +426,27 @@ def pool(array, kernel, stride=None, pad=0, rates=None):
 
 
 _pool_op = pool
+
+
+def _rate_pool(array, kernel, stride, pad, rates):
+    """Rate pooling (cpu/pool.cpp:88-137): per window the position of the
+    highest rate, its values at every step."""
+    k2 = expand2(kernel)
+    s2 = expand2(kernel if stride is None else stride)
+    p4 = expand4(pad)
+    if min(k2) < 1 or min(s2) < 1 or min(p4) < 0:
+        raise ValueError("Kernel, stride or pad items are incorrect.")
+    a = Bound(array)
+    x = a.dev.contiguous()
+    s = to5(list(x.shape))
+    r = Bound(rates, x.device).dev.contiguous()
+    if list(r.shape) != [s[0], s[2], s[3], s[4]]:
+        raise ValueError("Rates shape must be [B, C, H, W] of the input.")
+    oshape = shape.pool(s, k2, s2, p4)
+    out = torch.empty(oshape, dtype=x.dtype, device=x.device)
+    call("spk_rate_pool", ptr(x), ptr(r), type_code(x.dtype), type_code(r.dtype), ptr(out), s[0], s[1], s[2], s[3],
+         s[4], oshape[3], oshape[4], i64(*k2), i64(*s2), i64(*p4), stream())
+    return a.back(out)
 
 
 def inhibit(array, threshold: float = 0.0, inplace: bool = True):
