@@ -810,6 +810,73 @@ def sparse_arm(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+# ----------------------------------------------------------------------------
+# R-STDP (--workload rstdp)
+# ----------------------------------------------------------------------------
+RSTDP_WORKLOAD = ("rstdp-mozafari: 1024 x 28x28 labelled strokes, DoG 6 filters -> T=15 -> conv1 30x5x5 -> pool 2 -> "
+                  "conv2 250x3x3 -> pool 3 -> conv3 200x5x5 infinite readout, reward/punish STDP (layer-3 step)")
+
+
+def rstdp_arm(args, rank, world):
+    """The layer-3 R-STDP training step of the Mozafari network."""
+    if rank != 0:
+        return  # a one-GPU workload: under torchrun only rank 0 runs it
+    import torch
+
+    import spyker_b200 as spyker
+    from spyker_b200 import rstdp, synth
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    batch = args.batch if args.batch != BATCH else 1024
+    imgs, labels = synth.labelled_strokes(batch, seed=30)
+    host = torch.from_numpy(imgs).pin_memory()
+    y = torch.from_numpy(labels).to(dev)
+    net = rstdp.MozafariNetwork(device=dev, precision=args.precision, seed=1)
+    x = net.transform(host.to(dev).float().div_(255.0)[:, None])
+    for _ in range(args.warmup):
+        net.train_layer3(x, y)
+    torch.cuda.synchronize()
+    l0 = spyker._lib.lib.spk_launch_count()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(dev.index) as clk:
+        torch.cuda.synchronize()
+        a.record()
+        for _ in range(args.steps):
+            pred = net.train_layer3(x, y)
+        b.record()
+        torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / args.steps
+    launches = (spyker._lib.lib.spk_launch_count() - l0) // max(args.steps, 1)
+    # end to end: pinned images -> transform -> step -> labels read back
+    bufs = [torch.empty(batch, dtype=torch.int64).pin_memory() for _ in range(2)]
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for k in range(args.steps):
+        xe = net.transform(host.to(dev, non_blocking=True).float().div_(255.0)[:, None])
+        bufs[k % 2].copy_(net.train_layer3(xe, y), non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / args.steps
+    perf = rstdp.accuracy(pred.cpu(), torch.from_numpy(labels))
+    print(json.dumps({
+        "metric": "images/s (R-STDP layer-3 training step) on 1 B200",
+        "value": batch / (ms * 1e-3), "unit": "images/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": {"fp32": "f32", "bf16x2": "bf16x2-split/f32-acc", "bf16x3": "bf16x3-split/f32-acc"}[args.precision],
+        "data": "synthetic (seeded labelled stroke images, 10 classes)",
+        "config": {"workload": RSTDP_WORKLOAD.replace("1024 x", f"{batch} x"), "global_batch": batch, "seq_len": 15,
+                   "parallelism": "replicas1", "conv_precision": args.precision,
+                   "l2": "inputs larger than L2: the conv2 potentials are 1.5 GB per 1024 images"},
+        "e2e": {"value": batch / (e2e_ms * 1e-3), "unit": "images/s", "h2d_bytes_per_step": int(host.numel()),
+                "d2h_bytes_per_step": batch * 8},
+        "gpu_launches": int(launches),
+        "labels_right_wrong_silent": [int(v) for v in perf[:3]],
+        "clocks": clk.summary(),
+    }), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -823,11 +890,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32-compare", action="store_true")
     ap.add_argument("--no-spike-match", action="store_true")
-    ap.add_argument("--workload", default="kheradpisheh", choices=["kheradpisheh", "gabor256", "backprop", "sweep", "sparse"],
+    ap.add_argument("--workload", default="kheradpisheh", choices=["kheradpisheh", "gabor256", "backprop", "sweep", "sparse", "rstdp"],
                     help="kheradpisheh: the 2-layer STDP training step (the headline); gabor256: large-image "
                          "forward; backprop: temporal-backprop training of a 3-layer first-spike network; "
                          "sweep: 32 STDP networks on uneven image sizes in one CUDA graph; sparse: the event-list "
-                         "path at 1-5 % input density")
+                         "path at 1-5 % input density; rstdp: the reward-modulated layer of the Mozafari network")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", args.gpus if args.impl == "reference" else 1))
@@ -841,6 +908,8 @@ def main():
         sweep_arm(args, rank, world)
     elif args.workload == "sparse":
         sparse_arm(args, rank, world)
+    elif args.workload == "rstdp":
+        rstdp_arm(args, rank, world)
     else:
         gpu_arm(args, rank, world)
 
