@@ -355,6 +355,24 @@ spk_status spk_fst_conv_prespike(const float *t_in, int64_t b, int64_t cin, int6
                                  int64_t oh, int64_t ow, const int64_t *stride2_host, const int64_t *pad4_host,
                                  double *out, spk_stream stream);
 
+/* ---- ZCA whitening (Core::zca_fit / zca_trans / zca_split, impl.h:212-222;
+ * cpu/zca.cpp:67-155) with FP64 accumulation.  The eigendecomposition of the
+ * covariance between the two steps is the caller's (FP64, on the GPU). ---- */
+/* x [N, D] F32 -> mean [D] and covariance [D, D] (divisor N - 1), FP64.
+ * work: spk_zca_stats_workspace(n, d) bytes (split-K partial sums; 0 = none). */
+int64_t spk_zca_stats_workspace(int64_t n, int64_t d);
+spk_status spk_zca_stats(const float *x, int64_t n, int64_t d, double *mean, double *cov, void *work,
+                         int64_t work_bytes, spk_stream stream);
+/* vectors [D, D] (eigenvectors in columns, row-major), values [D] ->
+ * trans = U diag(1 / sqrt(max(values, 0) + epsilon)) U^T, FP64; work [D]. */
+spk_status spk_zca_matrix(const double *vectors, const double *values, int64_t d, double epsilon, double *work,
+                          double *trans, spk_stream stream);
+/* out [N, D] F32 = (x - mean) trans (FP64 sums); out must not alias x. */
+spk_status spk_zca_transform(const float *x, int64_t n, int64_t d, const double *mean, const double *trans, float *out,
+                             spk_stream stream);
+/* [N, D] -> [N, 2, D] = (max(x, 0), max(-x, 0)), F32 or F64. */
+spk_status spk_zca_split(const void *in, spk_dtype type, void *out, int64_t n, int64_t d, spk_stream stream);
+
 /* ---- rate (Poisson) coding (Core::rate_code / rate_fire / rate_gather /
  * rate_pool, impl.h:295-309) ----
  * Counts are cumulative: step t holds each neuron's spikes up to t. */

@@ -248,10 +248,98 @@ class LoG:
 
 
 class ZCA:
-    """ZCA whitening is not part of the GPU hot path of this build."""
+    """ZCA whitening (module.py ZCA, opers.cpp:807-831, cpu/zca.cpp:67-155).
+
+    ``fit`` computes the feature means and the covariance of ``[N, D]`` (the
+    input flattened per sample) with FP64 sums on the GPU, the symmetric
+    eigendecomposition of the covariance in FP64 (``torch.linalg.eigh`` on
+    the GPU), and the whitening matrix ``U diag(1 / sqrt(max(lambda, 0) +
+    epsilon)) U^T`` in FP64.  ``mean`` and ``transform`` are F32 like the
+    reference's; the FP64 copies are kept for applying the transform.
+    """
 
     def __init__(self) -> None:
-        raise NotImplementedError("ZCA whitening is not implemented in spyker_b200")
+        self.mean = None
+        self.transform = None
+        self._mean64 = None
+        self._trans64 = None
+
+    def fit(self, array, epsilon: float, transform: bool = False) -> "ZCA":
+        a = Bound(array)
+        x = a.dev
+        if x.dim() < 2:
+            raise ValueError("Input dimensions must be at least 2D.")
+        if x.dtype != torch.float32:
+            raise TypeError("Input data type must be F32.")
+        x2 = x.reshape(x.shape[0], -1)
+        n, d = x2.shape
+        mean = torch.empty(d, dtype=torch.float64, device=x.device)
+        cov = torch.empty((d, d), dtype=torch.float64, device=x.device)
+        wbytes = int(_lib.lib.spk_zca_stats_workspace(n, d))
+        work = torch.empty(max(wbytes, 1), dtype=torch.uint8, device=x.device)
+        call("spk_zca_stats", ptr(x2), n, d, ptr(mean), ptr(cov), ptr(work), wbytes, stream())
+        lam, vec = torch.linalg.eigh(cov)
+        vec = vec.contiguous()
+        work = torch.empty(d, dtype=torch.float64, device=x.device)
+        trans = torch.empty((d, d), dtype=torch.float64, device=x.device)
+        call("spk_zca_matrix", ptr(vec), ptr(lam.contiguous()), d, float(epsilon), ptr(work), ptr(trans), stream())
+        self._mean64, self._trans64 = mean, trans
+        self.mean, self.transform = mean.float(), trans.float()
+        if transform:
+            self(array)
+        return self
+
+    def _apply(self, array):
+        if self.mean is None or self.transform is None:
+            raise RuntimeError("ZCA layer is not initialized.")
+        a = Bound(array, writeable=True)
+        x = a.dev
+        if x.dim() < 2:
+            raise ValueError("Input dimensions must be at least 2D.")
+        if x.dtype != torch.float32:
+            raise TypeError("Input data type must be F32.")
+        x2 = x.reshape(x.shape[0], -1)
+        n, d = x2.shape
+        m64 = self._mean64 if self._mean64 is not None else self.mean.double()
+        t64 = self._trans64 if self._trans64 is not None else self.transform.double()
+        if m64.numel() != d or t64.shape != (d, d):
+            raise ValueError("Input shape does not match the fitted ZCA.")
+        m64, t64 = m64.to(x.device).contiguous(), t64.to(x.device).contiguous()
+        out = torch.empty_like(x2)
+        call("spk_zca_transform", ptr(x2), n, d, ptr(m64), ptr(t64), ptr(out), stream())
+        x2.copy_(out)
+        return a.write_back() if a.kind != "cuda" else array
+
+    def __call__(self, *array, inplace: bool = True):
+        if not inplace:
+            array = [clone_array(x) for x in array]
+        out = [self._apply(x) for x in array]
+        return tuple(out) if len(out) > 1 else out[0]
+
+    @staticmethod
+    def split(array):
+        """[N, ...] -> [N, 2, ...]: the positive and negative parts."""
+        a = Bound(array)
+        x = a.dev
+        if x.dim() < 2:
+            raise ValueError("Input dimensions must be more than 1.")
+        if x.dtype not in (torch.float32, torch.float64):
+            raise TypeError("ZCA split supports F32 and F64.")
+        n = x.shape[0]
+        d = x[0].numel() if x.dim() > 1 else 1
+        out = torch.empty((n, 2) + tuple(x.shape[1:]), dtype=x.dtype, device=x.device)
+        call("spk_zca_split", ptr(x), type_code(x.dtype), ptr(out), n, d, stream())
+        return a.back(out)
+
+    def save(self, path: str) -> None:
+        numpy.savez(path, mean=self.mean.cpu().numpy(), transform=self.transform.cpu().numpy())
+
+    def load(self, path: str) -> None:
+        data = numpy.load(path)
+        dev = default_device()
+        self.mean = torch.from_numpy(data["mean"]).to(dev)
+        self.transform = torch.from_numpy(data["transform"]).to(dev)
+        self._mean64 = self._trans64 = None
 
 
 # ---------------------------------------------------------------------------
