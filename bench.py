@@ -154,7 +154,7 @@ def gpu_arm(args, rank, world):
     import torch
 
     import spyker_b200 as spyker
-    from spyker_b200 import synth
+    from spyker_b200 import io, synth
 
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
@@ -202,22 +202,23 @@ def gpu_arm(args, rank, world):
     c1_ms = statistics.mean(conv_ms[id(net.conv1)])
     c2_ms = statistics.mean(conv_ms[id(net.conv2)])
 
-    # end to end: pinned host images -> features in pinned host memory.  Each
-    # step's features are copied back (asynchronously, two host buffers in
-    # turn) and the host queues the next step meanwhile; the timed region
-    # ends after the last copy has landed.
-    f0 = net.step(dev_imgs)
-    feats_host = [torch.empty(f0.shape, dtype=f0.dtype).pin_memory() for _ in range(2)]
+    # end to end: pinned host images -> features in pinned host memory.  The
+    # images of step k+1 are uploaded on a side stream while step k runs
+    # (io.Prefetcher) and each step's features are read back on another
+    # (io.Readback, two host buffers in turn); the timed region starts before
+    # the first upload and ends after the last read-back has landed.
+    net.step(dev_imgs)
+    uploads = io.Prefetcher([host] * args.steps, device=dev, depth=2)
+    back = io.Readback(depth=2, device=dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier()
     e0.record()
-    for k in range(args.steps):
-        x = host.to(dev, non_blocking=True).float().div_(255.0)[:, None]
-        feats_host[k % 2].copy_(net.step(x), non_blocking=True)
+    for raw in uploads:
+        feats = back.push(net.step(raw.float().div_(255.0)[:, None]))
+    back.wait()
     e1.record()
     barrier()
     e2e_ms = e0.elapsed_time(e1) / args.steps
-    feats = feats_host[(args.steps - 1) % 2]
 
     # the same step on the plain FP32 path (the comparison the metric names)
     fp32 = None

@@ -355,6 +355,16 @@ spk_status spk_fst_conv_prespike(const float *t_in, int64_t b, int64_t cin, int6
                                  int64_t oh, int64_t ow, const int64_t *stride2_host, const int64_t *pad4_host,
                                  double *out, spk_stream stream);
 
+/* ---- IDX (MNIST) files (Helper::mnistData / mnistLabel, helper/mnist.cpp:10-60)
+ * read into caller memory (pinned host memory for an overlapped upload). ---- */
+/* magic 2049 (labels: shape [N], ndim 1) or 2051 (images: [N, 1, rows, cols],
+ * ndim 4); offset = the payload's byte offset.  Fails on a missing file, a
+ * short header or another magic. */
+spk_status spk_idx_shape(const char *path, int32_t magic, int64_t *shape, int64_t *ndim, int64_t *offset);
+/* bytes of the payload at offset into dst, with up to `threads` positioned
+ * reads; fails on a short file. */
+spk_status spk_idx_read(const char *path, int64_t offset, void *dst, int64_t bytes, int threads);
+
 /* ---- ZCA whitening (Core::zca_fit / zca_trans / zca_split, impl.h:212-222;
  * cpu/zca.cpp:67-155) with FP64 accumulation.  The eigendecomposition of the
  * covariance between the two steps is the caller's (FP64, on the GPU). ---- */

@@ -328,6 +328,34 @@ class Oracle:
                    _i64(*kernel2), _i64(*stride2))
         return out
 
+    # -- data helpers (reference build only) -----------------------------
+    def csv_rows(self, path: str, delim: str = ", ", skip: int = 0, max_rows: int = 1 << 20):
+        """(skipped, rows) read by Helper::CSV (helper/csv.cpp:10-70)."""
+        cap = max(os.path.getsize(path) * 2 + 64, 64) if os.path.exists(path) else 64
+        out = C.create_string_buffer(cap)
+        ln, sk = C.c_int64(), C.c_int64()
+        fn = self.lib.orc_ref_csv
+        fn.restype = C.c_int
+        if fn(path.encode(), delim.encode(), _I(skip), _I(max_rows), out, _I(cap), C.byref(ln), C.byref(sk)) != 0:
+            raise RuntimeError(self.lib.orc_last_error().decode())
+        raw = out.raw[: ln.value].decode()
+        return sk.value, [r.split("\x1f") for r in raw.split("\x1e")[:-1]]
+
+    def idx(self, path: str, labels: bool):
+        """Helper::mnistLabel / mnistData (helper/mnist.cpp:31-60): None for
+        the empty tensor, else the u8 array."""
+        cap = os.path.getsize(path) if os.path.exists(path) else 0
+        out = np.zeros(max(cap, 1), dtype=np.uint8)
+        shape, ndim = np.zeros(4, dtype=np.int64), C.c_int64()
+        fn = self.lib.orc_ref_idx
+        fn.restype = C.c_int
+        if fn(path.encode(), _I(int(labels)), _P(_ptr(out)), _I(cap), _P(_ptr(shape)), C.byref(ndim)) != 0:
+            raise RuntimeError(self.lib.orc_last_error().decode())
+        if ndim.value == 0:
+            return None
+        dims = tuple(int(v) for v in shape[: ndim.value])
+        return out[: int(np.prod(dims))].reshape(dims).copy()
+
     # -- sparse event lists (offsets [U*T+1], zyx [N, 3]) -----------------
     def sparse_code(self, x, time: int, sort: bool = True):
         x = self._c(x)

@@ -16,6 +16,8 @@
 
 #include <spyker/impl.h>
 #include <spyker/cpu/base.h>
+#include <spyker/helper/csv.h>
+#include <spyker/helper/mnist.h>
 #include <spyker/shape.h>
 
 #include <cmath>
@@ -549,6 +551,46 @@ int orc_poisson_table(int64_t time, int64_t bins, uint16_t *out)
         auto v = poisson_create(time, bins);
         std::memcpy(out, v.data, size_t(time * bins) * sizeof(uint16_t));
         CPU::deinit(v);
+    });
+}
+
+// ---- reference-only: the data helpers (helper/csv.cpp, helper/mnist.cpp) ----
+// CSV rows read by Helper::CSV after skip(skip): fields joined by 0x1f, each
+// row ended by 0x1e, copied into out when cap allows; *len = bytes needed.
+int orc_ref_csv(const char *path, const char *delim, int64_t skip, int64_t max_rows, char *out, int64_t cap,
+                int64_t *len, int64_t *skipped)
+{
+    return guard([&] {
+        Helper::CSV csv(path, delim);
+        *skipped = int64_t(csv.skip(Size(skip)));
+        std::string buf;
+        std::vector<std::string> row;
+        for (int64_t r = 0; r < max_rows && csv.readline(row); ++r)
+        {
+            for (size_t i = 0; i < row.size(); ++i) buf += (i ? "\x1f" : "") + row[i];
+            buf += '\x1e';
+        }
+        *len = int64_t(buf.size());
+        if (*len <= cap) std::memcpy(out, buf.data(), buf.size());
+    });
+}
+
+// An IDX file through Helper::mnistLabel / mnistData: *ndim = 0 for the
+// empty tensor they return on failure, else the shape and (when cap allows)
+// the bytes.
+int orc_ref_idx(const char *path, int64_t labels, uint8_t *out, int64_t cap, int64_t *shape, int64_t *ndim)
+{
+    return guard([&] {
+        Tensor t = labels ? Helper::mnistLabel(path) : Helper::mnistData(path);
+        if (!t)
+        {
+            *ndim = 0;
+            return;
+        }
+        auto s = t.shape();
+        *ndim = int64_t(s.size());
+        for (size_t i = 0; i < s.size(); ++i) shape[i] = int64_t(s[i]);
+        if (int64_t(t.numel()) <= cap) std::memcpy(out, t.data(), size_t(t.numel()));
     });
 }
 }  // extern "C"

@@ -7,8 +7,9 @@ temporal-backprop helpers and the sparse event-list path.  Every operation
 runs on the GPU through the C ABI of ``include/spyker_b200.h``.
 """
 
-from . import sparse, temporal
+from . import io, sparse, temporal
 from ._lib import SpykerError
+from .io import CSV, Prefetcher, Readback, mnist_data, mnist_label, read_csv, read_mnist
 from .module import (FC, ZCA, BPConfig, Conv, conv_fire_wta, DoG, DoGFilter, Gabor, GaborFilter, LoG, STDPConfig, Winner, Winners,
                      backward, canny, code, conv, conv_precision, convwta, fc, fcwta, fire, gather, infinite,
                      inhibit, labelize, pad, pool, quantize, random_seed, scatter, set_conv_precision, stdp,

@@ -128,9 +128,37 @@ def to_torch(*arrays):
     return out[0] if len(out) == 1 else tuple(out)
 
 
-def to_tensor(*arrays):
-    """The device tensor of each array (copied to the GPU when on the host)."""
-    out = [Bound(a).dev.clone() if not (torch.is_tensor(a) and a.is_cuda) else a.clone() for a in arrays]
+class Tensor(torch.Tensor):
+    """A torch tensor whose ``to(other_tensor)`` copies its values into
+    ``other`` in place (casting, any devices, same element count) and
+    returns None, as the reference's ``Tensor::to(Tensor)``
+    (utils.cpp:149-170), which the examples use to load checkpoints into
+    kernels.  Every other form of ``to`` and every op are torch's, and op
+    results are plain tensors."""
+
+    __torch_function__ = torch._C._disabled_torch_function_impl
+
+    def to(self, *args, **kwargs):
+        if len(args) == 1 and not kwargs and torch.is_tensor(args[0]):
+            other = args[0]
+            if other.numel() != self.numel():
+                raise ValueError("Tensors must have the same numel.")
+            other.copy_(self.as_subclass(torch.Tensor).reshape(other.shape))
+            return None
+        return torch.Tensor.to(self.as_subclass(torch.Tensor), *args, **kwargs)
+
+
+def to_tensor(*arrays, pinned: bool = False, unified: bool = False):
+    """A new tensor holding each array: on the GPU, or in pinned host memory
+    with ``pinned=True`` (``unified`` is accepted and treated as the GPU)."""
+    out = []
+    for a in arrays:
+        if pinned:
+            t = to_torch(a).detach().cpu().clone()
+            t = t.pin_memory() if torch.cuda.is_available() else t
+        else:
+            t = Bound(a).dev.clone() if not (torch.is_tensor(a) and a.is_cuda) else a.clone()
+        out.append(t.as_subclass(Tensor))
     return out[0] if len(out) == 1 else tuple(out)
 
 
