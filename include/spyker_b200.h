@@ -355,6 +355,17 @@ spk_status spk_fst_conv_prespike(const float *t_in, int64_t b, int64_t cin, int6
                                  int64_t oh, int64_t ow, const int64_t *stride2_host, const int64_t *pad4_host,
                                  double *out, spk_stream stream);
 
+/* ---- Canny edges (Core::canny, impl.h; cpu/canny.cpp:9-214) and
+ * two-level quantize (Core::quantize; cpu/fire.cpp:116-131). ---- */
+/* u8 images [n, h, w] -> u8 edges [n, h, w]; low / high converted to u8;
+ * workspace spk_canny_workspace(n, h, w) bytes. */
+int64_t spk_canny_workspace(int64_t n, int64_t h, int64_t w);
+spk_status spk_canny(const uint8_t *in, uint8_t *out, int64_t n, int64_t h, int64_t w, double low, double high,
+                     void *ws, int64_t ws_bytes, spk_stream stream);
+/* in place: x < middle -> lower, else upper (values converted to the type). */
+spk_status spk_quantize(void *data, spk_dtype type, int64_t n, double lower, double middle, double upper,
+                        spk_stream stream);
+
 /* ---- IDX (MNIST) files (Helper::mnistData / mnistLabel, helper/mnist.cpp:10-60)
  * read into caller memory (pinned host memory for an overlapped upload). ---- */
 /* magic 2049 (labels: shape [N], ndim 1) or 2051 (images: [N, 1, rows, cols],

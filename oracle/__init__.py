@@ -356,6 +356,21 @@ class Oracle:
         dims = tuple(int(v) for v in shape[: ndim.value])
         return out[: int(np.prod(dims))].reshape(dims).copy()
 
+    def canny(self, x, low: float, high: float) -> np.ndarray:
+        """cpu/canny.cpp on u8 images [..., H, W] (reference build only)."""
+        x = self._c(x, np.uint8)
+        h, w = x.shape[-2:]
+        n = int(np.prod(x.shape[:-2]))
+        out = np.zeros_like(x)
+        self._call("orc_ref_canny", x, out, n, h, w, float(low), float(high))
+        return out
+
+    def quantize(self, x, lower: float, middle: float, upper: float) -> np.ndarray:
+        """cpu/fire.cpp:116-131 on a copy (reference build only)."""
+        x = self._c(x).copy()
+        self._call("orc_ref_quantize", x, _CODES[x.dtype], x.size, float(lower), float(middle), float(upper))
+        return x
+
     # -- sparse event lists (offsets [U*T+1], zyx [N, 3]) -----------------
     def sparse_code(self, x, time: int, sort: bool = True):
         x = self._c(x)

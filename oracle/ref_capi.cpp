@@ -20,6 +20,8 @@
 #include <spyker/helper/mnist.h>
 #include <spyker/shape.h>
 
+#include <omp.h>
+
 #include <cmath>
 #include <cstdint>
 #include <cstdlib>
@@ -592,5 +594,36 @@ int orc_ref_idx(const char *path, int64_t labels, uint8_t *out, int64_t cap, int
         for (size_t i = 0; i < s.size(); ++i) shape[i] = int64_t(s[i]);
         if (int64_t(t.numel()) <= cap) std::memcpy(out, t.data(), size_t(t.numel()));
     });
+}
+
+// ---- reference-only: Canny and quantize (cpu/canny.cpp, cpu/fire.cpp) ----
+// Canny runs on one OpenMP thread: cpu/canny.cpp:190-214 views u8 scratch
+// planes of image i at byte offset i*H*W of the F32 buffers, which hold the
+// F32 planes of image i/8, so images processed at once on several threads
+// overwrite one another's gradients and magnitudes (the result then depends
+// on the schedule); in order on one thread every overwritten plane has
+// already been used.
+int orc_ref_canny(const uint8_t *in, uint8_t *out, int64_t n, int64_t h, int64_t w, double low, double high)
+{
+    return guard([&] {
+        const int threads = omp_get_max_threads();
+        omp_set_num_threads(1);
+        try
+        {
+            cpu_canny(Dyn3((void *)in, Type::U8, n, h, w), Dyn3(out, Type::U8, n, h, w), Scalar(low),
+                      Scalar(high));
+        }
+        catch (...)
+        {
+            omp_set_num_threads(threads);
+            throw;
+        }
+        omp_set_num_threads(threads);
+    });
+}
+
+int orc_ref_quantize(void *data, int type, int64_t n, double lower, double middle, double upper)
+{
+    return guard([&] { cpu_quantize(Dyn1(data, ty(type), n), Scalar(lower), Scalar(middle), Scalar(upper)); });
 }
 }  // extern "C"

@@ -33,6 +33,9 @@ SIGNATURES = {
     "spk_log_kernel": (_INT, [_P, _I, _D]),
     "spk_rank_code_workspace": (_S, [_I, _I, _INT]),
     "spk_rank_code": (_INT, [_P, _INT, _P, _INT, _I, _I, _I, _INT, _P, _S, _P]),
+    "spk_canny_workspace": (_I, [_I, _I, _I]),
+    "spk_canny": (_INT, [_P, _P, _I, _I, _I, _D, _D, _P, _I, _P]),
+    "spk_quantize": (_INT, [_P, _INT, _I, _D, _D, _D, _P]),
     "spk_idx_shape": (_INT, [C.c_char_p, _INT, _P, _P, _P]),
     "spk_idx_read": (_INT, [C.c_char_p, _I, _P, _I, _INT]),
     "spk_zca_stats_workspace": (_I, [_I, _I]),

@@ -412,7 +412,15 @@ _threshold_op = threshold
 
 
 def quantize(array, lower: float, middle: float, upper: float, inplace: bool = True):
-    raise NotImplementedError("quantize is not part of the GPU hot path of this build")
+    """In place unless ``inplace=False``: ``x < middle -> lower``, else
+    ``upper`` (opers.cpp:480-486, cpu/fire.cpp:116-131); the three values
+    are converted to the array's type first."""
+    if not inplace:
+        array = clone_array(array)
+    a = Bound(array, writeable=True)
+    call("spk_quantize", ptr(a.dev), type_code(a.dev.dtype), a.dev.numel(), float(lower), float(middle), float(upper),
+         stream())
+    return a.write_back() if a.kind != "cuda" else array
 
 
 def code(array, time: int, sort: bool = True, dtype: str = "u8", code: str = "rank"):
@@ -789,4 +797,17 @@ def labelize(array, threshold: float):
 
 
 def canny(array, low: float, high: float):
-    raise NotImplementedError("Canny edge detection is not part of the GPU hot path of this build")
+    """Canny edges of u8 images (opers.cpp:223-243, cpu/canny.cpp:9-214):
+    ``[N, C, H, W]`` (or 3-D) in, u8 of the same shape out.  As in the
+    reference, the output is u8 and must have the input's type, so the
+    input must be u8; ``low`` and ``high`` are converted to u8."""
+    a = Bound(array)
+    x = a.dev
+    s4 = to4(list(x.shape))
+    if x.dtype != torch.uint8:
+        raise TypeError("Input and output must have the same type.")
+    n, h, w = s4[0] * s4[1], s4[2], s4[3]
+    out = torch.empty(x.shape, dtype=torch.uint8, device=x.device)
+    ws, nb = _workspace(int(_lib.lib.spk_canny_workspace(n, h, w)), x.device)
+    call("spk_canny", ptr(x), ptr(out), n, h, w, float(low), float(high), ptr(ws), nb, stream())
+    return a.back(out)
