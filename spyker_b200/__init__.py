@@ -7,8 +7,12 @@ temporal-backprop helpers and the sparse event-list path.  Every operation
 runs on the GPU through the C ABI of ``include/spyker_b200.h``.
 """
 
-from . import io, sparse, temporal
+from . import control, io, sparse, temporal
 from ._lib import SpykerError
+from .control import (all_devices, clear_context, cuda_arch_list, cuda_cache_clear, cuda_cache_enable, cuda_cache_enabled,
+                      cuda_cache_print, cuda_conv_force, cuda_conv_heuristic, cuda_conv_light, cuda_current_device,
+                      cuda_device_arch, cuda_memory_free, cuda_memory_taken, cuda_memory_total, cuda_memory_used,
+                      cuda_set_device, max_threads, set_max_threads)
 from .io import CSV, Prefetcher, Readback, mnist_data, mnist_label, read_csv, read_mnist
 from .module import (FC, ZCA, BPConfig, Conv, conv_fire_wta, DoG, DoGFilter, Gabor, GaborFilter, LoG, STDPConfig, Winner, Winners,
                      backward, canny, code, conv, conv_precision, convwta, fc, fcwta, fire, gather, infinite,
