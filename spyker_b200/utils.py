@@ -110,6 +110,61 @@ class Bound:
         return self.orig
 
 
+class _CudaBuffer:
+    """A device pointer seen through ``__cuda_array_interface__``."""
+
+    def __init__(self, ptr: int, shape, dtype: torch.dtype):
+        typestr = numpy.dtype(torch.empty(0, dtype=dtype).numpy().dtype).str
+        self.__cuda_array_interface__ = {"shape": tuple(int(v) for v in shape), "typestr": typestr,
+                                         "data": (int(ptr), False), "version": 3}
+
+
+def create_tensor(device, dtype, shape, pinned: bool = False, unified: bool = False, data: int | None = None):
+    """A tensor of ``shape`` and ``dtype`` ("u8", "f32", ... or a torch dtype)
+    on ``device`` (utils.py ``create_tensor`` of the reference): pinned host
+    memory with ``pinned=True`` on the CPU; ``unified`` is treated as the
+    device; ``data``, a raw pointer, is wrapped without a copy (the caller
+    keeps the memory alive)."""
+    dev = torch.device(device) if not isinstance(device, torch.device) else device
+    dt = torch_dtype(dtype)
+    shape = [int(v) for v in shape]
+    if any(v < 0 for v in shape):
+        raise ValueError("Tensor shape can't have negative dimensions.")
+    if data is not None:
+        if dev.type == "cuda":
+            return torch.as_tensor(_CudaBuffer(data, shape, dt), device=dev)
+        import ctypes
+
+        nbytes = int(numpy.prod(shape)) * torch.empty(0, dtype=dt).element_size()
+        buf = (ctypes.c_uint8 * nbytes).from_address(int(data))
+        return torch.frombuffer(buf, dtype=dt).view(shape) if nbytes else torch.empty(shape, dtype=dt)
+    if dev.type == "cpu":
+        return torch.empty(shape, dtype=dt, pin_memory=bool(pinned) and torch.cuda.is_available())
+    return torch.empty(shape, dtype=dt, device=dev)
+
+
+def wrap_array(array, writeable: bool = False):
+    """A zero-copy tensor view of a PyTorch tensor or NumPy array."""
+    if torch.is_tensor(array):
+        return array
+    if isinstance(array, numpy.ndarray):
+        if writeable and not array.flags["WRITEABLE"]:
+            raise TypeError('Input array is not writable. use "numpy.array(..., copy=True)" to make it writable.')
+        return torch.from_numpy(array)
+    raise TypeError(f"Input array {type(array)} can only be Numpy array or PyTorch tensor.")
+
+
+def create_array(array, dtype, shape):
+    """A new array of ``array``'s kind (NumPy, or a tensor on its device)."""
+    shape = [int(v) for v in shape]
+    if isinstance(array, numpy.ndarray):
+        dt = dtype if not isinstance(dtype, (str, torch.dtype)) else torch.empty(0, dtype=torch_dtype(dtype)).numpy().dtype
+        return numpy.empty(shape, dtype=dt)
+    if torch.is_tensor(array):
+        return torch.empty(shape, dtype=torch_dtype(dtype), device=array.device)
+    raise TypeError(f"Input array {type(array)} can only be Numpy array or PyTorch tensor.")
+
+
 def clone_array(array):
     if torch.is_tensor(array):
         return array.clone()
@@ -278,3 +333,24 @@ class shape:
     @staticmethod
     def gather(input):
         return [input[0]] + list(input[2:])
+
+
+def read_mnist(train_images: str, train_labels: str, test_images: str, test_labels: str):
+    """``spyker.utils.read_mnist``: the IDX reader of ``spyker_b200.io``."""
+    from .io import read_mnist as read
+
+    return read(train_images, train_labels, test_images, test_labels)
+
+
+def read_csv(path: str, delim: str = ", "):
+    """``spyker.utils.read_csv``: the CSV reader of ``spyker_b200.io``."""
+    from .io import read_csv as read
+
+    return read(path, delim)
+
+
+def to_sparse(*arrays, threshold: float = 0.0):
+    """``spyker.utils.to_sparse``: event lists of ``spyker_b200.sparse``."""
+    from .sparse import to_sparse as convert
+
+    return convert(*arrays, threshold=threshold)
