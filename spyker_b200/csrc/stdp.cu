@@ -237,20 +237,12 @@ __global__ void fc_prepost_kernel(const T *__restrict__ in, const T *__restrict_
 // pre address: pre + s * ps + j * pw + element; post index s * count + j.
 // F32_RULE: the event-list STDP of src/spyker/sparse/stdp.cpp:95-97, which
 // rounds the soft-bound factor and the updated weight to F32 before the clamp.
-// v rounded to the nearest F32 (ties to even), returned as a double.  In the
-// normal F32 range this is integer arithmetic on the double's bits (drop 29
-// mantissa bits, round to nearest even; a carry into the exponent is the
-// correct result), which keeps conversions off the weight's dependency
-// chain; zeros, F32 denormals and the top binade go through the conversion.
-__device__ __forceinline__ double round_f32(double v)
-{
-    const unsigned long long u = static_cast<unsigned long long>(__double_as_longlong(v));
-    const int ex = int((u >> 52) & 0x7FF);
-    if ((u << 1) == 0) return v;
-    if (ex < 1023 - 126 || ex >= 1023 + 127) return double(__double2float_rn(v));
-    const unsigned long long r = (u + 0x0FFFFFFFull + ((u >> 29) & 1ull)) & ~0x1FFFFFFFull;
-    return __longlong_as_double(static_cast<long long>(r));
-}
+// v rounded to the nearest F32 (ties to even), returned as a double: a
+// conversion there and back (exact for every value, infinities and
+// denormals included).  On B200 this is the shorter dependency: a chain of
+// updates measures about 95 cycles per update with it against 149 with the
+// rounding done by 64-bit integer operations on the double's bits.
+__device__ __forceinline__ double round_f32(double v) { return double(__double2float_rn(v)); }
 
 // One update of a weight kept as a double holding an F32 value.
 template <bool F32_RULE>
