@@ -1424,6 +1424,67 @@ __global__ void __launch_bounds__(256) fst_stage_words_kernel(const uint8_t *__r
     if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
 }
 
+// The same for a whole image per CTA whose step slab (C * H * W bytes) is a
+// multiple of 8: the slab is read as flat 8-byte words (a warp reads 256
+// contiguous bytes of every step, twice the run of the word version, which
+// keeps DRAM pages open longer), each byte placed by its (channel, pixel).
+__global__ void __launch_bounds__(256) fst_stage_slab_kernel(const uint8_t *__restrict__ in, uint8_t *__restrict__ fst,
+                                                             int *__restrict__ flag, int t, int c, int hw, int cp)
+{
+    extern __shared__ uint8_t tile[];  // [hw][cp + 1]
+    const int rs = cp + 1;
+    const int64_t smp = blockIdx.y;
+    const int64_t words = int64_t(c) * hw / 8;  // per step
+    const uint2 *base = reinterpret_cast<const uint2 *>(in + smp * t * c * int64_t(hw));
+    bool bad = false;
+    for (int it = threadIdx.x; it < words; it += blockDim.x)
+    {
+        const uint2 *src = base + it;
+        uint32_t s0 = 0, s1 = 0, p0 = 0, p1 = 0, odd = 0;
+        for (int q0 = 0; q0 < t; q0 += 16)
+        {
+            uint2 v[16];
+#pragma unroll
+            for (int u = 0; u < 16; ++u) v[u] = (q0 + u < t) ? src[int64_t(q0 + u) * words] : make_uint2(0u, 0u);
+#pragma unroll
+            for (int u = 0; u < 16; ++u)
+                if (q0 + u < t)  // the same for every thread
+                {
+                    s0 += v[u].x, s1 += v[u].y;
+                    odd |= (v[u].x & 0xFEFEFEFEu) | (p0 & ~v[u].x) | (v[u].y & 0xFEFEFEFEu) | (p1 & ~v[u].y);
+                    p0 = v[u].x, p1 = v[u].y;
+                }
+        }
+        bad |= odd != 0;
+        const uint32_t f0 = uint32_t(t) * 0x01010101u - s0, f1 = uint32_t(t) * 0x01010101u - s1;
+        int pos = 8 * it, ch = pos / hw, px = pos - ch * hw;
+#pragma unroll
+        for (int l = 0; l < 8; ++l)
+        {
+            tile[px * rs + ch] = uint8_t((l < 4 ? f0 : f1) >> (8 * (l & 3)));
+            if (++px == hw) px = 0, ++ch;
+        }
+    }
+    for (int it = threadIdx.x; it < hw * (cp - c); it += blockDim.x)
+    {
+        const int px = it / (cp - c);
+        tile[px * rs + c + (it - px * (cp - c))] = 0xFF;
+    }
+    __syncthreads();
+    uint8_t *dst = fst + smp * hw * int64_t(cp);
+    if (cp % 4 == 0)
+        for (int i = threadIdx.x; i < hw * cp / 4; i += blockDim.x)
+        {
+            const int px = (4 * i) / cp, ch = 4 * i - px * cp;
+            const uint8_t *r = tile + px * rs + ch;
+            reinterpret_cast<uint32_t *>(dst)[i] =
+                uint32_t(r[0]) | uint32_t(r[1]) << 8 | uint32_t(r[2]) << 16 | uint32_t(r[3]) << 24;
+        }
+    else
+        for (int i = threadIdx.x; i < hw * cp; i += blockDim.x) dst[i] = tile[(i / cp) * rs + i % cp];
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
+}
+
 // First-spike map [B, H, W, Cp] from F32 times [B, C, H, W] (values >= T or
 // not finite: never = T; pad channels 0xFF).
 __global__ void times_fst_kernel(const float *__restrict__ tin, uint8_t *__restrict__ fst, int64_t b, int c, int64_t hw,
@@ -1495,8 +1556,12 @@ TcParams prepare(const Plan &pl, const void *in, const float *kernel, int64_t n,
             // of whole words that do
             const int64_t ppc = std::min<int64_t>(h * w, (48 * 1024 / (cp + 1)) & ~int64_t(3));
             const size_t tile = size_t(ppc) * (cp + 1);
-            if ((h * w) % 4 == 0 && reinterpret_cast<uintptr_t>(a_src) % 4 == 0 && ppc >= 4 &&
-                h * w < (int64_t(1) << 31) && b <= 65535)
+            if (ppc == h * w && (cin * h * w) % 8 == 0 && reinterpret_cast<uintptr_t>(a_src) % 8 == 0 &&
+                b <= 65535)
+                fst_stage_slab_kernel<<<dim3(1u, unsigned(b)), 256, tile, s>>>(a_src, xt, flag, int(t_fused), int(cin),
+                                                                              int(h * w), int(cp));
+            else if ((h * w) % 4 == 0 && reinterpret_cast<uintptr_t>(a_src) % 4 == 0 && ppc >= 4 &&
+                     h * w < (int64_t(1) << 31) && b <= 65535)
                 fst_stage_words_kernel<<<dim3(unsigned(ceil_div(h * w, ppc)), unsigned(b)), 256, tile, s>>>(
                     a_src, xt, flag, int(t_fused), int(cin), int(h * w), int(cp), int(ppc));
             else
