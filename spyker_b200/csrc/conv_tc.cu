@@ -1250,6 +1250,75 @@ __global__ void wta_records_kernel(const int4 *__restrict__ records, const unsig
     if (threadIdx.x == 0) counts[b] = found;
 }
 
+// The same selection with one warp per sample for maps of up to 32 * KPL
+// pixels: lane l holds pixels l, l + 32, ... in registers, a round is a
+// lane-local best and a 5-step shuffle argmax (no block barriers), and the
+// suppression walks the lane's pixels with (y, x) advanced incrementally.
+template <int KPL>
+__global__ void __launch_bounds__(128) wta_records_warp_kernel(const int4 *__restrict__ records,
+                                                               const unsigned *__restrict__ mins,
+                                                               const unsigned *__restrict__ maxs, int64_t nb, int hw,
+                                                               int w, int T, int ry, int rx, int count,
+                                                               int32_t *__restrict__ winners,
+                                                               int32_t *__restrict__ counts)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t b = int64_t(blockIdx.x) * 4 + (threadIdx.x >> 5);
+    if (b >= nb) return;  // whole warps leave together
+    const float mn = order_dec(mins[b]), mx = order_dec(maxs[b]);
+    const float diff = __fmul_rn(__fsub_rn(mx, mn), 2.0f);
+    float key[KPL];
+    int flat[KPL];
+#pragma unroll
+    for (int q = 0; q < KPL; ++q)
+    {
+        const int p = lane + 32 * q;
+        key[q] = -INFINITY, flat[q] = INT_MAX;
+        if (p < hw)
+        {
+            const int4 r = records[b * hw + p];
+            if (r.y < T)
+            {
+                key[q] = __fadd_rn(float(T - r.y - 1), __fdiv_rn(__fsub_rn(__int_as_float(r.z), mn), diff));
+                flat[q] = r.x * hw + p;
+            }
+        }
+    }
+    int found = 0;
+    for (int round = 0; round < count; ++round)
+    {
+        float bv = -INFINITY;
+        int bi = INT_MAX;
+#pragma unroll
+        for (int q = 0; q < KPL; ++q)
+            if (key[q] > bv || (key[q] == bv && flat[q] < bi)) bv = key[q], bi = flat[q];
+        for (int o = 16; o > 0; o >>= 1)
+        {
+            const float ov = __shfl_xor_sync(0xffffffffu, bv, o);
+            const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+            if (ov > bv || (ov == bv && oi < bi)) bv = ov, bi = oi;
+        }
+        if (bi == INT_MAX) break;  // only sentinels left (the same in every lane)
+        const int z = bi / hw, p0 = bi % hw, y = p0 / w, x = p0 % w;
+        if (lane == 0)
+        {
+            int32_t *e = winners + (b * count + round) * 5;
+            e[0] = 0, e[1] = 0, e[2] = z, e[3] = y, e[4] = x;
+        }
+        int py = lane / w, px = lane - py * w;
+#pragma unroll
+        for (int q = 0; q < KPL; ++q)
+        {
+            const bool box = py >= y - ry && py <= y + ry && px >= x - rx && px <= x + rx;
+            if (box || (flat[q] != INT_MAX && flat[q] / hw == z)) key[q] = -INFINITY, flat[q] = INT_MAX;
+            px += 32;
+            while (px >= w) px -= w, ++py;
+        }
+        ++found;
+    }
+    if (lane == 0) counts[b] = found;
+}
+
 inline size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 
 // Schedule overrides of the tensor-core kernels (0 = automatic), set by an
@@ -1807,8 +1876,16 @@ void fused_layer(const void *in, spk_dtype itype, const float *kernel, int64_t b
     launch<kFused>(P, L.pl, s);
     if (count == 0) return;
     const int hw = int(L.oh * L.ow);
-    wta_records_kernel<<<unsigned(b), 256, size_t(hw) * 8, s>>>(P.records, P.mins, P.maxs, hw, int(L.ow), int(t),
-                                                                int(ry), int(rx), int(count), winners, counts);
+    const unsigned wgrid = unsigned(ceil_div(b, 4));
+    if (hw <= 256)
+        wta_records_warp_kernel<8><<<wgrid, 128, 0, s>>>(P.records, P.mins, P.maxs, b, hw, int(L.ow), int(t), int(ry),
+                                                          int(rx), int(count), winners, counts);
+    else if (hw <= 1024)
+        wta_records_warp_kernel<32><<<wgrid, 128, 0, s>>>(P.records, P.mins, P.maxs, b, hw, int(L.ow), int(t),
+                                                           int(ry), int(rx), int(count), winners, counts);
+    else
+        wta_records_kernel<<<unsigned(b), 256, size_t(hw) * 8, s>>>(P.records, P.mins, P.maxs, hw, int(L.ow), int(t),
+                                                                    int(ry), int(rx), int(count), winners, counts);
     SPK_LAUNCHED();
 }
 }  // namespace
