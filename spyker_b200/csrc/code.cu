@@ -93,6 +93,53 @@ __global__ void __launch_bounds__(kCodeThreads) rank_sorted_kernel(const I *__re
     if (threadIdx.x == 0) s_cnt = 0;
     __syncthreads();
 
+    if (npow2 == 2 * kCodeThreads && blockDim.x == kCodeThreads)
+    {
+        // Two keys per thread (elements 2 tid, 2 tid + 1) in registers: a
+        // stage of stride 1 is a swap inside the thread, strides 2..32 a
+        // shuffle with thread tid ^ (stride / 2) of the same warp, and only
+        // strides >= 64 go through shared memory (15 of the 66 stages).
+        const int e0 = 2 * threadIdx.x;
+        uint64_t k0 = keys[e0], k1 = keys[e0 + 1];
+        for (int size = 2; size <= npow2; size <<= 1)
+        {
+            if (size > 64)
+            {
+                __syncthreads();
+                keys[e0] = k0, keys[e0 + 1] = k1;
+                __syncthreads();
+                for (int stride = size >> 1; stride >= 64; stride >>= 1)
+                {
+                    const int i = threadIdx.x;
+                    const int lo = 2 * i - (i & (stride - 1)), hi = lo + stride;
+                    const bool up = (lo & size) == 0;
+                    const uint64_t a = keys[lo], c = keys[hi];
+                    if ((a > c) == up) keys[lo] = c, keys[hi] = a;
+                    __syncthreads();
+                }
+                k0 = keys[e0], k1 = keys[e0 + 1];
+            }
+            const bool up = (e0 & size) == 0;
+            for (int stride = (size >> 1) < 32 ? (size >> 1) : 32; stride >= 2; stride >>= 1)
+            {
+                const int lane_x = stride >> 1;
+                const uint64_t p0 = __shfl_xor_sync(0xffffffffu, k0, lane_x);
+                const uint64_t p1 = __shfl_xor_sync(0xffffffffu, k1, lane_x);
+                const bool lower = (e0 & stride) == 0;  // this thread's elements are the lower of their pairs
+                const bool keep_min = lower == up;
+                k0 = keep_min ? (k0 < p0 ? k0 : p0) : (k0 > p0 ? k0 : p0);
+                k1 = keep_min ? (k1 < p1 ? k1 : p1) : (k1 > p1 ? k1 : p1);
+            }
+            if ((k0 > k1) == up)
+            {
+                const uint64_t tmp = k0;
+                k0 = k1, k1 = tmp;
+            }
+        }
+        __syncthreads();
+        keys[e0] = k0, keys[e0 + 1] = k1;
+    }
+    else
     // Bitonic sort ascending.  Pair i of a stage is handled by thread i mod
     // blockDim; for strides <= 32 the pairs of a warp's 32 consecutive i
     // stay inside one 64-key segment, so two such stages in a row need only
