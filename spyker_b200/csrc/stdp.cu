@@ -243,9 +243,24 @@ __global__ void conv_prepost_map_kernel(const uint16_t *__restrict__ fst, const 
     const int k = cin * kh * kw;
     uint16_t *p = pre + (int64_t(s) * count + j) * k;
     const uint16_t *f = fst + int64_t(s) * cin * h * w;
+    // (c, ky, kx) of element i by multiplying with rounded reciprocals: for
+    // i < 2^16 the products' error (< 2^-7) stays below the 0.5 / divisor
+    // margin that the +0.5 keeps from the next integer, so the quotients are
+    // exact without integer divisions
+    const int taps = kh * kw;
+    const float inv_taps = 1.0f / float(taps), inv_kw = 1.0f / float(kw);
     for (int i = threadIdx.x; i < k; i += blockDim.x)
     {
-        const int c = i / (kh * kw), r = i % (kh * kw), ky = r / kw, kx = r % kw;
+        int c, r, ky;
+        if (k < 65536)
+        {
+            c = __float2int_rz(__fmul_rn(float(i) + 0.5f, inv_taps));
+            r = i - c * taps;
+            ky = __float2int_rz(__fmul_rn(float(r) + 0.5f, inv_kw));
+        }
+        else
+            c = i / taps, r = i - c * taps, ky = r / kw;
+        const int kx = r - ky * kw;
         const int yy = wy * sy + ky - top, xx = wx * sx + kx - left;
         p[i] = (yy >= 0 && yy < h && xx >= 0 && xx < w) ? f[(int64_t(c) * h + yy) * w + xx] : uint16_t(t);
     }
