@@ -767,13 +767,15 @@ __device__ __forceinline__ int ftab(int kblocks, int kb, int kc, int i)
 
 __device__ __forceinline__ FusedPixel fused_pixel(const TcParams &P, int64_t mt, int pl)
 {
+    // pixel indexes fit in 32 bits (checked on the host): 32-bit divisions
     FusedPixel u{};
-    const int64_t gp = mt * P.pp + pl;
-    u.ok = gp < P.npix;
+    const uint32_t gp = uint32_t(mt) * uint32_t(P.pp) + uint32_t(pl);
+    u.ok = int64_t(gp) < P.npix;
     if (u.ok)
     {
-        u.sample = gp / P.ohw;
-        const int pix = int(gp - u.sample * P.ohw), oy = pix / P.ow, ox = pix - oy * P.ow;
+        const uint32_t ohw = uint32_t(P.ohw), smp = gp / ohw, pix = gp - smp * ohw;
+        u.sample = smp;
+        const int oy = int(pix / uint32_t(P.ow)), ox = int(pix) - oy * P.ow;
         u.iy0 = oy * P.sy - P.top;
         u.ix0 = ox * P.sx - P.left;
     }
@@ -1880,6 +1882,9 @@ void fused_layer(const void *in, spk_dtype itype, const float *kernel, int64_t b
     if (hw <= 256)
         wta_records_warp_kernel<8><<<wgrid, 128, 0, s>>>(P.records, P.mins, P.maxs, b, hw, int(L.ow), int(t), int(ry),
                                                           int(rx), int(count), winners, counts);
+    else if (hw <= 800)
+        wta_records_warp_kernel<25><<<wgrid, 128, 0, s>>>(P.records, P.mins, P.maxs, b, hw, int(L.ow), int(t),
+                                                           int(ry), int(rx), int(count), winners, counts);
     else if (hw <= 1024)
         wta_records_warp_kernel<32><<<wgrid, 128, 0, s>>>(P.records, P.mins, P.maxs, b, hw, int(L.ow), int(t),
                                                            int(ry), int(rx), int(count), winners, counts);
