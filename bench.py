@@ -113,6 +113,9 @@ class Network:
             c.stdpconfig = [spyker.STDPConfig(0.004, -0.003)]
             c.precision = precision
         self.conv_events = []
+        # layer 1's STDP runs here while layer 2's forward runs on the main
+        # stream: layer 2 reads layer 1's spikes, not its weights
+        self.side = torch.cuda.Stream(dev)
 
     def _conv(self, layer, x):
         t = self.torch
@@ -143,9 +146,15 @@ class Network:
         sp = self.sp
         codes = sp.code(self.dog(images_f32), T)
         spk1, win1, pooled = self._layer(self.conv1, codes, 15.0, 3, 5, 2)
-        self.conv1.stdp(codes, win1, spk1)
+        main = self.torch.cuda.current_stream()
+        self.side.wait_stream(main)
+        with self.torch.cuda.stream(self.side):
+            self.conv1.stdp(codes, win1, spk1)
         spk2, win2, feats = self._layer(self.conv2, pooled, 10.0, 1, 8, 14)
         self.conv2.stdp(pooled, win2, spk2)
+        # the step ends when both streams have (the next step's layer 1
+        # reads the updated weights; this step's tensors are freed after it)
+        main.wait_stream(self.side)
         self.last_spikes = (spk1, spk2)
         return feats
 
