@@ -113,9 +113,12 @@ class Network:
             c.stdpconfig = [spyker.STDPConfig(0.004, -0.003)]
             c.precision = precision
         self.conv_events = []
-        # layer 1's STDP runs here while layer 2's forward runs on the main
-        # stream: layer 2 reads layer 1's spikes, not its weights
+        # layer 1's STDP runs on `side` while layer 2's forward runs on the
+        # main stream (layer 2 reads layer 1's spikes, not its weights), and
+        # layer 2's STDP on `side2` while the next step's front end and layer
+        # 1 run (joined before the next layer 2, and by finish())
         self.side = torch.cuda.Stream(dev)
+        self.side2 = torch.cuda.Stream(dev)
 
     def _conv(self, layer, x):
         t = self.torch
@@ -150,13 +153,22 @@ class Network:
         self.side.wait_stream(main)
         with self.torch.cuda.stream(self.side):
             self.conv1.stdp(codes, win1, spk1)
+        main.wait_stream(self.side2)  # the previous step's layer-2 update
         spk2, win2, feats = self._layer(self.conv2, pooled, 10.0, 1, 8, 14)
-        self.conv2.stdp(pooled, win2, spk2)
-        # the step ends when both streams have (the next step's layer 1
-        # reads the updated weights; this step's tensors are freed after it)
+        self.side2.wait_stream(main)
+        with self.torch.cuda.stream(self.side2):
+            self.conv2.stdp(pooled, win2, spk2)
+        for x in (pooled, spk2, win2.records, win2.counts):
+            x.record_stream(self.side2)  # not reused before the update has read them
+        # the next step's layer 1 reads the updated conv1 weights; this
+        # step's layer-1 tensors are freed after the join
         main.wait_stream(self.side)
         self.last_spikes = (spk1, spk2)
         return feats
+
+    def finish(self):
+        """Join the last layer-2 update into the current stream."""
+        self.torch.cuda.current_stream().wait_stream(self.side2)
 
 
 def gpu_arm(args, rank, world):
@@ -197,6 +209,7 @@ def gpu_arm(args, rank, world):
         start.record()
         for _ in range(args.steps):
             net.step(dev_imgs)
+        net.finish()
         end.record()
         barrier()
     launches = (spyker._lib.lib.spk_launch_count() - l0) // max(args.steps, 1)
@@ -224,6 +237,7 @@ def gpu_arm(args, rank, world):
     e0.record()
     for raw in uploads:
         feats = back.push(net.step(raw.float().div_(255.0)[:, None]))
+    net.finish()
     back.wait()
     e1.record()
     barrier()
@@ -239,6 +253,7 @@ def gpu_arm(args, rank, world):
         f0.record()
         for _ in range(2):
             ref_net.step(dev_imgs)
+        ref_net.finish()
         f1.record()
         barrier()
         fp32_ms = f0.elapsed_time(f1) / 2
