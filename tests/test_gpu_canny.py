@@ -65,3 +65,15 @@ def test_canny_edge_cases(ref):
             assert np.array_equal(got, ref.canny(img, lo, hi)), (img.shape, lo, hi)
     with pytest.raises(TypeError):
         spyker.canny(torch.zeros((1, 8, 8), device=DEV), 1, 2)
+
+
+def test_canny_multichannel_and_3d(ref):
+    # [N, C, H, W] is processed as N * C images; 3-D input as one batch
+    img = (synth.textures(3, size=40, seed=9) * 255).astype(np.uint8).reshape(3, 1, 40, 40)
+    img = np.concatenate([img, img[:, :, ::-1].copy()], axis=1)  # 2 channels
+    got = spyker.canny(torch.from_numpy(img).to(DEV), 35, 80).cpu().numpy()
+    assert got.shape == img.shape
+    assert np.array_equal(got, ref.canny(img, 35, 80))
+    flat = img.reshape(6, 40, 40)
+    assert np.array_equal(spyker.canny(torch.from_numpy(flat).to(DEV), 35, 80).cpu().numpy(),
+                          ref.canny(flat, 35, 80))

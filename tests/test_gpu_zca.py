@@ -98,3 +98,15 @@ def test_errors_and_save_load(tmp_path):
     assert torch.equal(w.mean.cpu(), z.mean.cpu()) and torch.equal(w.transform.cpu(), z.transform.cpu())
     assert _rel(w(x, inplace=False), oracle.zca_transform(x, z.mean.cpu().double().numpy(),
                                                            z.transform.cpu().double().numpy())) < 1e-5
+
+
+def test_cuda_tensor_in_place_and_split_after_transform():
+    x = torch.from_numpy(_samples(800, 48, seed=8)).to(DEV).view(800, 3, 4, 4)
+    keep = x.clone()
+    z = spyker.ZCA().fit(x, 1e-2, transform=True)  # in place on the device tensor
+    mean, trans = oracle.zca_fit(keep.cpu().numpy(), 1e-2)
+    want = oracle.zca_transform(keep.cpu().numpy(), mean, trans)
+    assert _rel(x.cpu().numpy(), want) < 1e-5
+    s = spyker.ZCA.split(x)
+    assert s.shape == (800, 2, 3, 4, 4)
+    assert np.array_equal(s.cpu().numpy(), oracle.zca_split(x.cpu().numpy()))
