@@ -240,6 +240,65 @@ __global__ void inhibit_kernel(T *__restrict__ data, int64_t b, int t, int c, in
         }
     }
 }
+// The same for F32 with 4 neighbouring pixels per thread (16-byte loads
+// and stores): a warp moves 512 contiguous bytes of every (step, channel)
+// row instead of 128, and each thread keeps 4 independent max chains.
+__global__ void inhibit_f32x4_kernel(float4 *__restrict__ data, int64_t b, int t, int c, int64_t x4, float thr)
+{
+    const int64_t total = b * x4;
+    for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < total; k += int64_t(gridDim.x) * blockDim.x)
+    {
+        const int64_t s = k / x4, j = k - s * x4;
+        float4 *base = data + s * int64_t(t) * c * x4 + j;
+        int sum[4] = {0, 0, 0, 0};
+        for (int q = 0; q < t; ++q)
+        {
+            const float4 *row = base + int64_t(q) * c * x4;
+            float4 m = row[0];
+#pragma unroll 4
+            for (int z = 1; z < c; ++z)
+            {
+                const float4 v = row[int64_t(z) * x4];
+                m.x = (v.x > m.x) ? v.x : m.x, m.y = (v.y > m.y) ? v.y : m.y;
+                m.z = (v.z > m.z) ? v.z : m.z, m.w = (v.w > m.w) ? v.w : m.w;
+            }
+            sum[0] += (m.x > thr), sum[1] += (m.y > thr), sum[2] += (m.z > thr), sum[3] += (m.w > thr);
+        }
+        int win[4];
+        float best[4];
+#pragma unroll
+        for (int l = 0; l < 4; ++l) win[l] = 0;
+        {
+            int ts[4];
+#pragma unroll
+            for (int l = 0; l < 4; ++l) ts[l] = t - (sum[l] > 1 ? sum[l] : 1);
+#pragma unroll
+            for (int l = 0; l < 4; ++l)
+                best[l] = reinterpret_cast<const float *>(base + int64_t(ts[l]) * c * x4)[l];
+            for (int z = 1; z < c; ++z)
+#pragma unroll
+                for (int l = 0; l < 4; ++l)
+                {
+                    const float v = reinterpret_cast<const float *>(base + (int64_t(ts[l]) * c + z) * x4)[l];
+                    if (v > best[l]) best[l] = v, win[l] = z;
+                }
+        }
+        for (int q = 0; q < t; ++q)
+        {
+            float4 *r = base + int64_t(q) * c * x4;
+#pragma unroll 4
+            for (int z = 0; z < c; ++z)
+            {
+                float4 v = r[int64_t(z) * x4];
+                if (z != win[0]) v.x = v.x * 0.0f;
+                if (z != win[1]) v.y = v.y * 0.0f;
+                if (z != win[2]) v.z = v.z * 0.0f;
+                if (z != win[3]) v.w = v.w * 0.0f;
+                r[int64_t(z) * x4] = v;
+            }
+        }
+    }
+}
 }  // namespace
 }  // namespace spk
 
@@ -317,6 +376,13 @@ spk_status spk_rank_inhibit(void *data, spk_dtype type, int64_t b, int64_t t, in
         SPK_REQUIRE(b >= 0 && t >= 1 && c >= 1 && x >= 0, "invalid dims");
         SPK_REQUIRE(c <= 65535 && t <= 65535, "channel and time counts are limited to 65535");
         if (b * x == 0) return;
+        if (type == SPK_F32 && x % 4 == 0 && reinterpret_cast<uintptr_t>(data) % 16 == 0)
+        {
+            inhibit_f32x4_kernel<<<grid_for(b * x / 4, 128), 128, 0, stream_of(stream)>>>(
+                static_cast<float4 *>(data), b, int(t), int(c), x / 4, scalar_to<float>(threshold));
+            SPK_LAUNCHED();
+            return;
+        }
         dispatch(type, [&](auto z) {
             using T = decltype(z);
             inhibit_kernel<T><<<grid_for(b * x, 128), 128, 0, stream_of(stream)>>>((T *)data, b, int(t), int(c), x,
