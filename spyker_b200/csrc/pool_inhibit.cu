@@ -242,24 +242,42 @@ __global__ void inhibit_kernel(T *__restrict__ data, int64_t b, int t, int c, in
 }
 // 2x2 windows of stride 2 on u8 planes straight from global memory: a
 // thread reads the two input rows of 2 output columns as two 4-byte words
-// (W % 4 == 0) and writes the 2 outputs as one 2-byte word (even output
-// width), so a warp moves contiguous runs with no staging.  Any odd last
+// (W % 4 == 0), for 7 output rows at once, and writes each pair of outputs
+// as one 2-byte word (even output width); no staging.  Any odd last
 // input row / column is outside every window (oh = H / 2, ow = W / 2).
 __global__ void pool2x2_u8_kernel(const uint8_t *__restrict__ in, uint8_t *__restrict__ out, int64_t n, int h, int w,
                                   int oh, int ow)
 {
-    const int g2 = ow / 2;  // 2-output groups per output row
-    const int64_t total = n * oh * g2;
+    // a thread takes 2 output columns of RY consecutive output rows (the
+    // 2 * RY input words of a column pair are all in flight together)
+    constexpr int RY = 7;
+    const int g2 = ow / 2;             // 2-output groups per output row
+    const int ry = (oh + RY - 1) / RY;  // row blocks per plane
+    const int64_t total = n * ry * g2;
     for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < total; k += int64_t(gridDim.x) * blockDim.x)
     {
+        const int g = int(k % g2);
         const int64_t r = k / g2;
-        const int g = int(k - r * g2);
-        const int64_t pl = r / oh;
-        const int yo = int(r - pl * oh);
-        const uint8_t *row = in + (pl * h + 2 * yo) * w + 4 * g;
-        const uint32_t m = bmax4(*reinterpret_cast<const uint32_t *>(row), *reinterpret_cast<const uint32_t *>(row + w));
-        const uint32_t v = bmax4(m, m >> 8);  // bytes 0 and 2 hold the two outputs
-        *reinterpret_cast<uint16_t *>(out + (pl * oh + yo) * ow + 2 * g) = uint16_t((v & 0xFFu) | ((v >> 8) & 0xFF00u));
+        const int64_t pl = r / ry;
+        const int y0 = int(r - pl * ry) * RY;
+        uint32_t a[RY][2];
+#pragma unroll
+        for (int q = 0; q < RY; ++q)
+            if (y0 + q < oh)
+            {
+                const uint8_t *row = in + (pl * h + 2 * (y0 + q)) * w + 4 * g;
+                a[q][0] = *reinterpret_cast<const uint32_t *>(row);
+                a[q][1] = *reinterpret_cast<const uint32_t *>(row + w);
+            }
+#pragma unroll
+        for (int q = 0; q < RY; ++q)
+            if (y0 + q < oh)
+            {
+                const uint32_t m = bmax4(a[q][0], a[q][1]);
+                const uint32_t v = bmax4(m, m >> 8);  // bytes 0 and 2 hold the two outputs
+                *reinterpret_cast<uint16_t *>(out + (pl * oh + y0 + q) * ow + 2 * g) =
+                    uint16_t((v & 0xFFu) | ((v >> 8) & 0xFF00u));
+            }
     }
 }
 
@@ -351,7 +369,7 @@ spk_status spk_rank_pool(const void *in, void *out, spk_dtype type, int64_t n, i
             if (pairs && ky == 2 && ow % 2 == 0 && ow * 2 <= w && oh * 2 <= h &&
                 reinterpret_cast<uintptr_t>(out) % 2 == 0)
             {
-                pool2x2_u8_kernel<<<grid_for(n * oh * (ow / 2), 256), 256, 0, stream_of(stream)>>>(
+                pool2x2_u8_kernel<<<grid_for(n * ceil_div(oh, 7) * (ow / 2), 256), 256, 0, stream_of(stream)>>>(
                     (const uint8_t *)in, (uint8_t *)out, n, int(h), int(w), int(oh), int(ow));
                 SPK_LAUNCHED();
                 return;
