@@ -51,6 +51,13 @@ def bf16_peak():
     return 1400.0, "sustained cuBLAS BF16 of an earlier measurement on this pool (of fallback)"
 
 
+def headline_config(batch: int, world: int) -> dict:
+    """The workload's `config`, shared by both arms of the bench."""
+    return {"workload": WORKLOAD.replace("4096 x", f"{batch} x"), "global_batch": batch * world, "seq_len": T,
+            "parallelism": f"replicas{world}",
+            "l2": "inputs larger than L2: each step writes its own 1.44 GB layer-1 spike tensor (126 MB L2)"}
+
+
 def flops_per_image():
     c1 = 2 * T * 28 * 28 * 30 * 2 * 25
     c2 = 2 * T * 14 * 14 * 100 * 30 * 25
@@ -135,6 +142,8 @@ class Network:
         t = self.torch
         a, b = t.cuda.Event(enable_timing=True), t.cuda.Event(enable_timing=True)
         a.record()
+        if getattr(self, "probe", None):
+            self.probe()
         if layer.precision == "fp32":
             out = self.sp.inhibit(self.sp.threshold(layer(x), theta))
             spk, wins = self.sp.fire(out), self.sp.convwta(out, radius, count)
@@ -143,6 +152,8 @@ class Network:
             spk, wins, pooled = self.sp.conv_fire_wta(x, layer, theta, radius, count, pool=pool)
         b.record()
         self.conv_events.append((a, b, layer))
+        if getattr(self, "probe", None):
+            self.probe()
         return spk, wins, pooled
 
     def step(self, images_f32):
@@ -199,6 +210,21 @@ def gpu_arm(args, rank, world):
 
     for _ in range(args.warmup):
         net.step(dev_imgs)
+    barrier()
+    # Training state over the warm-up: per step and layer, the rows the fused
+    # layers re-decided exactly and the layers' times (synchronised, untimed)
+    trajectory = []
+    for k in range(args.trajectory):
+        rec = []
+        net.conv_events.clear()
+        net.probe = lambda: (torch.cuda.synchronize(), rec.append(spyker._lib.lib.spk_recheck_count(1)))
+        spyker._lib.lib.spk_recheck_count(1)
+        net.step(dev_imgs)
+        net.finish()
+        torch.cuda.synchronize()
+        net.probe = None
+        c1, c2 = (a.elapsed_time(b) for a, b, _ in net.conv_events[:2])
+        trajectory.append({"step": args.warmup + k, "rechecks": rec, "conv_ms": [c1, c2]})
     barrier()
     net.conv_events.clear()
     l0 = spyker._lib.lib.spk_launch_count()
@@ -282,8 +308,8 @@ def gpu_arm(args, rank, world):
         "vs_baseline": None,
         "dtype": {"fp32": "f32", "bf16x2": "bf16x2-split/f32-acc", "bf16x3": "bf16x3-split/f32-acc"}[args.precision],
         "data": "synthetic (seeded stroke images, MNIST geometry)",
-        "config": {"workload": WORKLOAD.replace("4096 x", f"{BATCH} x"), "global_batch": BATCH * world, "seq_len": T, "parallelism": f"replicas{world}",
-                   "conv_precision": args.precision, "l2": "inputs larger than L2: each step writes its own 1.44 GB layer-1 spike tensor (126 MB L2)"},
+        "config": headline_config(BATCH, world),
+        "conv_precision": args.precision,
         "e2e": {"value": BATCH * world / (e2e_ms * 1e-3), "unit": "images/s", "h2d_bytes_per_step": BATCH * H * H,
                 "d2h_bytes_per_step": int(feats.numel() * feats.element_size())},
         "gpu_launches": int(launches),
@@ -297,19 +323,25 @@ def gpu_arm(args, rank, world):
         "spikes_per_s": spikes_per_step * world / (ms * 1e-3),
         "near_threshold_rechecks_per_step": rechecks,
     }
+    if trajectory:
+        line["trajectory"] = trajectory
+    if args.dump_weights:
+        np.savez(args.dump_weights, conv1=net.conv1.kernel.cpu().numpy(), conv2=net.conv2.kernel.cpu().numpy())
     if fp32 is not None:
         line["fp32_path"] = fp32
     if not args.no_cpu_baseline and world == 1:
         # the CPU leg: the oracle as the timed baseline and as the checker
         line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
         if not args.no_spike_match:
-            line["spike_match"] = spike_match(spyker, torch, dev, args.precision)
+            line["spike_match"] = spike_match(spyker, torch, dev, args.precision,
+                                              (net.conv1.kernel.cpu().numpy(), net.conv2.kernel.cpu().numpy()))
     print(json.dumps(line), flush=True)
 
 
-def spike_match(spyker, torch, dev, precision, n=32):
-    """Spike match %: both layers' fire spikes (fresh weights, no STDP) of
-    this path against the oracle's FP64 pipeline on `n` images."""
+def spike_match(spyker, torch, dev, precision, weights, n=32):
+    """Spike match %: both layers' fire spikes of this path against the
+    oracle's FP64 pipeline on `n` images, with the weights the timed steps'
+    STDP updates reached (the trained regime the bench measures)."""
     import oracle
     from spyker_b200 import synth
     from tests.golden.make_golden import dog_kernel
@@ -317,8 +349,10 @@ def spike_match(spyker, torch, dev, precision, n=32):
     kind = "reference" if oracle.available("reference") else "port"
     o = oracle.get(kind)
     imgs = synth.strokes(n, seed=7)
-    w1, w2 = synth.conv_weights(30, 2, 5, seed=1), synth.conv_weights(100, 30, 5, seed=2)
+    w1, w2 = weights
     net = Network(spyker, torch, dev, precision)
+    net.conv1.kernel.copy_(torch.from_numpy(w1))
+    net.conv2.kernel.copy_(torch.from_numpy(w2))
     x = torch.from_numpy(imgs).to(dev).float().div_(255.0)[:, None]
     codes = spyker.code(net.dog(x), T)
     s1, _, p1 = net._layer(net.conv1, codes, 15.0, 3, 5, 2)
@@ -330,7 +364,7 @@ def spike_match(spyker, torch, dev, precision, n=32):
     r1 = o.fire(o.inhibit(o.threshold(o.conv(ref_codes, w1, (1, 1), (2, 2, 2, 2)), 15.0)))
     r2 = o.fire(o.inhibit(o.threshold(o.conv(o.pool(r1, (2, 2)), w2, (1, 1), (2, 2, 2, 2)), 10.0)))
     return {"layer1_pct": 100.0 * float(np.mean(g1 == r1)), "layer2_pct": 100.0 * float(np.mean(g2 == r2)),
-            "images": n, "oracle": f"{kind} (FP64 convolution)"}
+            "images": n, "oracle": f"{kind} (FP64 convolution)", "weights": "after the timed steps"}
 
 
 # ----------------------------------------------------------------------------
@@ -359,12 +393,24 @@ def reference_step(o, torch, imgs, w1, w2, dk):
     return o.pool(s2, (14, 14))
 
 
+def load_synth():
+    """The synthetic-data module by file path: importing it through the
+    package would load the GPU library into the CPU-only reference arm."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("spyker_synth", os.path.join(ROOT, "spyker_b200", "synth.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
 def _ref_setup():
     import torch
 
     import oracle
-    from spyker_b200 import synth
     from tests.golden.make_golden import dog_kernel
+
+    synth = load_synth()
 
     kind = "reference" if oracle.available("reference") else "port"
     o = oracle.get(kind)
@@ -387,11 +433,15 @@ def cpu_baseline(seconds: float) -> dict:
 
 
 def reference_arm(args, rank, world):
+    """The reference's own CPU implementation on the host cores: a bounded
+    sample of each step's batch (the first `sample` of its 4096 images).  Every
+    op of the CPU path loops over the samples and its STDP scan walks the
+    winners one by one, so its images/s does not depend on the batch size."""
     if rank != 0:
         return
     o, kind, torch, synth, dk = _ref_setup()
-    sample = 256
-    imgs = synth.strokes(sample, seed=100)
+    sample = min(1024, args.batch)
+    imgs = synth.strokes(args.batch, seed=100)[:sample]
     w1, w2 = synth.conv_weights(30, 2, 5, seed=1), synth.conv_weights(100, 30, 5, seed=2)
     for _ in range(args.warmup):
         reference_step(o, torch, imgs, w1, w2, dk)
@@ -404,10 +454,10 @@ def reference_arm(args, rank, world):
         "impl": "reference", "metric": METRIC, "value": v, "unit": "images/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded stroke images, MNIST geometry)",
-        "config": {"workload": WORKLOAD, "global_batch": BATCH, "seq_len": T, "parallelism": "cpu",
-                   "reference_sample_images_per_step": sample},
+        "config": headline_config(args.batch, world),
         "cpu_baseline": {"value": v, "unit": "images/s", "cores": torch.get_num_threads(), "kind": kind,
-                         "sample": f"{sample} images per step through the same pipeline"},
+                         "sample": f"{sample} of each step's {args.batch} images per timed step (the CPU path's "
+                                   f"cost is per image), reference CPU backend + oneDNN convolution via torch"},
         "e2e": {"value": v, "unit": "images/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
@@ -915,6 +965,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32-compare", action="store_true")
     ap.add_argument("--no-spike-match", action="store_true")
+    ap.add_argument("--trajectory", type=int, default=0,
+                    help="after the warm-up, this many synchronised steps recording each layer's exact re-decisions")
+    ap.add_argument("--dump-weights", default="", help="save the trained kernels to this .npz")
     ap.add_argument("--workload", default="kheradpisheh", choices=["kheradpisheh", "gabor256", "backprop", "sweep", "sparse", "rstdp"],
                     help="kheradpisheh: the 2-layer STDP training step (the headline); gabor256: large-image "
                          "forward; backprop: temporal-backprop training of a 3-layer first-spike network; "

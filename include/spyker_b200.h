@@ -177,9 +177,11 @@ spk_status spk_rank_convstdp(const void *in, spk_dtype itype, int64_t b, int64_t
  * nothing.  Calls needing more scratch than that (2*B*count*Cin*KH*KW bytes
  * plus 2*B*count, each rounded up to 256) fail with SPK_ERR_ARGUMENT; split
  * the batch.
- * The first call on a device looks up the array's device address; make that
- * first call before any stream capture.  All calls share the array, so calls
- * that overlap on the GPU (different streams, or other threads) race. */
+ * Every call looks up the array's device address on the current device (a
+ * host-side lookup, no stream work); the first call on a device may also
+ * load the library's device code, so make it before any stream capture.
+ * All calls share the array, so calls that overlap on the GPU (different
+ * streams, or other threads) race. */
 spk_status spk_rank_convstdp_noalloc(const void *in, spk_dtype itype, int64_t b, int64_t t, int64_t cin, int64_t h,
                                      int64_t w, float *kernel, int64_t cout, int64_t kh, int64_t kw, const void *out,
                                      int64_t oh, int64_t ow, const double *configs_host, int64_t nconf,

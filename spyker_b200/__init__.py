@@ -19,8 +19,8 @@ from .module import (FC, ZCA, BPConfig, Conv, conv_fire_wta, DoG, DoGFilter, Gab
                      inhibit, labelize, pad, pool, quantize, random_seed, scatter, set_conv_precision, stdp,
                      threshold)
 from .sparse import SparseTensor, to_sparse
-from .utils import (copy_array, create_array, create_tensor, device, expand2, expand4, shape, to_numpy, to_tensor, to_torch,
-                    wrap_array)
+from .utils import (Tensor, copy_array, create_array, create_tensor, device, expand2, expand4, shape, to_numpy, to_tensor,
+                    to_torch, wrap_array)
 
 __version__ = "0.1.0"
 

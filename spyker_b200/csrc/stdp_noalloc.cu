@@ -13,8 +13,6 @@
 // (2 * B * count * Cin * KH * KW bytes for the receptive fields plus
 // 2 * B * count for the winners, each rounded up to 256 bytes) exceeds it is
 // rejected with SPK_ERR_ARGUMENT; split the batch into smaller calls.
-#include <mutex>
-
 #include "common.cuh"
 
 namespace spk
@@ -34,27 +32,17 @@ constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;
 // winner are written before they are read, and invalid slots are never read.
 static __device__ __align__(256) unsigned char g_stdp_scratch[kNoAllocScratchBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mutex;
-void *g_address[kMaxDevices] = {};
-
 // Device address of the static array on the current device.  In host code
 // `g_stdp_scratch` names a host-side stand-in, not device memory, so the
-// address is looked up once per device with that device current.
+// address is looked up with that device current.  The lookup runs on every
+// call (it is host-only and issues no stream work), so no address outlives a
+// cudaDeviceReset.
 void *scratch_address()
 {
-    int dev = -1;
-    SPK_CUDA(cudaGetDevice(&dev));
-    SPK_REQUIRE(dev >= 0 && dev < kMaxDevices, "device index out of range");
-    std::lock_guard<std::mutex> lock(g_mutex);
-    if (g_address[dev] == nullptr)
-    {
-        void *p = nullptr;
-        SPK_CUDA(cudaGetSymbolAddress(&p, g_stdp_scratch));
-        SPK_REQUIRE(p != nullptr, "no device address for the static scratch");
-        g_address[dev] = p;
-    }
-    return g_address[dev];
+    void *p = nullptr;
+    SPK_CUDA(cudaGetSymbolAddress(&p, g_stdp_scratch));
+    SPK_REQUIRE(p != nullptr, "no device address for the static scratch");
+    return p;
 }
 }  // namespace
 }  // namespace spk

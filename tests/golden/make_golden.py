@@ -30,7 +30,14 @@ ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)
 sys.path.insert(0, ROOT)
 
 import oracle  # noqa: E402
-from spyker_b200 import synth  # noqa: E402
+import importlib.util  # noqa: E402
+
+# the synthetic-data module by file path: the package itself would load the
+# GPU library, which the CPU-only users of this file (bench.py's reference
+# arm) must not do
+_spec = importlib.util.spec_from_file_location("spyker_synth", os.path.join(ROOT, "spyker_b200", "synth.py"))
+synth = importlib.util.module_from_spec(_spec)
+_spec.loader.exec_module(synth)
 
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "cfg0_small.npz")
 CFG = [(0.004, -0.003, 1.0, 0.0, 1.0)]

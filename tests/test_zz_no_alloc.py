@@ -74,3 +74,52 @@ def test_noalloc_rejects_oversized_calls(port):
                                             _lib.f64(CFG), 1, None, None, count, 1, 1, _lib.i64(5, 5, 5, 5), None)
     assert st == 1
     assert b"static scratch" in _lib.lib.spk_last_error()
+
+
+def _cumulative(rng, b, t, c, h, w):
+    first = rng.integers(0, t + 1, size=(b, 1, c, h, w))
+    return (np.arange(t)[None, :, None, None, None] >= first).astype(np.uint8)
+
+
+def test_noalloc_limit_boundary():
+    # 2*B*count*Cin*KH*KW + 2*B*count bytes, each rounded up to 256: exactly
+    # 32 MiB for B=4088, count=8, Cin=8, 8x8 kernels (accepted, and equal to
+    # the workspace entry point), 256 bytes more for B=5592402, count=1,
+    # Cin=1, 1x2 kernels (refused before any launch).
+    def need(b, count, k):
+        a = lambda v: (v + 255) // 256 * 256
+        return a(2 * b * count * k) + a(2 * b * count)
+
+    assert need(4088, 8, 512) == 32 << 20 and need(5592402, 1, 2) == (32 << 20) + 256
+    st = _lib.lib.spk_rank_convstdp_noalloc(None, 4, 5592402, 2, 1, 1, 2, None, 4, 1, 2, None, 1, 1,
+                                            _lib.f64(CFG), 1, None, None, 1, 1, 1, _lib.i64(0, 0, 0, 0), None)
+    assert st == 1 and b"static scratch" in _lib.lib.spk_last_error()
+
+    rng = np.random.default_rng(5)
+    b, t, cin, cout, count = 4088, 2, 8, 16, 8
+    codes = _cumulative(rng, b, t, cin, 8, 8)
+    out = _cumulative(rng, b, t, cout, 1, 1)
+    win = np.zeros((b, count, 5), dtype=np.int32)
+    win[:, :, 2] = rng.integers(0, cout, size=(b, count))
+    cnt = rng.integers(0, count + 1, size=b).astype(np.int32)
+    w = rng.uniform(0.2, 0.9, size=(cout, cin, 8, 8)).astype(np.float32)
+    dev = torch.device("cuda", 0)
+    x, o = torch.from_numpy(codes).to(dev), torch.from_numpy(out).to(dev)
+    rec, cn = torch.from_numpy(win).to(dev), torch.from_numpy(cnt).to(dev)
+    cfg, pad = _lib.f64(CFG), _lib.i64(0, 0, 0, 0)
+    s = torch.cuda.current_stream().cuda_stream
+    got = []
+    for entry in ("workspace", "noalloc"):
+        k = torch.from_numpy(w).to(dev)
+        args = (x.data_ptr(), 4, b, t, cin, 8, 8, k.data_ptr(), cout, 8, 8, o.data_ptr(), 1, 1, cfg, 1,
+                rec.data_ptr(), cn.data_ptr(), count, 1, 1, pad)
+        if entry == "workspace":
+            nb = _lib.lib.spk_rank_convstdp_workspace(b, count, cin, 8, 8, 8, 8)
+            ws = torch.empty(nb, dtype=torch.uint8, device=dev)
+            _lib.call("spk_rank_convstdp", *args, ws.data_ptr(), nb, s)
+        else:
+            _lib.call("spk_rank_convstdp_noalloc", *args, s)
+        torch.cuda.synchronize()
+        got.append(k.cpu().numpy())
+    assert not np.array_equal(got[0], w)
+    assert np.array_equal(got[0], got[1])
