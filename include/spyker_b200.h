@@ -85,6 +85,12 @@ int spk_device_status(int reset);
  * channel decision was within the FP32 error bound and was recomputed with
  * FP64 sums, since the last reset.  Synchronous; reset != 0 clears it. */
 unsigned long long spk_recheck_count(int reset);
+/* Number of rows of the fused layer's first-crossing search that even the
+ * exact term sums left open (a potential within its bound of a rounding
+ * boundary that decides) and that were recomputed from the F32 weights in
+ * the oracle's FP64 order, since the last reset.  Synchronous; reset != 0
+ * clears it. */
+unsigned long long spk_recompute_count(int reset);
 /* Schedule of the tensor-core conv / fused-layer kernels for the calls that
  * follow (0 = automatic): pipeline stages (2..6, capped by shared memory),
  * tensor-memory accumulators (1 or 2, where 2 fit), resident CTAs per SM.

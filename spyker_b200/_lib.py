@@ -25,6 +25,7 @@ SIGNATURES = {
     "spk_launch_count": (C.c_uint64, []),
     "spk_device_status": (_INT, [_INT]),
     "spk_recheck_count": (C.c_ulonglong, [_INT]),
+    "spk_recompute_count": (C.c_ulonglong, [_INT]),
     "spk_set_conv_schedule": (_INT, [_INT, _INT, _INT]),
     "spk_random_seed": (None, [C.c_uint64]),
     "spk_normal_kernel": (_INT, [_P, _I, _D, _D]),

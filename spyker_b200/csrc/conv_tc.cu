@@ -40,6 +40,9 @@ static __device__ int g_tc_status;
 // Rows (one pixel at one step) whose channel decision the FP32 bound could
 // not certify and that were recomputed with FP64 sums.
 static __device__ unsigned long long g_rechecks;
+// Rows of the search path that the term sums could not decide and that
+// were recomputed as the oracle does (search_fix_kernel).
+static __device__ unsigned long long g_recomputes;
 
 namespace
 {
@@ -87,11 +90,30 @@ struct TcParams
     int *negw;
     // kTimes: output times [B, Cout, OH, OW]
     float *tout;
+    // kSearch (the lean first-crossing search, see search_epilogue): round 0
+    // takes every pixel at step T - 1, round 1 the (pixel, step) entries of
+    // list_in, round 2 the (pixel, winner) entries of list_in at step T - 1
+    int round, wta;
+    const int2 *list_in;
+    const int *count_in;
+    int2 *list_out, *final_list;
+    int *count_out, *final_count;
+    int4 *fix_list;  // rows left for the exact recompute: (pixel, step, round, winner)
+    int *fix_count;
+    int4 *state;     // per pixel: (lo | hi << 8 | winner << 16, value, winner at T-1, value at T-1)
+    const float *echan;     // per channel bound of |oracle potential - exact term sum|
+    const unsigned *sinfo;  // [0] largest echan (bits), [1] largest channel exponent + 128
+    int kreal;              // real K (taps x input channels)
+    // kFused: leave at once when the search path ran (no negative weight and
+    // cumulative 0/1 input; these are the words of negw and flag)
+    int skip_when_lean;
 };
 
 // kTimes: the fused (pixel, time) rows with an epilogue that writes each
 // neuron's first step above threshold (F32 time, T = never).
-constexpr int kPotentials = 0, kFused = 1, kTimes = 2;
+constexpr int kPotentials = 0, kFused = 1, kTimes = 2, kSearch = 3;
+// Terms of the fixed-grid weight split of the search kernels.
+constexpr int kSearchTerms = 3;
 
 __device__ __forceinline__ unsigned order_enc(float f)
 {
@@ -924,6 +946,422 @@ __device__ __forceinline__ void fused_producer(const TcParams &P, const int4 *ta
     }
 }
 
+// ---- lean first-crossing search (kSearch) ------------------------------------
+// With no negative weight and cumulative 0/1 input spikes every potential
+// V_c(t) is non-decreasing in t.  When the thresholds satisfy
+// value <= inhibit, fire, WTA thresholds <= threshold, each of those tests on
+// the thresholded potential is the test V_c(t) > threshold, so one output
+// pixel is fixed by t0, the first step at which some channel exceeds the
+// threshold, and by w, the first channel of largest potential at t0
+// (cpu/inhibit.cpp:41-121 takes the winner at step T - #steps above):
+//   spikes   channel w from t0 to T - 1, nothing else (cpu/fire.cpp:67-82);
+//   record   (w, t0, V_w(t0)), the WTA key of cpu/wta.cpp:53-62;
+//   min/max  0 from the losing channels, `value` below the threshold, and
+//            V_w(T - 1) as the sample's largest inhibited potential.
+// A pixel with nothing above the threshold at T - 1 never fires (record
+// (0, T, value)).  The search evaluates one (pixel, step) row per pixel and
+// round: round 0 every pixel at T - 1, then a bisection of (lo, hi] over the
+// crossing pixels, then (with WTA) V_w(T - 1) where w is not also the
+// largest channel at T - 1.  ceil(log2 T) + 2 rows at most per crossing
+// pixel against T for the dense layer.
+//
+// Every decision is the oracle's: the potential of a row is the F32 rounding
+// of the FP64 sum of its products in (channel, ky, kx) order.  The weights
+// are split on fixed per-channel grids (fixed_split_kernel), so each
+// tensor-memory sum is exact and their total r_q is within echan[c] of the
+// oracle's FP64 sum.  Tier 1 adds the terms in FP32 and decides when the
+// rigorous bound 3.125 * 2^-24 |f| + c0 separates the largest potential from
+// the threshold and from the runner-up by more than an ulp; the winner's
+// value is then r_q rounded once, kept when r_q +- echan stays inside that
+// float's rounding interval.  Tier 2 (rows tier 1 leaves open) does the same
+// for every channel of the row and decides on the exact values, with the
+// possible neighbours of each uncertified one.  Rows still open go to
+// search_fix_kernel, which recomputes them as the oracle does.
+template <int NS>
+__device__ __forceinline__ void s_chunk(uint32_t lane_base, int c0, int n_tile, uint32_t (&q)[NS][kEpiChunk])
+{
+#pragma unroll
+    for (int j = 0; j < NS; ++j) tmem_ld8(lane_base + uint32_t(j * n_tile + c0), q[j]);
+}
+
+template <int NS>
+__device__ __forceinline__ void s_chunk_wait(uint32_t (&q)[NS][kEpiChunk])
+{
+#pragma unroll
+    for (int j = 0; j < NS; ++j) tmem_ld_wait8(q[j]);
+}
+
+template <int NS>
+__device__ __forceinline__ float s_fast(const uint32_t (&q)[NS][kEpiChunk], int j)
+{
+    float f = __fadd_rn(__uint_as_float(q[0][j]), __uint_as_float(q[1][j]));
+#pragma unroll
+    for (int i = 2; i < NS; ++i) f = __fadd_rn(f, __uint_as_float(q[i][j]));
+    return f;
+}
+
+// The exact sum of the terms (every term sum is a multiple of its grid and the
+// total spans at most 42 bits, so the FP64 additions are exact).
+template <int NS>
+__device__ __forceinline__ double s_exact(const uint32_t (&q)[NS][kEpiChunk], int j)
+{
+    double d = double(__uint_as_float(q[0][j]));
+#pragma unroll
+    for (int i = 1; i < NS; ++i) d += double(__uint_as_float(q[i][j]));
+    return d;
+}
+
+// Rounding of an exact sum S to P = float(S): lo / hi are the smallest and
+// largest float a value within E of S rounds to (ties at a boundary count
+// as both sides).
+__device__ __forceinline__ void s_round(double S, float E, float &P, float &lo, float &hi)
+{
+    P = float(S);
+    const double rho = S - double(P);
+    const double up = (double(nextafterf(P, INFINITY)) - double(P)) * 0.5;
+    const double dn = (double(P) - double(nextafterf(P, -INFINITY))) * 0.5;
+    hi = (rho + double(E) < up) ? P : nextafterf(P, INFINITY);
+    lo = (double(E) - rho < dn) ? P : nextafterf(P, -INFINITY);
+}
+
+// Exact term sum of column `col` of this lane's row (col < 0: none), the
+// warp's columns fetched one 8-column chunk at a time.  Warp-uniform.
+template <int NS>
+__device__ __forceinline__ double s_reload(uint32_t lane_base, int n_tile, int col)
+{
+    uint32_t pick[NS];
+#pragma unroll
+    for (int i = 0; i < NS; ++i) pick[i] = 0u;
+    unsigned pending = __ballot_sync(0xffffffffu, col >= 0);
+    while (pending)
+    {
+        const int c0 = (__shfl_sync(0xffffffffu, col, __ffs(pending) - 1) >> 3) << 3;
+        uint32_t q[NS][kEpiChunk];
+        s_chunk<NS>(lane_base, c0, n_tile, q);
+        s_chunk_wait<NS>(q);
+        const bool mine = col >= 0 && (col >> 3) == (c0 >> 3);
+        const int jj = col - c0;
+#pragma unroll
+        for (int j = 0; j < kEpiChunk; ++j)
+#pragma unroll
+            for (int i = 0; i < NS; ++i) pick[i] = (mine && jj == j) ? q[i][j] : pick[i];
+        pending &= ~__ballot_sync(0xffffffffu, mine);
+    }
+    double S = double(__uint_as_float(pick[0]));
+#pragma unroll
+    for (int i = 1; i < NS; ++i) S += double(__uint_as_float(pick[i]));
+    return S;
+}
+
+// Tier 2: every channel of the row from its exact sum.  dec: 0 open, 1 no
+// channel above thr, 2 crossing with winner a (first of the largest) of value v.
+template <int NS>
+__device__ __forceinline__ void s_tier2(const TcParams &P, uint32_t lane_base, float thr, int &dec, int &a, float &v)
+{
+    float mlo = -INFINITY, hmax = -INFINITY, hun = -INFINITY, vs = -INFINITY;
+    int as = -1;
+    for (int c0 = 0; c0 < P.n_tile; c0 += kEpiChunk)
+    {
+        uint32_t q[NS][kEpiChunk];
+        s_chunk<NS>(lane_base, c0, P.n_tile, q);
+        s_chunk_wait<NS>(q);
+#pragma unroll
+        for (int j = 0; j < kEpiChunk; ++j)
+        {
+            const int c = c0 + j;
+            const bool real = c < P.cout;
+            float pc, lo, hi;
+            s_round(s_exact<NS>(q, j), real ? __ldg(P.echan + c) : 0.f, pc, lo, hi);
+            if (!real) lo = hi = pc = -INFINITY;
+            mlo = fmaxf(mlo, lo);
+            hmax = fmaxf(hmax, hi);
+            const bool exact = lo == hi;
+            const bool better = exact && pc > vs;
+            vs = better ? pc : vs;
+            as = better ? c : as;
+            hun = exact ? hun : fmaxf(hun, hi);
+        }
+    }
+    dec = 0;
+    if (mlo > thr)
+    {
+        // the winner is among the channels that can reach mlo: decided when
+        // all of them are exact
+        if (hun < mlo && as >= 0) dec = 2, a = as, v = vs;
+    }
+    else if (hmax <= thr)
+        dec = 1;
+}
+
+// What a decided row does to its pixel (shared by the epilogue and the exact
+// recompute).  Returns the list entries to append and the sample maximum to
+// raise.
+struct SearchAct
+{
+    bool next = false, fin = false, max = false, thv = false;
+    int2 next_e, fin_e;
+    float maxv = 0.f;
+};
+
+__device__ __forceinline__ int4 s_pack(int lo, int hi, int w, float v, int at, float vt)
+{
+    return make_int4((lo & 0xFF) | ((hi & 0xFF) << 8) | (w << 16), __float_as_int(v), at, __float_as_int(vt));
+}
+
+__device__ __forceinline__ SearchAct search_act(const TcParams &P, int round, int pix, int t, int dec, int a,
+                                                float v)
+{
+    SearchAct r;
+    const int T = P.T;
+    if (round == 2)
+    {
+        r.max = true, r.maxv = v;
+        return r;
+    }
+    int lo, hi, w, at;
+    float vh, vt;
+    if (round == 0)
+    {
+        if (dec == 1)
+        {
+            P.records[pix] = make_int4(0, T, __float_as_int(P.thv), 0);
+            r.thv = true;
+            return r;
+        }
+        lo = -1, hi = T - 1, w = a, vh = v, at = a, vt = v;
+    }
+    else
+    {
+        const int4 s = P.state[pix];
+        lo = int(int8_t(s.x & 0xFF)), hi = int(int8_t((s.x >> 8) & 0xFF)), w = s.x >> 16;
+        vh = __int_as_float(s.y), at = s.z, vt = __int_as_float(s.w);
+        if (dec == 2)
+            hi = t, w = a, vh = v;
+        else
+            lo = t;
+    }
+    if (hi - lo > 1)
+    {
+        P.state[pix] = s_pack(lo, hi, w, vh, at, vt);
+        r.next = true, r.next_e = make_int2(pix, (lo + hi) >> 1);
+        return r;
+    }
+    // t0 = hi: the pixel is settled
+    P.records[pix] = make_int4(w, hi, __float_as_int(vh), 0);
+    if (P.wta)
+    {
+        r.thv = hi > 0;
+        if (w == at)
+            r.max = true, r.maxv = vt;
+        else
+            r.fin = true, r.fin_e = make_int2(pix, w);
+    }
+    return r;
+}
+
+// Warp-aggregated append of this lane's entry (if any) to a list.
+template <typename E>
+__device__ __forceinline__ void s_append(bool want, const E &e, E *list, int *count)
+{
+    const unsigned m = __ballot_sync(0xffffffffu, want);
+    if (!m) return;
+    const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(count, __popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (want) list[base + __popc(m & ((1u << lane) - 1u))] = e;
+}
+
+__device__ __forceinline__ void s_extremes(const TcParams &P, int pix, const SearchAct &r)
+{
+    const int smp = pix / int(P.ohw);
+    if (r.max) atomicMax(P.maxs + smp, order_enc(r.maxv));
+    if (r.thv && P.thv != 0.f)
+    {
+        atomicMin(P.mins + smp, order_enc(P.thv));
+        atomicMax(P.maxs + smp, order_enc(P.thv));
+    }
+}
+
+// Search epilogue of one row per thread (warps 0-3).  `c0` is the per-launch
+// part of the tier-1 bound.
+template <int NS>
+__device__ void search_epilogue(const TcParams &P, uint32_t acc, bool ok, int pix, int t, int aux, uint64_t *release,
+                                float c0)
+{
+    const int warp = threadIdx.x >> 5;
+    const uint32_t lane_base = acc + (uint32_t((warp & 3) * 32) << 16);
+    const float thr = P.thr;
+    int dec = 0, a = -1;
+    float v = 0.f;
+    if (P.round == 2)
+    {
+        const double S = s_reload<NS>(lane_base, P.n_tile, ok ? aux : -1);
+        tc_fence_before();
+        mbar_arrive(release);
+        if (ok)
+        {
+            float lo, hi;
+            s_round(S, __ldg(P.echan + aux), v, lo, hi);
+            dec = lo == hi ? 2 : 0;
+            a = aux;
+        }
+    }
+    else
+    {
+        // tier 1: the largest potential (first index), its runner-up
+        LeanMax st, st2;
+        {
+            constexpr int W = kEpiChunk;
+            uint32_t qa[NS][W], qb[NS][W];
+            s_chunk<NS>(lane_base, 0, P.n_tile, qa);
+            for (int cb = 0; cb < P.n_tile; cb += 2 * W)
+            {
+                s_chunk_wait<NS>(qa);
+                s_chunk<NS>(lane_base, cb + W, P.n_tile, qb);
+                const int lim = P.cout - cb;
+#pragma unroll
+                for (int j = 0; j < W; ++j)
+                {
+                    const float f = j < lim ? s_fast<NS>(qa, j) : -INFINITY;
+                    const bool gt = f > st.r1;
+                    st.r2 = gt ? st.r1 : fmaxf(st.r2, f);
+                    st.r1 = gt ? f : st.r1;
+                    st.a1 = gt ? cb + j : st.a1;
+                }
+                s_chunk_wait<NS>(qb);
+                if (cb + 2 * W < P.n_tile) s_chunk<NS>(lane_base, cb + 2 * W, P.n_tile, qa);
+                const int lim2 = lim - W;
+#pragma unroll
+                for (int j = 0; j < W; ++j)
+                {
+                    const float f = j < lim2 ? s_fast<NS>(qb, j) : -INFINITY;
+                    const bool gt = f > st2.r1;
+                    st2.r2 = gt ? st2.r1 : fmaxf(st2.r2, f);
+                    st2.r1 = gt ? f : st2.r1;
+                    st2.a1 = gt ? cb + W + j : st2.a1;
+                }
+            }
+            merge_lean(st, st2);
+        }
+        const float tol1 = __fmaf_ru(fabsf(st.r1), 0x1.9p-23f, c0);
+        int d1 = 0;  // tier-1 decision
+        if (__fadd_ru(st.r1, tol1) <= thr)
+            d1 = 1;
+        else if (__fsub_rd(st.r1, tol1) >= nextafterf(thr, INFINITY))
+        {
+            const float tol2 = __fmaf_ru(fabsf(st.r2), 0x1.9p-23f, c0);
+            const float gap = __fsub_rd(__fsub_rd(st.r1, tol1), __fadd_ru(st.r2, tol2));
+            if (gap > __fmaf_ru(fabsf(st.r1), 0x1p-23f, 0x1p-126f)) d1 = 2;
+        }
+        // the winner's exact value for tier-1 crossings; tier 2 for the rest
+        const double S = s_reload<NS>(lane_base, P.n_tile, (ok && d1 == 2) ? st.a1 : -1);
+        int d2 = 0, a2 = -1;
+        float v2 = 0.f;
+        const unsigned open1 = __ballot_sync(0xffffffffu, ok && d1 == 0);
+        if (open1)
+        {
+            if ((threadIdx.x & 31) == 0) atomicAdd(&g_rechecks, (unsigned long long)__popc(open1));
+            s_tier2<NS>(P, lane_base, thr, d2, a2, v2);
+        }
+        tc_fence_before();
+        mbar_arrive(release);
+        if (ok)
+        {
+            if (d1 == 1)
+                dec = 1;
+            else if (d1 == 2)
+            {
+                float lo, hi;
+                s_round(S, __ldg(P.echan + st.a1), v, lo, hi);
+                a = st.a1;
+                dec = lo == hi ? 2 : 0;
+            }
+            else
+                dec = d2, a = a2, v = v2;
+        }
+    }
+    SearchAct r;
+    if (ok && dec != 0) r = search_act(P, P.round, pix, t, dec, a, v);
+    s_append(ok && dec == 0, make_int4(pix, t, P.round, aux), P.fix_list, P.fix_count);
+    s_append(r.next, r.next_e, P.list_out, P.count_out);
+    s_append(r.fin, r.fin_e, P.final_list, P.final_count);
+    if (ok && P.wta) s_extremes(P, pix, r);
+}
+
+// Search producers: thread p (0..255) builds four (row, 8-wide K chunk)
+// units of every K block, one row each at that row's own step; the 8 lanes
+// of a quarter warp take 8 consecutive rows of one chunk (distinct 16-byte
+// bank groups).
+__device__ __forceinline__ int2 search_entry(const TcParams &P, int64_t idx)
+{
+    if (P.round == 0) return make_int2(int(idx), P.T - 1);
+    const int2 e = P.list_in[idx];
+    return P.round == 1 ? e : make_int2(e.x, P.T - 1);
+}
+
+__device__ __forceinline__ FusedPixel pixel_of(const TcParams &P, bool ok, int gp)
+{
+    FusedPixel u{};
+    u.ok = ok;
+    if (ok)
+    {
+        const uint32_t ohw = uint32_t(P.ohw), smp = uint32_t(gp) / ohw, pix = uint32_t(gp) - smp * ohw;
+        u.sample = smp;
+        const int oy = int(pix / uint32_t(P.ow)), ox = int(pix) - oy * P.ow;
+        u.iy0 = oy * P.sy - P.top;
+        u.ix0 = ox * P.sx - P.left;
+    }
+    return u;
+}
+
+__device__ __forceinline__ void search_producer(const TcParams &P, const int4 *tab, unsigned char *smem,
+                                                uint64_t *full_bar, uint64_t *empty_bar, int S, int stage_bytes,
+                                                int a_bytes, int b_bytes, int p, int64_t nrows, int64_t ntiles)
+{
+    int urow[4], ukc[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+    {
+        const int q = p + i * 256;
+        urow[i] = (q & 7) + 8 * (q >> 6), ukc[i] = (q >> 3) & 7;
+    }
+    uint32_t it = 0;
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
+    {
+        FusedPixel fu[4];
+        int ut[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+        {
+            const int64_t idx = tile * BM + urow[i];
+            const bool ok = idx < nrows;
+            const int2 e = ok ? search_entry(P, idx) : make_int2(0, 0);
+            fu[i] = pixel_of(P, ok, e.x);
+            ut[i] = e.y;
+        }
+        for (int kb = 0; kb < P.kblocks; ++kb, ++it)
+        {
+            uint2 f[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) f[i] = fst_chunk(P, tab, fu[i], kb, ukc[i]);
+            const int s = int(it % uint32_t(S));
+            const uint32_t u = it / uint32_t(S);
+            if (u > 0 && !wait_bounded(&empty_bar[s], (u - 1) & 1)) return;
+            unsigned char *sA = smem + s * stage_bytes;
+            if (p == 0)
+            {
+                arrive_expect_tx(&full_bar[s], uint32_t(b_bytes));
+                bulk_g2s(sA + a_bytes, P.wimg + int64_t(kb) * b_bytes, uint32_t(b_bytes), &full_bar[s]);
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i) store_fst_rows(sA, urow[i], ut[i], 1, ukc[i], f[i], 0);
+            fence_proxy_async_smem();
+            mbar_arrive(&full_bar[s]);
+        }
+    }
+}
+
 // Warp-specialised persistent kernel (416 threads):
 //   warps 4-11 producers: per K block, wait for a free stage, bulk-copy the
 //              weight block (thread 128) and gather half an A row each;
@@ -945,6 +1383,22 @@ __global__ void __launch_bounds__(kWsThreads, 1) conv_ws_kernel(TcParams P)
     __shared__ __align__(8) uint64_t full_bar[kMaxStages], empty_bar[kMaxStages], accf_bar[2], acce_bar[2], tim_bar;
     __shared__ uint32_t tmem_slot;
 
+    // the search kernels run only on the lean path, the dense fused kernel
+    // only off it (both words are set before the launch; uniform exit)
+    if constexpr (MODE == kSearch)
+    {
+        if (*P.negw || *P.flag) return;
+    }
+    if constexpr (MODE == kFused)
+    {
+        if (P.skip_when_lean && !*P.negw && !*P.flag) return;
+    }
+    int64_t nrows = 0, ntiles = P.tiles;
+    if constexpr (MODE == kSearch)
+    {
+        nrows = P.round == 0 ? P.npix : int64_t(*P.count_in);
+        ntiles = ceil_div(nrows, BM);
+    }
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int S = P.stages, nacc = P.nacc;
     const int a_bytes = BM * BK * 2;
@@ -1001,7 +1455,9 @@ __global__ void __launch_bounds__(kWsThreads, 1) conv_ws_kernel(TcParams P)
     const uint32_t tmem = tmem_slot;
     const int acc_cols = P.nsplit * P.n_tile;
 
-    if (MODE != kPotentials && warp >= 4 && warp < 12)
+    if (MODE == kSearch && warp >= 4 && warp < 12)
+        search_producer(P, tab, smem, full_bar, empty_bar, S, stage_bytes, a_bytes, b_bytes, tid - 128, nrows, ntiles);
+    else if (MODE != kPotentials && warp >= 4 && warp < 12)
     {
         // ---------------- fused producers (8 warps) ----------------
         if (P.tp_log2 >= 2)
@@ -1074,7 +1530,7 @@ __global__ void __launch_bounds__(kWsThreads, 1) conv_ws_kernel(TcParams P)
         {
             uint32_t it = 0, j = 0;
             bool failed = false;
-            for (int64_t tile = blockIdx.x; tile < P.tiles && !failed; tile += gridDim.x, ++j)
+            for (int64_t tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x, ++j)
             {
                 const int a = int(j % uint32_t(nacc));
                 const uint32_t ua = j / uint32_t(nacc);
@@ -1122,8 +1578,17 @@ __global__ void __launch_bounds__(kWsThreads, 1) conv_ws_kernel(TcParams P)
         // ---------------- epilogue (warps 0-3) ----------------
         // warp w reads tensor-memory lanes 32 w .. 32 w + 31 (rows of the tile)
         const int row = (warp & 3) * 32 + lane;
+        float c0 = 0.f;
+        if constexpr (MODE == kSearch)
+        {
+            // the launch-wide part of the tier-1 bound: 6.25 * 2^-24 times the
+            // largest third-term sums, plus the largest channel bound
+            const float emx = __uint_as_float(P.sinfo[0]);
+            const float lmax = ldexpf(float(P.kreal), int(P.sinfo[1]) - 128 - 16);
+            c0 = __fadd_ru(__fmaf_ru(lmax, 0x1.9p-22f, emx), 0x1p-126f);
+        }
         uint32_t j = 0;
-        for (int64_t tile = blockIdx.x; tile < P.tiles; tile += gridDim.x, ++j)
+        for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++j)
         {
             const int a = int(j % uint32_t(nacc));
             const uint32_t ua = j / uint32_t(nacc);
@@ -1131,7 +1596,8 @@ __global__ void __launch_bounds__(kWsThreads, 1) conv_ws_kernel(TcParams P)
             tc_fence_after();
             const int64_t mt = tile / P.n_tiles;
             const int nt = int(tile % P.n_tiles);
-            const RowInfo r = row_info<MODE>(P, mt, row);
+            RowInfo r{};
+            if constexpr (MODE != kSearch) r = row_info<MODE>(P, mt, row);
             const uint32_t acc = tmem + uint32_t(a * acc_cols);
             if constexpr (MODE == kPotentials)
             {
@@ -1158,6 +1624,19 @@ __global__ void __launch_bounds__(kWsThreads, 1) conv_ws_kernel(TcParams P)
                     times_epilogue<3>(P, acc, r.ok, mt, &acce_bar[a], s_cand, j, &tim_bar);
                 else
                     times_epilogue<2>(P, acc, r.ok, mt, &acce_bar[a], s_cand, j, &tim_bar);
+            }
+            else if constexpr (MODE == kSearch)
+            {
+                const int64_t idx = mt * BM + row;
+                const bool ok = idx < nrows;
+                int2 e = make_int2(0, 0);
+                int aux = 0;
+                if (ok)
+                {
+                    e = search_entry(P, idx);
+                    if (P.round == 2) aux = P.list_in[idx].y;
+                }
+                search_epilogue<kSearchTerms>(P, acc, ok, e.x, e.y, aux, &acce_bar[a], c0);
             }
             else if constexpr (MODE == kFused)
             {
@@ -1321,6 +1800,304 @@ __global__ void __launch_bounds__(128) wta_records_warp_kernel(const int4 *__res
     if (lane == 0) counts[b] = found;
 }
 
+// ---- search path: weight split, exact recompute, outputs ---------------------
+// Fixed-grid split of output channel n's weights into NS BF16 terms (one CTA
+// per channel of the padded tile).  With 2^e the smallest power of two at or
+// above the channel's largest |w| (clamped to [2^-100, 2^100] so that every
+// grid is a normal BF16 number), term j is the digit of the remainder on the
+// grid 2^(e - 8 (j + 1)), rounded to nearest: |digit| <= 256 for the first
+// term and <= 128 after, exact in BF16.  A product with a 0/1 spike is then
+// a multiple of its term's grid and every tensor-memory sum over K < 2^16
+// taps is exact.  echan[n] bounds |oracle - exact term total| for any 0/1
+// input: the sum of the remainders below the last grid (zero for weights in
+// [2^(e-1), 2^e] with NS = 3) plus K^2 2^(e-52) for the FP64 rounding of
+// the oracle's ordered sum of K products, rounded up.  Layout as
+// split_weights_kernel's (one N tile).
+template <int NS>
+__global__ void __launch_bounds__(256) fixed_split_kernel(const float *__restrict__ kernel, uint4 *__restrict__ wimg,
+                                                          int cout, int cin, int taps, int nhwc, int cpad,
+                                                          int kblocks, int n_tile, float *__restrict__ echan,
+                                                          unsigned *__restrict__ sinfo, int *__restrict__ negw)
+{
+    __shared__ float s_mx[8];
+    __shared__ double s_err[8];
+    const int n = blockIdx.x, tid = threadIdx.x;
+    const int kreal = nhwc ? taps * cpad : taps * cin;
+    const int K = kblocks * BK;
+    auto weight = [&](int k) -> float {
+        if (n >= cout || k >= kreal) return 0.f;
+        int c, tap;
+        if (nhwc)
+            tap = k / cpad, c = k % cpad;
+        else
+            c = k / taps, tap = k % taps;
+        return c < cin ? kernel[(int64_t(n) * cin + c) * taps + tap] : 0.f;
+    };
+    float mx = 0.f;
+    bool neg = false;
+    for (int k = tid; k < K; k += blockDim.x)
+    {
+        const float w = weight(k);
+        mx = fmaxf(mx, fabsf(w));
+        neg |= !(w >= 0.f);
+    }
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((tid & 31) == 0) s_mx[tid >> 5] = mx;
+    __syncthreads();
+    mx = s_mx[0];
+    for (int i = 1; i < int(blockDim.x >> 5); ++i) mx = fmaxf(mx, s_mx[i]);
+    int e = 0;
+    if (mx > 0.f)
+    {
+        int ex;
+        const float fr = frexpf(mx, &ex);  // mx = fr 2^ex, fr in [0.5, 1)
+        e = fr == 0.5f ? ex - 1 : ex;
+    }
+    e = max(-100, min(100, e));
+    double err = 0.0;
+    for (int i = tid; i < kblocks * 8; i += blockDim.x)
+    {
+        const int kb = i / 8, kc = i % 8;
+        uint32_t parts[NS][4];
+#pragma unroll
+        for (int e8 = 0; e8 < 8; e8 += 2)
+        {
+            uint32_t bits[2][NS];
+#pragma unroll
+            for (int q = 0; q < 2; ++q)
+            {
+                double r = double(weight(kb * BK + kc * 8 + e8 + q));
+#pragma unroll
+                for (int j = 0; j < NS; ++j)
+                {
+                    const double g = ldexp(1.0, e - 8 * (j + 1));
+                    const double d = rint(r / g) * g;
+                    r -= d;
+                    bits[q][j] = __bfloat16_as_ushort(__float2bfloat16_rn(float(d)));
+                }
+                err += fabs(r);
+            }
+#pragma unroll
+            for (int j = 0; j < NS; ++j) parts[j][e8 / 2] = bits[0][j] | (bits[1][j] << 16);
+        }
+#pragma unroll
+        for (int j = 0; j < NS; ++j)
+        {
+            const int64_t idx = (int64_t(kb) * NS + j) * (int64_t(n_tile) * 8) + (n / 8) * 64 + kc * 8 + (n % 8);
+            wimg[idx] = make_uint4(parts[j][0], parts[j][1], parts[j][2], parts[j][3]);
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) err += __shfl_xor_sync(0xffffffffu, err, o);
+    if ((tid & 31) == 0) s_err[tid >> 5] = err;
+    if (neg && n < cout) atomicOr(negw, 1);
+    __syncthreads();
+    if (tid == 0)
+    {
+        err = s_err[0];
+        for (int i = 1; i < int(blockDim.x >> 5); ++i) err += s_err[i];
+        const double bound = err + double(kreal) * double(kreal) * ldexp(1.0, e - 52);
+        const float eb = __double2float_ru(bound);
+        echan[n] = eb;
+        if (n < cout)
+        {
+            atomicMax(sinfo + 0, __float_as_uint(eb));
+            atomicMax(sinfo + 1, unsigned(e + 128));
+        }
+    }
+}
+
+// Per sample min / max of the inhibited potentials before the search adds to
+// them: on the search path the losing channels' zeros, on the dense path the
+// identities of the min / max (that kernel adds every value itself).
+__global__ void search_init_kernel(unsigned *mins, unsigned *maxs, int64_t b, const int *negw, const int *flag)
+{
+    const bool lean = !*negw && !*flag;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < b; i += int64_t(gridDim.x) * blockDim.x)
+    {
+        mins[i] = lean ? order_enc(0.f) : 0xFFFFFFFFu;
+        maxs[i] = lean ? order_enc(0.f) : 0u;
+    }
+}
+
+// Rows the search could not decide from the term sums (a potential within
+// echan of a rounding boundary that matters), recomputed as the oracle does:
+// per channel the FP64 sum of the F32 weights of the active inputs in
+// (channel, ky, kx) order (the oracle's convolution loop), rounded once to
+// F32.  One warp per row; its lanes take the output channels.
+__global__ void __launch_bounds__(128) search_fix_kernel(TcParams P, const float *__restrict__ kernel, int cp)
+{
+    if (*P.negw || *P.flag) return;
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = int64_t(gridDim.x) * (blockDim.x >> 5);
+    const int n = *P.fix_count;
+    const int taps = P.kh * P.kw;
+    for (int64_t q = int64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); q < n; q += nw)
+    {
+        const int4 e = P.fix_list[q];
+        const int pix = e.x, t = e.y, round = e.z, aux = e.w;
+        const int smp = pix / int(P.ohw), pp = pix - smp * int(P.ohw);
+        const int oy = pp / P.ow, ox = pp - oy * P.ow;
+        const int iy0 = oy * P.sy - P.top, ix0 = ox * P.sx - P.left;
+        const uint8_t *fm = P.in + int64_t(smp) * P.img_stride;
+        float best = -INFINITY, mine = 0.f;
+        int besti = INT_MAX;
+        for (int o = lane; o < P.cout; o += 32)
+        {
+            if (round == 2 && o != aux) continue;
+            double acc = 0.0;
+            const float *wk = kernel + int64_t(o) * P.cin * taps;
+            for (int c = 0; c < P.cin; ++c)
+                for (int ky = 0; ky < P.kh; ++ky)
+                {
+                    const int iy = iy0 + ky;
+                    if (iy < 0 || iy >= P.h) continue;
+                    for (int kx = 0; kx < P.kw; ++kx)
+                    {
+                        const int ix = ix0 + kx;
+                        if (ix < 0 || ix >= P.w) continue;
+                        if (int(fm[(int64_t(iy) * P.w + ix) * cp + c]) <= t)
+                            acc += double(wk[(c * P.kh + ky) * P.kw + kx]);
+                    }
+                }
+            const float pv = float(acc);
+            if (pv > best) best = pv, besti = o;
+            if (o == aux) mine = pv;
+        }
+        // first channel of the largest potential across the lanes
+        for (int off = 16; off > 0; off >>= 1)
+        {
+            const float ob = __shfl_xor_sync(0xffffffffu, best, off);
+            const int oi = __shfl_xor_sync(0xffffffffu, besti, off);
+            if (ob > best || (ob == best && oi < besti)) best = ob, besti = oi;
+        }
+        mine = __shfl_sync(0xffffffffu, mine, aux & 31);
+        if (lane == 0)
+        {
+            atomicAdd(&g_recomputes, 1ull);
+            int dec, a;
+            float v;
+            if (round == 2)
+                dec = 2, a = aux, v = mine;
+            else if (best > P.thr)
+                dec = 2, a = besti, v = best;
+            else
+                dec = 1, a = -1, v = 0.f;
+            const SearchAct r = search_act(P, round, pix, t, dec, a, v);
+            if (r.next) P.list_out[atomicAdd(P.count_out, 1)] = r.next_e;
+            if (r.fin) P.final_list[atomicAdd(P.final_count, 1)] = r.fin_e;
+            if (P.wta) s_extremes(P, pix, r);
+        }
+    }
+}
+
+// Per-pixel spike codes w | t0 << 16 (t0 = T: never) of maps too large to
+// stage in shared memory.
+__global__ void search_codes_kernel(const int4 *__restrict__ records, uint32_t *__restrict__ codes, int64_t npix,
+                                    int T, const int *negw, const int *flag)
+{
+    if (*negw || *flag) return;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < npix; i += int64_t(gridDim.x) * blockDim.x)
+    {
+        const int4 r = records[i];
+        codes[i] = uint32_t(r.x & 0xFFFF) | (uint32_t(min(r.y, T)) << 16);
+    }
+}
+
+// Spikes (and pooled spikes) of the search path from the per-pixel records:
+// channel w fires from step t0 on.  A CTA per sample writes its
+// [T, C, OH, OW] block as 16-byte words (and [T, C, POH, POW] when pooling:
+// a cell fires where any pixel of its window does), with the sample's codes
+// staged in shared memory (or read from `gcodes` for maps above 16384
+// pixels).  Off the search path (negative weights or other input) it writes
+// zeros, which the dense kernel then fills.
+__global__ void __launch_bounds__(256) search_write_kernel(const int4 *__restrict__ records,
+                                                           const uint32_t *__restrict__ gcodes, const int *negw,
+                                                           const int *flag, uint8_t *__restrict__ spikes,
+                                                           uint8_t *__restrict__ pooled, int64_t b, int T, int C,
+                                                           int ohw, int ow, int pky, int pkx, int poh, int pow_)
+{
+    extern __shared__ uint32_t scode[];  // per pixel: w | t0 << 16 (t0 = T: never)
+    const bool lean = !*negw && !*flag;
+    for (int64_t smp = blockIdx.x; smp < b; smp += gridDim.x)
+    {
+        const uint32_t *code = gcodes ? gcodes + smp * ohw : scode;
+        if (lean && !gcodes)
+        {
+            for (int p = threadIdx.x; p < ohw; p += blockDim.x)
+            {
+                const int4 r = records[smp * ohw + p];
+                scode[p] = uint32_t(r.x & 0xFFFF) | (uint32_t(min(r.y, T)) << 16);
+            }
+        }
+        __syncthreads();
+        for (int pass = 0; pass < (pooled ? 2 : 1); ++pass)
+        {
+            const int hw = pass == 0 ? ohw : poh * pow_;
+            const int64_t n = int64_t(T) * C * hw;
+            uint8_t *dst = (pass == 0 ? spikes : pooled) + smp * n;
+            // value of byte f of the block
+            auto spike = [&](int64_t f) -> uint32_t {
+                if (!lean) return 0u;
+                const int plane = int(f / hw), px = int(f - int64_t(plane) * hw);
+                const int t = plane / C, c = plane - t * C;
+                if (pass == 0)
+                {
+                    const uint32_t k = code[px];
+                    return (int(k & 0xFFFF) == c && int(k >> 16) <= t) ? 1u : 0u;
+                }
+                const int py = px / pow_, pxx = px - py * pow_;
+                uint32_t any = 0;
+                for (int dy = 0; dy < pky; ++dy)
+                    for (int dx = 0; dx < pkx; ++dx)
+                    {
+                        const uint32_t k = code[(py * pky + dy) * ow + pxx * pkx + dx];
+                        any |= (int(k & 0xFFFF) == c && int(k >> 16) <= t) ? 1u : 0u;
+                    }
+                return any;
+            };
+            const uintptr_t a = reinterpret_cast<uintptr_t>(dst);
+            const int64_t head = std::min<int64_t>(n, int64_t((16 - (a & 15)) & 15));
+            const int64_t words = (n - head) / 16;
+            for (int64_t f = threadIdx.x; f < head; f += blockDim.x) dst[f] = uint8_t(spike(f));
+            for (int64_t f = head + words * 16 + threadIdx.x; f < n; f += blockDim.x) dst[f] = uint8_t(spike(f));
+            uint4 *d4 = reinterpret_cast<uint4 *>(dst + head);
+            for (int64_t i = threadIdx.x; i < words; i += blockDim.x)
+            {
+                uint4 v = make_uint4(0, 0, 0, 0);
+                if (lean)
+                {
+                    const int64_t f0 = head + i * 16;
+                    uint32_t wv[4] = {0, 0, 0, 0};
+                    if (pass == 0)
+                    {
+                        int plane = int(f0 / hw), px = int(f0 - int64_t(plane) * hw);
+                        int t = plane / C, c = plane - t * C;
+#pragma unroll
+                        for (int j = 0; j < 16; ++j)
+                        {
+                            const uint32_t k = code[px];
+                            wv[j >> 2] |= ((int(k & 0xFFFF) == c && int(k >> 16) <= t) ? 1u : 0u) << (8 * (j & 3));
+                            if (++px == hw)
+                            {
+                                px = 0;
+                                if (++c == C) c = 0, ++t;
+                            }
+                        }
+                    }
+                    else
+                    {
+#pragma unroll 4
+                        for (int j = 0; j < 16; ++j) wv[j >> 2] |= spike(f0 + j) << (8 * (j & 3));
+                    }
+                    v = make_uint4(wv[0], wv[1], wv[2], wv[3]);
+                }
+                d4[i] = v;
+            }
+        }
+        __syncthreads();
+    }
+}
+
 inline size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 
 // Schedule overrides of the tensor-core kernels (0 = automatic), set by an
@@ -1342,10 +2119,10 @@ struct Plan
 
 // single_tile: all output channels in one CTA (required by the fused epilogue).
 Plan make_plan(int64_t n, int64_t cin, int64_t h, int64_t w, int64_t cout, int64_t kh, int64_t kw, int precision,
-               bool single_tile, int64_t t_fused = 0, bool times = false)
+               bool single_tile, int64_t t_fused = 0, bool times = false, int nsplit = 0)
 {
     Plan pl{};
-    pl.nsplit = precision == SPK_CONV_BF16X3 ? 3 : 2;
+    pl.nsplit = nsplit > 0 ? nsplit : (precision == SPK_CONV_BF16X3 ? 3 : 2);
     const int64_t npad = ceil_div(cout, 16) * 16;
     const int64_t cap = single_tile ? npad : (pl.nsplit == 3 ? 128 : 256);
     pl.n_tiles = int(ceil_div(npad, cap));
@@ -1689,10 +2466,16 @@ void launch(const TcParams &P, const Plan &pl, cudaStream_t s)
 
 struct FusedLayout
 {
-    Plan pl;
+    Plan pl, pl4;  // dense fused kernel; search kernels (kSearchTerms terms)
     int tp_log2, pp;
     int64_t npix, oh, ow;
-    size_t rec_off, min_off, max_off, total;
+    size_t rec_off, min_off, max_off;
+    // search path (search_ok): fixed-split weights, channel bounds + launch
+    // info, counters, per-pixel state, two bisection lists, the list of
+    // winners to re-read at T - 1, two lists of rows to recompute
+    bool search_ok;
+    size_t w4_off, echan_off, cnt_off, state_off, la_off, lb_off, fin_off, fa_off, fb_off;
+    size_t total;
 };
 
 FusedLayout fused_layout(int64_t b, int64_t t, int64_t cin, int64_t h, int64_t w, int64_t cout, int64_t kh, int64_t kw,
@@ -1714,6 +2497,22 @@ FusedLayout fused_layout(int64_t b, int64_t t, int64_t cin, int64_t h, int64_t w
     off += align256(size_t(b) * 4);
     L.max_off = off;
     off += align256(size_t(b) * 4);
+    L.pl4 = make_plan(b * t, cin, h, w, cout, kh, kw, precision, true, t, false, kSearchTerms);
+    L.search_ok = nnets == 1 && t <= 127 && L.pl4.n_tiles == 1 && L.pl4.nsplit * L.pl4.n_tile <= 512 &&
+                  L.pl4.stages >= 2 && L.pl4.smem <= 227 * 1024 && L.pl4.kblocks <= kMaxKBlocks;
+    if (L.search_ok)
+    {
+        const size_t np = size_t(L.npix);
+        L.w4_off = off, off += align256(L.pl4.wimg_bytes);
+        L.echan_off = off, off += align256(size_t(L.pl4.n_tile) * 4 + 8);
+        L.cnt_off = off, off += 256;
+        L.state_off = off, off += align256(np * 16);
+        L.la_off = off, off += align256(np * 8);
+        L.lb_off = off, off += align256(np * 8);
+        L.fin_off = off, off += align256(np * 8);
+        L.fa_off = off, off += align256(np * 16);
+        L.fb_off = off, off += align256(np * 16);
+    }
     L.total = off;
     return L;
 }
@@ -1767,6 +2566,18 @@ unsigned long long spk_recheck_count(int reset)
     return v;
 }
 
+unsigned long long spk_recompute_count(int reset)
+{
+    unsigned long long v = 0;
+    if (cudaMemcpyFromSymbol(&v, spk::g_recomputes, sizeof(v)) != cudaSuccess) return ~0ull;
+    if (reset)
+    {
+        unsigned long long z = 0;
+        if (cudaMemcpyToSymbol(spk::g_recomputes, &z, sizeof(z)) != cudaSuccess) return ~0ull;
+    }
+    return v;
+}
+
 int spk_device_status(int reset)
 {
     int v = 0;
@@ -1806,6 +2617,84 @@ struct Nets
     const int32_t *sample_net = nullptr;
     const float *threshold = nullptr;
 };
+
+// Launch sequence of the search path (see search_epilogue): the fixed-grid
+// split, round 0, ceil(log2 T) bisection rounds, the winners' values at
+// T - 1 (with WTA), each round followed by the exact recompute of the rows
+// it left open, then the spike writer.  The lists' lengths stay on the
+// device (each launch reads them).  Off the search path (device flags) every
+// one of these kernels leaves at once, except the writer, which zero-fills
+// the spikes for the dense kernel.
+void search_layer(const TcParams &P0, const FusedLayout &L, const float *kernel, int64_t count, int64_t pool_ky,
+                  int64_t pool_kx, int64_t poh, int64_t pow_, uint8_t *spikes, uint8_t *pooled, uint8_t *base,
+                  cudaStream_t s)
+{
+    const int64_t b = L.npix / (L.oh * L.ow);
+    TcParams P = P0;
+    const Plan &pl = L.pl4;
+    P.wimg = base + L.w4_off;
+    P.nsplit = pl.nsplit, P.n_tile = pl.n_tile, P.n_tiles = 1, P.kblocks = pl.kblocks;
+    P.tmem_cols = pl.tmem_cols, P.stages = pl.stages, P.nacc = pl.nacc;
+    float *echan = reinterpret_cast<float *>(base + L.echan_off);
+    unsigned *sinfo = reinterpret_cast<unsigned *>(echan + pl.n_tile);
+    int *cnt = reinterpret_cast<int *>(base + L.cnt_off);
+    P.echan = echan, P.sinfo = sinfo;
+    P.state = reinterpret_cast<int4 *>(base + L.state_off);
+    int2 *la = reinterpret_cast<int2 *>(base + L.la_off), *lb = reinterpret_cast<int2 *>(base + L.lb_off);
+    int4 *fa = reinterpret_cast<int4 *>(base + L.fa_off), *fb = reinterpret_cast<int4 *>(base + L.fb_off);
+    P.final_list = reinterpret_cast<int2 *>(base + L.fin_off);
+    P.final_count = cnt + 16;
+    P.wta = count > 0 ? 1 : 0;
+    const int taps = P.kh * P.kw;
+    P.kreal = P.nhwc ? taps * P.cpad : taps * P.cin;
+    P.tiles = ceil_div(L.npix, BM);
+    SPK_CUDA(cudaMemsetAsync(cnt, 0, 256, s));
+    SPK_CUDA(cudaMemsetAsync(sinfo, 0, 8, s));
+    fixed_split_kernel<kSearchTerms><<<unsigned(pl.n_tile), 256, 0, s>>>(
+        kernel, reinterpret_cast<uint4 *>(base + L.w4_off), P.cout, P.cin, taps, P.nhwc, P.cpad, pl.kblocks,
+        pl.n_tile, echan, sinfo, P.negw);
+    SPK_LAUNCHED();
+    if (count > 0)
+    {
+        search_init_kernel<<<grid_for(b, 256), 256, 0, s>>>(P.mins, P.maxs, b, P.negw, P.flag);
+        SPK_LAUNCHED();
+    }
+    const int cp = P.nhwc ? P.cpad : P.cin;
+    const unsigned fix_grid = unsigned(sm_count() * 4);
+    int nsr = 0;
+    while ((1 << nsr) < P.T) ++nsr;
+    const int rounds = 1 + nsr + (count > 0 ? 1 : 0);
+    for (int r = 0; r < rounds; ++r)
+    {
+        const bool final = count > 0 && r == rounds - 1;
+        P.round = r == 0 ? 0 : (final ? 2 : 1);
+        P.list_in = final ? P.final_list : (r & 1 ? la : lb);
+        P.count_in = final ? P.final_count : cnt + r;
+        P.list_out = r & 1 ? lb : la;
+        P.count_out = cnt + r + 1;
+        P.fix_list = r & 1 ? fb : fa;
+        P.fix_count = cnt + 17 + r;
+        launch<kSearch>(P, pl, s);
+        search_fix_kernel<<<fix_grid, 128, 0, s>>>(P, kernel, cp);
+        SPK_LAUNCHED();
+    }
+    const int ohw = int(L.oh * L.ow);
+    uint32_t *gcodes = nullptr;
+    size_t wsm = size_t(ohw) * 4;
+    if (ohw > 16384)
+    {
+        // the bisection state is no longer needed: its words hold the codes
+        gcodes = reinterpret_cast<uint32_t *>(P.state);
+        wsm = 0;
+        search_codes_kernel<<<grid_for(L.npix, 256), 256, 0, s>>>(P.records, gcodes, L.npix, P.T, P.negw, P.flag);
+        SPK_LAUNCHED();
+    }
+    SPK_CUDA(cudaFuncSetAttribute(search_write_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(wsm)));
+    search_write_kernel<<<unsigned(std::min<int64_t>(b, int64_t(sm_count()) * 16)), 256, wsm, s>>>(
+        P.records, gcodes, P.negw, P.flag, spikes, pool_ky > 0 ? pooled : nullptr, b, P.T, P.cout, ohw,
+        int(L.ow), int(pool_ky), int(pool_kx), int(poh), int(pow_));
+    SPK_LAUNCHED();
+}
 
 void fused_layer(const void *in, spk_dtype itype, const float *kernel, int64_t b, int64_t t, int64_t cin, int64_t h,
                  int64_t w, int64_t cout, int64_t kh, int64_t kw, int64_t sy, int64_t sx, const int64_t *pad4,
@@ -1863,18 +2752,38 @@ void fused_layer(const void *in, spk_dtype itype, const float *kernel, int64_t b
         SPK_REQUIRE(L.oh >= pool_ky && L.ow >= pool_kx, "the pooling window is larger than the output");
         P.pooled = pooled, P.pky = int(pool_ky), P.pkx = int(pool_kx), P.poh = int(poh), P.pow_ = int(pow_);
     }
-    if (count > 0)
+    // The search path (lean layers, kSearch): chosen here by the thresholds
+    // and by the fit of the layer; the kernels themselves check the weights'
+    // signs and the input's form and leave the work to the dense kernel
+    // otherwise.
+    const float fthr = float(threshold), fthv = float(value), finh = float(inhibit_threshold);
+    const float ffire = float(fire_threshold), fwta = float(wta_threshold);
+    const bool search = L.search_ok && !nets.offsets && fthv <= finh && fthv <= ffire && fthv <= fwta &&
+                        finh <= fthr && ffire <= fthr && fwta <= fthr;
+    if (count > 0 || search)
     {
         P.records = reinterpret_cast<int4 *>(base + L.rec_off);
         P.mins = reinterpret_cast<unsigned *>(base + L.min_off);
         P.maxs = reinterpret_cast<unsigned *>(base + L.max_off);
-        SPK_CUDA(cudaMemsetAsync(P.mins, 0xFF, size_t(b) * 4, s));
-        SPK_CUDA(cudaMemsetAsync(P.maxs, 0x00, size_t(b) * 4, s));
     }
     P.M = L.npix * (int64_t(1) << L.tp_log2);
     P.tiles = ceil_div(L.npix, L.pp);
-    SPK_CUDA(cudaMemsetAsync(spikes, 0, size_t(b) * t * cout * L.oh * L.ow, s));
-    if (pool_ky > 0) SPK_CUDA(cudaMemsetAsync(pooled, 0, size_t(b) * t * cout * poh * pow_, s));
+    if (search)
+    {
+        search_layer(P, L, kernel, count, pool_ky, pool_kx, poh, pow_, spikes, pooled, base, s);
+        P.skip_when_lean = 1;
+        if (count == 0) P.records = nullptr;
+    }
+    else
+    {
+        if (count > 0)
+        {
+            SPK_CUDA(cudaMemsetAsync(P.mins, 0xFF, size_t(b) * 4, s));
+            SPK_CUDA(cudaMemsetAsync(P.maxs, 0x00, size_t(b) * 4, s));
+        }
+        SPK_CUDA(cudaMemsetAsync(spikes, 0, size_t(b) * t * cout * L.oh * L.ow, s));
+        if (pool_ky > 0) SPK_CUDA(cudaMemsetAsync(pooled, 0, size_t(b) * t * cout * poh * pow_, s));
+    }
     launch<kFused>(P, L.pl, s);
     if (count == 0) return;
     const int hw = int(L.oh * L.ow);

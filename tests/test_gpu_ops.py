@@ -504,12 +504,13 @@ def test_fused_layer_matches_ops(port, case, prec):
     conv.kernel.copy_(cuda(rng.uniform(0.3, 1.0, size=(cout, cin, k, k)).astype(np.float32)))
     conv.precision = prec
     spikes, wins = spyker.conv_fire_wta(x, conv, theta, radius, count)
-    out = spyker.inhibit(spyker.threshold(conv(x), theta))
-    ref_spikes, ref_wins = spyker.fire(out), spyker.convwta(out, radius, count)
     assert spyker._lib.lib.spk_device_status(1) == 0
-    assert np.array_equal(host(spikes), host(ref_spikes))
-    got, want = winners_np(wins), winners_np(ref_wins)
-    assert np.array_equal(got[1], want[1]) and np.array_equal(got[0], want[0])
+    # against the oracle's FP64 pipeline (the layer's decisions are exact)
+    inh = port.inhibit(port.threshold(port.conv(host(x), host(conv.kernel), (1, 1), (pad,) * 4), theta))
+    assert np.array_equal(host(spikes), port.fire(inh))
+    got = winners_np(wins)
+    win, cnt = oracle_winners(*port.convwta(inh, (radius, radius), count))
+    assert np.array_equal(got[1], cnt) and np.array_equal(got[0], win)
     assert int(got[1].sum()) > 0
 
 
