@@ -217,14 +217,18 @@ def gpu_arm(args, rank, world):
     for k in range(args.trajectory):
         rec = []
         net.conv_events.clear()
-        net.probe = lambda: (torch.cuda.synchronize(), rec.append(spyker._lib.lib.spk_recheck_count(1)))
+        net.probe = lambda: (torch.cuda.synchronize(), rec.append((spyker._lib.lib.spk_recheck_count(1),
+                                                                  spyker._lib.lib.spk_recompute_count(1))))
         spyker._lib.lib.spk_recheck_count(1)
+        spyker._lib.lib.spk_recompute_count(1)
         net.step(dev_imgs)
         net.finish()
         torch.cuda.synchronize()
         net.probe = None
         c1, c2 = (a.elapsed_time(b) for a, b, _ in net.conv_events[:2])
-        trajectory.append({"step": args.warmup + k, "rechecks": rec, "conv_ms": [c1, c2]})
+        # per layer: rows re-decided from exact term sums, rows recomputed from the weights
+        trajectory.append({"step": args.warmup + k, "rechecks": [rec[1][0], rec[3][0]],
+                           "recomputes": [rec[1][1], rec[3][1]], "conv_ms": [c1, c2]})
     barrier()
     net.conv_events.clear()
     l0 = spyker._lib.lib.spk_launch_count()

@@ -100,6 +100,8 @@ struct TcParams
     int *count_out, *final_count;
     int4 *fix_list;  // rows left for the exact recompute: (pixel, step, round, winner)
     int *fix_count;
+    int4 *val_list;  // rows whose winner is decided but not its value: (pixel, step, round, winner)
+    int *val_count;
     int4 *state;     // per pixel: (lo | hi << 8 | winner << 16, value, winner at T-1, value at T-1)
     const float *echan;     // per channel bound of |oracle potential - exact term sum|
     const unsigned *sinfo;  // [0] largest echan (bits), [1] largest channel exponent + 128
@@ -112,8 +114,10 @@ struct TcParams
 // kTimes: the fused (pixel, time) rows with an epilogue that writes each
 // neuron's first step above threshold (F32 time, T = never).
 constexpr int kPotentials = 0, kFused = 1, kTimes = 2, kSearch = 3;
-// Terms of the fixed-grid weight split of the search kernels.
-constexpr int kSearchTerms = 3;
+// Terms of the fixed-grid weight split of the search kernels: four where
+// their accumulators fit the tensor memory (weights down to 2^-9 of their
+// channel's largest exact), else three.
+constexpr int kSearchTermsMax = 4, kSearchTermsMin = 3;
 
 __device__ __forceinline__ unsigned order_enc(float f)
 {
@@ -1017,6 +1021,12 @@ __device__ __forceinline__ double s_exact(const uint32_t (&q)[NS][kEpiChunk], in
 __device__ __forceinline__ void s_round(double S, float E, float &P, float &lo, float &hi)
 {
     P = float(S);
+    if (E == 0.f)
+    {
+        // the term total is the oracle's FP64 sum itself
+        lo = hi = P;
+        return;
+    }
     const double rho = S - double(P);
     const double up = (double(nextafterf(P, INFINITY)) - double(P)) * 0.5;
     const double dn = (double(P) - double(nextafterf(P, -INFINITY))) * 0.5;
@@ -1109,7 +1119,7 @@ __device__ __forceinline__ int4 s_pack(int lo, int hi, int w, float v, int at, f
 }
 
 __device__ __forceinline__ SearchAct search_act(const TcParams &P, int round, int pix, int t, int dec, int a,
-                                                float v)
+                                                float v, int4 s)
 {
     SearchAct r;
     const int T = P.T;
@@ -1132,7 +1142,6 @@ __device__ __forceinline__ SearchAct search_act(const TcParams &P, int round, in
     }
     else
     {
-        const int4 s = P.state[pix];
         lo = int(int8_t(s.x & 0xFF)), hi = int(int8_t((s.x >> 8) & 0xFF)), w = s.x >> 16;
         vh = __int_as_float(s.y), at = s.z, vt = __int_as_float(s.w);
         if (dec == 2)
@@ -1159,19 +1168,6 @@ __device__ __forceinline__ SearchAct search_act(const TcParams &P, int round, in
     return r;
 }
 
-// Warp-aggregated append of this lane's entry (if any) to a list.
-template <typename E>
-__device__ __forceinline__ void s_append(bool want, const E &e, E *list, int *count)
-{
-    const unsigned m = __ballot_sync(0xffffffffu, want);
-    if (!m) return;
-    const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
-    int base = 0;
-    if (lane == leader) base = atomicAdd(count, __popc(m));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    if (want) list[base + __popc(m & ((1u << lane) - 1u))] = e;
-}
-
 __device__ __forceinline__ void s_extremes(const TcParams &P, int pix, const SearchAct &r)
 {
     const int smp = pix / int(P.ohw);
@@ -1186,8 +1182,8 @@ __device__ __forceinline__ void s_extremes(const TcParams &P, int pix, const Sea
 // Search epilogue of one row per thread (warps 0-3).  `c0` is the per-launch
 // part of the tier-1 bound.
 template <int NS>
-__device__ void search_epilogue(const TcParams &P, uint32_t acc, bool ok, int pix, int t, int aux, uint64_t *release,
-                                float c0)
+__device__ void search_epilogue(const TcParams &P, uint32_t acc, bool ok, int pix, int t, int aux, int4 pstate,
+                                uint64_t *release, float c0)
 {
     const int warp = threadIdx.x >> 5;
     const uint32_t lane_base = acc + (uint32_t((warp & 3) * 32) << 16);
@@ -1203,7 +1199,7 @@ __device__ void search_epilogue(const TcParams &P, uint32_t acc, bool ok, int pi
         {
             float lo, hi;
             s_round(S, __ldg(P.echan + aux), v, lo, hi);
-            dec = lo == hi ? 2 : 0;
+            dec = lo == hi ? 2 : 3;
             a = aux;
         }
     }
@@ -1275,17 +1271,37 @@ __device__ void search_epilogue(const TcParams &P, uint32_t acc, bool ok, int pi
                 float lo, hi;
                 s_round(S, __ldg(P.echan + st.a1), v, lo, hi);
                 a = st.a1;
-                dec = lo == hi ? 2 : 0;
+                dec = lo == hi ? 2 : 3;
             }
             else
                 dec = d2, a = a2, v = v2;
         }
     }
+    // dec 3: the winner a is decided, its value is left to the exact sum
     SearchAct r;
-    if (ok && dec != 0) r = search_act(P, P.round, pix, t, dec, a, v);
-    s_append(ok && dec == 0, make_int4(pix, t, P.round, aux), P.fix_list, P.fix_count);
-    s_append(r.next, r.next_e, P.list_out, P.count_out);
-    s_append(r.fin, r.fin_e, P.final_list, P.final_count);
+    if (ok && (dec == 1 || dec == 2)) r = search_act(P, P.round, pix, t, dec, a, v, pstate);
+    // the four lists' slots: one atomic per list and warp, all in flight at once
+    const int lane = threadIdx.x & 31;
+    const bool wf = ok && dec == 0, wv = ok && dec == 3;
+    const unsigned mf = __ballot_sync(0xffffffffu, wf), mv = __ballot_sync(0xffffffffu, wv);
+    const unsigned mn = __ballot_sync(0xffffffffu, r.next), mi = __ballot_sync(0xffffffffu, r.fin);
+    int bf = 0, bv = 0, bn = 0, bi = 0;
+    if (lane == 0)
+    {
+        if (mf) bf = atomicAdd(P.fix_count, __popc(mf));
+        if (mv) bv = atomicAdd(P.val_count, __popc(mv));
+        if (mn) bn = atomicAdd(P.count_out, __popc(mn));
+        if (mi) bi = atomicAdd(P.final_count, __popc(mi));
+    }
+    const unsigned below = (1u << lane) - 1u;
+    bf = __shfl_sync(0xffffffffu, bf, 0) + __popc(mf & below);
+    bv = __shfl_sync(0xffffffffu, bv, 0) + __popc(mv & below);
+    bn = __shfl_sync(0xffffffffu, bn, 0) + __popc(mn & below);
+    bi = __shfl_sync(0xffffffffu, bi, 0) + __popc(mi & below);
+    if (wf) P.fix_list[bf] = make_int4(pix, t, P.round, aux);
+    if (wv) P.val_list[bv] = make_int4(pix, t, P.round, a);
+    if (r.next) P.list_out[bn] = r.next_e;
+    if (r.fin) P.final_list[bi] = r.fin_e;
     if (ok && P.wta) s_extremes(P, pix, r);
 }
 
@@ -1327,6 +1343,16 @@ __device__ __forceinline__ void search_producer(const TcParams &P, const int4 *t
         urow[i] = (q & 7) + 8 * (q >> 6), ukc[i] = (q >> 3) & 7;
     }
     uint32_t it = 0;
+    // the next tile's list entries are loaded while this tile is built
+    int2 ent[4];
+    bool eok[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+    {
+        const int64_t idx = int64_t(blockIdx.x) * BM + urow[i];
+        eok[i] = blockIdx.x < ntiles && idx < nrows;
+        ent[i] = eok[i] ? search_entry(P, idx) : make_int2(0, 0);
+    }
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
     {
         FusedPixel fu[4];
@@ -1334,11 +1360,11 @@ __device__ __forceinline__ void search_producer(const TcParams &P, const int4 *t
 #pragma unroll
         for (int i = 0; i < 4; ++i)
         {
-            const int64_t idx = tile * BM + urow[i];
-            const bool ok = idx < nrows;
-            const int2 e = ok ? search_entry(P, idx) : make_int2(0, 0);
-            fu[i] = pixel_of(P, ok, e.x);
-            ut[i] = e.y;
+            fu[i] = pixel_of(P, eok[i], ent[i].x);
+            ut[i] = ent[i].y;
+            const int64_t idx = (tile + gridDim.x) * BM + urow[i];
+            eok[i] = tile + gridDim.x < ntiles && idx < nrows;
+            ent[i] = eok[i] ? search_entry(P, idx) : make_int2(0, 0);
         }
         for (int kb = 0; kb < P.kblocks; ++kb, ++it)
         {
@@ -1592,6 +1618,29 @@ __global__ void __launch_bounds__(kWsThreads, 1) conv_ws_kernel(TcParams P)
         {
             const int a = int(j % uint32_t(nacc));
             const uint32_t ua = j / uint32_t(nacc);
+            // search rows: the row's list entry and pixel state are loaded
+            // before the wait, so their latency hides behind it
+            bool s_ok = false;
+            int2 s_e = make_int2(0, 0);
+            int s_aux = 0;
+            int4 s_st = make_int4(0, 0, 0, 0);
+            if constexpr (MODE == kSearch)
+            {
+                const int64_t idx = tile * BM + row;
+                s_ok = idx < nrows;
+                if (s_ok)
+                {
+                    if (P.round == 0)
+                        s_e = make_int2(int(idx), P.T - 1);
+                    else
+                    {
+                        const int2 le = P.list_in[idx];
+                        s_e = P.round == 1 ? le : make_int2(le.x, P.T - 1);
+                        s_aux = le.y;
+                        if (P.round == 1) s_st = P.state[le.x];
+                    }
+                }
+            }
             if (!wait_bounded(&accf_bar[a], ua & 1)) break;
             tc_fence_after();
             const int64_t mt = tile / P.n_tiles;
@@ -1627,16 +1676,10 @@ __global__ void __launch_bounds__(kWsThreads, 1) conv_ws_kernel(TcParams P)
             }
             else if constexpr (MODE == kSearch)
             {
-                const int64_t idx = mt * BM + row;
-                const bool ok = idx < nrows;
-                int2 e = make_int2(0, 0);
-                int aux = 0;
-                if (ok)
-                {
-                    e = search_entry(P, idx);
-                    if (P.round == 2) aux = P.list_in[idx].y;
-                }
-                search_epilogue<kSearchTerms>(P, acc, ok, e.x, e.y, aux, &acce_bar[a], c0);
+                if (P.nsplit == 4)
+                    search_epilogue<4>(P, acc, s_ok, s_e.x, s_e.y, P.round == 2 ? s_aux : 0, s_st, &acce_bar[a], c0);
+                else
+                    search_epilogue<3>(P, acc, s_ok, s_e.x, s_e.y, P.round == 2 ? s_aux : 0, s_st, &acce_bar[a], c0);
             }
             else if constexpr (MODE == kFused)
             {
@@ -1821,6 +1864,7 @@ __global__ void __launch_bounds__(256) fixed_split_kernel(const float *__restric
 {
     __shared__ float s_mx[8];
     __shared__ double s_err[8];
+    __shared__ int s_lsb[8];
     const int n = blockIdx.x, tid = threadIdx.x;
     const int kreal = nhwc ? taps * cpad : taps * cin;
     const int K = kblocks * BK;
@@ -1835,17 +1879,29 @@ __global__ void __launch_bounds__(256) fixed_split_kernel(const float *__restric
     };
     float mx = 0.f;
     bool neg = false;
+    int lsb = INT_MAX;  // exponent of the lowest set bit of any weight
     for (int k = tid; k < K; k += blockDim.x)
     {
         const float w = weight(k);
         mx = fmaxf(mx, fabsf(w));
         neg |= !(w >= 0.f);
+        const uint32_t bits = __float_as_uint(w) & 0x7FFFFFFFu;
+        if (bits != 0u && bits < 0x7F800000u)
+        {
+            const int ex = int(bits >> 23);
+            const uint32_t sig = ex ? ((bits & 0x7FFFFFu) | 0x800000u) : bits;
+            lsb = min(lsb, __ffs(int(sig)) - 1 + (ex ? ex : 1) - 150);
+        }
     }
-    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    if ((tid & 31) == 0) s_mx[tid >> 5] = mx;
+    for (int o = 16; o > 0; o >>= 1)
+    {
+        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        lsb = min(lsb, __shfl_xor_sync(0xffffffffu, lsb, o));
+    }
+    if ((tid & 31) == 0) s_mx[tid >> 5] = mx, s_lsb[tid >> 5] = lsb;
     __syncthreads();
-    mx = s_mx[0];
-    for (int i = 1; i < int(blockDim.x >> 5); ++i) mx = fmaxf(mx, s_mx[i]);
+    mx = s_mx[0], lsb = s_lsb[0];
+    for (int i = 1; i < int(blockDim.x >> 5); ++i) mx = fmaxf(mx, s_mx[i]), lsb = min(lsb, s_lsb[i]);
     int e = 0;
     if (mx > 0.f)
     {
@@ -1895,7 +1951,12 @@ __global__ void __launch_bounds__(256) fixed_split_kernel(const float *__restric
     {
         err = s_err[0];
         for (int i = 1; i < int(blockDim.x >> 5); ++i) err += s_err[i];
-        const double bound = err + double(kreal) * double(kreal) * ldexp(1.0, e - 52);
+        // the oracle's ordered FP64 sum is exact when every partial sum
+        // (a multiple of 2^lsb, at most kreal 2^e) fits in 53 bits
+        int lk = 0;
+        while ((1 << lk) < kreal) ++lk;
+        const bool exact64 = lsb == INT_MAX || e + lk - lsb <= 53;
+        const double bound = err + (exact64 ? 0.0 : double(kreal) * double(kreal) * ldexp(1.0, e - 52));
         const float eb = __double2float_ru(bound);
         echan[n] = eb;
         if (n < cout)
@@ -1924,13 +1985,57 @@ __global__ void search_init_kernel(unsigned *mins, unsigned *maxs, int64_t b, co
 // per channel the FP64 sum of the F32 weights of the active inputs in
 // (channel, ky, kx) order (the oracle's convolution loop), rounded once to
 // F32.  One warp per row; its lanes take the output channels.
+// The oracle's potential of one channel (weights wk [Cin, KH, KW]) at step t
+// for the pixel whose receptive field starts at (iy0, ix0): the FP64 sum of
+// the weights of the inputs that fired by t, in (channel, ky, kx) order,
+// positions outside the input skipped.
+__device__ __forceinline__ double oracle_sum(const TcParams &P, const uint8_t *fm, const float *wk, int iy0, int ix0,
+                                             int cp, int t)
+{
+    const int ky0 = max(0, -iy0), ky1 = min(P.kh, P.h - iy0);
+    const int kx0 = max(0, -ix0), kx1 = min(P.kw, P.w - ix0);
+    double acc = 0.0;
+    for (int c = 0; c < P.cin; ++c)
+        for (int ky = ky0; ky < ky1; ++ky)
+        {
+            const int64_t fr = (int64_t(iy0 + ky) * P.w + ix0) * cp + c;  // index of kx = 0 (may lie outside)
+            const float *wr = wk + (c * P.kh + ky) * P.kw;
+#pragma unroll 4
+            for (int kx = kx0; kx < kx1; ++kx)
+            {
+                const float wv = __ldg(wr + kx);
+                if (int(__ldg(fm + fr + int64_t(kx) * cp)) <= t) acc += double(wv);
+            }
+        }
+    return acc;
+}
+
 __global__ void __launch_bounds__(128) search_fix_kernel(TcParams P, const float *__restrict__ kernel, int cp)
 {
     if (*P.negw || *P.flag) return;
     const int lane = threadIdx.x & 31;
     const int64_t nw = int64_t(gridDim.x) * (blockDim.x >> 5);
-    const int n = *P.fix_count;
     const int taps = P.kh * P.kw;
+    // rows whose winner is decided: one lane per row sums the winner's
+    // products in the oracle's order
+    const int nv = *P.val_count;
+    for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < nv; q += int64_t(gridDim.x) * blockDim.x)
+    {
+        const int4 e = P.val_list[q];
+        const int pix = e.x, t = e.y, round = e.z, o = e.w;
+        const int smp = pix / int(P.ohw), pp = pix - smp * int(P.ohw);
+        const int oy = pp / P.ow, ox = pp - oy * P.ow;
+        const int iy0 = oy * P.sy - P.top, ix0 = ox * P.sx - P.left;
+        const uint8_t *fm = P.in + int64_t(smp) * P.img_stride;
+        const float *wk = kernel + int64_t(o) * P.cin * taps;
+        const double acc = oracle_sum(P, fm, wk, iy0, ix0, cp, t);
+        atomicAdd(&g_recomputes, 1ull);
+        const SearchAct r = search_act(P, round, pix, t, 2, o, float(acc), round == 1 ? P.state[pix] : int4{});
+        if (r.next) P.list_out[atomicAdd(P.count_out, 1)] = r.next_e;
+        if (r.fin) P.final_list[atomicAdd(P.final_count, 1)] = r.fin_e;
+        if (P.wta) s_extremes(P, pix, r);
+    }
+    const int n = *P.fix_count;
     for (int64_t q = int64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); q < n; q += nw)
     {
         const int4 e = P.fix_list[q];
@@ -1944,22 +2049,7 @@ __global__ void __launch_bounds__(128) search_fix_kernel(TcParams P, const float
         for (int o = lane; o < P.cout; o += 32)
         {
             if (round == 2 && o != aux) continue;
-            double acc = 0.0;
-            const float *wk = kernel + int64_t(o) * P.cin * taps;
-            for (int c = 0; c < P.cin; ++c)
-                for (int ky = 0; ky < P.kh; ++ky)
-                {
-                    const int iy = iy0 + ky;
-                    if (iy < 0 || iy >= P.h) continue;
-                    for (int kx = 0; kx < P.kw; ++kx)
-                    {
-                        const int ix = ix0 + kx;
-                        if (ix < 0 || ix >= P.w) continue;
-                        if (int(fm[(int64_t(iy) * P.w + ix) * cp + c]) <= t)
-                            acc += double(wk[(c * P.kh + ky) * P.kw + kx]);
-                    }
-                }
-            const float pv = float(acc);
+            const float pv = float(oracle_sum(P, fm, kernel + int64_t(o) * P.cin * taps, iy0, ix0, cp, t));
             if (pv > best) best = pv, besti = o;
             if (o == aux) mine = pv;
         }
@@ -1982,7 +2072,7 @@ __global__ void __launch_bounds__(128) search_fix_kernel(TcParams P, const float
                 dec = 2, a = besti, v = best;
             else
                 dec = 1, a = -1, v = 0.f;
-            const SearchAct r = search_act(P, round, pix, t, dec, a, v);
+            const SearchAct r = search_act(P, round, pix, t, dec, a, v, round == 1 ? P.state[pix] : int4{});
             if (r.next) P.list_out[atomicAdd(P.count_out, 1)] = r.next_e;
             if (r.fin) P.final_list[atomicAdd(P.final_count, 1)] = r.fin_e;
             if (P.wta) s_extremes(P, pix, r);
@@ -2005,37 +2095,54 @@ __global__ void search_codes_kernel(const int4 *__restrict__ records, uint32_t *
 
 // Spikes (and pooled spikes) of the search path from the per-pixel records:
 // channel w fires from step t0 on.  A CTA per sample writes its
-// [T, C, OH, OW] block as 16-byte words (and [T, C, POH, POW] when pooling:
-// a cell fires where any pixel of its window does), with the sample's codes
-// staged in shared memory (or read from `gcodes` for maps above 16384
-// pixels).  Off the search path (negative weights or other input) it writes
-// zeros, which the dense kernel then fills.
+// [T, C, OH, OW] block as 4-byte words, one output word per thread and
+// pass, with the sample's codes w | t0 << 16 in shared memory (or read from
+// `gcodes` for maps above 16384 pixels); consecutive threads read
+// consecutive 16-byte code groups, so the reads are free of bank conflicts.
+// Pooled spikes [T, C, POH, POW] come from a table of the first firing step
+// per (channel, cell): a cell fires from the earliest t0 of its window's
+// pixels won by that channel.  Off the search path (negative weights or
+// other input) it writes zeros, which the dense kernel then fills.
 __global__ void __launch_bounds__(256) search_write_kernel(const int4 *__restrict__ records,
                                                            const uint32_t *__restrict__ gcodes, const int *negw,
                                                            const int *flag, uint8_t *__restrict__ spikes,
                                                            uint8_t *__restrict__ pooled, int64_t b, int T, int C,
-                                                           int ohw, int ow, int pky, int pkx, int poh, int pow_)
+                                                           int ohw, int ow, int pky, int pkx, int poh, int pow_,
+                                                           int ptab)
 {
-    extern __shared__ uint32_t scode[];  // per pixel: w | t0 << 16 (t0 = T: never)
+    extern __shared__ uint32_t scode[];  // [ohw rounded to 4] codes, then [C][phw] first steps when ptab
     const bool lean = !*negw && !*flag;
+    const int ohw4 = (ohw + 3) & ~3, phw = poh * pow_;
+    uint32_t *first = scode + ohw4;
     for (int64_t smp = blockIdx.x; smp < b; smp += gridDim.x)
     {
         const uint32_t *code = gcodes ? gcodes + smp * ohw : scode;
         if (lean && !gcodes)
-        {
             for (int p = threadIdx.x; p < ohw; p += blockDim.x)
             {
                 const int4 r = records[smp * ohw + p];
                 scode[p] = uint32_t(r.x & 0xFFFF) | (uint32_t(min(r.y, T)) << 16);
             }
-        }
+        if (lean && ptab)
+            for (int i = threadIdx.x; i < C * phw; i += blockDim.x) first[i] = uint32_t(T);
         __syncthreads();
+        if (lean && ptab)
+        {
+            for (int p = threadIdx.x; p < ohw; p += blockDim.x)
+            {
+                const int y = p / ow, x = p - y * ow, py = y / pky, px = x / pkx;
+                const uint32_t k = code[p];
+                if (py < poh && px < pow_ && int(k >> 16) < T)
+                    atomicMin(first + int(k & 0xFFFF) * phw + py * pow_ + px, k >> 16);
+            }
+            __syncthreads();
+        }
         for (int pass = 0; pass < (pooled ? 2 : 1); ++pass)
         {
-            const int hw = pass == 0 ? ohw : poh * pow_;
+            const int hw = pass == 0 ? ohw : phw;
             const int64_t n = int64_t(T) * C * hw;
             uint8_t *dst = (pass == 0 ? spikes : pooled) + smp * n;
-            // value of byte f of the block
+            // byte f of the block
             auto spike = [&](int64_t f) -> uint32_t {
                 if (!lean) return 0u;
                 const int plane = int(f / hw), px = int(f - int64_t(plane) * hw);
@@ -2045,6 +2152,7 @@ __global__ void __launch_bounds__(256) search_write_kernel(const int4 *__restric
                     const uint32_t k = code[px];
                     return (int(k & 0xFFFF) == c && int(k >> 16) <= t) ? 1u : 0u;
                 }
+                if (ptab) return int(first[c * hw + px]) <= t ? 1u : 0u;
                 const int py = px / pow_, pxx = px - py * pow_;
                 uint32_t any = 0;
                 for (int dy = 0; dy < pky; ++dy)
@@ -2055,43 +2163,40 @@ __global__ void __launch_bounds__(256) search_write_kernel(const int4 *__restric
                     }
                 return any;
             };
-            const uintptr_t a = reinterpret_cast<uintptr_t>(dst);
-            const int64_t head = std::min<int64_t>(n, int64_t((16 - (a & 15)) & 15));
-            const int64_t words = (n - head) / 16;
-            for (int64_t f = threadIdx.x; f < head; f += blockDim.x) dst[f] = uint8_t(spike(f));
-            for (int64_t f = head + words * 16 + threadIdx.x; f < n; f += blockDim.x) dst[f] = uint8_t(spike(f));
-            uint4 *d4 = reinterpret_cast<uint4 *>(dst + head);
-            for (int64_t i = threadIdx.x; i < words; i += blockDim.x)
+            const bool words = hw % 4 == 0 && (reinterpret_cast<uintptr_t>(dst) & 3) == 0 &&
+                               (pass == 1 ? (ptab || !lean) : true);
+            if (!words)
             {
-                uint4 v = make_uint4(0, 0, 0, 0);
+                for (int64_t f = threadIdx.x; f < n; f += blockDim.x) dst[f] = uint8_t(spike(f));
+                continue;
+            }
+            uint32_t *d4 = reinterpret_cast<uint32_t *>(dst);
+            const uint32_t *src = pass == 0 ? code : first;
+            for (int64_t i = threadIdx.x; i < n / 4; i += blockDim.x)
+            {
+                uint32_t wv = 0;
                 if (lean)
                 {
-                    const int64_t f0 = head + i * 16;
-                    uint32_t wv[4] = {0, 0, 0, 0};
+                    const int plane = int((4 * i) / hw), px = int(4 * i - int64_t(plane) * hw);
+                    const int t = plane / C, c = plane - t * C;
                     if (pass == 0)
                     {
-                        int plane = int(f0 / hw), px = int(f0 - int64_t(plane) * hw);
-                        int t = plane / C, c = plane - t * C;
-#pragma unroll
-                        for (int j = 0; j < 16; ++j)
-                        {
-                            const uint32_t k = code[px];
-                            wv[j >> 2] |= ((int(k & 0xFFFF) == c && int(k >> 16) <= t) ? 1u : 0u) << (8 * (j & 3));
-                            if (++px == hw)
-                            {
-                                px = 0;
-                                if (++c == C) c = 0, ++t;
-                            }
-                        }
+                        const uint4 k = *reinterpret_cast<const uint4 *>(src + px);
+                        const uint32_t cc = uint32_t(c), tt = uint32_t(t);
+                        wv = ((k.x & 0xFFFF) == cc && (k.x >> 16) <= tt ? 1u : 0u) |
+                             ((k.y & 0xFFFF) == cc && (k.y >> 16) <= tt ? 1u << 8 : 0u) |
+                             ((k.z & 0xFFFF) == cc && (k.z >> 16) <= tt ? 1u << 16 : 0u) |
+                             ((k.w & 0xFFFF) == cc && (k.w >> 16) <= tt ? 1u << 24 : 0u);
                     }
                     else
                     {
-#pragma unroll 4
-                        for (int j = 0; j < 16; ++j) wv[j >> 2] |= spike(f0 + j) << (8 * (j & 3));
+                        const uint4 k = *reinterpret_cast<const uint4 *>(src + c * hw + px);
+                        const uint32_t tt = uint32_t(t);
+                        wv = (k.x <= tt ? 1u : 0u) | (k.y <= tt ? 1u << 8 : 0u) | (k.z <= tt ? 1u << 16 : 0u) |
+                             (k.w <= tt ? 1u << 24 : 0u);
                     }
-                    v = make_uint4(wv[0], wv[1], wv[2], wv[3]);
                 }
-                d4[i] = v;
+                d4[i] = wv;
             }
         }
         __syncthreads();
@@ -2466,7 +2571,7 @@ void launch(const TcParams &P, const Plan &pl, cudaStream_t s)
 
 struct FusedLayout
 {
-    Plan pl, pl4;  // dense fused kernel; search kernels (kSearchTerms terms)
+    Plan pl, pl4;  // dense fused kernel; search kernels (3 or 4 split terms)
     int tp_log2, pp;
     int64_t npix, oh, ow;
     size_t rec_off, min_off, max_off;
@@ -2474,7 +2579,7 @@ struct FusedLayout
     // info, counters, per-pixel state, two bisection lists, the list of
     // winners to re-read at T - 1, two lists of rows to recompute
     bool search_ok;
-    size_t w4_off, echan_off, cnt_off, state_off, la_off, lb_off, fin_off, fa_off, fb_off;
+    size_t w4_off, echan_off, cnt_off, state_off, la_off, lb_off, fin_off, fa_off, fb_off, va_off, vb_off;
     size_t total;
 };
 
@@ -2497,7 +2602,9 @@ FusedLayout fused_layout(int64_t b, int64_t t, int64_t cin, int64_t h, int64_t w
     off += align256(size_t(b) * 4);
     L.max_off = off;
     off += align256(size_t(b) * 4);
-    L.pl4 = make_plan(b * t, cin, h, w, cout, kh, kw, precision, true, t, false, kSearchTerms);
+    L.pl4 = make_plan(b * t, cin, h, w, cout, kh, kw, precision, true, t, false, kSearchTermsMax);
+    if (L.pl4.nsplit * L.pl4.n_tile > 512 || L.pl4.stages < 2)
+        L.pl4 = make_plan(b * t, cin, h, w, cout, kh, kw, precision, true, t, false, kSearchTermsMin);
     L.search_ok = nnets == 1 && t <= 127 && L.pl4.n_tiles == 1 && L.pl4.nsplit * L.pl4.n_tile <= 512 &&
                   L.pl4.stages >= 2 && L.pl4.smem <= 227 * 1024 && L.pl4.kblocks <= kMaxKBlocks;
     if (L.search_ok)
@@ -2505,13 +2612,15 @@ FusedLayout fused_layout(int64_t b, int64_t t, int64_t cin, int64_t h, int64_t w
         const size_t np = size_t(L.npix);
         L.w4_off = off, off += align256(L.pl4.wimg_bytes);
         L.echan_off = off, off += align256(size_t(L.pl4.n_tile) * 4 + 8);
-        L.cnt_off = off, off += 256;
+        L.cnt_off = off, off += 256;  // 64 counters
         L.state_off = off, off += align256(np * 16);
         L.la_off = off, off += align256(np * 8);
         L.lb_off = off, off += align256(np * 8);
         L.fin_off = off, off += align256(np * 8);
         L.fa_off = off, off += align256(np * 16);
         L.fb_off = off, off += align256(np * 16);
+        L.va_off = off, off += align256(np * 16);
+        L.vb_off = off, off += align256(np * 16);
     }
     L.total = off;
     return L;
@@ -2642,6 +2751,7 @@ void search_layer(const TcParams &P0, const FusedLayout &L, const float *kernel,
     P.state = reinterpret_cast<int4 *>(base + L.state_off);
     int2 *la = reinterpret_cast<int2 *>(base + L.la_off), *lb = reinterpret_cast<int2 *>(base + L.lb_off);
     int4 *fa = reinterpret_cast<int4 *>(base + L.fa_off), *fb = reinterpret_cast<int4 *>(base + L.fb_off);
+    int4 *va = reinterpret_cast<int4 *>(base + L.va_off), *vb = reinterpret_cast<int4 *>(base + L.vb_off);
     P.final_list = reinterpret_cast<int2 *>(base + L.fin_off);
     P.final_count = cnt + 16;
     P.wta = count > 0 ? 1 : 0;
@@ -2650,9 +2760,9 @@ void search_layer(const TcParams &P0, const FusedLayout &L, const float *kernel,
     P.tiles = ceil_div(L.npix, BM);
     SPK_CUDA(cudaMemsetAsync(cnt, 0, 256, s));
     SPK_CUDA(cudaMemsetAsync(sinfo, 0, 8, s));
-    fixed_split_kernel<kSearchTerms><<<unsigned(pl.n_tile), 256, 0, s>>>(
-        kernel, reinterpret_cast<uint4 *>(base + L.w4_off), P.cout, P.cin, taps, P.nhwc, P.cpad, pl.kblocks,
-        pl.n_tile, echan, sinfo, P.negw);
+    auto split = pl.nsplit == 4 ? fixed_split_kernel<4> : fixed_split_kernel<3>;
+    split<<<unsigned(pl.n_tile), 256, 0, s>>>(kernel, reinterpret_cast<uint4 *>(base + L.w4_off), P.cout, P.cin,
+                                              taps, P.nhwc, P.cpad, pl.kblocks, pl.n_tile, echan, sinfo, P.negw);
     SPK_LAUNCHED();
     if (count > 0)
     {
@@ -2674,13 +2784,15 @@ void search_layer(const TcParams &P0, const FusedLayout &L, const float *kernel,
         P.count_out = cnt + r + 1;
         P.fix_list = r & 1 ? fb : fa;
         P.fix_count = cnt + 17 + r;
+        P.val_list = r & 1 ? vb : va;
+        P.val_count = cnt + 40 + r;
         launch<kSearch>(P, pl, s);
         search_fix_kernel<<<fix_grid, 128, 0, s>>>(P, kernel, cp);
         SPK_LAUNCHED();
     }
     const int ohw = int(L.oh * L.ow);
     uint32_t *gcodes = nullptr;
-    size_t wsm = size_t(ohw) * 4;
+    size_t wsm = size_t((ohw + 3) & ~3) * 4;
     if (ohw > 16384)
     {
         // the bisection state is no longer needed: its words hold the codes
@@ -2689,10 +2801,14 @@ void search_layer(const TcParams &P0, const FusedLayout &L, const float *kernel,
         search_codes_kernel<<<grid_for(L.npix, 256), 256, 0, s>>>(P.records, gcodes, L.npix, P.T, P.negw, P.flag);
         SPK_LAUNCHED();
     }
+    // table of first firing steps per (channel, pooled cell) when it fits
+    const size_t tab_bytes = size_t(P.cout) * size_t(poh * pow_) * 4;
+    const int ptab = pool_ky > 0 && wsm + tab_bytes <= 160 * 1024 ? 1 : 0;
+    if (ptab) wsm += tab_bytes;
     SPK_CUDA(cudaFuncSetAttribute(search_write_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(wsm)));
     search_write_kernel<<<unsigned(std::min<int64_t>(b, int64_t(sm_count()) * 16)), 256, wsm, s>>>(
         P.records, gcodes, P.negw, P.flag, spikes, pool_ky > 0 ? pooled : nullptr, b, P.T, P.cout, ohw,
-        int(L.ow), int(pool_ky), int(pool_kx), int(poh), int(pow_));
+        int(L.ow), int(pool_ky), int(pool_kx), int(poh), int(pow_), ptab);
     SPK_LAUNCHED();
 }
 
