@@ -2172,13 +2172,18 @@ __global__ void __launch_bounds__(256) search_write_kernel(const int4 *__restric
             }
             uint32_t *d4 = reinterpret_cast<uint32_t *>(dst);
             const uint32_t *src = pass == 0 ? code : first;
-            for (int64_t i = threadIdx.x; i < n / 4; i += blockDim.x)
+            // word i = (plane, px / 4), plane = t C + c, advanced by the block
+            // stride without divisions
+            const int wpp = hw / 4, nwords = int(n / 4);
+            const int dplane = int(blockDim.x) / wpp, dw = int(blockDim.x) - dplane * wpp;
+            int wq = int(threadIdx.x) % wpp, plane = int(threadIdx.x) / wpp;
+            int t = plane / C, c = plane - t * C;
+            for (int i = threadIdx.x; i < nwords; i += blockDim.x)
             {
                 uint32_t wv = 0;
+                const int px = 4 * wq;
                 if (lean)
                 {
-                    const int plane = int((4 * i) / hw), px = int(4 * i - int64_t(plane) * hw);
-                    const int t = plane / C, c = plane - t * C;
                     if (pass == 0)
                     {
                         const uint4 k = *reinterpret_cast<const uint4 *>(src + px);
@@ -2197,6 +2202,9 @@ __global__ void __launch_bounds__(256) search_write_kernel(const int4 *__restric
                     }
                 }
                 d4[i] = wv;
+                wq += dw, c += dplane;
+                if (wq >= wpp) wq -= wpp, ++c;
+                while (c >= C) c -= C, ++t;
             }
         }
         __syncthreads();
