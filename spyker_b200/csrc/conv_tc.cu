@@ -106,6 +106,7 @@ struct TcParams
     const float *echan;     // per channel bound of |oracle potential - exact term sum|
     const unsigned *sinfo;  // [0] largest echan (bits), [1] largest channel exponent + 128
     int kreal;              // real K (taps x input channels)
+    int r0_list;            // round 0 takes the (pixel, T - 1) entries of list_in (bound pre-filter ran)
     // kFused: leave at once when the search path ran (no negative weight and
     // cumulative 0/1 input; these are the words of negw and flag)
     int skip_when_lean;
@@ -1205,8 +1206,12 @@ __device__ void search_epilogue(const TcParams &P, uint32_t acc, bool ok, int pi
     }
     else
     {
-        // tier 1: the largest potential (first index), its runner-up
+        // tier 1: the largest potential (first index), its runner-up, and the
+        // term sums of the largest
         LeanMax st, st2;
+        uint32_t wb[NS], wb2[NS];
+#pragma unroll
+        for (int i = 0; i < NS; ++i) wb[i] = wb2[i] = 0u;
         {
             constexpr int W = kEpiChunk;
             uint32_t qa[NS][W], qb[NS][W];
@@ -1224,6 +1229,8 @@ __device__ void search_epilogue(const TcParams &P, uint32_t acc, bool ok, int pi
                     st.r2 = gt ? st.r1 : fmaxf(st.r2, f);
                     st.r1 = gt ? f : st.r1;
                     st.a1 = gt ? cb + j : st.a1;
+#pragma unroll
+                    for (int i = 0; i < NS; ++i) wb[i] = gt ? qa[i][j] : wb[i];
                 }
                 s_chunk_wait<NS>(qb);
                 if (cb + 2 * W < P.n_tile) s_chunk<NS>(lane_base, cb + 2 * W, P.n_tile, qa);
@@ -1236,8 +1243,13 @@ __device__ void search_epilogue(const TcParams &P, uint32_t acc, bool ok, int pi
                     st2.r2 = gt ? st2.r1 : fmaxf(st2.r2, f);
                     st2.r1 = gt ? f : st2.r1;
                     st2.a1 = gt ? cb + W + j : st2.a1;
+#pragma unroll
+                    for (int i = 0; i < NS; ++i) wb2[i] = gt ? qb[i][j] : wb2[i];
                 }
             }
+            const bool take = st2.r1 > st.r1 || (st2.r1 == st.r1 && st2.a1 >= 0 && (st.a1 < 0 || st2.a1 < st.a1));
+#pragma unroll
+            for (int i = 0; i < NS; ++i) wb[i] = take ? wb2[i] : wb[i];
             merge_lean(st, st2);
         }
         const float tol1 = __fmaf_ru(fabsf(st.r1), 0x1.9p-23f, c0);
@@ -1250,8 +1262,11 @@ __device__ void search_epilogue(const TcParams &P, uint32_t acc, bool ok, int pi
             const float gap = __fsub_rd(__fsub_rd(st.r1, tol1), __fadd_ru(st.r2, tol2));
             if (gap > __fmaf_ru(fabsf(st.r1), 0x1p-23f, 0x1p-126f)) d1 = 2;
         }
-        // the winner's exact value for tier-1 crossings; tier 2 for the rest
-        const double S = s_reload<NS>(lane_base, P.n_tile, (ok && d1 == 2) ? st.a1 : -1);
+        // the winner's exact value for tier-1 crossings (its terms were kept
+        // in the scan); tier 2 for the rest
+        double S = double(__uint_as_float(wb[0]));
+#pragma unroll
+        for (int i = 1; i < NS; ++i) S += double(__uint_as_float(wb[i]));
         int d2 = 0, a2 = -1;
         float v2 = 0.f;
         const unsigned open1 = __ballot_sync(0xffffffffu, ok && d1 == 0);
@@ -1311,7 +1326,7 @@ __device__ void search_epilogue(const TcParams &P, uint32_t acc, bool ok, int pi
 // bank groups).
 __device__ __forceinline__ int2 search_entry(const TcParams &P, int64_t idx)
 {
-    if (P.round == 0) return make_int2(int(idx), P.T - 1);
+    if (P.round == 0 && !P.r0_list) return make_int2(int(idx), P.T - 1);
     const int2 e = P.list_in[idx];
     return P.round == 1 ? e : make_int2(e.x, P.T - 1);
 }
@@ -1342,49 +1357,76 @@ __device__ __forceinline__ void search_producer(const TcParams &P, const int4 *t
         const int q = p + i * 256;
         urow[i] = (q & 7) + 8 * (q >> 6), ukc[i] = (q >> 3) & 7;
     }
-    uint32_t it = 0;
-    // the next tile's list entries are loaded while this tile is built
+    if (int64_t(blockIdx.x) >= ntiles) return;
+    // One step ahead over (tile, K block): the gathers of the next step are
+    // in flight while this step waits for its stage and stores its rows, and
+    // the list entries of the tile after the next are loaded meanwhile.
+    FusedPixel fu[4], nfu[4];
+    int ut[4], nut[4];
     int2 ent[4];
     bool eok[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-    {
-        const int64_t idx = int64_t(blockIdx.x) * BM + urow[i];
-        eok[i] = blockIdx.x < ntiles && idx < nrows;
-        ent[i] = eok[i] ? search_entry(P, idx) : make_int2(0, 0);
-    }
-    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
-    {
-        FusedPixel fu[4];
-        int ut[4];
+    auto entries = [&](int64_t tile) {
 #pragma unroll
         for (int i = 0; i < 4; ++i)
         {
-            fu[i] = pixel_of(P, eok[i], ent[i].x);
-            ut[i] = ent[i].y;
-            const int64_t idx = (tile + gridDim.x) * BM + urow[i];
-            eok[i] = tile + gridDim.x < ntiles && idx < nrows;
+            const int64_t idx = tile * BM + urow[i];
+            eok[i] = tile < ntiles && idx < nrows;
             ent[i] = eok[i] ? search_entry(P, idx) : make_int2(0, 0);
         }
-        for (int kb = 0; kb < P.kblocks; ++kb, ++it)
-        {
-            uint2 f[4];
+    };
+    entries(blockIdx.x);
 #pragma unroll
-            for (int i = 0; i < 4; ++i) f[i] = fst_chunk(P, tab, fu[i], kb, ukc[i]);
-            const int s = int(it % uint32_t(S));
-            const uint32_t u = it / uint32_t(S);
-            if (u > 0 && !wait_bounded(&empty_bar[s], (u - 1) & 1)) return;
-            unsigned char *sA = smem + s * stage_bytes;
-            if (p == 0)
+    for (int i = 0; i < 4; ++i) fu[i] = pixel_of(P, eok[i], ent[i].x), ut[i] = ent[i].y;
+    entries(int64_t(blockIdx.x) + gridDim.x);
+    uint2 f[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) f[i] = fst_chunk(P, tab, fu[i], 0, ukc[i]);
+    uint32_t it = 0;
+    int64_t tile = blockIdx.x;
+    int kb = 0;
+    while (true)
+    {
+        // the next step and its gathers
+        int nkb = kb + 1;
+        int64_t ntile = tile;
+        bool newtile = false;
+        if (nkb == P.kblocks) nkb = 0, ntile += gridDim.x, newtile = true;
+        const bool more = ntile < ntiles;
+        uint2 nf[4];
+        if (more)
+        {
+            if (newtile)
             {
-                arrive_expect_tx(&full_bar[s], uint32_t(b_bytes));
-                bulk_g2s(sA + a_bytes, P.wimg + int64_t(kb) * b_bytes, uint32_t(b_bytes), &full_bar[s]);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) nfu[i] = pixel_of(P, eok[i], ent[i].x), nut[i] = ent[i].y;
+                entries(ntile + gridDim.x);
+            }
+            else
+            {
+#pragma unroll
+                for (int i = 0; i < 4; ++i) nfu[i] = fu[i], nut[i] = ut[i];
             }
 #pragma unroll
-            for (int i = 0; i < 4; ++i) store_fst_rows(sA, urow[i], ut[i], 1, ukc[i], f[i], 0);
-            fence_proxy_async_smem();
-            mbar_arrive(&full_bar[s]);
+            for (int i = 0; i < 4; ++i) nf[i] = fst_chunk(P, tab, nfu[i], nkb, ukc[i]);
         }
+        const int s = int(it % uint32_t(S));
+        const uint32_t u = it / uint32_t(S);
+        if (u > 0 && !wait_bounded(&empty_bar[s], (u - 1) & 1)) return;
+        unsigned char *sA = smem + s * stage_bytes;
+        if (p == 0)
+        {
+            arrive_expect_tx(&full_bar[s], uint32_t(b_bytes));
+            bulk_g2s(sA + a_bytes, P.wimg + int64_t(kb) * b_bytes, uint32_t(b_bytes), &full_bar[s]);
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) store_fst_rows(sA, urow[i], ut[i], 1, ukc[i], f[i], 0);
+        fence_proxy_async_smem();
+        mbar_arrive(&full_bar[s]);
+        ++it;
+        if (!more) break;
+        tile = ntile, kb = nkb;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) fu[i] = nfu[i], ut[i] = nut[i], f[i] = nf[i];
     }
 }
 
@@ -1422,7 +1464,7 @@ __global__ void __launch_bounds__(kWsThreads, 1) conv_ws_kernel(TcParams P)
     int64_t nrows = 0, ntiles = P.tiles;
     if constexpr (MODE == kSearch)
     {
-        nrows = P.round == 0 ? P.npix : int64_t(*P.count_in);
+        nrows = (P.round == 0 && !P.r0_list) ? P.npix : int64_t(*P.count_in);
         ntiles = ceil_div(nrows, BM);
     }
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -1630,8 +1672,10 @@ __global__ void __launch_bounds__(kWsThreads, 1) conv_ws_kernel(TcParams P)
                 s_ok = idx < nrows;
                 if (s_ok)
                 {
-                    if (P.round == 0)
+                    if (P.round == 0 && !P.r0_list)
                         s_e = make_int2(int(idx), P.T - 1);
+                    else if (P.round == 0)
+                        s_e = make_int2(P.list_in[idx].x, P.T - 1);
                     else
                     {
                         const int2 le = P.list_in[idx];
@@ -1860,7 +1904,8 @@ template <int NS>
 __global__ void __launch_bounds__(256) fixed_split_kernel(const float *__restrict__ kernel, uint4 *__restrict__ wimg,
                                                           int cout, int cin, int taps, int nhwc, int cpad,
                                                           int kblocks, int n_tile, float *__restrict__ echan,
-                                                          unsigned *__restrict__ sinfo, int *__restrict__ negw)
+                                                          unsigned *__restrict__ sinfo, int *__restrict__ negw,
+                                                          unsigned *__restrict__ wmax)
 {
     __shared__ float s_mx[8];
     __shared__ double s_err[8];
@@ -1885,6 +1930,12 @@ __global__ void __launch_bounds__(256) fixed_split_kernel(const float *__restric
         const float w = weight(k);
         mx = fmaxf(mx, fabsf(w));
         neg |= !(w >= 0.f);
+        if (wmax && n < cout && k < kreal && w > 0.f)
+        {
+            // largest weight of each input over the channels (oracle layout)
+            const int c = nhwc ? k % cpad : k / taps, tap = nhwc ? k / cpad : k % taps;
+            if (c < cin) atomicMax(wmax + c * taps + tap, __float_as_uint(w));
+        }
         const uint32_t bits = __float_as_uint(w) & 0x7FFFFFFFu;
         if (bits != 0u && bits < 0x7F800000u)
         {
@@ -1977,6 +2028,70 @@ __global__ void search_init_kernel(unsigned *mins, unsigned *maxs, int64_t b, co
     {
         mins[i] = lean ? order_enc(0.f) : 0xFFFFFFFFu;
         maxs[i] = lean ? order_enc(0.f) : 0u;
+    }
+}
+
+// Pre-filter of round 0 for layers with few inputs per output: with no
+// negative weight, a pixel's potential at T - 1 is at most U, the sum over the
+// inputs that fired of their largest weight over the channels.  A pixel with
+// U (FP64, widened by K 2^-50 for the roundings of U and of the oracle's own
+// sum) at or below the threshold never fires and is settled here; the others
+// go to round 0's list.  A CTA per sample with its first-spike map staged in
+// shared memory.
+__global__ void __launch_bounds__(256) search_bound_kernel(TcParams P, const unsigned *__restrict__ wmax, int cp,
+                                                           int2 *__restrict__ list, int *__restrict__ count)
+{
+    if (*P.negw || *P.flag) return;
+    extern __shared__ __align__(16) unsigned char bsm[];
+    const int taps = P.kh * P.kw, kr = P.cin * taps;
+    float *wm = reinterpret_cast<float *>(bsm);
+    uint8_t *fmap = bsm + ((kr * 4 + 15) & ~15);
+    for (int i = threadIdx.x; i < kr; i += blockDim.x) wm[i] = __uint_as_float(wmax[i]);
+    const int64_t b = P.npix / P.ohw;
+    const int mapb = P.h * P.w * cp, ohw = int(P.ohw);
+    const double widen = 1.0 + double(kr) * 0x1p-50;
+    const int lane = threadIdx.x & 31;
+    for (int64_t smp = blockIdx.x; smp < b; smp += gridDim.x)
+    {
+        __syncthreads();
+        const uint8_t *src = P.in + smp * P.img_stride;
+        for (int i = threadIdx.x; i < mapb; i += blockDim.x) fmap[i] = src[i];
+        __syncthreads();
+        for (int p0 = 0; p0 < ohw; p0 += blockDim.x)
+        {
+            const int p = p0 + int(threadIdx.x);
+            const bool ok = p < ohw;
+            bool cand = false;
+            if (ok)
+            {
+                const int oy = p / P.ow, ox = p - oy * P.ow;
+                const int iy0 = oy * P.sy - P.top, ix0 = ox * P.sx - P.left;
+                const int ky0 = max(0, -iy0), ky1 = min(P.kh, P.h - iy0);
+                const int kx0 = max(0, -ix0), kx1 = min(P.kw, P.w - ix0);
+                double u = 0.0;
+                for (int c = 0; c < P.cin; ++c)
+                    for (int ky = ky0; ky < ky1; ++ky)
+                        for (int kx = kx0; kx < kx1; ++kx)
+                            if (int(fmap[((iy0 + ky) * P.w + ix0 + kx) * cp + c]) < P.T)
+                                u += double(wm[(c * P.kh + ky) * P.kw + kx]);
+                cand = u * widen > double(P.thr);
+            }
+            const int64_t pix = smp * ohw + p;
+            if (ok && !cand)
+            {
+                P.records[pix] = make_int4(0, P.T, __float_as_int(P.thv), 0);
+                if (P.wta && P.thv != 0.f)
+                {
+                    atomicMin(P.mins + smp, order_enc(P.thv));
+                    atomicMax(P.maxs + smp, order_enc(P.thv));
+                }
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, cand);
+            int base = 0;
+            if (lane == 0 && m) base = atomicAdd(count, __popc(m));
+            base = __shfl_sync(0xffffffffu, base, 0) + __popc(m & ((1u << lane) - 1u));
+            if (cand) list[base] = make_int2(int(pix), P.T - 1);
+        }
     }
 }
 
@@ -2587,7 +2702,7 @@ struct FusedLayout
     // info, counters, per-pixel state, two bisection lists, the list of
     // winners to re-read at T - 1, two lists of rows to recompute
     bool search_ok;
-    size_t w4_off, echan_off, cnt_off, state_off, la_off, lb_off, fin_off, fa_off, fb_off, va_off, vb_off;
+    size_t w4_off, echan_off, wm_off, cnt_off, state_off, la_off, lb_off, fin_off, fa_off, fb_off, va_off, vb_off;
     size_t total;
 };
 
@@ -2620,6 +2735,7 @@ FusedLayout fused_layout(int64_t b, int64_t t, int64_t cin, int64_t h, int64_t w
         const size_t np = size_t(L.npix);
         L.w4_off = off, off += align256(L.pl4.wimg_bytes);
         L.echan_off = off, off += align256(size_t(L.pl4.n_tile) * 4 + 8);
+        L.wm_off = off, off += align256(size_t(cin * kh * kw) * 4);
         L.cnt_off = off, off += 256;  // 64 counters
         L.state_off = off, off += align256(np * 16);
         L.la_off = off, off += align256(np * 8);
@@ -2766,18 +2882,31 @@ void search_layer(const TcParams &P0, const FusedLayout &L, const float *kernel,
     const int taps = P.kh * P.kw;
     P.kreal = P.nhwc ? taps * P.cpad : taps * P.cin;
     P.tiles = ceil_div(L.npix, BM);
+    // the bound pre-filter of round 0, for layers with few inputs per output
+    const int cp = P.nhwc ? P.cpad : P.cin;
+    const int kr = P.cin * taps;
+    const size_t bsm = size_t((kr * 4 + 15) & ~15) + size_t(P.h) * P.w * cp;
+    const bool prefilter = kr <= 128 && bsm <= 48 * 1024;
+    unsigned *wmax = reinterpret_cast<unsigned *>(base + L.wm_off);
     SPK_CUDA(cudaMemsetAsync(cnt, 0, 256, s));
     SPK_CUDA(cudaMemsetAsync(sinfo, 0, 8, s));
+    if (prefilter) SPK_CUDA(cudaMemsetAsync(wmax, 0, size_t(kr) * 4, s));
     auto split = pl.nsplit == 4 ? fixed_split_kernel<4> : fixed_split_kernel<3>;
     split<<<unsigned(pl.n_tile), 256, 0, s>>>(kernel, reinterpret_cast<uint4 *>(base + L.w4_off), P.cout, P.cin,
-                                              taps, P.nhwc, P.cpad, pl.kblocks, pl.n_tile, echan, sinfo, P.negw);
+                                              taps, P.nhwc, P.cpad, pl.kblocks, pl.n_tile, echan, sinfo, P.negw,
+                                              prefilter ? wmax : nullptr);
     SPK_LAUNCHED();
     if (count > 0)
     {
         search_init_kernel<<<grid_for(b, 256), 256, 0, s>>>(P.mins, P.maxs, b, P.negw, P.flag);
         SPK_LAUNCHED();
     }
-    const int cp = P.nhwc ? P.cpad : P.cin;
+    if (prefilter)
+    {
+        search_bound_kernel<<<unsigned(std::min<int64_t>(b, int64_t(sm_count()) * 8)), 256, bsm, s>>>(P, wmax, cp,
+                                                                                                      lb, cnt);
+        SPK_LAUNCHED();
+    }
     const unsigned fix_grid = unsigned(sm_count() * 4);
     int nsr = 0;
     while ((1 << nsr) < P.T) ++nsr;
@@ -2786,6 +2915,7 @@ void search_layer(const TcParams &P0, const FusedLayout &L, const float *kernel,
     {
         const bool final = count > 0 && r == rounds - 1;
         P.round = r == 0 ? 0 : (final ? 2 : 1);
+        P.r0_list = (r == 0 && prefilter) ? 1 : 0;
         P.list_in = final ? P.final_list : (r & 1 ? la : lb);
         P.count_in = final ? P.final_count : cnt + r;
         P.list_out = r & 1 ? lb : la;
