@@ -28,6 +28,7 @@
 // mbarrier wait is bounded: on timeout the kernel records an error in the
 // device status word (spk_device_status) and leaves.
 #include <algorithm>
+#include <type_traits>
 
 #include "conv_tc.cuh"
 #include "tc_ptx.cuh"
@@ -2036,62 +2037,58 @@ __global__ void search_init_kernel(unsigned *mins, unsigned *maxs, int64_t b, co
 // inputs that fired of their largest weight over the channels.  A pixel with
 // U (FP64, widened by K 2^-50 for the roundings of U and of the oracle's own
 // sum) at or below the threshold never fires and is settled here; the others
-// go to round 0's list.  A CTA per sample with its first-spike map staged in
-// shared memory.
+// go to round 0's list.  One thread per output pixel, reading the first-spike
+// map through the L1 cache.
 __global__ void __launch_bounds__(256) search_bound_kernel(TcParams P, const unsigned *__restrict__ wmax, int cp,
                                                            int2 *__restrict__ list, int *__restrict__ count)
 {
     if (*P.negw || *P.flag) return;
-    extern __shared__ __align__(16) unsigned char bsm[];
+    __shared__ float wm[128];
     const int taps = P.kh * P.kw, kr = P.cin * taps;
-    float *wm = reinterpret_cast<float *>(bsm);
-    uint8_t *fmap = bsm + ((kr * 4 + 15) & ~15);
     for (int i = threadIdx.x; i < kr; i += blockDim.x) wm[i] = __uint_as_float(wmax[i]);
-    const int64_t b = P.npix / P.ohw;
-    const int mapb = P.h * P.w * cp, ohw = int(P.ohw);
+    __syncthreads();
     const double widen = 1.0 + double(kr) * 0x1p-50;
     const int lane = threadIdx.x & 31;
-    for (int64_t smp = blockIdx.x; smp < b; smp += gridDim.x)
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t base = int64_t(blockIdx.x) * blockDim.x; base < P.npix; base += stride)
     {
-        __syncthreads();
-        const uint8_t *src = P.in + smp * P.img_stride;
-        for (int i = threadIdx.x; i < mapb; i += blockDim.x) fmap[i] = src[i];
-        __syncthreads();
-        for (int p0 = 0; p0 < ohw; p0 += blockDim.x)
+        const int64_t pix = base + threadIdx.x;
+        const bool ok = pix < P.npix;
+        bool cand = false;
+        int smp = 0;
+        if (ok)
         {
-            const int p = p0 + int(threadIdx.x);
-            const bool ok = p < ohw;
-            bool cand = false;
-            if (ok)
-            {
-                const int oy = p / P.ow, ox = p - oy * P.ow;
-                const int iy0 = oy * P.sy - P.top, ix0 = ox * P.sx - P.left;
-                const int ky0 = max(0, -iy0), ky1 = min(P.kh, P.h - iy0);
-                const int kx0 = max(0, -ix0), kx1 = min(P.kw, P.w - ix0);
-                double u = 0.0;
-                for (int c = 0; c < P.cin; ++c)
-                    for (int ky = ky0; ky < ky1; ++ky)
-                        for (int kx = kx0; kx < kx1; ++kx)
-                            if (int(fmap[((iy0 + ky) * P.w + ix0 + kx) * cp + c]) < P.T)
-                                u += double(wm[(c * P.kh + ky) * P.kw + kx]);
-                cand = u * widen > double(P.thr);
-            }
-            const int64_t pix = smp * ohw + p;
-            if (ok && !cand)
-            {
-                P.records[pix] = make_int4(0, P.T, __float_as_int(P.thv), 0);
-                if (P.wta && P.thv != 0.f)
+            smp = int(pix / P.ohw);
+            const int p = int(pix - int64_t(smp) * P.ohw);
+            const int oy = p / P.ow, ox = p - oy * P.ow;
+            const int iy0 = oy * P.sy - P.top, ix0 = ox * P.sx - P.left;
+            const int ky0 = max(0, -iy0), ky1 = min(P.kh, P.h - iy0);
+            const int kx0 = max(0, -ix0), kx1 = min(P.kw, P.w - ix0);
+            const uint8_t *fm = P.in + int64_t(smp) * P.img_stride;
+            double u = 0.0;
+            for (int ky = ky0; ky < ky1; ++ky)
+                for (int kx = kx0; kx < kx1; ++kx)
                 {
-                    atomicMin(P.mins + smp, order_enc(P.thv));
-                    atomicMax(P.maxs + smp, order_enc(P.thv));
+                    const uint8_t *f = fm + (int64_t(iy0 + ky) * P.w + ix0 + kx) * cp;
+                    for (int c = 0; c < P.cin; ++c)
+                        if (int(__ldg(f + c)) < P.T) u += double(wm[(c * P.kh + ky) * P.kw + kx]);
                 }
-            }
-            const unsigned m = __ballot_sync(0xffffffffu, cand);
-            int base = 0;
-            if (lane == 0 && m) base = atomicAdd(count, __popc(m));
-            base = __shfl_sync(0xffffffffu, base, 0) + __popc(m & ((1u << lane) - 1u));
-            if (cand) list[base] = make_int2(int(pix), P.T - 1);
+            cand = u * widen > double(P.thr);
         }
+        if (ok && !cand)
+        {
+            P.records[pix] = make_int4(0, P.T, __float_as_int(P.thv), 0);
+            if (P.wta && P.thv != 0.f)
+            {
+                atomicMin(P.mins + smp, order_enc(P.thv));
+                atomicMax(P.maxs + smp, order_enc(P.thv));
+            }
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, cand);
+        int b0 = 0;
+        if (lane == 0 && m) b0 = atomicAdd(count, __popc(m));
+        b0 = __shfl_sync(0xffffffffu, b0, 0) + __popc(m & ((1u << lane) - 1u));
+        if (cand) list[b0] = make_int2(int(pix), P.T - 1);
     }
 }
 
@@ -2195,60 +2192,131 @@ __global__ void __launch_bounds__(128) search_fix_kernel(TcParams P, const float
     }
 }
 
-// Per-pixel spike codes w | t0 << 16 (t0 = T: never) of maps too large to
-// stage in shared memory.
-__global__ void search_codes_kernel(const int4 *__restrict__ records, uint32_t *__restrict__ codes, int64_t npix,
+// Per-pixel winner and first-step bytes (t0 = T: never) of maps too large to
+// stage in shared memory: wbytes [npix], then tbytes [npix].
+__global__ void search_codes_kernel(const int4 *__restrict__ records, uint8_t *__restrict__ codes, int64_t npix,
                                     int T, const int *negw, const int *flag)
 {
     if (*negw || *flag) return;
     for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < npix; i += int64_t(gridDim.x) * blockDim.x)
     {
         const int4 r = records[i];
-        codes[i] = uint32_t(r.x & 0xFFFF) | (uint32_t(min(r.y, T)) << 16);
+        codes[i] = uint8_t(r.x);
+        codes[npix + i] = uint8_t(min(r.y, T));
     }
 }
 
+// Byte-parallel tests on four pixels at once (bytes below 0x80): the bytes
+// of w that equal c, and the bytes of t0 at or below t, as 0x80 flags.
+__device__ __forceinline__ uint32_t bytes_eq(uint32_t w, uint32_t c4)
+{
+    const uint32_t x = w ^ c4;
+    return ~(((x & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | x | 0x7F7F7F7Fu);
+}
+__device__ __forceinline__ uint32_t bytes_le(uint32_t t0, uint32_t t4) { return ((t4 | 0x80808080u) - t0) & 0x80808080u; }
+
 // Spikes (and pooled spikes) of the search path from the per-pixel records:
 // channel w fires from step t0 on.  A CTA per sample writes its
-// [T, C, OH, OW] block as 4-byte words, one output word per thread and
-// pass, with the sample's codes w | t0 << 16 in shared memory (or read from
-// `gcodes` for maps above 16384 pixels); consecutive threads read
-// consecutive 16-byte code groups, so the reads are free of bank conflicts.
-// Pooled spikes [T, C, POH, POW] come from a table of the first firing step
-// per (channel, cell): a cell fires from the earliest t0 of its window's
-// pixels won by that channel.  Off the search path (negative weights or
-// other input) it writes zeros, which the dense kernel then fills.
-__global__ void __launch_bounds__(256) search_write_kernel(const int4 *__restrict__ records,
-                                                           const uint32_t *__restrict__ gcodes, const int *negw,
-                                                           const int *flag, uint8_t *__restrict__ spikes,
-                                                           uint8_t *__restrict__ pooled, int64_t b, int T, int C,
-                                                           int ohw, int ow, int pky, int pkx, int poh, int pow_,
-                                                           int ptab)
+// [T, C, OH, OW] block; per pixel the winner and first-step bytes sit in
+// shared memory (or in global memory for maps above 16384 pixels), and a
+// thread makes V output bytes per store (16 when a plane holds a multiple of
+// 16 pixels, else 4) with byte-parallel compares.  Pooled spikes
+// [T, C, POH, POW] come from a byte table of the first firing step per
+// (channel, cell): a cell fires from the earliest t0 of its window's pixels
+// won by that channel.  Off the search path (negative weights or other
+// input) it writes zeros, which the dense kernel then fills.
+template <int V>
+__device__ __forceinline__ void write_plane_words(uint8_t *dst, int64_t n, int hw, int C, bool lean, bool pass0,
+                                                  const uint8_t *wsrc, const uint8_t *tsrc, int tstride)
 {
-    extern __shared__ uint32_t scode[];  // [ohw rounded to 4] codes, then [C][phw] first steps when ptab
+    using Vec = typename std::conditional<V == 16, uint4, uint32_t>::type;
+    Vec *dv = reinterpret_cast<Vec *>(dst);
+    const int wpp = hw / V, nv = int(n / V);
+    const int dplane = int(blockDim.x) / wpp, dw = int(blockDim.x) - dplane * wpp;
+    int wq = int(threadIdx.x) % wpp, plane = int(threadIdx.x) / wpp;
+    int t = plane / C, c = plane - t * C;
+    for (int i = threadIdx.x; i < nv; i += blockDim.x)
+    {
+        uint32_t o[V / 4];
+#pragma unroll
+        for (int q = 0; q < V / 4; ++q) o[q] = 0u;
+        if (lean)
+        {
+            const int px = V * wq;
+            const uint32_t t4 = uint32_t(t) * 0x01010101u, c4 = uint32_t(c) * 0x01010101u;
+            if (pass0)
+            {
+#pragma unroll
+                for (int q = 0; q < V / 4; ++q)
+                {
+                    const uint32_t w = *reinterpret_cast<const uint32_t *>(wsrc + px + 4 * q);
+                    const uint32_t t0 = *reinterpret_cast<const uint32_t *>(tsrc + px + 4 * q);
+                    o[q] = ((bytes_eq(w, c4) & bytes_le(t0, t4)) >> 7);
+                }
+            }
+            else
+            {
+#pragma unroll
+                for (int q = 0; q < V / 4; ++q)
+                    o[q] = bytes_le(*reinterpret_cast<const uint32_t *>(tsrc + c * tstride + px + 4 * q), t4) >> 7;
+            }
+        }
+        if constexpr (V == 16)
+            dv[i] = make_uint4(o[0], o[1], o[2], o[3]);
+        else
+            dv[i] = o[0];
+        wq += dw, c += dplane;
+        if (wq >= wpp) wq -= wpp, ++c;
+        while (c >= C) c -= C, ++t;
+    }
+}
+
+__global__ void __launch_bounds__(256) search_write_kernel(const int4 *__restrict__ records,
+                                                           const uint8_t *__restrict__ gcodes, int64_t npix,
+                                                           const int *negw, const int *flag,
+                                                           uint8_t *__restrict__ spikes, uint8_t *__restrict__ pooled,
+                                                           int64_t b, int T, int C, int ohw, int ow, int pky,
+                                                           int pkx, int poh, int pow_, int ptab)
+{
+    // [ohw16] winner bytes, [ohw16] first-step bytes, then [C][phw16] pooled first steps
+    extern __shared__ __align__(16) uint8_t wsm_[];
     const bool lean = !*negw && !*flag;
-    const int ohw4 = (ohw + 3) & ~3, phw = poh * pow_;
-    uint32_t *first = scode + ohw4;
+    const int ohw16 = (ohw + 15) & ~15, phw = poh * pow_, phw16 = (phw + 15) & ~15;
+    uint8_t *sw = wsm_, *st = wsm_ + ohw16, *first = wsm_ + 2 * ohw16;
     for (int64_t smp = blockIdx.x; smp < b; smp += gridDim.x)
     {
-        const uint32_t *code = gcodes ? gcodes + smp * ohw : scode;
+        const uint8_t *wsrc = gcodes ? gcodes + smp * ohw : sw;
+        const uint8_t *tsrc = gcodes ? gcodes + npix + smp * ohw : st;
         if (lean && !gcodes)
             for (int p = threadIdx.x; p < ohw; p += blockDim.x)
             {
                 const int4 r = records[smp * ohw + p];
-                scode[p] = uint32_t(r.x & 0xFFFF) | (uint32_t(min(r.y, T)) << 16);
+                sw[p] = uint8_t(r.x), st[p] = uint8_t(min(r.y, T));
             }
         if (lean && ptab)
-            for (int i = threadIdx.x; i < C * phw; i += blockDim.x) first[i] = uint32_t(T);
+            for (int i = threadIdx.x; i < C * phw16; i += blockDim.x) first[i] = uint8_t(T);
         __syncthreads();
         if (lean && ptab)
         {
+            // earliest t0 per (channel, cell): bytes updated through their word
             for (int p = threadIdx.x; p < ohw; p += blockDim.x)
             {
                 const int y = p / ow, x = p - y * ow, py = y / pky, px = x / pkx;
-                const uint32_t k = code[p];
-                if (py < poh && px < pow_ && int(k >> 16) < T)
-                    atomicMin(first + int(k & 0xFFFF) * phw + py * pow_ + px, k >> 16);
+                const int t0 = int(tsrc[p]);
+                if (py < poh && px < pow_ && t0 < T)
+                {
+                    const int idx = int(wsrc[p]) * phw16 + py * pow_ + px;
+                    unsigned *word = reinterpret_cast<unsigned *>(first + (idx & ~3));
+                    const int sh = 8 * (idx & 3);
+                    unsigned old = *word;
+                    while (int((old >> sh) & 0xFF) > t0)
+                    {
+                        const unsigned nw = (old & ~(0xFFu << sh)) | (unsigned(t0) << sh);
+                        const unsigned seen = atomicCAS(word, old, nw);
+                        if (seen == old) break;
+                        old = seen;
+                    }
+                }
             }
             __syncthreads();
         }
@@ -2257,70 +2325,38 @@ __global__ void __launch_bounds__(256) search_write_kernel(const int4 *__restric
             const int hw = pass == 0 ? ohw : phw;
             const int64_t n = int64_t(T) * C * hw;
             uint8_t *dst = (pass == 0 ? spikes : pooled) + smp * n;
-            // byte f of the block
-            auto spike = [&](int64_t f) -> uint32_t {
-                if (!lean) return 0u;
-                const int plane = int(f / hw), px = int(f - int64_t(plane) * hw);
-                const int t = plane / C, c = plane - t * C;
-                if (pass == 0)
+            const bool table = pass == 0 || ptab || !lean;
+            const uintptr_t a = reinterpret_cast<uintptr_t>(dst);
+            const bool srcal = gcodes == nullptr || (ohw % 16 == 0);
+            if (table && hw % 16 == 0 && (a & 15) == 0 && srcal)
+                write_plane_words<16>(dst, n, hw, C, lean, pass == 0, wsrc, pass == 0 ? tsrc : first, phw16);
+            else if (table && hw % 4 == 0 && (a & 3) == 0 && (gcodes == nullptr || ohw % 4 == 0))
+                write_plane_words<4>(dst, n, hw, C, lean, pass == 0, wsrc, pass == 0 ? tsrc : first, phw16);
+            else
+                for (int64_t f = threadIdx.x; f < n; f += blockDim.x)
                 {
-                    const uint32_t k = code[px];
-                    return (int(k & 0xFFFF) == c && int(k >> 16) <= t) ? 1u : 0u;
+                    uint8_t v = 0;
+                    if (lean)
+                    {
+                        const int plane = int(f / hw), px = int(f - int64_t(plane) * hw);
+                        const int t = plane / C, c = plane - t * C;
+                        if (pass == 0)
+                            v = (int(wsrc[px]) == c && int(tsrc[px]) <= t) ? 1 : 0;
+                        else if (ptab)
+                            v = int(first[c * phw16 + px]) <= t ? 1 : 0;
+                        else
+                        {
+                            const int py = px / pow_, pxx = px - py * pow_;
+                            for (int dy = 0; dy < pky; ++dy)
+                                for (int dx = 0; dx < pkx; ++dx)
+                                {
+                                    const int q = (py * pky + dy) * ow + pxx * pkx + dx;
+                                    v |= (int(wsrc[q]) == c && int(tsrc[q]) <= t) ? 1 : 0;
+                                }
+                        }
+                    }
+                    dst[f] = v;
                 }
-                if (ptab) return int(first[c * hw + px]) <= t ? 1u : 0u;
-                const int py = px / pow_, pxx = px - py * pow_;
-                uint32_t any = 0;
-                for (int dy = 0; dy < pky; ++dy)
-                    for (int dx = 0; dx < pkx; ++dx)
-                    {
-                        const uint32_t k = code[(py * pky + dy) * ow + pxx * pkx + dx];
-                        any |= (int(k & 0xFFFF) == c && int(k >> 16) <= t) ? 1u : 0u;
-                    }
-                return any;
-            };
-            const bool words = hw % 4 == 0 && (reinterpret_cast<uintptr_t>(dst) & 3) == 0 &&
-                               (pass == 1 ? (ptab || !lean) : true);
-            if (!words)
-            {
-                for (int64_t f = threadIdx.x; f < n; f += blockDim.x) dst[f] = uint8_t(spike(f));
-                continue;
-            }
-            uint32_t *d4 = reinterpret_cast<uint32_t *>(dst);
-            const uint32_t *src = pass == 0 ? code : first;
-            // word i = (plane, px / 4), plane = t C + c, advanced by the block
-            // stride without divisions
-            const int wpp = hw / 4, nwords = int(n / 4);
-            const int dplane = int(blockDim.x) / wpp, dw = int(blockDim.x) - dplane * wpp;
-            int wq = int(threadIdx.x) % wpp, plane = int(threadIdx.x) / wpp;
-            int t = plane / C, c = plane - t * C;
-            for (int i = threadIdx.x; i < nwords; i += blockDim.x)
-            {
-                uint32_t wv = 0;
-                const int px = 4 * wq;
-                if (lean)
-                {
-                    if (pass == 0)
-                    {
-                        const uint4 k = *reinterpret_cast<const uint4 *>(src + px);
-                        const uint32_t cc = uint32_t(c), tt = uint32_t(t);
-                        wv = ((k.x & 0xFFFF) == cc && (k.x >> 16) <= tt ? 1u : 0u) |
-                             ((k.y & 0xFFFF) == cc && (k.y >> 16) <= tt ? 1u << 8 : 0u) |
-                             ((k.z & 0xFFFF) == cc && (k.z >> 16) <= tt ? 1u << 16 : 0u) |
-                             ((k.w & 0xFFFF) == cc && (k.w >> 16) <= tt ? 1u << 24 : 0u);
-                    }
-                    else
-                    {
-                        const uint4 k = *reinterpret_cast<const uint4 *>(src + c * hw + px);
-                        const uint32_t tt = uint32_t(t);
-                        wv = (k.x <= tt ? 1u : 0u) | (k.y <= tt ? 1u << 8 : 0u) | (k.z <= tt ? 1u << 16 : 0u) |
-                             (k.w <= tt ? 1u << 24 : 0u);
-                    }
-                }
-                d4[i] = wv;
-                wq += dw, c += dplane;
-                if (wq >= wpp) wq -= wpp, ++c;
-                while (c >= C) c -= C, ++t;
-            }
         }
         __syncthreads();
     }
@@ -2885,8 +2921,7 @@ void search_layer(const TcParams &P0, const FusedLayout &L, const float *kernel,
     // the bound pre-filter of round 0, for layers with few inputs per output
     const int cp = P.nhwc ? P.cpad : P.cin;
     const int kr = P.cin * taps;
-    const size_t bsm = size_t((kr * 4 + 15) & ~15) + size_t(P.h) * P.w * cp;
-    const bool prefilter = kr <= 128 && bsm <= 48 * 1024;
+    const bool prefilter = kr <= 128;
     unsigned *wmax = reinterpret_cast<unsigned *>(base + L.wm_off);
     SPK_CUDA(cudaMemsetAsync(cnt, 0, 256, s));
     SPK_CUDA(cudaMemsetAsync(sinfo, 0, 8, s));
@@ -2903,8 +2938,7 @@ void search_layer(const TcParams &P0, const FusedLayout &L, const float *kernel,
     }
     if (prefilter)
     {
-        search_bound_kernel<<<unsigned(std::min<int64_t>(b, int64_t(sm_count()) * 8)), 256, bsm, s>>>(P, wmax, cp,
-                                                                                                      lb, cnt);
+        search_bound_kernel<<<grid_for(L.npix, 256), 256, 0, s>>>(P, wmax, cp, lb, cnt);
         SPK_LAUNCHED();
     }
     const unsigned fix_grid = unsigned(sm_count() * 4);
@@ -2929,23 +2963,24 @@ void search_layer(const TcParams &P0, const FusedLayout &L, const float *kernel,
         SPK_LAUNCHED();
     }
     const int ohw = int(L.oh * L.ow);
-    uint32_t *gcodes = nullptr;
-    size_t wsm = size_t((ohw + 3) & ~3) * 4;
+    uint8_t *gcodes = nullptr;
+    const size_t ohw16 = size_t((ohw + 15) & ~15);
+    size_t wsm = 2 * ohw16;
     if (ohw > 16384)
     {
-        // the bisection state is no longer needed: its words hold the codes
-        gcodes = reinterpret_cast<uint32_t *>(P.state);
-        wsm = 0;
+        // the bisection state is no longer needed: its bytes hold the codes
+        gcodes = reinterpret_cast<uint8_t *>(P.state);
+        wsm = 2 * 16;
         search_codes_kernel<<<grid_for(L.npix, 256), 256, 0, s>>>(P.records, gcodes, L.npix, P.T, P.negw, P.flag);
         SPK_LAUNCHED();
     }
-    // table of first firing steps per (channel, pooled cell) when it fits
-    const size_t tab_bytes = size_t(P.cout) * size_t(poh * pow_) * 4;
+    // byte table of first firing steps per (channel, pooled cell) when it fits
+    const size_t tab_bytes = size_t(P.cout) * size_t(((poh * pow_) + 15) & ~15);
     const int ptab = pool_ky > 0 && wsm + tab_bytes <= 160 * 1024 ? 1 : 0;
     if (ptab) wsm += tab_bytes;
     SPK_CUDA(cudaFuncSetAttribute(search_write_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(wsm)));
     search_write_kernel<<<unsigned(std::min<int64_t>(b, int64_t(sm_count()) * 16)), 256, wsm, s>>>(
-        P.records, gcodes, P.negw, P.flag, spikes, pool_ky > 0 ? pooled : nullptr, b, P.T, P.cout, ohw,
+        P.records, gcodes, L.npix, P.negw, P.flag, spikes, pool_ky > 0 ? pooled : nullptr, b, P.T, P.cout, ohw,
         int(L.ow), int(pool_ky), int(pool_kx), int(poh), int(pow_), ptab);
     SPK_LAUNCHED();
 }
