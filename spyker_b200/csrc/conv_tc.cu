@@ -1208,50 +1208,29 @@ __device__ void search_epilogue(const TcParams &P, uint32_t acc, bool ok, int pi
     else
     {
         // tier 1: the largest potential (first index), its runner-up, and the
-        // term sums of the largest
-        LeanMax st, st2;
-        uint32_t wb[NS], wb2[NS];
+        // term sums of the largest; one 8-column chunk at a time (a second
+        // CTA on the SM hides the load latency)
+        LeanMax st;
+        uint32_t wb[NS];
 #pragma unroll
-        for (int i = 0; i < NS; ++i) wb[i] = wb2[i] = 0u;
+        for (int i = 0; i < NS; ++i) wb[i] = 0u;
+        for (int cb = 0; cb < P.n_tile; cb += kEpiChunk)
         {
-            constexpr int W = kEpiChunk;
-            uint32_t qa[NS][W], qb[NS][W];
-            s_chunk<NS>(lane_base, 0, P.n_tile, qa);
-            for (int cb = 0; cb < P.n_tile; cb += 2 * W)
+            uint32_t q[NS][kEpiChunk];
+            s_chunk<NS>(lane_base, cb, P.n_tile, q);
+            s_chunk_wait<NS>(q);
+            const int lim = P.cout - cb;
+#pragma unroll
+            for (int j = 0; j < kEpiChunk; ++j)
             {
-                s_chunk_wait<NS>(qa);
-                s_chunk<NS>(lane_base, cb + W, P.n_tile, qb);
-                const int lim = P.cout - cb;
+                const float f = j < lim ? s_fast<NS>(q, j) : -INFINITY;
+                const bool gt = f > st.r1;
+                st.r2 = gt ? st.r1 : fmaxf(st.r2, f);
+                st.r1 = gt ? f : st.r1;
+                st.a1 = gt ? cb + j : st.a1;
 #pragma unroll
-                for (int j = 0; j < W; ++j)
-                {
-                    const float f = j < lim ? s_fast<NS>(qa, j) : -INFINITY;
-                    const bool gt = f > st.r1;
-                    st.r2 = gt ? st.r1 : fmaxf(st.r2, f);
-                    st.r1 = gt ? f : st.r1;
-                    st.a1 = gt ? cb + j : st.a1;
-#pragma unroll
-                    for (int i = 0; i < NS; ++i) wb[i] = gt ? qa[i][j] : wb[i];
-                }
-                s_chunk_wait<NS>(qb);
-                if (cb + 2 * W < P.n_tile) s_chunk<NS>(lane_base, cb + 2 * W, P.n_tile, qa);
-                const int lim2 = lim - W;
-#pragma unroll
-                for (int j = 0; j < W; ++j)
-                {
-                    const float f = j < lim2 ? s_fast<NS>(qb, j) : -INFINITY;
-                    const bool gt = f > st2.r1;
-                    st2.r2 = gt ? st2.r1 : fmaxf(st2.r2, f);
-                    st2.r1 = gt ? f : st2.r1;
-                    st2.a1 = gt ? cb + W + j : st2.a1;
-#pragma unroll
-                    for (int i = 0; i < NS; ++i) wb2[i] = gt ? qb[i][j] : wb2[i];
-                }
+                for (int i = 0; i < NS; ++i) wb[i] = gt ? q[i][j] : wb[i];
             }
-            const bool take = st2.r1 > st.r1 || (st2.r1 == st.r1 && st2.a1 >= 0 && (st.a1 < 0 || st2.a1 < st.a1));
-#pragma unroll
-            for (int i = 0; i < NS; ++i) wb[i] = take ? wb2[i] : wb[i];
-            merge_lean(st, st2);
         }
         const float tol1 = __fmaf_ru(fabsf(st.r1), 0x1.9p-23f, c0);
         int d1 = 0;  // tier-1 decision
@@ -1347,87 +1326,87 @@ __device__ __forceinline__ FusedPixel pixel_of(const TcParams &P, bool ok, int g
     return u;
 }
 
+// A search row's pixel in three words: byte offset of its sample's
+// first-spike map (-1: no row), receptive-field origin (iy0, ix0) packed as
+// two 16-bit fields, and its step.
+__device__ __forceinline__ uint2 fst_chunk_c(const TcParams &P, const int4 *tab, int base, int yx, int kb, int kc)
+{
+    if (base < 0) return make_uint2(~0u, ~0u);
+    const int iy0 = int(uint32_t(yx) >> 16) - 32768, ix0 = int(uint32_t(yx) & 0xFFFFu) - 32768;
+    const uint8_t *img = P.in + base;
+    if (P.nhwc)
+    {
+        const int4 e = tab[ftab(P.kblocks, kb, kc, 0)];
+        const int iy = iy0 + e.y, ix = ix0 + e.z;
+        if (e.w && iy >= 0 && iy < P.h && ix >= 0 && ix < P.w)
+            return *reinterpret_cast<const uint2 *>(img + (iy * P.w + ix) * P.cpad + e.x);
+        return make_uint2(~0u, ~0u);
+    }
+    uint32_t w[2] = {0, 0};
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+    {
+        const int4 e = tab[ftab(P.kblocks, kb, kc, i)];
+        const int iy = iy0 + e.y, ix = ix0 + e.z;
+        uint32_t b = 0xFF;
+        if (e.w && iy >= 0 && iy < P.h && ix >= 0 && ix < P.w) b = img[(iy * P.w + ix) * P.cin + e.x];
+        w[i >> 2] |= b << (8 * (i & 3));
+    }
+    return make_uint2(w[0], w[1]);
+}
+
+// Search producers: a thread builds NU (row, 8-wide K chunk) units of every K
+// block, one row each at that row's own step.  Unit i of thread p is row
+// (p & 7) + 8 (p >> 6) + (1024 / NU / 8) i and chunk (p >> 3) & 7, so the 8
+// lanes of a quarter warp take 8 consecutive rows of one chunk (distinct
+// 16-byte bank groups).  The gathers of a step are issued before the wait for
+// its stage, all NU in flight together.
+template <int NU>
 __device__ __forceinline__ void search_producer(const TcParams &P, const int4 *tab, unsigned char *smem,
                                                 uint64_t *full_bar, uint64_t *empty_bar, int S, int stage_bytes,
                                                 int a_bytes, int b_bytes, int p, int64_t nrows, int64_t ntiles)
 {
-    int urow[4], ukc[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-    {
-        const int q = p + i * 256;
-        urow[i] = (q & 7) + 8 * (q >> 6), ukc[i] = (q >> 3) & 7;
-    }
+    constexpr int NT = 1024 / NU, RS = NT / 8;  // producer threads; row step between a thread's units
+    const int row0 = (p & 7) + 8 * (p >> 6), kc = (p >> 3) & 7;
     if (int64_t(blockIdx.x) >= ntiles) return;
-    // One step ahead over (tile, K block): the gathers of the next step are
-    // in flight while this step waits for its stage and stores its rows, and
-    // the list entries of the tile after the next are loaded meanwhile.
-    FusedPixel fu[4], nfu[4];
-    int ut[4], nut[4];
-    int2 ent[4];
-    bool eok[4];
-    auto entries = [&](int64_t tile) {
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-        {
-            const int64_t idx = tile * BM + urow[i];
-            eok[i] = tile < ntiles && idx < nrows;
-            ent[i] = eok[i] ? search_entry(P, idx) : make_int2(0, 0);
-        }
-    };
-    entries(blockIdx.x);
-#pragma unroll
-    for (int i = 0; i < 4; ++i) fu[i] = pixel_of(P, eok[i], ent[i].x), ut[i] = ent[i].y;
-    entries(int64_t(blockIdx.x) + gridDim.x);
-    uint2 f[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) f[i] = fst_chunk(P, tab, fu[i], 0, ukc[i]);
     uint32_t it = 0;
-    int64_t tile = blockIdx.x;
-    int kb = 0;
-    while (true)
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
     {
-        // the next step and its gathers
-        int nkb = kb + 1;
-        int64_t ntile = tile;
-        bool newtile = false;
-        if (nkb == P.kblocks) nkb = 0, ntile += gridDim.x, newtile = true;
-        const bool more = ntile < ntiles;
-        uint2 nf[4];
-        if (more)
+        int ubase[NU], uyx[NU], ut[NU];
+#pragma unroll
+        for (int i = 0; i < NU; ++i)
         {
-            if (newtile)
+            const int64_t idx = tile * BM + row0 + RS * i;
+            ubase[i] = -1, uyx[i] = 0, ut[i] = 0;
+            if (idx < nrows)
             {
-#pragma unroll
-                for (int i = 0; i < 4; ++i) nfu[i] = pixel_of(P, eok[i], ent[i].x), nut[i] = ent[i].y;
-                entries(ntile + gridDim.x);
+                const int2 e = search_entry(P, idx);
+                const uint32_t ohw = uint32_t(P.ohw), smp = uint32_t(e.x) / ohw, pix = uint32_t(e.x) - smp * ohw;
+                const int oy = int(pix / uint32_t(P.ow)), ox = int(pix) - oy * P.ow;
+                ubase[i] = int(int64_t(smp) * P.img_stride);
+                uyx[i] = int((uint32_t(oy * P.sy - P.top + 32768) << 16) | uint32_t(ox * P.sx - P.left + 32768));
+                ut[i] = e.y;
             }
-            else
-            {
-#pragma unroll
-                for (int i = 0; i < 4; ++i) nfu[i] = fu[i], nut[i] = ut[i];
-            }
-#pragma unroll
-            for (int i = 0; i < 4; ++i) nf[i] = fst_chunk(P, tab, nfu[i], nkb, ukc[i]);
         }
-        const int s = int(it % uint32_t(S));
-        const uint32_t u = it / uint32_t(S);
-        if (u > 0 && !wait_bounded(&empty_bar[s], (u - 1) & 1)) return;
-        unsigned char *sA = smem + s * stage_bytes;
-        if (p == 0)
+        for (int kb = 0; kb < P.kblocks; ++kb, ++it)
         {
-            arrive_expect_tx(&full_bar[s], uint32_t(b_bytes));
-            bulk_g2s(sA + a_bytes, P.wimg + int64_t(kb) * b_bytes, uint32_t(b_bytes), &full_bar[s]);
+            uint2 f[NU];
+#pragma unroll
+            for (int i = 0; i < NU; ++i) f[i] = fst_chunk_c(P, tab, ubase[i], uyx[i], kb, kc);
+            const int s = int(it % uint32_t(S));
+            const uint32_t u = it / uint32_t(S);
+            if (u > 0 && !wait_bounded(&empty_bar[s], (u - 1) & 1)) return;
+            unsigned char *sA = smem + s * stage_bytes;
+            if (p == 0)
+            {
+                arrive_expect_tx(&full_bar[s], uint32_t(b_bytes));
+                bulk_g2s(sA + a_bytes, P.wimg + int64_t(kb) * b_bytes, uint32_t(b_bytes), &full_bar[s]);
+            }
+#pragma unroll
+            for (int i = 0; i < NU; ++i) store_fst_rows(sA, row0 + RS * i, ut[i], 1, kc, f[i], 0);
+            fence_proxy_async_smem();
+            mbar_arrive(&full_bar[s]);
         }
-#pragma unroll
-        for (int i = 0; i < 4; ++i) store_fst_rows(sA, urow[i], ut[i], 1, ukc[i], f[i], 0);
-        fence_proxy_async_smem();
-        mbar_arrive(&full_bar[s]);
-        ++it;
-        if (!more) break;
-        tile = ntile, kb = nkb;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) fu[i] = nfu[i], ut[i] = nut[i], f[i] = nf[i];
     }
 }
 
@@ -1442,11 +1421,14 @@ __device__ __forceinline__ void search_producer(const TcParams &P, const int4 *t
 // (MMA commit); accumulators: acc_full[a] (MMA commit), acc_empty[a] (128
 // epilogue arrivals).  Every wait is bounded; a timeout raises the device
 // status word and makes every role leave.
-constexpr int kWsThreads = 416, kMaxStages = 6;
-__host__ __device__ constexpr int ws_threads(int) { return kWsThreads; }
+//
+// The search kernel (kSearch) runs with 4 producer warps (288 threads) so
+// that two CTAs fit on an SM where their tensor memory allows: its
+// per-tile work is latency-bound, and a second CTA hides those latencies.
+constexpr int kWsThreads = 416, kSearchThreads = 288, kMaxStages = 6;
 
-template <int MODE>
-__global__ void __launch_bounds__(kWsThreads, 1) conv_ws_kernel(TcParams P)
+template <int MODE, int NPW>
+__device__ __forceinline__ void conv_ws_body(const TcParams &P)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ __align__(8) uint64_t full_bar[kMaxStages], empty_bar[kMaxStages], accf_bar[2], acce_bar[2], tim_bar;
@@ -1508,7 +1490,8 @@ __global__ void __launch_bounds__(kWsThreads, 1) conv_ws_kernel(TcParams P)
     }
     if (tid == 0)
     {
-        for (int s = 0; s < S; ++s) mbar_init(&full_bar[s], 257), mbar_init(&empty_bar[s], 1);
+        for (int s = 0; s < S; ++s)
+            mbar_init(&full_bar[s], 1 + 32 * NPW), mbar_init(&empty_bar[s], 1);
         for (int a = 0; a < 2; ++a) mbar_init(&accf_bar[a], 1), mbar_init(&acce_bar[a], 128);
         mbar_init(&tim_bar, 128);
         fence_mbar_init();
@@ -1524,9 +1507,11 @@ __global__ void __launch_bounds__(kWsThreads, 1) conv_ws_kernel(TcParams P)
     const uint32_t tmem = tmem_slot;
     const int acc_cols = P.nsplit * P.n_tile;
 
-    if (MODE == kSearch && warp >= 4 && warp < 12)
-        search_producer(P, tab, smem, full_bar, empty_bar, S, stage_bytes, a_bytes, b_bytes, tid - 128, nrows, ntiles);
-    else if (MODE != kPotentials && warp >= 4 && warp < 12)
+    constexpr int kMmaWarp = 4 + NPW;
+    if (MODE == kSearch && warp >= 4 && warp < kMmaWarp)
+        search_producer<1024 / (32 * NPW)>(P, tab, smem, full_bar, empty_bar, S, stage_bytes, a_bytes, b_bytes,
+                                           tid - 128, nrows, ntiles);
+    else if (MODE != kPotentials && MODE != kSearch && warp >= 4 && warp < kMmaWarp)
     {
         // ---------------- fused producers (8 warps) ----------------
         if (P.tp_log2 >= 2)
@@ -1534,7 +1519,7 @@ __global__ void __launch_bounds__(kWsThreads, 1) conv_ws_kernel(TcParams P)
         else
             fused_producer<4>(P, tab, smem, full_bar, empty_bar, S, stage_bytes, a_bytes, b_bytes, tid - 128);
     }
-    else if (warp >= 4 && warp < 12)
+    else if (MODE == kPotentials && warp >= 4 && warp < kMmaWarp)
     {
         // ---------------- producers (8 warps) ----------------
         // Thread p gathers K chunks c_lo..c_lo+3 of row prow.  The loads of the
@@ -1592,7 +1577,7 @@ __global__ void __launch_bounds__(kWsThreads, 1) conv_ws_kernel(TcParams P)
             }
         }
     }
-    else if (warp == 12)
+    else if (warp == kMmaWarp)
     {
         // ---------------- MMA issuer ----------------
         if (lane == 0)
@@ -1750,6 +1735,16 @@ __global__ void __launch_bounds__(kWsThreads, 1) conv_ws_kernel(TcParams P)
         tmem_dealloc(tmem, P.tmem_cols);
     }
 }
+
+template <int MODE>
+__global__ void __launch_bounds__(kWsThreads, 1) conv_ws_kernel(TcParams P)
+{
+    conv_ws_body<MODE, 8>(P);
+}
+
+// The search kernel for layers whose accumulators leave room for a second
+// CTA on the SM (4 producer warps).
+__global__ void __launch_bounds__(kSearchThreads, 2) search_ws_kernel(TcParams P) { conv_ws_body<kSearch, 4>(P); }
 
 // WTA over the per-pixel records of one sample (one CTA per sample).  Keys
 // follow cpu/wta.cpp:53-62 with the sample's min / max; ties resolve to the
@@ -2416,7 +2411,9 @@ Plan make_plan(int64_t n, int64_t cin, int64_t h, int64_t w, int64_t cout, int64
                        : !pl.nhwc   ? size_t(pl.kblocks) * BK * 16
                                     : size_t(pl.kblocks) * 8 * 16;
     const size_t stage = size_t(BM * BK * 2) + size_t(pl.nsplit) * pl.n_tile * BK * 2;
-    const size_t budget = 225 * 1024 - tab;
+    // the search kernel aims at two CTAs per SM where its tensor memory allows
+    const bool two = nsplit > 0 && cols <= 256;
+    const size_t budget = (two ? 110 * 1024 : 225 * 1024) - tab;
     pl.stages = int(std::min<size_t>(g_schedule.stages > 0 ? size_t(g_schedule.stages) : 4, budget / stage));
     size_t smem = size_t(pl.stages) * stage + tab;
     // At most 512 / tmem_cols CTAs may share an SM's tensor memory: size the
@@ -2717,14 +2714,21 @@ TcParams prepare(const Plan &pl, const void *in, const float *kernel, int64_t n,
 template <int MODE>
 void launch(const TcParams &P, const Plan &pl, cudaStream_t s)
 {
-    auto kern = conv_ws_kernel<MODE>;
+    const bool two = MODE == kSearch && pl.tmem_cols <= 256;
+    auto kern = two ? search_ws_kernel : conv_ws_kernel<MODE>;
+    const int threads = two ? kSearchThreads : kWsThreads;
     SPK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(pl.smem)));
+    SPK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
     int per_sm = 1;
-    SPK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, ws_threads(MODE), pl.smem));
+    SPK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, pl.smem));
+    // the two-CTA search kernel is sized for two per SM (its registers, shared
+    // memory and tensor memory were chosen for it); the runtime's estimate
+    // can fall short of what the hardware places
+    if (two) per_sm = std::max(per_sm, 2);
     per_sm = std::max(1, std::min<int>(per_sm, int(512 / pl.tmem_cols)));
     if (g_schedule.ctas > 0) per_sm = std::min(per_sm, g_schedule.ctas);
     const int64_t grid = std::min<int64_t>(P.tiles, int64_t(sm_count()) * per_sm);
-    kern<<<unsigned(grid), ws_threads(MODE), pl.smem, s>>>(P);
+    kern<<<unsigned(grid), threads, pl.smem, s>>>(P);
     SPK_LAUNCHED();
 }
 
@@ -2765,7 +2769,8 @@ FusedLayout fused_layout(int64_t b, int64_t t, int64_t cin, int64_t h, int64_t w
     if (L.pl4.nsplit * L.pl4.n_tile > 512 || L.pl4.stages < 2)
         L.pl4 = make_plan(b * t, cin, h, w, cout, kh, kw, precision, true, t, false, kSearchTermsMin);
     L.search_ok = nnets == 1 && t <= 127 && L.pl4.n_tiles == 1 && L.pl4.nsplit * L.pl4.n_tile <= 512 &&
-                  L.pl4.stages >= 2 && L.pl4.smem <= 227 * 1024 && L.pl4.kblocks <= kMaxKBlocks;
+                  L.pl4.stages >= 2 && L.pl4.smem <= 227 * 1024 && L.pl4.kblocks <= kMaxKBlocks &&
+                  L.pl.xt_bytes < (size_t(1) << 31) && h < 30000 && w < 30000;
     if (L.search_ok)
     {
         const size_t np = size_t(L.npix);
