@@ -51,10 +51,10 @@ def bf16_peak():
     return 1400.0, "sustained cuBLAS BF16 of an earlier measurement on this pool (of fallback)"
 
 
-def headline_config(batch: int, world: int) -> dict:
+def headline_config(batch: int, world: int, mode: str = "replicas") -> dict:
     """The workload's `config`, shared by both arms of the bench."""
     return {"workload": WORKLOAD.replace("4096 x", f"{batch} x"), "global_batch": batch * world, "seq_len": T,
-            "parallelism": f"replicas{world}",
+            "parallelism": f"{mode}{world}",
             "l2": "inputs larger than L2: each step writes its own 1.44 GB layer-1 spike tensor (126 MB L2)"}
 
 
@@ -126,6 +126,9 @@ class Network:
         # 1 run (joined before the next layer 2, and by finish())
         self.side = torch.cuda.Stream(dev)
         self.side2 = torch.cuda.Stream(dev)
+        # the STDP update of a layer: this rank's batch alone, or (data
+        # parallel) the whole batch over the ranks
+        self.stdp_fn = lambda layer, x, win, spk: layer.stdp(x, win, spk)
 
     def _conv(self, layer, x):
         t = self.torch
@@ -140,8 +143,10 @@ class Network:
         """conv -> threshold -> inhibit -> (fire, convwta) -> pool: one fused
         kernel on the tensor-core precisions, op by op on the FP32 path."""
         t = self.torch
+        timed = not t.cuda.is_current_stream_capturing()  # no timing events inside a CUDA graph
         a, b = t.cuda.Event(enable_timing=True), t.cuda.Event(enable_timing=True)
-        a.record()
+        if timed:
+            a.record()
         if getattr(self, "probe", None):
             self.probe()
         if layer.precision == "fp32":
@@ -150,8 +155,9 @@ class Network:
             pooled = self.sp.pool(spk, pool)
         else:
             spk, wins, pooled = self.sp.conv_fire_wta(x, layer, theta, radius, count, pool=pool)
-        b.record()
-        self.conv_events.append((a, b, layer))
+        if timed:
+            b.record()
+            self.conv_events.append((a, b, layer))
         if getattr(self, "probe", None):
             self.probe()
         return spk, wins, pooled
@@ -163,14 +169,15 @@ class Network:
         main = self.torch.cuda.current_stream()
         self.side.wait_stream(main)
         with self.torch.cuda.stream(self.side):
-            self.conv1.stdp(codes, win1, spk1)
+            self.stdp_fn(self.conv1, codes, win1, spk1)
         main.wait_stream(self.side2)  # the previous step's layer-2 update
         spk2, win2, feats = self._layer(self.conv2, pooled, 10.0, 1, 8, 14)
         self.side2.wait_stream(main)
         with self.torch.cuda.stream(self.side2):
-            self.conv2.stdp(pooled, win2, spk2)
-        for x in (pooled, spk2, win2.records, win2.counts):
-            x.record_stream(self.side2)  # not reused before the update has read them
+            self.stdp_fn(self.conv2, pooled, win2, spk2)
+        if not self.torch.cuda.is_current_stream_capturing():
+            for x in (pooled, spk2, win2.records, win2.counts):
+                x.record_stream(self.side2)  # not reused before the update has read them
         # the next step's layer 1 reads the updated conv1 weights; this
         # step's layer-1 tensors are freed after the join
         main.wait_stream(self.side)
@@ -202,6 +209,15 @@ def gpu_arm(args, rank, world):
     host = torch.from_numpy(imgs).pin_memory()
     dev_imgs = host.to(dev).float().div_(255.0)[:, None]
     net = Network(spyker, torch, dev, args.precision)
+    if args.mode == "dp":
+        # one network over the ranks: each rank's 4096 images are its shard
+        # of a BATCH * world batch; the winners' (pre, post) times of all
+        # ranks are gathered (one all-gather per layer) and every rank applies
+        # the ordered update of the whole batch
+        from spyker_b200 import replicas
+
+        net.stdp_fn = lambda layer, x, win, spk: replicas.conv_stdp(layer, x, win, spk, batch=BATCH * world)
+        args.graph = False  # collectives stay outside the captured graph
 
     def barrier():
         if dist is not None:
@@ -231,20 +247,56 @@ def gpu_arm(args, rank, world):
                            "recomputes": [rec[1][1], rec[3][1]], "conv_ms": [c1, c2]})
     barrier()
     net.conv_events.clear()
-    l0 = spyker._lib.lib.spk_launch_count()
+    # The step as one CUDA graph: images from a u8 device buffer (the e2e leg
+    # copies each step's images into it) to the features, both layers' STDP
+    # updates included, captured once and replayed; launch gaps and host work
+    # leave the step.
+    static_u8 = torch.from_numpy(imgs).to(dev)
+    graph = None
+    if args.graph:
+        def gstep():
+            # both side streams fork from the capturing stream first, so that
+            # every wait of the step refers to captured work
+            cur = torch.cuda.current_stream()
+            net.side.wait_stream(cur)
+            net.side2.wait_stream(cur)
+            f = net.step(static_u8.float().div_(255.0)[:, None])
+            net.finish()
+            return f
+        gstep()
+        barrier()
+        graph = torch.cuda.CUDAGraph()
+        l0 = spyker._lib.lib.spk_launch_count()
+        with torch.cuda.graph(graph):
+            feats_g = gstep()
+        launches = spyker._lib.lib.spk_launch_count() - l0
+        graph.replay()
+        barrier()
+    else:
+        l0 = spyker._lib.lib.spk_launch_count()
     spyker._lib.lib.spk_recheck_count(1)
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with Clocks(dev.index) as clk:
         barrier()
         start.record()
         for _ in range(args.steps):
-            net.step(dev_imgs)
+            if graph is not None:
+                graph.replay()
+            else:
+                net.step(dev_imgs)
         net.finish()
         end.record()
         barrier()
-    launches = (spyker._lib.lib.spk_launch_count() - l0) // max(args.steps, 1)
+    if graph is None:
+        launches = (spyker._lib.lib.spk_launch_count() - l0) // max(args.steps, 1)
     rechecks = spyker._lib.lib.spk_recheck_count(1) / max(args.steps, 1)
     ms = start.elapsed_time(end) / args.steps
+    if graph is not None:
+        # per-layer times from two eager steps (timing events cannot sit in a graph)
+        for _ in range(2):
+            net.step(dev_imgs)
+        net.finish()
+        barrier()
     # fired neurons of one step: a cumulative spike tensor's last step
     spikes_per_step = sum(int(s[:, -1].sum().item()) for s in net.last_spikes)
     conv_ms = {}
@@ -260,17 +312,30 @@ def gpu_arm(args, rank, world):
     # (io.Readback, two host buffers in turn); the timed region starts before
     # the first upload and ends after the last read-back has landed.
     net.step(dev_imgs)
-    uploads = io.Prefetcher([host] * args.steps, device=dev, depth=2)
     back = io.Readback(depth=2, device=dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    barrier()
-    e0.record()
-    for raw in uploads:
-        feats = back.push(net.step(raw.float().div_(255.0)[:, None]))
-    net.finish()
-    back.wait()
-    e1.record()
-    barrier()
+    if graph is not None:
+        # each step: pinned host images -> the graph's input buffer, replay,
+        # features read back on a side stream (two host buffers in turn)
+        barrier()
+        e0.record()
+        for _ in range(args.steps):
+            static_u8.copy_(host, non_blocking=True)
+            graph.replay()
+            feats = back.push(feats_g)
+        back.wait()
+        e1.record()
+        barrier()
+    else:
+        uploads = io.Prefetcher([host] * args.steps, device=dev, depth=2)
+        barrier()
+        e0.record()
+        for raw in uploads:
+            feats = back.push(net.step(raw.float().div_(255.0)[:, None]))
+        net.finish()
+        back.wait()
+        e1.record()
+        barrier()
     e2e_ms = e0.elapsed_time(e1) / args.steps
 
     # the same step on the plain FP32 path (the comparison the metric names)
@@ -312,11 +377,12 @@ def gpu_arm(args, rank, world):
         "vs_baseline": None,
         "dtype": {"fp32": "f32", "bf16x2": "bf16x2-split/f32-acc", "bf16x3": "bf16x3-split/f32-acc"}[args.precision],
         "data": "synthetic (seeded stroke images, MNIST geometry)",
-        "config": headline_config(BATCH, world),
+        "config": headline_config(BATCH, world, args.mode),
         "conv_precision": args.precision,
         "e2e": {"value": BATCH * world / (e2e_ms * 1e-3), "unit": "images/s", "h2d_bytes_per_step": BATCH * H * H,
                 "d2h_bytes_per_step": int(feats.numel() * feats.element_size())},
         "gpu_launches": int(launches),
+        "cuda_graph": graph is not None,
         "roofline": {"bound": "tensor", "kernel": "conv2 (30->100, 5x5, M=12.0M, K=750)", "achieved": achieved,
                      "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                      "traffic": CONV2_TRAFFIC_BYTES * BATCH // 4096 if args.precision != "fp32" else None,
@@ -458,7 +524,7 @@ def reference_arm(args, rank, world):
         "impl": "reference", "metric": METRIC, "value": v, "unit": "images/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded stroke images, MNIST geometry)",
-        "config": headline_config(args.batch, world),
+        "config": headline_config(args.batch, world, args.mode),
         "cpu_baseline": {"value": v, "unit": "images/s", "cores": torch.get_num_threads(), "kind": kind,
                          "sample": f"{sample} of each step's {args.batch} images per timed step (the CPU path's "
                                    f"cost is per image), reference CPU backend + oneDNN convolution via torch"},
@@ -972,6 +1038,11 @@ def main():
     ap.add_argument("--trajectory", type=int, default=0,
                     help="after the warm-up, this many synchronised steps recording each layer's exact re-decisions")
     ap.add_argument("--dump-weights", default="", help="save the trained kernels to this .npz")
+    ap.add_argument("--mode", default="replicas", choices=["replicas", "dp"],
+                    help="several GPUs: independent networks (replicas, the default) or one network trained data "
+                         "parallel (dp: one all-gather of the winners per layer and step)")
+    ap.add_argument("--no-graph", dest="graph", action="store_false",
+                    help="run the headline step eagerly instead of as a captured CUDA graph")
     ap.add_argument("--workload", default="kheradpisheh", choices=["kheradpisheh", "gabor256", "backprop", "sweep", "sparse", "rstdp"],
                     help="kheradpisheh: the 2-layer STDP training step (the headline); gabor256: large-image "
                          "forward; backprop: temporal-backprop training of a 3-layer first-spike network; "

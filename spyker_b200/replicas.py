@@ -62,6 +62,50 @@ def gather_rows(t: torch.Tensor, group: Optional[dist.ProcessGroup] = None) -> t
     return out.view(t.dtype).reshape((sum(sizes),) + tuple(t.shape[1:]))
 
 
+def gather_packed(parts, rows_per_rank, group: Optional[dist.ProcessGroup] = None):
+    """Rank-ordered concatenation of several per-sample tensors in ONE
+    all-gather and without a host synchronisation: ``parts`` are this rank's
+    tensors (same first dimension, any dtypes), ``rows_per_rank`` the first
+    dimension of every rank (known from the shard arithmetic, e.g.
+    :func:`shard`).  Each sample's rows of all parts travel as one byte row;
+    shards shorter than the longest are padded.  Returns the gathered tensors
+    in the order of ``parts``."""
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    if len(rows_per_rank) != world:
+        raise ValueError("rows_per_rank must give every rank's rows")
+    if world == 1:
+        return [p for p in parts]
+    n = int(rows_per_rank[rank])
+    dev = parts[0].device
+    widths, flats = [], []
+    for p in parts:
+        if p.shape[0] != n:
+            raise ValueError("every part must have this rank's rows")
+        f = p.contiguous().reshape(n, -1).view(torch.uint8) if p.numel() else torch.empty((n, 0), dtype=torch.uint8,
+                                                                                              device=dev)
+        flats.append(f)
+        widths.append(f.shape[1])
+    most = max(int(r) for r in rows_per_rank)
+    row = sum(widths)
+    buf = torch.zeros((most, row), dtype=torch.uint8, device=dev)
+    col = 0
+    for f, w in zip(flats, widths):
+        buf[:n, col:col + w] = f
+        col += w
+    out = torch.empty((world * most, row), dtype=torch.uint8, device=dev)
+    dist.all_gather_into_tensor(out, buf, group=group)
+    keep = torch.cat([torch.arange(q * most, q * most + int(r), device=dev) for q, r in enumerate(rows_per_rank)])
+    rows = out.index_select(0, keep)
+    total = int(sum(int(r) for r in rows_per_rank))
+    res, col = [], 0
+    for p, w in zip(parts, widths):
+        piece = rows[:, col:col + w].contiguous()
+        col += w
+        res.append(piece.view(p.dtype).reshape((total,) + tuple(p.shape[1:])))
+    return res
+
+
 def max_over_ranks(x: float, group: Optional[dist.ProcessGroup] = None, device=None) -> float:
     """The largest ``x`` over the ranks (step times are reported this way)."""
     if not dist.is_initialized() or dist.get_world_size(group) == 1:
@@ -72,11 +116,14 @@ def max_over_ranks(x: float, group: Optional[dist.ProcessGroup] = None, device=N
 
 
 def conv_stdp(layer, array: torch.Tensor, winners, output: torch.Tensor,
-              group: Optional[dist.ProcessGroup] = None) -> None:
+              group: Optional[dist.ProcessGroup] = None, batch: Optional[int] = None) -> None:
     """``layer.stdp(array, winners, output)`` for the whole batch split over
     the ranks: ``array``, ``output`` and ``winners`` are this rank's shard
     (consecutive images, shards in rank order); every rank's ``layer.kernel``
-    receives the update of the full batch."""
+    receives the update of the full batch.  With ``batch`` (the full batch,
+    sharded by :func:`shard`) the winners and (pre, post) times of all ranks
+    travel in one all-gather with no host synchronisation; without it the
+    shard sizes are gathered first."""
     from .module import Winners, _check_winners, _configs
     from .utils import Bound, to5
 
@@ -96,7 +143,11 @@ def conv_stdp(layer, array: torch.Tensor, winners, output: torch.Tensor,
     call("spk_rank_convstdp_prepost", ptr(x), _code(x.dtype), s[0], s[1], cin, s[3], s[4], cout, kh, kw, ptr(o), so[3],
          so[4], ptr(w.records), ptr(w.counts), w.count, layer._stride[0], layer._stride[1], i64(*layer._pad), ptr(pre),
          ptr(post), ptr(ws), int(nb), stream())
-    if dist.is_initialized():
+    if dist.is_initialized() and batch is not None:
+        world = dist.get_world_size(group)
+        sizes = [len(range(batch)[shard(batch, r, world)]) for r in range(world)]
+        records, counts, pre, post = gather_packed([w.records, w.counts, pre, post], sizes, group)
+    elif dist.is_initialized():
         records, counts = gather_rows(w.records, group), gather_rows(w.counts, group)
         pre, post = gather_rows(pre, group), gather_rows(post, group)
     else:

@@ -107,3 +107,30 @@ def _stdp_worker(rank, world, port, root):
 def test_stdp_winners_gathered_in_order(port):
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     mp.spawn(_stdp_worker, args=(2, _free_port(), root), nprocs=2, join=True)
+
+
+def _packed_worker(rank, world, port):
+    """The winners' records (int32) and (pre, post) first-spike times (int16)
+    of unequal shards travel in one all-gather and come back bit for bit in
+    rank order."""
+    _init(rank, world, port)
+    try:
+        batch = 7
+        sizes = [len(range(batch)[replicas.shard(batch, r, world)]) for r in range(world)]
+        g = torch.Generator().manual_seed(5)
+        full_rec = torch.randint(-2 ** 31, 2 ** 31 - 1, (batch, 3, 5), dtype=torch.int32, generator=g)
+        full_cnt = torch.randint(0, 4, (batch,), dtype=torch.int32, generator=g)
+        full_pre = torch.randint(-2 ** 15, 2 ** 15 - 1, (batch, 3, 50), dtype=torch.int16, generator=g)
+        full_post = torch.randint(0, 16, (batch, 3), dtype=torch.int16, generator=g)
+        sl = replicas.shard(batch, rank, world)
+        got = replicas.gather_packed([full_rec[sl], full_cnt[sl], full_pre[sl], full_post[sl]], sizes)
+        for a, b in zip(got, (full_rec, full_cnt, full_pre, full_post)):
+            assert a.dtype == b.dtype and a.shape == b.shape and torch.equal(a, b)
+        with pytest.raises(ValueError):
+            replicas.gather_packed([full_rec[sl]], sizes[:1])
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gather_packed_int16_two_ranks():
+    mp.spawn(_packed_worker, args=(2, _free_port()), nprocs=2, join=True)
