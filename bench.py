@@ -1041,8 +1041,9 @@ def main():
     ap.add_argument("--mode", default="replicas", choices=["replicas", "dp"],
                     help="several GPUs: independent networks (replicas, the default) or one network trained data "
                          "parallel (dp: one all-gather of the winners per layer and step)")
-    ap.add_argument("--no-graph", dest="graph", action="store_false",
-                    help="run the headline step eagerly instead of as a captured CUDA graph")
+    ap.add_argument("--graph", action="store_true",
+                    help="run the headline step as one captured CUDA graph (measured at the eager step's time: "
+                         "the kernels dominate and the eager queue already hides the launches)")
     ap.add_argument("--workload", default="kheradpisheh", choices=["kheradpisheh", "gabor256", "backprop", "sweep", "sparse", "rstdp"],
                     help="kheradpisheh: the 2-layer STDP training step (the headline); gabor256: large-image "
                          "forward; backprop: temporal-backprop training of a 3-layer first-spike network; "

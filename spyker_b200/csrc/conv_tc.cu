@@ -105,6 +105,7 @@ struct TcParams
     int *val_count;
     int4 *state;     // per pixel: (lo | hi << 8 | winner << 16, value, winner at T-1, value at T-1)
     const float *echan;     // per channel bound of |oracle potential - exact term sum|
+    const float *cscale;    // per channel 2^(e - 32): the value of one unit of the term total
     const unsigned *sinfo;  // [0] largest echan (bits), [1] largest channel exponent + 128
     int kreal;              // real K (taps x input channels)
     int r0_list;            // round 0 takes the (pixel, T - 1) entries of list_in (bound pre-filter ran)
@@ -116,10 +117,8 @@ struct TcParams
 // kTimes: the fused (pixel, time) rows with an epilogue that writes each
 // neuron's first step above threshold (F32 time, T = never).
 constexpr int kPotentials = 0, kFused = 1, kTimes = 2, kSearch = 3;
-// Terms of the fixed-grid weight split of the search kernels: four where
-// their accumulators fit the tensor memory (weights down to 2^-9 of their
-// channel's largest exact), else three.
-constexpr int kSearchTermsMax = 4, kSearchTermsMin = 3;
+// Base-256 digits per weight of the search kernels' 8-bit split.
+constexpr int kSearchTerms = 4;
 
 __device__ __forceinline__ unsigned order_enc(float f)
 {
@@ -997,53 +996,38 @@ __device__ __forceinline__ void s_chunk_wait(uint32_t (&q)[NS][kEpiChunk])
     for (int j = 0; j < NS; ++j) tmem_ld_wait8(q[j]);
 }
 
+// Exact term total of a column: the NS 32-bit accumulators hold sums of
+// base-256 digit products, so the total is an integer below 2^46.
 template <int NS>
-__device__ __forceinline__ float s_fast(const uint32_t (&q)[NS][kEpiChunk], int j)
+__device__ __forceinline__ uint64_t s_total(const uint32_t (&q)[NS][kEpiChunk], int j)
 {
-    float f = __fadd_rn(__uint_as_float(q[0][j]), __uint_as_float(q[1][j]));
+    uint64_t r = 0;
 #pragma unroll
-    for (int i = 2; i < NS; ++i) f = __fadd_rn(f, __uint_as_float(q[i][j]));
-    return f;
+    for (int i = 0; i < NS; ++i) r = (r << 8) + uint64_t(q[i][j]);
+    return r;
 }
 
-// The exact sum of the terms (every term sum is a multiple of its grid and the
-// total spans at most 42 bits, so the FP64 additions are exact).
-template <int NS>
-__device__ __forceinline__ double s_exact(const uint32_t (&q)[NS][kEpiChunk], int j)
-{
-    double d = double(__uint_as_float(q[0][j]));
-#pragma unroll
-    for (int i = 1; i < NS; ++i) d += double(__uint_as_float(q[i][j]));
-    return d;
-}
-
-// Rounding of an exact sum S to P = float(S): lo / hi are the smallest and
-// largest float a value within E of S rounds to (ties at a boundary count
-// as both sides).
+// The floats a potential within E of the exact S (= R * scale) can round to:
+// [lo, hi] = [RN(S - E), RN(S + E)] (RN is monotone); lo == hi: P is the
+// oracle's value.  E == 0: the term total is the oracle's FP64 sum itself.
 __device__ __forceinline__ void s_round(double S, float E, float &P, float &lo, float &hi)
 {
     P = float(S);
     if (E == 0.f)
     {
-        // the term total is the oracle's FP64 sum itself
         lo = hi = P;
         return;
     }
-    const double rho = S - double(P);
-    const double up = (double(nextafterf(P, INFINITY)) - double(P)) * 0.5;
-    const double dn = (double(P) - double(nextafterf(P, -INFINITY))) * 0.5;
-    hi = (rho + double(E) < up) ? P : nextafterf(P, INFINITY);
-    lo = (double(E) - rho < dn) ? P : nextafterf(P, -INFINITY);
+    lo = float(__dsub_rd(S, double(E)));
+    hi = float(__dadd_ru(S, double(E)));
 }
 
-// Exact term sum of column `col` of this lane's row (col < 0: none), the
+// Exact term total of column `col` of this lane's row (col < 0: none), the
 // warp's columns fetched one 8-column chunk at a time.  Warp-uniform.
 template <int NS>
-__device__ __forceinline__ double s_reload(uint32_t lane_base, int n_tile, int col)
+__device__ __forceinline__ uint64_t s_reload(uint32_t lane_base, int n_tile, int col)
 {
-    uint32_t pick[NS];
-#pragma unroll
-    for (int i = 0; i < NS; ++i) pick[i] = 0u;
+    uint64_t R = 0;
     unsigned pending = __ballot_sync(0xffffffffu, col >= 0);
     while (pending)
     {
@@ -1054,21 +1038,17 @@ __device__ __forceinline__ double s_reload(uint32_t lane_base, int n_tile, int c
         const bool mine = col >= 0 && (col >> 3) == (c0 >> 3);
         const int jj = col - c0;
 #pragma unroll
-        for (int j = 0; j < kEpiChunk; ++j)
-#pragma unroll
-            for (int i = 0; i < NS; ++i) pick[i] = (mine && jj == j) ? q[i][j] : pick[i];
+        for (int j = 0; j < kEpiChunk; ++j) R = (mine && jj == j) ? s_total<NS>(q, j) : R;
         pending &= ~__ballot_sync(0xffffffffu, mine);
     }
-    double S = double(__uint_as_float(pick[0]));
-#pragma unroll
-    for (int i = 1; i < NS; ++i) S += double(__uint_as_float(pick[i]));
-    return S;
+    return R;
 }
 
-// Tier 2: every channel of the row from its exact sum.  dec: 0 open, 1 no
+// Tier 2: every channel of the row from its exact total.  dec: 0 open, 1 no
 // channel above thr, 2 crossing with winner a (first of the largest) of value v.
 template <int NS>
-__device__ __forceinline__ void s_tier2(const TcParams &P, uint32_t lane_base, float thr, int &dec, int &a, float &v)
+__device__ __forceinline__ void s_tier2(const TcParams &P, uint32_t lane_base, float thr, int &dec, int &a, float &v,
+                                        const float *scale, const float *bound)
 {
     float mlo = -INFINITY, hmax = -INFINITY, hun = -INFINITY, vs = -INFINITY;
     int as = -1;
@@ -1083,7 +1063,8 @@ __device__ __forceinline__ void s_tier2(const TcParams &P, uint32_t lane_base, f
             const int c = c0 + j;
             const bool real = c < P.cout;
             float pc, lo, hi;
-            s_round(s_exact<NS>(q, j), real ? __ldg(P.echan + c) : 0.f, pc, lo, hi);
+            const double S = double(s_total<NS>(q, j)) * double(real ? scale[c] : 0.f);
+            s_round(S, real ? bound[c] : 0.f, pc, lo, hi);
             if (!real) lo = hi = pc = -INFINITY;
             mlo = fmaxf(mlo, lo);
             hmax = fmaxf(hmax, hi);
@@ -1103,6 +1084,14 @@ __device__ __forceinline__ void s_tier2(const TcParams &P, uint32_t lane_base, f
     }
     else if (hmax <= thr)
         dec = 1;
+}
+
+// The largest float any channel of value P (its exact total within the
+// rounding cell of P) can round to when the oracle's sum is within E of it.
+__device__ __forceinline__ float s_upper(float P, float E)
+{
+    const double up = double(P) + 0.5 * (double(nextafterf(P, INFINITY)) - double(P));
+    return float(__dadd_ru(up, double(E)));
 }
 
 // What a decided row does to its pixel (shared by the epilogue and the exact
@@ -1181,11 +1170,16 @@ __device__ __forceinline__ void s_extremes(const TcParams &P, int pix, const Sea
     }
 }
 
-// Search epilogue of one row per thread (warps 0-3).  `c0` is the per-launch
-// part of the tier-1 bound.
+// Search epilogue of one row per thread (warps 0-3).  `emax` is the largest
+// channel bound.  Tier 1 scans the row: each channel's exact total R, its
+// float P = RN(R) * 2^(e - 32) (exact scaling by the channel's power of two),
+// the three largest (first index first).  The winner's value and, when the
+// runner-up is within two ulps, the runner-up's, are certified against their
+// channel bounds; nothing else can change a decision unless the third value
+// comes that close too.
 template <int NS>
 __device__ void search_epilogue(const TcParams &P, uint32_t acc, bool ok, int pix, int t, int aux, int4 pstate,
-                                uint64_t *release, float c0)
+                                uint64_t *release, float emax, const float *scale, const float *bound)
 {
     const int warp = threadIdx.x >> 5;
     const uint32_t lane_base = acc + (uint32_t((warp & 3) * 32) << 16);
@@ -1194,26 +1188,22 @@ __device__ void search_epilogue(const TcParams &P, uint32_t acc, bool ok, int pi
     float v = 0.f;
     if (P.round == 2)
     {
-        const double S = s_reload<NS>(lane_base, P.n_tile, ok ? aux : -1);
+        const uint64_t R = s_reload<NS>(lane_base, P.n_tile, ok ? aux : -1);
         tc_fence_before();
         mbar_arrive(release);
         if (ok)
         {
             float lo, hi;
-            s_round(S, __ldg(P.echan + aux), v, lo, hi);
+            s_round(double(R) * double(scale[aux]), bound[aux], v, lo, hi);
             dec = lo == hi ? 2 : 3;
             a = aux;
         }
     }
     else
     {
-        // tier 1: the largest potential (first index), its runner-up, and the
-        // term sums of the largest; one 8-column chunk at a time (a second
-        // CTA on the SM hides the load latency)
-        LeanMax st;
-        uint32_t wb[NS];
-#pragma unroll
-        for (int i = 0; i < NS; ++i) wb[i] = 0u;
+        float p1 = -INFINITY, p2 = -INFINITY, p3 = -INFINITY;
+        int a1 = -1, a2 = -1;
+        uint64_t r1 = 0, r2 = 0;
         for (int cb = 0; cb < P.n_tile; cb += kEpiChunk)
         {
             uint32_t q[NS][kEpiChunk];
@@ -1223,37 +1213,50 @@ __device__ void search_epilogue(const TcParams &P, uint32_t acc, bool ok, int pi
 #pragma unroll
             for (int j = 0; j < kEpiChunk; ++j)
             {
-                const float f = j < lim ? s_fast<NS>(q, j) : -INFINITY;
-                const bool gt = f > st.r1;
-                st.r2 = gt ? st.r1 : fmaxf(st.r2, f);
-                st.r1 = gt ? f : st.r1;
-                st.a1 = gt ? cb + j : st.a1;
-#pragma unroll
-                for (int i = 0; i < NS; ++i) wb[i] = gt ? q[i][j] : wb[i];
+                const uint64_t R = s_total<NS>(q, j);
+                const float pv = j < lim ? __ll2float_rn((long long)R) * scale[cb + j] : -INFINITY;
+                const bool g1 = pv > p1, g2 = !g1 && pv > p2, g3 = !g1 && !g2 && pv > p3;
+                p3 = g1 || g2 ? p2 : (g3 ? pv : p3);
+                p2 = g1 ? p1 : (g2 ? pv : p2);
+                a2 = g1 ? a1 : (g2 ? cb + j : a2);
+                r2 = g1 ? r1 : (g2 ? R : r2);
+                p1 = g1 ? pv : p1;
+                a1 = g1 ? cb + j : a1;
+                r1 = g1 ? R : r1;
             }
         }
-        const float tol1 = __fmaf_ru(fabsf(st.r1), 0x1.9p-23f, c0);
-        int d1 = 0;  // tier-1 decision
-        if (__fadd_ru(st.r1, tol1) <= thr)
-            d1 = 1;
-        else if (__fsub_rd(st.r1, tol1) >= nextafterf(thr, INFINITY))
+        int d1 = 0;  // tier-1 decision: 0 open, 1 below, 2 winner decided (value certified or not)
+        bool vexact = false;
+        if (ok)
         {
-            const float tol2 = __fmaf_ru(fabsf(st.r2), 0x1.9p-23f, c0);
-            const float gap = __fsub_rd(__fsub_rd(st.r1, tol1), __fadd_ru(st.r2, tol2));
-            if (gap > __fmaf_ru(fabsf(st.r1), 0x1p-23f, 0x1p-126f)) d1 = 2;
+            if (s_upper(p1, emax) <= thr)
+                d1 = 1;  // no channel's value can round above the threshold
+            else
+            {
+                float pa, lo1, hi1;
+                s_round(double(r1) * double(scale[a1]), bound[a1], pa, lo1, hi1);
+                const float near = nextafterf(nextafterf(p1, -INFINITY), -INFINITY);
+                if (lo1 > thr && !(p3 >= near && s_upper(p3, emax) >= lo1))
+                {
+                    bool win = true;
+                    if (p2 >= near && s_upper(p2, emax) >= lo1)
+                    {
+                        float pb, lo2, hi2;
+                        s_round(double(r2) * double(scale[a2]), bound[a2], pb, lo2, hi2);
+                        // both exact: the larger wins, ties to the lower index (a1)
+                        win = lo1 > hi2 || (lo1 == hi1 && lo2 == hi2 && pa >= pb);
+                    }
+                    if (win) d1 = 2, vexact = lo1 == hi1, v = pa;
+                }
+            }
         }
-        // the winner's exact value for tier-1 crossings (its terms were kept
-        // in the scan); tier 2 for the rest
-        double S = double(__uint_as_float(wb[0]));
-#pragma unroll
-        for (int i = 1; i < NS; ++i) S += double(__uint_as_float(wb[i]));
-        int d2 = 0, a2 = -1;
+        int d2 = 0, a2t = -1;
         float v2 = 0.f;
         const unsigned open1 = __ballot_sync(0xffffffffu, ok && d1 == 0);
         if (open1)
         {
             if ((threadIdx.x & 31) == 0) atomicAdd(&g_rechecks, (unsigned long long)__popc(open1));
-            s_tier2<NS>(P, lane_base, thr, d2, a2, v2);
+            s_tier2<NS>(P, lane_base, thr, d2, a2t, v2, scale, bound);
         }
         tc_fence_before();
         mbar_arrive(release);
@@ -1262,14 +1265,9 @@ __device__ void search_epilogue(const TcParams &P, uint32_t acc, bool ok, int pi
             if (d1 == 1)
                 dec = 1;
             else if (d1 == 2)
-            {
-                float lo, hi;
-                s_round(S, __ldg(P.echan + st.a1), v, lo, hi);
-                a = st.a1;
-                dec = lo == hi ? 2 : 3;
-            }
+                a = a1, dec = vexact ? 2 : 3;
             else
-                dec = d2, a = a2, v = v2;
+                dec = d2, a = a2t, v = v2;
         }
     }
     // dec 3: the winner a is decided, its value is left to the exact sum
@@ -1300,10 +1298,6 @@ __device__ void search_epilogue(const TcParams &P, uint32_t acc, bool ok, int pi
     if (ok && P.wta) s_extremes(P, pix, r);
 }
 
-// Search producers: thread p (0..255) builds four (row, 8-wide K chunk)
-// units of every K block, one row each at that row's own step; the 8 lanes
-// of a quarter warp take 8 consecutive rows of one chunk (distinct 16-byte
-// bank groups).
 __device__ __forceinline__ int2 search_entry(const TcParams &P, int64_t idx)
 {
     if (P.round == 0 && !P.r0_list) return make_int2(int(idx), P.T - 1);
@@ -1328,39 +1322,33 @@ __device__ __forceinline__ FusedPixel pixel_of(const TcParams &P, bool ok, int g
 
 // A search row's pixel in three words: byte offset of its sample's
 // first-spike map (-1: no row), receptive-field origin (iy0, ix0) packed as
-// two 16-bit fields, and its step.
-__device__ __forceinline__ uint2 fst_chunk_c(const TcParams &P, const int4 *tab, int base, int yx, int kb, int kc)
+// two 16-bit fields, and its step.  The search operands are 8-bit and
+// channels-last: a 16-byte chunk of a row is two 8-channel groups, each one
+// 8-byte load of the first-spike map (0xFF: outside the input).
+__device__ __forceinline__ uint2 fst_group(const TcParams &P, const int4 *tab, int base, int yx, int g)
 {
     if (base < 0) return make_uint2(~0u, ~0u);
     const int iy0 = int(uint32_t(yx) >> 16) - 32768, ix0 = int(uint32_t(yx) & 0xFFFFu) - 32768;
-    const uint8_t *img = P.in + base;
-    if (P.nhwc)
-    {
-        const int4 e = tab[ftab(P.kblocks, kb, kc, 0)];
-        const int iy = iy0 + e.y, ix = ix0 + e.z;
-        if (e.w && iy >= 0 && iy < P.h && ix >= 0 && ix < P.w)
-            return *reinterpret_cast<const uint2 *>(img + (iy * P.w + ix) * P.cpad + e.x);
-        return make_uint2(~0u, ~0u);
-    }
-    uint32_t w[2] = {0, 0};
-#pragma unroll
-    for (int i = 0; i < 8; ++i)
-    {
-        const int4 e = tab[ftab(P.kblocks, kb, kc, i)];
-        const int iy = iy0 + e.y, ix = ix0 + e.z;
-        uint32_t b = 0xFF;
-        if (e.w && iy >= 0 && iy < P.h && ix >= 0 && ix < P.w) b = img[(iy * P.w + ix) * P.cin + e.x];
-        w[i >> 2] |= b << (8 * (i & 3));
-    }
-    return make_uint2(w[0], w[1]);
+    const int4 e = tab[g];
+    const int iy = iy0 + e.y, ix = ix0 + e.z;
+    if (e.w && iy >= 0 && iy < P.h && ix >= 0 && ix < P.w)
+        return __ldg(reinterpret_cast<const uint2 *>(P.in + base + (iy * P.w + ix) * P.cpad + e.x));
+    return make_uint2(~0u, ~0u);
 }
 
-// Search producers: a thread builds NU (row, 8-wide K chunk) units of every K
-// block, one row each at that row's own step.  Unit i of thread p is row
-// (p & 7) + 8 (p >> 6) + (1024 / NU / 8) i and chunk (p >> 3) & 7, so the 8
-// lanes of a quarter warp take 8 consecutive rows of one chunk (distinct
-// 16-byte bank groups).  The gathers of a step are issued before the wait for
-// its stage, all NU in flight together.
+// Bytes 1 where the first-spike byte f <= t, else 0; tt = (t + 1) * 0x01010101
+// ((f | 0x80) - (t + 1) keeps bit 7 iff f > t, no borrow between bytes).
+__device__ __forceinline__ uint32_t spike_bytes(uint32_t f, uint32_t tt)
+{
+    return (~((f | 0x80808080u) - tt) >> 7) & 0x01010101u;
+}
+
+// Search producers: a thread builds NU (row, 16-byte chunk) units of every K
+// block (128 U8 elements), one row each at that row's own step.  Unit i of
+// thread p is row (p & 7) + 8 (p >> 6) + (1024 / NU / 8) i and chunk
+// (p >> 3) & 7, so the 8 lanes of a quarter warp take 8 consecutive rows of
+// one chunk (distinct 16-byte bank groups).  The gathers of a step are issued
+// before the wait for its stage, all in flight together.
 template <int NU>
 __device__ __forceinline__ void search_producer(const TcParams &P, const int4 *tab, unsigned char *smem,
                                                 uint64_t *full_bar, uint64_t *empty_bar, int S, int stage_bytes,
@@ -1372,12 +1360,13 @@ __device__ __forceinline__ void search_producer(const TcParams &P, const int4 *t
     uint32_t it = 0;
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
     {
-        int ubase[NU], uyx[NU], ut[NU];
+        int ubase[NU], uyx[NU];
+        uint32_t utt[NU];
 #pragma unroll
         for (int i = 0; i < NU; ++i)
         {
             const int64_t idx = tile * BM + row0 + RS * i;
-            ubase[i] = -1, uyx[i] = 0, ut[i] = 0;
+            ubase[i] = -1, uyx[i] = 0, utt[i] = 0x01010101u;
             if (idx < nrows)
             {
                 const int2 e = search_entry(P, idx);
@@ -1385,14 +1374,18 @@ __device__ __forceinline__ void search_producer(const TcParams &P, const int4 *t
                 const int oy = int(pix / uint32_t(P.ow)), ox = int(pix) - oy * P.ow;
                 ubase[i] = int(int64_t(smp) * P.img_stride);
                 uyx[i] = int((uint32_t(oy * P.sy - P.top + 32768) << 16) | uint32_t(ox * P.sx - P.left + 32768));
-                ut[i] = e.y;
+                utt[i] = uint32_t(e.y + 1) * 0x01010101u;
             }
         }
         for (int kb = 0; kb < P.kblocks; ++kb, ++it)
         {
-            uint2 f[NU];
+            uint2 fa[NU], fb[NU];
 #pragma unroll
-            for (int i = 0; i < NU; ++i) f[i] = fst_chunk_c(P, tab, ubase[i], uyx[i], kb, kc);
+            for (int i = 0; i < NU; ++i)
+            {
+                fa[i] = fst_group(P, tab, ubase[i], uyx[i], kb * 16 + 2 * kc);
+                fb[i] = fst_group(P, tab, ubase[i], uyx[i], kb * 16 + 2 * kc + 1);
+            }
             const int s = int(it % uint32_t(S));
             const uint32_t u = it / uint32_t(S);
             if (u > 0 && !wait_bounded(&empty_bar[s], (u - 1) & 1)) return;
@@ -1403,7 +1396,10 @@ __device__ __forceinline__ void search_producer(const TcParams &P, const int4 *t
                 bulk_g2s(sA + a_bytes, P.wimg + int64_t(kb) * b_bytes, uint32_t(b_bytes), &full_bar[s]);
             }
 #pragma unroll
-            for (int i = 0; i < NU; ++i) store_fst_rows(sA, row0 + RS * i, ut[i], 1, kc, f[i], 0);
+            for (int i = 0; i < NU; ++i)
+                *reinterpret_cast<uint4 *>(a_row_chunk(sA, row0 + RS * i, kc)) =
+                    make_uint4(spike_bytes(fa[i].x, utt[i]), spike_bytes(fa[i].y, utt[i]),
+                               spike_bytes(fb[i].x, utt[i]), spike_bytes(fb[i].y, utt[i]));
             fence_proxy_async_smem();
             mbar_arrive(&full_bar[s]);
         }
@@ -1457,7 +1453,20 @@ __device__ __forceinline__ void conv_ws_body(const TcParams &P)
     const int stage_bytes = a_bytes + b_bytes;
     int4 *tab = reinterpret_cast<int4 *>(smem + S * stage_bytes);
     const int taps = P.kh * P.kw;
-    if constexpr (MODE != kPotentials)
+    // search: the channels' scales and bounds, staged after the table
+    float *s_scale = reinterpret_cast<float *>(tab + P.kblocks * 16), *s_bound = s_scale + P.n_tile;
+    if constexpr (MODE == kSearch)
+    {
+        // per 8-element group of a 128-element K block (channels-last, 8-bit
+        // operands): (first channel, ky, kx, valid)
+        for (int g = tid; g < P.kblocks * 16; g += blockDim.x)
+        {
+            const int k = g * 8, tap = k / P.cpad, c = k % P.cpad;
+            tab[g] = make_int4(c, tap / P.kw, tap % P.kw, (tap < taps && c < P.cin) ? 1 : 0);
+        }
+        for (int c = tid; c < P.n_tile; c += blockDim.x) s_scale[c] = P.cscale[c], s_bound[c] = P.echan[c];
+    }
+    else if constexpr (MODE != kPotentials)
     {
         // per K element: (channel, ky, kx, valid) in the weight image's order
         for (int k = tid; k < P.kblocks * BK; k += blockDim.x)
@@ -1611,13 +1620,18 @@ __device__ __forceinline__ void conv_ws_body(const TcParams &P)
                     for (int c = 0; c < ncols; c += 256)
                     {
                         const int n = ncols - c < 256 ? ncols - c : 256;
-                        const uint32_t idesc = idesc_bf16_f32(BM, n);
+                        // the same 32-byte steps of each 128-byte row: 16
+                        // BF16 or (search) 32 U8 elements per instruction
+                        const uint32_t idesc = MODE == kSearch ? idesc_u8_s32(BM, n) : idesc_bf16_f32(BM, n);
 #pragma unroll
                         for (int k16 = 0; k16 < BK / 16; ++k16)
                         {
                             const uint64_t ad = smem_desc(a_base + k16 * 256, 128, 1024);
                             const uint64_t bd = smem_desc(b_base + c * 128 + k16 * 256, 128, 1024);
-                            mma_bf16(d + uint32_t(c), ad, bd, idesc, (kb > 0 || k16 > 0) ? 1u : 0u);
+                            if constexpr (MODE == kSearch)
+                                mma_u8(d + uint32_t(c), ad, bd, idesc, (kb > 0 || k16 > 0) ? 1u : 0u);
+                            else
+                                mma_bf16(d + uint32_t(c), ad, bd, idesc, (kb > 0 || k16 > 0) ? 1u : 0u);
                         }
                     }
                     mma_commit(&empty_bar[s]);
@@ -1632,15 +1646,9 @@ __device__ __forceinline__ void conv_ws_body(const TcParams &P)
         // ---------------- epilogue (warps 0-3) ----------------
         // warp w reads tensor-memory lanes 32 w .. 32 w + 31 (rows of the tile)
         const int row = (warp & 3) * 32 + lane;
-        float c0 = 0.f;
-        if constexpr (MODE == kSearch)
-        {
-            // the launch-wide part of the tier-1 bound: 6.25 * 2^-24 times the
-            // largest third-term sums, plus the largest channel bound
-            const float emx = __uint_as_float(P.sinfo[0]);
-            const float lmax = ldexpf(float(P.kreal), int(P.sinfo[1]) - 128 - 16);
-            c0 = __fadd_ru(__fmaf_ru(lmax, 0x1.9p-22f, emx), 0x1p-126f);
-        }
+        // the largest channel bound (search)
+        float emax = 0.f;
+        if constexpr (MODE == kSearch) emax = __uint_as_float(P.sinfo[0]);
         uint32_t j = 0;
         for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++j)
         {
@@ -1706,10 +1714,8 @@ __device__ __forceinline__ void conv_ws_body(const TcParams &P)
             }
             else if constexpr (MODE == kSearch)
             {
-                if (P.nsplit == 4)
-                    search_epilogue<4>(P, acc, s_ok, s_e.x, s_e.y, P.round == 2 ? s_aux : 0, s_st, &acce_bar[a], c0);
-                else
-                    search_epilogue<3>(P, acc, s_ok, s_e.x, s_e.y, P.round == 2 ? s_aux : 0, s_st, &acce_bar[a], c0);
+                search_epilogue<kSearchTerms>(P, acc, s_ok, s_e.x, s_e.y, P.round == 2 ? s_aux : 0, s_st,
+                                              &acce_bar[a], emax, s_scale, s_bound);
             }
             else if constexpr (MODE == kFused)
             {
@@ -1884,38 +1890,35 @@ __global__ void __launch_bounds__(128) wta_records_warp_kernel(const int4 *__res
 }
 
 // ---- search path: weight split, exact recompute, outputs ---------------------
-// Fixed-grid split of output channel n's weights into NS BF16 terms (one CTA
-// per channel of the padded tile).  With 2^e the smallest power of two at or
-// above the channel's largest |w| (clamped to [2^-100, 2^100] so that every
-// grid is a normal BF16 number), term j is the digit of the remainder on the
-// grid 2^(e - 8 (j + 1)), rounded to nearest: |digit| <= 256 for the first
-// term and <= 128 after, exact in BF16.  A product with a 0/1 spike is then
-// a multiple of its term's grid and every tensor-memory sum over K < 2^16
-// taps is exact.  echan[n] bounds |oracle - exact term total| for any 0/1
-// input: the sum of the remainders below the last grid (zero for weights in
-// [2^(e-1), 2^e] with NS = 3) plus K^2 2^(e-52) for the FP64 rounding of
-// the oracle's ordered sum of K products, rounded up.  Layout as
-// split_weights_kernel's (one N tile).
+// Split of output channel n's weights into NS base-256 digits (one CTA per
+// channel of the padded tile).  With 2^e the smallest power of two above the
+// channel's largest weight (e clamped to [-94, 100]), w = 2^e sum_j d_j
+// 256^-(j+1) + rem, digits d_j in [0, 255] (floor), 0 <= rem < 2^(e - 8 NS).
+// A 0/1 spike times a digit is an exact 8-bit product and the tensor core's
+// 32-bit integer sums are exact, so the row's term total R (an integer) times
+// cscale[n] = 2^(e - 8 NS) is the potential of the digit weights exactly.
+// echan[n] bounds |oracle - R cscale| for any 0/1 input: the sum of the
+// remainders (zero when every weight lies on the 2^(e - 8 NS) grid) plus,
+// unless the oracle's ordered FP64 sum is exact for these weights, K^2
+// 2^(e-52).  Negative weights only raise *negw (the search then stands down).
+// The operand layout is split_weights_kernel's, with 16 U8 elements per
+// 16-byte chunk (128 per K block), K in channels-last order.
 template <int NS>
 __global__ void __launch_bounds__(256) fixed_split_kernel(const float *__restrict__ kernel, uint4 *__restrict__ wimg,
-                                                          int cout, int cin, int taps, int nhwc, int cpad,
-                                                          int kblocks, int n_tile, float *__restrict__ echan,
-                                                          unsigned *__restrict__ sinfo, int *__restrict__ negw,
-                                                          unsigned *__restrict__ wmax)
+                                                          int cout, int cin, int taps, int cpad, int kblocks,
+                                                          int n_tile, float *__restrict__ echan,
+                                                          float *__restrict__ cscale, unsigned *__restrict__ sinfo,
+                                                          int *__restrict__ negw, unsigned *__restrict__ wmax)
 {
     __shared__ float s_mx[8];
     __shared__ double s_err[8];
     __shared__ int s_lsb[8];
     const int n = blockIdx.x, tid = threadIdx.x;
-    const int kreal = nhwc ? taps * cpad : taps * cin;
-    const int K = kblocks * BK;
+    const int kreal = taps * cpad;
+    const int K = kblocks * 2 * BK;
     auto weight = [&](int k) -> float {
         if (n >= cout || k >= kreal) return 0.f;
-        int c, tap;
-        if (nhwc)
-            tap = k / cpad, c = k % cpad;
-        else
-            c = k / taps, tap = k % taps;
+        const int tap = k / cpad, c = k % cpad;
         return c < cin ? kernel[(int64_t(n) * cin + c) * taps + tap] : 0.f;
     };
     float mx = 0.f;
@@ -1929,7 +1932,7 @@ __global__ void __launch_bounds__(256) fixed_split_kernel(const float *__restric
         if (wmax && n < cout && k < kreal && w > 0.f)
         {
             // largest weight of each input over the channels (oracle layout)
-            const int c = nhwc ? k % cpad : k / taps, tap = nhwc ? k / cpad : k % taps;
+            const int tap = k / cpad, c = k % cpad;
             if (c < cin) atomicMax(wmax + c * taps + tap, __float_as_uint(w));
         }
         const uint32_t bits = __float_as_uint(w) & 0x7FFFFFFFu;
@@ -1953,35 +1956,32 @@ __global__ void __launch_bounds__(256) fixed_split_kernel(const float *__restric
     if (mx > 0.f)
     {
         int ex;
-        const float fr = frexpf(mx, &ex);  // mx = fr 2^ex, fr in [0.5, 1)
-        e = fr == 0.5f ? ex - 1 : ex;
+        frexpf(mx, &ex);  // mx = fr 2^ex, fr in [0.5, 1): mx < 2^ex
+        e = ex;
     }
-    e = max(-100, min(100, e));
+    e = max(-94, min(100, e));
     double err = 0.0;
     for (int i = tid; i < kblocks * 8; i += blockDim.x)
     {
         const int kb = i / 8, kc = i % 8;
         uint32_t parts[NS][4];
 #pragma unroll
-        for (int e8 = 0; e8 < 8; e8 += 2)
+        for (int j = 0; j < NS; ++j)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) parts[j][q] = 0u;
+#pragma unroll
+        for (int e16 = 0; e16 < 16; ++e16)
         {
-            uint32_t bits[2][NS];
+            const double w = fmax(double(weight(kb * 2 * BK + kc * 16 + e16)), 0.0);
+            double r = ldexp(w, -e);  // in [0, 1)
 #pragma unroll
-            for (int q = 0; q < 2; ++q)
+            for (int j = 0; j < NS; ++j)
             {
-                double r = double(weight(kb * BK + kc * 8 + e8 + q));
-#pragma unroll
-                for (int j = 0; j < NS; ++j)
-                {
-                    const double g = ldexp(1.0, e - 8 * (j + 1));
-                    const double d = rint(r / g) * g;
-                    r -= d;
-                    bits[q][j] = __bfloat16_as_ushort(__float2bfloat16_rn(float(d)));
-                }
-                err += fabs(r);
+                const double d = floor(r * 256.0);
+                r = r * 256.0 - d;
+                parts[j][e16 >> 2] |= uint32_t(d) << (8 * (e16 & 3));
             }
-#pragma unroll
-            for (int j = 0; j < NS; ++j) parts[j][e8 / 2] = bits[0][j] | (bits[1][j] << 16);
+            err += ldexp(r, e - 8 * NS);
         }
 #pragma unroll
         for (int j = 0; j < NS; ++j)
@@ -2006,6 +2006,7 @@ __global__ void __launch_bounds__(256) fixed_split_kernel(const float *__restric
         const double bound = err + (exact64 ? 0.0 : double(kreal) * double(kreal) * ldexp(1.0, e - 52));
         const float eb = __double2float_ru(bound);
         echan[n] = eb;
+        cscale[n] = ldexpf(1.f, e - 8 * NS);
         if (n < cout)
         {
             atomicMax(sinfo + 0, __float_as_uint(eb));
@@ -2378,7 +2379,7 @@ struct Plan
 
 // single_tile: all output channels in one CTA (required by the fused epilogue).
 Plan make_plan(int64_t n, int64_t cin, int64_t h, int64_t w, int64_t cout, int64_t kh, int64_t kw, int precision,
-               bool single_tile, int64_t t_fused = 0, bool times = false, int nsplit = 0)
+               bool single_tile, int64_t t_fused = 0, bool times = false, int nsplit = 0, bool cl = false)
 {
     Plan pl{};
     pl.nsplit = nsplit > 0 ? nsplit : (precision == SPK_CONV_BF16X3 ? 3 : 2);
@@ -2386,10 +2387,14 @@ Plan make_plan(int64_t n, int64_t cin, int64_t h, int64_t w, int64_t cout, int64
     const int64_t cap = single_tile ? npad : (pl.nsplit == 3 ? 128 : 256);
     pl.n_tiles = int(ceil_div(npad, cap));
     pl.n_tile = int(ceil_div(ceil_div(npad, pl.n_tiles), 16) * 16);
-    pl.nhwc = cin >= 8;
+    // channels-last from 8 input channels, and always where the fused layer
+    // can take the search path (cl; its kernels gather 8-channel groups)
+    pl.nhwc = cin >= 8 || cl || nsplit > 0;
     pl.cpad = int(ceil_div(cin, 8) * 8);
     const int64_t kreal = pl.nhwc ? kh * kw * pl.cpad : kh * kw * cin;
-    pl.kblocks = int(ceil_div(kreal, BK));
+    // search plans (nsplit given): 8-bit operands, 128 elements per K block
+    // in the same 128-byte rows
+    pl.kblocks = int(ceil_div(kreal, nsplit > 0 ? 2 * BK : BK));
     // two accumulators (the epilogue of one tile overlaps the MMAs of the
     // next) when they fit in the 512 tensor-memory columns
     const uint32_t acc_cols = uint32_t(pl.nsplit * pl.n_tile);
@@ -2407,7 +2412,9 @@ Plan make_plan(int64_t n, int64_t cin, int64_t h, int64_t w, int64_t cout, int64
         pl.xt_bytes = pl.nhwc ? size_t(n) * h * w * pl.cpad : 0;
     // (kTimes: the table is followed by the per-warp first-step candidates,
     // two buffers of 4 warps x n_tile ints)
-    const size_t tab = t_fused > 0  ? (size_t(pl.kblocks) * BK + 8) * 16 + (times ? size_t(pl.n_tile) * 32 : 0)
+    // (search: 16 group entries per K block, then the channels' scales and bounds)
+    const size_t tab = nsplit > 0   ? size_t(pl.kblocks) * 256 + size_t(pl.n_tile) * 8 + 64
+                       : t_fused > 0 ? (size_t(pl.kblocks) * BK + 8) * 16 + (times ? size_t(pl.n_tile) * 32 : 0)
                        : !pl.nhwc   ? size_t(pl.kblocks) * BK * 16
                                     : size_t(pl.kblocks) * 8 * 16;
     const size_t stage = size_t(BM * BK * 2) + size_t(pl.nsplit) * pl.n_tile * BK * 2;
@@ -2752,7 +2759,7 @@ FusedLayout fused_layout(int64_t b, int64_t t, int64_t cin, int64_t h, int64_t w
     FusedLayout L{};
     L.oh = (h + p.top + p.bottom - kh) / sy + 1;
     L.ow = (w + p.left + p.right - kw) / sx + 1;
-    L.pl = make_plan(b * t, cin, h, w, cout, kh, kw, precision, true, t);
+    L.pl = make_plan(b * t, cin, h, w, cout, kh, kw, precision, true, t, false, 0, nnets == 1);
     int tp = 1, lg = 0;
     while (tp < t) tp <<= 1, ++lg;
     L.tp_log2 = lg;
@@ -2765,9 +2772,7 @@ FusedLayout fused_layout(int64_t b, int64_t t, int64_t cin, int64_t h, int64_t w
     off += align256(size_t(b) * 4);
     L.max_off = off;
     off += align256(size_t(b) * 4);
-    L.pl4 = make_plan(b * t, cin, h, w, cout, kh, kw, precision, true, t, false, kSearchTermsMax);
-    if (L.pl4.nsplit * L.pl4.n_tile > 512 || L.pl4.stages < 2)
-        L.pl4 = make_plan(b * t, cin, h, w, cout, kh, kw, precision, true, t, false, kSearchTermsMin);
+    L.pl4 = make_plan(b * t, cin, h, w, cout, kh, kw, precision, true, t, false, kSearchTerms);
     L.search_ok = nnets == 1 && t <= 127 && L.pl4.n_tiles == 1 && L.pl4.nsplit * L.pl4.n_tile <= 512 &&
                   L.pl4.stages >= 2 && L.pl4.smem <= 227 * 1024 && L.pl4.kblocks <= kMaxKBlocks &&
                   L.pl.xt_bytes < (size_t(1) << 31) && h < 30000 && w < 30000;
@@ -2775,7 +2780,7 @@ FusedLayout fused_layout(int64_t b, int64_t t, int64_t cin, int64_t h, int64_t w
     {
         const size_t np = size_t(L.npix);
         L.w4_off = off, off += align256(L.pl4.wimg_bytes);
-        L.echan_off = off, off += align256(size_t(L.pl4.n_tile) * 4 + 8);
+        L.echan_off = off, off += align256(size_t(L.pl4.n_tile) * 8 + 8);
         L.wm_off = off, off += align256(size_t(cin * kh * kw) * 4);
         L.cnt_off = off, off += 256;  // 64 counters
         L.state_off = off, off += align256(np * 16);
@@ -2910,7 +2915,9 @@ void search_layer(const TcParams &P0, const FusedLayout &L, const float *kernel,
     P.nsplit = pl.nsplit, P.n_tile = pl.n_tile, P.n_tiles = 1, P.kblocks = pl.kblocks;
     P.tmem_cols = pl.tmem_cols, P.stages = pl.stages, P.nacc = pl.nacc;
     float *echan = reinterpret_cast<float *>(base + L.echan_off);
-    unsigned *sinfo = reinterpret_cast<unsigned *>(echan + pl.n_tile);
+    float *cscale = echan + pl.n_tile;
+    unsigned *sinfo = reinterpret_cast<unsigned *>(cscale + pl.n_tile);
+    P.cscale = cscale;
     int *cnt = reinterpret_cast<int *>(base + L.cnt_off);
     P.echan = echan, P.sinfo = sinfo;
     P.state = reinterpret_cast<int4 *>(base + L.state_off);
@@ -2931,10 +2938,9 @@ void search_layer(const TcParams &P0, const FusedLayout &L, const float *kernel,
     SPK_CUDA(cudaMemsetAsync(cnt, 0, 256, s));
     SPK_CUDA(cudaMemsetAsync(sinfo, 0, 8, s));
     if (prefilter) SPK_CUDA(cudaMemsetAsync(wmax, 0, size_t(kr) * 4, s));
-    auto split = pl.nsplit == 4 ? fixed_split_kernel<4> : fixed_split_kernel<3>;
-    split<<<unsigned(pl.n_tile), 256, 0, s>>>(kernel, reinterpret_cast<uint4 *>(base + L.w4_off), P.cout, P.cin,
-                                              taps, P.nhwc, P.cpad, pl.kblocks, pl.n_tile, echan, sinfo, P.negw,
-                                              prefilter ? wmax : nullptr);
+    fixed_split_kernel<kSearchTerms><<<unsigned(pl.n_tile), 256, 0, s>>>(
+        kernel, reinterpret_cast<uint4 *>(base + L.w4_off), P.cout, P.cin, taps, P.cpad, pl.kblocks, pl.n_tile, echan,
+        cscale, sinfo, P.negw, prefilter ? wmax : nullptr);
     SPK_LAUNCHED();
     if (count > 0)
     {

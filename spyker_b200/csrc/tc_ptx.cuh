@@ -81,6 +81,29 @@ __host__ __device__ constexpr uint32_t idesc_bf16_f32(int m, int n)
            | (uint32_t(m >> 4) << 24);     // M / 16
 }
 
+// kind::i8 instruction descriptor: U8 x U8 -> S32, both K-major.
+__host__ __device__ constexpr uint32_t idesc_u8_s32(int m, int n)
+{
+    return (2u << 4)                       // D format S32
+           | (0u << 7)                     // A format U8
+           | (0u << 10)                    // B format U8
+           | (uint32_t(n >> 3) << 17)      // N / 8
+           | (uint32_t(m >> 4) << 24);     // M / 16
+}
+
+// D[tmem] (+)= A[smem] * B[smem]^T over 8-bit integers (K = 32 per
+// instruction), issued by one thread.
+__device__ __forceinline__ void mma_u8(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                       uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
 // D[tmem] (+)= A[smem] * B[smem]^T, issued by one thread.
 __device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
                                          uint32_t accumulate)
