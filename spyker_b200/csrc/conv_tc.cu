@@ -1177,9 +1177,24 @@ __device__ __forceinline__ void s_extremes(const TcParams &P, int pix, const Sea
 // runner-up is within two ulps, the runner-up's, are certified against their
 // channel bounds; nothing else can change a decision unless the third value
 // comes that close too.
+// Warp-wide flush of a warp's buffered list entries: one atomic for all.
+__device__ __forceinline__ void s_flush(int2 *buf, int &fill, int2 *list, int *count)
+{
+    __syncwarp();
+    if (fill == 0) return;
+    const int lane = threadIdx.x & 31;
+    int base = 0;
+    if (lane == 0) base = atomicAdd(count, fill);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    for (int i = lane; i < fill; i += 32) list[base + i] = buf[i];
+    __syncwarp();
+    fill = 0;
+}
+
 template <int NS>
 __device__ void search_epilogue(const TcParams &P, uint32_t acc, bool ok, int pix, int t, int aux, int4 pstate,
-                                uint64_t *release, float emax, const float *scale, const float *bound)
+                                uint64_t *release, float emax, const float *scale, const float *bound, int2 *nbuf,
+                                int &nfill)
 {
     const int warp = threadIdx.x >> 5;
     const uint32_t lane_base = acc + (uint32_t((warp & 3) * 32) << 16);
@@ -1273,29 +1288,47 @@ __device__ void search_epilogue(const TcParams &P, uint32_t acc, bool ok, int pi
     // dec 3: the winner a is decided, its value is left to the exact sum
     SearchAct r;
     if (ok && (dec == 1 || dec == 2)) r = search_act(P, P.round, pix, t, dec, a, v, pstate);
-    // the four lists' slots: one atomic per list and warp, all in flight at once
+    // the next round's entries go to this warp's buffer (flushed with one
+    // atomic when it fills); the rarer lists take one atomic per warp each,
+    // all in flight at once
     const int lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1u;
+    const unsigned mn = __ballot_sync(0xffffffffu, r.next);
+    if (r.next) nbuf[nfill + __popc(mn & below)] = r.next_e;
+    nfill += __popc(mn);
+    if (nfill > 256 - 32) s_flush(nbuf, nfill, P.list_out, P.count_out);
     const bool wf = ok && dec == 0, wv = ok && dec == 3;
     const unsigned mf = __ballot_sync(0xffffffffu, wf), mv = __ballot_sync(0xffffffffu, wv);
-    const unsigned mn = __ballot_sync(0xffffffffu, r.next), mi = __ballot_sync(0xffffffffu, r.fin);
-    int bf = 0, bv = 0, bn = 0, bi = 0;
+    const unsigned mi = __ballot_sync(0xffffffffu, r.fin);
+    int bf = 0, bv = 0, bi = 0;
     if (lane == 0)
     {
         if (mf) bf = atomicAdd(P.fix_count, __popc(mf));
         if (mv) bv = atomicAdd(P.val_count, __popc(mv));
-        if (mn) bn = atomicAdd(P.count_out, __popc(mn));
         if (mi) bi = atomicAdd(P.final_count, __popc(mi));
     }
-    const unsigned below = (1u << lane) - 1u;
     bf = __shfl_sync(0xffffffffu, bf, 0) + __popc(mf & below);
     bv = __shfl_sync(0xffffffffu, bv, 0) + __popc(mv & below);
-    bn = __shfl_sync(0xffffffffu, bn, 0) + __popc(mn & below);
     bi = __shfl_sync(0xffffffffu, bi, 0) + __popc(mi & below);
     if (wf) P.fix_list[bf] = make_int4(pix, t, P.round, aux);
     if (wv) P.val_list[bv] = make_int4(pix, t, P.round, a);
-    if (r.next) P.list_out[bn] = r.next_e;
     if (r.fin) P.final_list[bi] = r.fin_e;
-    if (ok && P.wta) s_extremes(P, pix, r);
+    if (P.wta)
+    {
+        // the sample maxima: one atomic per sample among the warp's lanes
+        const int smp = ok ? pix / int(P.ohw) : -1;
+        const bool has = ok && r.max;
+        const unsigned key = has ? unsigned(smp) : 0xFFFFFFFFu;
+        const unsigned peers = __match_any_sync(0xffffffffu, key);
+        const unsigned enc = has ? order_enc(r.maxv) : 0u;
+        const unsigned best = __reduce_max_sync(peers, enc);
+        if (has && lane == __ffs(peers) - 1) atomicMax(P.maxs + smp, best);
+        if (ok && r.thv && P.thv != 0.f)
+        {
+            atomicMin(P.mins + smp, order_enc(P.thv));
+            atomicMax(P.maxs + smp, order_enc(P.thv));
+        }
+    }
 }
 
 __device__ __forceinline__ int2 search_entry(const TcParams &P, int64_t idx)
@@ -1455,6 +1488,8 @@ __device__ __forceinline__ void conv_ws_body(const TcParams &P)
     const int taps = P.kh * P.kw;
     // search: the channels' scales and bounds, staged after the table
     float *s_scale = reinterpret_cast<float *>(tab + P.kblocks * 16), *s_bound = s_scale + P.n_tile;
+    // search: per epilogue warp, a buffer of next-round list entries
+    int2 *s_nbuf = reinterpret_cast<int2 *>(s_bound + P.n_tile + ((16 - ((2 * P.n_tile) & 15)) & 15));
     if constexpr (MODE == kSearch)
     {
         // per 8-element group of a 128-element K block (channels-last, 8-bit
@@ -1646,8 +1681,10 @@ __device__ __forceinline__ void conv_ws_body(const TcParams &P)
         // ---------------- epilogue (warps 0-3) ----------------
         // warp w reads tensor-memory lanes 32 w .. 32 w + 31 (rows of the tile)
         const int row = (warp & 3) * 32 + lane;
-        // the largest channel bound (search)
+        // the largest channel bound, this warp's list buffer and its fill (search)
         float emax = 0.f;
+        int2 *nbuf = s_nbuf + (warp & 3) * 256;
+        int nfill = 0;
         if constexpr (MODE == kSearch) emax = __uint_as_float(P.sinfo[0]);
         uint32_t j = 0;
         for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++j)
@@ -1715,7 +1752,7 @@ __device__ __forceinline__ void conv_ws_body(const TcParams &P)
             else if constexpr (MODE == kSearch)
             {
                 search_epilogue<kSearchTerms>(P, acc, s_ok, s_e.x, s_e.y, P.round == 2 ? s_aux : 0, s_st,
-                                              &acce_bar[a], emax, s_scale, s_bound);
+                                              &acce_bar[a], emax, s_scale, s_bound, nbuf, nfill);
             }
             else if constexpr (MODE == kFused)
             {
@@ -1732,6 +1769,7 @@ __device__ __forceinline__ void conv_ws_body(const TcParams &P)
                 mbar_arrive(&acce_bar[a]);
             }
         }
+        if constexpr (MODE == kSearch) s_flush(nbuf, nfill, P.list_out, P.count_out);
     }
     tc_fence_before();
     __syncthreads();
@@ -2039,37 +2077,55 @@ __global__ void __launch_bounds__(256) search_bound_kernel(TcParams P, const uns
                                                            int2 *__restrict__ list, int *__restrict__ count)
 {
     if (*P.negw || *P.flag) return;
-    __shared__ float wm[128];
+    __shared__ float wm[32][8];    // per tap, the 8 channels of one first-spike word
+    __shared__ int2 lbuf[8][256];  // per warp: candidates awaiting one atomic
     const int taps = P.kh * P.kw, kr = P.cin * taps;
-    for (int i = threadIdx.x; i < kr; i += blockDim.x) wm[i] = __uint_as_float(wmax[i]);
-    __syncthreads();
-    const double widen = 1.0 + double(kr) * 0x1p-50;
-    const int lane = threadIdx.x & 31;
-    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
-    for (int64_t base = int64_t(blockIdx.x) * blockDim.x; base < P.npix; base += stride)
+    for (int i = threadIdx.x; i < 32 * 8; i += blockDim.x)
     {
-        const int64_t pix = base + threadIdx.x;
-        const bool ok = pix < P.npix;
+        const int tap = i / 8, c = i % 8;
+        wm[tap][c] = (tap < taps && c < P.cin) ? __uint_as_float(wmax[c * taps + tap]) : 0.f;
+    }
+    __syncthreads();
+    int2 *buf = lbuf[threadIdx.x >> 5];
+    int fill = 0;
+    // FP32 sum of at most kr non-negative terms: within kr 2^-24 of the exact
+    // sum, itself at least the oracle's FP64 sum / (1 + kr 2^-53)
+    const float widen = 1.f + float(kr + 2) * 0x1p-23f;
+    const int lane = threadIdx.x & 31;
+    const int ohw = int(P.ohw), npix = int(P.npix);
+    const int stride = int(gridDim.x) * blockDim.x;
+    for (int base = int(blockIdx.x) * blockDim.x; base < npix; base += stride)
+    {
+        const int pix = base + int(threadIdx.x);
+        const bool ok = pix < npix;
         bool cand = false;
         int smp = 0;
         if (ok)
         {
-            smp = int(pix / P.ohw);
-            const int p = int(pix - int64_t(smp) * P.ohw);
+            smp = pix / ohw;
+            const int p = pix - smp * ohw;
             const int oy = p / P.ow, ox = p - oy * P.ow;
             const int iy0 = oy * P.sy - P.top, ix0 = ox * P.sx - P.left;
             const int ky0 = max(0, -iy0), ky1 = min(P.kh, P.h - iy0);
             const int kx0 = max(0, -ix0), kx1 = min(P.kw, P.w - ix0);
             const uint8_t *fm = P.in + int64_t(smp) * P.img_stride;
-            double u = 0.0;
+            const uint32_t tt = uint32_t(P.T) * 0x01010101u;
+            float u = 0.f;
             for (int ky = ky0; ky < ky1; ++ky)
                 for (int kx = kx0; kx < kx1; ++kx)
                 {
-                    const uint8_t *f = fm + (int64_t(iy0 + ky) * P.w + ix0 + kx) * cp;
-                    for (int c = 0; c < P.cin; ++c)
-                        if (int(__ldg(f + c)) < P.T) u += double(wm[(c * P.kh + ky) * P.kw + kx]);
+                    const uint2 f = __ldg(reinterpret_cast<const uint2 *>(fm + ((iy0 + ky) * P.w + ix0 + kx) * cp));
+                    // 0x80 in the bytes that fired by step T - 1 (byte < T)
+                    const uint32_t lo = ((f.x | 0x80808080u) - tt) ^ 0x80808080u, hi = ((f.y | 0x80808080u) - tt) ^ 0x80808080u;
+                    const float *w = wm[ky * P.kw + kx];
+#pragma unroll
+                    for (int c = 0; c < 4; ++c)
+                    {
+                        u += (lo >> (8 * c + 7)) & 1u ? w[c] : 0.f;
+                        u += (hi >> (8 * c + 7)) & 1u ? w[c + 4] : 0.f;
+                    }
                 }
-            cand = u * widen > double(P.thr);
+            cand = __fmul_ru(u, widen) > P.thr;
         }
         if (ok && !cand)
         {
@@ -2081,11 +2137,11 @@ __global__ void __launch_bounds__(256) search_bound_kernel(TcParams P, const uns
             }
         }
         const unsigned m = __ballot_sync(0xffffffffu, cand);
-        int b0 = 0;
-        if (lane == 0 && m) b0 = atomicAdd(count, __popc(m));
-        b0 = __shfl_sync(0xffffffffu, b0, 0) + __popc(m & ((1u << lane) - 1u));
-        if (cand) list[b0] = make_int2(int(pix), P.T - 1);
+        if (cand) buf[fill + __popc(m & ((1u << lane) - 1u))] = make_int2(pix, P.T - 1);
+        fill += __popc(m);
+        if (fill > 256 - 32) s_flush(buf, fill, list, count);
     }
+    s_flush(buf, fill, list, count);
 }
 
 // Rows the search could not decide from the term sums (a potential within
@@ -2413,7 +2469,7 @@ Plan make_plan(int64_t n, int64_t cin, int64_t h, int64_t w, int64_t cout, int64
     // (kTimes: the table is followed by the per-warp first-step candidates,
     // two buffers of 4 warps x n_tile ints)
     // (search: 16 group entries per K block, then the channels' scales and bounds)
-    const size_t tab = nsplit > 0   ? size_t(pl.kblocks) * 256 + size_t(pl.n_tile) * 8 + 64
+    const size_t tab = nsplit > 0   ? size_t(pl.kblocks) * 256 + size_t(pl.n_tile) * 8 + 64 + 4 * 256 * 8
                        : t_fused > 0 ? (size_t(pl.kblocks) * BK + 8) * 16 + (times ? size_t(pl.n_tile) * 32 : 0)
                        : !pl.nhwc   ? size_t(pl.kblocks) * BK * 16
                                     : size_t(pl.kblocks) * 8 * 16;
@@ -2933,7 +2989,7 @@ void search_layer(const TcParams &P0, const FusedLayout &L, const float *kernel,
     // the bound pre-filter of round 0, for layers with few inputs per output
     const int cp = P.nhwc ? P.cpad : P.cin;
     const int kr = P.cin * taps;
-    const bool prefilter = kr <= 128;
+    const bool prefilter = P.cin <= 8 && taps <= 32 && P.cpad == 8;
     unsigned *wmax = reinterpret_cast<unsigned *>(base + L.wm_off);
     SPK_CUDA(cudaMemsetAsync(cnt, 0, 256, s));
     SPK_CUDA(cudaMemsetAsync(sinfo, 0, 8, s));
