@@ -109,6 +109,7 @@ struct TcParams
     const unsigned *sinfo;  // [0] largest echan (bits), [1] largest channel exponent + 128
     int kreal;              // real K (taps x input channels)
     int r0_list;            // round 0 takes the (pixel, T - 1) entries of list_in (bound pre-filter ran)
+    int nparts;             // channel parts of n_tile per tile (search)
     // kFused: leave at once when the search path ran (no negative weight and
     // cumulative 0/1 input; these are the words of negw and flag)
     int skip_when_lean;
@@ -1177,6 +1178,16 @@ __device__ __forceinline__ void s_extremes(const TcParams &P, int pix, const Sea
 // runner-up is within two ulps, the runner-up's, are certified against their
 // channel bounds; nothing else can change a decision unless the third value
 // comes that close too.
+// Running state of a row's scan over the channel parts of a tile: the three
+// largest potentials, the channels of the first two and their term totals
+// (r1 also carries the winner's total in the last round).
+struct SearchScan
+{
+    float p1 = -INFINITY, p2 = -INFINITY, p3 = -INFINITY;
+    int a1 = -1, a2 = -1;
+    uint64_t r1 = 0, r2 = 0;
+};
+
 // Warp-wide flush of a warp's buffered list entries: one atomic for all.
 __device__ __forceinline__ void s_flush(int2 *buf, int &fill, int2 *list, int *count)
 {
@@ -1194,51 +1205,63 @@ __device__ __forceinline__ void s_flush(int2 *buf, int &fill, int2 *list, int *c
 template <int NS>
 __device__ void search_epilogue(const TcParams &P, uint32_t acc, bool ok, int pix, int t, int aux, int4 pstate,
                                 uint64_t *release, float emax, const float *scale, const float *bound, int2 *nbuf,
-                                int &nfill)
+                                int &nfill, int part, SearchScan &sc)
 {
     const int warp = threadIdx.x >> 5;
     const uint32_t lane_base = acc + (uint32_t((warp & 3) * 32) << 16);
     const float thr = P.thr;
+    const bool last = part == P.nparts - 1;
+    const int cg = part * P.n_tile;  // first channel of this part
     int dec = 0, a = -1;
     float v = 0.f;
     if (P.round == 2)
     {
-        const uint64_t R = s_reload<NS>(lane_base, P.n_tile, ok ? aux : -1);
+        const int col = (ok && aux >= cg && aux < cg + P.n_tile) ? aux - cg : -1;
+        const uint64_t R = s_reload<NS>(lane_base, P.n_tile, col);
+        if (col >= 0) sc.r1 = R;
         tc_fence_before();
         mbar_arrive(release);
+        if (!last) return;
         if (ok)
         {
             float lo, hi;
-            s_round(double(R) * double(scale[aux]), bound[aux], v, lo, hi);
+            s_round(double(sc.r1) * double(scale[aux]), bound[aux], v, lo, hi);
             dec = lo == hi ? 2 : 3;
             a = aux;
         }
     }
     else
     {
-        float p1 = -INFINITY, p2 = -INFINITY, p3 = -INFINITY;
-        int a1 = -1, a2 = -1;
-        uint64_t r1 = 0, r2 = 0;
+        float &p1 = sc.p1, &p2 = sc.p2, &p3 = sc.p3;
+        int &a1 = sc.a1, &a2 = sc.a2;
+        uint64_t &r1 = sc.r1, &r2 = sc.r2;
         for (int cb = 0; cb < P.n_tile; cb += kEpiChunk)
         {
             uint32_t q[NS][kEpiChunk];
             s_chunk<NS>(lane_base, cb, P.n_tile, q);
             s_chunk_wait<NS>(q);
-            const int lim = P.cout - cb;
+            const int lim = P.cout - cg - cb;
 #pragma unroll
             for (int j = 0; j < kEpiChunk; ++j)
             {
                 const uint64_t R = s_total<NS>(q, j);
-                const float pv = j < lim ? __ll2float_rn((long long)R) * scale[cb + j] : -INFINITY;
+                const int c = cg + cb + j;
+                const float pv = j < lim ? __ll2float_rn((long long)R) * scale[c] : -INFINITY;
                 const bool g1 = pv > p1, g2 = !g1 && pv > p2, g3 = !g1 && !g2 && pv > p3;
                 p3 = g1 || g2 ? p2 : (g3 ? pv : p3);
                 p2 = g1 ? p1 : (g2 ? pv : p2);
-                a2 = g1 ? a1 : (g2 ? cb + j : a2);
+                a2 = g1 ? a1 : (g2 ? c : a2);
                 r2 = g1 ? r1 : (g2 ? R : r2);
                 p1 = g1 ? pv : p1;
-                a1 = g1 ? cb + j : a1;
+                a1 = g1 ? c : a1;
                 r1 = g1 ? R : r1;
             }
+        }
+        if (!last)
+        {
+            tc_fence_before();
+            mbar_arrive(release);
+            return;
         }
         int d1 = 0;  // tier-1 decision: 0 open, 1 below, 2 winner decided (value certified or not)
         bool vexact = false;
@@ -1268,7 +1291,9 @@ __device__ void search_epilogue(const TcParams &P, uint32_t acc, bool ok, int pi
         int d2 = 0, a2t = -1;
         float v2 = 0.f;
         const unsigned open1 = __ballot_sync(0xffffffffu, ok && d1 == 0);
-        if (open1)
+        // tier 2 reads every channel from tensor memory: one part only (with
+        // several, the row goes to the exact recompute)
+        if (open1 && P.nparts == 1)
         {
             if ((threadIdx.x & 31) == 0) atomicAdd(&g_rechecks, (unsigned long long)__popc(open1));
             s_tier2<NS>(P, lane_base, thr, d2, a2t, v2, scale, bound);
@@ -1410,6 +1435,7 @@ __device__ __forceinline__ void search_producer(const TcParams &P, const int4 *t
                 utt[i] = uint32_t(e.y + 1) * 0x01010101u;
             }
         }
+        for (int part = 0; part < P.nparts; ++part)
         for (int kb = 0; kb < P.kblocks; ++kb, ++it)
         {
             uint2 fa[NU], fb[NU];
@@ -1426,7 +1452,8 @@ __device__ __forceinline__ void search_producer(const TcParams &P, const int4 *t
             if (p == 0)
             {
                 arrive_expect_tx(&full_bar[s], uint32_t(b_bytes));
-                bulk_g2s(sA + a_bytes, P.wimg + int64_t(kb) * b_bytes, uint32_t(b_bytes), &full_bar[s]);
+                bulk_g2s(sA + a_bytes, P.wimg + (int64_t(part) * P.kblocks + kb) * b_bytes, uint32_t(b_bytes),
+                         &full_bar[s]);
             }
 #pragma unroll
             for (int i = 0; i < NU; ++i)
@@ -1487,9 +1514,10 @@ __device__ __forceinline__ void conv_ws_body(const TcParams &P)
     int4 *tab = reinterpret_cast<int4 *>(smem + S * stage_bytes);
     const int taps = P.kh * P.kw;
     // search: the channels' scales and bounds, staged after the table
-    float *s_scale = reinterpret_cast<float *>(tab + P.kblocks * 16), *s_bound = s_scale + P.n_tile;
+    const int nch = MODE == kSearch ? P.nparts * P.n_tile : P.n_tile;  // channels of the tables
+    float *s_scale = reinterpret_cast<float *>(tab + P.kblocks * 16), *s_bound = s_scale + nch;
     // search: per epilogue warp, a buffer of next-round list entries
-    int2 *s_nbuf = reinterpret_cast<int2 *>(s_bound + P.n_tile + ((16 - ((2 * P.n_tile) & 15)) & 15));
+    int2 *s_nbuf = reinterpret_cast<int2 *>(s_bound + nch + ((16 - ((2 * nch) & 15)) & 15));
     if constexpr (MODE == kSearch)
     {
         // per 8-element group of a 128-element K block (channels-last, 8-bit
@@ -1499,7 +1527,7 @@ __device__ __forceinline__ void conv_ws_body(const TcParams &P)
             const int k = g * 8, tap = k / P.cpad, c = k % P.cpad;
             tab[g] = make_int4(c, tap / P.kw, tap % P.kw, (tap < taps && c < P.cin) ? 1 : 0);
         }
-        for (int c = tid; c < P.n_tile; c += blockDim.x) s_scale[c] = P.cscale[c], s_bound[c] = P.echan[c];
+        for (int c = tid; c < nch; c += blockDim.x) s_scale[c] = P.cscale[c], s_bound[c] = P.echan[c];
     }
     else if constexpr (MODE != kPotentials)
     {
@@ -1628,7 +1656,9 @@ __device__ __forceinline__ void conv_ws_body(const TcParams &P)
         {
             uint32_t it = 0, j = 0;
             bool failed = false;
-            for (int64_t tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x, ++j)
+            const int parts = MODE == kSearch ? P.nparts : 1;
+            for (int64_t unit = blockIdx.x * int64_t(parts); unit < ntiles * parts && !failed;
+                 unit += (unit % parts == parts - 1) ? int64_t(gridDim.x - 1) * parts + 1 : 1, ++j)
             {
                 const int a = int(j % uint32_t(nacc));
                 const uint32_t ua = j / uint32_t(nacc);
@@ -1687,8 +1717,13 @@ __device__ __forceinline__ void conv_ws_body(const TcParams &P)
         int nfill = 0;
         if constexpr (MODE == kSearch) emax = __uint_as_float(P.sinfo[0]);
         uint32_t j = 0;
-        for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++j)
+        const int parts = MODE == kSearch ? P.nparts : 1;
+        SearchScan scan;
+        for (int64_t unit = blockIdx.x * int64_t(parts); unit < ntiles * parts;
+             unit += (unit % parts == parts - 1) ? int64_t(gridDim.x - 1) * parts + 1 : 1, ++j)
         {
+            const int64_t tile = unit / parts;
+            const int part = int(unit % parts);
             const int a = int(j % uint32_t(nacc));
             const uint32_t ua = j / uint32_t(nacc);
             // search rows: the row's list entry and pixel state are loaded
@@ -1751,8 +1786,9 @@ __device__ __forceinline__ void conv_ws_body(const TcParams &P)
             }
             else if constexpr (MODE == kSearch)
             {
+                if (part == 0) scan = SearchScan{};
                 search_epilogue<kSearchTerms>(P, acc, s_ok, s_e.x, s_e.y, P.round == 2 ? s_aux : 0, s_st,
-                                              &acce_bar[a], emax, s_scale, s_bound, nbuf, nfill);
+                                              &acce_bar[a], emax, s_scale, s_bound, nbuf, nfill, part, scan);
             }
             else if constexpr (MODE == kFused)
             {
@@ -2024,7 +2060,10 @@ __global__ void __launch_bounds__(256) fixed_split_kernel(const float *__restric
 #pragma unroll
         for (int j = 0; j < NS; ++j)
         {
-            const int64_t idx = (int64_t(kb) * NS + j) * (int64_t(n_tile) * 8) + (n / 8) * 64 + kc * 8 + (n % 8);
+            // part n / n_tile of the channels, row n % n_tile within it
+            const int part = n / n_tile, nl = n % n_tile;
+            const int64_t idx = ((int64_t(part) * kblocks + kb) * NS + j) * (int64_t(n_tile) * 8) + (nl / 8) * 64 +
+                                kc * 8 + (nl % 8);
             wimg[idx] = make_uint4(parts[j][0], parts[j][1], parts[j][2], parts[j][3]);
         }
     }
@@ -2428,6 +2467,7 @@ Schedule g_schedule;
 struct Plan
 {
     int nsplit, n_tile, n_tiles, kblocks, cpad, stages, nacc;
+    int parts = 1;  // search plans: channel parts of n_tile run one after another per tile
     bool nhwc;
     uint32_t tmem_cols;
     size_t wimg_bytes, xt_bytes, smem;
@@ -2443,6 +2483,12 @@ Plan make_plan(int64_t n, int64_t cin, int64_t h, int64_t w, int64_t cout, int64
     const int64_t cap = single_tile ? npad : (pl.nsplit == 3 ? 128 : 256);
     pl.n_tiles = int(ceil_div(npad, cap));
     pl.n_tile = int(ceil_div(ceil_div(npad, pl.n_tiles), 16) * 16);
+    if (nsplit > 0)
+    {
+        // search: the channels in parts whose accumulators fit the tensor memory
+        while (int64_t(pl.nsplit) * ceil_div(ceil_div(npad, pl.parts), 16) * 16 > 512) ++pl.parts;
+        pl.n_tile = int(ceil_div(ceil_div(npad, pl.parts), 16) * 16);
+    }
     // channels-last from 8 input channels, and always where the fused layer
     // can take the search path (cl; its kernels gather 8-channel groups)
     pl.nhwc = cin >= 8 || cl || nsplit > 0;
@@ -2459,7 +2505,7 @@ Plan make_plan(int64_t n, int64_t cin, int64_t h, int64_t w, int64_t cout, int64
     uint32_t cols = 32;
     while (cols < pl.nacc * acc_cols) cols <<= 1;
     pl.tmem_cols = cols;
-    pl.wimg_bytes = size_t(pl.n_tiles) * pl.kblocks * pl.nsplit * pl.n_tile * BK * 2;
+    pl.wimg_bytes = size_t(pl.n_tiles) * pl.parts * pl.kblocks * pl.nsplit * pl.n_tile * BK * 2;
     // staged copy of the spikes: channels-last [N, H, W, Cpad] (plain), or
     // the first-spike map [B, H, W, Cpad or Cin] plus a flag word (fused)
     if (t_fused > 0)
@@ -2469,7 +2515,7 @@ Plan make_plan(int64_t n, int64_t cin, int64_t h, int64_t w, int64_t cout, int64
     // (kTimes: the table is followed by the per-warp first-step candidates,
     // two buffers of 4 warps x n_tile ints)
     // (search: 16 group entries per K block, then the channels' scales and bounds)
-    const size_t tab = nsplit > 0   ? size_t(pl.kblocks) * 256 + size_t(pl.n_tile) * 8 + 64 + 4 * 256 * 8
+    const size_t tab = nsplit > 0   ? size_t(pl.kblocks) * 256 + size_t(pl.parts) * pl.n_tile * 8 + 64 + 4 * 256 * 8
                        : t_fused > 0 ? (size_t(pl.kblocks) * BK + 8) * 16 + (times ? size_t(pl.n_tile) * 32 : 0)
                        : !pl.nhwc   ? size_t(pl.kblocks) * BK * 16
                                     : size_t(pl.kblocks) * 8 * 16;
@@ -2829,14 +2875,15 @@ FusedLayout fused_layout(int64_t b, int64_t t, int64_t cin, int64_t h, int64_t w
     L.max_off = off;
     off += align256(size_t(b) * 4);
     L.pl4 = make_plan(b * t, cin, h, w, cout, kh, kw, precision, true, t, false, kSearchTerms);
-    L.search_ok = nnets == 1 && t <= 127 && L.pl4.n_tiles == 1 && L.pl4.nsplit * L.pl4.n_tile <= 512 &&
+    L.search_ok = nnets == 1 && t <= 127 && L.pl4.n_tiles == 1 && L.pl4.parts <= 8 &&
+                  L.pl4.nsplit * L.pl4.n_tile <= 512 &&
                   L.pl4.stages >= 2 && L.pl4.smem <= 227 * 1024 && L.pl4.kblocks <= kMaxKBlocks &&
                   L.pl.xt_bytes < (size_t(1) << 31) && h < 30000 && w < 30000;
     if (L.search_ok)
     {
         const size_t np = size_t(L.npix);
         L.w4_off = off, off += align256(L.pl4.wimg_bytes);
-        L.echan_off = off, off += align256(size_t(L.pl4.n_tile) * 8 + 8);
+        L.echan_off = off, off += align256(size_t(L.pl4.parts) * L.pl4.n_tile * 8 + 8);
         L.wm_off = off, off += align256(size_t(cin * kh * kw) * 4);
         L.cnt_off = off, off += 256;  // 64 counters
         L.state_off = off, off += align256(np * 16);
@@ -2970,9 +3017,11 @@ void search_layer(const TcParams &P0, const FusedLayout &L, const float *kernel,
     P.wimg = base + L.w4_off;
     P.nsplit = pl.nsplit, P.n_tile = pl.n_tile, P.n_tiles = 1, P.kblocks = pl.kblocks;
     P.tmem_cols = pl.tmem_cols, P.stages = pl.stages, P.nacc = pl.nacc;
+    const int nch = pl.parts * pl.n_tile;
     float *echan = reinterpret_cast<float *>(base + L.echan_off);
-    float *cscale = echan + pl.n_tile;
-    unsigned *sinfo = reinterpret_cast<unsigned *>(cscale + pl.n_tile);
+    float *cscale = echan + nch;
+    unsigned *sinfo = reinterpret_cast<unsigned *>(cscale + nch);
+    P.nparts = pl.parts;
     P.cscale = cscale;
     int *cnt = reinterpret_cast<int *>(base + L.cnt_off);
     P.echan = echan, P.sinfo = sinfo;
@@ -2994,7 +3043,7 @@ void search_layer(const TcParams &P0, const FusedLayout &L, const float *kernel,
     SPK_CUDA(cudaMemsetAsync(cnt, 0, 256, s));
     SPK_CUDA(cudaMemsetAsync(sinfo, 0, 8, s));
     if (prefilter) SPK_CUDA(cudaMemsetAsync(wmax, 0, size_t(kr) * 4, s));
-    fixed_split_kernel<kSearchTerms><<<unsigned(pl.n_tile), 256, 0, s>>>(
+    fixed_split_kernel<kSearchTerms><<<unsigned(nch), 256, 0, s>>>(
         kernel, reinterpret_cast<uint4 *>(base + L.w4_off), P.cout, P.cin, taps, P.cpad, pl.kblocks, pl.n_tile, echan,
         cscale, sinfo, P.negw, prefilter ? wmax : nullptr);
     SPK_LAUNCHED();

@@ -160,3 +160,17 @@ def test_search_trained_weights_fresh_images(port, trained):
     d = port.filter("dog", img[:, None], make_golden.dog_kernel(port), (3, 3, 3, 3))
     codes = port.rank_code(d, 15)
     assert check(port, codes, w1, 15.0, 3, 5, 2)[0] > 0
+
+
+@pytest.mark.parametrize("kind", ["binary", "halves", "log_uniform"])
+def test_search_channel_parts(port, kind):
+    """256 output channels: the search runs the channels in two parts per
+    tile and merges the parts' maxima; ties and saturated weights across the
+    part boundary still resolve as the oracle does (first channel wins)."""
+    rng = np.random.default_rng(sum(map(ord, kind)) + 256)
+    b, t, cin, h, wd, cout, k, pad = 2, 15, 16, 10, 10, 256, 3, 1
+    x = cumulative(rng, b, t, cin, h, wd)
+    w = weights(kind, rng, (cout, cin, k, k))
+    w[200:] = w[:56]  # channels 200.. tie exactly with channels 0..55 (other part)
+    th = float(np.round(np.median(port.conv(x[:, -1:], w, (1, 1), (pad,) * 4)) * 2) / 2)
+    assert check(port, x, w, max(th, 1.0), 1, 4, pad)[0] > 0

@@ -490,6 +490,8 @@ FUSED = [
     (4, 2, 2, 12, 12, 8, 5, 2, 3.0, 2, 5),
     (4, 1, 5, 7, 6, 12, 3, 0, 2.0, 1, 2),
     (2, 6, 64, 32, 32, 32, 3, 1, 120.0, 1, 4),  # first-spike staging in two pixel runs
+    (2, 30, 64, 12, 12, 256, 5, 2, 600.0, 1, 4),  # the large-image conv2 shape: channels in two parts
+    (3, 15, 16, 10, 9, 200, 3, 1, 40.0, 2, 6),  # 200 channels: two parts with padding
 ]
 
 
