@@ -51,6 +51,18 @@ def bf16_peak():
     return 1400.0, "sustained cuBLAS BF16 of an earlier measurement on this pool (of fallback)"
 
 
+def path_dtype(precision: str):
+    """(dtype, arithmetic) of the fused layers.  With non-negative weights
+    (STDP keeps them in [0, 1]) a fused layer takes the first-crossing search:
+    u8 spikes x u8 base-256 weight digits on the tensor cores with exact S32
+    sums, each potential rounded once from the exact sum; other weights take
+    the dense split kernel of ``precision``."""
+    if precision == "fp32":
+        return "f32", "FP32 SIMT convolution, op by op"
+    return "u8", (f"u8 spikes x 4 u8 weight digits (tcgen05 kind::i8, exact S32 sums, potentials rounded once "
+                  f"from the exact sum); {precision}-split/f32-acc dense kernel when a weight is negative")
+
+
 def headline_config(batch: int, world: int, mode: str = "replicas") -> dict:
     """The workload's `config`, shared by both arms of the bench."""
     return {"workload": WORKLOAD.replace("4096 x", f"{batch} x"), "global_batch": batch * world, "seq_len": T,
@@ -375,7 +387,8 @@ def gpu_arm(args, rank, world):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": {"fp32": "f32", "bf16x2": "bf16x2-split/f32-acc", "bf16x3": "bf16x3-split/f32-acc"}[args.precision],
+        "dtype": path_dtype(args.precision)[0],
+        "arithmetic": path_dtype(args.precision)[1],
         "data": "synthetic (seeded stroke images, MNIST geometry)",
         "config": headline_config(BATCH, world, args.mode),
         "conv_precision": args.precision,
@@ -533,6 +546,142 @@ def reference_arm(args, rank, world):
 
 
 # ----------------------------------------------------------------------------
+# One-layer STDP on 64 images (--workload config0)
+# ----------------------------------------------------------------------------
+CFG0_WORKLOAD = ("one-layer-stdp: 64 x 28x28 strokes, T=15, DoG 2x7x7 -> conv 30x5x5 th15 -> inhibit -> "
+                 "convwta r3k5 -> fire -> STDP(0.004, -0.003) -> pool 2")
+
+
+def config0_ref_step(o, torch, imgs, w1, dk):
+    """The reference's CPU path of the one-layer pipeline (the first layer of
+    :func:`reference_step`), weights updated in place."""
+    x = imgs.astype(np.float32) / np.float32(255)
+    codes = o.rank_code(o.filter("dog", x[:, None], dk, (3, 3, 3, 3)), T)
+    b = codes.shape[0]
+    f = torch.from_numpy(codes.reshape(b * T, 2, 28, 28).astype(np.float32))
+    p1 = torch.nn.functional.conv2d(f, torch.from_numpy(w1), padding=2).numpy().reshape(b, T, 30, 28, 28)
+    inh1 = o.inhibit(o.threshold(p1, 15.0))
+    s1 = o.fire(inh1)
+    win, cnt = o.convwta(inh1, (3, 3), 5)
+    w1[:] = o.convstdp(codes, w1, s1, [(0.004, -0.003, 1, 0, 1)], win, cnt, (1, 1), (2, 2, 2, 2))
+    return o.pool(s1, (2, 2))
+
+
+def config0_arm(args, rank, world):
+    """The small one-layer training step: 64 images through DoG, rank code
+    and the fused conv1 layer, its STDP update and the pool, as one captured
+    CUDA graph (the step is a few dozen microseconds of launches); weights
+    carried from step to step.  Spikes, winners and weights after the timed
+    steps are compared with the reference's CPU path run on the same images
+    for the same number of steps."""
+    if rank != 0:
+        return
+    import torch
+
+    import spyker_b200 as spyker
+    from spyker_b200 import synth
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    batch = args.batch if args.batch != BATCH else 64
+    imgs = synth.strokes(batch, seed=0)
+    host = torch.from_numpy(imgs).pin_memory()
+    static_u8 = host.to(dev)
+    dog = spyker.DoG(3, [spyker.DoGFilter(1, 2), spyker.DoGFilter(2, 1)], pad=3, device=dev)
+    conv = spyker.Conv(2, 30, 5, pad=2, device=dev)
+    w0 = synth.conv_weights(30, 2, 5, seed=1)
+    conv.kernel.copy_(torch.from_numpy(w0))
+    conv.stdpconfig = [spyker.STDPConfig(0.004, -0.003)]
+    conv.precision = args.precision
+
+    def step():
+        codes = spyker.code(dog(static_u8.float().div_(255.0)[:, None]), T)
+        spk, win, pooled = spyker.conv_fire_wta(codes, conv, 15.0, 3, 5, pool=2)
+        conv.stdp(codes, win, spk)
+        return spk, pooled
+
+    step()
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    l0 = spyker._lib.lib.spk_launch_count()
+    with torch.cuda.graph(graph):
+        spk_g, pooled_g = step()
+    launches = spyker._lib.lib.spk_launch_count() - l0
+    # parity run: restart from the initial weights, warm-up + timed steps
+    # replay the graph, the reference repeats the same number of steps
+    conv.kernel.copy_(torch.from_numpy(w0))
+    for _ in range(args.warmup):
+        graph.replay()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(dev.index) as clk:
+        a.record()
+        for _ in range(args.steps):
+            graph.replay()
+        b.record()
+        torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / args.steps
+    w_gpu = conv.kernel.cpu().numpy().copy()
+    spk_last = spk_g.cpu().numpy().copy()
+    # end to end: pinned host images -> graph input, replay, pooled map back
+    out = torch.empty(pooled_g.shape, dtype=pooled_g.dtype).pin_memory()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(args.steps):
+        static_u8.copy_(host, non_blocking=True)
+        graph.replay()
+        out.copy_(pooled_g, non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / args.steps
+    del graph
+    o, kind, torch_, _, dk = _ref_setup()
+    w_ref, w_prev = w0.copy(), w0.copy()
+    steps = args.warmup + args.steps
+    t0 = time.perf_counter()
+    for k in range(steps):
+        if k == steps - 1:
+            w_prev = w_ref.copy()  # the weights the last step's spikes come from
+        config0_ref_step(o, torch_, imgs, w_ref, dk)
+    ref_s = (time.perf_counter() - t0) / steps
+    x = imgs.astype(np.float32) / np.float32(255)
+    codes = o.rank_code(o.filter("dog", x[:, None], dk, (3, 3, 3, 3)), T)
+    b_ = codes.shape[0]
+    f = torch_.from_numpy(codes.reshape(b_ * T, 2, 28, 28).astype(np.float32))
+    p1 = torch_.nn.functional.conv2d(f, torch_.from_numpy(w_prev), padding=2).numpy().reshape(b_, T, 30, 28, 28)
+    s_ref = o.fire(o.inhibit(o.threshold(p1, 15.0)))
+    rel = float(np.max(np.abs(w_gpu.astype(np.float64) - w_ref) / np.maximum(np.abs(w_ref), 1e-30)))
+    flops = 2 * T * 784 * 30 * 50
+    peak, peak_source = bf16_peak()
+    layer_ms = ms  # the whole step bounds the fused layer's time from above
+    print(json.dumps({
+        "metric": "images/s (one-layer STDP train + fwd, 64 images) on 1 B200; spike match %",
+        "value": batch / (ms * 1e-3), "unit": "images/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": path_dtype(args.precision)[0], "arithmetic": path_dtype(args.precision)[1],
+        "data": "synthetic (seeded stroke images, MNIST geometry)",
+        "config": {"workload": CFG0_WORKLOAD.replace("64 x", f"{batch} x"), "global_batch": batch, "seq_len": T,
+                   "parallelism": "replicas1", "conv_precision": args.precision,
+                   "l2": "inputs smaller than L2 (the reference's small CPU case): the step's tensors stay in L2"},
+        "e2e": {"value": batch / (e2e_ms * 1e-3), "unit": "images/s", "h2d_bytes_per_step": int(host.numel()),
+                "d2h_bytes_per_step": int(out.numel() * out.element_size())},
+        "gpu_launches": int(launches), "cuda_graph": True,
+        "roofline": {"bound": "tensor", "kernel": "whole step (launch-latency bound at 64 images); algorithmic conv "
+                                                  "FLOPs 35.3 MFLOP/img",
+                     "achieved": flops * batch / (layer_ms * 1e-3) / 1e12, "peak": peak, "unit": "TFLOP/s",
+                     "frac": flops * batch / (layer_ms * 1e-3) / 1e12 / peak, "traffic": None,
+                     "peak_source": peak_source},
+        "spike_match_vs_reference_pct": 100.0 * float(np.mean(spk_last == s_ref)),
+        "weights_max_rel_diff_vs_reference": rel,
+        "cpu_baseline": {"value": batch / ref_s, "unit": "images/s", "cores": torch_.get_num_threads(), "kind": kind,
+                         "sample": f"{steps} steps of the same {batch} images, reference CPU backend + oneDNN "
+                                   f"convolution via torch"},
+        "clocks": clk.summary(),
+    }), flush=True)
+
+
+# ----------------------------------------------------------------------------
 # Large-image forward feature extraction (--workload gabor256)
 # ----------------------------------------------------------------------------
 GABOR_WORKLOAD = ("gabor256-forward: 256 x 256x256 textures, Gabor 4 orientations x 2 wavelengths 11x11, T=30, "
@@ -561,8 +710,9 @@ class GaborNet:
 
 
 def gabor_arm(args, rank, world):
-    """Config-2 style forward pass (no STDP): BF16-split fused layers against
-    the FP32 op-by-op path, potential errors against FP64 on the same GPU."""
+    """Large-image forward pass (no STDP): the fused layers against the FP32
+    op-by-op path and against the oracle's FP64 pipeline, conv1 potential
+    errors against FP64 on the same GPU, and the reference's CPU path."""
     if rank != 0:
         return  # a one-GPU workload: under torchrun only rank 0 runs it
     import torch
@@ -573,7 +723,9 @@ def gabor_arm(args, rank, world):
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
     batch = args.batch if args.batch != BATCH else 256
-    prec = "bf16x2" if args.precision == "bf16x3" else args.precision  # 3 x 256 columns exceed tensor memory
+    # the fused layers take the exact search path (non-negative weights) at
+    # either split precision; the precision names the op-by-op potentials
+    prec = args.precision
     host = torch.from_numpy(synth.textures(batch, seed=2 + rank)).pin_memory()
     imgs = host.to(dev)[:, None]
     net = GaborNet(spyker, torch, dev, prec)
@@ -581,6 +733,7 @@ def gabor_arm(args, rank, world):
         net.step(imgs)
     torch.cuda.synchronize()
     spyker._lib.lib.spk_recheck_count(1)
+    spyker._lib.lib.spk_recompute_count(1)
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with Clocks(dev.index) as clk:
         torch.cuda.synchronize()
@@ -590,6 +743,8 @@ def gabor_arm(args, rank, world):
         b.record()
         torch.cuda.synchronize()
     ms = a.elapsed_time(b) / args.steps
+    rechecks = spyker._lib.lib.spk_recheck_count(1) / args.steps
+    recomputes = spyker._lib.lib.spk_recompute_count(1) / args.steps
     del feats
     # end to end: pinned host images -> first-spike maps of the features on the host
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -613,6 +768,9 @@ def gabor_arm(args, rank, world):
     fp32_ms = f0.elapsed_time(f1)
     got = net.step(imgs[:sub])
     match = float((got == want).float().mean().item()) * 100
+    # against the oracle's FP64 pipeline on a 64x64 texture of the same
+    # generator (at 256x256 the oracle's convolutions take minutes)
+    oracle_match = gabor_oracle_match(spyker, torch, dev, net, prec)
     codes = spyker.code(net.gabor(imgs[:1]), 30)
     pot = spyker.conv(codes, net.conv1.kernel, 1, 3, prec)
     x64 = codes[0].double()
@@ -623,10 +781,11 @@ def gabor_arm(args, rank, world):
     peak, peak_source = bf16_peak()
     achieved = (c1 + c2) * batch / (ms * 1e-3) / 1e12
     print(json.dumps({
-        "metric": "images/s (forward feature extraction), BF16-split vs FP32 on 1 B200; spike match %",
+        "metric": "images/s (forward feature extraction), tensor-core path vs FP32 on 1 B200; spike match %",
         "value": batch / (ms * 1e-3), "unit": "images/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": prec + "-split/f32-acc", "data": "synthetic (seeded 1/f textures + Gaussian blobs, 256x256)",
+        "dtype": path_dtype(prec)[0], "arithmetic": path_dtype(prec)[1],
+        "data": "synthetic (seeded 1/f textures + Gaussian blobs, 256x256)",
         "config": {"workload": GABOR_WORKLOAD.replace("256 x", f"{batch} x"), "global_batch": batch, "seq_len": 30,
                    "parallelism": "replicas1", "conv_precision": prec,
                    "l2": "inputs larger than L2: the layer-1 spikes are 128 MB per image"},
@@ -637,10 +796,70 @@ def gabor_arm(args, rank, world):
                      "peak_source": peak_source},
         "fp32_path": {"value": sub / (fp32_ms * 1e-3), "unit": "images/s", "sample": f"{sub} images"},
         "feature_match_vs_fp32_pct": match,
+        "spike_match_vs_oracle": oracle_match,
         "conv1_potential_max_rel_error_vs_fp64": rel,
-        "near_threshold_rechecks_per_step": spyker._lib.lib.spk_recheck_count(1) / max(args.steps * 2 + 1, 1),
+        "rows_redecided_exactly_per_step": rechecks,
+        "rows_recomputed_per_step": recomputes,
+        "cpu_baseline": gabor_cpu_baseline(args.cpu_seconds, net) if not args.no_cpu_baseline else None,
         "clocks": clk.summary(),
     }), flush=True)
+
+
+def gabor_oracle_match(spyker, torch, dev, net, prec, size=64):
+    """Both layers' spikes and the pooled features of the fused GPU layers
+    against the oracle's FP64 pipeline on one seeded texture."""
+    import oracle
+    from spyker_b200 import synth
+
+    kind = "reference" if oracle.available("reference") else "port"
+    o = oracle.get(kind)
+    img = synth.textures(1, seed=9, size=size)
+    x = torch.from_numpy(img).to(dev)[:, None]
+    codes = spyker.code(net.gabor(x), 30)
+    s1, _, p1 = spyker.conv_fire_wta(codes, net.conv1, 20.0, 0, 0, pool=2)
+    s2, _, p2 = spyker.conv_fire_wta(p1, net.conv2, 12.0, 0, 0, pool=2)
+    hc = codes.cpu().numpy()
+    w1, w2 = net.conv1.kernel.cpu().numpy(), net.conv2.kernel.cpu().numpy()
+    r1 = o.fire(o.inhibit(o.threshold(o.conv(hc, w1, (1, 1), (3, 3, 3, 3)), 20.0)))
+    q1 = o.pool(r1, (2, 2))
+    r2 = o.fire(o.inhibit(o.threshold(o.conv(q1, w2, (1, 1), (2, 2, 2, 2)), 12.0)))
+    q2 = o.pool(r2, (2, 2))
+    return {"layer1_pct": 100.0 * float(np.mean(s1.cpu().numpy() == r1)),
+            "layer2_pct": 100.0 * float(np.mean(s2.cpu().numpy() == r2)),
+            "features_pct": 100.0 * float(np.mean(p2.cpu().numpy() == q2)),
+            "sample": f"1 texture {size}x{size}", "oracle": f"{kind} (FP64 convolution)"}
+
+
+def gabor_cpu_baseline(seconds: float, net) -> dict:
+    """The reference's CPU implementation of the large-image forward pass
+    (its Gabor filter, rank code, threshold / inhibit / fire / pool; oneDNN
+    convolution through torch) on 256x256 textures, one image at a time for
+    a bounded time, with the GPU network's kernels."""
+    o, kind, torch, synth, _ = _ref_setup()
+    gk = net.gabor.kernel.cpu().numpy()
+    w1, w2 = net.conv1.kernel.cpu().numpy(), net.conv2.kernel.cpu().numpy()
+    imgs = synth.textures(4, seed=3)
+    _gabor_ref_step(o, torch, imgs[:1], gk, w1, w2)
+    n, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < seconds and n < 64:
+        _gabor_ref_step(o, torch, imgs[n % 4:n % 4 + 1], gk, w1, w2)
+        n += 1
+    dt = time.perf_counter() - t0
+    return {"value": n / dt, "unit": "images/s", "cores": torch.get_num_threads(), "kind": kind,
+            "sample": f"{n} images of 256x256, one at a time, {dt:.1f} s"}
+
+
+def _gabor_ref_step(o, torch, img, gk, w1, w2):
+    x = o.filter("gabor", img[:, None], gk, (5, 5, 5, 5))
+    codes = o.rank_code(x, 30)
+    b = codes.shape[0]
+    f = torch.from_numpy(codes.reshape(b * 30, 8, 256, 256).astype(np.float32))
+    p1 = torch.nn.functional.conv2d(f, torch.from_numpy(w1), padding=3).numpy().reshape(b, 30, 64, 256, 256)
+    q1 = o.pool(o.fire(o.inhibit(o.threshold(p1, 20.0))), (2, 2))
+    del p1
+    f2 = torch.from_numpy(q1.reshape(b * 30, 64, 128, 128).astype(np.float32))
+    p2 = torch.nn.functional.conv2d(f2, torch.from_numpy(w2), padding=2).numpy().reshape(b, 30, 256, 128, 128)
+    return o.pool(o.fire(o.inhibit(o.threshold(p2, 12.0))), (2, 2))
 
 
 # ----------------------------------------------------------------------------
@@ -717,6 +936,8 @@ def backprop_arm(args, rank, world):
         torch.cuda.synchronize()
         fp32 = {"value": batch / (g0.elapsed_time(g1) * 1e-3), "unit": "images/s", "steps": 1}
     fwd_flops = 2 * 64 * (784 * 32 * 25 + 196 * 64 * 288 + 10 * 3136)
+    peak, peak_source = bf16_peak()
+    fwd_achieved = fwd_flops * batch / (fwd_ms * 1e-3) / 1e12
     line = {
         "metric": "images/s (temporal-backprop training step) on 1 B200",
         "value": batch / (ms * 1e-3), "unit": "images/s", "n_gpus": world, "steps": args.steps,
@@ -731,14 +952,62 @@ def backprop_arm(args, rank, world):
                 "d2h_bytes_per_step": int(loss_host.numel() * loss_host.element_size())},
         "gpu_launches": int(launches),
         "kernels_ms": {"forward_and_loss": fwd_ms, "backward": bwd_ms},
-        "forward_tflops": fwd_flops * batch / (fwd_ms * 1e-3) / 1e12,
+        "roofline": {"bound": "tensor", "kernel": "forward: the 3 fused first-spike layers (dense T-step potentials "
+                                                    "as algorithmic FLOPs, 0.54 GFLOP/img)",
+                     "achieved": fwd_achieved, "peak": peak, "unit": "TFLOP/s", "frac": fwd_achieved / peak,
+                     "traffic": None, "peak_source": peak_source},
         "loss": float(loss_host),
         "outputs_fired_pct": 100.0 * float((t_out < 64).float().mean()),
         "clocks": clk.summary(),
     }
     if fp32 is not None:
         line["fp32_path"] = fp32
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = backprop_cpu_baseline(args.cpu_seconds, net, imgs, labels)
     print(json.dumps(line), flush=True)
+
+
+def backprop_cpu_baseline(seconds: float, net, imgs, labels) -> dict:
+    """The training step on the host cores through the oracle's FP64 NumPy
+    restatement (the reference has no conv backward: its temporal rule exists
+    for fc layers only, cpu/backprop.cpp:105-160), two images at a time for a
+    bounded time, with the GPU network's weights."""
+    import torch
+
+    import oracle
+    from oracle import temporal as ot
+
+    o = oracle.get("port")
+    torch.set_num_threads(os.cpu_count() or 1)
+    T, th, gamma = net.time, net.thresholds, net.gamma
+    w1, w2, w3 = (w.detach().cpu().numpy().astype(np.float64) for w in net.weights)
+    w3c = w3.reshape(w3.shape[0], -1, 1, 1)
+
+    def step(x, y):
+        codes = o.rank_code(x[:, None].astype(np.float32) / 255.0, T)
+        t0 = (T - codes.astype(np.int64).sum(axis=1)).astype(np.float64)
+        a1 = ot.conv_forward(t0, w1, th[0], T, (1, 1), (2, 2, 2, 2))
+        p1 = ot.pool_forward(a1, (2, 2), time=T)
+        a2 = ot.conv_forward(p1, w2, th[1], T, (1, 1), (1, 1, 1, 1))
+        p2 = ot.pool_forward(a2, (2, 2), time=T)
+        f = p2.reshape(p2.shape[0], -1, 1, 1)
+        a3 = ot.conv_forward(f, w3c, th[2], T)
+        g3 = -ot.target_rule(a3[:, :, 0, 0], y, T, gamma)[:, :, None, None]
+        gf, _ = ot.conv_backward(f, w3c, a3, g3)
+        gp2 = ot.pool_backward(a2, gf.reshape(p2.shape), (2, 2))
+        gp1, _ = ot.conv_backward(p1, w2, a2, gp2, (1, 1), (1, 1, 1, 1))
+        ga1 = ot.pool_backward(a1, gp1, (2, 2))
+        ot.conv_backward(t0, w1, a1, ga1, (1, 1), (2, 2, 2, 2))
+
+    step(imgs[:2], labels[:2])
+    n, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < seconds and n < 256:
+        i = n % (imgs.shape[0] - 1)
+        step(imgs[i:i + 2], labels[i:i + 2])
+        n += 2
+    dt = time.perf_counter() - t0
+    return {"value": n / dt, "unit": "images/s", "cores": torch.get_num_threads(), "kind": "port",
+            "sample": f"{n} images, two per step, forward + target rule + backward in FP64 NumPy, {dt:.1f} s"}
 
 
 # ----------------------------------------------------------------------------
@@ -1044,8 +1313,10 @@ def main():
     ap.add_argument("--graph", action="store_true",
                     help="run the headline step as one captured CUDA graph (measured at the eager step's time: "
                          "the kernels dominate and the eager queue already hides the launches)")
-    ap.add_argument("--workload", default="kheradpisheh", choices=["kheradpisheh", "gabor256", "backprop", "sweep", "sparse", "rstdp"],
-                    help="kheradpisheh: the 2-layer STDP training step (the headline); gabor256: large-image "
+    ap.add_argument("--workload", default="kheradpisheh", choices=["kheradpisheh", "config0", "gabor256", "backprop", "sweep", "sparse",
+                                                                   "rstdp"],
+                    help="kheradpisheh: the 2-layer STDP training step (the headline); config0: the one-layer "
+                         "STDP step on 64 images against the reference's CPU path; gabor256: large-image "
                          "forward; backprop: temporal-backprop training of a 3-layer first-spike network; "
                          "sweep: 32 STDP networks on uneven image sizes in one CUDA graph; sparse: the event-list "
                          "path at 1-5 % input density; rstdp: the reward-modulated layer of the Mozafari network")
@@ -1054,6 +1325,8 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", args.gpus if args.impl == "reference" else 1))
     if args.impl == "reference":
         reference_arm(args, rank, world)
+    elif args.workload == "config0":
+        config0_arm(args, rank, world)
     elif args.workload == "gabor256":
         gabor_arm(args, rank, world)
     elif args.workload == "backprop":
