@@ -2862,6 +2862,11 @@ FusedLayout fused_layout(int64_t b, int64_t t, int64_t cin, int64_t h, int64_t w
     L.oh = (h + p.top + p.bottom - kh) / sy + 1;
     L.ow = (w + p.left + p.right - kw) / sx + 1;
     L.pl = make_plan(b * t, cin, h, w, cout, kh, kw, precision, true, t, false, 0, nnets == 1);
+    // three-term accumulators of more than 170 channels exceed the 512
+    // tensor-memory columns: the dense kernel then keeps two terms (its
+    // near-threshold rows are re-decided in FP64 at either split)
+    if (precision == SPK_CONV_BF16X3 && L.pl.nsplit * L.pl.n_tile > 512)
+        L.pl = make_plan(b * t, cin, h, w, cout, kh, kw, SPK_CONV_BF16X2, true, t, false, 0, nnets == 1);
     int tp = 1, lg = 0;
     while (tp < t) tp <<= 1, ++lg;
     L.tp_log2 = lg;

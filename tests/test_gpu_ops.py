@@ -516,12 +516,14 @@ def test_fused_layer_matches_ops(port, case, prec):
     assert int(got[1].sum()) > 0
 
 
+@pytest.mark.parametrize("cout", [20, 256])
 @pytest.mark.parametrize("kind", ["negative_weights", "value_above_threshold"])
-def test_fused_layer_general_argmax(kind):
+def test_fused_layer_general_argmax(kind, cout):
     """Negative weights, or a threshold value above the threshold, take the
     epilogue's general argmax (the lean one needs neither); results equal
-    the op-by-op pipeline."""
-    b, t, cin, h, w, cout = 6, 15, 4, 12, 11, 20
+    the op-by-op pipeline.  At 256 channels the three-term accumulators do
+    not fit the tensor memory and the dense kernel runs with two terms."""
+    b, t, cin, h, w = 6, 15, 4, 12, 11
     rng = np.random.default_rng(11 if kind == "negative_weights" else 12)
     fst = rng.integers(0, t + 4, size=(b, cin, h, w))
     x = cuda((fst[:, None] <= np.arange(t)[None, :, None, None, None]).astype(np.uint8))
