@@ -256,7 +256,14 @@ spk_status spk_conv(const void *in, spk_dtype itype, const float *kernel, float 
  * OW / pool_kx] U8; pooled may be null when pool_ky == 0.  count == 0
  * skips the winner selection (winners and counts may then be null).  The
  * workspace query returns 0 for layers whose accumulators (terms x Cout,
- * Cout rounded up to 16) exceed the 512 tensor-memory columns of a CTA. */
+ * Cout rounded up to 16) exceed the 512 tensor-memory columns of a CTA even
+ * with two terms (a three-term request above 170 channels keeps two: every
+ * near-threshold decision is re-made exactly at either split).  With no
+ * negative weight, cumulative 0/1 input and value <= the inhibit / fire / WTA
+ * thresholds <= threshold, the layer runs as a first-crossing search on u8
+ * weight digits (exact integer sums) instead of the dense kernel; results
+ * are the same.  spk_recheck_count / spk_recompute_count count its rows
+ * re-decided from exact sums and recomputed from the F32 weights. */
 size_t spk_conv_fire_wta_workspace(int64_t b, int64_t t, int64_t cin, int64_t h, int64_t w, int64_t cout, int64_t kh,
                                    int64_t kw, int64_t sy, int64_t sx, const int64_t *pad4_host, int precision);
 spk_status spk_conv_fire_wta(const void *in, spk_dtype itype, const float *kernel, int64_t b, int64_t t, int64_t cin,

@@ -1,0 +1,651 @@
+/* C++ layer of spyker_b200: the reference's `Spyker::` API for the dense
+ * spiking-CNN hot path (src/spyker/opers.h:130-760, src/spyker/utils.h:96-524),
+ * header-only, over the C ABI of spyker_b200.h.
+ *
+ * Same names, argument order, defaults and error conditions as the reference
+ * for: Tensor (device tensors only), Expand2 / Expand4, DoGFilter, DoG, Conv
+ * (operator(), stdp), STDPConfig, Winner / Winners, code, threshold,
+ * infinite, fire, gather, scatter, pad, pool, inhibit, convwta, fcwta, conv.
+ * Tensors live in the current CUDA device's memory; the reference's host
+ * tensors become Tensor::from_host / Tensor::to_host.  Every call is queued on
+ * Spyker::stream() (the legacy default stream unless set), so calls run in
+ * program order; functions that return host data (convwta, fcwta, to_host)
+ * wait for the stream.  Errors throw Spyker::Error with the library's message
+ * (the reference's SpykerCompare / SpykerAssert throw std::runtime_error).
+ *
+ * Not a counterpart of the reference: conv_fire_wta, the fused layer
+ * (conv -> threshold -> inhibit -> fire + convwta [+ pool]) of
+ * spk_conv_fire_wta, with the op-by-op composition as its fallback.
+ *
+ * Link: -lspyker_b200 -lcudart (spyker_b200/lib). */
+#ifndef SPYKER_B200_HPP
+#define SPYKER_B200_HPP
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "spyker_b200.h"
+
+namespace Spyker
+{
+using Size = int64_t;
+using F64 = double;
+using Shape = std::vector<Size>;
+
+/* utils.h:96-120: the same order as spk_dtype. */
+enum class Type : int32_t
+{
+    I8,
+    I16,
+    I32,
+    I64,
+    U8,
+    U16,
+    U32,
+    U64,
+    F16,
+    F32,
+    F64
+};
+
+struct Error : std::runtime_error
+{
+    using std::runtime_error::runtime_error;
+};
+
+namespace detail
+{
+inline cudaStream_t &stream_ref()
+{
+    static thread_local cudaStream_t s = nullptr;
+    return s;
+}
+
+inline void check(spk_status s, const char *what)
+{
+    if (s != SPK_OK) throw Error(std::string(what) + ": " + spk_last_error());
+}
+
+inline void cuda(cudaError_t e, const char *what)
+{
+    if (e != cudaSuccess) throw Error(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+inline void require(bool ok, const char *msg)
+{
+    if (!ok) throw Error(msg);
+}
+
+inline size_t type_size(Type t)
+{
+    static const size_t sz[] = {1, 2, 4, 8, 1, 2, 4, 8, 2, 4, 8};
+    return sz[int(t)];
+}
+
+inline Size prod(const Shape &s, size_t from = 0, size_t to = size_t(-1))
+{
+    Size p = 1;
+    for (size_t i = from; i < s.size() && i < to; ++i) p *= s[i];
+    return p;
+}
+
+/* Stream-ordered scratch of one call (freed on the same stream). */
+struct Scratch
+{
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    explicit Scratch(size_t n) : bytes(n)
+    {
+        if (n > 0) cuda(cudaMallocAsync(&ptr, n, stream_ref()), "workspace allocation");
+    }
+    ~Scratch()
+    {
+        if (ptr) cudaFreeAsync(ptr, stream_ref());
+    }
+    Scratch(const Scratch &) = delete;
+    Scratch &operator=(const Scratch &) = delete;
+};
+}  // namespace detail
+
+/* The stream every call of this layer is queued on. */
+inline cudaStream_t stream() { return detail::stream_ref(); }
+inline void setStream(cudaStream_t s) { detail::stream_ref() = s; }
+inline void synchronize() { detail::cuda(cudaStreamSynchronize(stream()), "synchronize"); }
+
+/* opers.h:130-142: one value for both, or (y, x). */
+class Expand2
+{
+    Shape data;
+
+public:
+    Expand2() : data{0, 0} {}
+    Expand2(Size a) : data{a, a} {}
+    Expand2(Size a, Size b) : data{a, b} {}
+    Size operator[](Size i) const { return data[size_t(i)]; }
+    Shape get() const { return data; }
+};
+
+/* opers.h:147-160: (top, left, bottom, right); two values = (y, x). */
+class Expand4
+{
+    Shape data;
+
+public:
+    Expand4() : data{0, 0, 0, 0} {}
+    Expand4(Size a) : data{a, a, a, a} {}
+    Expand4(Size a, Size b) : data{a, b, a, b} {}
+    Expand4(Size a, Size b, Size c, Size d) : data{a, b, c, d} {}
+    Size operator[](Size i) const { return data[size_t(i)]; }
+    Shape get() const { return data; }
+};
+
+/* A dense tensor in device memory (the reference's Tensor on a CUDA
+ * device, utils.h / base.h).  Copies share the buffer, as there. */
+class Tensor
+{
+    std::shared_ptr<void> _data;
+    Shape _shape;
+    Type _type = Type::F32;
+
+public:
+    Tensor() = default;
+    Tensor(Type type, const Shape &shape) : _shape(shape), _type(type)
+    {
+        for (Size d : shape) detail::require(d >= 0, "Tensor shape can't be negative.");
+        void *p = nullptr;
+        const size_t n = size_t(detail::prod(shape)) * detail::type_size(type);
+        detail::cuda(cudaMalloc(&p, n > 0 ? n : 1), "Tensor allocation");
+        detail::cuda(cudaMemsetAsync(p, 0, n, stream()), "Tensor initialisation");
+        _data = std::shared_ptr<void>(p, [](void *q) { cudaFree(q); });
+    }
+    explicit Tensor(const Shape &shape, Type type = Type::F32) : Tensor(type, shape) {}
+
+    static Tensor from_host(const void *host, Type type, const Shape &shape)
+    {
+        Tensor t(type, shape);
+        detail::cuda(cudaMemcpyAsync(t.data(), host, t.bytes(), cudaMemcpyHostToDevice, stream()), "Tensor upload");
+        detail::cuda(cudaStreamSynchronize(stream()), "Tensor upload");
+        return t;
+    }
+    void to_host(void *host) const
+    {
+        detail::cuda(cudaMemcpyAsync(host, data(), bytes(), cudaMemcpyDeviceToHost, stream()), "Tensor download");
+        detail::cuda(cudaStreamSynchronize(stream()), "Tensor download");
+    }
+    template <typename T>
+    std::vector<T> to_vector() const
+    {
+        detail::require(sizeof(T) == detail::type_size(_type), "Tensor element size mismatch.");
+        std::vector<T> v(static_cast<size_t>(numel()));
+        if (!v.empty()) to_host(v.data());
+        return v;
+    }
+
+    bool valid() const { return bool(_data); }
+    void *data() const { return _data.get(); }
+    template <typename T>
+    T *data() const
+    {
+        return static_cast<T *>(_data.get());
+    }
+    Type type() const { return _type; }
+    Shape shape() const { return _shape; }
+    Size shape(Size i) const { return _shape[size_t(i)]; }
+    Size dims() const { return Size(_shape.size()); }
+    Size numel() const { return detail::prod(_shape); }
+    size_t bytes() const { return size_t(numel()) * detail::type_size(_type); }
+    Tensor reshape(const Shape &shape) const
+    {
+        detail::require(detail::prod(shape) == numel(), "Tensor reshape can't change the element count.");
+        Tensor t = *this;
+        t._shape = shape;
+        return t;
+    }
+    Tensor copy() const
+    {
+        Tensor t(_type, _shape);
+        detail::cuda(cudaMemcpyAsync(t.data(), data(), bytes(), cudaMemcpyDeviceToDevice, stream()), "Tensor copy");
+        return t;
+    }
+};
+
+/* utils.h:483-502. */
+struct Winner
+{
+    Size c, t, z, y, x;
+};
+using Winners = std::vector<std::vector<Winner>>;
+
+/* utils.h:505-524. */
+struct STDPConfig
+{
+    F64 positive = 0, negative = 0;
+    bool stabilize = true;
+    F64 lower = 0, upper = 1;
+    STDPConfig() {}
+    STDPConfig(F64 positive, F64 negative, bool stabilize = true, F64 lower = 0, F64 upper = 1)
+        : positive(positive), negative(negative), stabilize(stabilize), lower(lower), upper(upper)
+    {
+    }
+};
+
+/* opers.h:163-174. */
+struct DoGFilter
+{
+    F64 std1, std2;
+    DoGFilter(F64 std1, F64 std2) : std1(std1), std2(std2) {}
+};
+
+namespace detail
+{
+inline spk_dtype dt(Type t) { return spk_dtype(int(t)); }
+
+inline std::vector<int64_t> pad4(const Expand4 &p) { return {p[0], p[1], p[2], p[3]}; }
+
+/* [B, count, 5] int32 records + counts [B] -> nested winners (one copy). */
+inline Winners winners_from(const Tensor &records, const Tensor &counts, Size count)
+{
+    const Size b = counts.numel();
+    std::vector<int32_t> rec = records.to_vector<int32_t>(), cnt = counts.to_vector<int32_t>();
+    Winners w(static_cast<size_t>(b));
+    for (Size i = 0; i < b; ++i)
+        for (Size j = 0; j < cnt[size_t(i)] && j < count; ++j)
+        {
+            const int32_t *r = &rec[size_t((i * count + j) * 5)];
+            w[size_t(i)].push_back(Winner{r[0], r[1], r[2], r[3], r[4]});
+        }
+    return w;
+}
+
+/* Nested winners -> device records [B, count, 5] and counts [B]. */
+inline std::pair<Tensor, Tensor> winners_to(const Winners &w, Size batch, Size &count)
+{
+    require(Size(w.size()) == batch, "Winners count must match the input batch.");
+    count = 1;
+    for (const auto &v : w) count = std::max<Size>(count, Size(v.size()));
+    std::vector<int32_t> rec(static_cast<size_t>(batch * count * 5), 0), cnt(static_cast<size_t>(batch), 0);
+    for (Size i = 0; i < batch; ++i)
+    {
+        cnt[size_t(i)] = int32_t(w[size_t(i)].size());
+        for (size_t j = 0; j < w[size_t(i)].size(); ++j)
+        {
+            const Winner &x = w[size_t(i)][j];
+            int32_t *r = &rec[size_t((i * count + Size(j)) * 5)];
+            r[0] = int32_t(x.c), r[1] = int32_t(x.t), r[2] = int32_t(x.z), r[3] = int32_t(x.y), r[4] = int32_t(x.x);
+        }
+    }
+    return {Tensor::from_host(rec.data(), Type::I32, {batch, count, 5}),
+            Tensor::from_host(cnt.data(), Type::I32, {batch})};
+}
+
+inline std::vector<F64> configs(const std::vector<STDPConfig> &c)
+{
+    std::vector<F64> v;
+    for (const auto &x : c) v.insert(v.end(), {x.positive, x.negative, F64(x.stabilize), x.lower, x.upper});
+    return v;
+}
+}  // namespace detail
+
+/* ---- coding and elementwise (opers.h:598-700) ----------------------------- */
+
+/* [B, ...] -> [B, T, ...] cumulative spikes; sort: rank order (opers.cpp code). */
+inline Tensor code(Tensor input, Size time, bool sort = true, Type type = Type::U8)
+{
+    detail::require(time > 0, "Input time can't be less than 1.");
+    detail::require(input.dims() >= 2, "Input dimensions must be at least 2.");
+    const Shape s = input.shape();
+    Shape o{s[0], time};
+    o.insert(o.end(), s.begin() + 1, s.end());
+    Tensor out(type, o);
+    const Size x = detail::prod(s, 1);
+    detail::Scratch ws(spk_rank_code_workspace(s[0], x, int(sort)));
+    detail::check(spk_rank_code(input.data(), detail::dt(input.type()), out.data(), detail::dt(type), s[0], time, x,
+                                int(sort), ws.ptr, ws.bytes, stream()),
+                  "code");
+    return out;
+}
+
+inline Tensor threshold(Tensor input, F64 threshold, F64 value = 0, bool inplace = true)
+{
+    Tensor t = inplace ? input : input.copy();
+    detail::check(spk_threshold(t.data(), detail::dt(t.type()), t.numel(), threshold, value, stream()), "threshold");
+    return t;
+}
+
+/* [B, T, ...]: steps 0 .. T-2 set to value (cpu/fire.cpp). */
+inline Tensor infinite(Tensor input, F64 value = 0, bool inplace = true)
+{
+    detail::require(input.dims() >= 3, "Input dimensions must be at least 3.");
+    Tensor t = inplace ? input : input.copy();
+    detail::check(spk_rank_infinite(t.data(), detail::dt(t.type()), t.shape(0), t.shape(1),
+                                    detail::prod(t.shape(), 2), value, stream()),
+                  "infinite");
+    return t;
+}
+
+inline Tensor fire(Tensor input, F64 threshold = 0, Type type = Type::U8)
+{
+    Tensor out(type, input.shape());
+    detail::check(spk_rank_fire(input.data(), detail::dt(input.type()), out.data(), detail::dt(type), input.numel(),
+                                threshold, stream()),
+                  "fire");
+    return out;
+}
+
+/* [B, T, ...] -> [B, ...] first step above the threshold (T when none). */
+inline Tensor gather(Tensor input, F64 threshold = 0, Type type = Type::U8)
+{
+    detail::require(input.dims() >= 3, "Input dimensions must be at least 3.");
+    Shape o{input.shape(0)};
+    const Shape s = input.shape();
+    o.insert(o.end(), s.begin() + 2, s.end());
+    Tensor out(type, o);
+    detail::check(spk_rank_gather(input.data(), detail::dt(input.type()), out.data(), detail::dt(type), s[0], s[1],
+                                  detail::prod(s, 2), threshold, stream()),
+                  "gather");
+    return out;
+}
+
+/* [B, ...] first-spike times -> [B, T, ...] cumulative spikes. */
+inline Tensor scatter(Tensor input, Size time, Type type = Type::U8)
+{
+    detail::require(time > 0, "Input time can't be less than 1.");
+    const Shape s = input.shape();
+    Shape o{s[0], time};
+    o.insert(o.end(), s.begin() + 1, s.end());
+    Tensor out(type, o);
+    detail::check(spk_rank_scatter(input.data(), detail::dt(input.type()), out.data(), detail::dt(type), s[0], time,
+                                   detail::prod(s, 1), stream()),
+                  "scatter");
+    return out;
+}
+
+/* [..., H, W] -> [..., H + top + bottom, W + left + right]. */
+inline Tensor pad(Tensor input, Expand4 pad, F64 value = 0)
+{
+    detail::require(input.dims() >= 2, "Input dimensions must be at least 2.");
+    detail::require(pad[0] >= 0 && pad[1] >= 0 && pad[2] >= 0 && pad[3] >= 0, "Pad items are incorrect.");
+    Shape o = input.shape();
+    const Size h = o[o.size() - 2], w = o[o.size() - 1];
+    o[o.size() - 2] = h + pad[0] + pad[2], o[o.size() - 1] = w + pad[1] + pad[3];
+    Tensor out(input.type(), o);
+    const auto p = detail::pad4(pad);
+    detail::check(spk_pad(input.data(), out.data(), detail::dt(input.type()), input.numel() / (h * w), h, w, p.data(),
+                          value, stream()),
+                  "pad");
+    return out;
+}
+
+/* Max pooling of the last two dimensions; stride 0 = the window
+ * (opers.h:709, cpu/pool.cpp:53-86). */
+inline Tensor pool(Tensor input, Expand2 kernel, Expand2 stride = 0, Expand4 pad = 0)
+{
+    detail::require(input.dims() >= 3, "Input dimensions must be at least 3.");
+    if (stride[0] == 0 && stride[1] == 0) stride = kernel;
+    detail::require(kernel[0] > 0 && kernel[1] > 0 && stride[0] > 0 && stride[1] > 0 && pad[0] >= 0 && pad[1] >= 0 &&
+                        pad[2] >= 0 && pad[3] >= 0,
+                    "Kernel, stride or pad items are incorrect.");
+    Shape o = input.shape();
+    const Size h = o[o.size() - 2], w = o[o.size() - 1];
+    const Size oh = (h + pad[0] + pad[2] - kernel[0]) / stride[0] + 1;
+    const Size ow = (w + pad[1] + pad[3] - kernel[1]) / stride[1] + 1;
+    detail::require(oh > 0 && ow > 0, "Input and kernel shapes are not compatible.");
+    o[o.size() - 2] = oh, o[o.size() - 1] = ow;
+    Tensor out(input.type(), o);
+    const auto p = detail::pad4(pad);
+    detail::check(spk_rank_pool(input.data(), out.data(), detail::dt(input.type()), input.numel() / (h * w), h, w, oh,
+                                ow, kernel[0], kernel[1], stride[0], stride[1], p.data(), stream()),
+                  "pool");
+    return out;
+}
+
+/* [B, T, C, ...] lateral inhibition (cpu/inhibit.cpp:41-121). */
+inline Tensor inhibit(Tensor input, F64 threshold = 0, bool inplace = true)
+{
+    detail::require(input.dims() >= 4, "Input dimensions must be at least 4.");
+    Tensor t = inplace ? input : input.copy();
+    const Shape s = t.shape();
+    detail::check(spk_rank_inhibit(t.data(), detail::dt(t.type()), s[0], s[1], s[2], detail::prod(s, 3), threshold,
+                                   stream()),
+                  "inhibit");
+    return t;
+}
+
+/* [B, T, C, H, W] -> up to count winners per sample (cpu/wta.cpp:123-152). */
+inline Winners convwta(Tensor input, Expand2 radius, Size count, F64 threshold = 0)
+{
+    detail::require(input.dims() == 5, "Input dimensions must be 5.");
+    detail::require(count >= 0 && radius[0] >= 0 && radius[1] >= 0, "Winners count or radius are incorrect.");
+    const Shape s = input.shape();
+    if (count == 0) return Winners(size_t(s[0]));
+    Tensor rec(Type::I32, {s[0], count, 5}), cnt(Type::I32, {s[0]});
+    detail::Scratch ws(spk_rank_convwta_workspace(s[0], s[1], s[2], s[3], s[4]));
+    detail::check(spk_rank_convwta(input.data(), detail::dt(input.type()), s[0], s[1], s[2], s[3], s[4], radius[0],
+                                   radius[1], count, threshold, rec.data<int32_t>(), cnt.data<int32_t>(), ws.ptr,
+                                   ws.bytes, stream()),
+                  "convwta");
+    return detail::winners_from(rec, cnt, count);
+}
+
+/* [B, T, N] -> up to count winners per sample (cpu/wta.cpp:72-96). */
+inline Winners fcwta(Tensor input, Size radius, Size count, F64 threshold = 0)
+{
+    detail::require(input.dims() == 3, "Input dimensions must be 3.");
+    detail::require(count >= 0 && radius >= 0, "Winners count or radius are incorrect.");
+    const Shape s = input.shape();
+    if (count == 0) return Winners(size_t(s[0]));
+    Tensor rec(Type::I32, {s[0], count, 5}), cnt(Type::I32, {s[0]});
+    detail::Scratch ws(spk_rank_fcwta_workspace(s[0], s[1], s[2]));
+    detail::check(spk_rank_fcwta(input.data(), detail::dt(input.type()), s[0], s[1], s[2], radius, count, threshold,
+                                 rec.data<int32_t>(), cnt.data<int32_t>(), ws.ptr, ws.bytes, stream()),
+                  "fcwta");
+    return detail::winners_from(rec, cnt, count);
+}
+
+/* ---- convolution (opers.h:545-555) ------------------------------------------ */
+
+/* [B, T, Cin, H, W] (or [N, Cin, H, W]) x [Cout, Cin, KH, KW] F32 ->
+ * F32 potentials [B, T, Cout, OH, OW]. */
+inline Tensor conv(Tensor input, Tensor kernel, Expand2 stride = 1, Expand4 pad = 0,
+                   int precision = SPK_CONV_FP32)
+{
+    detail::require(input.dims() == 4 || input.dims() == 5, "Input dimensions must be 4 or 5.");
+    detail::require(kernel.dims() == 4 && kernel.type() == Type::F32, "Kernel must be a 4D F32 tensor.");
+    detail::require(stride[0] > 0 && stride[1] > 0 && pad[0] >= 0 && pad[1] >= 0 && pad[2] >= 0 && pad[3] >= 0,
+                    "Stride or pad items are incorrect.");
+    const Shape s = input.shape();
+    const size_t d = s.size();
+    const Size cin = s[d - 3], h = s[d - 2], w = s[d - 1];
+    const Size cout = kernel.shape(0), kh = kernel.shape(2), kw = kernel.shape(3);
+    detail::require(kernel.shape(1) == cin, "Input and kernel channels are not compatible.");
+    const Size oh = (h + pad[0] + pad[2] - kh) / stride[0] + 1, ow = (w + pad[1] + pad[3] - kw) / stride[1] + 1;
+    detail::require(oh > 0 && ow > 0, "Input and kernel shapes are not compatible.");
+    Shape o(s.begin(), s.end() - 3);
+    o.insert(o.end(), {cout, oh, ow});
+    Tensor out(Type::F32, o);
+    const Size n = detail::prod(s, 0, d - 3);
+    const auto p = detail::pad4(pad);
+    detail::Scratch ws(spk_conv_workspace(n, cin, h, w, cout, kh, kw, precision));
+    detail::check(spk_conv(input.data(), detail::dt(input.type()), kernel.data<float>(), out.data<float>(), n, cin, h, w,
+                           cout, kh, kw, stride[0], stride[1], p.data(), precision, ws.ptr, ws.bytes, stream()),
+                  "conv");
+    return out;
+}
+
+/* ---- modules (opers.h:211-456) ---------------------------------------------- */
+
+/* Difference-of-Gaussians bank, window 2 size + 1: [B, C, H, W] ->
+ * [B, C F, OH, OW] (cpu/dog.cpp). */
+class DoG
+{
+    Expand4 _pad;
+
+public:
+    Tensor kernel;  // F32 [2, F, 2 size + 1, 2 size + 1]
+
+    DoG() {}
+    DoG(Size size, const std::vector<DoGFilter> &filters, Expand4 pad = 0) : _pad(pad)
+    {
+        detail::require(size > 0, "Input size can't be less than 1.");
+        detail::require(!filters.empty(), "Input filters count can't be less then 1.");
+        detail::require(pad[0] >= 0 && pad[1] >= 0 && pad[2] >= 0 && pad[3] >= 0, "Pad items are incorrect.");
+        const Size n = 2 * size + 1, f = Size(filters.size());
+        std::vector<double> g(static_cast<size_t>(n * n));
+        std::vector<float> k(static_cast<size_t>(2 * f * n * n));
+        for (Size i = 0; i < f; ++i)
+            for (int which = 0; which < 2; ++which)
+            {
+                detail::check(spk_gaussian_kernel(g.data(), n, which ? filters[size_t(i)].std2 : filters[size_t(i)].std1),
+                              "DoG kernel");
+                for (Size j = 0; j < n * n; ++j) k[size_t((which * f + i) * n * n + j)] = float(g[size_t(j)]);
+            }
+        kernel = Tensor::from_host(k.data(), Type::F32, {2, f, n, n});
+    }
+
+    Tensor operator()(Tensor input)
+    {
+        detail::require(kernel.valid(), "DoG is not initialized.");
+        detail::require(input.dims() == 4, "Input dimensions must be 4.");
+        detail::require(input.type() == Type::F32, "DoG takes F32 input.");
+        const Tensor &x = input;
+        const Shape s = x.shape();
+        const Size f = kernel.shape(1), kh = kernel.shape(2), kw = kernel.shape(3);
+        const Size oh = s[2] + _pad[0] + _pad[2] - kh + 1, ow = s[3] + _pad[1] + _pad[3] - kw + 1;
+        detail::require(oh > 0 && ow > 0, "Input and kernel shapes are not compatible.");
+        Tensor out(Type::F32, {s[0], s[1] * f, oh, ow});
+        const auto p = detail::pad4(_pad);
+        detail::check(spk_filter(0, x.data<float>(), kernel.data<float>(), out.data<float>(), s[0] * s[1], s[2], s[3], f,
+                                 kh, kw, oh, ow, p.data(), stream()),
+                      "DoG");
+        return out;
+    }
+};
+
+/* 2D convolution module with STDP (opers.h:378-456, cpu/stdp.cpp:99-169). */
+class Conv
+{
+    Expand2 _stride;
+    Expand4 _pad;
+
+public:
+    Tensor kernel;  // F32 [Cout, Cin, KH, KW]
+    std::vector<STDPConfig> stdpconfig;
+    int precision = SPK_CONV_FP32;  // SPK_CONV_BF16X2 / X3: the tensor-core paths
+
+    Conv() {}
+    Conv(Size input, Size output, Expand2 kernel_, Expand2 stride = 1, Expand4 pad = 0, F64 mean = .5, F64 std = .02)
+        : _stride(stride), _pad(pad)
+    {
+        detail::require(input > 0 && output > 0, "Input or output channels can't be less than 1.");
+        detail::require(kernel_[0] > 0 && kernel_[1] > 0 && stride[0] > 0 && stride[1] > 0 && pad[0] >= 0 &&
+                            pad[1] >= 0 && pad[2] >= 0 && pad[3] >= 0,
+                        "Kernel, stride or pad items are incorrect.");
+        const Size n = output * input * kernel_[0] * kernel_[1];
+        std::vector<double> w(static_cast<size_t>(n));
+        detail::check(spk_normal_kernel(w.data(), n, mean, std), "Conv kernel");
+        std::vector<float> f(w.begin(), w.end());
+        kernel = Tensor::from_host(f.data(), Type::F32, {output, input, kernel_[0], kernel_[1]});
+    }
+
+    Expand2 stride() const { return _stride; }
+    Expand4 pad() const { return _pad; }
+
+    Tensor operator()(Tensor input)
+    {
+        detail::require(kernel.valid(), "Conv is not initialized.");
+        return conv(input, kernel, _stride, _pad, precision);
+    }
+
+    /* input [B, T, Cin, H, W] spikes, output [B, T, Cout, OH, OW] spikes. */
+    void stdp(Tensor input, const Winners &winners, Tensor output)
+    {
+        detail::require(!stdpconfig.empty(), "At least one STDP Config must be given.");
+        detail::require(input.dims() == 5 && output.dims() == 5, "Input and output dimensions must be 5.");
+        const Shape s = input.shape(), o = output.shape();
+        for (const auto &v : winners)
+            for (const auto &x : v)
+                detail::require(x.c >= 0 && x.c < Size(stdpconfig.size()), "Winner STDP config index out of range.");
+        Size count = 0;
+        auto rc = detail::winners_to(winners, s[0], count);
+        const auto cfg = detail::configs(stdpconfig);
+        const auto p = detail::pad4(_pad);
+        detail::Scratch ws(spk_rank_convstdp_workspace(s[0], count, s[2], s[3], s[4], kernel.shape(2), kernel.shape(3)));
+        detail::check(spk_rank_convstdp(input.data(), detail::dt(input.type()), s[0], s[1], s[2], s[3], s[4],
+                                        kernel.data<float>(), kernel.shape(0), kernel.shape(2), kernel.shape(3),
+                                        output.data(), o[3], o[4], cfg.data(), Size(stdpconfig.size()),
+                                        rc.first.data<int32_t>(), rc.second.data<int32_t>(), count, _stride[0],
+                                        _stride[1], p.data(), ws.ptr, ws.bytes, stream()),
+                      "Conv::stdp");
+        synchronize();  // the host winner arrays are freed on return
+    }
+};
+
+/* ---- the fused layer (spyker_b200 only) ------------------------------------ */
+
+struct LayerOutput
+{
+    Tensor spikes;    // U8 [B, T, Cout, OH, OW]
+    Winners winners;  // convwta of the inhibited potentials
+    Tensor pooled;    // U8 [B, T, Cout, OH / py, OW / px] when a pool window is given
+};
+
+/* spikes = fire(out), winners = convwta(out, radius, count) and, with a pool
+ * window, pooled = pool(spikes, window) for out = inhibit(threshold(conv(input),
+ * threshold)): one tensor-core kernel on the BF16 precisions (the potentials
+ * never reach memory), else the ops one by one. */
+inline LayerOutput conv_fire_wta(Tensor input, Conv &layer, F64 threshold, Expand2 radius, Size count,
+                                 Expand2 pool_window = 0)
+{
+    detail::require(input.dims() == 5, "Input dimensions must be 5.");
+    detail::require(count >= 0 && radius[0] >= 0 && radius[1] >= 0, "Winners count or radius are incorrect.");
+    const Shape s = input.shape();
+    const Size cout = layer.kernel.shape(0), cin = s[2], kh = layer.kernel.shape(2), kw = layer.kernel.shape(3);
+    const Expand2 st = layer.stride();
+    const Expand4 pd = layer.pad();
+    const auto p = detail::pad4(pd);
+    const bool pooled = pool_window[0] > 0 && pool_window[1] > 0;
+    size_t nb = 0;
+    bool fused = layer.precision != SPK_CONV_FP32 && input.type() == Type::U8 && s[1] <= 32 && cout >= 2;
+    if (fused)
+    {
+        Size tp = 1;
+        while (tp < s[1]) tp <<= 1;
+        nb = spk_conv_fire_wta_workspace(s[0], s[1], cin, s[3], s[4], cout, kh, kw, st[0], st[1], p.data(),
+                                         layer.precision);
+        fused = nb > 0 && s[1] * cout * (128 / tp) <= 32768;
+    }
+    LayerOutput r;
+    if (!fused)
+    {
+        Tensor out = inhibit(Spyker::threshold(layer(input), threshold));
+        r.spikes = fire(out);
+        r.winners = count > 0 ? convwta(out, radius, count) : Winners(size_t(s[0]));
+        if (pooled) r.pooled = pool(r.spikes, pool_window);
+        return r;
+    }
+    const Size oh = (s[3] + pd[0] + pd[2] - kh) / st[0] + 1, ow = (s[4] + pd[1] + pd[3] - kw) / st[1] + 1;
+    r.spikes = Tensor(Type::U8, {s[0], s[1], cout, oh, ow});
+    if (pooled) r.pooled = Tensor(Type::U8, {s[0], s[1], cout, oh / pool_window[0], ow / pool_window[1]});
+    Tensor rec, cnt;
+    if (count > 0) rec = Tensor(Type::I32, {s[0], count, 5}), cnt = Tensor(Type::I32, {s[0]});
+    detail::Scratch ws(nb);
+    detail::check(spk_conv_fire_wta(input.data(), SPK_U8, layer.kernel.data<float>(), s[0], s[1], cin, s[3], s[4], cout,
+                                    kh, kw, st[0], st[1], p.data(), threshold, 0.0, 0.0, 0.0, radius[0], radius[1],
+                                    count, 0.0, r.spikes.data<uint8_t>(),
+                                    count > 0 ? rec.data<int32_t>() : nullptr, count > 0 ? cnt.data<int32_t>() : nullptr,
+                                    pooled ? pool_window[0] : 0, pooled ? pool_window[1] : 0,
+                                    pooled ? r.pooled.data<uint8_t>() : nullptr, layer.precision, ws.ptr, ws.bytes,
+                                    stream()),
+                  "conv_fire_wta");
+    r.winners = count > 0 ? detail::winners_from(rec, cnt, count) : Winners(size_t(s[0]));
+    return r;
+}
+}  // namespace Spyker
+
+#endif

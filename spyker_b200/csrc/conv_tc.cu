@@ -2108,10 +2108,11 @@ __global__ void search_init_kernel(unsigned *mins, unsigned *maxs, int64_t b, co
 // Pre-filter of round 0 for layers with few inputs per output: with no
 // negative weight, a pixel's potential at T - 1 is at most U, the sum over the
 // inputs that fired of their largest weight over the channels.  A pixel with
-// U (FP64, widened by K 2^-50 for the roundings of U and of the oracle's own
-// sum) at or below the threshold never fires and is settled here; the others
-// go to round 0's list.  One thread per output pixel, reading the first-spike
-// map through the L1 cache.
+// U at or below the threshold never fires and is settled here; the others go
+// to round 0's list.  U is summed in FP32 (non-negative terms) and multiplied,
+// rounding up, by 1 + (K + 2) 2^-23, which covers the roundings of that sum,
+// of the oracle's FP64 sum and of its rounding to F32.  One thread per output
+// pixel; the 8 channels of a tap are one 8-byte load of the first-spike map.
 __global__ void __launch_bounds__(256) search_bound_kernel(TcParams P, const unsigned *__restrict__ wmax, int cp,
                                                            int2 *__restrict__ list, int *__restrict__ count)
 {
