@@ -2363,6 +2363,51 @@ __device__ __forceinline__ void write_plane_words(uint8_t *dst, int64_t n, int h
     }
 }
 
+// The same with 16-byte stores when a plane holds a multiple of 4 pixels but
+// not of 16 (e.g. 14 x 14 maps): each 4-byte word lies in one plane, so a
+// 16-byte chunk spans at most two planes when a plane has 16 pixels or more.
+__device__ __forceinline__ void write_block_words(uint8_t *dst, int64_t n, int hw, int C, bool lean, bool pass0,
+                                                  const uint8_t *wsrc, const uint8_t *tsrc, int tstride)
+{
+    uint4 *dv = reinterpret_cast<uint4 *>(dst);
+    const int wpp = hw / 4, nv = int(n / 16);
+    const int step = 4 * int(blockDim.x);  // words per iteration of the block
+    const int dplane = step / wpp, dw = step - dplane * wpp;
+    int wq = (4 * int(threadIdx.x)) % wpp, plane = (4 * int(threadIdx.x)) / wpp;
+    int t = plane / C, c = plane - t * C;
+    for (int i = threadIdx.x; i < nv; i += blockDim.x)
+    {
+        uint32_t o[4] = {0u, 0u, 0u, 0u};
+        if (lean)
+        {
+            int qw = wq, qc = c, qt = t;
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+            {
+                if (q > 0 && ++qw == wpp)
+                {
+                    qw = 0;
+                    if (++qc == C) qc = 0, ++qt;
+                }
+                const int px = 4 * qw;
+                const uint32_t t4 = uint32_t(qt) * 0x01010101u;
+                if (pass0)
+                {
+                    const uint32_t w = *reinterpret_cast<const uint32_t *>(wsrc + px);
+                    const uint32_t t0 = *reinterpret_cast<const uint32_t *>(tsrc + px);
+                    o[q] = (bytes_eq(w, uint32_t(qc) * 0x01010101u) & bytes_le(t0, t4)) >> 7;
+                }
+                else
+                    o[q] = bytes_le(*reinterpret_cast<const uint32_t *>(tsrc + qc * tstride + px), t4) >> 7;
+            }
+        }
+        dv[i] = make_uint4(o[0], o[1], o[2], o[3]);
+        wq += dw, c += dplane;
+        if (wq >= wpp) wq -= wpp, ++c;
+        while (c >= C) c -= C, ++t;
+    }
+}
+
 __global__ void __launch_bounds__(256) search_write_kernel(const int4 *__restrict__ records,
                                                            const uint8_t *__restrict__ gcodes, int64_t npix,
                                                            const int *negw, const int *flag,
@@ -2422,6 +2467,9 @@ __global__ void __launch_bounds__(256) search_write_kernel(const int4 *__restric
             const bool srcal = gcodes == nullptr || (ohw % 16 == 0);
             if (table && hw % 16 == 0 && (a & 15) == 0 && srcal)
                 write_plane_words<16>(dst, n, hw, C, lean, pass == 0, wsrc, pass == 0 ? tsrc : first, phw16);
+            else if (table && hw % 4 == 0 && hw >= 16 && n % 16 == 0 && (a & 15) == 0 &&
+                     (gcodes == nullptr || ohw % 4 == 0))
+                write_block_words(dst, n, hw, C, lean, pass == 0, wsrc, pass == 0 ? tsrc : first, phw16);
             else if (table && hw % 4 == 0 && (a & 3) == 0 && (gcodes == nullptr || ohw % 4 == 0))
                 write_plane_words<4>(dst, n, hw, C, lean, pass == 0, wsrc, pass == 0 ? tsrc : first, phw16);
             else

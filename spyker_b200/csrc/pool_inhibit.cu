@@ -340,6 +340,126 @@ __global__ void inhibit_f32x4_kernel(float4 *__restrict__ data, int64_t b, int t
         }
     }
 }
+// F32 inhibition with V neighbouring pixels per thread (V = 1, 2 or 4, the
+// widest that still gives the grid two waves of threads) and 8 loads in
+// flight per thread.  The per-step maximum only feeds the count of steps
+// above the threshold, so it is taken over two interleaved chains: chain A
+// starts at channel 0 and takes the even channels, chain B starts at -inf
+// and takes the odd ones; the merged value is above the threshold exactly
+// when the reference's sequential maximum is (a NaN in channel 0 stays NaN in
+// A and the merge keeps it; other NaNs are skipped by both).  The winner at
+// step T - max(count, 1) and the zeroing keep the reference's order.
+template <int V>
+struct F32Vec;
+template <>
+struct F32Vec<1>
+{
+    using T = float;
+    static __device__ __forceinline__ float get(const float &v, int) { return v; }
+    static __device__ __forceinline__ void set(float &v, int, float x) { v = x; }
+};
+template <>
+struct F32Vec<2>
+{
+    using T = float2;
+    static __device__ __forceinline__ float get(const float2 &v, int l) { return l ? v.y : v.x; }
+    static __device__ __forceinline__ void set(float2 &v, int l, float x) { (l ? v.y : v.x) = x; }
+};
+template <>
+struct F32Vec<4>
+{
+    using T = float4;
+    static __device__ __forceinline__ float get(const float4 &v, int l)
+    {
+        return l == 0 ? v.x : (l == 1 ? v.y : (l == 2 ? v.z : v.w));
+    }
+    static __device__ __forceinline__ void set(float4 &v, int l, float x)
+    {
+        (l == 0 ? v.x : (l == 1 ? v.y : (l == 2 ? v.z : v.w))) = x;
+    }
+};
+
+template <int V>
+__global__ void __launch_bounds__(256) inhibit_f32v_kernel(float *__restrict__ data, int64_t b, int t, int c,
+                                                           int64_t xv, float thr)
+{
+    using F = F32Vec<V>;
+    using Vec = typename F::T;
+    const int64_t total = b * xv;
+    for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < total; k += int64_t(gridDim.x) * blockDim.x)
+    {
+        const int64_t s = k / xv, j = k - s * xv;
+        Vec *base = reinterpret_cast<Vec *>(data) + s * int64_t(t) * c * xv + j;
+        int sum[V];
+#pragma unroll
+        for (int l = 0; l < V; ++l) sum[l] = 0;
+        for (int q = 0; q < t; ++q)
+        {
+            const Vec *row = base + int64_t(q) * c * xv;
+            float ma[V], mb[V];
+            const Vec r0 = row[0];
+#pragma unroll
+            for (int l = 0; l < V; ++l) ma[l] = F::get(r0, l), mb[l] = -INFINITY;
+            int z = 1;
+#pragma unroll 4
+            for (; z + 1 < c; z += 2)
+            {
+                const Vec u = row[int64_t(z) * xv], w = row[int64_t(z + 1) * xv];
+#pragma unroll
+                for (int l = 0; l < V; ++l)
+                {
+                    const float vu = F::get(u, l), vw = F::get(w, l);
+                    mb[l] = vu > mb[l] ? vu : mb[l];
+                    ma[l] = vw > ma[l] ? vw : ma[l];
+                }
+            }
+            if (z < c)
+            {
+                const Vec u = row[int64_t(z) * xv];
+#pragma unroll
+                for (int l = 0; l < V; ++l)
+                {
+                    const float vu = F::get(u, l);
+                    mb[l] = vu > mb[l] ? vu : mb[l];
+                }
+            }
+#pragma unroll
+            for (int l = 0; l < V; ++l)
+            {
+                const float m = mb[l] > ma[l] ? mb[l] : ma[l];
+                sum[l] += (m > thr);
+            }
+        }
+        int win[V];
+#pragma unroll
+        for (int l = 0; l < V; ++l)
+        {
+            const int ts = t - (sum[l] > 1 ? sum[l] : 1);
+            const float *col = reinterpret_cast<const float *>(base + int64_t(ts) * c * xv) + l;
+            float best = col[0];
+            int w = 0;
+            for (int z = 1; z < c; ++z)
+            {
+                const float v = col[int64_t(z) * xv * V];
+                if (v > best) best = v, w = z;
+            }
+            win[l] = w;
+        }
+        for (int q = 0; q < t; ++q)
+        {
+            Vec *r = base + int64_t(q) * c * xv;
+#pragma unroll 8
+            for (int z = 0; z < c; ++z)
+            {
+                Vec v = r[int64_t(z) * xv];
+#pragma unroll
+                for (int l = 0; l < V; ++l)
+                    if (z != win[l]) F::set(v, l, F::get(v, l) * 0.0f);
+                r[int64_t(z) * xv] = v;
+            }
+        }
+    }
+}
 }  // namespace
 }  // namespace spk
 
@@ -425,10 +545,22 @@ spk_status spk_rank_inhibit(void *data, spk_dtype type, int64_t b, int64_t t, in
         SPK_REQUIRE(b >= 0 && t >= 1 && c >= 1 && x >= 0, "invalid dims");
         SPK_REQUIRE(c <= 65535 && t <= 65535, "channel and time counts are limited to 65535");
         if (b * x == 0) return;
-        if (type == SPK_F32 && x % 4 == 0 && reinterpret_cast<uintptr_t>(data) % 16 == 0)
+        if (type == SPK_F32)
         {
-            inhibit_f32x4_kernel<<<grid_for(b * x / 4, 128), 128, 0, stream_of(stream)>>>(
-                static_cast<float4 *>(data), b, int(t), int(c), x / 4, scalar_to<float>(threshold));
+            // the widest vector that still leaves two waves of threads
+            const int64_t waves2 = int64_t(sm_count()) * 2048 * 2;
+            const uintptr_t a = reinterpret_cast<uintptr_t>(data);
+            const float th = scalar_to<float>(threshold);
+            float *d = static_cast<float *>(data);
+            if (x % 4 == 0 && a % 16 == 0 && b * x / 4 >= waves2)
+                inhibit_f32v_kernel<4><<<grid_for(b * x / 4, 256), 256, 0, stream_of(stream)>>>(d, b, int(t), int(c),
+                                                                                              x / 4, th);
+            else if (x % 2 == 0 && a % 8 == 0 && b * x / 2 >= waves2)
+                inhibit_f32v_kernel<2><<<grid_for(b * x / 2, 256), 256, 0, stream_of(stream)>>>(d, b, int(t), int(c),
+                                                                                              x / 2, th);
+            else
+                inhibit_f32v_kernel<1><<<grid_for(b * x, 256), 256, 0, stream_of(stream)>>>(d, b, int(t), int(c), x,
+                                                                                          th);
             SPK_LAUNCHED();
             return;
         }
