@@ -731,8 +731,6 @@ def gabor_arm(args, rank, world):
     """Large-image forward pass (no STDP): the fused layers against the FP32
     op-by-op path and against the oracle's FP64 pipeline, conv1 potential
     errors against FP64 on the same GPU, and the reference's CPU path."""
-    if rank != 0:
-        return  # a one-GPU workload: under torchrun only rank 0 runs it
     import torch
 
     import spyker_b200 as spyker
@@ -740,6 +738,20 @@ def gabor_arm(args, rank, world):
 
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
+    # several GPUs: replicas, each rank its own images (no exchange)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
     batch = args.batch if args.batch != BATCH else 256
     # the fused layers take the exact search path (non-negative weights) at
     # either split precision; the precision names the op-by-op potentials
@@ -749,30 +761,37 @@ def gabor_arm(args, rank, world):
     net = GaborNet(spyker, torch, dev, prec)
     for _ in range(args.warmup):
         net.step(imgs)
-    torch.cuda.synchronize()
+    barrier()
     spyker._lib.lib.spk_recheck_count(1)
     spyker._lib.lib.spk_recompute_count(1)
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with Clocks(dev.index) as clk:
-        torch.cuda.synchronize()
+        barrier()
         a.record()
         for _ in range(args.steps):
             feats = net.step(imgs)
         b.record()
-        torch.cuda.synchronize()
+        barrier()
     ms = a.elapsed_time(b) / args.steps
     rechecks = spyker._lib.lib.spk_recheck_count(1) / args.steps
     recomputes = spyker._lib.lib.spk_recompute_count(1) / args.steps
     del feats
     # end to end: pinned host images -> first-spike maps of the features on the host
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
+    barrier()
     e0.record()
     for _ in range(args.steps):
         out = spyker.gather(net.step(host.to(dev, non_blocking=True)[:, None])).cpu()
     e1.record()
-    torch.cuda.synchronize()
+    barrier()
     e2e_ms = e0.elapsed_time(e1) / args.steps
+    t_max = torch.tensor([ms, e2e_ms], device=dev)
+    if dist is not None:
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+        dist.destroy_process_group()
+    ms, e2e_ms = float(t_max[0]), float(t_max[1])
+    if rank != 0:
+        return  # the comparisons and the CPU leg run on rank 0 only
     # FP32 op-by-op path and potential errors on a sub-batch
     sub = min(4, batch)
     ref = GaborNet(spyker, torch, dev, "fp32")
@@ -800,15 +819,16 @@ def gabor_arm(args, rank, world):
     achieved = (c1 + c2) * batch / (ms * 1e-3) / 1e12
     print(json.dumps({
         "metric": "images/s (forward feature extraction), tensor-core path vs FP32 on 1 B200; spike match %",
-        "value": batch / (ms * 1e-3), "unit": "images/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "value": batch * world / (ms * 1e-3), "unit": "images/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": path_dtype(prec)[0], "arithmetic": path_dtype(prec)[1],
         "data": "synthetic (seeded 1/f textures + Gaussian blobs, 256x256)",
-        "config": {"workload": GABOR_WORKLOAD.replace("256 x", f"{batch} x"), "global_batch": batch, "seq_len": 30,
-                   "parallelism": "replicas1", "conv_precision": prec,
+        "config": {"workload": GABOR_WORKLOAD.replace("256 x", f"{batch} x"), "global_batch": batch * world,
+                   "seq_len": 30, "parallelism": f"replicas{world}", "conv_precision": prec,
                    "l2": "inputs larger than L2: the layer-1 spikes are 128 MB per image"},
-        "e2e": {"value": batch / (e2e_ms * 1e-3), "unit": "images/s", "h2d_bytes_per_step": int(host.numel() * 4),
-                "d2h_bytes_per_step": int(out.numel() * out.element_size())},
+        "e2e": {"value": batch * world / (e2e_ms * 1e-3), "unit": "images/s",
+                "h2d_bytes_per_step": int(host.numel() * 4) * world,
+                "d2h_bytes_per_step": int(out.numel() * out.element_size()) * world},
         "roofline": {"bound": "tensor", "kernel": "both fused layers (algorithmic conv FLOPs)", "achieved": achieved,
                      "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                      "peak_source": peak_source},
@@ -1038,9 +1058,9 @@ SWEEP_WORKLOAD = ("sweep: 32 independent 2-layer STDP networks x 512 stroke imag
 def sweep_arm(args, rank, world):
     """All networks' training step: per size one multi-network fused launch
     per layer and one multi-network STDP scan per layer, captured once as a
-    CUDA graph and replayed; schedules picked by the autotuner."""
-    if rank != 0:
-        return  # a one-GPU workload: under torchrun only rank 0 runs it
+    CUDA graph and replayed; schedules picked by the autotuner.  Several
+    GPUs: each rank trains its own 32 networks (seeds differ by rank), no
+    exchange; time = max over ranks."""
     import torch
 
     import spyker_b200 as spyker
@@ -1048,22 +1068,34 @@ def sweep_arm(args, rank, world):
 
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
     nets = 32
     images = 512 if args.batch == BATCH else args.batch
     sw = sweep.Sweep(nets=nets, images=images, seed=10 * rank, device=dev, precision=args.precision, tune=True)
     sw.capture()
     for _ in range(max(args.warmup - 1, 0)):
         sw.replay()
-    torch.cuda.synchronize()
-    l0 = spyker._lib.lib.spk_launch_count()
+    barrier()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with Clocks(dev.index) as clk:
-        torch.cuda.synchronize()
+        barrier()
         a.record()
         for _ in range(args.steps):
             sw.replay()
         b.record()
-        torch.cuda.synchronize()
+        barrier()
     ms = a.elapsed_time(b) / args.steps
     # launches inside one graph (counted while capturing a second one)
     l1 = spyker._lib.lib.spk_launch_count()
@@ -1082,15 +1114,22 @@ def sweep_arm(args, rank, world):
     # end to end: pinned host images into the graph's inputs, features back
     h2d = sum(int(g.host.numel()) for g in sw.groups)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
+    barrier()
     e0.record()
     for _ in range(args.steps):
         for g in sw.groups:
             g.images.copy_(g.host.to(dev, non_blocking=True).float().div_(255.0)[:, None])
         feats = [f.cpu() for f in sw.replay()]
     e1.record()
-    torch.cuda.synchronize()
+    barrier()
     e2e_ms = e0.elapsed_time(e1) / args.steps
+    t_max = torch.tensor([ms, e2e_ms], device=dev)
+    if dist is not None:
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+        dist.destroy_process_group()
+    ms, e2e_ms = float(t_max[0]), float(t_max[1])
+    if rank != 0:
+        return
     n_img = sw.images_per_step
     flops = sum(
         sum(len(g.per_net[n][1]) for n in range(nets)) * 2 * 15 * (g.size ** 2 * 30 * 50 + (g.size // 2) ** 2 * 100 * 750)
@@ -1099,16 +1138,17 @@ def sweep_arm(args, rank, world):
     achieved = flops / (ms * 1e-3) / 1e12
     print(json.dumps({
         "metric": "images/s (32-network STDP sweep, train + fwd) on 1 B200",
-        "value": n_img / (ms * 1e-3), "unit": "images/s", "n_gpus": world, "steps": args.steps,
+        "value": n_img * world / (ms * 1e-3), "unit": "images/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": {"fp32": "f32", "bf16x2": "bf16x2-split/f32-acc", "bf16x3": "bf16x3-split/f32-acc"}[args.precision],
         "data": "synthetic (seeded stroke images of 4 sizes)",
-        "config": {"workload": SWEEP_WORKLOAD, "global_batch": n_img, "seq_len": 15, "parallelism": "replicas1",
+        "config": {"workload": SWEEP_WORKLOAD, "global_batch": n_img * world, "seq_len": 15,
+                   "parallelism": f"replicas{world}",
                    "networks": nets, "padded_samples": sw.total, "cuda_graph": True,
                    "schedules": {f"{sw.groups[g].size}px/layer{l + 1}": list(v) for (g, l), v in sw.schedules.items()},
                    "l2": "inputs larger than L2: 2.0 GB of layer-1 spikes per step"},
-        "e2e": {"value": n_img / (e2e_ms * 1e-3), "unit": "images/s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": int(sum(f.numel() for f in feats))},
+        "e2e": {"value": n_img * world / (e2e_ms * 1e-3), "unit": "images/s", "h2d_bytes_per_step": h2d * world,
+                "d2h_bytes_per_step": int(sum(f.numel() for f in feats)) * world},
         "gpu_launches": int(launches),
         "eager_step_ms": eager_ms,
         "roofline": {"bound": "tensor", "kernel": "all fused layers (algorithmic conv FLOPs of the real images)",
