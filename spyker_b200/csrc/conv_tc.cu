@@ -49,7 +49,7 @@ namespace
 {
 using namespace tc;
 
-constexpr int BM = 128, BK = 64, kTcThreads = 256;
+constexpr int BM = 128, BK = 64;
 constexpr uint32_t kMaxProbes = 1u << 22;
 constexpr int kMaxKBlocks = 128;  // K up to 8192
 
@@ -253,6 +253,15 @@ __device__ __forceinline__ void arrive_expect_tx(uint64_t *bar, uint32_t bytes)
 {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
+
+// 8-byte asynchronous global -> shared copy (both addresses 8-byte aligned),
+// completed for the issuing thread by cp_async_wait_all.
+__device__ __forceinline__ void cp_async8(void *dst, const void *src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // Bulk (non-tensor) global -> shared copy completing on `bar`; both addresses
 // 16-byte aligned, size a multiple of 16.
@@ -1356,33 +1365,21 @@ __device__ void search_epilogue(const TcParams &P, uint32_t acc, bool ok, int pi
     }
 }
 
-__device__ __forceinline__ int2 search_entry(const TcParams &P, int64_t idx)
-{
-    if (P.round == 0 && !P.r0_list) return make_int2(int(idx), P.T - 1);
-    const int2 e = P.list_in[idx];
-    return P.round == 1 ? e : make_int2(e.x, P.T - 1);
-}
-
-__device__ __forceinline__ FusedPixel pixel_of(const TcParams &P, bool ok, int gp)
-{
-    FusedPixel u{};
-    u.ok = ok;
-    if (ok)
-    {
-        const uint32_t ohw = uint32_t(P.ohw), smp = uint32_t(gp) / ohw, pix = uint32_t(gp) - smp * ohw;
-        u.sample = smp;
-        const int oy = int(pix / uint32_t(P.ow)), ox = int(pix) - oy * P.ow;
-        u.iy0 = oy * P.sy - P.top;
-        u.ix0 = ox * P.sx - P.left;
-    }
-    return u;
-}
-
 // A search row's pixel in three words: byte offset of its sample's
 // first-spike map (-1: no row), receptive-field origin (iy0, ix0) packed as
 // two 16-bit fields, and its step.  The search operands are 8-bit and
-// channels-last: a 16-byte chunk of a row is two 8-channel groups, each one
-// 8-byte load of the first-spike map (0xFF: outside the input).
+// channels-last: a 16-byte chunk of a row is two 8-channel groups, each 8
+// bytes of the first-spike map (0xFF: outside the input).
+
+// Bytes 1 where the first-spike byte f <= t, else 0; tt = (t + 1) * 0x01010101
+// ((f | 0x80) - (t + 1) keeps bit 7 iff f > t, no borrow between bytes).
+__device__ __forceinline__ uint32_t spike_bytes(uint32_t f, uint32_t tt)
+{
+    return (~((f | 0x80808080u) - tt) >> 7) & 0x01010101u;
+}
+
+// 8-channel group g of a search row (tab entry: first channel, ky, kx,
+// valid); 0xFF bytes outside the input.
 __device__ __forceinline__ uint2 fst_group(const TcParams &P, const int4 *tab, int base, int yx, int g)
 {
     if (base < 0) return make_uint2(~0u, ~0u);
@@ -1394,11 +1391,19 @@ __device__ __forceinline__ uint2 fst_group(const TcParams &P, const int4 *tab, i
     return make_uint2(~0u, ~0u);
 }
 
-// Bytes 1 where the first-spike byte f <= t, else 0; tt = (t + 1) * 0x01010101
-// ((f | 0x80) - (t + 1) keeps bit 7 iff f > t, no borrow between bytes).
-__device__ __forceinline__ uint32_t spike_bytes(uint32_t f, uint32_t tt)
+// The list entries of the rows a thread with kc == 0 covers in `tile`, copied
+// into `buf` (128 entries, by row) asynchronously.
+template <int NU>
+__device__ __forceinline__ void entry_prefetch(const TcParams &P, int2 *buf, int64_t tile, int row0, int rs,
+                                               int64_t nrows)
 {
-    return (~((f | 0x80808080u) - tt) >> 7) & 0x01010101u;
+#pragma unroll
+    for (int i = 0; i < NU; ++i)
+    {
+        const int64_t idx = tile * BM + row0 + rs * i;
+        if (idx < nrows) cp_async8(buf + row0 + rs * i, P.list_in + idx);
+    }
+    cp_async_commit();
 }
 
 // Search producers: a thread builds NU (row, 16-byte chunk) units of every K
@@ -1406,18 +1411,38 @@ __device__ __forceinline__ uint32_t spike_bytes(uint32_t f, uint32_t tt)
 // thread p is row (p & 7) + 8 (p >> 6) + (1024 / NU / 8) i and chunk
 // (p >> 3) & 7, so the 8 lanes of a quarter warp take 8 consecutive rows of
 // one chunk (distinct 16-byte bank groups).  The gathers of a step are issued
-// before the wait for its stage, all in flight together.
+// before the wait for its stage, all in flight together.  (Copying them into
+// the stage with 8-byte cp.async and converting in place one step later
+// measured slower: the per-copy issue cost outweighed the deeper pipeline.)
+// In rounds with a row list the threads with kc == 0
+// (together one per row) fetch the next tile's list entries into shared
+// memory (cp.async) while the current tile is built, so their latency leaves
+// the per-tile chain; every producer thread reads them after an mbarrier of
+// the NT producers (two buffers, by tile parity).
 template <int NU>
 __device__ __forceinline__ void search_producer(const TcParams &P, const int4 *tab, unsigned char *smem,
                                                 uint64_t *full_bar, uint64_t *empty_bar, int S, int stage_bytes,
-                                                int a_bytes, int b_bytes, int p, int64_t nrows, int64_t ntiles)
+                                                int a_bytes, int b_bytes, int p, int64_t nrows, int64_t ntiles,
+                                                int2 *s_ent, uint64_t *ent_bar)
 {
     constexpr int NT = 1024 / NU, RS = NT / 8;  // producer threads; row step between a thread's units
     const int row0 = (p & 7) + 8 * (p >> 6), kc = (p >> 3) & 7;
     if (int64_t(blockIdx.x) >= ntiles) return;
-    uint32_t it = 0;
-    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
+    const bool listed = !(P.round == 0 && !P.r0_list);
+    if (listed && kc == 0) entry_prefetch<NU>(P, s_ent, blockIdx.x, row0, RS, nrows);
+    uint32_t it = 0, k = 0;
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++k)
     {
+        const int cb = int(k & 1);
+        if (listed)
+        {
+            if (kc == 0) cp_async_wait_all();
+            mbar_arrive(&ent_bar[cb]);
+            if (!wait_bounded(&ent_bar[cb], (k >> 1) & 1)) return;
+            // every thread has read the other buffer (the previous tile's)
+            if (kc == 0 && tile + gridDim.x < ntiles)
+                entry_prefetch<NU>(P, s_ent + (cb ^ 1) * BM, tile + gridDim.x, row0, RS, nrows);
+        }
         int ubase[NU], uyx[NU];
         uint32_t utt[NU];
 #pragma unroll
@@ -1427,7 +1452,12 @@ __device__ __forceinline__ void search_producer(const TcParams &P, const int4 *t
             ubase[i] = -1, uyx[i] = 0, utt[i] = 0x01010101u;
             if (idx < nrows)
             {
-                const int2 e = search_entry(P, idx);
+                int2 e = make_int2(int(idx), P.T - 1);
+                if (listed)
+                {
+                    e = s_ent[cb * BM + row0 + RS * i];
+                    if (P.round != 1) e.y = P.T - 1;
+                }
                 const uint32_t ohw = uint32_t(P.ohw), smp = uint32_t(e.x) / ohw, pix = uint32_t(e.x) - smp * ohw;
                 const int oy = int(pix / uint32_t(P.ow)), ox = int(pix) - oy * P.ow;
                 ubase[i] = int(int64_t(smp) * P.img_stride);
@@ -1436,33 +1466,33 @@ __device__ __forceinline__ void search_producer(const TcParams &P, const int4 *t
             }
         }
         for (int part = 0; part < P.nparts; ++part)
-        for (int kb = 0; kb < P.kblocks; ++kb, ++it)
-        {
-            uint2 fa[NU], fb[NU];
-#pragma unroll
-            for (int i = 0; i < NU; ++i)
+            for (int kb = 0; kb < P.kblocks; ++kb, ++it)
             {
-                fa[i] = fst_group(P, tab, ubase[i], uyx[i], kb * 16 + 2 * kc);
-                fb[i] = fst_group(P, tab, ubase[i], uyx[i], kb * 16 + 2 * kc + 1);
-            }
-            const int s = int(it % uint32_t(S));
-            const uint32_t u = it / uint32_t(S);
-            if (u > 0 && !wait_bounded(&empty_bar[s], (u - 1) & 1)) return;
-            unsigned char *sA = smem + s * stage_bytes;
-            if (p == 0)
-            {
-                arrive_expect_tx(&full_bar[s], uint32_t(b_bytes));
-                bulk_g2s(sA + a_bytes, P.wimg + (int64_t(part) * P.kblocks + kb) * b_bytes, uint32_t(b_bytes),
-                         &full_bar[s]);
-            }
+                uint2 fa[NU], fb[NU];
 #pragma unroll
-            for (int i = 0; i < NU; ++i)
-                *reinterpret_cast<uint4 *>(a_row_chunk(sA, row0 + RS * i, kc)) =
-                    make_uint4(spike_bytes(fa[i].x, utt[i]), spike_bytes(fa[i].y, utt[i]),
-                               spike_bytes(fb[i].x, utt[i]), spike_bytes(fb[i].y, utt[i]));
-            fence_proxy_async_smem();
-            mbar_arrive(&full_bar[s]);
-        }
+                for (int i = 0; i < NU; ++i)
+                {
+                    fa[i] = fst_group(P, tab, ubase[i], uyx[i], kb * 16 + 2 * kc);
+                    fb[i] = fst_group(P, tab, ubase[i], uyx[i], kb * 16 + 2 * kc + 1);
+                }
+                const int s = int(it % uint32_t(S));
+                const uint32_t u = it / uint32_t(S);
+                if (u > 0 && !wait_bounded(&empty_bar[s], (u - 1) & 1)) return;
+                unsigned char *sA = smem + s * stage_bytes;
+                if (p == 0)
+                {
+                    arrive_expect_tx(&full_bar[s], uint32_t(b_bytes));
+                    bulk_g2s(sA + a_bytes, P.wimg + (int64_t(part) * P.kblocks + kb) * b_bytes, uint32_t(b_bytes),
+                             &full_bar[s]);
+                }
+#pragma unroll
+                for (int i = 0; i < NU; ++i)
+                    *reinterpret_cast<uint4 *>(a_row_chunk(sA, row0 + RS * i, kc)) =
+                        make_uint4(spike_bytes(fa[i].x, utt[i]), spike_bytes(fa[i].y, utt[i]),
+                                   spike_bytes(fb[i].x, utt[i]), spike_bytes(fb[i].y, utt[i]));
+                fence_proxy_async_smem();
+                mbar_arrive(&full_bar[s]);
+            }
     }
 }
 
@@ -1487,7 +1517,8 @@ template <int MODE, int NPW>
 __device__ __forceinline__ void conv_ws_body(const TcParams &P)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
-    __shared__ __align__(8) uint64_t full_bar[kMaxStages], empty_bar[kMaxStages], accf_bar[2], acce_bar[2], tim_bar;
+    __shared__ __align__(8) uint64_t full_bar[kMaxStages], empty_bar[kMaxStages], accf_bar[2], acce_bar[2], tim_bar,
+        ent_bar[2];
     __shared__ uint32_t tmem_slot;
 
     // the search kernels run only on the lean path, the dense fused kernel
@@ -1518,6 +1549,8 @@ __device__ __forceinline__ void conv_ws_body(const TcParams &P)
     float *s_scale = reinterpret_cast<float *>(tab + P.kblocks * 16), *s_bound = s_scale + nch;
     // search: per epilogue warp, a buffer of next-round list entries
     int2 *s_nbuf = reinterpret_cast<int2 *>(s_bound + nch + ((16 - ((2 * nch) & 15)) & 15));
+    // search: two buffers of the next tile's list entries (128 each)
+    int2 *s_ent = s_nbuf + 4 * 256;
     if constexpr (MODE == kSearch)
     {
         // per 8-element group of a 128-element K block (channels-last, 8-bit
@@ -1566,6 +1599,7 @@ __device__ __forceinline__ void conv_ws_body(const TcParams &P)
             mbar_init(&full_bar[s], 1 + 32 * NPW), mbar_init(&empty_bar[s], 1);
         for (int a = 0; a < 2; ++a) mbar_init(&accf_bar[a], 1), mbar_init(&acce_bar[a], 128);
         mbar_init(&tim_bar, 128);
+        for (int b = 0; b < 2; ++b) mbar_init(&ent_bar[b], 32 * NPW);
         fence_mbar_init();
     }
     if (warp == 0)
@@ -1582,7 +1616,7 @@ __device__ __forceinline__ void conv_ws_body(const TcParams &P)
     constexpr int kMmaWarp = 4 + NPW;
     if (MODE == kSearch && warp >= 4 && warp < kMmaWarp)
         search_producer<1024 / (32 * NPW)>(P, tab, smem, full_bar, empty_bar, S, stage_bytes, a_bytes, b_bytes,
-                                           tid - 128, nrows, ntiles);
+                                           tid - 128, nrows, ntiles, s_ent, ent_bar);
     else if (MODE != kPotentials && MODE != kSearch && warp >= 4 && warp < kMmaWarp)
     {
         // ---------------- fused producers (8 warps) ----------------
@@ -2563,8 +2597,10 @@ Plan make_plan(int64_t n, int64_t cin, int64_t h, int64_t w, int64_t cout, int64
         pl.xt_bytes = pl.nhwc ? size_t(n) * h * w * pl.cpad : 0;
     // (kTimes: the table is followed by the per-warp first-step candidates,
     // two buffers of 4 warps x n_tile ints)
-    // (search: 16 group entries per K block, then the channels' scales and bounds)
-    const size_t tab = nsplit > 0   ? size_t(pl.kblocks) * 256 + size_t(pl.parts) * pl.n_tile * 8 + 64 + 4 * 256 * 8
+    // (search: 16 group entries per K block, the channels' scales and bounds,
+    // the epilogue warps' list buffers and two buffers of tile entries)
+    const size_t tab = nsplit > 0   ? size_t(pl.kblocks) * 256 + size_t(pl.parts) * pl.n_tile * 8 + 64 + 4 * 256 * 8 +
+                                        2 * BM * 8
                        : t_fused > 0 ? (size_t(pl.kblocks) * BK + 8) * 16 + (times ? size_t(pl.n_tile) * 32 : 0)
                        : !pl.nhwc   ? size_t(pl.kblocks) * BK * 16
                                     : size_t(pl.kblocks) * 8 * 16;

@@ -340,9 +340,9 @@ __global__ void inhibit_f32x4_kernel(float4 *__restrict__ data, int64_t b, int t
         }
     }
 }
-// F32 inhibition with V neighbouring pixels per thread (V = 1, 2 or 4, the
-// widest that still gives the grid two waves of threads) and 8 loads in
-// flight per thread.  The per-step maximum only feeds the count of steps
+// F32 inhibition with V neighbouring pixels per thread (V = 4 where the
+// plane size and alignment allow, else 2 or 1) and 8 loads in flight per
+// thread.  The per-step maximum only feeds the count of steps
 // above the threshold, so it is taken over two interleaved chains: chain A
 // starts at channel 0 and takes the even channels, chain B starts at -inf
 // and takes the odd ones; the merged value is above the threshold exactly
@@ -438,6 +438,7 @@ __global__ void __launch_bounds__(256) inhibit_f32v_kernel(float *__restrict__ d
             const float *col = reinterpret_cast<const float *>(base + int64_t(ts) * c * xv) + l;
             float best = col[0];
             int w = 0;
+#pragma unroll 4
             for (int z = 1; z < c; ++z)
             {
                 const float v = col[int64_t(z) * xv * V];
@@ -547,8 +548,8 @@ spk_status spk_rank_inhibit(void *data, spk_dtype type, int64_t b, int64_t t, in
         if (b * x == 0) return;
         if (type == SPK_F32)
         {
-            // the widest vector that still leaves two waves of threads
-            const int64_t waves2 = int64_t(sm_count()) * 2048 * 2;
+            // the widest vector that still leaves a block of threads per SM
+            const int64_t waves2 = int64_t(sm_count()) * 256;
             const uintptr_t a = reinterpret_cast<uintptr_t>(data);
             const float th = scalar_to<float>(threshold);
             float *d = static_cast<float *>(data);
