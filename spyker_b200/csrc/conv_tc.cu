@@ -97,11 +97,11 @@ struct TcParams
     int round, wta;
     const int2 *list_in;
     const int *count_in;
-    int2 *list_out, *final_list;
-    int *count_out, *final_count;
-    int4 *fix_list;  // rows left for the exact recompute: (pixel, step, round, winner)
+    int2 *list_out, *final_list;  // list_out: each row's next entry at the row's index
+    int *final_count;
+    int4 *fix_list;  // rows left for the exact recompute: (pixel, step, row index, winner)
     int *fix_count;
-    int4 *val_list;  // rows whose winner is decided but not its value: (pixel, step, round, winner)
+    int4 *val_list;  // rows whose winner is decided but not its value: (pixel, step, row index, winner)
     int *val_count;
     int4 *state;     // per pixel: (lo | hi << 8 | winner << 16, value, winner at T-1, value at T-1)
     const float *echan;     // per channel bound of |oracle potential - exact term sum|
@@ -1197,24 +1197,10 @@ struct SearchScan
     uint64_t r1 = 0, r2 = 0;
 };
 
-// Warp-wide flush of a warp's buffered list entries: one atomic for all.
-__device__ __forceinline__ void s_flush(int2 *buf, int &fill, int2 *list, int *count)
-{
-    __syncwarp();
-    if (fill == 0) return;
-    const int lane = threadIdx.x & 31;
-    int base = 0;
-    if (lane == 0) base = atomicAdd(count, fill);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    for (int i = lane; i < fill; i += 32) list[base + i] = buf[i];
-    __syncwarp();
-    fill = 0;
-}
-
 template <int NS>
 __device__ void search_epilogue(const TcParams &P, uint32_t acc, bool ok, int pix, int t, int aux, int4 pstate,
-                                uint64_t *release, float emax, const float *scale, const float *bound, int2 *nbuf,
-                                int &nfill, int part, SearchScan &sc)
+                                uint64_t *release, float emax, const float *scale, const float *bound, int idx,
+                                int part, SearchScan &sc)
 {
     const int warp = threadIdx.x >> 5;
     const uint32_t lane_base = acc + (uint32_t((warp & 3) * 32) << 16);
@@ -1322,15 +1308,14 @@ __device__ void search_epilogue(const TcParams &P, uint32_t acc, bool ok, int pi
     // dec 3: the winner a is decided, its value is left to the exact sum
     SearchAct r;
     if (ok && (dec == 1 || dec == 2)) r = search_act(P, P.round, pix, t, dec, a, v, pstate);
-    // the next round's entries go to this warp's buffer (flushed with one
-    // atomic when it fills); the rarer lists take one atomic per warp each,
-    // all in flight at once
+    // a decided row writes its pixel's entry of the next round at its own
+    // index (the next step, or -1 when the pixel is settled; a compaction
+    // keeps the list in pixel order); rows left open are written by the
+    // exact recompute.  The rarer lists take one atomic per warp each, all
+    // in flight at once.
+    if (ok && P.round != 2 && (dec == 1 || dec == 2)) P.list_out[idx] = r.next ? r.next_e : make_int2(pix, -1);
     const int lane = threadIdx.x & 31;
     const unsigned below = (1u << lane) - 1u;
-    const unsigned mn = __ballot_sync(0xffffffffu, r.next);
-    if (r.next) nbuf[nfill + __popc(mn & below)] = r.next_e;
-    nfill += __popc(mn);
-    if (nfill > 256 - 32) s_flush(nbuf, nfill, P.list_out, P.count_out);
     const bool wf = ok && dec == 0, wv = ok && dec == 3;
     const unsigned mf = __ballot_sync(0xffffffffu, wf), mv = __ballot_sync(0xffffffffu, wv);
     const unsigned mi = __ballot_sync(0xffffffffu, r.fin);
@@ -1344,8 +1329,8 @@ __device__ void search_epilogue(const TcParams &P, uint32_t acc, bool ok, int pi
     bf = __shfl_sync(0xffffffffu, bf, 0) + __popc(mf & below);
     bv = __shfl_sync(0xffffffffu, bv, 0) + __popc(mv & below);
     bi = __shfl_sync(0xffffffffu, bi, 0) + __popc(mi & below);
-    if (wf) P.fix_list[bf] = make_int4(pix, t, P.round, aux);
-    if (wv) P.val_list[bv] = make_int4(pix, t, P.round, a);
+    if (wf) P.fix_list[bf] = make_int4(pix, t, idx, aux);
+    if (wv) P.val_list[bv] = make_int4(pix, t, idx, a);
     if (r.fin) P.final_list[bi] = r.fin_e;
     if (P.wta)
     {
@@ -1547,10 +1532,8 @@ __device__ __forceinline__ void conv_ws_body(const TcParams &P)
     // search: the channels' scales and bounds, staged after the table
     const int nch = MODE == kSearch ? P.nparts * P.n_tile : P.n_tile;  // channels of the tables
     float *s_scale = reinterpret_cast<float *>(tab + P.kblocks * 16), *s_bound = s_scale + nch;
-    // search: per epilogue warp, a buffer of next-round list entries
-    int2 *s_nbuf = reinterpret_cast<int2 *>(s_bound + nch + ((16 - ((2 * nch) & 15)) & 15));
     // search: two buffers of the next tile's list entries (128 each)
-    int2 *s_ent = s_nbuf + 4 * 256;
+    int2 *s_ent = reinterpret_cast<int2 *>(s_bound + nch + ((16 - ((2 * nch) & 15)) & 15));
     if constexpr (MODE == kSearch)
     {
         // per 8-element group of a 128-element K block (channels-last, 8-bit
@@ -1745,10 +1728,8 @@ __device__ __forceinline__ void conv_ws_body(const TcParams &P)
         // ---------------- epilogue (warps 0-3) ----------------
         // warp w reads tensor-memory lanes 32 w .. 32 w + 31 (rows of the tile)
         const int row = (warp & 3) * 32 + lane;
-        // the largest channel bound, this warp's list buffer and its fill (search)
+        // the largest channel bound (search)
         float emax = 0.f;
-        int2 *nbuf = s_nbuf + (warp & 3) * 256;
-        int nfill = 0;
         if constexpr (MODE == kSearch) emax = __uint_as_float(P.sinfo[0]);
         uint32_t j = 0;
         const int parts = MODE == kSearch ? P.nparts : 1;
@@ -1822,7 +1803,7 @@ __device__ __forceinline__ void conv_ws_body(const TcParams &P)
             {
                 if (part == 0) scan = SearchScan{};
                 search_epilogue<kSearchTerms>(P, acc, s_ok, s_e.x, s_e.y, P.round == 2 ? s_aux : 0, s_st,
-                                              &acce_bar[a], emax, s_scale, s_bound, nbuf, nfill, part, scan);
+                                              &acce_bar[a], emax, s_scale, s_bound, int(tile * BM + row), part, scan);
             }
             else if constexpr (MODE == kFused)
             {
@@ -1839,7 +1820,6 @@ __device__ __forceinline__ void conv_ws_body(const TcParams &P)
                 mbar_arrive(&acce_bar[a]);
             }
         }
-        if constexpr (MODE == kSearch) s_flush(nbuf, nfill, P.list_out, P.count_out);
     }
     tc_fence_before();
     __syncthreads();
@@ -2143,16 +2123,16 @@ __global__ void search_init_kernel(unsigned *mins, unsigned *maxs, int64_t b, co
 // negative weight, a pixel's potential at T - 1 is at most U, the sum over the
 // inputs that fired of their largest weight over the channels.  A pixel with
 // U at or below the threshold never fires and is settled here; the others go
-// to round 0's list.  U is summed in FP32 (non-negative terms) and multiplied,
+// to round 0's list (entry (pixel, T - 1) at the pixel's index, -1 for settled
+// pixels; the list is then compacted in pixel order).  U is summed in FP32 (non-negative terms) and multiplied,
 // rounding up, by 1 + (K + 2) 2^-23, which covers the roundings of that sum,
 // of the oracle's FP64 sum and of its rounding to F32.  One thread per output
 // pixel; the 8 channels of a tap are one 8-byte load of the first-spike map.
 __global__ void __launch_bounds__(256) search_bound_kernel(TcParams P, const unsigned *__restrict__ wmax, int cp,
-                                                           int2 *__restrict__ list, int *__restrict__ count)
+                                                           int2 *__restrict__ list)
 {
     if (*P.negw || *P.flag) return;
-    __shared__ float wm[32][8];    // per tap, the 8 channels of one first-spike word
-    __shared__ int2 lbuf[8][256];  // per warp: candidates awaiting one atomic
+    __shared__ float wm[32][8];  // per tap, the 8 channels of one first-spike word
     const int taps = P.kh * P.kw, kr = P.cin * taps;
     for (int i = threadIdx.x; i < 32 * 8; i += blockDim.x)
     {
@@ -2160,12 +2140,9 @@ __global__ void __launch_bounds__(256) search_bound_kernel(TcParams P, const uns
         wm[tap][c] = (tap < taps && c < P.cin) ? __uint_as_float(wmax[c * taps + tap]) : 0.f;
     }
     __syncthreads();
-    int2 *buf = lbuf[threadIdx.x >> 5];
-    int fill = 0;
     // FP32 sum of at most kr non-negative terms: within kr 2^-24 of the exact
     // sum, itself at least the oracle's FP64 sum / (1 + kr 2^-53)
     const float widen = 1.f + float(kr + 2) * 0x1p-23f;
-    const int lane = threadIdx.x & 31;
     const int ohw = int(P.ohw), npix = int(P.npix);
     const int stride = int(gridDim.x) * blockDim.x;
     for (int base = int(blockIdx.x) * blockDim.x; base < npix; base += stride)
@@ -2210,12 +2187,112 @@ __global__ void __launch_bounds__(256) search_bound_kernel(TcParams P, const uns
                 atomicMax(P.maxs + smp, order_enc(P.thv));
             }
         }
-        const unsigned m = __ballot_sync(0xffffffffu, cand);
-        if (cand) buf[fill + __popc(m & ((1u << lane) - 1u))] = make_int2(pix, P.T - 1);
-        fill += __popc(m);
-        if (fill > 256 - 32) s_flush(buf, fill, list, count);
+        if (ok) list[pix] = make_int2(pix, cand ? P.T - 1 : -1);
     }
-    s_flush(buf, fill, list, count);
+}
+
+// Stable compaction of a row list: the entries with a step >= 0 of
+// in[0 .. n) (n = *n_dev, or n_max when n_dev is null) go to out in their
+// order, their number to *count_out.  Three launches: per-block counts of
+// kCompactItems entries, one block's exclusive scan of the counts, and the
+// scatter (a block writes its entries from its offset, ranked by warp
+// ballots).  The lists stay in pixel order, so a tile's rows lie in a few
+// neighbouring images.
+constexpr int kCompactItems = 2048;
+
+__device__ __forceinline__ int64_t list_len(const int *n_dev, int64_t n_max) { return n_dev ? int64_t(*n_dev) : n_max; }
+
+__global__ void __launch_bounds__(256) list_count_kernel(const int2 *__restrict__ in, const int *n_dev, int64_t n_max,
+                                                         int *__restrict__ bcount, const int *negw, const int *flag)
+{
+    if (*negw || *flag) return;
+    __shared__ int ws[8];
+    const int64_t n = list_len(n_dev, n_max), b0 = int64_t(blockIdx.x) * kCompactItems;
+    int c = 0;
+    for (int i = threadIdx.x; i < kCompactItems; i += blockDim.x)
+    {
+        const int64_t j = b0 + i;
+        c += (j < n && in[j].y >= 0) ? 1 : 0;
+    }
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        int t = 0;
+        for (int w = 0; w < int(blockDim.x >> 5); ++w) t += ws[w];
+        bcount[blockIdx.x] = t;
+    }
+}
+
+// One block of 1024 threads: bcount[0 .. nb) becomes its exclusive prefix sum.
+__global__ void __launch_bounds__(1024) list_scan_kernel(int *__restrict__ bcount, int nb, int *__restrict__ count_out,
+                                                         const int *negw, const int *flag)
+{
+    if (*negw || *flag) return;
+    __shared__ int ws[32];
+    const int per = (nb + 1023) / 1024, lo = threadIdx.x * per, hi = min(nb, lo + per);
+    int sum = 0;
+    for (int i = lo; i < hi; ++i) sum += bcount[i];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int incl = sum;
+    for (int o = 1; o < 32; o <<= 1)
+    {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    if (lane == 31) ws[warp] = incl;
+    __syncthreads();
+    if (warp == 0)
+    {
+        int w = ws[lane], wi = w;
+        for (int o = 1; o < 32; o <<= 1)
+        {
+            const int v = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += v;
+        }
+        ws[lane] = wi - w;  // exclusive prefix of the warps
+        if (lane == 31) *count_out = wi;
+    }
+    __syncthreads();
+    int run = ws[warp] + incl - sum;
+    for (int i = lo; i < hi; ++i)
+    {
+        const int v = bcount[i];
+        bcount[i] = run;
+        run += v;
+    }
+}
+
+__global__ void __launch_bounds__(256) list_scatter_kernel(const int2 *__restrict__ in, const int *n_dev,
+                                                           int64_t n_max, const int *__restrict__ boff,
+                                                           int2 *__restrict__ out, const int *negw, const int *flag)
+{
+    if (*negw || *flag) return;
+    __shared__ int ws[8];
+    const int64_t n = list_len(n_dev, n_max), b0 = int64_t(blockIdx.x) * kCompactItems;
+    if (b0 >= n) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int base = boff[blockIdx.x];
+    for (int q = 0; q < kCompactItems; q += blockDim.x)
+    {
+        const int64_t j = b0 + q + threadIdx.x;
+        int2 e = make_int2(0, -1);
+        if (j < n) e = in[j];
+        const bool keep = e.y >= 0;
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        if (lane == 0) ws[warp] = __popc(m);
+        __syncthreads();
+        int before = 0, total = 0;
+        for (int w = 0; w < int(blockDim.x >> 5); ++w)
+        {
+            before += w < warp ? ws[w] : 0;
+            total += ws[w];
+        }
+        if (keep) out[base + before + __popc(m & ((1u << lane) - 1u))] = e;
+        base += total;
+        __syncthreads();
+    }
 }
 
 // Rows the search could not decide from the term sums (a potential within
@@ -2260,7 +2337,7 @@ __global__ void __launch_bounds__(128) search_fix_kernel(TcParams P, const float
     for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < nv; q += int64_t(gridDim.x) * blockDim.x)
     {
         const int4 e = P.val_list[q];
-        const int pix = e.x, t = e.y, round = e.z, o = e.w;
+        const int pix = e.x, t = e.y, idx = e.z, o = e.w, round = P.round;
         const int smp = pix / int(P.ohw), pp = pix - smp * int(P.ohw);
         const int oy = pp / P.ow, ox = pp - oy * P.ow;
         const int iy0 = oy * P.sy - P.top, ix0 = ox * P.sx - P.left;
@@ -2269,7 +2346,7 @@ __global__ void __launch_bounds__(128) search_fix_kernel(TcParams P, const float
         const double acc = oracle_sum(P, fm, wk, iy0, ix0, cp, t);
         atomicAdd(&g_recomputes, 1ull);
         const SearchAct r = search_act(P, round, pix, t, 2, o, float(acc), round == 1 ? P.state[pix] : int4{});
-        if (r.next) P.list_out[atomicAdd(P.count_out, 1)] = r.next_e;
+        if (round != 2) P.list_out[idx] = r.next ? r.next_e : make_int2(pix, -1);
         if (r.fin) P.final_list[atomicAdd(P.final_count, 1)] = r.fin_e;
         if (P.wta) s_extremes(P, pix, r);
     }
@@ -2277,7 +2354,7 @@ __global__ void __launch_bounds__(128) search_fix_kernel(TcParams P, const float
     for (int64_t q = int64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); q < n; q += nw)
     {
         const int4 e = P.fix_list[q];
-        const int pix = e.x, t = e.y, round = e.z, aux = e.w;
+        const int pix = e.x, t = e.y, idx = e.z, aux = e.w, round = P.round;
         const int smp = pix / int(P.ohw), pp = pix - smp * int(P.ohw);
         const int oy = pp / P.ow, ox = pp - oy * P.ow;
         const int iy0 = oy * P.sy - P.top, ix0 = ox * P.sx - P.left;
@@ -2311,7 +2388,7 @@ __global__ void __launch_bounds__(128) search_fix_kernel(TcParams P, const float
             else
                 dec = 1, a = -1, v = 0.f;
             const SearchAct r = search_act(P, round, pix, t, dec, a, v, round == 1 ? P.state[pix] : int4{});
-            if (r.next) P.list_out[atomicAdd(P.count_out, 1)] = r.next_e;
+            if (round != 2) P.list_out[idx] = r.next ? r.next_e : make_int2(pix, -1);
             if (r.fin) P.final_list[atomicAdd(P.final_count, 1)] = r.fin_e;
             if (P.wta) s_extremes(P, pix, r);
         }
@@ -2597,10 +2674,9 @@ Plan make_plan(int64_t n, int64_t cin, int64_t h, int64_t w, int64_t cout, int64
         pl.xt_bytes = pl.nhwc ? size_t(n) * h * w * pl.cpad : 0;
     // (kTimes: the table is followed by the per-warp first-step candidates,
     // two buffers of 4 warps x n_tile ints)
-    // (search: 16 group entries per K block, the channels' scales and bounds,
-    // the epilogue warps' list buffers and two buffers of tile entries)
-    const size_t tab = nsplit > 0   ? size_t(pl.kblocks) * 256 + size_t(pl.parts) * pl.n_tile * 8 + 64 + 4 * 256 * 8 +
-                                        2 * BM * 8
+    // (search: 16 group entries per K block, the channels' scales and bounds
+    // and two buffers of tile entries)
+    const size_t tab = nsplit > 0   ? size_t(pl.kblocks) * 256 + size_t(pl.parts) * pl.n_tile * 8 + 64 + 2 * BM * 8
                        : t_fused > 0 ? (size_t(pl.kblocks) * BK + 8) * 16 + (times ? size_t(pl.n_tile) * 32 : 0)
                        : !pl.nhwc   ? size_t(pl.kblocks) * BK * 16
                                     : size_t(pl.kblocks) * 8 * 16;
@@ -2937,6 +3013,7 @@ struct FusedLayout
     // winners to re-read at T - 1, two lists of rows to recompute
     bool search_ok;
     size_t w4_off, echan_off, wm_off, cnt_off, state_off, la_off, lb_off, fin_off, fa_off, fb_off, va_off, vb_off;
+    size_t lt_off, bc_off;  // the rows' next entries by row index, per-block counts of the compaction
     size_t total;
 };
 
@@ -2984,6 +3061,8 @@ FusedLayout fused_layout(int64_t b, int64_t t, int64_t cin, int64_t h, int64_t w
         L.fb_off = off, off += align256(np * 16);
         L.va_off = off, off += align256(np * 16);
         L.vb_off = off, off += align256(np * 16);
+        L.lt_off = off, off += align256(np * 8);
+        L.bc_off = off, off += align256((np / kCompactItems + 2) * 4);
     }
     L.total = off;
     return L;
@@ -3142,10 +3221,25 @@ void search_layer(const TcParams &P0, const FusedLayout &L, const float *kernel,
         search_init_kernel<<<grid_for(b, 256), 256, 0, s>>>(P.mins, P.maxs, b, P.negw, P.flag);
         SPK_LAUNCHED();
     }
+    // Rows write their next entry at their own index of lt (step -1: settled);
+    // a stable compaction makes the next round's list, in pixel order.
+    int2 *lt = reinterpret_cast<int2 *>(base + L.lt_off);
+    int *bc = reinterpret_cast<int *>(base + L.bc_off);
+    const unsigned cblocks = unsigned((L.npix + kCompactItems - 1) / kCompactItems);
+    SPK_REQUIRE(cblocks <= 1024u * 64u, "too many output pixels for the list compaction");
+    auto compact = [&](const int *n_dev, int2 *out, int *count_out) {
+        list_count_kernel<<<cblocks, 256, 0, s>>>(lt, n_dev, L.npix, bc, P.negw, P.flag);
+        SPK_LAUNCHED();
+        list_scan_kernel<<<1, 1024, 0, s>>>(bc, int(cblocks), count_out, P.negw, P.flag);
+        SPK_LAUNCHED();
+        list_scatter_kernel<<<cblocks, 256, 0, s>>>(lt, n_dev, L.npix, bc, out, P.negw, P.flag);
+        SPK_LAUNCHED();
+    };
     if (prefilter)
     {
-        search_bound_kernel<<<grid_for(L.npix, 256), 256, 0, s>>>(P, wmax, cp, lb, cnt);
+        search_bound_kernel<<<grid_for(L.npix, 256), 256, 0, s>>>(P, wmax, cp, lt);
         SPK_LAUNCHED();
+        compact(nullptr, lb, cnt);
     }
     const unsigned fix_grid = unsigned(sm_count() * 4);
     int nsr = 0;
@@ -3158,8 +3252,7 @@ void search_layer(const TcParams &P0, const FusedLayout &L, const float *kernel,
         P.r0_list = (r == 0 && prefilter) ? 1 : 0;
         P.list_in = final ? P.final_list : (r & 1 ? la : lb);
         P.count_in = final ? P.final_count : cnt + r;
-        P.list_out = r & 1 ? lb : la;
-        P.count_out = cnt + r + 1;
+        P.list_out = lt;
         P.fix_list = r & 1 ? fb : fa;
         P.fix_count = cnt + 17 + r;
         P.val_list = r & 1 ? vb : va;
@@ -3167,6 +3260,8 @@ void search_layer(const TcParams &P0, const FusedLayout &L, const float *kernel,
         launch<kSearch>(P, pl, s);
         search_fix_kernel<<<fix_grid, 128, 0, s>>>(P, kernel, cp);
         SPK_LAUNCHED();
+        // the next bisection round's list (round 0 without a list: all pixels)
+        if (r < nsr) compact(r == 0 && !prefilter ? nullptr : P.count_in, r & 1 ? lb : la, cnt + r + 1);
     }
     const int ohw = int(L.oh * L.ow);
     uint8_t *gcodes = nullptr;
