@@ -186,6 +186,141 @@ __global__ void __launch_bounds__(kCodeThreads) rank_sorted_kernel(const I *__re
         write_rows<O>(out + int64_t(blockIdx.x) * t * x, tm, x, t);
 }
 
+// The same for rows of 256 ITEMS / 2 < X <= 256 ITEMS values with 256
+// threads: thread i holds the keys of positions ITEMS i .. ITEMS i + ITEMS - 1
+// in registers, so a bitonic stage of stride < ITEMS is a compare-exchange
+// inside the thread, strides up to 32 ITEMS / 2 a shuffle with the thread
+// owning the partner positions, and only larger strides go through shared
+// memory (6 of the 66 stages at 2048 keys).  Small blocks let several images
+// share an SM.  The count of values above the minimum comes from the sorted
+// keys.
+constexpr int kRegThreads = 256;
+
+template <typename I, typename O, bool TIMES, int ITEMS>
+__global__ void __launch_bounds__(kRegThreads) rank_sorted_reg_kernel(const I *__restrict__ in, O *__restrict__ out,
+                                                                      int64_t x, int t)
+{
+    constexpr int N = kRegThreads * ITEMS;
+    __shared__ uint64_t keys[N];
+    __shared__ __align__(16) uint16_t tm[N];
+    __shared__ uint32_t s_cnt, s_minkey;
+    const int tid = threadIdx.x, e0 = ITEMS * tid;
+    const I *row = in + int64_t(blockIdx.x) * x;
+    uint64_t k[ITEMS];
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j)
+    {
+        const int i = e0 + j;
+        k[j] = i < x ? (uint64_t(~order_key(row[i])) << 32) | uint32_t(i) : ~uint64_t(0);
+    }
+    if (tid == 0) s_cnt = 0;
+    for (int size = 2; size <= N; size <<= 1)
+    {
+        int stride = size >> 1;
+        if (stride >= 32 * ITEMS)
+        {
+            __syncthreads();
+#pragma unroll
+            for (int j = 0; j < ITEMS; ++j) keys[e0 + j] = k[j];
+            __syncthreads();
+            for (; stride >= 32 * ITEMS; stride >>= 1)
+            {
+                for (int q = tid; q < N / 2; q += kRegThreads)
+                {
+                    const int lo = 2 * q - (q & (stride - 1)), hi = lo + stride;
+                    const bool up = (lo & size) == 0;
+                    const uint64_t a = keys[lo], c = keys[hi];
+                    if ((a > c) == up) keys[lo] = c, keys[hi] = a;
+                }
+                __syncthreads();
+            }
+#pragma unroll
+            for (int j = 0; j < ITEMS; ++j) k[j] = keys[e0 + j];
+        }
+        for (; stride >= ITEMS; stride >>= 1)
+        {
+            const int lx = stride / ITEMS;
+            const bool lower = (e0 & stride) == 0;
+            const bool keep_min = lower == ((e0 & size) == 0);
+#pragma unroll
+            for (int j = 0; j < ITEMS; ++j)
+            {
+                const uint64_t pk = __shfl_xor_sync(0xffffffffu, k[j], lx);
+                k[j] = keep_min ? (k[j] < pk ? k[j] : pk) : (k[j] > pk ? k[j] : pk);
+            }
+        }
+        // strides below ITEMS: compile-time strides keep k[] in registers
+#pragma unroll
+        for (int st = ITEMS / 2; st >= 1; st >>= 1)
+        {
+            if (st > stride) continue;
+#pragma unroll
+            for (int j = 0; j < ITEMS; ++j)
+                if ((j & st) == 0)
+                {
+                    const bool up = ((e0 + j) & size) == 0;
+                    const uint64_t a = k[j], c = k[j + st];
+                    if ((a > c) == up) k[j] = c, k[j + st] = a;
+                }
+        }
+    }
+    // the row minimum's key: the last real position
+    if (x - 1 >= e0 && x - 1 < e0 + ITEMS)
+    {
+#pragma unroll
+        for (int j = 0; j < ITEMS; ++j)
+            if (e0 + j == x - 1) s_minkey = uint32_t(k[j] >> 32);
+    }
+    __syncthreads();
+    uint32_t local = 0;
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) local += (e0 + j < x && uint32_t(k[j] >> 32) != s_minkey) ? 1u : 0u;
+    for (int o = 16; o > 0; o >>= 1) local += __shfl_xor_sync(0xffffffffu, local, o);
+    if ((tid & 31) == 0) atomicAdd(&s_cnt, local);
+    __syncthreads();
+    const float scale = (float(t) + 1e-5f) / float(s_cnt);
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j)
+        if (e0 + j < x) tm[uint32_t(k[j])] = f2u16(float(e0 + j) * scale);
+    __syncthreads();
+    if constexpr (TIMES)
+    {
+        for (int64_t j = tid; j < x; j += kRegThreads) out[int64_t(blockIdx.x) * x + j] = O(tm[j]);
+    }
+    else
+    {
+        O *o = out + int64_t(blockIdx.x) * t * x;
+        if (sizeof(O) == 1 && x % 16 == 0 && (reinterpret_cast<uintptr_t>(o) & 15) == 0)
+        {
+            // (row, 16-position vector) pairs over the block
+            const int nv = int(x / 16);
+            for (int q = tid; q < t * nv; q += kRegThreads)
+            {
+                const int srow = q / nv, v = q - srow * nv;
+                const uint4 ta = *reinterpret_cast<const uint4 *>(tm + 16 * v);
+                const uint4 tb = *reinterpret_cast<const uint4 *>(tm + 16 * v + 8);
+                const uint32_t hw[8] = {ta.x, ta.y, ta.z, ta.w, tb.x, tb.y, tb.z, tb.w};
+                uint32_t w[4];
+#pragma unroll
+                for (int r = 0; r < 4; ++r)
+                {
+                    const uint32_t a = hw[2 * r], b = hw[2 * r + 1];
+                    w[r] = uint32_t((a & 0xFFFFu) <= uint32_t(srow)) | (uint32_t((a >> 16) <= uint32_t(srow)) << 8) |
+                           (uint32_t((b & 0xFFFFu) <= uint32_t(srow)) << 16) |
+                           (uint32_t((b >> 16) <= uint32_t(srow)) << 24);
+                }
+                reinterpret_cast<uint4 *>(o + int64_t(srow) * x)[v] = make_uint4(w[0], w[1], w[2], w[3]);
+            }
+        }
+        else
+            for (int64_t j = tid; j < x; j += kRegThreads)
+            {
+                const uint16_t m = tm[j];
+                for (int srow = 0; srow < t; ++srow) o[int64_t(srow) * x + j] = O(m <= uint16_t(srow));
+            }
+    }
+}
+
 // Reduction type of the latency code: the value itself for floats, int for
 // u8 (the reference subtracts promoted integers).
 template <typename I>
@@ -413,6 +548,22 @@ uint16_t *large_times_slot(void *ws, int64_t b, int64_t x)
 // Bytes of scratch the sorted code needs (0 when X <= 16384).
 size_t rank_times_ws(int64_t b, int64_t x, int sort) { return (sort && x > kMaxSortX) ? large_sort_ws(b, x) : 0; }
 
+// The register kernel for rows of 257 .. 2048 values (false: not taken).
+template <typename I, typename O, bool TIMES>
+bool rank_reg(const I *in, O *out, int64_t b, int64_t t, int64_t x, cudaStream_t s)
+{
+    if (x <= 256 || x > 8 * kRegThreads || b > 0x7FFFFFFF) return false;
+    const unsigned g = unsigned(b);
+    if (x <= 2 * kRegThreads)
+        rank_sorted_reg_kernel<I, O, TIMES, 2><<<g, kRegThreads, 0, s>>>(in, out, x, int(t));
+    else if (x <= 4 * kRegThreads)
+        rank_sorted_reg_kernel<I, O, TIMES, 4><<<g, kRegThreads, 0, s>>>(in, out, x, int(t));
+    else
+        rank_sorted_reg_kernel<I, O, TIMES, 8><<<g, kRegThreads, 0, s>>>(in, out, x, int(t));
+    SPK_LAUNCHED();
+    return true;
+}
+
 // First-spike times [B, X] u16 of the rank-order (sort) or latency code.
 void rank_times(const void *in, spk_dtype itype, uint16_t *times, int64_t b, int64_t t, int64_t x, int sort, void *ws,
                 cudaStream_t s)
@@ -438,8 +589,11 @@ void rank_times(const void *in, spk_dtype itype, uint16_t *times, int64_t b, int
             k<<<unsigned(b), kCodeThreads, smem, s>>>(p, times, x, int(t), npow2);
         };
         if (itype == SPK_F32)
-            go(rank_sorted_kernel<float, uint16_t, true>, (const float *)in);
-        else
+        {
+            if (!rank_reg<float, uint16_t, true>((const float *)in, times, b, t, x, s))
+                go(rank_sorted_kernel<float, uint16_t, true>, (const float *)in);
+        }
+        else if (!rank_reg<uint8_t, uint16_t, true>((const uint8_t *)in, times, b, t, x, s))
             go(rank_sorted_kernel<uint8_t, uint16_t, true>, (const uint8_t *)in);
     }
     else if (itype == SPK_F32)
@@ -488,6 +642,16 @@ spk_status spk_rank_code(const void *in, spk_dtype itype, void *out, spk_dtype o
             while (npow2 < x) npow2 <<= 1;
             size_t smem = size_t(npow2) * 8 + size_t(x) * 2 + 16;
             SPK_REQUIRE(otype == SPK_U8 || otype == SPK_F32, "output type must be U8 or F32");
+            cudaStream_t cs = stream_of(stream);
+            if (itype == SPK_F32 && otype == SPK_U8 && rank_reg<float, uint8_t, false>((const float *)in, (uint8_t *)out,
+                                                                                       b, t, x, cs))
+                return;
+            if (itype == SPK_F32 && otype == SPK_F32 && rank_reg<float, float, false>((const float *)in, (float *)out,
+                                                                                      b, t, x, cs))
+                return;
+            if (itype == SPK_U8 && otype == SPK_U8 && rank_reg<uint8_t, uint8_t, false>((const uint8_t *)in,
+                                                                                        (uint8_t *)out, b, t, x, cs))
+                return;
             if (itype == SPK_F32 && otype == SPK_U8)
             {
                 auto k = rank_sorted_kernel<float, uint8_t>;

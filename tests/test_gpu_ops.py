@@ -136,6 +136,29 @@ def test_code_large_images(port):
     assert np.array_equal(off, want[0]) and np.array_equal(zyx, want[1].reshape(-1, 3))
 
 
+@pytest.mark.parametrize("x", [257, 300, 512, 513, 700, 1024, 1100, 1568, 2000, 2048])
+def test_code_row_sizes(port, x):
+    """Rows of 257..2048 values take the 256-thread register sort (2, 4 or 8
+    keys per thread): F32 with a tied minimum and ties inside, u8 full of
+    ties, F32 output, sizes off the 16-byte vector width, and the event-list
+    times."""
+    rng = np.random.default_rng(x)
+    f = rng.random((5, x), dtype=np.float32)
+    f[f < 0.4] = 0
+    f[:, ::7] = f[:, 3:4]  # equal values across the row
+    assert np.array_equal(host(spyker.code(cuda(f), 15)), stable_code(f, 15))
+    u8 = (rng.random((3, x)) * 9).astype(np.uint8)
+    assert np.array_equal(host(spyker.code(cuda(u8), 11)), stable_code(u8, 11))
+    assert np.array_equal(host(spyker.code(cuda(f), 7, dtype="f32")), stable_code(f, 7).astype(np.float32))
+    if x % 16:
+        return  # event coordinates are 8-bit: lay the row out as [x / 16, 1, 16]
+    img = f.reshape(5, x // 16, 1, 16)
+    ev = spyker.sparse.code(cuda(img), 15)
+    want = port.sparse_from_dense(stable_code(img, 15).reshape(5, 15, x // 16, 1, 16))
+    off, zyx = ev.lists()
+    assert np.array_equal(off, want[0]) and np.array_equal(zyx, want[1].reshape(-1, 3))
+
+
 def test_code_u8_and_edges(port):
     img = synth.strokes(16, seed=3)
     assert np.array_equal(host(spyker.code(cuda(img), 10, sort=False)), port.rank_code(img, 10, False))
