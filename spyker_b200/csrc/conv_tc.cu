@@ -2519,6 +2519,45 @@ __device__ __forceinline__ void write_block_words(uint8_t *dst, int64_t n, int h
     }
 }
 
+// The same from the (channel, pixel) slab of one step: when a slab of C x HW
+// bytes is a multiple of 16 and a plane a multiple of 4 pixels, a thread
+// takes one 16-byte chunk of the slab (four 4-pixel words, each inside one
+// plane), reads its pixels' winner and first-step bytes once and writes that
+// chunk for every step (T stores of one compare and mask per word).
+__device__ __forceinline__ void write_slab_words(uint8_t *dst, int T, int C, int hw, bool lean, bool pass0,
+                                                 const uint8_t *wsrc, const uint8_t *tsrc, int tstride)
+{
+    const int slab = C * hw, nq = slab / 16;
+    for (int q = threadIdx.x; q < nq; q += blockDim.x)
+    {
+        uint32_t eq[4], tw[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+        {
+            const int f = 16 * q + 4 * r, c = f / hw, px = f - c * hw;
+            if (pass0)
+            {
+                eq[r] = bytes_eq(*reinterpret_cast<const uint32_t *>(wsrc + px), uint32_t(c) * 0x01010101u);
+                tw[r] = *reinterpret_cast<const uint32_t *>(tsrc + px);
+            }
+            else
+            {
+                eq[r] = 0x80808080u;
+                tw[r] = *reinterpret_cast<const uint32_t *>(tsrc + c * tstride + px);
+            }
+            if (!lean) eq[r] = 0u;
+        }
+        uint4 *d = reinterpret_cast<uint4 *>(dst) + q;
+        for (int t = 0; t < T; ++t)
+        {
+            const uint32_t t4 = uint32_t(t) * 0x01010101u;
+            d[int64_t(t) * (slab / 16)] =
+                make_uint4((eq[0] & bytes_le(tw[0], t4)) >> 7, (eq[1] & bytes_le(tw[1], t4)) >> 7,
+                           (eq[2] & bytes_le(tw[2], t4)) >> 7, (eq[3] & bytes_le(tw[3], t4)) >> 7);
+        }
+    }
+}
+
 __global__ void __launch_bounds__(256) search_write_kernel(const int4 *__restrict__ records,
                                                            const uint8_t *__restrict__ gcodes, int64_t npix,
                                                            const int *negw, const int *flag,
@@ -2575,9 +2614,9 @@ __global__ void __launch_bounds__(256) search_write_kernel(const int4 *__restric
             uint8_t *dst = (pass == 0 ? spikes : pooled) + smp * n;
             const bool table = pass == 0 || ptab || !lean;
             const uintptr_t a = reinterpret_cast<uintptr_t>(dst);
-            const bool srcal = gcodes == nullptr || (ohw % 16 == 0);
-            if (table && hw % 16 == 0 && (a & 15) == 0 && srcal)
-                write_plane_words<16>(dst, n, hw, C, lean, pass == 0, wsrc, pass == 0 ? tsrc : first, phw16);
+            if (table && (int64_t(C) * hw) % 16 == 0 && hw % 4 == 0 && (a & 15) == 0 &&
+                (gcodes == nullptr || ohw % 4 == 0))
+                write_slab_words(dst, T, C, hw, lean, pass == 0, wsrc, pass == 0 ? tsrc : first, phw16);
             else if (table && hw % 4 == 0 && hw >= 16 && n % 16 == 0 && (a & 15) == 0 &&
                      (gcodes == nullptr || ohw % 4 == 0))
                 write_block_words(dst, n, hw, C, lean, pass == 0, wsrc, pass == 0 ? tsrc : first, phw16);
