@@ -2421,120 +2421,32 @@ __device__ __forceinline__ uint32_t bytes_le(uint32_t t0, uint32_t t4) { return 
 // Spikes (and pooled spikes) of the search path from the per-pixel records:
 // channel w fires from step t0 on.  A CTA per sample writes its
 // [T, C, OH, OW] block; per pixel the winner and first-step bytes sit in
-// shared memory (or in global memory for maps above 16384 pixels), and a
-// thread makes V output bytes per store (16 when a plane holds a multiple of
-// 16 pixels, else 4) with byte-parallel compares.  Pooled spikes
-// [T, C, POH, POW] come from a byte table of the first firing step per
-// (channel, cell): a cell fires from the earliest t0 of its window's pixels
-// won by that channel.  Off the search path (negative weights or other
-// input) it writes zeros, which the dense kernel then fills.
+// shared memory (or in global memory for maps above 16384 pixels).  Pooled
+// spikes [T, C, POH, POW] come from a byte table of the first firing step
+// per (channel, cell): a cell fires from the earliest t0 of its window's
+// pixels won by that channel.  Off the search path (negative weights or
+// other input) it writes zeros, which the dense kernel then fills.
+//
+// The block is written by (channel, pixel) slabs of one step: when a slab of
+// C x HW bytes is a multiple of V (16 or 4) and a plane a multiple of 4
+// pixels, a thread takes one V-byte chunk of the slab (4-pixel words, each
+// inside one plane), reads its pixels' winner and first-step bytes once and
+// writes that chunk for every step (T stores of one byte-parallel compare
+// and mask per word); other shapes take a byte per thread.
 template <int V>
-__device__ __forceinline__ void write_plane_words(uint8_t *dst, int64_t n, int hw, int C, bool lean, bool pass0,
-                                                  const uint8_t *wsrc, const uint8_t *tsrc, int tstride)
-{
-    using Vec = typename std::conditional<V == 16, uint4, uint32_t>::type;
-    Vec *dv = reinterpret_cast<Vec *>(dst);
-    const int wpp = hw / V, nv = int(n / V);
-    const int dplane = int(blockDim.x) / wpp, dw = int(blockDim.x) - dplane * wpp;
-    int wq = int(threadIdx.x) % wpp, plane = int(threadIdx.x) / wpp;
-    int t = plane / C, c = plane - t * C;
-    for (int i = threadIdx.x; i < nv; i += blockDim.x)
-    {
-        uint32_t o[V / 4];
-#pragma unroll
-        for (int q = 0; q < V / 4; ++q) o[q] = 0u;
-        if (lean)
-        {
-            const int px = V * wq;
-            const uint32_t t4 = uint32_t(t) * 0x01010101u, c4 = uint32_t(c) * 0x01010101u;
-            if (pass0)
-            {
-#pragma unroll
-                for (int q = 0; q < V / 4; ++q)
-                {
-                    const uint32_t w = *reinterpret_cast<const uint32_t *>(wsrc + px + 4 * q);
-                    const uint32_t t0 = *reinterpret_cast<const uint32_t *>(tsrc + px + 4 * q);
-                    o[q] = ((bytes_eq(w, c4) & bytes_le(t0, t4)) >> 7);
-                }
-            }
-            else
-            {
-#pragma unroll
-                for (int q = 0; q < V / 4; ++q)
-                    o[q] = bytes_le(*reinterpret_cast<const uint32_t *>(tsrc + c * tstride + px + 4 * q), t4) >> 7;
-            }
-        }
-        if constexpr (V == 16)
-            dv[i] = make_uint4(o[0], o[1], o[2], o[3]);
-        else
-            dv[i] = o[0];
-        wq += dw, c += dplane;
-        if (wq >= wpp) wq -= wpp, ++c;
-        while (c >= C) c -= C, ++t;
-    }
-}
-
-// The same with 16-byte stores when a plane holds a multiple of 4 pixels but
-// not of 16 (e.g. 14 x 14 maps): each 4-byte word lies in one plane, so a
-// 16-byte chunk spans at most two planes when a plane has 16 pixels or more.
-__device__ __forceinline__ void write_block_words(uint8_t *dst, int64_t n, int hw, int C, bool lean, bool pass0,
-                                                  const uint8_t *wsrc, const uint8_t *tsrc, int tstride)
-{
-    uint4 *dv = reinterpret_cast<uint4 *>(dst);
-    const int wpp = hw / 4, nv = int(n / 16);
-    const int step = 4 * int(blockDim.x);  // words per iteration of the block
-    const int dplane = step / wpp, dw = step - dplane * wpp;
-    int wq = (4 * int(threadIdx.x)) % wpp, plane = (4 * int(threadIdx.x)) / wpp;
-    int t = plane / C, c = plane - t * C;
-    for (int i = threadIdx.x; i < nv; i += blockDim.x)
-    {
-        uint32_t o[4] = {0u, 0u, 0u, 0u};
-        if (lean)
-        {
-            int qw = wq, qc = c, qt = t;
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-            {
-                if (q > 0 && ++qw == wpp)
-                {
-                    qw = 0;
-                    if (++qc == C) qc = 0, ++qt;
-                }
-                const int px = 4 * qw;
-                const uint32_t t4 = uint32_t(qt) * 0x01010101u;
-                if (pass0)
-                {
-                    const uint32_t w = *reinterpret_cast<const uint32_t *>(wsrc + px);
-                    const uint32_t t0 = *reinterpret_cast<const uint32_t *>(tsrc + px);
-                    o[q] = (bytes_eq(w, uint32_t(qc) * 0x01010101u) & bytes_le(t0, t4)) >> 7;
-                }
-                else
-                    o[q] = bytes_le(*reinterpret_cast<const uint32_t *>(tsrc + qc * tstride + px), t4) >> 7;
-            }
-        }
-        dv[i] = make_uint4(o[0], o[1], o[2], o[3]);
-        wq += dw, c += dplane;
-        if (wq >= wpp) wq -= wpp, ++c;
-        while (c >= C) c -= C, ++t;
-    }
-}
-
-// The same from the (channel, pixel) slab of one step: when a slab of C x HW
-// bytes is a multiple of 16 and a plane a multiple of 4 pixels, a thread
-// takes one 16-byte chunk of the slab (four 4-pixel words, each inside one
-// plane), reads its pixels' winner and first-step bytes once and writes that
-// chunk for every step (T stores of one compare and mask per word).
 __device__ __forceinline__ void write_slab_words(uint8_t *dst, int T, int C, int hw, bool lean, bool pass0,
                                                  const uint8_t *wsrc, const uint8_t *tsrc, int tstride)
 {
-    const int slab = C * hw, nq = slab / 16;
+    constexpr int NW = V / 4;
+    using Vec = typename std::conditional<V == 16, uint4, uint32_t>::type;
+    const int slab = C * hw, nq = slab / V;
     for (int q = threadIdx.x; q < nq; q += blockDim.x)
     {
-        uint32_t eq[4], tw[4];
+        uint32_t eq[NW], tw[NW];
 #pragma unroll
-        for (int r = 0; r < 4; ++r)
+        for (int r = 0; r < NW; ++r)
         {
-            const int f = 16 * q + 4 * r, c = f / hw, px = f - c * hw;
+            const int f = V * q + 4 * r, c = f / hw, px = f - c * hw;
             if (pass0)
             {
                 eq[r] = bytes_eq(*reinterpret_cast<const uint32_t *>(wsrc + px), uint32_t(c) * 0x01010101u);
@@ -2547,13 +2459,16 @@ __device__ __forceinline__ void write_slab_words(uint8_t *dst, int T, int C, int
             }
             if (!lean) eq[r] = 0u;
         }
-        uint4 *d = reinterpret_cast<uint4 *>(dst) + q;
+        Vec *d = reinterpret_cast<Vec *>(dst) + q;
         for (int t = 0; t < T; ++t)
         {
             const uint32_t t4 = uint32_t(t) * 0x01010101u;
-            d[int64_t(t) * (slab / 16)] =
-                make_uint4((eq[0] & bytes_le(tw[0], t4)) >> 7, (eq[1] & bytes_le(tw[1], t4)) >> 7,
-                           (eq[2] & bytes_le(tw[2], t4)) >> 7, (eq[3] & bytes_le(tw[3], t4)) >> 7);
+            if constexpr (V == 16)
+                d[int64_t(t) * nq] =
+                    make_uint4((eq[0] & bytes_le(tw[0], t4)) >> 7, (eq[1] & bytes_le(tw[1], t4)) >> 7,
+                               (eq[2] & bytes_le(tw[2], t4)) >> 7, (eq[3] & bytes_le(tw[3], t4)) >> 7);
+            else
+                d[int64_t(t) * nq] = (eq[0] & bytes_le(tw[0], t4)) >> 7;
         }
     }
 }
@@ -2616,12 +2531,10 @@ __global__ void __launch_bounds__(256) search_write_kernel(const int4 *__restric
             const uintptr_t a = reinterpret_cast<uintptr_t>(dst);
             if (table && (int64_t(C) * hw) % 16 == 0 && hw % 4 == 0 && (a & 15) == 0 &&
                 (gcodes == nullptr || ohw % 4 == 0))
-                write_slab_words(dst, T, C, hw, lean, pass == 0, wsrc, pass == 0 ? tsrc : first, phw16);
-            else if (table && hw % 4 == 0 && hw >= 16 && n % 16 == 0 && (a & 15) == 0 &&
+                write_slab_words<16>(dst, T, C, hw, lean, pass == 0, wsrc, pass == 0 ? tsrc : first, phw16);
+            else if (table && (int64_t(C) * hw) % 4 == 0 && hw % 4 == 0 && (a & 3) == 0 &&
                      (gcodes == nullptr || ohw % 4 == 0))
-                write_block_words(dst, n, hw, C, lean, pass == 0, wsrc, pass == 0 ? tsrc : first, phw16);
-            else if (table && hw % 4 == 0 && (a & 3) == 0 && (gcodes == nullptr || ohw % 4 == 0))
-                write_plane_words<4>(dst, n, hw, C, lean, pass == 0, wsrc, pass == 0 ? tsrc : first, phw16);
+                write_slab_words<4>(dst, T, C, hw, lean, pass == 0, wsrc, pass == 0 ? tsrc : first, phw16);
             else
                 for (int64_t f = threadIdx.x; f < n; f += blockDim.x)
                 {
