@@ -2124,15 +2124,18 @@ __global__ void search_init_kernel(unsigned *mins, unsigned *maxs, int64_t b, co
 // inputs that fired of their largest weight over the channels.  A pixel with
 // U at or below the threshold never fires and is settled here; the others go
 // to round 0's list (entry (pixel, T - 1) at the pixel's index, -1 for settled
-// pixels; the list is then compacted in pixel order).  U is summed in FP32 (non-negative terms) and multiplied,
-// rounding up, by 1 + (K + 2) 2^-23, which covers the roundings of that sum,
-// of the oracle's FP64 sum and of its rounding to F32.  One thread per output
-// pixel; the 8 channels of a tap are one 8-byte load of the first-spike map.
+// pixels; the list is then compacted in pixel order).  U is summed in FP32
+// (non-negative terms) and multiplied, rounding up, by 1 + (K + 2) 2^-23,
+// which covers the roundings of that sum, of the oracle's FP64 sum and of its
+// rounding to F32.  A CTA per sample: the sample's first-spike map becomes a
+// byte per input pixel (the channels fired by T - 1) in shared memory, then a
+// thread per output pixel sums its taps from there.
 __global__ void __launch_bounds__(256) search_bound_kernel(TcParams P, const unsigned *__restrict__ wmax, int cp,
                                                            int2 *__restrict__ list)
 {
     if (*P.negw || *P.flag) return;
-    __shared__ float wm[32][8];  // per tap, the 8 channels of one first-spike word
+    extern __shared__ uint8_t s_fired[];  // [H * W]: bit c set when channel c fired by T - 1
+    __shared__ float wm[32][8];          // per tap, the 8 channels of one first-spike word
     const int taps = P.kh * P.kw, kr = P.cin * taps;
     for (int i = threadIdx.x; i < 32 * 8; i += blockDim.x)
     {
@@ -2143,51 +2146,56 @@ __global__ void __launch_bounds__(256) search_bound_kernel(TcParams P, const uns
     // FP32 sum of at most kr non-negative terms: within kr 2^-24 of the exact
     // sum, itself at least the oracle's FP64 sum / (1 + kr 2^-53)
     const float widen = 1.f + float(kr + 2) * 0x1p-23f;
-    const int ohw = int(P.ohw), npix = int(P.npix);
-    const int stride = int(gridDim.x) * blockDim.x;
-    for (int base = int(blockIdx.x) * blockDim.x; base < npix; base += stride)
+    const int ohw = int(P.ohw), hw = P.h * P.w;
+    const uint32_t tt = uint32_t(P.T) * 0x01010101u;
+    const int64_t b = P.npix / ohw;
+    for (int64_t smp = blockIdx.x; smp < b; smp += gridDim.x)
     {
-        const int pix = base + int(threadIdx.x);
-        const bool ok = pix < npix;
-        bool cand = false;
-        int smp = 0;
-        if (ok)
+        const uint8_t *fm = P.in + smp * P.img_stride;
+        __syncthreads();  // the previous sample's bytes are read
+        for (int q = threadIdx.x; q < hw; q += blockDim.x)
         {
-            smp = pix / ohw;
-            const int p = pix - smp * ohw;
+            const uint2 f = __ldg(reinterpret_cast<const uint2 *>(fm + int64_t(q) * cp));
+            // 0x80 in the bytes that fired by step T - 1 (byte < T)
+            const uint32_t lo = ((f.x | 0x80808080u) - tt) ^ 0x80808080u, hi = ((f.y | 0x80808080u) - tt) ^ 0x80808080u;
+            uint32_t m = 0;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) m |= ((lo >> (8 * c + 7)) & 1u) << c | ((hi >> (8 * c + 7)) & 1u) << (c + 4);
+            s_fired[q] = uint8_t(m);
+        }
+        __syncthreads();
+        for (int p = threadIdx.x; p < ohw; p += blockDim.x)
+        {
+            const int pix = int(smp * ohw) + p;
             const int oy = p / P.ow, ox = p - oy * P.ow;
             const int iy0 = oy * P.sy - P.top, ix0 = ox * P.sx - P.left;
             const int ky0 = max(0, -iy0), ky1 = min(P.kh, P.h - iy0);
             const int kx0 = max(0, -ix0), kx1 = min(P.kw, P.w - ix0);
-            const uint8_t *fm = P.in + int64_t(smp) * P.img_stride;
-            const uint32_t tt = uint32_t(P.T) * 0x01010101u;
             float u = 0.f;
             for (int ky = ky0; ky < ky1; ++ky)
                 for (int kx = kx0; kx < kx1; ++kx)
                 {
-                    const uint2 f = __ldg(reinterpret_cast<const uint2 *>(fm + ((iy0 + ky) * P.w + ix0 + kx) * cp));
-                    // 0x80 in the bytes that fired by step T - 1 (byte < T)
-                    const uint32_t lo = ((f.x | 0x80808080u) - tt) ^ 0x80808080u, hi = ((f.y | 0x80808080u) - tt) ^ 0x80808080u;
+                    const uint32_t m = s_fired[(iy0 + ky) * P.w + ix0 + kx];
                     const float *w = wm[ky * P.kw + kx];
 #pragma unroll
                     for (int c = 0; c < 4; ++c)
                     {
-                        u += (lo >> (8 * c + 7)) & 1u ? w[c] : 0.f;
-                        u += (hi >> (8 * c + 7)) & 1u ? w[c + 4] : 0.f;
+                        u += (m >> c) & 1u ? w[c] : 0.f;
+                        u += (m >> (c + 4)) & 1u ? w[c + 4] : 0.f;
                     }
                 }
-            cand = __fmul_ru(u, widen) > P.thr;
-        }
-        if (ok && !cand)
-        {
-            P.records[pix] = make_int4(0, P.T, __float_as_int(P.thv), 0);
-            if (P.wta && P.thv != 0.f)
+            const bool cand = __fmul_ru(u, widen) > P.thr;
+            if (!cand)
             {
-                atomicMin(P.mins + smp, order_enc(P.thv));
-                atomicMax(P.maxs + smp, order_enc(P.thv));
+                P.records[pix] = make_int4(0, P.T, __float_as_int(P.thv), 0);
+                if (P.wta && P.thv != 0.f)
+                {
+                    atomicMin(P.mins + smp, order_enc(P.thv));
+                    atomicMax(P.maxs + smp, order_enc(P.thv));
+                }
             }
+            list[pix] = make_int2(pix, cand ? P.T - 1 : -1);
         }
-        if (ok) list[pix] = make_int2(pix, cand ? P.T - 1 : -1);
     }
 }
 
@@ -3159,7 +3167,7 @@ void search_layer(const TcParams &P0, const FusedLayout &L, const float *kernel,
     // the bound pre-filter of round 0, for layers with few inputs per output
     const int cp = P.nhwc ? P.cpad : P.cin;
     const int kr = P.cin * taps;
-    const bool prefilter = P.cin <= 8 && taps <= 32 && P.cpad == 8;
+    const bool prefilter = P.cin <= 8 && taps <= 32 && P.cpad == 8 && int64_t(P.h) * P.w <= 32768;
     unsigned *wmax = reinterpret_cast<unsigned *>(base + L.wm_off);
     SPK_CUDA(cudaMemsetAsync(cnt, 0, 256, s));
     SPK_CUDA(cudaMemsetAsync(sinfo, 0, 8, s));
@@ -3189,7 +3197,10 @@ void search_layer(const TcParams &P0, const FusedLayout &L, const float *kernel,
     };
     if (prefilter)
     {
-        search_bound_kernel<<<grid_for(L.npix, 256), 256, 0, s>>>(P, wmax, cp, lt);
+        const int64_t hw = P.h * P.w;
+        SPK_CUDA(cudaFuncSetAttribute(search_bound_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(hw)));
+        search_bound_kernel<<<unsigned(std::min<int64_t>(b, int64_t(sm_count()) * 8)), 256, size_t(hw), s>>>(P, wmax,
+                                                                                                        cp, lt);
         SPK_LAUNCHED();
         compact(nullptr, lb, cnt);
     }
