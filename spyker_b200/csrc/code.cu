@@ -186,34 +186,27 @@ __global__ void __launch_bounds__(kCodeThreads) rank_sorted_kernel(const I *__re
         write_rows<O>(out + int64_t(blockIdx.x) * t * x, tm, x, t);
 }
 
-// The same for rows of 256 ITEMS / 2 < X <= 256 ITEMS values with 256
-// threads: thread i holds the keys of positions ITEMS i .. ITEMS i + ITEMS - 1
-// in registers, so a bitonic stage of stride < ITEMS is a compare-exchange
-// inside the thread, strides up to 32 ITEMS / 2 a shuffle with the thread
-// owning the partner positions, and only larger strides go through shared
-// memory (6 of the 66 stages at 2048 keys).  Small blocks let several images
-// share an SM.  The count of values above the minimum comes from the sorted
-// keys.
-constexpr int kRegThreads = 256;
+// Rows of 257 .. 2048 values with 256 threads.  Only the values above the
+// row minimum are sorted: they are compacted in index order into shared
+// memory (a value equal to the minimum at index i has rank cnt + the number
+// of minimum values before it, known from the same prefix count), then
+// sorted by a bitonic network on N = 512, 1024 or 2048 keys (the next power
+// of two, at least 512) whose keys stay in registers: thread i holds
+// positions ITEMS i .. ITEMS i + ITEMS - 1 (ITEMS = N / 256), a stage of
+// stride < ITEMS is a compare-exchange inside the thread, strides up to
+// 32 ITEMS / 2 a shuffle with the thread owning the partner positions, and
+// only larger strides go through shared memory.  With many values tied at
+// the minimum (zero filter responses) the sort is a fraction of the row.
+constexpr int kRegThreads = 256, kRegMax = 8 * kRegThreads;
 
-template <typename I, typename O, bool TIMES, int ITEMS>
-__global__ void __launch_bounds__(kRegThreads) rank_sorted_reg_kernel(const I *__restrict__ in, O *__restrict__ out,
-                                                                      int64_t x, int t)
+template <int ITEMS>
+__device__ __forceinline__ void bitonic_block(uint64_t *keys)
 {
     constexpr int N = kRegThreads * ITEMS;
-    __shared__ uint64_t keys[N];
-    __shared__ __align__(16) uint16_t tm[N];
-    __shared__ uint32_t s_cnt, s_minkey;
     const int tid = threadIdx.x, e0 = ITEMS * tid;
-    const I *row = in + int64_t(blockIdx.x) * x;
     uint64_t k[ITEMS];
 #pragma unroll
-    for (int j = 0; j < ITEMS; ++j)
-    {
-        const int i = e0 + j;
-        k[j] = i < x ? (uint64_t(~order_key(row[i])) << 32) | uint32_t(i) : ~uint64_t(0);
-    }
-    if (tid == 0) s_cnt = 0;
+    for (int j = 0; j < ITEMS; ++j) k[j] = keys[e0 + j];
     for (int size = 2; size <= N; size <<= 1)
     {
         int stride = size >> 1;
@@ -240,8 +233,7 @@ __global__ void __launch_bounds__(kRegThreads) rank_sorted_reg_kernel(const I *_
         for (; stride >= ITEMS; stride >>= 1)
         {
             const int lx = stride / ITEMS;
-            const bool lower = (e0 & stride) == 0;
-            const bool keep_min = lower == ((e0 & size) == 0);
+            const bool keep_min = ((e0 & stride) == 0) == ((e0 & size) == 0);
 #pragma unroll
             for (int j = 0; j < ITEMS; ++j)
             {
@@ -264,24 +256,86 @@ __global__ void __launch_bounds__(kRegThreads) rank_sorted_reg_kernel(const I *_
                 }
         }
     }
-    // the row minimum's key: the last real position
-    if (x - 1 >= e0 && x - 1 < e0 + ITEMS)
-    {
+    __syncthreads();
 #pragma unroll
-        for (int j = 0; j < ITEMS; ++j)
-            if (e0 + j == x - 1) s_minkey = uint32_t(k[j] >> 32);
+    for (int j = 0; j < ITEMS; ++j) keys[e0 + j] = k[j];
+    __syncthreads();
+}
+
+template <typename I, typename O, bool TIMES>
+__global__ void __launch_bounds__(kRegThreads) rank_compact_kernel(const I *__restrict__ in, O *__restrict__ out,
+                                                                   int64_t x, int t)
+{
+    constexpr int IT = kRegMax / kRegThreads;  // values per thread on load
+    __shared__ uint64_t keys[kRegMax];
+    __shared__ __align__(16) uint16_t tm[kRegMax];
+    __shared__ uint32_t s_warp[kRegThreads / 32], s_min, s_off[kRegThreads / 32];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, e0 = IT * tid;
+    const I *row = in + int64_t(blockIdx.x) * x;
+    uint32_t kv[IT];
+    uint32_t mn = 0xFFFFFFFFu;
+#pragma unroll
+    for (int j = 0; j < IT; ++j)
+    {
+        kv[j] = e0 + j < x ? order_key(row[e0 + j]) : 0xFFFFFFFFu;
+        mn = min(mn, kv[j]);
+    }
+    mn = __reduce_min_sync(0xffffffffu, mn);
+    if (lane == 0) s_warp[warp] = mn;
+    __syncthreads();
+    if (tid == 0)
+    {
+        uint32_t m = s_warp[0];
+        for (int w = 1; w < kRegThreads / 32; ++w) m = min(m, s_warp[w]);
+        s_min = m;
     }
     __syncthreads();
-    uint32_t local = 0;
+    const uint32_t minkey = s_min;
+    // keep: the values above the minimum, compacted in index order
+    uint32_t mine = 0;
 #pragma unroll
-    for (int j = 0; j < ITEMS; ++j) local += (e0 + j < x && uint32_t(k[j] >> 32) != s_minkey) ? 1u : 0u;
-    for (int o = 16; o > 0; o >>= 1) local += __shfl_xor_sync(0xffffffffu, local, o);
-    if ((tid & 31) == 0) atomicAdd(&s_cnt, local);
+    for (int j = 0; j < IT; ++j) mine += (e0 + j < x && kv[j] != minkey) ? 1u : 0u;
+    uint32_t incl = mine;
+    for (int o = 1; o < 32; o <<= 1)
+    {
+        const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    if (lane == 31) s_warp[warp] = incl;
     __syncthreads();
-    const float scale = (float(t) + 1e-5f) / float(s_cnt);
+    if (tid == 0)
+    {
+        uint32_t run = 0;
+        for (int w = 0; w < kRegThreads / 32; ++w) s_off[w] = run, run += s_warp[w];
+        s_min = run;  // cnt
+    }
+    __syncthreads();
+    const int cnt = int(s_min);
+    const float scale = (float(t) + 1e-5f) / float(cnt);
+    int kp = int(s_off[warp] + incl - mine);  // keep values before this thread's first
 #pragma unroll
-    for (int j = 0; j < ITEMS; ++j)
-        if (e0 + j < x) tm[uint32_t(k[j])] = f2u16(float(e0 + j) * scale);
+    for (int j = 0; j < IT; ++j)
+    {
+        const int i = e0 + j;
+        if (i < x)
+        {
+            if (kv[j] != minkey)
+                keys[kp++] = (uint64_t(~kv[j]) << 32) | uint32_t(i);
+            else
+                tm[i] = f2u16(float(cnt + i - kp) * scale);  // rank among the ties at the minimum
+        }
+    }
+    int n = 512;
+    while (n < cnt) n <<= 1;
+    for (int i = cnt + tid; i < n; i += kRegThreads) keys[i] = ~uint64_t(0);
+    __syncthreads();
+    if (n == 512)
+        bitonic_block<2>(keys);
+    else if (n == 1024)
+        bitonic_block<4>(keys);
+    else
+        bitonic_block<8>(keys);
+    for (int i = tid; i < cnt; i += kRegThreads) tm[uint32_t(keys[i])] = f2u16(float(i) * scale);
     __syncthreads();
     if constexpr (TIMES)
     {
@@ -548,18 +602,12 @@ uint16_t *large_times_slot(void *ws, int64_t b, int64_t x)
 // Bytes of scratch the sorted code needs (0 when X <= 16384).
 size_t rank_times_ws(int64_t b, int64_t x, int sort) { return (sort && x > kMaxSortX) ? large_sort_ws(b, x) : 0; }
 
-// The register kernel for rows of 257 .. 2048 values (false: not taken).
+// The compacting kernel for rows of 257 .. 2048 values (false: not taken).
 template <typename I, typename O, bool TIMES>
 bool rank_reg(const I *in, O *out, int64_t b, int64_t t, int64_t x, cudaStream_t s)
 {
-    if (x <= 256 || x > 8 * kRegThreads || b > 0x7FFFFFFF) return false;
-    const unsigned g = unsigned(b);
-    if (x <= 2 * kRegThreads)
-        rank_sorted_reg_kernel<I, O, TIMES, 2><<<g, kRegThreads, 0, s>>>(in, out, x, int(t));
-    else if (x <= 4 * kRegThreads)
-        rank_sorted_reg_kernel<I, O, TIMES, 4><<<g, kRegThreads, 0, s>>>(in, out, x, int(t));
-    else
-        rank_sorted_reg_kernel<I, O, TIMES, 8><<<g, kRegThreads, 0, s>>>(in, out, x, int(t));
+    if (x <= 256 || x > kRegMax || b > 0x7FFFFFFF) return false;
+    rank_compact_kernel<I, O, TIMES><<<unsigned(b), kRegThreads, 0, s>>>(in, out, x, int(t));
     SPK_LAUNCHED();
     return true;
 }

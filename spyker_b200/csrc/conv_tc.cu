@@ -2177,12 +2177,7 @@ __global__ void __launch_bounds__(256) search_bound_kernel(TcParams P, const uns
                 {
                     const uint32_t m = s_fired[(iy0 + ky) * P.w + ix0 + kx];
                     const float *w = wm[ky * P.kw + kx];
-#pragma unroll
-                    for (int c = 0; c < 4; ++c)
-                    {
-                        u += (m >> c) & 1u ? w[c] : 0.f;
-                        u += (m >> (c + 4)) & 1u ? w[c + 4] : 0.f;
-                    }
+                    for (int c = 0; c < P.cin; ++c) u += (m >> c) & 1u ? w[c] : 0.f;
                 }
             const bool cand = __fmul_ru(u, widen) > P.thr;
             if (!cand)
