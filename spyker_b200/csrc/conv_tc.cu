@@ -2119,49 +2119,56 @@ __global__ void search_init_kernel(unsigned *mins, unsigned *maxs, int64_t b, co
     }
 }
 
-// Pre-filter of round 0 for layers with few inputs per output: with no
-// negative weight, a pixel's potential at T - 1 is at most U, the sum over the
-// inputs that fired of their largest weight over the channels.  A pixel with
-// U at or below the threshold never fires and is settled here; the others go
-// to round 0's list (entry (pixel, T - 1) at the pixel's index, -1 for settled
-// pixels; the list is then compacted in pixel order).  U is summed in FP32
-// (non-negative terms) and multiplied, rounding up, by 1 + (K + 2) 2^-23,
-// which covers the roundings of that sum, of the oracle's FP64 sum and of its
-// rounding to F32.  A CTA per sample: the sample's first-spike map becomes a
-// byte per input pixel (the channels fired by T - 1) in shared memory, then a
-// thread per output pixel sums its taps from there.
+// Pre-filter of round 0: with no negative weight, a pixel's potential at
+// T - 1 is at most U, the sum over the inputs that fired of their largest
+// weight over the channels.  A pixel with U at or below the threshold never
+// fires and is settled here; the others go to round 0's list (entry
+// (pixel, T - 1) at the pixel's index, -1 for settled pixels; the list is
+// then compacted in pixel order).  U is summed in FP32 (non-negative terms)
+// and multiplied, rounding up, by 1 + (K + 2) 2^-23, which covers the
+// roundings of that sum, of the oracle's FP64 sum and of its rounding to F32.
+// A CTA per sample: the sample's first-spike map becomes a 32-bit mask per
+// input pixel (the channels fired by T - 1, up to 32) in shared memory, the
+// per-tap channel maxima a table beside it; a thread per output pixel adds
+// the maxima of its taps' set bits.
 __global__ void __launch_bounds__(256) search_bound_kernel(TcParams P, const unsigned *__restrict__ wmax, int cp,
                                                            int2 *__restrict__ list)
 {
     if (*P.negw || *P.flag) return;
-    extern __shared__ uint8_t s_fired[];  // [H * W]: bit c set when channel c fired by T - 1
-    __shared__ float wm[32][8];          // per tap, the 8 channels of one first-spike word
-    const int taps = P.kh * P.kw, kr = P.cin * taps;
-    for (int i = threadIdx.x; i < 32 * 8; i += blockDim.x)
+    extern __shared__ uint32_t s_bound_sm[];
+    const int taps = P.kh * P.kw, kr = P.cin * taps, hw = P.h * P.w;
+    uint32_t *s_fired = s_bound_sm;                              // [H * W]
+    float *wm = reinterpret_cast<float *>(s_bound_sm + hw);     // [taps][cp]
+    for (int i = threadIdx.x; i < taps * cp; i += blockDim.x)
     {
-        const int tap = i / 8, c = i % 8;
-        wm[tap][c] = (tap < taps && c < P.cin) ? __uint_as_float(wmax[c * taps + tap]) : 0.f;
+        const int tap = i / cp, c = i % cp;
+        wm[i] = c < P.cin ? __uint_as_float(wmax[c * taps + tap]) : 0.f;
     }
-    __syncthreads();
     // FP32 sum of at most kr non-negative terms: within kr 2^-24 of the exact
     // sum, itself at least the oracle's FP64 sum / (1 + kr 2^-53)
     const float widen = 1.f + float(kr + 2) * 0x1p-23f;
-    const int ohw = int(P.ohw), hw = P.h * P.w;
+    const int ohw = int(P.ohw);
     const uint32_t tt = uint32_t(P.T) * 0x01010101u;
     const int64_t b = P.npix / ohw;
+    const int words = cp / 8;
     for (int64_t smp = blockIdx.x; smp < b; smp += gridDim.x)
     {
         const uint8_t *fm = P.in + smp * P.img_stride;
-        __syncthreads();  // the previous sample's bytes are read
+        __syncthreads();  // the previous sample's masks are read (and the table written)
         for (int q = threadIdx.x; q < hw; q += blockDim.x)
         {
-            const uint2 f = __ldg(reinterpret_cast<const uint2 *>(fm + int64_t(q) * cp));
-            // 0x80 in the bytes that fired by step T - 1 (byte < T)
-            const uint32_t lo = ((f.x | 0x80808080u) - tt) ^ 0x80808080u, hi = ((f.y | 0x80808080u) - tt) ^ 0x80808080u;
             uint32_t m = 0;
+            for (int g = 0; g < words; ++g)
+            {
+                const uint2 f = __ldg(reinterpret_cast<const uint2 *>(fm + int64_t(q) * cp) + g);
+                // 0x80 in the bytes that fired by step T - 1 (byte < T)
+                const uint32_t lo = ((f.x | 0x80808080u) - tt) ^ 0x80808080u;
+                const uint32_t hi = ((f.y | 0x80808080u) - tt) ^ 0x80808080u;
 #pragma unroll
-            for (int c = 0; c < 4; ++c) m |= ((lo >> (8 * c + 7)) & 1u) << c | ((hi >> (8 * c + 7)) & 1u) << (c + 4);
-            s_fired[q] = uint8_t(m);
+                for (int c = 0; c < 4; ++c)
+                    m |= (((lo >> (8 * c + 7)) & 1u) << (8 * g + c)) | (((hi >> (8 * c + 7)) & 1u) << (8 * g + c + 4));
+            }
+            s_fired[q] = m;
         }
         __syncthreads();
         for (int p = threadIdx.x; p < ohw; p += blockDim.x)
@@ -2175,9 +2182,13 @@ __global__ void __launch_bounds__(256) search_bound_kernel(TcParams P, const uns
             for (int ky = ky0; ky < ky1; ++ky)
                 for (int kx = kx0; kx < kx1; ++kx)
                 {
-                    const uint32_t m = s_fired[(iy0 + ky) * P.w + ix0 + kx];
-                    const float *w = wm[ky * P.kw + kx];
-                    for (int c = 0; c < P.cin; ++c) u += (m >> c) & 1u ? w[c] : 0.f;
+                    uint32_t m = s_fired[(iy0 + ky) * P.w + ix0 + kx];
+                    const float *w = wm + (ky * P.kw + kx) * cp;
+                    while (m)
+                    {
+                        u += w[__ffs(int(m)) - 1];
+                        m &= m - 1u;
+                    }
                 }
             const bool cand = __fmul_ru(u, widen) > P.thr;
             if (!cand)
@@ -3162,7 +3173,8 @@ void search_layer(const TcParams &P0, const FusedLayout &L, const float *kernel,
     // the bound pre-filter of round 0, for layers with few inputs per output
     const int cp = P.nhwc ? P.cpad : P.cin;
     const int kr = P.cin * taps;
-    const bool prefilter = P.cin <= 8 && taps <= 32 && P.cpad == 8 && int64_t(P.h) * P.w <= 32768;
+    const int64_t bound_smem = int64_t(P.h) * P.w * 4 + int64_t(taps) * P.cpad * 4;
+    const bool prefilter = P.nhwc && P.cpad <= 32 && bound_smem <= 48 * 1024;
     unsigned *wmax = reinterpret_cast<unsigned *>(base + L.wm_off);
     SPK_CUDA(cudaMemsetAsync(cnt, 0, 256, s));
     SPK_CUDA(cudaMemsetAsync(sinfo, 0, 8, s));
@@ -3192,10 +3204,8 @@ void search_layer(const TcParams &P0, const FusedLayout &L, const float *kernel,
     };
     if (prefilter)
     {
-        const int64_t hw = P.h * P.w;
-        SPK_CUDA(cudaFuncSetAttribute(search_bound_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(hw)));
-        search_bound_kernel<<<unsigned(std::min<int64_t>(b, int64_t(sm_count()) * 8)), 256, size_t(hw), s>>>(P, wmax,
-                                                                                                        cp, lt);
+        search_bound_kernel<<<unsigned(std::min<int64_t>(b, int64_t(sm_count()) * 8)), 256, size_t(bound_smem), s>>>(
+            P, wmax, cp, lt);
         SPK_LAUNCHED();
         compact(nullptr, lb, cnt);
     }
