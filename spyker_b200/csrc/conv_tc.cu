@@ -110,6 +110,7 @@ struct TcParams
     int kreal;              // real K (taps x input channels)
     int r0_list;            // round 0 takes the (pixel, T - 1) entries of list_in (bound pre-filter ran)
     int nparts;             // channel parts of n_tile per tile (search)
+    const uint8_t *tlo;     // search: per pixel, the first step the bound allows a spike at (null: 0)
     // kFused: leave at once when the search path ran (no negative weight and
     // cumulative 0/1 input; these are the words of negw and flag)
     int skip_when_lean;
@@ -1139,7 +1140,7 @@ __device__ __forceinline__ SearchAct search_act(const TcParams &P, int round, in
             r.thv = true;
             return r;
         }
-        lo = -1, hi = T - 1, w = a, vh = v, at = a, vt = v;
+        lo = (P.tlo ? int(P.tlo[pix]) : 0) - 1, hi = T - 1, w = a, vh = v, at = a, vt = v;
     }
     else
     {
@@ -2130,15 +2131,25 @@ __global__ void search_init_kernel(unsigned *mins, unsigned *maxs, int64_t b, co
 // A CTA per sample: the sample's first-spike map becomes a 32-bit mask per
 // input pixel (the channels fired by T - 1, up to 32) in shared memory, the
 // per-tap channel maxima a table beside it; a thread per output pixel adds
-// the maxima of its taps' set bits.
+// the maxima of its taps' set bits.  For a pixel that may fire, the same
+// terms binned by their inputs' first steps (T <= 32: one bin per step and
+// thread in shared memory) give U(t) for every t, and t_lo, the first step
+// whose U(t) (widened the same way) is above the threshold: no channel
+// fires before t_lo, so the bisection starts from (t_lo - 1, T - 1].
 __global__ void __launch_bounds__(256) search_bound_kernel(TcParams P, const unsigned *__restrict__ wmax, int cp,
-                                                           int2 *__restrict__ list)
+                                                           int2 *__restrict__ list, uint8_t *__restrict__ tlo)
 {
     if (*P.negw || *P.flag) return;
-    extern __shared__ uint32_t s_bound_sm[];
+    extern __shared__ __align__(16) uint8_t s_bound_sm[];
     const int taps = P.kh * P.kw, kr = P.cin * taps, hw = P.h * P.w;
-    uint32_t *s_fired = s_bound_sm;                              // [H * W]
-    float *wm = reinterpret_cast<float *>(s_bound_sm + hw);     // [taps][cp]
+    // regions, each 16-byte aligned: masks [H * W], channel maxima [taps][cp],
+    // (tlo) bins [T][blockDim] and the map's bytes [H * W][cp]
+    const int o_w = (hw * 4 + 15) & ~15, o_acc = o_w + ((taps * cp * 4 + 15) & ~15);
+    const int o_fb = o_acc + ((P.T * int(blockDim.x) * 4 + 15) & ~15);
+    uint32_t *s_fired = reinterpret_cast<uint32_t *>(s_bound_sm);
+    float *wm = reinterpret_cast<float *>(s_bound_sm + o_w);
+    float *s_acc = reinterpret_cast<float *>(s_bound_sm + o_acc);
+    uint8_t *s_fb = s_bound_sm + o_fb;
     for (int i = threadIdx.x; i < taps * cp; i += blockDim.x)
     {
         const int tap = i / cp, c = i % cp;
@@ -2161,6 +2172,7 @@ __global__ void __launch_bounds__(256) search_bound_kernel(TcParams P, const uns
             for (int g = 0; g < words; ++g)
             {
                 const uint2 f = __ldg(reinterpret_cast<const uint2 *>(fm + int64_t(q) * cp) + g);
+                if (tlo) reinterpret_cast<uint2 *>(s_fb + q * cp)[g] = f;
                 // 0x80 in the bytes that fired by step T - 1 (byte < T)
                 const uint32_t lo = ((f.x | 0x80808080u) - tt) ^ 0x80808080u;
                 const uint32_t hi = ((f.y | 0x80808080u) - tt) ^ 0x80808080u;
@@ -2191,6 +2203,36 @@ __global__ void __launch_bounds__(256) search_bound_kernel(TcParams P, const uns
                     }
                 }
             const bool cand = __fmul_ru(u, widen) > P.thr;
+            if (cand && tlo)
+            {
+                float *acc = s_acc + threadIdx.x;
+                for (int t = 0; t < P.T; ++t) acc[t * blockDim.x] = 0.f;
+                for (int ky = ky0; ky < ky1; ++ky)
+                    for (int kx = kx0; kx < kx1; ++kx)
+                    {
+                        const int q = (iy0 + ky) * P.w + ix0 + kx;
+                        uint32_t m = s_fired[q];
+                        const float *w = wm + (ky * P.kw + kx) * cp;
+                        while (m)
+                        {
+                            const int c = __ffs(int(m)) - 1;
+                            acc[int(s_fb[q * cp + c]) * blockDim.x] += w[c];
+                            m &= m - 1u;
+                        }
+                    }
+                float run = 0.f;
+                int t0 = P.T - 1;  // no step below T - 1 can fire either when none passes
+                for (int t = 0; t < P.T - 1; ++t)
+                {
+                    run += acc[t * blockDim.x];
+                    if (__fmul_ru(run, widen) > P.thr)
+                    {
+                        t0 = t;
+                        break;
+                    }
+                }
+                tlo[pix] = uint8_t(t0);
+            }
             if (!cand)
             {
                 P.records[pix] = make_int4(0, P.T, __float_as_int(P.thv), 0);
@@ -2980,6 +3022,7 @@ struct FusedLayout
     bool search_ok;
     size_t w4_off, echan_off, wm_off, cnt_off, state_off, la_off, lb_off, fin_off, fa_off, fb_off, va_off, vb_off;
     size_t lt_off, bc_off;  // the rows' next entries by row index, per-block counts of the compaction
+    size_t tlo_off;         // per pixel, the first step the bound allows a spike at
     size_t total;
 };
 
@@ -3029,6 +3072,7 @@ FusedLayout fused_layout(int64_t b, int64_t t, int64_t cin, int64_t h, int64_t w
         L.vb_off = off, off += align256(np * 16);
         L.lt_off = off, off += align256(np * 8);
         L.bc_off = off, off += align256((np / kCompactItems + 2) * 4);
+        L.tlo_off = off, off += align256(np);
     }
     L.total = off;
     return L;
@@ -3173,9 +3217,16 @@ void search_layer(const TcParams &P0, const FusedLayout &L, const float *kernel,
     // the bound pre-filter of round 0, for layers with few inputs per output
     const int cp = P.nhwc ? P.cpad : P.cin;
     const int kr = P.cin * taps;
-    const int64_t bound_smem = int64_t(P.h) * P.w * 4 + int64_t(taps) * P.cpad * 4;
+    // with T <= 32 the pre-filter also bounds each pixel's first step (a bin
+    // per step and thread, and the map's bytes, in shared memory)
+    const bool want_tlo = P.T <= 32;
+    const int64_t bound_base = ((int64_t(P.h) * P.w * 4 + 15) & ~int64_t(15)) + ((int64_t(taps) * P.cpad * 4 + 15) & ~int64_t(15));
+    const int64_t bound_tlo = bound_base + ((int64_t(P.T) * 256 * 4 + 15) & ~int64_t(15)) + int64_t(P.h) * P.w * P.cpad;
+    const bool use_tlo = want_tlo && bound_tlo <= 48 * 1024;
+    const int64_t bound_smem = use_tlo ? bound_tlo : bound_base;
     const bool prefilter = P.nhwc && P.cpad <= 32 && bound_smem <= 48 * 1024;
     unsigned *wmax = reinterpret_cast<unsigned *>(base + L.wm_off);
+    uint8_t *tlo = base + L.tlo_off;
     SPK_CUDA(cudaMemsetAsync(cnt, 0, 256, s));
     SPK_CUDA(cudaMemsetAsync(sinfo, 0, 8, s));
     if (prefilter) SPK_CUDA(cudaMemsetAsync(wmax, 0, size_t(kr) * 4, s));
@@ -3205,10 +3256,11 @@ void search_layer(const TcParams &P0, const FusedLayout &L, const float *kernel,
     if (prefilter)
     {
         search_bound_kernel<<<unsigned(std::min<int64_t>(b, int64_t(sm_count()) * 8)), 256, size_t(bound_smem), s>>>(
-            P, wmax, cp, lt);
+            P, wmax, cp, lt, use_tlo ? tlo : nullptr);
         SPK_LAUNCHED();
         compact(nullptr, lb, cnt);
     }
+    P.tlo = prefilter && use_tlo ? tlo : nullptr;
     const unsigned fix_grid = unsigned(sm_count() * 4);
     int nsr = 0;
     while ((1 << nsr) < P.T) ++nsr;
