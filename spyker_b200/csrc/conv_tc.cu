@@ -3255,7 +3255,7 @@ void search_layer(const TcParams &P0, const FusedLayout &L, const float *kernel,
     };
     if (prefilter)
     {
-        search_bound_kernel<<<unsigned(std::min<int64_t>(b, int64_t(sm_count()) * 8)), 256, size_t(bound_smem), s>>>(
+        search_bound_kernel<<<unsigned(std::min<int64_t>(b, 0x7FFFFFFF)), 256, size_t(bound_smem), s>>>(
             P, wmax, cp, lt, use_tlo ? tlo : nullptr);
         SPK_LAUNCHED();
         compact(nullptr, lb, cnt);
