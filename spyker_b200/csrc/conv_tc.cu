@@ -2529,6 +2529,71 @@ __device__ __forceinline__ void write_slab_words(uint8_t *dst, int T, int C, int
     }
 }
 
+// Maps above 16384 pixels (per-pixel winner and first-step bytes in global
+// memory): a grid of CTAs per sample (blockIdx.y), each thread one 16-byte
+// chunk of a step's (channel, pixel) slab for every step; pooled spikes a
+// 4-cell word at a time, each cell's first firing step for the word's channel
+// taken over its window (T: never) and compared with every step.  Needs
+// C x OH x OW a multiple of 16, OH x OW and the pooled width multiples of 4.
+__global__ void __launch_bounds__(256) search_write_large_kernel(const uint8_t *__restrict__ codes, int64_t npix,
+                                                                 const int *negw, const int *flag,
+                                                                 uint8_t *__restrict__ spikes,
+                                                                 uint8_t *__restrict__ pooled, int T, int C, int ohw,
+                                                                 int ow, int pky, int pkx, int poh, int pow_)
+{
+    const bool lean = !*negw && !*flag;
+    const int64_t smp = blockIdx.y;
+    const uint8_t *wb = codes + smp * ohw, *tb = codes + npix + smp * ohw;
+    const int64_t step = int64_t(gridDim.x) * blockDim.x;
+    {
+        const int64_t slab = int64_t(C) * ohw, nq = slab / 16;
+        uint4 *dst = reinterpret_cast<uint4 *>(spikes + smp * T * slab);
+        for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < nq; q += step)
+        {
+            uint32_t eq[4], tw[4];
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+            {
+                const int64_t f = 16 * q + 4 * r;
+                const int c = int(f / ohw), px = int(f - int64_t(c) * ohw);
+                eq[r] = lean ? bytes_eq(*reinterpret_cast<const uint32_t *>(wb + px), uint32_t(c) * 0x01010101u) : 0u;
+                tw[r] = *reinterpret_cast<const uint32_t *>(tb + px);
+            }
+            for (int t = 0; t < T; ++t)
+            {
+                const uint32_t t4 = uint32_t(t) * 0x01010101u;
+                dst[int64_t(t) * nq + q] =
+                    make_uint4((eq[0] & bytes_le(tw[0], t4)) >> 7, (eq[1] & bytes_le(tw[1], t4)) >> 7,
+                               (eq[2] & bytes_le(tw[2], t4)) >> 7, (eq[3] & bytes_le(tw[3], t4)) >> 7);
+            }
+        }
+    }
+    if (pooled == nullptr) return;
+    const int phw = poh * pow_;
+    const int64_t slab = int64_t(C) * phw, nw = slab / 4;
+    uint32_t *dst = reinterpret_cast<uint32_t *>(pooled + smp * T * slab);
+    for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < nw; q += step)
+    {
+        const int64_t f = 4 * q;
+        const int c = int(f / phw), cell = int(f - int64_t(c) * phw), py = cell / pow_, px = cell - py * pow_;
+        uint32_t first = 0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+        {
+            int m = T;
+            for (int dy = 0; dy < pky; ++dy)
+                for (int dx = 0; dx < pkx; ++dx)
+                {
+                    const int i = (py * pky + dy) * ow + (px + j) * pkx + dx;
+                    if (int(wb[i]) == c) m = min(m, int(tb[i]));
+                }
+            first |= uint32_t(m) << (8 * j);
+        }
+        for (int t = 0; t < T; ++t)
+            dst[int64_t(t) * nw + q] = lean ? bytes_le(first, uint32_t(t) * 0x01010101u) >> 7 : 0u;
+    }
+}
+
 __global__ void __launch_bounds__(256) search_write_kernel(const int4 *__restrict__ records,
                                                            const uint8_t *__restrict__ gcodes, int64_t npix,
                                                            const int *negw, const int *flag,
@@ -2540,7 +2605,9 @@ __global__ void __launch_bounds__(256) search_write_kernel(const int4 *__restric
     extern __shared__ __align__(16) uint8_t wsm_[];
     const bool lean = !*negw && !*flag;
     const int ohw16 = (ohw + 15) & ~15, phw = poh * pow_, phw16 = (phw + 15) & ~15;
-    uint8_t *sw = wsm_, *st = wsm_ + ohw16, *first = wsm_ + 2 * ohw16;
+    // (maps above 16384 pixels keep their bytes in global memory: the table
+    // then starts at byte 32, as the launch sizes it)
+    uint8_t *sw = wsm_, *st = wsm_ + ohw16, *first = wsm_ + (gcodes ? 32 : 2 * ohw16);
     for (int64_t smp = blockIdx.x; smp < b; smp += gridDim.x)
     {
         const uint8_t *wsrc = gcodes ? gcodes + smp * ohw : sw;
@@ -3294,6 +3361,18 @@ void search_layer(const TcParams &P0, const FusedLayout &L, const float *kernel,
         wsm = 2 * 16;
         search_codes_kernel<<<grid_for(L.npix, 256), 256, 0, s>>>(P.records, gcodes, L.npix, P.T, P.negw, P.flag);
         SPK_LAUNCHED();
+    }
+    if (gcodes && (int64_t(P.cout) * ohw) % 16 == 0 && ohw % 4 == 0 && reinterpret_cast<uintptr_t>(spikes) % 16 == 0 &&
+        (pool_ky == 0 || (pow_ % 4 == 0 && reinterpret_cast<uintptr_t>(pooled) % 4 == 0)) && b <= 65535)
+    {
+        const int64_t nq = int64_t(P.cout) * ohw / 16;
+        const unsigned xb = unsigned(std::max<int64_t>(1, std::min<int64_t>(ceil_div(nq, 256 * 8),
+                                                                            ceil_div(int64_t(sm_count()) * 8, b))));
+        search_write_large_kernel<<<dim3(xb, unsigned(b)), 256, 0, s>>>(
+            gcodes, L.npix, P.negw, P.flag, spikes, pool_ky > 0 ? pooled : nullptr, P.T, P.cout, ohw, int(L.ow),
+            int(pool_ky), int(pool_kx), int(poh), int(pow_));
+        SPK_LAUNCHED();
+        return;
     }
     // byte table of first firing steps per (channel, pooled cell) when it fits
     const size_t tab_bytes = size_t(P.cout) * size_t(((poh * pow_) + 15) & ~15);

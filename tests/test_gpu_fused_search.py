@@ -174,3 +174,22 @@ def test_search_channel_parts(port, kind):
     w[200:] = w[:56]  # channels 200.. tie exactly with channels 0..55 (other part)
     th = float(np.round(np.median(port.conv(x[:, -1:], w, (1, 1), (pad,) * 4)) * 2) / 2)
     assert check(port, x, w, max(th, 1.0), 1, 4, pad)[0] > 0
+
+
+@pytest.mark.parametrize("side", [136, 132])
+def test_search_large_maps(port, side):
+    """Maps above 16384 output pixels (per-pixel codes in global memory, no
+    WTA): 136 x 136 takes the multi-CTA writer (pooled width a multiple of
+    4), 132 x 132 the per-sample one; spikes and pooled spikes equal the
+    oracle's pipeline."""
+    rng = np.random.default_rng(side)
+    x = cumulative(rng, 2, 6, 2, side, side)
+    w = rng.uniform(0.3, 1.0, size=(8, 2, 3, 3)).astype(np.float32)
+    conv = spyker.Conv(2, 8, 3, pad=1)
+    conv.kernel.copy_(cuda(w))
+    conv.precision = "bf16x3"
+    spk, wins, pooled = spyker.conv_fire_wta(cuda(x), conv, 4.0, 0, 0, pool=2)
+    assert wins is None and spyker._lib.lib.spk_device_status(1) == 0
+    ref = port.fire(port.inhibit(port.threshold(port.conv(x, w, (1, 1), (1, 1, 1, 1)), 4.0)))
+    assert np.array_equal(host(spk), ref) and int(ref.sum()) > 0
+    assert np.array_equal(host(pooled), port.pool(ref, (2, 2)))
