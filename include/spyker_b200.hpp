@@ -165,6 +165,14 @@ public:
         _data = std::shared_ptr<void>(p, [](void *q) { cudaFree(q); });
     }
     explicit Tensor(const Shape &shape, Type type = Type::F32) : Tensor(type, shape) {}
+    /* A view of caller-owned device memory (not freed here); the reference's
+     * Tensor(data, device, type, shape) wrapping a raw pointer. */
+    Tensor(void *device_data, Type type, const Shape &shape) : _shape(shape), _type(type)
+    {
+        for (Size d : shape) detail::require(d >= 0, "Tensor shape can't be negative.");
+        detail::require(device_data != nullptr || detail::prod(shape) == 0, "Tensor data can't be null.");
+        _data = std::shared_ptr<void>(device_data, [](void *) {});
+    }
 
     static Tensor from_host(const void *host, Type type, const Shape &shape)
     {
@@ -294,21 +302,37 @@ inline std::vector<F64> configs(const std::vector<STDPConfig> &c)
 
 /* ---- coding and elementwise (opers.h:598-700) ----------------------------- */
 
-/* [B, ...] -> [B, T, ...] cumulative spikes; sort: rank order (opers.cpp code). */
-inline Tensor code(Tensor input, Size time, bool sort = true, Type type = Type::U8)
+namespace detail
+{
+inline void require_shape(const Tensor &t, const Shape &s, const char *msg) { require(t.shape() == s, msg); }
+}  // namespace detail
+
+/* [B, ...] -> output [B, T, ...] cumulative spikes; sort: rank order
+ * (opers.h:632, the output's type chosen by the caller). */
+inline Tensor code(Tensor input, Tensor output, Size time, bool sort = true)
 {
     detail::require(time > 0, "Input time can't be less than 1.");
     detail::require(input.dims() >= 2, "Input dimensions must be at least 2.");
     const Shape s = input.shape();
     Shape o{s[0], time};
     o.insert(o.end(), s.begin() + 1, s.end());
-    Tensor out(type, o);
+    detail::require_shape(output, o, "Output shape is not compatible with the input.");
     const Size x = detail::prod(s, 1);
     detail::Scratch ws(spk_rank_code_workspace(s[0], x, int(sort)));
-    detail::check(spk_rank_code(input.data(), detail::dt(input.type()), out.data(), detail::dt(type), s[0], time, x,
-                                int(sort), ws.ptr, ws.bytes, stream()),
+    detail::check(spk_rank_code(input.data(), detail::dt(input.type()), output.data(), detail::dt(output.type()), s[0],
+                                time, x, int(sort), ws.ptr, ws.bytes, stream()),
                   "code");
-    return out;
+    return output;
+}
+
+/* [B, ...] -> [B, T, ...] cumulative spikes; sort: rank order (opers.h:621). */
+inline Tensor code(Tensor input, Size time, bool sort = true, Type type = Type::U8)
+{
+    detail::require(input.dims() >= 2, "Input dimensions must be at least 2.");
+    const Shape s = input.shape();
+    Shape o{s[0], std::max<Size>(time, 0)};
+    o.insert(o.end(), s.begin() + 1, s.end());
+    return code(input, Tensor(type, o), time, sort);
 }
 
 inline Tensor threshold(Tensor input, F64 threshold, F64 value = 0, bool inplace = true)
@@ -329,27 +353,41 @@ inline Tensor infinite(Tensor input, F64 value = 0, bool inplace = true)
     return t;
 }
 
+inline Tensor fire(Tensor input, Tensor output, F64 threshold = 0)
+{
+    detail::require_shape(output, input.shape(), "Output shape is not compatible with the input.");
+    detail::check(spk_rank_fire(input.data(), detail::dt(input.type()), output.data(), detail::dt(output.type()),
+                                input.numel(), threshold, stream()),
+                  "fire");
+    return output;
+}
+
 inline Tensor fire(Tensor input, F64 threshold = 0, Type type = Type::U8)
 {
-    Tensor out(type, input.shape());
-    detail::check(spk_rank_fire(input.data(), detail::dt(input.type()), out.data(), detail::dt(type), input.numel(),
-                                threshold, stream()),
-                  "fire");
-    return out;
+    return fire(input, Tensor(type, input.shape()), threshold);
 }
 
 /* [B, T, ...] -> [B, ...] first step above the threshold (T when none). */
+inline Tensor gather(Tensor input, Tensor output, F64 threshold = 0)
+{
+    detail::require(input.dims() >= 3, "Input dimensions must be at least 3.");
+    Shape o{input.shape(0)};
+    const Shape s = input.shape();
+    o.insert(o.end(), s.begin() + 2, s.end());
+    detail::require_shape(output, o, "Output shape is not compatible with the input.");
+    detail::check(spk_rank_gather(input.data(), detail::dt(input.type()), output.data(), detail::dt(output.type()), s[0],
+                                  s[1], detail::prod(s, 2), threshold, stream()),
+                  "gather");
+    return output;
+}
+
 inline Tensor gather(Tensor input, F64 threshold = 0, Type type = Type::U8)
 {
     detail::require(input.dims() >= 3, "Input dimensions must be at least 3.");
     Shape o{input.shape(0)};
     const Shape s = input.shape();
     o.insert(o.end(), s.begin() + 2, s.end());
-    Tensor out(type, o);
-    detail::check(spk_rank_gather(input.data(), detail::dt(input.type()), out.data(), detail::dt(type), s[0], s[1],
-                                  detail::prod(s, 2), threshold, stream()),
-                  "gather");
-    return out;
+    return gather(input, Tensor(type, o), threshold);
 }
 
 /* [B, ...] first-spike times -> [B, T, ...] cumulative spikes. */
@@ -384,6 +422,28 @@ inline Tensor pad(Tensor input, Expand4 pad, F64 value = 0)
 
 /* Max pooling of the last two dimensions; stride 0 = the window
  * (opers.h:709, cpu/pool.cpp:53-86). */
+inline Tensor pool(Tensor input, Tensor output, Expand2 kernel, Expand2 stride = 0, Expand4 pad = 0)
+{
+    detail::require(input.dims() >= 3, "Input dimensions must be at least 3.");
+    detail::require(output.type() == input.type(), "Output type must be the input's.");
+    if (stride[0] == 0 && stride[1] == 0) stride = kernel;
+    detail::require(kernel[0] > 0 && kernel[1] > 0 && stride[0] > 0 && stride[1] > 0 && pad[0] >= 0 && pad[1] >= 0 &&
+                        pad[2] >= 0 && pad[3] >= 0,
+                    "Kernel, stride or pad items are incorrect.");
+    Shape o = input.shape();
+    const Size h = o[o.size() - 2], w = o[o.size() - 1];
+    const Size oh = (h + pad[0] + pad[2] - kernel[0]) / stride[0] + 1;
+    const Size ow = (w + pad[1] + pad[3] - kernel[1]) / stride[1] + 1;
+    detail::require(oh > 0 && ow > 0, "Input and kernel shapes are not compatible.");
+    o[o.size() - 2] = oh, o[o.size() - 1] = ow;
+    detail::require_shape(output, o, "Output shape is not compatible with the input.");
+    const auto p = detail::pad4(pad);
+    detail::check(spk_rank_pool(input.data(), output.data(), detail::dt(input.type()), input.numel() / (h * w), h, w,
+                                oh, ow, kernel[0], kernel[1], stride[0], stride[1], p.data(), stream()),
+                  "pool");
+    return output;
+}
+
 inline Tensor pool(Tensor input, Expand2 kernel, Expand2 stride = 0, Expand4 pad = 0)
 {
     detail::require(input.dims() >= 3, "Input dimensions must be at least 3.");
@@ -451,7 +511,35 @@ inline Winners fcwta(Tensor input, Size radius, Size count, F64 threshold = 0)
 /* ---- convolution (opers.h:545-555) ------------------------------------------ */
 
 /* [B, T, Cin, H, W] (or [N, Cin, H, W]) x [Cout, Cin, KH, KW] F32 ->
- * F32 potentials [B, T, Cout, OH, OW]. */
+ * F32 potentials [B, T, Cout, OH, OW] written to output (opers.h:555). */
+inline Tensor conv(Tensor input, Tensor kernel, Tensor output, Expand2 stride = 1, Expand4 pad = 0,
+                   int precision = SPK_CONV_FP32)
+{
+    detail::require(input.dims() == 4 || input.dims() == 5, "Input dimensions must be 4 or 5.");
+    detail::require(kernel.dims() == 4 && kernel.type() == Type::F32, "Kernel must be a 4D F32 tensor.");
+    detail::require(output.type() == Type::F32, "Output must be F32.");
+    detail::require(stride[0] > 0 && stride[1] > 0 && pad[0] >= 0 && pad[1] >= 0 && pad[2] >= 0 && pad[3] >= 0,
+                    "Stride or pad items are incorrect.");
+    const Shape s = input.shape();
+    const size_t d = s.size();
+    const Size cin = s[d - 3], h = s[d - 2], w = s[d - 1];
+    const Size cout = kernel.shape(0), kh = kernel.shape(2), kw = kernel.shape(3);
+    detail::require(kernel.shape(1) == cin, "Input and kernel channels are not compatible.");
+    const Size oh = (h + pad[0] + pad[2] - kh) / stride[0] + 1, ow = (w + pad[1] + pad[3] - kw) / stride[1] + 1;
+    detail::require(oh > 0 && ow > 0, "Input and kernel shapes are not compatible.");
+    Shape o(s.begin(), s.end() - 3);
+    o.insert(o.end(), {cout, oh, ow});
+    detail::require_shape(output, o, "Output shape is not compatible with the input.");
+    const Size n = detail::prod(s, 0, d - 3);
+    const auto p = detail::pad4(pad);
+    detail::Scratch ws(spk_conv_workspace(n, cin, h, w, cout, kh, kw, precision));
+    detail::check(spk_conv(input.data(), detail::dt(input.type()), kernel.data<float>(), output.data<float>(), n, cin, h,
+                           w, cout, kh, kw, stride[0], stride[1], p.data(), precision, ws.ptr, ws.bytes, stream()),
+                  "conv");
+    return output;
+}
+
+/* The same into a new F32 tensor (opers.h:545). */
 inline Tensor conv(Tensor input, Tensor kernel, Expand2 stride = 1, Expand4 pad = 0,
                    int precision = SPK_CONV_FP32)
 {

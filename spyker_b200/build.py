@@ -72,5 +72,31 @@ def build(verbose: bool = False, force: bool = False) -> str:
     return LIB
 
 
+def build_plugin(verbose: bool = False, force: bool = False) -> str:
+    """The pybind11 module ``spyker_b200_plugin`` (plugin/plugin.cpp over the
+    C++ layer include/spyker_b200.hpp) next to the library, which it links."""
+    import sysconfig
+
+    import pybind11
+
+    src = os.path.join(HERE, "plugin", "plugin.cpp")
+    out = os.path.join(LIB_DIR, "spyker_b200_plugin" + sysconfig.get_config_var("EXT_SUFFIX"))
+    deps = [src, LIB, os.path.join(ROOT, "include", "spyker_b200.hpp"), os.path.join(ROOT, "include", "spyker_b200.h")]
+    if os.path.exists(out) and not force and os.path.getmtime(out) >= max(os.path.getmtime(d) for d in deps):
+        return out
+    cuda = os.path.dirname(os.path.dirname(nvcc()))
+    cmd = [shutil.which("g++") or "g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-I", os.path.join(ROOT, "include"),
+           "-I", os.path.join(cuda, "include"), "-I", pybind11.get_include(), "-I", sysconfig.get_paths()["include"],
+           src, "-o", out, "-L", LIB_DIR, "-lspyker_b200", "-L", os.path.join(cuda, "lib64"), "-lcudart",
+           "-Wl,-rpath,$ORIGIN", "-Wl,-rpath," + os.path.join(cuda, "lib64")]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"plugin build failed:\n{res.stdout}\n{res.stderr}")
+    return out
+
+
 if __name__ == "__main__":
     print(build(verbose="-v" in sys.argv, force="-f" in sys.argv))
+    print(build_plugin(verbose="-v" in sys.argv, force="-f" in sys.argv))

@@ -94,3 +94,76 @@ def test_cpp_layer_matches_python(tmp_path):
     k1 = _load(out, "kernel1", np.float32, (12, 2, 5, 5))
     assert np.array_equal(conv.kernel.cpu().numpy(), k1)
     assert not np.array_equal(k1, _load(out, "kernel0", np.float32, (12, 2, 5, 5)))
+
+
+def _plugin():
+    import importlib.util
+    import sysconfig
+
+    path = os.path.join(LIB, "spyker_b200_plugin" + sysconfig.get_config_var("EXT_SUFFIX"))
+    if not os.path.exists(path):
+        pytest.skip("plugin not built")
+    spec = importlib.util.spec_from_file_location("spyker_b200_plugin", path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def test_plugin_surface():
+    """The pybind11 module exposes the reference plugin's hot-path names."""
+    p = _plugin()
+    for name in ("Tensor", "tensor", "from_numpy", "Winner", "DoGFilter", "STDPConfig", "DoG", "Conv", "conv", "pad",
+                 "threshold", "code", "infinite", "fire", "gather", "pool", "inhibit", "fcwta", "convwta",
+                 "conv_fire_wta", "synchronize"):
+        assert hasattr(p, name), name
+
+
+@pytest.mark.gpu
+def test_plugin_matches_python():
+    """A layer step through the plugin on views of torch CUDA tensors equals
+    the Python API's: rank code into a given output, the plain ops, the fused
+    layer, and STDP with the fused layer's winners."""
+    import torch
+
+    import spyker_b200 as spyker
+
+    p = _plugin()
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(5)
+    b, t = 4, 15
+    img = torch.from_numpy(rng.random((b, 2, 20, 22), dtype=np.float32)).to(dev)
+    img[img < 0.5] = 0
+    codes = torch.empty((b, t, 2, 20, 22), dtype=torch.uint8, device=dev)
+    view = lambda x, ty: p.tensor(x.data_ptr(), ty, list(x.shape))  # noqa: E731
+    p.code(view(img, "f32"), view(codes, "u8"), t, True, "rank")
+    p.synchronize()
+    assert torch.equal(codes, spyker.code(img, t))
+    w = torch.from_numpy(rng.uniform(0.3, 1.0, size=(10, 2, 5, 5)).astype(np.float32)).to(dev)
+    pot = torch.empty((b, t, 10, 20, 22), dtype=torch.float32, device=dev)
+    p.conv(view(codes, "u8"), view(w, "f32"), view(pot, "f32"), [1], [2])
+    p.threshold(view(pot, "f32"), 4.0, 0.0)
+    p.inhibit(view(pot, "f32"), 0.0)
+    spk = torch.empty_like(pot, dtype=torch.uint8)
+    p.fire(view(pot, "f32"), view(spk, "u8"), 0.0, "rank")
+    wins = p.convwta(view(pot, "f32"), [2], 3, 0.0)
+    p.synchronize()
+    conv = spyker.Conv(2, 10, 5, pad=2)
+    conv.kernel.copy_(w)
+    conv.precision = "fp32"
+    ref = spyker.inhibit(spyker.threshold(conv(codes), 4.0))
+    assert torch.equal(spk, spyker.fire(ref))
+    rw = spyker.convwta(ref, 2, 3)
+    assert [[(x.c, x.t, x.z, x.y, x.x) for x in s] for s in wins] == [[(x.c, x.t, x.z, x.y, x.x) for x in s] for s in rw]
+    layer = p.Conv(2, 10, [5], [1], [2], 0.5, 0.02)
+    p.from_numpy(w.cpu().numpy())  # host round trip
+    layer.kernel = p.from_numpy(w.cpu().numpy())
+    layer.precision = p.CONV_BF16X3
+    layer.stdpconfig = [p.STDPConfig(0.004, -0.003)]
+    fspk, fwins, fpool = p.conv_fire_wta(view(codes, "u8"), layer, 4.0, [2], 3, [2])
+    conv.precision = "bf16x3"
+    gspk, gwins, gpool = spyker.conv_fire_wta(codes, conv, 4.0, 2, 3, pool=2)
+    assert np.array_equal(fspk.numpy(), gspk.cpu().numpy()) and np.array_equal(fpool.numpy(), gpool.cpu().numpy())
+    layer._stdp(view(codes, "u8"), fwins, fspk)
+    conv.stdpconfig = [spyker.STDPConfig(0.004, -0.003)]
+    conv.stdp(codes, gwins, gspk)
+    assert np.array_equal(layer.kernel.numpy(), conv.kernel.cpu().numpy())
