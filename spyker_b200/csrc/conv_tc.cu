@@ -52,6 +52,8 @@ using namespace tc;
 constexpr int BM = 128, BK = 64;
 constexpr uint32_t kMaxProbes = 1u << 22;
 constexpr int kMaxKBlocks = 128;  // K up to 8192
+// entries per block of a row-list compaction
+constexpr int kCompactShift = 11, kCompactItems = 1 << kCompactShift;
 
 struct TcParams
 {
@@ -98,6 +100,7 @@ struct TcParams
     const int2 *list_in;
     const int *count_in;
     int2 *list_out, *final_list;  // list_out: each row's next entry at the row's index
+    int *list_bc;                 // per compaction block of list_out, its entries with a step (added by the writers)
     int *final_count;
     int4 *fix_list;  // rows left for the exact recompute: (pixel, step, row index, winner)
     int *fix_count;
@@ -1170,6 +1173,16 @@ __device__ __forceinline__ SearchAct search_act(const TcParams &P, int round, in
     return r;
 }
 
+// A row's next-round entry (valid: it has a step) counted into its
+// compaction block, one atomic per block a warp's entries fall in.  Every
+// lane of the warp calls it.
+__device__ __forceinline__ void list_count_warp(int *bc, int idx, bool valid)
+{
+    const int key = valid ? (idx >> kCompactShift) : -1;
+    const unsigned grp = __match_any_sync(0xffffffffu, key);
+    if (valid && int(threadIdx.x & 31) == __ffs(int(grp)) - 1) atomicAdd(bc + key, __popc(grp));
+}
+
 __device__ __forceinline__ void s_extremes(const TcParams &P, int pix, const SearchAct &r)
 {
     const int smp = pix / int(P.ohw);
@@ -1315,6 +1328,7 @@ __device__ void search_epilogue(const TcParams &P, uint32_t acc, bool ok, int pi
     // exact recompute.  The rarer lists take one atomic per warp each, all
     // in flight at once.
     if (ok && P.round != 2 && (dec == 1 || dec == 2)) P.list_out[idx] = r.next ? r.next_e : make_int2(pix, -1);
+    if (P.round != 2) list_count_warp(P.list_bc, idx, ok && (dec == 1 || dec == 2) && r.next);
     const int lane = threadIdx.x & 31;
     const unsigned below = (1u << lane) - 1u;
     const bool wf = ok && dec == 0, wv = ok && dec == 3;
@@ -1416,7 +1430,9 @@ __device__ __forceinline__ void search_producer(const TcParams &P, const int4 *t
     if (int64_t(blockIdx.x) >= ntiles) return;
     const bool listed = !(P.round == 0 && !P.r0_list);
     if (listed && kc == 0) entry_prefetch<NU>(P, s_ent, blockIdx.x, row0, RS, nrows);
-    uint32_t it = 0, k = 0;
+    uint32_t k = 0;
+    int ss = 0;  // the stage ring: slot and pass of the next K block
+    uint32_t su = 0;
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++k)
     {
         const int cb = int(k & 1);
@@ -1452,7 +1468,7 @@ __device__ __forceinline__ void search_producer(const TcParams &P, const int4 *t
             }
         }
         for (int part = 0; part < P.nparts; ++part)
-            for (int kb = 0; kb < P.kblocks; ++kb, ++it)
+            for (int kb = 0; kb < P.kblocks; ++kb)
             {
                 uint2 fa[NU], fb[NU];
 #pragma unroll
@@ -1461,9 +1477,8 @@ __device__ __forceinline__ void search_producer(const TcParams &P, const int4 *t
                     fa[i] = fst_group(P, tab, ubase[i], uyx[i], kb * 16 + 2 * kc);
                     fb[i] = fst_group(P, tab, ubase[i], uyx[i], kb * 16 + 2 * kc + 1);
                 }
-                const int s = int(it % uint32_t(S));
-                const uint32_t u = it / uint32_t(S);
-                if (u > 0 && !wait_bounded(&empty_bar[s], (u - 1) & 1)) return;
+                const int s = ss;
+                if (su > 0 && !wait_bounded(&empty_bar[s], (su - 1) & 1)) return;
                 unsigned char *sA = smem + s * stage_bytes;
                 if (p == 0)
                 {
@@ -1478,6 +1493,7 @@ __device__ __forceinline__ void search_producer(const TcParams &P, const int4 *t
                                    spike_bytes(fb[i].x, utt[i]), spike_bytes(fb[i].y, utt[i]));
                 fence_proxy_async_smem();
                 mbar_arrive(&full_bar[s]);
+                if (++ss == S) ss = 0, ++su;
             }
     }
 }
@@ -2183,78 +2199,88 @@ __global__ void __launch_bounds__(256) search_bound_kernel(TcParams P, const uns
             s_fired[q] = m;
         }
         __syncthreads();
-        for (int p = threadIdx.x; p < ohw; p += blockDim.x)
+        for (int p0 = 0; p0 < ohw; p0 += int(blockDim.x))
         {
+            // warp-uniform trips: the candidates are counted per warp
+            const int p = p0 + int(threadIdx.x);
             const int pix = int(smp * ohw) + p;
-            const int oy = p / P.ow, ox = p - oy * P.ow;
-            const int iy0 = oy * P.sy - P.top, ix0 = ox * P.sx - P.left;
-            const int ky0 = max(0, -iy0), ky1 = min(P.kh, P.h - iy0);
-            const int kx0 = max(0, -ix0), kx1 = min(P.kw, P.w - ix0);
-            float u = 0.f;
-            for (int ky = ky0; ky < ky1; ++ky)
-                for (int kx = kx0; kx < kx1; ++kx)
-                {
-                    uint32_t m = s_fired[(iy0 + ky) * P.w + ix0 + kx];
-                    const float *w = wm + (ky * P.kw + kx) * cp;
-                    while (m)
-                    {
-                        u += w[__ffs(int(m)) - 1];
-                        m &= m - 1u;
-                    }
-                }
-            const bool cand = __fmul_ru(u, widen) > P.thr;
-            if (cand && tlo)
+            bool cand = false;
+            if (p < ohw)
             {
-                float *acc = s_acc + threadIdx.x;
-                for (int t = 0; t < P.T; ++t) acc[t * blockDim.x] = 0.f;
+                const int oy = p / P.ow, ox = p - oy * P.ow;
+                const int iy0 = oy * P.sy - P.top, ix0 = ox * P.sx - P.left;
+                const int ky0 = max(0, -iy0), ky1 = min(P.kh, P.h - iy0);
+                const int kx0 = max(0, -ix0), kx1 = min(P.kw, P.w - ix0);
+                float u = 0.f;
                 for (int ky = ky0; ky < ky1; ++ky)
                     for (int kx = kx0; kx < kx1; ++kx)
                     {
-                        const int q = (iy0 + ky) * P.w + ix0 + kx;
-                        uint32_t m = s_fired[q];
+                        uint32_t m = s_fired[(iy0 + ky) * P.w + ix0 + kx];
                         const float *w = wm + (ky * P.kw + kx) * cp;
                         while (m)
                         {
-                            const int c = __ffs(int(m)) - 1;
-                            acc[int(s_fb[q * cp + c]) * blockDim.x] += w[c];
+                            u += w[__ffs(int(m)) - 1];
                             m &= m - 1u;
                         }
                     }
-                float run = 0.f;
-                int t0 = P.T - 1;  // no step below T - 1 can fire either when none passes
-                for (int t = 0; t < P.T - 1; ++t)
+                cand = __fmul_ru(u, widen) > P.thr;
+                if (cand && tlo)
                 {
-                    run += acc[t * blockDim.x];
-                    if (__fmul_ru(run, widen) > P.thr)
+                    float *acc = s_acc + threadIdx.x;
+                    for (int t = 0; t < P.T; ++t) acc[t * blockDim.x] = 0.f;
+                    for (int ky = ky0; ky < ky1; ++ky)
+                        for (int kx = kx0; kx < kx1; ++kx)
+                        {
+                            const int q = (iy0 + ky) * P.w + ix0 + kx;
+                            uint32_t m = s_fired[q];
+                            const float *w = wm + (ky * P.kw + kx) * cp;
+                            while (m)
+                            {
+                                const int c = __ffs(int(m)) - 1;
+                                acc[int(s_fb[q * cp + c]) * blockDim.x] += w[c];
+                                m &= m - 1u;
+                            }
+                        }
+                    float run = 0.f;
+                    int t0 = P.T - 1;  // no step below T - 1 can fire either when none passes
+                    for (int t = 0; t < P.T - 1; ++t)
                     {
-                        t0 = t;
-                        break;
+                        run += acc[t * blockDim.x];
+                        if (__fmul_ru(run, widen) > P.thr)
+                        {
+                            t0 = t;
+                            break;
+                        }
+                    }
+                    tlo[pix] = uint8_t(t0);
+                }
+                if (!cand)
+                {
+                    P.records[pix] = make_int4(0, P.T, __float_as_int(P.thv), 0);
+                    if (P.wta && P.thv != 0.f)
+                    {
+                        atomicMin(P.mins + smp, order_enc(P.thv));
+                        atomicMax(P.maxs + smp, order_enc(P.thv));
                     }
                 }
-                tlo[pix] = uint8_t(t0);
+                list[pix] = make_int2(pix, cand ? P.T - 1 : -1);
             }
-            if (!cand)
-            {
-                P.records[pix] = make_int4(0, P.T, __float_as_int(P.thv), 0);
-                if (P.wta && P.thv != 0.f)
-                {
-                    atomicMin(P.mins + smp, order_enc(P.thv));
-                    atomicMax(P.maxs + smp, order_enc(P.thv));
-                }
-            }
-            list[pix] = make_int2(pix, cand ? P.T - 1 : -1);
+            list_count_warp(P.list_bc, pix, cand);
         }
     }
 }
 
 // Stable compaction of a row list: the entries with a step >= 0 of
 // in[0 .. n) (n = *n_dev, or n_max when n_dev is null) go to out in their
-// order, their number to *count_out.  Three launches: per-block counts of
-// kCompactItems entries, one block's exclusive scan of the counts, and the
-// scatter (a block writes its entries from its offset, ranked by warp
-// ballots).  The lists stay in pixel order, so a tile's rows lie in a few
-// neighbouring images.
-constexpr int kCompactItems = 2048;
+// order, their number to *count_out.  The kernels that write the list also
+// count its valid entries per block of kCompactItems (list_count_warp), so
+// for up to kSelfPrefixBlocks blocks the compaction is one launch: each
+// scatter block sums the counts before its own.  Longer lists take three:
+// per-block counts, one block's exclusive scan of them, and the scatter (a
+// block writes its entries from its offset, ranked by warp ballots).  The
+// lists stay in pixel order, so a tile's rows lie in a few neighbouring
+// images.
+constexpr int kSelfPrefixBlocks = 2048;
 
 __device__ __forceinline__ int64_t list_len(const int *n_dev, int64_t n_max) { return n_dev ? int64_t(*n_dev) : n_max; }
 
@@ -2320,35 +2346,74 @@ __global__ void __launch_bounds__(1024) list_scan_kernel(int *__restrict__ bcoun
     }
 }
 
+// The scatter (256 threads, kCompactItems entries a block, all loaded at
+// once).  A block's offset is boff[block] (the scan's output) or, with
+// self_prefix, the sum of the entry counts of the blocks before it, which the
+// list's writers added to bcount: then the block holding the list's last
+// entry also writes *count_out.  Every launch zeroes bzero[0 .. nbz), the
+// counts of the next compaction.
 __global__ void __launch_bounds__(256) list_scatter_kernel(const int2 *__restrict__ in, const int *n_dev,
                                                            int64_t n_max, const int *__restrict__ boff,
-                                                           int2 *__restrict__ out, const int *negw, const int *flag)
+                                                           int self_prefix, int *__restrict__ count_out,
+                                                           int *__restrict__ bzero, int nbz, int2 *__restrict__ out,
+                                                           const int *negw, const int *flag)
 {
     if (*negw || *flag) return;
-    __shared__ int ws[8];
+    constexpr int Q = kCompactItems / 256;
+    __shared__ int ws[Q][8], wsum[8];
+    for (int i = int(blockIdx.x * blockDim.x + threadIdx.x); i < nbz; i += int(gridDim.x * blockDim.x)) bzero[i] = 0;
     const int64_t n = list_len(n_dev, n_max), b0 = int64_t(blockIdx.x) * kCompactItems;
-    if (b0 >= n) return;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int base = boff[blockIdx.x];
-    for (int q = 0; q < kCompactItems; q += blockDim.x)
+    if (b0 >= n)
     {
-        const int64_t j = b0 + q + threadIdx.x;
-        int2 e = make_int2(0, -1);
-        if (j < n) e = in[j];
-        const bool keep = e.y >= 0;
-        const unsigned m = __ballot_sync(0xffffffffu, keep);
-        if (lane == 0) ws[warp] = __popc(m);
-        __syncthreads();
-        int before = 0, total = 0;
-        for (int w = 0; w < int(blockDim.x >> 5); ++w)
-        {
-            before += w < warp ? ws[w] : 0;
-            total += ws[w];
-        }
-        if (keep) out[base + before + __popc(m & ((1u << lane) - 1u))] = e;
-        base += total;
-        __syncthreads();
+        if (self_prefix && blockIdx.x == 0 && threadIdx.x == 0) *count_out = 0;
+        return;
     }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int2 e[Q];
+    unsigned m[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q)
+    {
+        const int64_t j = b0 + q * 256 + threadIdx.x;
+        e[q] = j < n ? in[j] : make_int2(0, -1);
+    }
+#pragma unroll
+    for (int q = 0; q < Q; ++q)
+    {
+        m[q] = __ballot_sync(0xffffffffu, e[q].y >= 0);
+        if (lane == 0) ws[q][warp] = __popc(m[q]);
+    }
+    if (self_prefix)
+    {
+        int acc = 0;
+        for (int i = threadIdx.x; i < int(blockIdx.x); i += 256) acc += boff[i];
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) wsum[warp] = acc;
+    }
+    __syncthreads();
+    int off = 0;
+    if (self_prefix)
+    {
+#pragma unroll
+        for (int w = 0; w < 8; ++w) off += wsum[w];
+    }
+    else
+        off = boff[blockIdx.x];
+    const unsigned below = (1u << lane) - 1u;
+#pragma unroll
+    for (int q = 0; q < Q; ++q)
+    {
+        int before = 0, total = 0;
+#pragma unroll
+        for (int w = 0; w < 8; ++w)
+        {
+            before += w < warp ? ws[q][w] : 0;
+            total += ws[q][w];
+        }
+        if (e[q].y >= 0) out[off + before + __popc(m[q] & below)] = e[q];
+        off += total;
+    }
+    if (self_prefix && threadIdx.x == 0 && b0 + kCompactItems >= n) *count_out = off;
 }
 
 // Rows the search could not decide from the term sums (a potential within
@@ -2360,9 +2425,46 @@ __global__ void __launch_bounds__(256) list_scatter_kernel(const int2 *__restric
 // for the pixel whose receptive field starts at (iy0, ix0): the FP64 sum of
 // the weights of the inputs that fired by t, in (channel, ky, kx) order,
 // positions outside the input skipped.
+// The same sum for maps of 8 padded channels and windows up to 5 x 5: the
+// window's first-spike words are loaded first, all in flight together (0xFF
+// bytes outside the input never fire), then summed in the same order.
+__device__ __forceinline__ double oracle_sum_small(const TcParams &P, const uint8_t *fm, const float *wk, int iy0,
+                                                   int ix0, int t)
+{
+    uint2 f[25];
+#pragma unroll
+    for (int ky = 0; ky < 5; ++ky)
+#pragma unroll
+        for (int kx = 0; kx < 5; ++kx)
+        {
+            const int iy = iy0 + ky, ix = ix0 + kx;
+            f[ky * 5 + kx] = (ky < P.kh && kx < P.kw && iy >= 0 && iy < P.h && ix >= 0 && ix < P.w)
+                                 ? __ldg(reinterpret_cast<const uint2 *>(fm + (int64_t(iy) * P.w + ix) * 8))
+                                 : make_uint2(~0u, ~0u);
+        }
+    double acc = 0.0;
+    for (int c = 0; c < P.cin; ++c)
+    {
+        const int sh = (c & 3) * 8;
+        const float *wc = wk + c * P.kh * P.kw;
+#pragma unroll
+        for (int ky = 0; ky < 5; ++ky)
+#pragma unroll
+            for (int kx = 0; kx < 5; ++kx)
+                if (ky < P.kh && kx < P.kw)
+                {
+                    const double wv = double(__ldg(wc + ky * P.kw + kx));
+                    const uint32_t word = c < 4 ? f[ky * 5 + kx].x : f[ky * 5 + kx].y;
+                    if (int((word >> sh) & 0xFFu) <= t) acc += wv;
+                }
+    }
+    return acc;
+}
+
 __device__ __forceinline__ double oracle_sum(const TcParams &P, const uint8_t *fm, const float *wk, int iy0, int ix0,
                                              int cp, int t)
 {
+    if (cp == 8 && P.kh <= 5 && P.kw <= 5) return oracle_sum_small(P, fm, wk, iy0, ix0, t);
     const int ky0 = max(0, -iy0), ky1 = min(P.kh, P.h - iy0);
     const int kx0 = max(0, -ix0), kx1 = min(P.kw, P.w - ix0);
     double acc = 0.0;
@@ -2403,6 +2505,7 @@ __global__ void __launch_bounds__(128) search_fix_kernel(TcParams P, const float
         atomicAdd(&g_recomputes, 1ull);
         const SearchAct r = search_act(P, round, pix, t, 2, o, float(acc), round == 1 ? P.state[pix] : int4{});
         if (round != 2) P.list_out[idx] = r.next ? r.next_e : make_int2(pix, -1);
+        if (round != 2 && r.next) atomicAdd(P.list_bc + (idx >> kCompactShift), 1);
         if (r.fin) P.final_list[atomicAdd(P.final_count, 1)] = r.fin_e;
         if (P.wta) s_extremes(P, pix, r);
     }
@@ -2445,6 +2548,7 @@ __global__ void __launch_bounds__(128) search_fix_kernel(TcParams P, const float
                 dec = 1, a = -1, v = 0.f;
             const SearchAct r = search_act(P, round, pix, t, dec, a, v, round == 1 ? P.state[pix] : int4{});
             if (round != 2) P.list_out[idx] = r.next ? r.next_e : make_int2(pix, -1);
+            if (round != 2 && r.next) atomicAdd(P.list_bc + (idx >> kCompactShift), 1);
             if (r.fin) P.final_list[atomicAdd(P.final_count, 1)] = r.fin_e;
             if (P.wta) s_extremes(P, pix, r);
         }
@@ -3088,7 +3192,7 @@ struct FusedLayout
     // winners to re-read at T - 1, two lists of rows to recompute
     bool search_ok;
     size_t w4_off, echan_off, wm_off, cnt_off, state_off, la_off, lb_off, fin_off, fa_off, fb_off, va_off, vb_off;
-    size_t lt_off, bc_off;  // the rows' next entries by row index, per-block counts of the compaction
+    size_t lt_off, bc_off;  // the rows' next entries by row index; the compaction's per-block counts
     size_t tlo_off;         // per pixel, the first step the bound allows a spike at
     size_t total;
 };
@@ -3128,7 +3232,10 @@ FusedLayout fused_layout(int64_t b, int64_t t, int64_t cin, int64_t h, int64_t w
         L.w4_off = off, off += align256(L.pl4.wimg_bytes);
         L.echan_off = off, off += align256(size_t(L.pl4.parts) * L.pl4.n_tile * 8 + 8);
         L.wm_off = off, off += align256(size_t(cin * kh * kw) * 4);
-        L.cnt_off = off, off += 256;  // 64 counters
+        // 64 counters, then two buffers of per-block entry counts of the list
+        // compaction (zeroed together)
+        L.cnt_off = off, off += 256 + 2 * align256((np / kCompactItems + 2) * 4);
+        L.bc_off = L.cnt_off + 256;
         L.state_off = off, off += align256(np * 16);
         L.la_off = off, off += align256(np * 8);
         L.lb_off = off, off += align256(np * 8);
@@ -3138,7 +3245,6 @@ FusedLayout fused_layout(int64_t b, int64_t t, int64_t cin, int64_t h, int64_t w
         L.va_off = off, off += align256(np * 16);
         L.vb_off = off, off += align256(np * 16);
         L.lt_off = off, off += align256(np * 8);
-        L.bc_off = off, off += align256((np / kCompactItems + 2) * 4);
         L.tlo_off = off, off += align256(np);
     }
     L.total = off;
@@ -3294,7 +3400,8 @@ void search_layer(const TcParams &P0, const FusedLayout &L, const float *kernel,
     const bool prefilter = P.nhwc && P.cpad <= 32 && bound_smem <= 48 * 1024;
     unsigned *wmax = reinterpret_cast<unsigned *>(base + L.wm_off);
     uint8_t *tlo = base + L.tlo_off;
-    SPK_CUDA(cudaMemsetAsync(cnt, 0, 256, s));
+    const size_t bcn = align256((size_t(L.npix) / kCompactItems + 2) * 4) / 4;  // ints per count buffer
+    SPK_CUDA(cudaMemsetAsync(cnt, 0, 256 + 2 * bcn * 4, s));
     SPK_CUDA(cudaMemsetAsync(sinfo, 0, 8, s));
     if (prefilter) SPK_CUDA(cudaMemsetAsync(wmax, 0, size_t(kr) * 4, s));
     fixed_split_kernel<kSearchTerms><<<unsigned(nch), 256, 0, s>>>(
@@ -3308,18 +3415,30 @@ void search_layer(const TcParams &P0, const FusedLayout &L, const float *kernel,
     }
     // Rows write their next entry at their own index of lt (step -1: settled);
     // a stable compaction makes the next round's list, in pixel order.
+    // The writers of each list also count its valid entries per compaction
+    // block, into the buffer of the compaction that will read them (two
+    // buffers in turn; each compaction zeroes the other one).
     int2 *lt = reinterpret_cast<int2 *>(base + L.lt_off);
-    int *bc = reinterpret_cast<int *>(base + L.bc_off);
+    int *bcs[2] = {reinterpret_cast<int *>(base + L.bc_off), reinterpret_cast<int *>(base + L.bc_off) + bcn};
     const unsigned cblocks = unsigned((L.npix + kCompactItems - 1) / kCompactItems);
     SPK_REQUIRE(cblocks <= 1024u * 64u, "too many output pixels for the list compaction");
+    const int self_prefix = cblocks <= unsigned(kSelfPrefixBlocks) ? 1 : 0;
+    int ncompact = 0;
     auto compact = [&](const int *n_dev, int2 *out, int *count_out) {
-        list_count_kernel<<<cblocks, 256, 0, s>>>(lt, n_dev, L.npix, bc, P.negw, P.flag);
+        int *bc = bcs[ncompact & 1], *bnext = bcs[(ncompact + 1) & 1];
+        if (!self_prefix)
+        {
+            list_count_kernel<<<cblocks, 256, 0, s>>>(lt, n_dev, L.npix, bc, P.negw, P.flag);
+            SPK_LAUNCHED();
+            list_scan_kernel<<<1, 1024, 0, s>>>(bc, int(cblocks), count_out, P.negw, P.flag);
+            SPK_LAUNCHED();
+        }
+        list_scatter_kernel<<<cblocks, 256, 0, s>>>(lt, n_dev, L.npix, bc, self_prefix, count_out, bnext,
+                                                    int(cblocks), out, P.negw, P.flag);
         SPK_LAUNCHED();
-        list_scan_kernel<<<1, 1024, 0, s>>>(bc, int(cblocks), count_out, P.negw, P.flag);
-        SPK_LAUNCHED();
-        list_scatter_kernel<<<cblocks, 256, 0, s>>>(lt, n_dev, L.npix, bc, out, P.negw, P.flag);
-        SPK_LAUNCHED();
+        ++ncompact;
     };
+    P.list_bc = bcs[0];
     if (prefilter)
     {
         search_bound_kernel<<<unsigned(std::min<int64_t>(b, 0x7FFFFFFF)), 256, size_t(bound_smem), s>>>(
@@ -3340,6 +3459,7 @@ void search_layer(const TcParams &P0, const FusedLayout &L, const float *kernel,
         P.list_in = final ? P.final_list : (r & 1 ? la : lb);
         P.count_in = final ? P.final_count : cnt + r;
         P.list_out = lt;
+        P.list_bc = bcs[ncompact & 1];
         P.fix_list = r & 1 ? fb : fa;
         P.fix_count = cnt + 17 + r;
         P.val_list = r & 1 ? vb : va;
