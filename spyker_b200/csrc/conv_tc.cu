@@ -101,6 +101,7 @@ struct TcParams
     const int *count_in;
     int2 *list_out, *final_list;  // list_out: each row's next entry at the row's index
     int *list_bc;                 // per compaction block of list_out, its entries with a step (added by the writers)
+    int *tile_ctr;                // search: tickets of the tiles after each CTA's first (zeroed; null: static)
     int *final_count;
     int4 *fix_list;  // rows left for the exact recompute: (pixel, step, row index, winner)
     int *fix_count;
@@ -1423,28 +1424,42 @@ template <int NU>
 __device__ __forceinline__ void search_producer(const TcParams &P, const int4 *tab, unsigned char *smem,
                                                 uint64_t *full_bar, uint64_t *empty_bar, int S, int stage_bytes,
                                                 int a_bytes, int b_bytes, int p, int64_t nrows, int64_t ntiles,
-                                                int2 *s_ent, uint64_t *ent_bar)
+                                                int2 *s_ent, uint64_t *ent_bar, int *s_tiles, uint64_t *tq_bar)
 {
     constexpr int NT = 1024 / NU, RS = NT / 8;  // producer threads; row step between a thread's units
     const int row0 = (p & 7) + 8 * (p >> 6), kc = (p >> 3) & 7;
     if (int64_t(blockIdx.x) >= ntiles) return;
     const bool listed = !(P.round == 0 && !P.r0_list);
+    const bool dyn = P.tile_ctr != nullptr;
+    int ticket = 0;  // (thread 0) the claimed ticket of the tile after the next one
+    if (p == 0)
+    {
+        s_tiles[0] = int(blockIdx.x);
+        mbar_arrive(&tq_bar[0]);
+        if (dyn) ticket = atomicAdd(P.tile_ctr, 1);
+    }
     if (listed && kc == 0) entry_prefetch<NU>(P, s_ent, blockIdx.x, row0, RS, nrows);
-    uint32_t k = 0;
     int ss = 0;  // the stage ring: slot and pass of the next K block
     uint32_t su = 0;
-    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++k)
+    int64_t tile = blockIdx.x;
+    for (uint32_t k = 0;; ++k)
     {
         const int cb = int(k & 1);
-        if (listed)
+        // thread 0 publishes the tile after this one in the ring (-1: none)
+        if (p == 0)
         {
-            if (kc == 0) cp_async_wait_all();
-            mbar_arrive(&ent_bar[cb]);
-            if (!wait_bounded(&ent_bar[cb], (k >> 1) & 1)) return;
-            // every thread has read the other buffer (the previous tile's)
-            if (kc == 0 && tile + gridDim.x < ntiles)
-                entry_prefetch<NU>(P, s_ent + (cb ^ 1) * BM, tile + gridDim.x, row0, RS, nrows);
+            const int64_t nt = dyn ? int64_t(gridDim.x) + ticket : tile + gridDim.x;
+            s_tiles[(k + 1) & 15] = nt < ntiles ? int(nt) : -1;
+            mbar_arrive(&tq_bar[(k + 1) & 15]);
         }
+        if (listed && kc == 0) cp_async_wait_all();
+        mbar_arrive(&ent_bar[cb]);
+        if (!wait_bounded(&ent_bar[cb], (k >> 1) & 1)) return;
+        // every thread has read the other entry buffer (the previous tile's)
+        // and sees the next tile
+        const int next = s_tiles[(k + 1) & 15];
+        if (p == 0 && dyn && next >= 0) ticket = atomicAdd(P.tile_ctr, 1);
+        if (listed && kc == 0 && next >= 0) entry_prefetch<NU>(P, s_ent + (cb ^ 1) * BM, next, row0, RS, nrows);
         int ubase[NU], uyx[NU];
         uint32_t utt[NU];
 #pragma unroll
@@ -1495,6 +1510,8 @@ __device__ __forceinline__ void search_producer(const TcParams &P, const int4 *t
                 mbar_arrive(&full_bar[s]);
                 if (++ss == S) ss = 0, ++su;
             }
+        if (next < 0) break;
+        tile = next;
     }
 }
 
@@ -1520,7 +1537,10 @@ __device__ __forceinline__ void conv_ws_body(const TcParams &P)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ __align__(8) uint64_t full_bar[kMaxStages], empty_bar[kMaxStages], accf_bar[2], acce_bar[2], tim_bar,
-        ent_bar[2];
+        ent_bar[2], tq_bar[16];
+    // search: the CTA's tiles in order (slot k & 15 holds its k-th tile, -1
+    // after the last), each published by a producer arrival on tq_bar
+    __shared__ int s_tiles[16];
     __shared__ uint32_t tmem_slot;
 
     // the search kernels run only on the lean path, the dense fused kernel
@@ -1600,6 +1620,7 @@ __device__ __forceinline__ void conv_ws_body(const TcParams &P)
         for (int a = 0; a < 2; ++a) mbar_init(&accf_bar[a], 1), mbar_init(&acce_bar[a], 128);
         mbar_init(&tim_bar, 128);
         for (int b = 0; b < 2; ++b) mbar_init(&ent_bar[b], 32 * NPW);
+        for (int q = 0; q < 16; ++q) mbar_init(&tq_bar[q], 1);
         fence_mbar_init();
     }
     if (warp == 0)
@@ -1616,7 +1637,7 @@ __device__ __forceinline__ void conv_ws_body(const TcParams &P)
     constexpr int kMmaWarp = 4 + NPW;
     if (MODE == kSearch && warp >= 4 && warp < kMmaWarp)
         search_producer<1024 / (32 * NPW)>(P, tab, smem, full_bar, empty_bar, S, stage_bytes, a_bytes, b_bytes,
-                                           tid - 128, nrows, ntiles, s_ent, ent_bar);
+                                           tid - 128, nrows, ntiles, s_ent, ent_bar, s_tiles, tq_bar);
     else if (MODE != kPotentials && MODE != kSearch && warp >= 4 && warp < kMmaWarp)
     {
         // ---------------- fused producers (8 warps) ----------------
@@ -1688,12 +1709,30 @@ __device__ __forceinline__ void conv_ws_body(const TcParams &P)
         // ---------------- MMA issuer ----------------
         if (lane == 0)
         {
-            uint32_t it = 0, j = 0;
+            uint32_t it = 0, j = 0, k = 0;
             bool failed = false;
             const int parts = MODE == kSearch ? P.nparts : 1;
-            for (int64_t unit = blockIdx.x * int64_t(parts); unit < ntiles * parts && !failed;
-                 unit += (unit % parts == parts - 1) ? int64_t(gridDim.x - 1) * parts + 1 : 1, ++j)
+            int64_t tile = blockIdx.x;
+            // units (tile, part) in the CTA's order: the tiles stride by the
+            // grid, or (search) come from the producers' ring
+            for (int part = 0; tile >= 0 && tile < ntiles && !failed; ++j)
             {
+                if (j > 0 && part == 0)
+                {
+                    // (after the last part of a tile) the next tile
+                    if constexpr (MODE == kSearch)
+                    {
+                        if (!wait_bounded(&tq_bar[k & 15], (k >> 4) & 1)) break;
+                        tile = s_tiles[k & 15];
+                        if (tile < 0) break;
+                    }
+                    else
+                    {
+                        tile += gridDim.x;
+                        if (tile >= ntiles) break;
+                    }
+                }
+                if (++part == parts) part = 0, ++k;
                 const int a = int(j % uint32_t(nacc));
                 const uint32_t ua = j / uint32_t(nacc);
                 if (ua > 0 && !wait_bounded(&acce_bar[a], (ua - 1) & 1)) break;
@@ -1748,14 +1787,29 @@ __device__ __forceinline__ void conv_ws_body(const TcParams &P)
         // the largest channel bound (search)
         float emax = 0.f;
         if constexpr (MODE == kSearch) emax = __uint_as_float(P.sinfo[0]);
-        uint32_t j = 0;
+        uint32_t j = 0, k = 0;
         const int parts = MODE == kSearch ? P.nparts : 1;
         SearchScan scan;
-        for (int64_t unit = blockIdx.x * int64_t(parts); unit < ntiles * parts;
-             unit += (unit % parts == parts - 1) ? int64_t(gridDim.x - 1) * parts + 1 : 1, ++j)
+        int64_t tile = blockIdx.x;
+        // the MMA issuer's order of units (tile, part)
+        for (int part = 0, nextp = 0; tile >= 0 && tile < ntiles; ++j, part = nextp)
         {
-            const int64_t tile = unit / parts;
-            const int part = int(unit % parts);
+            if (j > 0 && part == 0)
+            {
+                if constexpr (MODE == kSearch)
+                {
+                    if (!wait_bounded(&tq_bar[k & 15], (k >> 4) & 1)) break;
+                    tile = s_tiles[k & 15];
+                    if (tile < 0) break;
+                }
+                else
+                {
+                    tile += gridDim.x;
+                    if (tile >= ntiles) break;
+                }
+            }
+            nextp = part + 1;
+            if (nextp == parts) nextp = 0, ++k;
             const int a = int(j % uint32_t(nacc));
             const uint32_t ua = j / uint32_t(nacc);
             // search rows: the row's list entry and pixel state are loaded
@@ -1959,6 +2013,18 @@ __global__ void __launch_bounds__(128) wta_records_warp_kernel(const int4 *__res
             }
         }
     }
+    // each slot's (row, column), packed, for the suppression boxes
+    int pyx[KPL];
+    {
+        int py = lane / w, px = lane - py * w;
+#pragma unroll
+        for (int q = 0; q < KPL; ++q)
+        {
+            pyx[q] = (py << 16) | px;
+            px += 32;
+            while (px >= w) px -= w, ++py;
+        }
+    }
     int found = 0;
     for (int round = 0; round < count; ++round)
     {
@@ -1974,20 +2040,20 @@ __global__ void __launch_bounds__(128) wta_records_warp_kernel(const int4 *__res
             if (ov > bv || (ov == bv && oi < bi)) bv = ov, bi = oi;
         }
         if (bi == INT_MAX) break;  // only sentinels left (the same in every lane)
-        const int z = bi / hw, p0 = bi % hw, y = p0 / w, x = p0 % w;
+        const int z = bi / hw, p0 = bi - z * hw, y = p0 / w, x = p0 - y * w;
         if (lane == 0)
         {
             int32_t *e = winners + (b * count + round) * 5;
             e[0] = 0, e[1] = 0, e[2] = z, e[3] = y, e[4] = x;
         }
-        int py = lane / w, px = lane - py * w;
+        // the winner's box (every channel) and the winner's channel leave
+        const int zlo = z * hw, zhi = zlo + hw;
 #pragma unroll
         for (int q = 0; q < KPL; ++q)
         {
+            const int py = pyx[q] >> 16, px = pyx[q] & 0xFFFF;
             const bool box = py >= y - ry && py <= y + ry && px >= x - rx && px <= x + rx;
-            if (box || (flat[q] != INT_MAX && flat[q] / hw == z)) key[q] = -INFINITY, flat[q] = INT_MAX;
-            px += 32;
-            while (px >= w) px -= w, ++py;
+            if (box || (flat[q] >= zlo && flat[q] < zhi)) key[q] = -INFINITY, flat[q] = INT_MAX;
         }
         ++found;
     }
@@ -2147,11 +2213,12 @@ __global__ void search_init_kernel(unsigned *mins, unsigned *maxs, int64_t b, co
 // A CTA per sample: the sample's first-spike map becomes a 32-bit mask per
 // input pixel (the channels fired by T - 1, up to 32) in shared memory, the
 // per-tap channel maxima a table beside it; a thread per output pixel adds
-// the maxima of its taps' set bits.  For a pixel that may fire, the same
-// terms binned by their inputs' first steps (T <= 32: one bin per step and
-// thread in shared memory) give U(t) for every t, and t_lo, the first step
-// whose U(t) (widened the same way) is above the threshold: no channel
-// fires before t_lo, so the bisection starts from (t_lo - 1, T - 1].
+// the maxima of its taps' set bits.  With T <= 32 it adds them into bins by
+// their inputs' first steps (one bin per step and thread in shared memory):
+// the running sums of the bins give U(t) for every t, U = U(T - 1), and
+// t_lo, the first step whose U(t) (widened the same way) is above the
+// threshold: no channel fires before t_lo, so the bisection starts from
+// (t_lo - 1, T - 1].
 __global__ void __launch_bounds__(256) search_bound_kernel(TcParams P, const unsigned *__restrict__ wmax, int cp,
                                                            int2 *__restrict__ list, uint8_t *__restrict__ tlo)
 {
@@ -2211,21 +2278,11 @@ __global__ void __launch_bounds__(256) search_bound_kernel(TcParams P, const uns
                 const int iy0 = oy * P.sy - P.top, ix0 = ox * P.sx - P.left;
                 const int ky0 = max(0, -iy0), ky1 = min(P.kh, P.h - iy0);
                 const int kx0 = max(0, -ix0), kx1 = min(P.kw, P.w - ix0);
-                float u = 0.f;
-                for (int ky = ky0; ky < ky1; ++ky)
-                    for (int kx = kx0; kx < kx1; ++kx)
-                    {
-                        uint32_t m = s_fired[(iy0 + ky) * P.w + ix0 + kx];
-                        const float *w = wm + (ky * P.kw + kx) * cp;
-                        while (m)
-                        {
-                            u += w[__ffs(int(m)) - 1];
-                            m &= m - 1u;
-                        }
-                    }
-                cand = __fmul_ru(u, widen) > P.thr;
-                if (cand && tlo)
+                if (tlo)
                 {
+                    // one pass: the terms binned by their inputs' first steps
+                    // (all below T); U is the sum of the bins, the same terms
+                    // summed in another order (the widening covers any order)
                     float *acc = s_acc + threadIdx.x;
                     for (int t = 0; t < P.T; ++t) acc[t * blockDim.x] = 0.f;
                     for (int ky = ky0; ky < ky1; ++ky)
@@ -2243,16 +2300,29 @@ __global__ void __launch_bounds__(256) search_bound_kernel(TcParams P, const uns
                         }
                     float run = 0.f;
                     int t0 = P.T - 1;  // no step below T - 1 can fire either when none passes
-                    for (int t = 0; t < P.T - 1; ++t)
+                    for (int t = 0; t < P.T; ++t)
                     {
                         run += acc[t * blockDim.x];
-                        if (__fmul_ru(run, widen) > P.thr)
-                        {
-                            t0 = t;
-                            break;
-                        }
+                        if (t0 == P.T - 1 && t < P.T - 1 && __fmul_ru(run, widen) > P.thr) t0 = t;
                     }
-                    tlo[pix] = uint8_t(t0);
+                    cand = __fmul_ru(run, widen) > P.thr;
+                    if (cand) tlo[pix] = uint8_t(t0);
+                }
+                else
+                {
+                    float u = 0.f;
+                    for (int ky = ky0; ky < ky1; ++ky)
+                        for (int kx = kx0; kx < kx1; ++kx)
+                        {
+                            uint32_t m = s_fired[(iy0 + ky) * P.w + ix0 + kx];
+                            const float *w = wm + (ky * P.kw + kx) * cp;
+                            while (m)
+                            {
+                                u += w[__ffs(int(m)) - 1];
+                                m &= m - 1u;
+                            }
+                        }
+                    cand = __fmul_ru(u, widen) > P.thr;
                 }
                 if (!cand)
                 {
@@ -3460,6 +3530,7 @@ void search_layer(const TcParams &P0, const FusedLayout &L, const float *kernel,
         P.count_in = final ? P.final_count : cnt + r;
         P.list_out = lt;
         P.list_bc = bcs[ncompact & 1];
+        P.tile_ctr = cnt + 48 + r;  // tiles claimed in turn by the CTAs that are running
         P.fix_list = r & 1 ? fb : fa;
         P.fix_count = cnt + 17 + r;
         P.val_list = r & 1 ? vb : va;

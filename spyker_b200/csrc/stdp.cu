@@ -388,8 +388,11 @@ struct NetScan
     const double *net_cfg;
 };
 
+// At most 40 registers a thread (six CTAs' worth of an SM's registers): a
+// CTA of this long-running scan then fits beside two CTAs of the fused
+// layer's search kernel when the update overlaps that layer's rounds.
 template <bool F32_RULE, bool NETS>
-__global__ void __launch_bounds__(kScanThreads)
+__global__ void __launch_bounds__(kScanThreads, 6)
     stdp_scan_kernel(float *__restrict__ kernel, int64_t k, int64_t b, int count, int field,
                      const int32_t *__restrict__ winners, const int32_t *__restrict__ counts,
                      const uint16_t *__restrict__ pre, int64_t ps, int64_t pw, const uint16_t *__restrict__ post,
