@@ -132,12 +132,12 @@ class Network:
             c.stdpconfig = [spyker.STDPConfig(0.004, -0.003)]
             c.precision = precision
         self.conv_events = []
-        # Both STDP updates run on side streams after the step's forward
-        # passes: layer 1's on `side` while the next step's front end (DoG,
-        # rank code) runs, joined before the next layer 1; layer 2's on
-        # `side2` while the next front end and layer 1 run, joined before the
-        # next layer 2 (and both by finish()).  Neither overlaps a layer-2
-        # search round, whose CTAs each take a whole SM's shared memory.
+        # Layer 1's STDP runs on `side` while layer 2's forward runs on the
+        # main stream (layer 2 reads layer 1's spikes, not its weights),
+        # joined before the next layer 1; layer 2's on `side2` while the next
+        # step's front end and layer 1 run, joined before the next layer 2
+        # (both by finish()).  The search rounds claim their tiles as CTAs
+        # become free, so an SM held by an update's CTA delays no tile.
         self.side = torch.cuda.Stream(dev)
         self.side2 = torch.cuda.Stream(dev)
         # the STDP update of a layer: this rank's batch alone, or (data
@@ -182,11 +182,11 @@ class Network:
         main = self.torch.cuda.current_stream()
         main.wait_stream(self.side)  # the previous step's layer-1 update
         spk1, win1, pooled = self._layer(self.conv1, codes, 15.0, 3, 5, 2)
-        main.wait_stream(self.side2)  # the previous step's layer-2 update
-        spk2, win2, feats = self._layer(self.conv2, pooled, 10.0, 1, 8, 14)
         self.side.wait_stream(main)
         with self.torch.cuda.stream(self.side):
             self.stdp_fn(self.conv1, codes, win1, spk1)
+        main.wait_stream(self.side2)  # the previous step's layer-2 update
+        spk2, win2, feats = self._layer(self.conv2, pooled, 10.0, 1, 8, 14)
         self.side2.wait_stream(main)
         with self.torch.cuda.stream(self.side2):
             self.stdp_fn(self.conv2, pooled, win2, spk2)
