@@ -68,16 +68,13 @@ __global__ void filter_kernel(int which, const float *__restrict__ in, const flo
 
 // The same filters with the plane staged in shared memory as FP64 (zero
 // halo) and the kernels as FP64: a CTA takes rows [r0, r0 + rows) of one
-// plane for every filter; a thread computes XB neighbouring outputs of a
-// row, reusing each loaded input for XB products (and each loaded kernel
-// value for XB: XB = 7 or 8 when the row splits evenly, else 4).  Every
-// output is still
+// plane for every filter; a thread computes kXB neighbouring outputs of a
+// row, reusing each loaded input for kXB products.  Every output is still
 // one FMA chain over (a, b) in row-major order, so the result equals
 // filter_kernel's bit for bit (a zero-halo term adds +-0 to the chain, which
 // leaves it unchanged).
-constexpr int kMaxKw = 16;
+constexpr int kXB = 4, kMaxKw = 16;
 
-template <int XB>
 __global__ void __launch_bounds__(256) filter_tiled_kernel(int which, const float *__restrict__ in,
                                                            const float *__restrict__ kernel, float *__restrict__ out,
                                                            int h, int w, int f, int kh, int kw, int oh, int ow, int top,
@@ -85,7 +82,7 @@ __global__ void __launch_bounds__(256) filter_tiled_kernel(int which, const floa
 {
     extern __shared__ double fsm[];
     const int nk = which == 1 ? f : 2 * f, kk = kh * kw;
-    const int sw = ow + kw - 1 + XB;  // staged row width (zero beyond the plane)
+    const int sw = ow + kw - 1 + kXB;  // staged row width (zero beyond the plane)
     const int srows = rows + kh - 1;
     double *sk = fsm, *sp = fsm + nk * kk;
     const int64_t p = blockIdx.y;
@@ -100,39 +97,39 @@ __global__ void __launch_bounds__(256) filter_tiled_kernel(int which, const floa
     __syncthreads();
     const int fo = which == 2 ? 2 * f : f;
     const int64_t plane_out = int64_t(oh) * ow;
-    const int xg = (ow + XB - 1) / XB;
+    const int xg = (ow + kXB - 1) / kXB;
     for (int it = threadIdx.x; it < f * nr * xg; it += blockDim.x)
     {
-        const int q = it / (nr * xg), rem = it - q * nr * xg, ry = rem / xg, x0 = (rem - ry * xg) * XB;
-        double g1[XB], g2[XB];
+        const int q = it / (nr * xg), rem = it - q * nr * xg, ry = rem / xg, x0 = (rem - ry * xg) * kXB;
+        double g1[kXB], g2[kXB];
 #pragma unroll
-        for (int i = 0; i < XB; ++i) g1[i] = 0.0, g2[i] = 0.0;
+        for (int i = 0; i < kXB; ++i) g1[i] = 0.0, g2[i] = 0.0;
         const double *k1 = sk + q * kk, *k2 = sk + (f + q) * kk;
         for (int a = 0; a < kh; ++a)
         {
             const double *row = sp + (ry + a) * sw + x0;
-            double v[kMaxKw + XB - 1];
+            double v[kMaxKw + kXB - 1];
 #pragma unroll
-            for (int j = 0; j < kMaxKw + XB - 1; ++j)
-                if (j < kw + XB - 1) v[j] = row[j];
+            for (int j = 0; j < kMaxKw + kXB - 1; ++j)
+                if (j < kw + kXB - 1) v[j] = row[j];
 #pragma unroll
             for (int bb = 0; bb < kMaxKw; ++bb)
             {
                 if (bb >= kw) break;
                 const double c1 = k1[a * kw + bb];
 #pragma unroll
-                for (int i = 0; i < XB; ++i) g1[i] = fma(v[i + bb], c1, g1[i]);
+                for (int i = 0; i < kXB; ++i) g1[i] = fma(v[i + bb], c1, g1[i]);
                 if (which != 1)
                 {
                     const double c2 = k2[a * kw + bb];
 #pragma unroll
-                    for (int i = 0; i < XB; ++i) g2[i] = fma(v[i + bb], c2, g2[i]);
+                    for (int i = 0; i < kXB; ++i) g2[i] = fma(v[i + bb], c2, g2[i]);
                 }
             }
         }
         float *o = out + p * fo * plane_out + int64_t(r0 + ry) * ow;
 #pragma unroll
-        for (int i = 0; i < XB; ++i)
+        for (int i = 0; i < kXB; ++i)
         {
             const int x = x0 + i;
             if (x >= ow) break;
@@ -192,17 +189,15 @@ spk_status spk_filter(int which, const float *in, const float *kernel, float *ou
                     "input and kernel shapes are not compatible");
         if (n == 0) return;
         // tiled: as many output rows per CTA as fit 48 KB of FP64 staging
-        const int xb = ow % 8 == 0 ? 8 : (ow % 7 == 0 ? 7 : 4);
-        const int64_t nk = which == 1 ? f : 2 * f, sw = ow + kw - 1 + xb;
+        const int64_t nk = which == 1 ? f : 2 * f, sw = ow + kw - 1 + kXB;
         const int64_t avail = (48 * 1024) / 8 - nk * kh * kw;
         const int64_t rows = std::min<int64_t>(oh, avail / sw - (kh - 1));
         if (kw <= kMaxKw && rows >= 1 && n <= 65535 && h * w < (int64_t(1) << 31))
         {
             const size_t smem = size_t(nk * kh * kw + (rows + kh - 1) * sw) * 8;
-            const dim3 grid(unsigned(ceil_div(oh, rows)), unsigned(n));
-            const auto kern = xb == 8 ? filter_tiled_kernel<8> : (xb == 7 ? filter_tiled_kernel<7> : filter_tiled_kernel<4>);
-            kern<<<grid, 256, smem, stream_of(stream)>>>(which, in, kernel, out, int(h), int(w), int(f), int(kh),
-                                                         int(kw), int(oh), int(ow), int(p.top), int(p.left), int(rows));
+            filter_tiled_kernel<<<dim3(unsigned(ceil_div(oh, rows)), unsigned(n)), 256, smem, stream_of(stream)>>>(
+                which, in, kernel, out, int(h), int(w), int(f), int(kh), int(kw), int(oh), int(ow), int(p.top),
+                int(p.left), int(rows));
         }
         else
             filter_kernel<<<grid_for(n * f * oh * ow, 256), 256, 0, stream_of(stream)>>>(
