@@ -32,10 +32,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 BATCH, T, H = 4096, 15, 28
-# DRAM bytes (read + write) of one conv2 launch of the fused layer kernel:
-# ncu's dram__bytes_read.sum + dram__bytes_write.sum for the 256-image case
-# (--batch 256), scaled by 16 (the kernel's traffic grows with the batch).
-CONV2_TRAFFIC_BYTES = int((3.516928 + 1.249536) * 1e6 * 16)
+# DRAM bytes (read + write) of one conv2 layer call (its 27 launches, the
+# 4096-image step): ncu's dram__bytes_read.sum + dram__bytes_write.sum summed
+# over the call's launches, 611.6 MB read + 1169.6 MB written (1.20 GB of it
+# the layer's [B, T, 100, 14, 14] spike output).
+CONV2_TRAFFIC_BYTES = int((611.6 + 1169.6) * 1e6)
 METRIC = "images/s (STDP train + fwd), BF16-split vs FP32 on 1 B200; spike match %"
 WORKLOAD = "kheradpisheh-2layer-stdp: 4096 x 28x28 strokes, T=15, conv1 30x5x5 th15 r3k5, conv2 100x5x5 th10 r1k8"
 
@@ -406,7 +407,8 @@ def gpu_arm(args, rank, world):
         "roofline": {"bound": "tensor", "kernel": "conv2 (30->100, 5x5, M=12.0M, K=750)", "achieved": achieved,
                      "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                      "traffic": CONV2_TRAFFIC_BYTES * BATCH // 4096 if args.precision != "fp32" else None,
-                     "traffic_source": "ncu dram__bytes_read+write of the 256-image capture, scaled",
+                     "traffic_source": "ncu dram__bytes_read+write summed over the conv2 layer call's launches "
+                                       "(4096 images; scaled by the batch)",
                      "peak_source": peak_source},
         "kernels_ms": {"conv1": c1_ms, "conv2": c2_ms, "rest": ms - c1_ms - c2_ms},
         "clocks": clk.summary(),
