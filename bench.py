@@ -298,6 +298,7 @@ def gpu_arm(args, rank, world):
     with Clocks(dev.index) as clk:
         barrier()
         start.record()
+        h0 = time.perf_counter()
         for _ in range(args.steps):
             if graph is not None:
                 graph.replay()
@@ -305,6 +306,9 @@ def gpu_arm(args, rank, world):
                 net.step(dev_imgs)
         net.finish()
         end.record()
+        # host time to enqueue the steps (the GPU runs behind it unless the
+        # host is the slower side)
+        host_ms = (time.perf_counter() - h0) * 1e3 / max(args.steps, 1)
         barrier()
     if graph is None:
         launches = (spyker._lib.lib.spk_launch_count() - l0) // max(args.steps, 1)
@@ -403,6 +407,7 @@ def gpu_arm(args, rank, world):
         "e2e": {"value": BATCH * world / (e2e_ms * 1e-3), "unit": "images/s", "h2d_bytes_per_step": BATCH * H * H,
                 "d2h_bytes_per_step": int(feats.numel() * feats.element_size())},
         "gpu_launches": int(launches),
+        "host_enqueue_ms_per_step": host_ms,
         "cuda_graph": graph is not None,
         "roofline": {"bound": "tensor", "kernel": "conv2 (30->100, 5x5, M=12.0M, K=750)", "achieved": achieved,
                      "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,

@@ -55,6 +55,30 @@ constexpr int kMaxKBlocks = 128;  // K up to 8192
 // entries per block of a row-list compaction
 constexpr int kCompactShift = 11, kCompactItems = 1 << kCompactShift;
 
+// Division of any 32-bit n by an invariant d >= 1 (Granlund and Montgomery,
+// "Division by Invariant Integers using Multiplication", PLDI 1994, fig. 4.1):
+// with l = ceil(log2 d) and m = floor(2^32 (2^l - d) / d) + 1,
+// n / d = (t + ((n - t) >> min(l, 1))) >> max(l - 1, 0), t = umulhi(m, n).
+// sh packs the two shifts (low byte, next byte).
+struct DivMagic
+{
+    uint32_t m, sh;
+};
+
+inline DivMagic div_magic(uint32_t d)
+{
+    int l = 0;
+    while (l < 32 && (uint64_t(1) << l) < d) ++l;
+    const uint64_t m = ((uint64_t(1) << 32) * ((uint64_t(1) << l) - d)) / d + 1;
+    return DivMagic{uint32_t(m), uint32_t(l < 1 ? l : 1) | (uint32_t(l > 1 ? l - 1 : 0) << 8)};
+}
+
+__device__ __forceinline__ uint32_t div_by(uint32_t n, uint32_t m, uint32_t sh)
+{
+    const uint32_t t = __umulhi(n, m);
+    return (t + ((n - t) >> (sh & 0xFFu))) >> (sh >> 8);
+}
+
 struct TcParams
 {
     const uint8_t *in;  // channel-major input, or its channels-last copy
@@ -102,6 +126,7 @@ struct TcParams
     int2 *list_out, *final_list;  // list_out: each row's next entry at the row's index
     int *list_bc;                 // per compaction block of list_out, its entries with a step (added by the writers)
     int *tile_ctr;                // search: tickets of the tiles after each CTA's first (zeroed; null: static)
+    uint32_t ohw_m, ohw_sh, ow_m, ow_sh;  // division by ohw and ow: div_magic's multiplier and shifts
     int *final_count;
     int4 *fix_list;  // rows left for the exact recompute: (pixel, step, row index, winner)
     int *fix_count;
@@ -1186,7 +1211,7 @@ __device__ __forceinline__ void list_count_warp(int *bc, int idx, bool valid)
 
 __device__ __forceinline__ void s_extremes(const TcParams &P, int pix, const SearchAct &r)
 {
-    const int smp = pix / int(P.ohw);
+    const int smp = int(div_by(uint32_t(pix), P.ohw_m, P.ohw_sh));
     if (r.max) atomicMax(P.maxs + smp, order_enc(r.maxv));
     if (r.thv && P.thv != 0.f)
     {
@@ -1475,8 +1500,9 @@ __device__ __forceinline__ void search_producer(const TcParams &P, const int4 *t
                     e = s_ent[cb * BM + row0 + RS * i];
                     if (P.round != 1) e.y = P.T - 1;
                 }
-                const uint32_t ohw = uint32_t(P.ohw), smp = uint32_t(e.x) / ohw, pix = uint32_t(e.x) - smp * ohw;
-                const int oy = int(pix / uint32_t(P.ow)), ox = int(pix) - oy * P.ow;
+                const uint32_t smp = div_by(uint32_t(e.x), P.ohw_m, P.ohw_sh);
+                const uint32_t pix = uint32_t(e.x) - smp * uint32_t(P.ohw);
+                const int oy = int(div_by(pix, P.ow_m, P.ow_sh)), ox = int(pix) - oy * P.ow;
                 ubase[i] = int(int64_t(smp) * P.img_stride);
                 uyx[i] = int((uint32_t(oy * P.sy - P.top + 32768) << 16) | uint32_t(ox * P.sx - P.left + 32768));
                 utt[i] = uint32_t(e.y + 1) * 0x01010101u;
@@ -3220,6 +3246,10 @@ TcParams prepare(const Plan &pl, const void *in, const float *kernel, int64_t n,
     P.in = a_src;
     P.wimg = wimg;
     P.ohw = oh * ow;
+    {
+        const DivMagic a = div_magic(uint32_t(oh * ow)), c = div_magic(uint32_t(ow));
+        P.ohw_m = a.m, P.ohw_sh = a.sh, P.ow_m = c.m, P.ow_sh = c.sh;
+    }
     P.cin = int(cin), P.h = int(h), P.w = int(w), P.cout = int(cout), P.kh = int(kh), P.kw = int(kw);
     P.oh = int(oh), P.ow = int(ow), P.sy = int(sy), P.sx = int(sx), P.top = int(p.top), P.left = int(p.left);
     P.kblocks = pl.kblocks, P.n_tile = pl.n_tile, P.n_tiles = pl.n_tiles, P.nsplit = pl.nsplit;

@@ -193,3 +193,24 @@ def test_search_large_maps(port, side):
     ref = port.fire(port.inhibit(port.threshold(port.conv(x, w, (1, 1), (1, 1, 1, 1)), 4.0)))
     assert np.array_equal(host(spk), ref) and int(ref.sum()) > 0
     assert np.array_equal(host(pooled), port.pool(ref, (2, 2)))
+
+
+def test_search_long_lists():
+    """More than 2048 x 2048 output pixels in one call: the list compactions
+    take the three-launch form (per-block counts, one-block scan, scatter);
+    the result equals the two halves of the batch run separately (each on
+    the one-launch form; samples are independent without WTA)."""
+    rng = np.random.default_rng(5)
+    b, side = 66, 256  # 66 * 256 * 256 = 4.33M output pixels
+    x = cumulative(rng, b, 4, 2, side, side)
+    w = rng.uniform(0.3, 1.0, size=(8, 2, 3, 3)).astype(np.float32)
+    conv = spyker.Conv(2, 8, 3, pad=1)
+    conv.kernel.copy_(cuda(w))
+    conv.precision = "bf16x3"
+    xd = cuda(x)
+    spk, _, pooled = spyker.conv_fire_wta(xd, conv, 4.0, 0, 0, pool=2)
+    assert spyker._lib.lib.spk_device_status(1) == 0
+    for lo, hi in ((0, b // 2), (b // 2, b)):
+        s_h, _, p_h = spyker.conv_fire_wta(xd[lo:hi].contiguous(), conv, 4.0, 0, 0, pool=2)
+        assert torch.equal(spk[lo:hi], s_h) and torch.equal(pooled[lo:hi], p_h)
+    assert int(spk[:, -1].sum()) > 0
