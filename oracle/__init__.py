@@ -371,6 +371,33 @@ class Oracle:
         self._call("orc_ref_quantize", x, _CODES[x.dtype], x.size, float(lower), float(middle), float(upper))
         return x
 
+    def zca_fit(self, x, epsilon: float, transform: bool = False):
+        """cpu/zca.cpp:67-105 on samples [N, ...] (F32/F64; reference build
+        only): (mean [D], trans [D, D], x whitened in place if `transform`)."""
+        x = self._c(x).copy()
+        n, d = x.shape[0], int(np.prod(x.shape[1:]))
+        mean = np.zeros(d, dtype=x.dtype)
+        trans = np.zeros((d, d), dtype=x.dtype)
+        self._call("orc_ref_zca_fit", x, _CODES[x.dtype], n, d, mean, trans, float(epsilon), int(transform))
+        return mean, trans, x
+
+    def zca_trans(self, x, mean, trans):
+        """cpu/zca.cpp:107-118: (x - mean) trans on a copy (reference build only)."""
+        x = self._c(x).copy()
+        n, d = x.shape[0], int(np.prod(x.shape[1:]))
+        mean = np.ascontiguousarray(mean, dtype=x.dtype)
+        trans = np.ascontiguousarray(trans, dtype=x.dtype)
+        self._call("orc_ref_zca_trans", x, _CODES[x.dtype], n, d, mean, trans)
+        return x
+
+    def zca_split(self, x):
+        """cpu/zca.cpp:139-155: [N, ...] -> [N, 2, ...] (reference build only)."""
+        x = self._c(x)
+        n, d = x.shape[0], int(np.prod(x.shape[1:]))
+        out = np.zeros((n, 2) + x.shape[1:], dtype=x.dtype)
+        self._call("orc_ref_zca_split", x, _CODES[x.dtype], n, d, out)
+        return out
+
     # -- sparse event lists (offsets [U*T+1], zyx [N, 3]) -----------------
     def sparse_code(self, x, time: int, sort: bool = True):
         x = self._c(x)

@@ -622,6 +622,29 @@ int orc_ref_canny(const uint8_t *in, uint8_t *out, int64_t n, int64_t h, int64_t
     });
 }
 
+// cpu/zca.cpp:67-118 (ZCA fit, with the in-place transform when `transform`)
+// on input [n, d] F32/F64, mean [d] and trans [d, d] of the same type.
+int orc_ref_zca_fit(void *in, int type, int64_t n, int64_t d, void *mean, void *trans, double epsilon,
+                    int transform)
+{
+    return guard([&] {
+        cpu_zca_fit(Dyn2(in, ty(type), n, d), Dyn1(mean, ty(type), d), Dyn2(trans, ty(type), d, d),
+                    Scalar(epsilon), transform != 0);
+    });
+}
+
+// cpu/zca.cpp:107-118 (in-place ZCA transform of input [n, d])
+int orc_ref_zca_trans(void *in, int type, int64_t n, int64_t d, void *mean, void *trans)
+{
+    return guard([&] { cpu_zca_trans(Dyn2(in, ty(type), n, d), Dyn1(mean, ty(type), d), Dyn2(trans, ty(type), d, d)); });
+}
+
+// cpu/zca.cpp:139-155 (split [n, d] -> [n, 2, d])
+int orc_ref_zca_split(void *in, int type, int64_t n, int64_t d, void *out)
+{
+    return guard([&] { cpu_zca_split(Dyn2(in, ty(type), n, d), Dyn3(out, ty(type), n, 2, d)); });
+}
+
 int orc_ref_quantize(void *data, int type, int64_t n, double lower, double middle, double upper)
 {
     return guard([&] { cpu_quantize(Dyn1(data, ty(type), n), Scalar(lower), Scalar(middle), Scalar(upper)); });

@@ -9,10 +9,14 @@ Follows src/spyker/cpu/zca.cpp:67-155 (zca_fit, zca_trans, zca_split):
   transform: X <- (X - mean) trans                          (zca.cpp:99-118)
   split: [N, D] -> [N, 2, D] = (max(x, 0), max(-x, 0))      (zca.cpp:140-155)
 
-Parity unpinned against the reference build: its ZCA needs BLAS and LAPACK
-(zca.cpp:121-136 refuses without them), neither is present here, and the
-reference ships no ZCA test or fixture.  The restatement is pinned by the
-defining properties instead (tests/test_zca_rule.py).
+Pinned to the reference's own cpu/zca.cpp: that file needs the Blasw
+BLAS/LAPACK wrapper (github.com/Mathific/Blasw, an empty submodule in the
+reference tree; zca.cpp:121-136 refuses without it), so oracle/Makefile
+compiles it unmodified against oracle/blasw_shim (a stand-in giving gemv,
+gemm/symm, syrk and a Jacobi eigensolver the semantics zca.cpp relies on),
+and tests/test_zca_rule.py compares this restatement with that build as well
+as with the defining properties of ZCA whitening.  The eigensolver inside the
+pinned build is the stand-in's, not the reference's LAPACK.
 """
 
 from __future__ import annotations
