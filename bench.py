@@ -502,6 +502,19 @@ def load_synth():
     return mod
 
 
+def cpu_model() -> str:
+    """The host CPU's model name (/proc/cpuinfo), recorded beside each CPU
+    baseline together with the thread count it ran with."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def _ref_setup():
     import torch
 
@@ -526,7 +539,7 @@ def cpu_baseline(seconds: float) -> dict:
         reference_step(o, torch, imgs, w1, w2, dk)
         n += 64
     dt = time.perf_counter() - t0
-    return {"value": n / dt, "unit": "images/s", "cores": torch.get_num_threads(), "kind": kind,
+    return {"value": n / dt, "unit": "images/s", "cores": torch.get_num_threads(), "kind": kind, "cpu": cpu_model(),
             "sample": f"{n} images in batches of 64 through the same 2-layer pipeline, {dt:.1f} s"}
 
 
@@ -553,7 +566,7 @@ def reference_arm(args, rank, world):
         "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded stroke images, MNIST geometry)",
         "config": headline_config(args.batch, world, args.mode),
-        "cpu_baseline": {"value": v, "unit": "images/s", "cores": torch.get_num_threads(), "kind": kind,
+        "cpu_baseline": {"value": v, "unit": "images/s", "cores": torch.get_num_threads(), "kind": kind, "cpu": cpu_model(),
                          "sample": f"{sample} of each step's {args.batch} images per timed step (the CPU path's "
                                    f"cost is per image), reference CPU backend + oneDNN convolution via torch"},
         "e2e": {"value": v, "unit": "images/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -704,7 +717,7 @@ def config0_arm(args, rank, world):
         "parity_note": f"after {steps} training steps; the reference's layer and STDP run on the GPU's rank code",
         "rank_code_match_vs_reference_pct": 100.0 * float(np.mean(codes_gpu == codes_ref)),
         "weights_max_rel_diff_vs_reference_own_code": rel_own,
-        "cpu_baseline": {"value": batch / ref_s, "unit": "images/s", "cores": torch_.get_num_threads(), "kind": kind,
+        "cpu_baseline": {"value": batch / ref_s, "unit": "images/s", "cores": torch_.get_num_threads(), "kind": kind, "cpu": cpu_model(),
                          "sample": f"{steps} steps of the same {batch} images, reference CPU backend + oneDNN "
                                    f"convolution via torch"},
         "clocks": clk.summary(),
@@ -900,7 +913,7 @@ def gabor_cpu_baseline(seconds: float, net) -> dict:
         _gabor_ref_step(o, torch, imgs[n % 4:n % 4 + 1], gk, w1, w2)
         n += 1
     dt = time.perf_counter() - t0
-    return {"value": n / dt, "unit": "images/s", "cores": torch.get_num_threads(), "kind": kind,
+    return {"value": n / dt, "unit": "images/s", "cores": torch.get_num_threads(), "kind": kind, "cpu": cpu_model(),
             "sample": f"{n} images of 256x256, one at a time, {dt:.1f} s"}
 
 
@@ -1061,7 +1074,7 @@ def backprop_cpu_baseline(seconds: float, net, imgs, labels) -> dict:
         step(imgs[i:i + 2], labels[i:i + 2])
         n += 2
     dt = time.perf_counter() - t0
-    return {"value": n / dt, "unit": "images/s", "cores": torch.get_num_threads(), "kind": "port",
+    return {"value": n / dt, "unit": "images/s", "cores": torch.get_num_threads(), "kind": "port", "cpu": cpu_model(),
             "sample": f"{n} images, two per step, forward + target rule + backward in FP64 NumPy, {dt:.1f} s"}
 
 
@@ -1293,7 +1306,7 @@ def sparse_arm(args, rank, world):
             ref_step(w1, w2)
             k += n
         dt = time.perf_counter() - t0
-        line["cpu_baseline"] = {"value": k / dt, "unit": "images/s", "cores": os.cpu_count() or 1, "kind": kind,
+        line["cpu_baseline"] = {"value": k / dt, "unit": "images/s", "cores": os.cpu_count() or 1, "kind": kind, "cpu": cpu_model(),
                                 "sample": f"{k} images at 2 % density in batches of {n} (reference sparse backend, "
                                           f"its OpenMP threads), {dt:.1f} s"}
     print(json.dumps(line), flush=True)
