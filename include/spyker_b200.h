@@ -176,9 +176,9 @@ spk_status spk_rank_convstdp(const void *in, spk_dtype itype, int64_t b, int64_t
                              const int32_t *counts, int64_t count, int64_t sy, int64_t sx, const int64_t *pad4_host,
                              void *ws, size_t ws_bytes, spk_stream stream);
 /* No counterpart in the reference.  The same update as spk_rank_convstdp for
- * callers that cannot allocate device memory (e.g. code that must not call
- * cudaMalloc while a CUDA graph is being captured, or hosts whose allocator
- * owns the device): its scratch lives in a static 32 MiB device array that
+ * callers that cannot allocate device memory (hosts whose allocator owns all
+ * of the device's memory, or C callers without a device allocator): its
+ * scratch lives in a static 32 MiB device array that
  * every GPU loading the library holds until exit, so the call allocates
  * nothing.  Calls needing more scratch than that (2*B*count*Cin*KH*KW bytes
  * plus 2*B*count, each rounded up to 256) fail with SPK_ERR_ARGUMENT; split

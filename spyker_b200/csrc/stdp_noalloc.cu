@@ -2,9 +2,9 @@
 //
 // spk_rank_convstdp needs a scratch buffer for the first-spike times of every
 // winner's receptive field, and expects the caller to provide it.  Some
-// callers cannot call cudaMalloc at all: code running inside a CUDA-graph
-// capture that must not allocate, plug-in hosts whose allocator owns all
-// device memory, or C callers without a device allocator of their own.  For
+// callers cannot call cudaMalloc at all: plug-in hosts whose allocator owns
+// all device memory (a second allocator would fragment it or exceed its
+// budget), or C callers without a device allocator of their own.  For
 // them this file gives the same update with its scratch in a fixed static
 // device array, so the call allocates nothing.
 //

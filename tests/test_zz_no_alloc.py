@@ -1,7 +1,7 @@
 """spk_rank_convstdp_noalloc: conv STDP for callers that cannot allocate.
 
-Such callers (code that must not call cudaMalloc during a CUDA-graph capture,
-hosts whose allocator owns the device) cannot hand spk_rank_convstdp a
+Such callers (hosts whose allocator owns all of the device's memory, C code
+without a device allocator) cannot hand spk_rank_convstdp a
 workspace; the no-alloc entry point keeps its scratch in a static device
 array instead.  This checks, through the C ABI, that two calls in a row give
 exactly the weights of the workspace entry point (STDP results are compared
