@@ -1086,9 +1086,11 @@ SWEEP_WORKLOAD = ("sweep: 32 independent 2-layer STDP networks x 512 stroke imag
 
 
 def sweep_arm(args, rank, world):
-    """All networks' training step: per size one multi-network fused launch
-    per layer and one multi-network STDP scan per layer, captured once as a
-    CUDA graph and replayed; schedules picked by the autotuner.  Several
+    """All networks' training step: per size and layer each network's
+    single-network fused search call (``--sweep-path search``) or one
+    multi-network fused launch with autotuned schedules (``dense``), and one
+    multi-network STDP scan per layer, captured once as a CUDA graph and
+    replayed.  Several
     GPUs: each rank trains its own 32 networks (seeds differ by rank), no
     exchange; time = max over ranks."""
     import torch
@@ -1113,7 +1115,8 @@ def sweep_arm(args, rank, world):
 
     nets = 32
     images = 512 if args.batch == BATCH else args.batch
-    sw = sweep.Sweep(nets=nets, images=images, seed=10 * rank, device=dev, precision=args.precision, tune=True)
+    sw = sweep.Sweep(nets=nets, images=images, seed=10 * rank, device=dev, precision=args.precision, tune=True,
+                     path=args.sweep_path)
     sw.capture()
     for _ in range(max(args.warmup - 1, 0)):
         sw.replay()
@@ -1174,14 +1177,15 @@ def sweep_arm(args, rank, world):
         "data": "synthetic (seeded stroke images of 4 sizes)",
         "config": {"workload": SWEEP_WORKLOAD, "global_batch": n_img * world, "seq_len": 15,
                    "parallelism": f"replicas{world}",
-                   "networks": nets, "padded_samples": sw.total, "cuda_graph": True,
+                   "networks": nets, "padded_samples": sw.total, "cuda_graph": True, "path": sw.path,
                    "schedules": {f"{sw.groups[g].size}px/layer{l + 1}": list(v) for (g, l), v in sw.schedules.items()},
                    "l2": "inputs larger than L2: 2.0 GB of layer-1 spikes per step"},
         "e2e": {"value": n_img * world / (e2e_ms * 1e-3), "unit": "images/s", "h2d_bytes_per_step": h2d * world,
                 "d2h_bytes_per_step": int(sum(f.numel() for f in feats)) * world},
         "gpu_launches": int(launches),
         "eager_step_ms": eager_ms,
-        "roofline": {"bound": "tensor", "kernel": "all fused layers (algorithmic conv FLOPs of the real images)",
+        "roofline": {"bound": "tensor", "kernel": "all fused layers (algorithmic conv FLOPs of the real images"
+                               + ("; dense-equivalent: the search evaluates fewer rows)" if sw.path == "search" else ")"),
                      "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                      "peak_source": peak_source},
         "clocks": clk.summary(),
@@ -1398,6 +1402,9 @@ def main():
     ap.add_argument("--mode", default="replicas", choices=["replicas", "dp"],
                     help="several GPUs: independent networks (replicas, the default) or one network trained data "
                          "parallel (dp: one all-gather of the winners per layer and step)")
+    ap.add_argument("--sweep-path", default="search", choices=["dense", "search"],
+                    help="sweep workload: one multi-network fused launch per size and layer (dense), or the "
+                         "single-network first-crossing search per network (search)")
     ap.add_argument("--graph", action="store_true",
                     help="run the headline step as one captured CUDA graph (measured at the eager step's time: "
                          "the kernels dominate and the eager queue already hides the launches)")

@@ -8,7 +8,12 @@ uneven sizes.  One step trains every network on its whole stream:
 
 * images are grouped by size; per size and layer ONE fused tcgen05 launch
   (``spk_conv_fire_wta_nets``) runs all networks, each tile reading its
-  network's weight image and threshold;
+  network's weight image and threshold (``path="dense"``); or, with
+  ``path="search"``, each network's share of the group takes the
+  single-network fused layer (``spk_conv_fire_wta``), whose first-crossing
+  search on u8 tensor cores evaluates about log2(T) + 2 of a pixel's T
+  potential rows where the weights are non-negative (more launches, much
+  less work per image);
 * per layer ONE ordered STDP scan (``spk_stdp_scan_nets``) updates all
   networks, each walking its winners in the order of its own image stream
   (the reference's per-sample sequential rule, cpu/stdp.cpp:99-169), across
@@ -98,9 +103,11 @@ class Sweep:
     uniformly from ``sizes``."""
 
     def __init__(self, nets: int = 32, images: int = 512, sizes=(20, 28, 40, 64), seed: int = 0, device=None,
-                 precision: str = "bf16x3", tune: bool = True):
+                 precision: str = "bf16x3", tune: bool = True, path: str = "dense"):
+        if path not in ("dense", "search"):
+            raise ValueError("path must be 'dense' or 'search'")
         dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
-        self.dev, self.precision, self.nets = dev, precision, nets
+        self.dev, self.precision, self.nets, self.path = dev, precision, nets, path
         self.specs = [NetworkSpec(n, seed, images, sizes) for n in range(nets)]
         self.dog = M.DoG(3, [M.DoGFilter(1, 2), M.DoGFilter(2, 1)], pad=3, device=dev)
         self.w1 = torch.from_numpy(numpy.stack([s.w1 for s in self.specs])).to(dev)
@@ -143,12 +150,14 @@ class Sweep:
                     torch.zeros((b, COUNT2, C1 * 25), dtype=torch.int16, device=dev)]
         self.post = [torch.zeros((b, c), dtype=torch.int16, device=dev) for c in (COUNT1, COUNT2)]
         self.schedules = {}
-        if tune:
+        if tune and path == "dense":  # the schedules are the multi-network kernel's
             self.tune()
         self.graph = None
 
     # -- one layer of one size group, all networks -----------------------
     def _layer(self, gi, layer, x, pool, sched=None):
+        if self.path == "search":
+            return self._layer_search(gi, layer, x, pool)
         g = self.groups[gi]
         w, thr, cout, count, radius = ((self.w1, self.thr1, C1, COUNT1, RADIUS1) if layer == 0
                                        else (self.w2, self.thr2, C2, COUNT2, RADIUS2))
@@ -173,6 +182,38 @@ class Sweep:
                  stream())
         finally:
             call("spk_set_conv_schedule", 0, 0, 0)
+        return spikes, pooled
+
+    def _layer_search(self, gi, layer, x, pool):
+        """The group's layer as one single-network fused call per network, on
+        that network's contiguous share of the group (its weights and
+        threshold); records and counts land in the same slots as on the
+        multi-network kernel."""
+        g = self.groups[gi]
+        w, cout, count, radius = ((self.w1, C1, COUNT1, RADIUS1) if layer == 0 else (self.w2, C2, COUNT2, RADIUS2))
+        b, _, cin, h, wd = x.shape
+        ph, pw = (h, wd) if pool == "global" else (pool, pool)
+        spikes = torch.empty((b, T, cout, h, wd), dtype=torch.uint8, device=x.device)
+        pooled = torch.empty((b, T, cout, h // ph, wd // pw), dtype=torch.uint8, device=x.device)
+        o = int(self.goff[gi])
+        rec, cnt = self.rec[layer][o:o + b], self.cnt[layer][o:o + b]
+        rec.zero_()
+        cnt.zero_()
+        prec = M._PRECISION[self.precision]
+        sizes = [int(g.offsets[n + 1] - g.offsets[n]) for n in range(self.nets)]
+        nb = _lib.lib.spk_conv_fire_wta_workspace(max(sizes), T, cin, h, wd, cout, 5, 5, 1, 1, i64(2, 2, 2, 2), prec)
+        if nb == 0:
+            raise RuntimeError("layer does not fit the fused single-network kernel")
+        ws, wsb = M._workspace(nb, x.device)
+        for n, k in enumerate(sizes):
+            if k == 0:
+                continue
+            lo = int(g.offsets[n])
+            sl = slice(lo, lo + k)
+            thr = self.specs[n].theta if layer == 0 else self.specs[n].theta2
+            call("spk_conv_fire_wta", ptr(x[sl]), 4, ptr(w[n]), k, T, cin, h, wd, cout, 5, 5, 1, 1, i64(2, 2, 2, 2),
+                 float(thr), 0.0, 0.0, 0.0, radius, radius, count, 0.0, ptr(spikes[sl]), ptr(rec[sl]), ptr(cnt[sl]),
+                 ph, pw, ptr(pooled[sl]), prec, ptr(ws), wsb, stream())
         return spikes, pooled
 
     def _prepost(self, gi, layer, x, spikes):

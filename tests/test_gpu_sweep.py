@@ -166,8 +166,9 @@ def _alone(sw, n):
     return c1.kernel, c2.kernel
 
 
-def test_sweep_step_equals_each_network_alone():
-    sw = sweep.Sweep(nets=3, images=7, sizes=(20, 28), seed=1, device=DEV, tune=False)
+@pytest.mark.parametrize("path", ["dense", "search"])
+def test_sweep_step_equals_each_network_alone(path):
+    sw = sweep.Sweep(nets=3, images=7, sizes=(20, 28), seed=1, device=DEV, tune=False, path=path)
     sw.step()
     assert _lib.lib.spk_device_status(1) == 0
     for n in range(3):
@@ -188,4 +189,24 @@ def test_sweep_graph_replay_and_tuned_schedules():
     torch.cuda.synchronize()
     assert torch.equal(tuned.w1, eager.w1) and torch.equal(tuned.w2, eager.w2)
     for a, b in zip(tuned.graph_features, eager.last_features):
+        assert torch.equal(a, b)
+
+
+def test_sweep_search_path_equals_dense_path_and_replays():
+    """Per-network single-network calls (path="search") against the
+    multi-network kernel (path="dense") over all four image sizes: two
+    steps, the search path's second one a CUDA-graph replay; weights and
+    features equal bit for bit."""
+    dense = sweep.Sweep(nets=4, images=6, sizes=(20, 28, 40, 64), seed=2, device=DEV, tune=False, path="dense")
+    dense.step()
+    dense.step()
+    srch = sweep.Sweep(nets=4, images=6, sizes=(20, 28, 40, 64), seed=2, device=DEV, tune=False, path="search")
+    assert srch.schedules == {}
+    srch.capture()  # runs one step while warming up
+    srch.replay()
+    torch.cuda.synchronize()
+    assert _lib.lib.spk_device_status(1) == 0
+    assert torch.equal(srch.w1, dense.w1) and torch.equal(srch.w2, dense.w2)
+    assert not torch.equal(srch.w2, torch.from_numpy(np.stack([s.w2 for s in srch.specs])).to(DEV))
+    for a, b in zip(srch.graph_features, dense.last_features):
         assert torch.equal(a, b)
