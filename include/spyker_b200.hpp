@@ -3,9 +3,11 @@
  * header-only, over the C ABI of spyker_b200.h.
  *
  * Same names, argument order, defaults and error conditions as the reference
- * for: Tensor (device tensors only), Expand2 / Expand4, DoGFilter, DoG, Conv
- * (operator(), stdp), STDPConfig, Winner / Winners, code, threshold,
- * infinite, fire, gather, scatter, pad, pool, inhibit, convwta, fcwta, conv.
+ * for: Tensor (device tensors only), Expand2 / Expand4, DoGFilter, DoG,
+ * GaborFilter, Gabor, LoG, Conv (operator(), stdp), FC (operator(), stdp,
+ * backward), STDPConfig, BPConfig, Winner / Winners, code, threshold,
+ * infinite, fire, gather, scatter, pad, pool, inhibit, convwta, fcwta, conv,
+ * fc, backward, labelize.
  * Tensors live in the current CUDA device's memory; the reference's host
  * tensors become Tensor::from_host / Tensor::to_host.  Every call is queued on
  * Spyker::stream() (the legacy default stream unless set), so calls run in
@@ -23,6 +25,7 @@
 
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdint>
 #include <memory>
 #include <stdexcept>
@@ -248,6 +251,27 @@ struct DoGFilter
 {
     F64 std1, std2;
     DoGFilter(F64 std1, F64 std2) : std1(std1), std2(std2) {}
+};
+
+/* opers.h:176-206: theta given in degrees, kept in radians. */
+struct GaborFilter
+{
+    F64 sigma, theta, gamma, lambda, psi;
+    GaborFilter(F64 sigma, F64 theta, F64 gamma, F64 lambda, F64 psi)
+        : sigma(sigma), theta(theta * 0.017453292519943295), gamma(gamma), lambda(lambda), psi(psi)
+    {
+    }
+};
+
+/* utils.h:525-547. */
+struct BPConfig
+{
+    float sfactor = 1, lrate = 1, lrf = 1, lambda = 0;
+    BPConfig() {}
+    BPConfig(float sfactor, float lrate, float lrf, float lambda)
+        : sfactor(sfactor), lrate(lrate), lrf(lrf), lambda(lambda)
+    {
+    }
 };
 
 namespace detail
@@ -566,6 +590,78 @@ inline Tensor conv(Tensor input, Tensor kernel, Expand2 stride = 1, Expand4 pad 
     return out;
 }
 
+/* ---- fully connected and temporal backprop (opers.h:560-580, 755-761) ------ */
+
+/* input [B, T, I] (U8 or F32; [T, I] is one sample), kernel [O, I] F32 ->
+ * output [B, T, O] F32; sign: the kernel's signs (cpu/fc.cpp). */
+inline Tensor fc(Tensor input, Tensor kernel, Tensor output, bool sign = false)
+{
+    detail::require(input.dims() == 2 || input.dims() == 3, "Input dimensions couldn't be viewed as 3D.");
+    detail::require(input.type() == Type::U8 || input.type() == Type::F32, "fc takes U8 or F32 input.");
+    detail::require(kernel.dims() == 2 && kernel.type() == Type::F32, "Kernel must be a 2D F32 tensor.");
+    Shape s = input.shape();
+    if (s.size() == 2) s.insert(s.begin(), 1);
+    detail::require(s[2] == kernel.shape(1), "Input and kernel shapes don't match.");
+    detail::require(output.type() == Type::F32 && output.numel() == s[0] * s[1] * kernel.shape(0),
+                    "Output shape is not compatible with the input.");
+    detail::check(spk_fc(input.data(), detail::dt(input.type()), kernel.data<float>(), output.data<float>(), s[0] * s[1],
+                         s[2], kernel.shape(0), int(sign), stream()),
+                  "fc");
+    return output;
+}
+
+inline Tensor fc(Tensor input, Tensor kernel, bool sign = false)
+{
+    Shape s = input.shape();
+    detail::require(!s.empty(), "Input dimensions couldn't be viewed as 3D.");
+    s.back() = kernel.dims() == 2 ? kernel.shape(0) : 0;
+    Tensor out(Type::F32, s);
+    return fc(input, kernel, out, sign);
+}
+
+/* Target-rule gradient of first-spike times: input / output [B, ...] F32,
+ * target [B] I64 (cpu/backprop.cpp:40-62). */
+inline Tensor backward(Tensor input, Tensor output, Tensor target, Size time, F64 gamma)
+{
+    detail::require(time > 0, "Time steps must be higher than zero.");
+    detail::require(input.type() == Type::F32 && output.type() == Type::F32, "backward takes F32 tensors.");
+    detail::require(target.type() == Type::I64, "Target type must have I64 type.");
+    detail::require(input.dims() >= 1 && target.numel() == input.shape(0), "Input and target shapes are not compatible.");
+    detail::require(output.shape() == input.shape(), "Output shape is not compatible with the input.");
+    const Size b = input.shape(0);
+    detail::check(spk_backward(input.data<float>(), output.data<float>(), target.data<int64_t>(), b,
+                               b > 0 ? input.numel() / b : 0, time, gamma, stream()),
+                  "backward");
+    return output;
+}
+
+inline Tensor backward(Tensor input, Tensor target, Size time, F64 gamma)
+{
+    Tensor out(Type::F32, input.shape());
+    return backward(input, out, target, time, gamma);
+}
+
+/* input [B, T, N, ...] F32 -> output [B] I64 labels (cpu/backprop.cpp:68-99). */
+inline Tensor labelize(Tensor input, Tensor output, F64 threshold)
+{
+    detail::require(input.dims() >= 3, "Input dimensions must be at least 3.");
+    detail::require(input.type() == Type::F32, "labelize takes F32 input.");
+    detail::require(output.type() == Type::I64 && output.numel() == input.shape(0),
+                    "Output shape is not compatible with the input.");
+    const Size b = input.shape(0), t = input.shape(1);
+    detail::check(spk_labelize(input.data(), detail::dt(input.type()), output.data<int64_t>(), b, t,
+                               detail::prod(input.shape(), 2), threshold, stream()),
+                  "labelize");
+    return output;
+}
+
+inline Tensor labelize(Tensor input, F64 threshold)
+{
+    detail::require(input.dims() >= 3, "Input dimensions must be at least 3.");
+    Tensor out(Type::I64, {input.shape(0)});
+    return labelize(input, out, threshold);
+}
+
 /* ---- modules (opers.h:211-456) ---------------------------------------------- */
 
 /* Difference-of-Gaussians bank, window 2 size + 1: [B, C, H, W] ->
@@ -612,6 +708,98 @@ public:
                                  kh, kw, oh, ow, p.data(), stream()),
                       "DoG");
         return out;
+    }
+};
+
+namespace detail
+{
+/* A filter bank's planes: [B, C, H, W] F32 -> [B, C fo, OH, OW] (spk_filter
+ * kind `which`, `nk` kernels of the bank). */
+inline Tensor filter_bank(int which, const Tensor &kernel, const Expand4 &pad, Tensor input, Size nk, Size fo,
+                          const char *what)
+{
+    require(kernel.valid(), "Filter is not initialized.");
+    require(input.dims() == 4, "Input dimensions must be 4.");
+    require(input.type() == Type::F32, "Filters take F32 input.");
+    const Shape s = input.shape();
+    const Size kh = kernel.shape(kernel.dims() - 2), kw = kernel.shape(kernel.dims() - 1);
+    const Size oh = s[2] + pad[0] + pad[2] - kh + 1, ow = s[3] + pad[1] + pad[3] - kw + 1;
+    require(oh > 0 && ow > 0, "Input and kernel shapes are not compatible.");
+    Tensor out(Type::F32, {s[0], s[1] * fo, oh, ow});
+    const auto p = pad4(pad);
+    check(spk_filter(which, input.data<float>(), kernel.data<float>(), out.data<float>(), s[0] * s[1], s[2], s[3], nk,
+                     kh, kw, oh, ow, p.data(), stream()),
+          what);
+    return out;
+}
+}  // namespace detail
+
+/* Gabor bank, window 2 size + 1: [B, C, H, W] -> [B, C F, OH, OW] raw
+ * responses (opers.h:254-291, cpu/dog.cpp). */
+class Gabor
+{
+    Expand4 _pad;
+
+public:
+    Tensor kernel;  // F32 [F, 2 size + 1, 2 size + 1]
+
+    Gabor() {}
+    Gabor(Size size, const std::vector<GaborFilter> &filters, Expand4 pad = 0) : _pad(pad)
+    {
+        detail::require(size > 0, "Input size can't be less than 1.");
+        detail::require(!filters.empty(), "Input filters count can't be less then 1.");
+        detail::require(pad[0] >= 0 && pad[1] >= 0 && pad[2] >= 0 && pad[3] >= 0, "Pad items are incorrect.");
+        const Size n = 2 * size + 1, f = Size(filters.size());
+        std::vector<double> g(static_cast<size_t>(n * n));
+        std::vector<float> k(static_cast<size_t>(f * n * n));
+        for (Size i = 0; i < f; ++i)
+        {
+            const GaborFilter &q = filters[size_t(i)];
+            detail::check(spk_gabor_kernel(g.data(), n, q.sigma, q.theta, q.gamma, q.lambda, q.psi), "Gabor kernel");
+            for (Size j = 0; j < n * n; ++j) k[size_t(i * n * n + j)] = float(g[size_t(j)]);
+        }
+        kernel = Tensor::from_host(k.data(), Type::F32, {f, n, n});
+    }
+
+    Tensor operator()(Tensor input)
+    {
+        const Size f = kernel.valid() ? kernel.shape(0) : 0;
+        return detail::filter_bank(1, kernel, _pad, input, f, f, "Gabor");
+    }
+};
+
+/* Laplacian-of-Gaussian bank as DoG(std / sqrt 2, std sqrt 2), on and off
+ * parts: [B, C, H, W] -> [B, 2 C F, OH, OW] (opers.h:297-334, cpu/dog.cpp). */
+class LoG
+{
+    Expand4 _pad;
+
+public:
+    Tensor kernel;  // F32 [2, F, 2 size + 1, 2 size + 1]
+
+    LoG() {}
+    LoG(Size size, const std::vector<F64> &stds, Expand4 pad = 0) : _pad(pad)
+    {
+        detail::require(size > 0, "Input size can't be less than 1.");
+        detail::require(!stds.empty(), "Input stds count can't be less then 1.");
+        detail::require(pad[0] >= 0 && pad[1] >= 0 && pad[2] >= 0 && pad[3] >= 0, "Pad items are incorrect.");
+        const Size n = 2 * size + 1, f = Size(stds.size());
+        std::vector<double> g(static_cast<size_t>(n * n));
+        std::vector<float> k(static_cast<size_t>(2 * f * n * n));
+        for (Size i = 0; i < f; ++i)
+            for (int which = 0; which < 2; ++which)
+            {
+                const F64 sd = which ? stds[size_t(i)] * std::sqrt(2.0) : stds[size_t(i)] / std::sqrt(2.0);
+                detail::check(spk_gaussian_kernel(g.data(), n, sd), "LoG kernel");
+                for (Size j = 0; j < n * n; ++j) k[size_t((which * f + i) * n * n + j)] = float(g[size_t(j)]);
+            }
+        kernel = Tensor::from_host(k.data(), Type::F32, {2, f, n, n});
+    }
+
+    Tensor operator()(Tensor input)
+    {
+        const Size f = kernel.valid() ? kernel.shape(1) : 0;
+        return detail::filter_bank(2, kernel, _pad, input, f, 2 * f, "LoG");
     }
 };
 
@@ -671,6 +859,89 @@ public:
                                         _stride[1], p.data(), ws.ptr, ws.bytes, stream()),
                       "Conv::stdp");
         synchronize();  // the host winner arrays are freed on return
+    }
+};
+
+/* Fully connected module with STDP and the target-rule backward
+ * (opers.h:457-518, cpu/fc.cpp, cpu/stdp.cpp:42-97, cpu/backprop.cpp:105-160). */
+class FC
+{
+public:
+    Tensor kernel;  // F32 [O, I]
+    std::vector<STDPConfig> stdpconfig;
+    BPConfig bpconfig;
+
+    FC() {}
+    FC(Size input, Size output, F64 mean = .5, F64 std = .02)
+    {
+        detail::require(input > 0 && output > 0, "Input and output sizes can't be less than 1.");
+        const Size n = output * input;
+        std::vector<double> w(static_cast<size_t>(n));
+        detail::check(spk_normal_kernel(w.data(), n, mean, std), "FC kernel");
+        std::vector<float> f(w.begin(), w.end());
+        kernel = Tensor::from_host(f.data(), Type::F32, {output, input});
+    }
+
+    Tensor operator()(Tensor input, Tensor output, bool sign = false)
+    {
+        detail::require(kernel.valid(), "FC is not initialized.");
+        return fc(input, kernel, output, sign);
+    }
+    Tensor operator()(Tensor input, bool sign = false)
+    {
+        detail::require(kernel.valid(), "FC is not initialized.");
+        return fc(input, kernel, sign);
+    }
+
+    /* input [B, T, I] spikes, output [B, T, O] spikes. */
+    void stdp(Tensor input, const Winners &winners, Tensor output)
+    {
+        detail::require(!stdpconfig.empty(), "At least one STDP Config must be given.");
+        detail::require(input.dims() == 3 && output.dims() == 3, "Input and output dimensions must be 3.");
+        const Shape s = input.shape(), o = output.shape();
+        detail::require(o[0] == s[0] && o[1] == s[1] && o[2] == kernel.shape(0) && s[2] == kernel.shape(1),
+                        "Tensor shapes are not compatible.");
+        for (const auto &v : winners)
+            for (const auto &x : v)
+                detail::require(x.c >= 0 && x.c < Size(stdpconfig.size()), "Winner STDP config index out of range.");
+        Size count = 0;
+        auto rc = detail::winners_to(winners, s[0], count);
+        const auto cfg = detail::configs(stdpconfig);
+        detail::Scratch ws(spk_rank_fcstdp_workspace(s[0], s[1], s[2]));
+        detail::check(spk_rank_fcstdp(input.data(), detail::dt(input.type()), s[0], s[1], s[2], kernel.data<float>(),
+                                      kernel.shape(0), output.data(), cfg.data(), Size(stdpconfig.size()),
+                                      rc.first.data<int32_t>(), rc.second.data<int32_t>(), count, ws.ptr, ws.bytes,
+                                      stream()),
+                      "FC::stdp");
+        synchronize();  // the host winner arrays are freed on return
+    }
+
+    /* input [B, I], output and grad [B, O] F32: updates the kernel and
+     * bpconfig.sfactor and writes next [B, I], the gradient for the layer
+     * below (waits for the stream). */
+    Tensor backward(Tensor input, Tensor output, Tensor grad, Tensor next)
+    {
+        detail::require(kernel.valid(), "FC is not initialized.");
+        const Size no = kernel.shape(0), ni = kernel.shape(1);
+        detail::require(input.type() == Type::F32 && output.type() == Type::F32 && grad.type() == Type::F32 &&
+                            next.type() == Type::F32,
+                        "FC::backward takes F32 tensors.");
+        const Size b = input.dims() > 0 ? input.shape(0) : 0;
+        detail::require(input.numel() == b * ni && output.numel() == b * no && grad.numel() == b * no &&
+                            next.numel() == b * ni,
+                        "Tensor shapes are not compatible.");
+        float bp[4] = {bpconfig.sfactor, bpconfig.lrate, bpconfig.lrf, bpconfig.lambda};
+        detail::Scratch ws(spk_fcbackward_workspace(no, ni));
+        detail::check(spk_fcbackward(kernel.data<float>(), no, ni, input.data<float>(), output.data<float>(),
+                                     grad.data<float>(), next.data<float>(), b, bp, ws.ptr, ws.bytes, stream()),
+                      "FC::backward");
+        bpconfig.sfactor = bp[0];
+        return next;
+    }
+    Tensor backward(Tensor input, Tensor output, Tensor grad)
+    {
+        Tensor next(Type::F32, input.shape());
+        return backward(input, output, grad, next);
     }
 };
 

@@ -1,7 +1,8 @@
 """The C++ ``Spyker::`` layer (include/spyker_b200.hpp) over the C ABI.
 
-CPU: the header compiles with the reference's names, and a program using
-it links against the library.  GPU: that program runs one layer step (DoG,
+CPU: the header compiles with the reference's names, and programs using
+it (the layer step, and every module and function of the layer) link
+against the library.  GPU: that program runs one layer step (DoG,
 rank code, the plain FP32 ops, the fused tensor-core layer with pooling, STDP
 on its winners) and every result equals the Python API's on the same
 inputs."""
@@ -43,6 +44,20 @@ def test_program_links(tmp_path):
     if not os.path.exists(os.path.join(LIB, "libspyker_b200.so")):
         pytest.skip("library not built")
     assert os.path.exists(_build(tmp_path))
+
+
+def test_full_surface_links(tmp_path):
+    """Every module and function of the layer named after the reference's
+    opers.h (Gabor, LoG, FC with stdp / backward, fc, backward, labelize
+    beside the layer-step ones) compiles with the reference's argument forms
+    and links against the library."""
+    if not os.path.exists(os.path.join(LIB, "libspyker_b200.so")):
+        pytest.skip("library not built")
+    exe = str(tmp_path / "api_surface")
+    subprocess.check_call(["g++", *_flags(), os.path.join(ROOT, "tests", "cpp", "api_surface.cpp"), "-o", exe,
+                           "-L" + LIB, "-lspyker_b200", "-L" + os.path.join(CUDA, "lib64"), "-lcudart",
+                           "-Wl,-rpath," + LIB])
+    assert os.path.exists(exe)
 
 
 def _load(d, name, dtype, shape=None):
