@@ -7,7 +7,9 @@
  * GaborFilter, Gabor, LoG, Conv (operator(), stdp), FC (operator(), stdp,
  * backward), STDPConfig, BPConfig, Winner / Winners, code, threshold,
  * infinite, fire, gather, scatter, pad, pool, inhibit, convwta, fcwta, conv,
- * fc, backward, labelize.
+ * fc, backward, labelize, and the event-list path: SparseTensor, Sparse::code,
+ * conv, pad, gather, pool, inhibit, convwta, Conv on a SparseTensor and its
+ * stdp.
  * Tensors live in the current CUDA device's memory; the reference's host
  * tensors become Tensor::from_host / Tensor::to_host.  Every call is queued on
  * Spyker::stream() (the legacy default stream unless set), so calls run in
@@ -25,6 +27,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <memory>
@@ -803,6 +806,189 @@ public:
     }
 };
 
+/* Sparse binary spikes [U, T, C, H, W] as per-(sample, step) event lists
+ * (utils.h:369-420): on the device one CSR array, offsets I64 [U T + 1] and
+ * events I32 (x | y << 8 | z << 16), sized for the worst case so no call
+ * waits for the host. */
+class SparseTensor
+{
+public:
+    Tensor offsets, events;
+    Shape shape;
+
+    SparseTensor() {}
+    SparseTensor(const Shape &shape_, Size capacity)
+        : offsets(Type::I64, {shape_[0] * shape_[1] + 1}), events(Type::I32, {std::max<Size>(capacity, 1)}),
+          shape(shape_)
+    {
+    }
+    /* An event at the first step whose value exceeds threshold, per position
+     * of a dense [U, T, C, H, W] tensor (sparse/opers.cpp:59-86). */
+    explicit SparseTensor(Tensor dense, F64 threshold = 0)
+    {
+        detail::require(dense.dims() == 5, "Input dimensions must be 5.");
+        const Shape s = dense.shape();
+        *this = SparseTensor(s, s[0] * s[2] * s[3] * s[4]);
+        detail::Scratch ws(spk_sparse_from_dense_workspace(s[0], s[1], s[2], s[3], s[4]));
+        detail::check(spk_sparse_from_dense(dense.data(), detail::dt(dense.type()), s[0], s[1], s[2], s[3], s[4],
+                                            threshold, offsets.data<int64_t>(), events.data<uint32_t>(),
+                                            capacity(), ws.ptr, ws.bytes, stream()),
+                      "SparseTensor");
+    }
+
+    Size capacity() const { return events.numel(); }
+    /* Number of events (waits for the stream). */
+    Size numel() const
+    {
+        int64_t n = 0;
+        detail::cuda(cudaMemcpyAsync(&n, offsets.data<int64_t>() + (offsets.numel() - 1), sizeof(n),
+                                     cudaMemcpyDeviceToHost, stream()),
+                     "SparseTensor::numel");
+        detail::cuda(cudaStreamSynchronize(stream()), "SparseTensor::numel");
+        return Size(n);
+    }
+    F64 sparsity() const { return F64(numel()) / F64(detail::prod(shape)); }
+    /* Cumulative U8 spikes [U, T, C, H, W] (sparse/opers.cpp:88-104). */
+    Tensor dense() const
+    {
+        Tensor out(Type::U8, shape);
+        detail::Scratch ws(spk_sparse_dense_workspace(shape[0], shape[2], shape[3], shape[4]));
+        detail::check(spk_sparse_to_dense(offsets.data<int64_t>(), events.data<uint32_t>(), shape[0], shape[1],
+                                          shape[2], shape[3], shape[4], out.data(), SPK_U8, ws.ptr, ws.bytes,
+                                          stream()),
+                      "SparseTensor::dense");
+        return out;
+    }
+};
+
+/* The event-list path (opers.h:763-790, src/spyker/sparse/). */
+namespace Sparse
+{
+/* Rank-order (sort) or latency code of [U, C, H, W] into event lists
+ * (sparse/code.cpp:39-130). */
+inline SparseTensor code(Tensor input, Size time, bool sort = true)
+{
+    detail::require(time > 0, "Input time can't be less than 1.");
+    detail::require(input.dims() == 4, "Input dimensions must be 4.");
+    const Shape s = input.shape();
+    SparseTensor out({s[0], time, s[1], s[2], s[3]}, s[0] * s[1] * s[2] * s[3]);
+    detail::Scratch ws(spk_sparse_code_workspace(s[0], time, s[1], s[2], s[3]));
+    detail::check(spk_sparse_code(input.data(), detail::dt(input.type()), s[0], s[1], s[2], s[3], time, int(sort),
+                                  out.offsets.data<int64_t>(), out.events.data<uint32_t>(), out.capacity(), ws.ptr,
+                                  ws.bytes, stream()),
+                  "Sparse::code");
+    return out;
+}
+
+/* Incremental convolution and fire on event lists (sparse/conv.cpp:42-160). */
+inline SparseTensor conv(SparseTensor input, Tensor kernel, F64 threshold, Expand2 stride = 1, Expand4 pad = 0)
+{
+    detail::require(kernel.dims() == 4 && kernel.type() == Type::F32, "Kernel must be a 4D F32 tensor.");
+    const Shape &s = input.shape;
+    const Size cout = kernel.shape(0), kh = kernel.shape(2), kw = kernel.shape(3);
+    detail::require(kernel.shape(1) == s[2], "Input and kernel channels are not compatible.");
+    const Size oh = s[3] + pad[0] + pad[2] - kh + 1, ow = s[4] + pad[1] + pad[3] - kw + 1;
+    SparseTensor out({s[0], s[1], cout, oh, ow}, s[0] * cout * std::max<Size>(oh, 1) * std::max<Size>(ow, 1));
+    const auto s2 = stride.get();
+    const auto p = detail::pad4(pad);
+    detail::Scratch ws(spk_sparse_conv_workspace(s[0], s[1], s[3], s[4], cout, kh, kw, p.data()));
+    detail::check(spk_sparse_conv(input.offsets.data<int64_t>(), input.events.data<uint32_t>(), s[0], s[1], s[2],
+                                  s[3], s[4], kernel.data<float>(), cout, kh, kw, threshold, s2.data(), p.data(),
+                                  out.offsets.data<int64_t>(), out.events.data<uint32_t>(), out.capacity(), ws.ptr,
+                                  ws.bytes, stream()),
+                  "Sparse::conv");
+    return out;
+}
+
+/* Every event shifted by (top, left) (sparse/pad.cpp:37-55). */
+inline SparseTensor pad(SparseTensor input, Expand4 pad)
+{
+    detail::require(pad[0] >= 0 && pad[1] >= 0 && pad[2] >= 0 && pad[3] >= 0, "Pad items are incorrect.");
+    const Shape &s = input.shape;
+    SparseTensor out({s[0], s[1], s[2], s[3] + pad[0] + pad[2], s[4] + pad[1] + pad[3]}, input.capacity());
+    const auto p = detail::pad4(pad);
+    detail::check(spk_sparse_pad(input.offsets.data<int64_t>(), input.events.data<uint32_t>(), input.capacity(), s[0],
+                                 s[1], s[2], s[3], s[4], p.data(), out.offsets.data<int64_t>(),
+                                 out.events.data<uint32_t>(), out.capacity(), stream()),
+                  "Sparse::pad");
+    return out;
+}
+
+/* First event time per position [U, C, H, W], T when silent
+ * (sparse/opers.cpp:106-118). */
+inline Tensor gather(SparseTensor input, Tensor output)
+{
+    const Shape &s = input.shape;
+    detail::require(output.shape() == Shape({s[0], s[2], s[3], s[4]}), "Output shape is not compatible with the input.");
+    detail::Scratch ws(spk_sparse_dense_workspace(s[0], s[2], s[3], s[4]));
+    detail::check(spk_sparse_gather(input.offsets.data<int64_t>(), input.events.data<uint32_t>(), s[0], s[1], s[2],
+                                    s[3], s[4], output.data(), detail::dt(output.type()), ws.ptr, ws.bytes, stream()),
+                  "Sparse::gather");
+    return output;
+}
+
+inline Tensor gather(SparseTensor input, Type type = Type::U8)
+{
+    const Shape &s = input.shape;
+    Tensor out(type, {s[0], s[2], s[3], s[4]});
+    return gather(input, out);
+}
+
+/* The first event of every pooled cell; stride must equal the kernel
+ * (sparse/pool.cpp:37-64). */
+inline SparseTensor pool(SparseTensor input, Expand2 kernel, Expand2 stride = 0, Expand4 pad = 0)
+{
+    if (stride[0] == 0 && stride[1] == 0) stride = kernel;
+    detail::require(kernel[0] >= 1 && kernel[1] >= 1 && stride[0] >= 1 && stride[1] >= 1 && pad[0] >= 0 &&
+                        pad[1] >= 0 && pad[2] >= 0 && pad[3] >= 0,
+                    "Kernel, stride or pad items are incorrect.");
+    const Shape &s = input.shape;
+    const Size oh = (s[3] + pad[0] + pad[2] - kernel[0]) / stride[0] + 1;
+    const Size ow = (s[4] + pad[1] + pad[3] - kernel[1]) / stride[1] + 1;
+    detail::require(oh > 0 && ow > 0, "Input and kernel shapes are not compatible.");
+    const Size cap = std::max<Size>(1, std::min<Size>(input.capacity(), s[0] * s[2] * oh * ow));
+    SparseTensor out({s[0], s[1], s[2], oh, ow}, cap);
+    const auto k2 = kernel.get(), s2 = stride.get();
+    const auto p = detail::pad4(pad);
+    detail::Scratch ws(spk_sparse_pool_workspace(s[0], s[2], oh, ow, input.capacity()));
+    detail::check(spk_sparse_pool(input.offsets.data<int64_t>(), input.events.data<uint32_t>(), input.capacity(), s[0],
+                                  s[1], s[2], s[3], s[4], k2.data(), s2.data(), p.data(), oh, ow,
+                                  out.offsets.data<int64_t>(), out.events.data<uint32_t>(), out.capacity(), ws.ptr,
+                                  ws.bytes, stream()),
+                  "Sparse::pool");
+    return out;
+}
+
+/* Per pixel only the channel of its first event survives
+ * (sparse/inhibit.cpp:37-65). */
+inline SparseTensor inhibit(SparseTensor input)
+{
+    const Shape &s = input.shape;
+    SparseTensor out(s, input.capacity());
+    detail::Scratch ws(spk_sparse_inhibit_workspace(s[0], s[3], s[4], input.capacity()));
+    detail::check(spk_sparse_inhibit(input.offsets.data<int64_t>(), input.events.data<uint32_t>(), input.capacity(),
+                                     s[0], s[1], s[2], s[3], s[4], out.offsets.data<int64_t>(),
+                                     out.events.data<uint32_t>(), out.capacity(), ws.ptr, ws.bytes, stream()),
+                  "Sparse::inhibit");
+    return out;
+}
+
+/* Winners in (step, list) order outside every accepted box
+ * (sparse/wta.cpp:44-95; waits for the stream). */
+inline Winners convwta(SparseTensor input, Expand2 radius, Size count)
+{
+    detail::require(radius[0] >= 0 && radius[1] >= 0, "Radius items are incorrect.");
+    detail::require(count > 0, "Winners count can't be less than 1.");
+    const Shape &s = input.shape;
+    Tensor rec(Type::I32, {s[0], count, 5}), cnt(Type::I32, {s[0]});
+    const auto r2 = radius.get();
+    detail::check(spk_sparse_convwta(input.offsets.data<int64_t>(), input.events.data<uint32_t>(), s[0], s[1], s[2],
+                                     s[3], s[4], r2.data(), count, rec.data<int32_t>(), cnt.data<int32_t>(), stream()),
+                  "Sparse::convwta");
+    return detail::winners_from(rec, cnt, count);
+}
+}  // namespace Sparse
+
 /* 2D convolution module with STDP (opers.h:378-456, cpu/stdp.cpp:99-169). */
 class Conv
 {
@@ -836,6 +1022,37 @@ public:
     {
         detail::require(kernel.valid(), "Conv is not initialized.");
         return conv(input, kernel, _stride, _pad, precision);
+    }
+
+    /* The event-list form: incremental convolution and fire (opers.h:436). */
+    SparseTensor operator()(SparseTensor input, F64 threshold)
+    {
+        detail::require(kernel.valid(), "Conv is not initialized.");
+        return Sparse::conv(input, kernel, threshold, _stride, _pad);
+    }
+
+    /* STDP from event lists, F32 update arithmetic (opers.h:450,
+     * sparse/stdp.cpp:41-133). */
+    void stdp(SparseTensor input, const Winners &winners)
+    {
+        detail::require(!stdpconfig.empty(), "At least one STDP Config must be given.");
+        const Shape &s = input.shape;
+        detail::require(kernel.shape(1) == s[2], "Input and kernel channels are not compatible.");
+        for (const auto &v : winners)
+            for (const auto &x : v)
+                detail::require(x.c >= 0 && x.c < Size(stdpconfig.size()), "Winner STDP config index out of range.");
+        Size count = 0;
+        auto rc = detail::winners_to(winners, s[0], count);
+        const auto cfg = detail::configs(stdpconfig);
+        const auto p = detail::pad4(_pad);
+        detail::Scratch ws(spk_sparse_stdp_workspace(s[0], count, s[2], s[3], s[4], kernel.shape(2), kernel.shape(3),
+                                                     p.data()));
+        detail::check(spk_sparse_stdp(input.offsets.data<int64_t>(), input.events.data<uint32_t>(), s[0], s[1], s[2],
+                                      s[3], s[4], kernel.data<float>(), kernel.shape(0), kernel.shape(2),
+                                      kernel.shape(3), cfg.data(), Size(stdpconfig.size()), rc.first.data<int32_t>(),
+                                      rc.second.data<int32_t>(), count, p.data(), ws.ptr, ws.bytes, stream()),
+                      "Conv::stdp");
+        synchronize();  // the host winner arrays are freed on return
     }
 
     /* input [B, T, Cin, H, W] spikes, output [B, T, Cout, OH, OW] spikes. */

@@ -39,6 +39,13 @@ int main()
     Tensor next = fc1.backward(in2, times, grad);
     Tensor labels = labelize(Tensor(Type::F32, {2, 15, 10}), 1.0);
     LayerOutput lo = conv_fire_wta(codes, conv, 15, 3, 5, 2);
+    SparseTensor sc = Sparse::code(d, 15), sd(codes, 0.0);
+    SparseTensor sp = Sparse::inhibit(conv(sc, 15.0));
+    Winners sw = Sparse::convwta(sp, 3, 5);
+    conv.stdp(sc, sw);
+    SparseTensor sq = Sparse::pool(Sparse::pad(sp, 1), 2), sr = Sparse::conv(sd, conv.kernel, 15.0, 1, 2);
+    Tensor first = Sparse::gather(sq), dense = sr.dense();
+    std::printf("%lld %f %d %d\n", (long long)sq.numel(), sp.sparsity(), int(first.dims()), int(dense.dims()));
     synchronize();
     std::printf("%d %d %d %d %d %d %d %d %d\n", int(g.dims()), int(l.dims()), int(lat.dims()), int(padded.dims()),
                 int(back.dims()), int(inf.dims()), int(sout.dims() + plain.dims()), int(next.dims() + labels.dims()),
