@@ -137,12 +137,62 @@ PYBIND11_MODULE(spyker_b200_plugin, m)
         .def_readwrite("lower", &STDPConfig::lower)
         .def_readwrite("upper", &STDPConfig::upper);
 
+    py::class_<GaborFilter>(m, "GaborFilter")
+        .def(py::init<F64, F64, F64, F64, F64>())
+        .def_readwrite("sigma", &GaborFilter::sigma)
+        .def_readwrite("theta", &GaborFilter::theta)
+        .def_readwrite("gamma", &GaborFilter::gamma)
+        .def_readwrite("lambda_", &GaborFilter::lambda)
+        .def_readwrite("psi", &GaborFilter::psi);
+    py::class_<BPConfig>(m, "BPConfig")
+        .def(py::init<>())
+        .def(py::init<float, float, float, float>())
+        .def_readwrite("sfactor", &BPConfig::sfactor)
+        .def_readwrite("lrate", &BPConfig::lrate)
+        .def_readwrite("lrf", &BPConfig::lrf)
+        .def_readwrite("lamda", &BPConfig::lambda);
+
+    // bind.cpp:241-250: event lists on the device
+    py::class_<SparseTensor>(m, "SparseTensor")
+        .def(py::init<Tensor, F64>(), py::arg("tensor"), py::arg("threshold") = 0.0)
+        .def_property_readonly("numel", &SparseTensor::numel)
+        .def_property_readonly("dims", [](const SparseTensor &t) { return Size(t.shape.size()); })
+        .def_property_readonly("shape", [](const SparseTensor &t) { return t.shape; })
+        .def_property_readonly("capacity", &SparseTensor::capacity)
+        .def("__bool__", [](const SparseTensor &t) { return t.offsets.valid(); })
+        .def("dense", &SparseTensor::dense)
+        .def("sparsity", &SparseTensor::sparsity);
+
     py::class_<DoG>(m, "DoG")
         .def(py::init([](Size size, const std::vector<DoGFilter> &filters, Shape pad) {
             return DoG(size, filters, e4(pad));
         }))
         .def_readwrite("kernel", &DoG::kernel)
         .def("_forward", [](DoG &layer, Tensor input) { return layer(input); });
+
+    py::class_<Gabor>(m, "Gabor")
+        .def(py::init([](Size size, const std::vector<GaborFilter> &filters, Shape pad) {
+            return Gabor(size, filters, e4(pad));
+        }))
+        .def_readwrite("kernel", &Gabor::kernel)
+        .def("_forward", [](Gabor &layer, Tensor input) { return layer(input); });
+    py::class_<LoG>(m, "LoG")
+        .def(py::init([](Size size, const std::vector<F64> &stds, Shape pad) { return LoG(size, stds, e4(pad)); }))
+        .def_readwrite("kernel", &LoG::kernel)
+        .def("_forward", [](LoG &layer, Tensor input) { return layer(input); });
+
+    py::class_<FC>(m, "FC")
+        .def(py::init([](Size input, Size output, F64 mean, F64 std) { return FC(input, output, mean, std); }))
+        .def_readwrite("kernel", &FC::kernel)
+        .def_readwrite("stdpconfig", &FC::stdpconfig)
+        .def_readwrite("bpconfig", &FC::bpconfig)
+        .def("_forward", [](FC &layer, Tensor input, Tensor output, bool sign) { return layer(input, output, sign); })
+        .def("_stdp", [](FC &layer, Tensor input, const Winners &winners, Tensor output) {
+            layer.stdp(input, winners, output);
+        })
+        .def("_backward", [](FC &layer, Tensor input, Tensor output, Tensor grad, Tensor next) {
+            layer.backward(input, output, grad, next);
+        });
 
     py::class_<Conv>(m, "Conv")
         .def(py::init([](Size input, Size output, Shape kernel, Shape stride, Shape pad, F64 mean, F64 std) {
@@ -154,9 +204,11 @@ PYBIND11_MODULE(spyker_b200_plugin, m)
         .def("_forward", [](Conv &layer, Tensor input, Tensor output) {
             conv(input, layer.kernel, output, layer.stride(), layer.pad(), layer.precision);
         })
+        .def("_forward", [](Conv &layer, SparseTensor input, F64 threshold) { return layer(input, threshold); })
         .def("_stdp", [](Conv &layer, Tensor input, const Winners &winners, Tensor output) {
             layer.stdp(input, winners, output);
-        });
+        })
+        .def("_stdp", [](Conv &layer, SparseTensor input, const Winners &winners) { layer.stdp(input, winners); });
 
     // bind.cpp:365-392, the dense hot path
     m.def("conv", [](Tensor input, Tensor kernel, Tensor output, Shape stride, Shape pad) {
@@ -193,6 +245,36 @@ PYBIND11_MODULE(spyker_b200_plugin, m)
     m.def("convwta", [](Tensor input, Shape radius, Size count, F64 threshold) {
         return Spyker::convwta(input, e2(radius), count, threshold);
     });
+    m.def("fc", [](Tensor input, Tensor kernel, Tensor output, bool sign) { Spyker::fc(input, kernel, output, sign); });
+    m.def("scatter", [](Tensor input, Tensor output) {
+        detail::require(output.dims() >= 2, "Output dimensions must be at least 2.");
+        Tensor out = Spyker::scatter(input, output.shape(1), output.type());
+        detail::require(out.shape() == output.shape(), "Output shape is not compatible with the input.");
+        detail::cuda(cudaMemcpyAsync(output.data(), out.data(), out.bytes(), cudaMemcpyDeviceToDevice, stream()),
+                     "scatter");
+    });
+    m.def("backward", [](Tensor input, Tensor output, Tensor target, Size time, F64 gamma) {
+        Spyker::backward(input, output, target, time, gamma);
+    });
+    m.def("labelize", [](Tensor input, Tensor output, F64 threshold) { Spyker::labelize(input, output, threshold); });
+
+    // bind.cpp:396-407, the event-list path
+    py::module_ sp = m.def_submodule("sparse");
+    sp.def("conv", [](SparseTensor input, Tensor kernel, F64 threshold, Shape stride, Shape pad) {
+        return Sparse::conv(input, kernel, threshold, e2(stride), e4(pad));
+    });
+    sp.def("pad", [](SparseTensor input, Shape pad) { return Sparse::pad(input, e4(pad)); });
+    sp.def("code", [](Tensor input, Size time, bool sort) { return Sparse::code(input, time, sort); });
+    sp.def("gather", [](SparseTensor input, std::string type) { return Sparse::gather(input, str2type(type)); });
+    sp.def("pool", [](SparseTensor input, Shape kernel, Shape stride, Shape pad) {
+        return Sparse::pool(input, e2(kernel), stride.empty() ? Expand2(0) : e2(stride),
+                            pad.empty() ? Expand4(0) : e4(pad));
+    });
+    sp.def("inhibit", [](SparseTensor input) { return Sparse::inhibit(input); });
+    sp.def("convwta", [](SparseTensor input, Shape radius, Size count) {
+        return Sparse::convwta(input, e2(radius), count);
+    });
+
     // no counterpart in the plugin: the fused layer
     m.def("conv_fire_wta", [](Tensor input, Conv &layer, F64 threshold, Shape radius, Size count, Shape pool) {
         LayerOutput r = Spyker::conv_fire_wta(input, layer, threshold, e2(radius), count,

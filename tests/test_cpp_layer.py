@@ -125,12 +125,25 @@ def _plugin():
 
 
 def test_plugin_surface():
-    """The pybind11 module exposes the reference plugin's hot-path names."""
+    """The pybind11 module exposes the reference plugin's hot-path names
+    (bind.cpp:241-407): modules with their ``_forward`` / ``_stdp`` /
+    ``_backward`` methods, the free functions and the ``sparse`` submodule."""
     p = _plugin()
-    for name in ("Tensor", "tensor", "from_numpy", "Winner", "DoGFilter", "STDPConfig", "DoG", "Conv", "conv", "pad",
-                 "threshold", "code", "infinite", "fire", "gather", "pool", "inhibit", "fcwta", "convwta",
-                 "conv_fire_wta", "synchronize"):
+    for name in ("Tensor", "tensor", "from_numpy", "Winner", "DoGFilter", "GaborFilter", "STDPConfig", "BPConfig",
+                 "SparseTensor", "DoG", "Gabor", "LoG", "FC", "Conv", "conv", "fc", "pad", "threshold", "code",
+                 "infinite", "fire", "gather", "scatter", "pool", "inhibit", "fcwta", "convwta", "backward",
+                 "labelize", "conv_fire_wta", "synchronize", "sparse"):
         assert hasattr(p, name), name
+    for cls, methods in (("DoG", ["_forward"]), ("Gabor", ["_forward"]), ("LoG", ["_forward"]),
+                         ("FC", ["_forward", "_stdp", "_backward"]), ("Conv", ["_forward", "_stdp"]),
+                         ("SparseTensor", ["dense", "sparsity"])):
+        for meth in methods:
+            assert hasattr(getattr(p, cls), meth), f"{cls}.{meth}"
+    for name in ("conv", "pad", "code", "gather", "pool", "inhibit", "convwta"):
+        assert hasattr(p.sparse, name), f"sparse.{name}"
+    assert p.GaborFilter(2.0, 90.0, 0.5, 4.0, 0.0).theta == pytest.approx(np.pi / 2)
+    bp = p.BPConfig(1.0, 0.01, 0.1, 0.001)
+    assert (bp.sfactor, bp.lrf) == (1.0, pytest.approx(0.1))
 
 
 @pytest.mark.gpu
