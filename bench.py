@@ -468,27 +468,51 @@ def spike_match(spyker, torch, dev, precision, weights, n=32):
 # ----------------------------------------------------------------------------
 # CPU reference arm (the reference's own CPU backend)
 # ----------------------------------------------------------------------------
-def reference_step(o, torch, imgs, w1, w2, dk):
+def reference_step(o, torch, imgs, w1, w2, dk, ops=None):
     """The same pipeline with the reference's CPU code (oracle/_ref) and the
-    oneDNN convolution its CPU backend uses (through torch), in place."""
+    oneDNN convolution its CPU backend uses (through torch), in place.  With
+    a dict ``ops``, each op's wall time (s) is added under its name."""
+    clock = [time.perf_counter()]
+
+    def lap(name):
+        if ops is not None:
+            now = time.perf_counter()
+            ops[name] = ops.get(name, 0.0) + now - clock[0]
+            clock[0] = now
+
     x = imgs.astype(np.float32) / np.float32(255)
     dog = o.filter("dog", x[:, None], dk, (3, 3, 3, 3))
+    lap("dog")
     codes = o.rank_code(dog, T)
+    lap("code")
     b = codes.shape[0]
     f = torch.from_numpy(codes.reshape(b * T, 2, 28, 28).astype(np.float32))
     p1 = torch.nn.functional.conv2d(f, torch.from_numpy(w1), padding=2).numpy().reshape(b, T, 30, 28, 28)
+    lap("conv1")
     inh1 = o.inhibit(o.threshold(p1, 15.0))
+    lap("threshold+inhibit1")
     s1 = o.fire(inh1)
+    lap("fire1")
     win, cnt = o.convwta(inh1, (3, 3), 5)
+    lap("convwta1")
     w1[:] = o.convstdp(codes, w1, s1, [(0.004, -0.003, 1, 0, 1)], win, cnt, (1, 1), (2, 2, 2, 2))
+    lap("stdp1")
     q = o.pool(s1, (2, 2))
+    lap("pool1")
     f2 = torch.from_numpy(q.reshape(b * T, 30, 14, 14).astype(np.float32))
     p2 = torch.nn.functional.conv2d(f2, torch.from_numpy(w2), padding=2).numpy().reshape(b, T, 100, 14, 14)
+    lap("conv2")
     inh2 = o.inhibit(o.threshold(p2, 10.0))
+    lap("threshold+inhibit2")
     s2 = o.fire(inh2)
+    lap("fire2")
     win, cnt = o.convwta(inh2, (1, 1), 8)
+    lap("convwta2")
     w2[:] = o.convstdp(q, w2, s2, [(0.004, -0.003, 1, 0, 1)], win, cnt, (1, 1), (2, 2, 2, 2))
-    return o.pool(s2, (14, 14))
+    lap("stdp2")
+    out = o.pool(s2, (14, 14))
+    lap("pool2")
+    return out
 
 
 def load_synth():
@@ -534,13 +558,14 @@ def cpu_baseline(seconds: float) -> dict:
     imgs = synth.strokes(64, seed=5)
     w1, w2 = synth.conv_weights(30, 2, 5, seed=1), synth.conv_weights(100, 30, 5, seed=2)
     reference_step(o, torch, imgs, w1, w2, dk)
-    n, t0 = 0, time.perf_counter()
+    n, t0, ops = 0, time.perf_counter(), {}
     while time.perf_counter() - t0 < seconds:
-        reference_step(o, torch, imgs, w1, w2, dk)
+        reference_step(o, torch, imgs, w1, w2, dk, ops)
         n += 64
     dt = time.perf_counter() - t0
     return {"value": n / dt, "unit": "images/s", "cores": torch.get_num_threads(), "kind": kind, "cpu": cpu_model(),
-            "sample": f"{n} images in batches of 64 through the same 2-layer pipeline, {dt:.1f} s"}
+            "sample": f"{n} images in batches of 64 through the same 2-layer pipeline, {dt:.1f} s",
+            "ops_us_per_image": {k: round(v / n * 1e6, 2) for k, v in ops.items()}}
 
 
 def reference_arm(args, rank, world):
