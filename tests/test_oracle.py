@@ -179,3 +179,36 @@ def test_oracle_reports_errors(port):
         o = np.zeros((1, 2, 1, 5, 5), np.uint8)
         w = np.zeros((1, 1, 1, 1), np.float32)
         port.convstdp(x, w, o, CFG, np.array([[[3, 0, 0, 0, 0]]]), np.array([1]))
+
+
+def test_ties_and_boundaries(port, ref):
+    """The survey's parity hazards on crafted inputs: values exactly at the
+    threshold (threshold zeroes <=, fire is strict >), channels with equal
+    potentials (inhibit keeps the first, cpu/inhibit.cpp:59), WTA keys tied
+    across channels and positions (first index, cpu/wta.cpp:53-62,133),
+    one time step, odd map sizes for pooling; an empty batch on the
+    restatement (the reference build stops with a division by zero on
+    one)."""
+    rng = np.random.default_rng(21)
+    b, t, c, h, w = 3, 6, 4, 9, 7
+    base = rng.integers(0, 4, size=(b, t, 1, h, w)).astype(np.float32) * 2.5  # 0, 2.5, 5, 7.5
+    pot = np.repeat(base, c, axis=2)  # every channel tied
+    pot[:, :, 2] += (rng.random((b, t, h, w)) < 0.2) * 2.5  # some channel-2 wins
+    pot = np.cumsum(pot, axis=1).astype(np.float32)  # monotone in t, as potentials are
+    for thr in (5.0, 7.5, 10.0):
+        _eq(port.threshold(pot, thr), ref.threshold(pot, thr))
+        _eq(port.fire(pot, thr), ref.fire(pot, thr))
+    th = port.threshold(pot, 5.0)
+    _eq(port.inhibit(th), ref.inhibit(th))
+    _eq(port.inhibit(th, 10.0), ref.inhibit(th, 10.0))
+    for r, k in (((1, 1), 3), ((0, 0), 50), ((2, 3), 2)):
+        _eq(port.convwta(th, r, k), ref.convwta(th, r, k))
+        _eq(port.convwta(port.inhibit(th), r, k), ref.convwta(port.inhibit(th), r, k))
+    spk = port.fire(port.inhibit(th))
+    _eq(port.pool(spk, (2, 2)), ref.pool(spk, (2, 2)))
+    _eq(port.pool(spk, (3, 2), (2, 2), (0, 1, 1, 0)), ref.pool(spk, (3, 2), (2, 2), (0, 1, 1, 0)))
+    x = rng.random((4, 30)).astype(np.float32)
+    _eq(port.rank_code(x, 1), ref.rank_code(x, 1))
+    _eq(port.rank_code(x, 1, False), ref.rank_code(x, 1, False))
+    empty = np.zeros((0, t, c, h, w), np.float32)
+    assert port.threshold(empty, 1.0).shape == empty.shape and port.fire(empty, 1.0).shape == empty.shape
