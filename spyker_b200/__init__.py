@@ -8,7 +8,7 @@ runs on the GPU through the C ABI of ``include/spyker_b200.h``.
 """
 
 from . import control, io, sparse, temporal
-from ._lib import SpykerError
+from ._lib import SpykerError, set_nvtx
 from .control import (all_devices, clear_context, cuda_arch_list, cuda_cache_clear, cuda_cache_enable, cuda_cache_enabled,
                       cuda_cache_print, cuda_conv_force, cuda_conv_heuristic, cuda_conv_light, cuda_current_device,
                       cuda_device_arch, cuda_memory_free, cuda_memory_taken, cuda_memory_total, cuda_memory_used,

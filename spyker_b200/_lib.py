@@ -142,7 +142,27 @@ def check(status: int) -> None:
         raise SpykerError(lib.spk_last_error().decode())
 
 
+# NVTX ranges around every C-ABI call, named after the entry point (for
+# nsys timelines and `ncu --nvtx --nvtx-include`); off unless SPYKER_NVTX is
+# set to a non-zero value or set_nvtx(True) is called.  Without a profiler
+# attached a range costs a no-op call.
+_nvtx = os.environ.get("SPYKER_NVTX", "0") not in ("", "0")
+
+
+def set_nvtx(enabled: bool) -> None:
+    """Turn the per-call NVTX ranges on or off."""
+    global _nvtx
+    _nvtx = bool(enabled)
+
+
 def call(name: str, *args) -> None:
+    if _nvtx:
+        torch.cuda.nvtx.range_push(name)
+        try:
+            check(getattr(lib, name)(*args))
+        finally:
+            torch.cuda.nvtx.range_pop()
+        return
     check(getattr(lib, name)(*args))
 
 

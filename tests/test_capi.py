@@ -97,3 +97,26 @@ def test_shape_helpers():
     assert shape.pool([4, 15, 30, 28, 28], (2, 2), (2, 2), (1, 1, 1, 1)) == [4, 15, 30, 15, 15]
     with pytest.raises(ValueError):
         shape.conv([4, 15, 3, 28, 28], [30, 2, 5, 5], (1, 1), (0, 0, 0, 0))
+
+
+def test_nvtx_ranges_wrap_calls(port, monkeypatch):
+    """With the NVTX ranges on, every call is bracketed by one push and one
+    pop named after the entry point, also when the call fails; results are
+    unchanged."""
+    import torch
+
+    events = []
+    monkeypatch.setattr(torch.cuda.nvtx, "range_push", lambda n: events.append(("push", n)))
+    monkeypatch.setattr(torch.cuda.nvtx, "range_pop", lambda: events.append(("pop",)))
+    _lib.set_nvtx(True)
+    try:
+        k = np.zeros((7, 7))
+        _lib.call("spk_gaussian_kernel", k.ctypes.data, 7, 1.3)
+        assert np.array_equal(k, port.gaussian_kernel(7, 1.3))
+        with pytest.raises(_lib.SpykerError):
+            _lib.call("spk_rank_code", None, 9, None, 4, 1, 0, 10, 1, None, 0, None)
+    finally:
+        _lib.set_nvtx(False)
+    assert events == [("push", "spk_gaussian_kernel"), ("pop",), ("push", "spk_rank_code"), ("pop",)]
+    _lib.call("spk_gaussian_kernel", k.ctypes.data, 7, 1.3)
+    assert len(events) == 4
