@@ -459,6 +459,8 @@ inline Tensor pool(Tensor input, Tensor output, Expand2 kernel, Expand2 stride =
                     "Kernel, stride or pad items are incorrect.");
     Shape o = input.shape();
     const Size h = o[o.size() - 2], w = o[o.size() - 1];
+    detail::require(h + pad[0] + pad[2] >= kernel[0] && w + pad[1] + pad[3] >= kernel[1],
+                    "Input and kernel shapes are not compatible.");
     const Size oh = (h + pad[0] + pad[2] - kernel[0]) / stride[0] + 1;
     const Size ow = (w + pad[1] + pad[3] - kernel[1]) / stride[1] + 1;
     detail::require(oh > 0 && ow > 0, "Input and kernel shapes are not compatible.");
@@ -480,6 +482,8 @@ inline Tensor pool(Tensor input, Expand2 kernel, Expand2 stride = 0, Expand4 pad
                     "Kernel, stride or pad items are incorrect.");
     Shape o = input.shape();
     const Size h = o[o.size() - 2], w = o[o.size() - 1];
+    detail::require(h + pad[0] + pad[2] >= kernel[0] && w + pad[1] + pad[3] >= kernel[1],
+                    "Input and kernel shapes are not compatible.");
     const Size oh = (h + pad[0] + pad[2] - kernel[0]) / stride[0] + 1;
     const Size ow = (w + pad[1] + pad[3] - kernel[1]) / stride[1] + 1;
     detail::require(oh > 0 && ow > 0, "Input and kernel shapes are not compatible.");
@@ -552,6 +556,7 @@ inline Tensor conv(Tensor input, Tensor kernel, Tensor output, Expand2 stride = 
     const Size cin = s[d - 3], h = s[d - 2], w = s[d - 1];
     const Size cout = kernel.shape(0), kh = kernel.shape(2), kw = kernel.shape(3);
     detail::require(kernel.shape(1) == cin, "Input and kernel channels are not compatible.");
+    detail::require(h + pad[0] + pad[2] >= kh && w + pad[1] + pad[3] >= kw, "Input and kernel shapes are not compatible.");
     const Size oh = (h + pad[0] + pad[2] - kh) / stride[0] + 1, ow = (w + pad[1] + pad[3] - kw) / stride[1] + 1;
     detail::require(oh > 0 && ow > 0, "Input and kernel shapes are not compatible.");
     Shape o(s.begin(), s.end() - 3);
@@ -579,6 +584,7 @@ inline Tensor conv(Tensor input, Tensor kernel, Expand2 stride = 1, Expand4 pad 
     const Size cin = s[d - 3], h = s[d - 2], w = s[d - 1];
     const Size cout = kernel.shape(0), kh = kernel.shape(2), kw = kernel.shape(3);
     detail::require(kernel.shape(1) == cin, "Input and kernel channels are not compatible.");
+    detail::require(h + pad[0] + pad[2] >= kh && w + pad[1] + pad[3] >= kw, "Input and kernel shapes are not compatible.");
     const Size oh = (h + pad[0] + pad[2] - kh) / stride[0] + 1, ow = (w + pad[1] + pad[3] - kw) / stride[1] + 1;
     detail::require(oh > 0 && ow > 0, "Input and kernel shapes are not compatible.");
     Shape o(s.begin(), s.end() - 3);
@@ -943,6 +949,8 @@ inline SparseTensor pool(SparseTensor input, Expand2 kernel, Expand2 stride = 0,
                         pad[1] >= 0 && pad[2] >= 0 && pad[3] >= 0,
                     "Kernel, stride or pad items are incorrect.");
     const Shape &s = input.shape;
+    detail::require(s[3] + pad[0] + pad[2] >= kernel[0] && s[4] + pad[1] + pad[3] >= kernel[1],
+                    "Input and kernel shapes are not compatible.");
     const Size oh = (s[3] + pad[0] + pad[2] - kernel[0]) / stride[0] + 1;
     const Size ow = (s[4] + pad[1] + pad[3] - kernel[1]) / stride[1] + 1;
     detail::require(oh > 0 && ow > 0, "Input and kernel shapes are not compatible.");

@@ -475,6 +475,10 @@ spk_status spk_rank_pool(const void *in, void *out, spk_dtype type, int64_t n, i
     return guarded([&] {
         Pad4 p = pad_of(pad4);
         SPK_REQUIRE(ky >= 1 && kx >= 1 && sy >= 1 && sx >= 1, "kernel and stride must be at least 1");
+        // a window larger than the padded plane has no output (the staged
+        // kernels read whole windows inside the plane)
+        SPK_REQUIRE(h + p.top + p.bottom >= ky && w + p.left + p.right >= kx,
+                    "input and kernel shapes are not compatible");
         SPK_REQUIRE(oh == (h + p.top + p.bottom - ky) / sy + 1 && ow == (w + p.left + p.right - kx) / sx + 1,
                     "output shape is not compatible");
         SPK_REQUIRE(oh > 0 && ow > 0, "input and kernel shapes are not compatible");

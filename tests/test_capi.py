@@ -120,3 +120,15 @@ def test_nvtx_ranges_wrap_calls(port, monkeypatch):
     assert events == [("push", "spk_gaussian_kernel"), ("pop",), ("push", "spk_rank_code"), ("pop",)]
     _lib.call("spk_gaussian_kernel", k.ctypes.data, 7, 1.3)
     assert len(events) == 4
+
+
+def test_pool_window_larger_than_plane_is_refused():
+    """A window taller or wider than the padded plane has no output: refused
+    before any launch (C division would give one output row)."""
+    pad = _lib.i64(0, 0, 0, 0)
+    # h = 1 under a 2x2 window: (1 - 2) / 2 + 1 == 1 in C
+    st = _status("spk_rank_pool", C.c_void_p(16), C.c_void_p(16), 4, 1, 1, 8, 1, 4, 2, 2, 2, 2, pad, None)
+    assert st == 1 and b"not compatible" in _lib.lib.spk_last_error()
+    # the same plane padded to the window's height is fine up to the launch (n = 0: nothing runs)
+    st = _status("spk_rank_pool", None, None, 4, 0, 1, 8, 1, 4, 2, 2, 2, 2, _lib.i64(1, 0, 0, 0), None)
+    assert st == 0
