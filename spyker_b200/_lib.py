@@ -123,8 +123,9 @@ class SpykerError(RuntimeError):
 def _load() -> C.CDLL:
     if not os.path.exists(LIB_PATH):
         raise ImportError(
-            f"spyker_b200: the CUDA library {LIB_PATH} is not built; run `python -m spyker_b200.build` "
-            "(there is no CPU fallback)"
+            f"spyker_b200: the CUDA library {LIB_PATH} is not built; run "
+            f"`python {os.path.join(os.path.dirname(os.path.abspath(__file__)), 'build.py')}` "
+            "(a script: importing the package needs the library; there is no CPU fallback)"
         )
     lib = C.CDLL(LIB_PATH)
     for name, (res, args) in SIGNATURES.items():
